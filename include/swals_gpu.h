@@ -1,0 +1,191 @@
+/*
+ * swals_gpu.h -- C ABI of the B200 (sm_100a) implementation of the SWALS
+ * shallow-water time-step hot path.
+ *
+ * The reference (GeoscienceAustralia/ptha, propagation/SWALS) has no device
+ * boundary: Fortran type-bound procedures of domain_type / multidomain_type
+ * advance host arrays.  This header is the drop-in boundary a Fortran
+ * ISO_C_BINDING shim (or ctypes / any FFI) binds.  Every entry point names
+ * the reference interface it replaces, as file:line relative to
+ * propagation/SWALS/src/shallow_water/.
+ *
+ * Conventions
+ *  - Plain C types only; status is an int (SWALS_OK == 0).  The Fortran shim
+ *    maps a nonzero status to generic_stop (util/stop_mod.f90:7-33), which
+ *    keeps the reference's fatal-error semantics.
+ *  - Host arrays use the reference's Fortran column-major layout: U(i,j,k),
+ *    i fastest, leading dimensions nx then ny; k = STG(1), UH(2), VH(3), ELV(4)
+ *    (domain_mod.f90:79).  Element type is double, or float when the domain
+ *    was created with real_bytes = 4 (the -DREALFLOAT build).
+ *  - A handle owns one CUDA stream; calls on one handle are not thread-safe.
+ *    Stepping calls are stream-ordered and return without waiting; calls
+ *    that hand data back to the host synchronise the handle's stream.
+ *  - There is no CPU fallback: without a CUDA device, creation fails with
+ *    SWALS_ERR_NO_DEVICE.
+ */
+#ifndef SWALS_GPU_H
+#define SWALS_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+#define SWALS_OK                        0
+#define SWALS_ERR_INVALID_ARGUMENT      1
+#define SWALS_ERR_UNKNOWN_METHOD        2  /* timestepping_method string not one of SWALS's 8 */
+#define SWALS_ERR_UNSUPPORTED           3  /* valid SWALS option that this GPU path does not implement */
+#define SWALS_ERR_CUDA                  4
+#define SWALS_ERR_NONFINITE             5  /* NaN/Inf found by a stability check */
+#define SWALS_ERR_UNSUPPORTED_CALLBACK  6  /* host boundary/forcing procedure pointer given */
+#define SWALS_ERR_TIMESTEP_REQUIRED     7  /* staggered methods need an explicit timestep */
+#define SWALS_ERR_OUT_OF_MEMORY         8
+#define SWALS_ERR_NO_DEVICE             9
+#define SWALS_ERR_CAPACITY             10  /* a fixed-size buffer (e.g. gauge records) is full */
+
+/* ---- boundary conditions (boundary_mod.f90) ------------------------------ */
+#define SWALS_BC_NONE                              0 /* walls via high elevation, no routine */
+#define SWALS_BC_TRANSMISSIVE                      1 /* transmissive_boundary, boundary_mod.f90:21-75 */
+#define SWALS_BC_STAGE_TRANSMISSIVE_NORMAL_MOMENTUM 2 /* boundary_mod.f90:78-163 */
+
+/* Device-native boundary_function kinds (domain_mod.f90:594-633 interface). */
+#define SWALS_BF_NONE                   0
+#define SWALS_BF_SOLITARY_WEST_WALLS    1 /* params: H, depth, x0. West edge: stage = H sech^2(k(x-x0-ct)), elev = -depth;
+                                             other edges: stage = elev = wall_elevation. */
+
+/* friction_type (domain_mod.f90:178) */
+#define SWALS_FRICTION_MANNING 0
+#define SWALS_FRICTION_CHEZY   1
+
+typedef struct swals_domain_desc {
+    int32_t nx[2];                  /* domain%nx */
+    double  lw[2];                  /* domain%lw */
+    double  lower_left[2];          /* domain%lower_left */
+    char    timestepping_method[64];/* domain%timestepping_method, NUL-terminated */
+    double  cfl;                    /* domain%cfl; -DBL_MAX = method default */
+    double  theta;                  /* domain%theta; -DBL_MAX = method default */
+    double  msl_linear;             /* domain%msl_linear */
+    double  linear_friction_coeff;  /* domain%linear_friction_coeff */
+    double  maximum_timestep;       /* domain%maximum_timestep (default 1e20) */
+    int32_t linear_solver_is_truely_linear;
+    int32_t friction_type;          /* SWALS_FRICTION_* */
+    int32_t spherical;              /* compile-time -DSPHERICAL in the reference */
+    int32_t coriolis;               /* CORIOLIS: spherical and not -DNOCORIOLIS */
+    int32_t nofriction;             /* -DNOFRICTION */
+    int32_t real_bytes;             /* 8: FP64 state (default); 4: FP32 state (-DREALFLOAT) */
+    int32_t xL, xU, yL, yU;         /* domain%xL.. (1-based); 0 = 1/nx/1/ny */
+    int32_t boundary_exterior[4];   /* domain%boundary_exterior, order N,E,S,W */
+    int32_t boundary_kind;          /* SWALS_BC_* (domain%boundary_subroutine) */
+    int32_t boundary_function_kind; /* SWALS_BF_* (domain%boundary_function) */
+    double  boundary_function_params[8];
+    int32_t record_max_stage;       /* 'max_stage' in nontemporal_grids_to_store (default 1) */
+    int32_t exterior_cells_width;   /* domain%exterior_cells_width (default 2) */
+    int32_t has_host_boundary_subroutine; /* nonzero: a host callback was set -> rejected */
+    int32_t has_host_forcing_subroutine;  /* nonzero: a host callback was set -> rejected */
+    int32_t device;                 /* CUDA device ordinal; -1 = the calling thread's current device */
+} swals_domain_desc;
+
+typedef struct swals_domain_state {
+    double  time;                   /* domain%time */
+    double  max_dt;                 /* domain%max_dt */
+    double  dt_last_update;         /* domain%dt_last_update */
+    double  evolve_step_dt;         /* domain%evolve_step_dt */
+    int64_t nsteps_advanced;        /* domain%nsteps_advanced */
+    int64_t negative_depth_fix_counter; /* domain%negative_depth_fix_counter */
+    double  boundary_flux_store[4];         /* N,E,S,W of the last flux evaluation */
+    double  boundary_flux_evolve_integral;  /* last evolve_one_step */
+    double  boundary_flux_time_integral;    /* running total */
+} swals_domain_state;
+
+typedef struct swals_domain swals_domain;  /* opaque */
+
+/* Fills *desc with domain_type's initial values (domain_mod.f90:142-220). */
+int swals_gpu_desc_init(swals_domain_desc *desc);
+
+/* domain%allocate_quantities (domain_mod.f90:852-1358) on the device. */
+int swals_gpu_domain_create(const swals_domain_desc *desc, swals_domain **out);
+int swals_gpu_domain_destroy(swals_domain *d);
+
+/* domain%U = host U (column-major nx*ny*4), and the reverse. */
+int swals_gpu_upload_U(swals_domain *d, const void *U_host);
+int swals_gpu_download_U(swals_domain *d, void *U_host);
+/* One variable (k = 1..4) as an (nx,ny) column-major host array. */
+int swals_gpu_upload_var(swals_domain *d, int32_t k, const void *host);
+int swals_gpu_download_var(swals_domain *d, int32_t k, void *host);
+/* domain%manning_squared (domain_mod.f90:1179-1188), (nx,ny) column-major. */
+int swals_gpu_upload_manning_squared(swals_domain *d, const void *host);
+
+/* Geometry arrays of allocate_quantities (domain_mod.f90:925-1014), computed
+ * on the host at creation.  Lengths: x nx, y ny, dxb ny+1, dyl nx+1, area ny,
+ * coriolis ny, coriolis_bottom_edge ny+1, tanlat_on_radius_earth ny.
+ * upload_metrics lets a Fortran caller pass its own arrays instead. */
+int swals_gpu_get_metrics(swals_domain *d, double *x, double *y, double *dxb, double *dyl,
+                          double *area, double *coriolis, double *coriolis_bottom_edge,
+                          double *tanlat_on_radius_earth);
+int swals_gpu_upload_metrics(swals_domain *d, const double *dxb, const double *dyl,
+                             const double *area, const double *coriolis,
+                             const double *coriolis_bottom_edge, const double *tanlat_on_radius_earth);
+
+/* domain%evolve_one_step([timestep]) (domain_mod.f90:1679-1813).
+ * has_timestep == 0 selects adaptive (CFL) stepping for the FV methods. */
+int swals_gpu_evolve_one_step(swals_domain *d, double timestep, int32_t has_timestep);
+/* nsteps repeated evolve_one_step calls, launched back to back (no host sync). */
+int swals_gpu_evolve_steps(swals_domain *d, int32_t nsteps, double timestep, int32_t has_timestep);
+
+int swals_gpu_get_state(swals_domain *d, swals_domain_state *st);
+int swals_gpu_set_time(swals_domain *d, double time);      /* domain%time = time */
+int swals_gpu_synchronize(swals_domain *d);
+
+/* domain%max_U(:,:,1) ('max_stage'), column-major (nx,ny). */
+int swals_gpu_download_max_stage(swals_domain *d, void *host);
+
+/* domain%linear_timestep_max / nonlinear_stationary_timestep_max /
+ * stationary_timestep_max (domain_mod.f90:1906-2022). */
+int swals_gpu_linear_timestep_max(swals_domain *d, double *out);
+int swals_gpu_nonlinear_stationary_timestep_max(swals_domain *d, double *out);
+int swals_gpu_stationary_timestep_max(swals_domain *d, double *out);
+
+/* domain%volume_interior (domain_mod.f90:1815-1849), FP64, row order fixed. */
+int swals_gpu_volume_interior(swals_domain *d, double *out);
+
+/* Point gauges (point_gauge_mod.f90:208-245,336-340).  xy is (2,n)
+ * column-major (x1,y1,x2,y2,...).  After setup, every evolve_one_step appends
+ * [STG,UH,VH] at each site to a device buffer of `capacity` records;
+ * read returns records * n * 3 values (record-major, then gauge, then var). */
+int swals_gpu_gauges_setup(swals_domain *d, const double *xy, int32_t n, int32_t capacity);
+int swals_gpu_gauges_site_index(swals_domain *d, int32_t *site_index_1based);
+int swals_gpu_gauges_read(swals_domain *d, double *out, int32_t max_records, int32_t *n_records);
+int swals_gpu_gauges_reset(swals_domain *d);
+
+/* Per-kernel CUDA-event timers, the device analogue of the reference's
+ * EVOLVE_TIMER sections (domain_mod.f90:10-17).  While enabled, every kernel
+ * launch of a step is bracketed by events on the handle's stream.
+ * timers_read synchronises and writes, for each category c < n/2,
+ * ms_out[2c] = total milliseconds and ms_out[2c+1] = number of launches;
+ * categories: 0 CFL pre-pass, 1 FV stage 1, 2 boundary after stage 1,
+ * 3 FV stage 2 (+rk2 average), 4 boundary after stage 2, 5 step finalise,
+ * 6 leapfrog edge/boundary, 7 leapfrog fused step, 8 gauges, 9 max_stage. */
+#define SWALS_TIMER_CATEGORIES 10
+int swals_gpu_timers_enable(swals_domain *d, int32_t enable);
+int swals_gpu_timers_read(swals_domain *d, double *ms_out, int32_t n, int32_t *n_written);
+/* Number of kernels this handle has launched since creation. */
+int swals_gpu_launch_count(swals_domain *d, int64_t *count);
+
+/* The handle's CUDA stream (cudaStream_t) and device pointers, for callers
+ * that keep data on the device (the PyTorch harness). */
+int swals_gpu_stream(swals_domain *d, void **stream_out);
+int swals_gpu_device_planes(swals_domain *d, void **stg, void **uh, void **vh, void **elv,
+                            int64_t *pitch_elems);
+
+/* Last error message of this thread (util/stop_mod.f90 prints before stopping). */
+int swals_gpu_last_error(char *buf, size_t len);
+/* Library version string. */
+const char *swals_gpu_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

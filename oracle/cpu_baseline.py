@@ -1,0 +1,64 @@
+"""Test infrastructure: time the CPU oracle (the restatement of SWALS's
+OpenMP loops) on a bounded sample of a benchmark workload.
+
+Used only by bench.py's cpu_baseline leg and its `--impl reference` arm.
+Runs in its own process so the oracle's OpenMP runtime never shares a
+process with the GPU runtime.  Prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="rk2_beach")
+    ap.add_argument("--min-seconds", type=float, default=10.0)
+    ap.add_argument("--max-steps", type=int, default=1000)
+    ap.add_argument("--exact-steps", type=int, default=0)
+    args = ap.parse_args()
+    from ptha_b200 import workloads
+    from tests.pairs import oracle_from_kw
+    if args.workload == "rk2_beach":
+        kw, U, gauges, nsq = workloads.rk2_beach()
+        o = oracle_from_kw(kw)
+        o.U[:] = U
+        o.manning_squared[:] = nsq
+        dt = None
+    elif args.workload == "linear_gaussian_basin":
+        kw, U, gauges = workloads.linear_gaussian_basin()
+        o = oracle_from_kw(kw)
+        o.U[:] = U
+        dt = o.linear_timestep_max()
+    else:
+        raise SystemExit(f"unknown workload {args.workload}")
+    nx, ny = kw["nx"]
+    o.evolve_one_step(dt)  # untimed first step (page-in, thread start)
+    steps = 0
+    t0 = time.perf_counter()
+    while True:
+        o.evolve_one_step(dt)
+        steps += 1
+        el = time.perf_counter() - t0
+        if args.exact_steps:
+            if steps >= args.exact_steps:
+                break
+        elif el >= args.min_seconds or steps >= args.max_steps:
+            break
+    el = time.perf_counter() - t0
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    print(json.dumps({"value": nx * ny * steps / el, "unit": "cell-updates/s", "cores": threads,
+                      "steps": steps, "seconds": el, "cells": nx * ny,
+                      "sample": f"{args.workload} {nx}x{ny}: {steps} timesteps after 1 untimed"}))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,225 @@
+"""Test infrastructure only: ctypes wrapper around the C oracle (swals_oracle.c).
+
+The oracle is the CPU restatement of SWALS's time-step hot path that the CUDA
+implementation is checked against.  Only tests, the smoke check and the CPU
+baseline leg of bench.py may import this module.
+
+Arrays are numpy arrays in the reference's Fortran layout: ``U`` has shape
+``(4, ny, nx)`` here, i.e. C-order planes ``U[k-1, j-1, i-1]`` equal to the
+reference's column-major ``U(i, j, k)`` (i fastest in memory in both).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+METHODS = {
+    "rk2": 1, "rk2n": 2, "midpoint": 3, "euler": 4, "linear": 5,
+    "leapfrog_linear_plus_nonlinear_friction": 6, "cliffs": 7, "leapfrog_nonlinear": 8,
+}
+BC_NONE, BC_TRANSMISSIVE, BC_STAGE_TRANSMISSIVE_NORMAL_MOMENTUM = 0, 1, 2
+BF_SOLITARY_WEST_WALLS = 1
+NEG_HUGE = -np.finfo(np.float64).max
+
+
+def build():
+    """Compile both oracle variants (idempotent)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def _load(real32: bool):
+    name = "liboracle32.so" if real32 else "liboracle64.so"
+    path = os.path.join(HERE, name)
+    if not os.path.exists(path):
+        build()
+    return ctypes.CDLL(path)
+
+
+class _OracleDomainC(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int32), ("ny", ctypes.c_int32),
+        ("lw", ctypes.c_double * 2), ("lower_left", ctypes.c_double * 2),
+        ("method", ctypes.c_int32), ("spherical", ctypes.c_int32), ("coriolis", ctypes.c_int32),
+        ("nofriction", ctypes.c_int32), ("truely_linear", ctypes.c_int32), ("friction_chezy", ctypes.c_int32),
+        ("xL", ctypes.c_int32), ("xU", ctypes.c_int32), ("yL", ctypes.c_int32), ("yU", ctypes.c_int32),
+        ("exterior_cells_width", ctypes.c_int32), ("boundary_exterior", ctypes.c_int32 * 4),
+        ("bc_kind", ctypes.c_int32), ("bf_kind", ctypes.c_int32), ("record_max_stage", ctypes.c_int32),
+        ("pad0", ctypes.c_int32),
+        ("theta", ctypes.c_double), ("cfl", ctypes.c_double), ("msl_linear", ctypes.c_double),
+        ("linear_friction_coeff", ctypes.c_double), ("maximum_timestep", ctypes.c_double),
+        ("bf_params", ctypes.c_double * 8),
+        ("time", ctypes.c_double), ("max_dt", ctypes.c_double), ("dt_last_update", ctypes.c_double),
+        ("evolve_step_dt", ctypes.c_double),
+        ("nsteps_advanced", ctypes.c_int64), ("negative_depth_fix_counter", ctypes.c_int64),
+        ("boundary_flux_store", ctypes.c_double * 4),
+        ("boundary_flux_evolve_integral", ctypes.c_double),
+        ("boundary_flux_time_integral", ctypes.c_double),
+        ("U", ctypes.c_void_p), ("max_stage", ctypes.c_void_p), ("manning_squared", ctypes.c_void_p),
+        ("x", ctypes.c_void_p), ("y", ctypes.c_void_p), ("dxb", ctypes.c_void_p), ("dyl", ctypes.c_void_p),
+        ("area", ctypes.c_void_p), ("coriolis_c", ctypes.c_void_p), ("coriolis_be", ctypes.c_void_p),
+        ("tanlat_on_R", ctypes.c_void_p),
+        ("depth", ctypes.c_void_p), ("velocity", ctypes.c_void_p), ("flux_NS", ctypes.c_void_p),
+        ("flux_EW", ctypes.c_void_p), ("explicit_source", ctypes.c_void_p),
+        ("explicit_source_VH_j_minus_1", ctypes.c_void_p), ("backup_U", ctypes.c_void_p),
+    ]
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class OracleDomain:
+    """One SWALS ``domain_type`` restated on the CPU (test checker)."""
+
+    def __init__(self, nx, ny, lw, lower_left=(0.0, 0.0), timestepping_method="linear",
+                 spherical=False, coriolis=None, nofriction=False, truely_linear=True,
+                 friction_type="manning", cfl=None, theta=None, msl_linear=0.0,
+                 linear_friction_coeff=0.0, maximum_timestep=1.0e20,
+                 boundary_exterior=(True, True, True, True), bc_kind=BC_NONE,
+                 bf_kind=0, bf_params=(), record_max_stage=True, real32=False,
+                 xL=0, xU=0, yL=0, yU=0):
+        self.real32 = real32
+        self.dtype = np.float32 if real32 else np.float64
+        self.lib = _load(real32)
+        self.pref = "oracle32_" if real32 else "oracle64_"
+        if coriolis is None:
+            coriolis = bool(spherical)
+        c = _OracleDomainC()
+        c.nx, c.ny = nx, ny
+        c.lw[0], c.lw[1] = lw
+        c.lower_left[0], c.lower_left[1] = lower_left
+        c.method = METHODS[timestepping_method]
+        c.spherical, c.coriolis, c.nofriction = int(spherical), int(coriolis), int(nofriction)
+        c.truely_linear = int(truely_linear)
+        c.friction_chezy = int(friction_type == "chezy")
+        c.xL, c.xU, c.yL, c.yU = xL, xU, yL, yU
+        c.exterior_cells_width = 2
+        for k in range(4):
+            c.boundary_exterior[k] = int(boundary_exterior[k])
+        c.bc_kind, c.bf_kind = bc_kind, bf_kind
+        for k, v in enumerate(bf_params):
+            c.bf_params[k] = v
+        c.record_max_stage = int(record_max_stage)
+        c.theta = NEG_HUGE if theta is None else theta
+        c.cfl = NEG_HUGE if cfl is None else cfl
+        c.msl_linear = msl_linear
+        c.linear_friction_coeff = linear_friction_coeff
+        c.maximum_timestep = maximum_timestep
+        self.c = c
+        dt = self.dtype
+        self.U = np.zeros((4, ny, nx), dtype=dt)
+        # -0.99 * huge(real(1.0, output_precision)) evaluated in float32 (domain_mod.f90:1108)
+        init = np.float32(-0.99) * np.finfo(np.float32).max
+        self.max_stage = np.full((ny, nx), init, dtype=dt)
+        self.manning_squared = np.zeros((ny, nx), dtype=dt)
+        self.x = np.zeros(nx, dt); self.y = np.zeros(ny, dt)
+        self.dxb = np.zeros(ny + 1, dt); self.dyl = np.zeros(nx + 1, dt)
+        self.area = np.zeros(ny, dt); self.coriolis_c = np.zeros(ny, dt)
+        self.coriolis_be = np.zeros(ny + 1, dt); self.tanlat_on_R = np.zeros(ny, dt)
+        self.depth = np.zeros((ny, nx), dt)
+        self.velocity = np.zeros((2, ny, nx), dt)
+        self.flux_NS = np.zeros((3, ny + 1, nx), dt)
+        self.flux_EW = np.zeros((3, ny, nx + 1), dt)
+        self.explicit_source = np.zeros((2, ny, nx), np.float64)
+        self.es_jm1 = np.zeros((ny + 1, nx), np.float64)
+        self.backup_U = np.zeros((3, ny, nx), dt)
+        for name, arr in [("U", self.U), ("max_stage", self.max_stage), ("manning_squared", self.manning_squared),
+                          ("x", self.x), ("y", self.y), ("dxb", self.dxb), ("dyl", self.dyl), ("area", self.area),
+                          ("coriolis_c", self.coriolis_c), ("coriolis_be", self.coriolis_be),
+                          ("tanlat_on_R", self.tanlat_on_R), ("depth", self.depth), ("velocity", self.velocity),
+                          ("flux_NS", self.flux_NS), ("flux_EW", self.flux_EW),
+                          ("explicit_source", self.explicit_source),
+                          ("explicit_source_VH_j_minus_1", self.es_jm1), ("backup_U", self.backup_U)]:
+            setattr(c, name, _ptr(arr))
+        self._fn("apply_method_defaults")(ctypes.byref(c))
+        self._fn("setup_geometry")(ctypes.byref(c))
+
+    def _fn(self, name, restype=None):
+        f = getattr(self.lib, self.pref + name)
+        f.restype = restype
+        return f
+
+    # --- reference-named API -------------------------------------------
+    def evolve_one_step(self, timestep=None):
+        f = self._fn("evolve_one_step", ctypes.c_int)
+        f.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
+        rc = f(ctypes.addressof(self.c), 0.0 if timestep is None else float(timestep), 0 if timestep is None else 1)
+        if rc != 0:
+            raise RuntimeError(f"oracle evolve_one_step failed rc={rc}")
+
+    def linear_timestep_max(self):
+        f = self._fn("linear_timestep_max", ctypes.c_double)
+        f.argtypes = [ctypes.c_void_p]
+        return f(ctypes.addressof(self.c))
+
+    def nonlinear_stationary_timestep_max(self):
+        f = self._fn("nonlinear_stationary_timestep_max", ctypes.c_double)
+        f.argtypes = [ctypes.c_void_p]
+        return f(ctypes.addressof(self.c))
+
+    def volume_interior(self):
+        f = self._fn("volume_interior", ctypes.c_double)
+        f.argtypes = [ctypes.c_void_p]
+        return f(ctypes.addressof(self.c))
+
+    @property
+    def time(self):
+        return self.c.time
+
+    @property
+    def max_dt(self):
+        return self.c.max_dt
+
+    @property
+    def nsteps_advanced(self):
+        return self.c.nsteps_advanced
+
+    @property
+    def negative_depth_fix_counter(self):
+        return self.c.negative_depth_fix_counter
+
+    @property
+    def theta(self):
+        return self.c.theta
+
+    @property
+    def cfl(self):
+        return self.c.cfl
+
+
+def limited_gradient_dx(U_local, U_lower, U_upper, theta, real32=False):
+    """MC limiter of extrapolation_limiting_mod.f90:44-79 (vectorised form)."""
+    dt = np.float32 if real32 else np.float64
+    lib = _load(real32)
+    f = getattr(lib, ("oracle32_" if real32 else "oracle64_") + "limited_gradient_dx_vectorized")
+    f.restype = None
+    arrs = [np.ascontiguousarray(a, dtype=dt) for a in (U_local, U_lower, U_upper, theta)]
+    out = np.zeros_like(arrs[0])
+    f(*[_ptr(a) for a in arrs], _ptr(out), ctypes.c_int32(len(out)))
+    return out
+
+
+def area_lonlat_rectangle(lon1, lat1, dlon, dlat, flat=False):
+    lib = _load(False)
+    f = lib.oracle64_area_lonlat_rectangle
+    f.restype = ctypes.c_double
+    f.argtypes = [ctypes.c_double] * 4 + [ctypes.c_int]
+    return f(lon1, lat1, dlon, dlat, int(flat))
+
+
+def gauge_site_index(xy, ll, dx, nxy):
+    """point_gauge_mod.f90:336-340; returns 1-based (n,2) indices."""
+    lib = _load(False)
+    xy = np.ascontiguousarray(xy, dtype=np.float64)
+    n = xy.shape[0]
+    out = np.zeros((n, 2), dtype=np.int32)
+    f = lib.oracle64_gauge_site_index
+    f.restype = None
+    f(_ptr(xy), ctypes.c_int32(n), _ptr(np.asarray(ll, np.float64)), _ptr(np.asarray(dx, np.float64)),
+      _ptr(np.asarray(nxy, np.int32)), _ptr(out))
+    return out

@@ -1,0 +1,913 @@
+/*
+ * swals_oracle.c -- TEST INFRASTRUCTURE ONLY (the checker, never the product).
+ *
+ * IEEE-strict C restatement of the SWALS time-step hot path.  Each routine
+ * cites the reference routine it restates (paths relative to
+ * propagation/SWALS/src/shallow_water/ in GeoscienceAustralia/ptha).
+ * Built with -O2 -fno-fast-math -ffp-contract=off so that every operation is
+ * a single correctly rounded IEEE operation, in the reference's source order.
+ *
+ * The loops are written the way the reference writes them (1-based, column
+ * major, row-by-row with per-row work arrays).  Where the reference uses
+ * hand-made OpenMP chunking only to avoid copying old values (the Coriolis
+ * terms of the linear solver), this restatement copies the old values
+ * instead; the arithmetic is unchanged.
+ */
+#include "swals_oracle.h"
+
+#include <math.h>
+#include <float.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* global_mod.f90:37-55 */
+#define GRAVITY ((REAL)9.8)
+#define ADVECTION_BETA ((REAL)1.0)
+#define RADIUS_EARTH ((REAL)6371000.0)
+#define MINIMUM_ALLOWED_DEPTH ((REAL)1.0e-05)
+#define WALL_ELEVATION ((REAL)1.0e+6)
+#define HALF ((REAL)0.5)
+#ifdef ORACLE_REAL32
+#define RPOW powf
+#else
+#define RPOW pow
+#endif
+#define ZERO ((REAL)0.0)
+#define ONE ((REAL)1.0)
+/* domain_mod.f90:111-117 */
+#define LIMITER_COEF1 ((REAL)0.1)
+#define LIMITER_COEF2 ((REAL)0.3)
+#define LIMITER_COEF3 ((REAL)100.0)
+/* spherical_mod.f90:9-17 */
+#define EARTH_ANGULAR_FREQ ((REAL)7.292115e-05)
+
+static REAL or_pi(void) { return (REAL)acos((REAL)-1.0); }
+static REAL or_deg2rad(void) { return or_pi() / (REAL)180.0; }
+static REAL limiter_coef4(void) { return ONE / (LIMITER_COEF2 - LIMITER_COEF1); }
+
+static inline REAL rmin(REAL a, REAL b) { return (b < a) ? b : a; }
+static inline REAL rmax(REAL a, REAL b) { return (b > a) ? b : a; }
+static inline double dmin(double a, double b) { return (b < a) ? b : a; }
+static inline double dmax(double a, double b) { return (b > a) ? b : a; }
+
+/* 1-based column-major indexing */
+#define IDX(i, j) ((size_t)((i) - 1) + (size_t)((j) - 1) * (size_t)nx)
+#define UU(k, i, j) d->U[(size_t)((k) - 1) * (size_t)nx * (size_t)ny + IDX(i, j)]
+
+/* ------------------------------------------------------------------------ */
+/* allocate_quantities defaults (domain_mod.f90:880-890; timestepping_metadata_mod.f90:135-232) */
+void ORACLE_FN(apply_method_defaults)(oracle_domain *d)
+{
+    double def_cfl = -1.0, def_theta = -1.0;
+    switch (d->method) {
+    case OR_METHOD_RK2: def_cfl = 0.99; def_theta = 1.6; break;
+    case OR_METHOD_RK2N: def_cfl = 0.99; def_theta = 1.6; break;
+    case OR_METHOD_MIDPOINT: def_cfl = 0.99; def_theta = 1.6; break;
+    case OR_METHOD_EULER: def_cfl = 0.9; def_theta = 0.9; break;
+    default: def_cfl = 0.7; def_theta = -1.0; break;
+    }
+    if (d->cfl == -DBL_MAX) d->cfl = (REAL)def_cfl;
+    if (d->theta == -DBL_MAX) d->theta = (REAL)def_theta;
+    if (d->maximum_timestep <= 0.0) d->maximum_timestep = (REAL)1.0e+20;
+    if (d->xL <= 0) d->xL = 1;
+    if (d->yL <= 0) d->yL = 1;
+    if (d->xU <= 0) d->xU = d->nx;
+    if (d->yU <= 0) d->yU = d->ny;
+    if (d->exterior_cells_width <= 0) d->exterior_cells_width = 2;
+}
+
+/* Geometry: domain_mod.f90:925-1014, spherical_mod.f90:20-62 */
+double ORACLE_FN(area_lonlat_rectangle)(double lon1, double lat1, double dlon, double dlat, int flat)
+{
+    REAL deg2rad = or_deg2rad();
+    if (flat) {
+        REAL lat1r = (REAL)lat1, dlatr = (REAL)dlat, dlonr = (REAL)dlon;
+        REAL a = RADIUS_EARTH * RADIUS_EARTH;
+        a = a * (REAL)cos((lat1r + (REAL)0.5 * dlatr) * deg2rad);
+        a = a * (REAL)fabs(dlatr);
+        a = a * deg2rad;
+        a = a * (REAL)fmod(fabs(dlonr), (REAL)360.0);
+        a = a * deg2rad;
+        return a;
+    } else {
+        double d2r = (double)deg2rad;
+        double sin1 = sin(lat1 * d2r);
+        double sin2 = sin((lat1 + dlat) * d2r);
+        REAL a = RADIUS_EARTH * RADIUS_EARTH;
+        double r = (double)a * fabs(sin1 - sin2);
+        REAL rr = (REAL)r;
+        rr = rr * (REAL)fmod(fabs((REAL)dlon), (REAL)360.0);
+        rr = rr * deg2rad;
+        return rr;
+    }
+}
+
+void ORACLE_FN(setup_geometry)(oracle_domain *d)
+{
+    const int nx = d->nx, ny = d->ny;
+    REAL dx1 = (REAL)d->lw[0] / ((REAL)nx * ONE);
+    REAL dx2 = (REAL)d->lw[1] / ((REAL)ny * ONE);
+    REAL deg2rad = or_deg2rad();
+    for (int i = 1; i <= nx; i++)
+        d->x[i - 1] = (REAL)d->lower_left[0] + (((REAL)i - HALF) / ((REAL)nx * ONE)) * (REAL)d->lw[0];
+    for (int i = 1; i <= ny; i++)
+        d->y[i - 1] = (REAL)d->lower_left[1] + (((REAL)i - HALF) / ((REAL)ny * ONE)) * (REAL)d->lw[1];
+    if (d->spherical) {
+        for (int i = 1; i <= ny; i++) {
+            d->tanlat_on_R[i - 1] = (REAL)tan(d->y[i - 1] * deg2rad) / RADIUS_EARTH;
+        }
+        if (d->coriolis) {
+            for (int i = 1; i <= ny; i++) {
+                d->coriolis_c[i - 1] = ((REAL)2.0 * (REAL)sin(d->y[i - 1] * deg2rad)) * EARTH_ANGULAR_FREQ;
+                d->coriolis_be[i - 1] = ((REAL)2.0 * EARTH_ANGULAR_FREQ) *
+                    (REAL)sin((d->y[i - 1] - HALF * dx2) * deg2rad);
+            }
+            d->coriolis_be[ny] = ((REAL)2.0 * EARTH_ANGULAR_FREQ) *
+                (REAL)sin((d->y[ny - 1] + HALF * dx2) * deg2rad);
+        } else {
+            for (int i = 0; i < ny; i++) d->coriolis_c[i] = ZERO;
+            for (int i = 0; i <= ny; i++) d->coriolis_be[i] = ZERO;
+        }
+        for (int i = 1; i <= nx + 1; i++) d->dyl[i - 1] = (dx2 * deg2rad) * RADIUS_EARTH;
+        for (int i = 1; i <= ny + 1; i++) {
+            REAL coslat_be;
+            if (i <= ny) coslat_be = (REAL)cos((d->y[i - 1] - HALF * dx2) * deg2rad);
+            else coslat_be = (REAL)cos((d->y[ny - 1] + HALF * dx2) * deg2rad);
+            d->dxb[i - 1] = ((dx1 * deg2rad) * RADIUS_EARTH) * coslat_be;
+        }
+        for (int i = 1; i <= ny; i++)
+            d->area[i - 1] = (REAL)ORACLE_FN(area_lonlat_rectangle)(
+                d->x[0] - dx1 * HALF, d->y[i - 1] - dx2 * HALF, dx1, dx2, 1);
+    } else {
+        for (int i = 0; i < ny; i++) { d->tanlat_on_R[i] = ZERO; d->coriolis_c[i] = ZERO; }
+        for (int i = 0; i <= ny; i++) d->coriolis_be[i] = ZERO;
+        for (int i = 1; i <= nx + 1; i++) d->dyl[i - 1] = dx2;
+        for (int i = 1; i <= ny + 1; i++) d->dxb[i - 1] = dx1;
+        for (int i = 1; i <= ny; i++) d->area[i - 1] = dx1 * dx2;
+    }
+}
+
+/* point_gauge_mod.f90:336-340: site = 1 + min(floor((xy-ll)/dx), nx-1) */
+void ORACLE_FN(gauge_site_index)(const double *xy, int32_t n, const double *ll,
+        const double *dx, const int32_t *nxy, int32_t *site_index)
+{
+    for (int g = 0; g < n; g++) {
+        for (int k = 0; k < 2; k++) {
+            REAL q = ((REAL)xy[2 * g + k] - (REAL)ll[k]) / (REAL)dx[k];
+            int32_t f = (int32_t)floor(q);
+            if (nxy[k] - 1 < f) f = nxy[k] - 1;
+            site_index[2 * g + k] = 1 + f;
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Boundary conditions (boundary_mod.f90) */
+
+void ORACLE_FN(boundary_function)(const oracle_domain *d, double t, int32_t i, int32_t j, REAL *out)
+{
+    (void)j;
+    if (d->bf_kind == OR_BF_SOLITARY_WEST_WALLS) {
+        /* params: H, depth, x0 (crest position at t=0) */
+        REAL H = (REAL)d->bf_params[0], dep = (REAL)d->bf_params[1], x0 = (REAL)d->bf_params[2];
+        if (i == 1) {
+            REAL k = (REAL)sqrt((REAL)3.0 * H / ((REAL)4.0 * dep * dep * dep));
+            REAL c = (REAL)sqrt(GRAVITY * (dep + H));
+            REAL arg = k * (d->x[0] - x0 - c * (REAL)t);
+            REAL ch = (REAL)cosh(arg);
+            out[0] = H / (ch * ch);
+            out[1] = ZERO; out[2] = ZERO; out[3] = -dep;
+        } else {
+            out[0] = WALL_ELEVATION; out[1] = ZERO; out[2] = ZERO; out[3] = WALL_ELEVATION;
+        }
+    } else {
+        out[0] = ZERO; out[1] = ZERO; out[2] = ZERO; out[3] = ZERO;
+    }
+}
+
+static int is_staggered(const oracle_domain *d)
+{
+    return d->method == OR_METHOD_LINEAR || d->method == OR_METHOD_LEAPFROG_LINEAR_PLUS_NONLINEAR_FRICTION ||
+           d->method == OR_METHOD_LEAPFROG_NONLINEAR;
+}
+
+static void update_boundary(oracle_domain *d)
+{
+    const int nx = d->nx, ny = d->ny;
+    if (d->bc_kind == OR_BC_TRANSMISSIVE) {
+        /* boundary_mod.f90:41-73 */
+        for (int k = 1; k <= 4; k++)
+            for (int j = 1; j <= ny; j++) {
+                if (d->boundary_exterior[3]) UU(k, 1, j) = UU(k, 2, j);
+                if (d->boundary_exterior[1]) UU(k, nx, j) = UU(k, nx - 1, j);
+            }
+        for (int k = 1; k <= 4; k++)
+            for (int i = 1; i <= nx; i++) {
+                if (d->boundary_exterior[2]) UU(k, i, 1) = UU(k, i, 2);
+                if (d->boundary_exterior[0]) UU(k, i, ny) = UU(k, i, ny - 1);
+            }
+    } else if (d->bc_kind == OR_BC_STAGE_TRANSMISSIVE_NORMAL_MOMENTUM) {
+        /* boundary_mod.f90:94-161 */
+        int stag = is_staggered(d);
+        REAL bc[4];
+        for (int j = 1; j <= ny; j++) {
+            if (d->boundary_exterior[3]) {
+                int i = 1;
+                ORACLE_FN(boundary_function)(d, d->time, i, j, bc);
+                UU(OR_STG, i, j) = bc[0];
+                UU(OR_ELV, i, j) = bc[3];
+                if (!stag) { UU(OR_UH, i, j) = UU(OR_UH, i + 1, j); UU(OR_VH, i, j) = ZERO; }
+            }
+            if (d->boundary_exterior[1]) {
+                int i = nx;
+                ORACLE_FN(boundary_function)(d, d->time, i, j, bc);
+                UU(OR_STG, i, j) = bc[0];
+                UU(OR_ELV, i, j) = bc[3];
+                if (!stag) { UU(OR_UH, i, j) = UU(OR_UH, i - 1, j); UU(OR_VH, i, j) = ZERO; }
+            }
+        }
+        for (int i = 1; i <= nx; i++) {
+            if (d->boundary_exterior[2]) {
+                int j = 1;
+                ORACLE_FN(boundary_function)(d, d->time, i, j, bc);
+                UU(OR_STG, i, j) = bc[0];
+                UU(OR_ELV, i, j) = bc[3];
+                if (!stag) { UU(OR_VH, i, j) = UU(OR_VH, i, j + 1); UU(OR_UH, i, j) = ZERO; }
+            }
+            if (d->boundary_exterior[0]) {
+                int j = ny;
+                ORACLE_FN(boundary_function)(d, d->time, i, j, bc);
+                UU(OR_STG, i, j) = bc[0];
+                UU(OR_ELV, i, j) = bc[3];
+                if (!stag) { UU(OR_VH, i, j) = UU(OR_VH, i, j - 1); UU(OR_UH, i, j) = ZERO; }
+            }
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* max_U tracking: domain_mod.f90:2243-2290 (max_stage, dry cells included) */
+void ORACLE_FN(update_max_quantities)(oracle_domain *d)
+{
+    const int nx = d->nx, ny = d->ny;
+    if (!d->record_max_stage || !d->max_stage) return;
+    for (int j = d->yL; j <= d->yU; j++)
+        for (int i = d->xL; i <= d->xU; i++) {
+            REAL m = d->max_stage[IDX(i, j)];
+            REAL s = UU(OR_STG, i, j);
+            d->max_stage[IDX(i, j)] = (s > m) ? s : m;
+        }
+}
+
+/* domain_mod.f90:1906-1931 */
+double ORACLE_FN(linear_timestep_max)(const oracle_domain *d)
+{
+    const int nx = d->nx, ny = d->ny;
+    REAL ts_max = (sizeof(REAL) == 8) ? (REAL)DBL_MAX : (REAL)FLT_MAX;
+    for (int j = 1; j <= ny; j++)
+        for (int i = 1; i <= nx; i++) {
+            REAL sdx = d->dxb[j - 1] + d->dxb[j];
+            REAL sdy = d->dyl[i - 1] + d->dyl[i];
+            REAL dep = rmax((REAL)d->msl_linear - UU(OR_ELV, i, j), MINIMUM_ALLOWED_DEPTH);
+            REAL v = (REAL)0.5 * rmin(sdx, sdy) / (REAL)sqrt(GRAVITY * dep);
+            ts_max = rmin(ts_max, v);
+        }
+    return ts_max * (REAL)d->cfl;
+}
+
+/* domain_mod.f90:1933-1960 */
+double ORACLE_FN(nonlinear_stationary_timestep_max)(const oracle_domain *d)
+{
+    const int nx = d->nx, ny = d->ny;
+    REAL ts_max = (sizeof(REAL) == 8) ? (REAL)DBL_MAX : (REAL)FLT_MAX;
+    for (int j = 1; j <= ny; j++)
+        for (int i = 1; i <= nx; i++) {
+            REAL sdx = d->dxb[j] + d->dxb[j - 1];
+            REAL sdy = d->dyl[i] + d->dyl[i - 1];
+            REAL dep = rmax(UU(OR_STG, i, j) - UU(OR_ELV, i, j), MINIMUM_ALLOWED_DEPTH);
+            REAL v = (REAL)0.5 * rmin(sdx, sdy) / (REAL)sqrt(GRAVITY * dep);
+            ts_max = rmin(ts_max, v);
+        }
+    return ts_max * (REAL)d->cfl;
+}
+
+/* domain_mod.f90:1815-1849 (sequential row order) */
+double ORACLE_FN(volume_interior)(const oracle_domain *d)
+{
+    const int nx = d->nx, ny = d->ny;
+    int n_ext = d->exterior_cells_width;
+    double vol = 0.0;
+    for (int j = 1 + n_ext; j <= ny - n_ext; j++) {
+        double local_sum = 0.0;
+        for (int i = 1 + n_ext; i <= nx - n_ext; i++)
+            local_sum += (double)UU(OR_STG, i, j) - (double)UU(OR_ELV, i, j);
+        vol = vol + (double)((double)d->area[j - 1] * local_sum);
+    }
+    return vol;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Linear leapfrog: domain_mod_linear_solver_include.f90:58-571 */
+static void linear_leapfrog_step(oracle_domain *d, REAL dt)
+{
+    const int nx = d->nx, ny = d->ny;
+    const int xL = d->xL, xU = d->xU, yL = d->yL, yU = d->yU;
+    const int truely_linear = d->truely_linear;
+    const REAL msl = (REAL)d->msl_linear;
+    d->dt_last_update = dt;
+
+    /* Stage update (:92-115) */
+    #pragma omp parallel for schedule(static)
+    for (int j = yL + 1; j <= yU - 1; j++) {
+        REAL inv_cell_area_dt = dt / d->area[j - 1];
+        for (int i = xL + 1; i <= xU - 1; i++) {
+            REAL a = (UU(OR_UH, i, j) - UU(OR_UH, i - 1, j)) * d->dyl[i - 1];
+            REAL b = UU(OR_VH, i, j) * d->dxb[j] - UU(OR_VH, i, j - 1) * d->dxb[j - 1];
+            UU(OR_STG, i, j) = UU(OR_STG, i, j) - inv_cell_area_dt * (a + b);
+        }
+    }
+    d->time = d->time + (double)(dt * HALF);
+
+    update_boundary(d);
+
+    /* Boundary flux integration (:130-150); single-domain case */
+    {
+        int n_ext = d->exterior_cells_width;
+        REAL s;
+        s = ZERO; for (int i = n_ext + 1; i <= nx - n_ext; i++) s += UU(OR_VH, i, ny - n_ext);
+        d->boundary_flux_store[0] = (double)(s * d->dxb[ny - n_ext]);
+        s = ZERO; for (int j = 1 + n_ext; j <= ny - n_ext; j++) s += UU(OR_UH, nx - n_ext, j);
+        d->boundary_flux_store[1] = (double)(s * d->dyl[nx - n_ext]);
+        s = ZERO; for (int i = n_ext + 1; i <= nx - n_ext; i++) s += UU(OR_VH, i, n_ext);
+        d->boundary_flux_store[2] = (double)(-(s * d->dxb[n_ext]));
+        s = ZERO; for (int j = 1 + n_ext; j <= ny - n_ext; j++) s += UU(OR_UH, n_ext, j);
+        d->boundary_flux_store[3] = (double)(-(s * d->dyl[n_ext]));
+        double tot = 0.0;
+        for (int k = 0; k < 4; k++) tot += d->boundary_flux_store[k];
+        d->boundary_flux_evolve_integral = tot * (double)dt;
+    }
+
+    /* Momentum update (:225-567).  Old UH/VH are copied so the Coriolis
+     * averages use pre-update values exactly as the reference's carried row
+     * buffers and thread-boundary snapshots do. */
+    size_t plane = (size_t)nx * (size_t)ny;
+    REAL *uh_old = NULL, *vh_old = NULL;
+    if (d->coriolis) {
+        uh_old = (REAL *)malloc(plane * sizeof(REAL));
+        vh_old = (REAL *)malloc(plane * sizeof(REAL));
+        memcpy(uh_old, &UU(OR_UH, 1, 1), plane * sizeof(REAL));
+        memcpy(vh_old, &UU(OR_VH, 1, 1), plane * sizeof(REAL));
+    }
+    REAL lin_fric_mult = ZERO;
+    int lin_fric = ((REAL)d->linear_friction_coeff != ZERO);
+    if (lin_fric) lin_fric_mult = ONE / (ONE + dt * (REAL)d->linear_friction_coeff);
+
+    #pragma omp parallel
+    {
+        REAL *dw_j = (REAL *)malloc((size_t)nx * sizeof(REAL));
+        REAL *h_jph = (REAL *)malloc((size_t)nx * sizeof(REAL));
+        REAL *h_iph = (REAL *)malloc((size_t)nx * sizeof(REAL));
+        REAL *h_jph_wet = (REAL *)malloc((size_t)nx * sizeof(REAL));
+        REAL *h_iph_wet = (REAL *)malloc((size_t)nx * sizeof(REAL));
+        REAL *dthc = (REAL *)malloc((size_t)nx * sizeof(REAL));
+        REAL *dthc_jph = (REAL *)malloc((size_t)nx * sizeof(REAL));
+        #pragma omp for schedule(static)
+        for (int j = yL; j <= yU - 1; j++) {
+            REAL inv_cell_area_dt_g = GRAVITY * dt / d->area[j - 1];
+            REAL inv_cell_area_dt_vh_g = GRAVITY * dt / (HALF * (d->area[j - 1] + d->area[j]));
+            for (int i = xL; i <= xU - 1; i++) dw_j[i - 1] = UU(OR_STG, i, j + 1) - UU(OR_STG, i, j);
+            if (truely_linear) {
+                for (int i = xL; i <= xU; i++) {
+                    int wet = (UU(OR_ELV, i, j + 1) < -MINIMUM_ALLOWED_DEPTH + msl) &&
+                              (UU(OR_ELV, i, j) < -MINIMUM_ALLOWED_DEPTH + msl);
+                    h_jph[i - 1] = wet ? (msl - HALF * (UU(OR_ELV, i, j + 1) + UU(OR_ELV, i, j))) : ZERO;
+                    h_jph_wet[i - 1] = ONE;
+                }
+                for (int i = xL; i <= xU - 1; i++) {
+                    int wet = (UU(OR_ELV, i, j) < -MINIMUM_ALLOWED_DEPTH + msl) &&
+                              (UU(OR_ELV, i + 1, j) < -MINIMUM_ALLOWED_DEPTH + msl);
+                    h_iph[i - 1] = wet ? (msl - HALF * (UU(OR_ELV, i + 1, j) + UU(OR_ELV, i, j))) : ZERO;
+                    h_iph_wet[i - 1] = ONE;
+                }
+            } else {
+                for (int i = xL; i <= xU; i++) {
+                    int wet = (UU(OR_STG, i, j + 1) - UU(OR_ELV, i, j + 1) > MINIMUM_ALLOWED_DEPTH) &&
+                              (UU(OR_STG, i, j) - UU(OR_ELV, i, j) > MINIMUM_ALLOWED_DEPTH);
+                    h_jph[i - 1] = wet ? (HALF * ((UU(OR_STG, i, j + 1) + UU(OR_STG, i, j)) -
+                                                  (UU(OR_ELV, i, j + 1) + UU(OR_ELV, i, j)))) : ZERO;
+                    h_jph_wet[i - 1] = (h_jph[i - 1] > ZERO) ? ONE : ZERO;
+                }
+                for (int i = xL; i <= xU - 1; i++) {
+                    int wet = (UU(OR_STG, i, j) - UU(OR_ELV, i, j) > MINIMUM_ALLOWED_DEPTH) &&
+                              (UU(OR_STG, i + 1, j) - UU(OR_ELV, i + 1, j) > MINIMUM_ALLOWED_DEPTH);
+                    h_iph[i - 1] = wet ? (HALF * ((UU(OR_STG, i + 1, j) + UU(OR_STG, i, j)) -
+                                                  (UU(OR_ELV, i + 1, j) + UU(OR_ELV, i, j)))) : ZERO;
+                    h_iph_wet[i - 1] = (h_iph[i - 1] > ZERO) ? ONE : ZERO;
+                }
+            }
+            if (d->coriolis) {
+                for (int i = xL; i <= xU - 1; i++) {
+                    dthc[i - 1] = dt * d->coriolis_c[j - 1] * HALF * ((h_iph[i - 1] > ZERO) ? ONE : ZERO);
+                    dthc_jph[i - 1] = dt * d->coriolis_be[j] * HALF * ((h_jph[i - 1] > ZERO) ? ONE : ZERO);
+                }
+            }
+            for (int i = xL; i <= xU - 1; i++) {
+                REAL uh = UU(OR_UH, i, j) * h_iph_wet[i - 1] -
+                          inv_cell_area_dt_g * h_iph[i - 1] * (UU(OR_STG, i + 1, j) - UU(OR_STG, i, j)) * d->dyl[i];
+                REAL vh = UU(OR_VH, i, j) * h_jph_wet[i - 1] -
+                          inv_cell_area_dt_vh_g * h_jph[i - 1] * dw_j[i - 1] * d->dxb[j];
+                if (d->coriolis) {
+                    int jm = (j > 1) ? j - 1 : 1;
+                    REAL vh_iph_jmh = HALF * (vh_old[IDX(i, jm)] + vh_old[IDX(i + 1, jm)]);
+                    REAL vh_iph_jph = HALF * (vh_old[IDX(i, j)] + vh_old[IDX(i + 1, j)]);
+                    int im = (i > xL) ? i - 1 : ((xL - 1 > 1) ? xL - 1 : 1);
+                    REAL uh_i_j = HALF * (uh_old[IDX(i, j)] + uh_old[IDX(im, j)]);
+                    REAL uh_i_jp1 = HALF * (uh_old[IDX(i, j + 1)] + uh_old[IDX(im, j + 1)]);
+                    uh = uh + dthc[i - 1] * (vh_iph_jmh + vh_iph_jph);
+                    vh = vh - dthc_jph[i - 1] * (uh_i_j + uh_i_jp1);
+                }
+                UU(OR_UH, i, j) = uh;
+                UU(OR_VH, i, j) = vh;
+            }
+            if (lin_fric) {
+                for (int i = xL; i <= xU - 1; i++) {
+                    UU(OR_UH, i, j) = lin_fric_mult * UU(OR_UH, i, j);
+                    UU(OR_VH, i, j) = lin_fric_mult * UU(OR_VH, i, j);
+                }
+            }
+        }
+        free(dw_j); free(h_jph); free(h_iph); free(h_jph_wet); free(h_iph_wet); free(dthc); free(dthc_jph);
+    }
+    free(uh_old); free(vh_old);
+    d->time = d->time + (double)(HALF * dt);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Nonlinear finite-volume pieces */
+
+/* domain_mod.f90:1360-1419 */
+void ORACLE_FN(compute_depth_and_velocity)(oracle_domain *d)
+{
+    const int nx = d->nx, ny = d->ny;
+    int64_t masscon_error = 0;
+    REAL *vu = d->velocity, *vv = d->velocity + (size_t)nx * ny;
+    #pragma omp parallel for schedule(static) reduction(+:masscon_error)
+    for (int j = 1; j <= ny; j++)
+        for (int i = 1; i <= nx; i++) {
+            REAL dep = UU(OR_STG, i, j) - UU(OR_ELV, i, j);
+            d->depth[IDX(i, j)] = dep;
+            if (dep > MINIMUM_ALLOWED_DEPTH) {
+                REAL depth_inv = ONE / dep;
+                vu[IDX(i, j)] = UU(OR_UH, i, j) * depth_inv;
+                vv[IDX(i, j)] = UU(OR_VH, i, j) * depth_inv;
+            } else {
+                if (dep < ZERO) {
+                    d->depth[IDX(i, j)] = ZERO;
+                    UU(OR_STG, i, j) = UU(OR_ELV, i, j);
+                    masscon_error += 1;
+                }
+                vu[IDX(i, j)] = ZERO;
+                vv[IDX(i, j)] = ZERO;
+                UU(OR_UH, i, j) = ZERO;
+                UU(OR_VH, i, j) = ZERO;
+            }
+        }
+    d->negative_depth_fix_counter += masscon_error;
+}
+
+/* extrapolation_limiting_mod.f90:44-79, MC limiter.  sign(1,a) is copysign. */
+void ORACLE_FN(limited_gradient_dx_vectorized)(const REAL *U_local, const REAL *U_lower,
+        const REAL *U_upper, const REAL *theta, REAL *gradient_dx, int32_t n)
+{
+    for (int i = 0; i < n; i++) {
+        REAL a = U_upper[i] - U_local[i];
+        REAL b = U_local[i] - U_lower[i];
+        REAL th = theta[i];
+        REAL sa = (REAL)copysign(ONE, a);
+        REAL sb = (REAL)copysign(ONE, b);
+        REAL half_sasb = HALF * (sa + sb);
+        REAL dd = rmin((REAL)fabs(a), (REAL)fabs(b)) * half_sasb * th;
+        REAL e = HALF * (a + b);
+        REAL c = (dd == ZERO) ? ZERO : e;
+        gradient_dx[i] = (dd > ZERO) ? rmin(c, dd) : rmax(c, dd);
+    }
+}
+
+#define LGD ORACLE_FN(limited_gradient_dx_vectorized)
+
+typedef struct {
+    REAL *theta, *dstage, *ddepth, *du, *dv;
+} grad_set;
+
+static void grad_alloc(grad_set *g, int n)
+{
+    g->theta = (REAL *)calloc((size_t)n, sizeof(REAL));
+    g->dstage = (REAL *)calloc((size_t)n, sizeof(REAL));
+    g->ddepth = (REAL *)calloc((size_t)n, sizeof(REAL));
+    g->du = (REAL *)calloc((size_t)n, sizeof(REAL));
+    g->dv = (REAL *)calloc((size_t)n, sizeof(REAL));
+}
+static void grad_free(grad_set *g)
+{
+    free(g->theta); free(g->dstage); free(g->ddepth); free(g->du); free(g->dv);
+}
+
+/* DE1_inner_include.f90:735-795 */
+static void get_NS_limited_gradient_dx(oracle_domain *d, int j, grad_set *g)
+{
+    const int nx = d->nx, ny = d->ny;
+    REAL *vu = d->velocity, *vv = d->velocity + (size_t)nx * ny;
+    if (j > 1 && j < ny) {
+        REAL c4 = limiter_coef4();
+        for (int i = 1; i <= nx; i++) {
+            REAL d0 = d->depth[IDX(i, j - 1)], d1 = d->depth[IDX(i, j)], d2 = d->depth[IDX(i, j + 1)];
+            REAL mindep = rmin(rmin(d0, d1), d2) - MINIMUM_ALLOWED_DEPTH;
+            REAL maxdep = rmax(rmax(d0, d1), d2) + LIMITER_COEF3 * MINIMUM_ALLOWED_DEPTH;
+            REAL theta_local = c4 * (mindep / maxdep - LIMITER_COEF1);
+            g->theta[i - 1] = rmax((REAL)d->theta * rmin(ONE, theta_local), ZERO);
+        }
+        LGD(&UU(OR_STG, 1, j), &UU(OR_STG, 1, j - 1), &UU(OR_STG, 1, j + 1), g->theta, g->dstage, nx);
+        LGD(&d->depth[IDX(1, j)], &d->depth[IDX(1, j - 1)], &d->depth[IDX(1, j + 1)], g->theta, g->ddepth, nx);
+        LGD(&vu[IDX(1, j)], &vu[IDX(1, j - 1)], &vu[IDX(1, j + 1)], g->theta, g->du, nx);
+        LGD(&vv[IDX(1, j)], &vv[IDX(1, j - 1)], &vv[IDX(1, j + 1)], g->theta, g->dv, nx);
+    } else {
+        for (int i = 0; i < nx; i++) { g->theta[i] = ZERO; g->dstage[i] = ZERO; g->ddepth[i] = ZERO; g->du[i] = ZERO; g->dv[i] = ZERO; }
+    }
+}
+
+/* DE1_inner_include.f90:800-862.  The reference passes length nx-2 slices
+ * with n=nx; only the nx-2 interior results are used, which is what is
+ * computed here. */
+static void get_EW_limited_gradient_dx(oracle_domain *d, int j, grad_set *g)
+{
+    const int nx = d->nx, ny = d->ny;
+    REAL *vu = d->velocity, *vv = d->velocity + (size_t)nx * ny;
+    REAL c4 = limiter_coef4();
+    (void)ny;
+    for (int i = 2; i <= nx - 1; i++) {
+        REAL d0 = d->depth[IDX(i - 1, j)], d1 = d->depth[IDX(i, j)], d2 = d->depth[IDX(i + 1, j)];
+        REAL mindep = rmin(rmin(d0, d1), d2) - MINIMUM_ALLOWED_DEPTH;
+        REAL maxdep = rmax(rmax(d0, d1), d2) + LIMITER_COEF3 * MINIMUM_ALLOWED_DEPTH;
+        REAL theta_local = c4 * (mindep / maxdep - LIMITER_COEF1);
+        g->theta[i - 1] = rmax((REAL)d->theta * rmin(ONE, theta_local), ZERO);
+    }
+    if (nx >= 3) {
+        LGD(&UU(OR_STG, 2, j), &UU(OR_STG, 1, j), &UU(OR_STG, 3, j), &g->theta[1], &g->dstage[1], nx - 2);
+        LGD(&d->depth[IDX(2, j)], &d->depth[IDX(1, j)], &d->depth[IDX(3, j)], &g->theta[1], &g->ddepth[1], nx - 2);
+        LGD(&vu[IDX(2, j)], &vu[IDX(1, j)], &vu[IDX(3, j)], &g->theta[1], &g->du[1], nx - 2);
+        LGD(&vv[IDX(2, j)], &vv[IDX(1, j)], &vv[IDX(3, j)], &g->theta[1], &g->dv[1], nx - 2);
+    }
+    g->dstage[0] = ZERO; g->dstage[nx - 1] = ZERO;
+    g->ddepth[0] = ZERO; g->ddepth[nx - 1] = ZERO;
+    g->du[0] = ZERO; g->du[nx - 1] = ZERO;
+    g->dv[0] = ZERO; g->dv[nx - 1] = ZERO;
+}
+
+/* DE1_inner_include.f90:78-727 with reduced_momentum_diffusion=.true.,
+ * upwind_transverse_momentum=.false., use_eddy_viscosity=.false.
+ * (compute_fluxes_alternatives_include.f90:25-36). */
+double ORACLE_FN(compute_fluxes_DE1_low_fr_diffusion)(oracle_domain *d)
+{
+    const int nx = d->nx, ny = d->ny;
+    const size_t fns_plane = (size_t)nx * (size_t)(ny + 1);
+    const size_t few_plane = (size_t)(nx + 1) * (size_t)ny;
+    const size_t es_plane = (size_t)nx * (size_t)ny;
+#define FNS(i, j, k) d->flux_NS[(size_t)((k) - 1) * fns_plane + (size_t)((i) - 1) + (size_t)((j) - 1) * (size_t)nx]
+#define FEW(i, j, k) d->flux_EW[(size_t)((k) - 1) * few_plane + (size_t)((i) - 1) + (size_t)((j) - 1) * (size_t)(nx + 1)]
+#define ES(i, j, k) d->explicit_source[(size_t)((k) - 2) * es_plane + IDX(i, j)]
+#define ESJM1(i, j) d->explicit_source_VH_j_minus_1[(size_t)((i) - 1) + (size_t)((j) - 1) * (size_t)nx]
+    REAL *vu = d->velocity, *vv = d->velocity + (size_t)nx * ny;
+    const REAL half_cfl = HALF * (REAL)d->cfl;
+    const double half_gravity = (double)(HALF * GRAVITY);
+    const REAL EPS = (REAL)1.0e-12;
+    const REAL EPS_gs = (REAL)sqrt(GRAVITY * MINIMUM_ALLOWED_DEPTH);
+    double max_dt = (REAL)d->maximum_timestep;
+    REAL max_dt_inv_global;
+
+    {
+        REAL init = (REAL)(ONE / max_dt);
+        max_dt_inv_global = init;
+    }
+
+    #pragma omp parallel
+    {
+        grad_set ns_lower, ns, ew;
+        grad_alloc(&ns_lower, nx); grad_alloc(&ns, nx); grad_alloc(&ew, nx);
+        REAL *bed_j_minus_1 = (REAL *)malloc((size_t)nx * sizeof(REAL));
+        REAL *max_dt_inv_work = (REAL *)malloc((size_t)nx * sizeof(REAL));
+        double *es_im1_work = (double *)malloc((size_t)nx * sizeof(double));
+        for (int i = 0; i < nx; i++) max_dt_inv_work[i] = (REAL)(ONE / max_dt);
+
+        #pragma omp for schedule(static)
+        for (int j = 2; j <= ny; j++) {
+            for (int i = 1; i <= nx; i++) { ES(i, j, OR_UH) = 0.0; ES(i, j, OR_VH) = 0.0; ESJM1(i, j) = 0.0; es_im1_work[i - 1] = 0.0; }
+            REAL dx_cfl_half_inv1 = ONE / (d->dxb[j - 1] * half_cfl);
+            REAL dx_cfl_half_inv2 = ONE / (d->dyl[0] * half_cfl);
+            for (int i = 1; i <= nx; i++) bed_j_minus_1[i - 1] = UU(OR_ELV, i, j - 1);
+            get_NS_limited_gradient_dx(d, j - 1, &ns_lower);
+            get_NS_limited_gradient_dx(d, j, &ns);
+
+            /* North-South fluxes (:178-432) */
+            for (int i = 2; i <= nx; i++) {
+                REAL stage_neg = UU(OR_STG, i, j - 1) + HALF * ns_lower.dstage[i - 1];
+                REAL stage_pos = UU(OR_STG, i, j) - HALF * ns.dstage[i - 1];
+                double depth_neg = (double)(d->depth[IDX(i, j - 1)] + HALF * ns_lower.ddepth[i - 1]);
+                double depth_pos = (double)(d->depth[IDX(i, j)] - HALF * ns.ddepth[i - 1]);
+                REAL u_neg = vu[IDX(i, j - 1)] + HALF * ns_lower.du[i - 1];
+                REAL u_pos = vu[IDX(i, j)] - HALF * ns.du[i - 1];
+                REAL v_neg = vv[IDX(i, j - 1)] + HALF * ns_lower.dv[i - 1];
+                REAL v_pos = vv[IDX(i, j)] - HALF * ns.dv[i - 1];
+                double depth_neg_c = (double)d->depth[IDX(i, j - 1)];
+                double depth_pos_c = (double)d->depth[IDX(i, j)];
+
+                REAL z_neg = (REAL)((double)stage_neg - depth_neg);
+                REAL z_pos = (REAL)((double)stage_pos - depth_pos);
+                REAL z_half = rmax(z_neg, z_pos);
+
+                REAL stage_neg_star = rmax(stage_neg, z_half);
+                double depth_neg_star = (double)(stage_neg_star - z_half);
+                if (depth_neg_star == 0.0) { v_neg = ZERO; u_neg = ZERO; }
+                REAL vd_neg = (REAL)((double)v_neg * depth_neg_star);
+                REAL ud_neg = (REAL)((double)u_neg * depth_neg_star);
+                REAL gs_neg = (REAL)sqrt((double)GRAVITY * depth_neg_star);
+
+                REAL stage_pos_star = rmax(stage_pos, z_half);
+                double depth_pos_star = (double)(stage_pos_star - z_half);
+                if (depth_pos_star == 0.0) { v_pos = ZERO; u_pos = ZERO; }
+                REAL vd_pos = (REAL)((double)v_pos * depth_pos_star);
+                REAL ud_pos = (REAL)((double)u_pos * depth_pos_star);
+                REAL gs_pos = (REAL)sqrt((double)GRAVITY * depth_pos_star);
+
+                REAL vel_beta_neg = v_neg * ADVECTION_BETA;
+                REAL vel_beta_pos = v_pos * ADVECTION_BETA;
+
+                REAL s_max = rmax(rmax(vel_beta_neg + gs_neg, vel_beta_pos + gs_pos), ZERO);
+                REAL s_min = rmin(rmin(vel_beta_neg - gs_neg, vel_beta_pos - gs_pos), ZERO);
+                double denom = (double)(s_max - s_min);
+                double inv_denom;
+                if (denom > (double)EPS && (gs_pos > EPS_gs || gs_neg > EPS_gs))
+                    inv_denom = (double)d->dxb[j - 1] / denom;
+                else
+                    inv_denom = 0.0;
+                REAL sminsmax = s_min * s_max * ONE;
+                REAL fr2num = ((v_neg * v_neg + v_pos * v_pos) + u_neg * u_neg) + u_pos * u_pos;
+                REAL fr2den = ((gs_neg * gs_neg + gs_pos * gs_pos) + (REAL)1.0e-10);
+                REAL fr2 = ADVECTION_BETA * (REAL)sqrt(rmax((REAL)0.001, rmin(ONE, fr2num / fr2den)));
+
+                FNS(i, j, OR_STG) = (REAL)((double)((s_max * vd_neg - s_min * vd_pos) +
+                                                     sminsmax * (stage_pos_star - stage_neg_star)) * inv_denom);
+                FNS(i, j, OR_UH) = (REAL)((double)((s_max * ud_neg * vel_beta_neg - s_min * ud_pos * vel_beta_pos) +
+                                                    fr2 * sminsmax * (ud_pos - ud_neg)) * inv_denom);
+                FNS(i, j, OR_VH) = (REAL)((double)((s_max * vd_neg * vel_beta_neg - s_min * vd_pos * vel_beta_pos) +
+                                                    fr2 * sminsmax * (vd_pos - vd_neg)) * inv_denom);
+
+                double half_g_hh_edge = inv_denom * half_gravity *
+                    ((double)s_max * depth_neg_star * depth_neg_star - (double)s_min * depth_pos_star * depth_pos_star);
+                double bed_slope_pressure_n = half_gravity *
+                    ((depth_neg_star - depth_neg) * (depth_neg_star + depth_neg) -
+                     (depth_neg + depth_neg_c) * (double)(z_neg - bed_j_minus_1[i - 1]));
+                ESJM1(i, j) = bed_slope_pressure_n * (double)d->dxb[j - 1] - half_g_hh_edge;
+                double bed_slope_pressure_s = half_gravity *
+                    ((depth_pos_star - depth_pos) * (depth_pos_star + depth_pos) -
+                     (depth_pos + depth_pos_c) * (double)(z_pos - UU(OR_ELV, i, j)));
+                ES(i, j, OR_VH) = (ES(i, j, OR_VH) - bed_slope_pressure_s * (double)d->dxb[j - 1]) + half_g_hh_edge;
+
+                double max_speed = (double)rmax(s_max, -s_min);
+                if (max_speed > (double)EPS) {
+                    double cand = max_speed * (double)dx_cfl_half_inv2;
+                    max_dt_inv_work[i - 1] = (REAL)dmax((double)max_dt_inv_work[i - 1], cand);
+                }
+            }
+
+            /* East-West fluxes (:446-718) */
+            get_EW_limited_gradient_dx(d, j, &ew);
+            for (int i = 2; i <= nx; i++) {
+                REAL stage_neg = UU(OR_STG, i - 1, j) + HALF * ew.dstage[i - 2];
+                REAL stage_pos = UU(OR_STG, i, j) - HALF * ew.dstage[i - 1];
+                double depth_neg = (double)(d->depth[IDX(i - 1, j)] + HALF * ew.ddepth[i - 2]);
+                double depth_pos = (double)(d->depth[IDX(i, j)] - HALF * ew.ddepth[i - 1]);
+                REAL u_neg = vu[IDX(i - 1, j)] + HALF * ew.du[i - 2];
+                REAL u_pos = vu[IDX(i, j)] - HALF * ew.du[i - 1];
+                REAL v_neg = vv[IDX(i - 1, j)] + HALF * ew.dv[i - 2];
+                REAL v_pos = vv[IDX(i, j)] - HALF * ew.dv[i - 1];
+                double depth_neg_c = (double)d->depth[IDX(i - 1, j)];
+                double depth_pos_c = (double)d->depth[IDX(i, j)];
+
+                REAL z_neg = (REAL)((double)stage_neg - depth_neg);
+                REAL z_pos = (REAL)((double)stage_pos - depth_pos);
+                REAL z_half = rmax(z_neg, z_pos);
+
+                REAL stage_neg_star = rmax(stage_neg, z_half);
+                double depth_neg_star = (double)(stage_neg_star - z_half);
+                if (depth_neg_star == 0.0) { u_neg = ZERO; v_neg = ZERO; }
+                REAL ud_neg = (REAL)((double)u_neg * depth_neg_star);
+                REAL vd_neg = (REAL)((double)v_neg * depth_neg_star);
+                REAL gs_neg = (REAL)sqrt((double)GRAVITY * depth_neg_star);
+
+                REAL stage_pos_star = rmax(stage_pos, z_half);
+                double depth_pos_star = (double)(stage_pos_star - z_half);
+                if (depth_pos_star == 0.0) { u_pos = ZERO; v_pos = ZERO; }
+                REAL ud_pos = (REAL)((double)u_pos * depth_pos_star);
+                REAL vd_pos = (REAL)((double)v_pos * depth_pos_star);
+                REAL gs_pos = (REAL)sqrt((double)GRAVITY * depth_pos_star);
+
+                REAL vel_beta_neg = u_neg * ADVECTION_BETA;
+                REAL vel_beta_pos = u_pos * ADVECTION_BETA;
+
+                REAL s_max = rmax(rmax(vel_beta_neg + gs_neg, vel_beta_pos + gs_pos), ZERO);
+                REAL s_min = rmin(rmin(vel_beta_neg - gs_neg, vel_beta_pos - gs_pos), ZERO);
+                double denom = (double)(s_max - s_min);
+                double inv_denom;
+                if (denom > (double)EPS && (gs_pos > EPS_gs || gs_neg > EPS_gs))
+                    inv_denom = (double)d->dyl[i - 1] / denom;
+                else
+                    inv_denom = 0.0;
+                REAL sminsmax = s_min * s_max * ONE;
+                REAL fr2num = ((v_neg * v_neg + v_pos * v_pos) + u_neg * u_neg) + u_pos * u_pos;
+                REAL fr2den = ((gs_neg * gs_neg + gs_pos * gs_pos) + (REAL)1.0e-10);
+                REAL fr2 = ADVECTION_BETA * (REAL)sqrt(rmax((REAL)0.001, rmin(ONE, fr2num / fr2den)));
+
+                FEW(i, j, OR_STG) = (REAL)((double)((s_max * ud_neg - s_min * ud_pos) +
+                                                     sminsmax * (stage_pos_star - stage_neg_star)) * inv_denom);
+                FEW(i, j, OR_UH) = (REAL)((double)((s_max * ud_neg * vel_beta_neg - s_min * ud_pos * vel_beta_pos) +
+                                                    fr2 * sminsmax * (ud_pos - ud_neg)) * inv_denom);
+                FEW(i, j, OR_VH) = (REAL)((double)((s_max * vd_neg * vel_beta_neg - s_min * vd_pos * vel_beta_pos) +
+                                                    fr2 * sminsmax * (vd_pos - vd_neg)) * inv_denom);
+
+                double half_g_hh_edge = inv_denom * half_gravity *
+                    ((double)s_max * depth_neg_star * depth_neg_star - (double)s_min * depth_pos_star * depth_pos_star);
+                double bed_slope_pressure_e = half_gravity *
+                    ((depth_neg_star - depth_neg) * (depth_neg_star + depth_neg) -
+                     (depth_neg + depth_neg_c) * (double)(z_neg - UU(OR_ELV, i - 1, j)));
+                es_im1_work[i - 2] = bed_slope_pressure_e * (double)d->dyl[i - 1] - half_g_hh_edge;
+                double bed_slope_pressure_w = half_gravity *
+                    ((depth_pos_star - depth_pos) * (depth_pos_star + depth_pos) -
+                     (depth_pos + depth_pos_c) * (double)(z_pos - UU(OR_ELV, i, j)));
+                ES(i, j, OR_UH) = (ES(i, j, OR_UH) - bed_slope_pressure_w * (double)d->dyl[i - 1]) + half_g_hh_edge;
+
+                if (d->spherical) {
+                    double dep_ij = (double)d->depth[IDX(i, j)];
+                    ES(i, j, OR_VH) = ES(i, j, OR_VH) +
+                        half_gravity * dep_ij * dep_ij * (double)(d->dxb[j] - d->dxb[j - 1]);
+                    if (d->coriolis) {
+                        REAL cm = d->area[j - 1] * d->coriolis_c[j - 1];
+                        ES(i, j, OR_UH) = ES(i, j, OR_UH) + (double)(cm * UU(OR_VH, i, j));
+                        ES(i, j, OR_VH) = ES(i, j, OR_VH) - (double)(cm * UU(OR_UH, i, j));
+                    }
+                    REAL cm2 = d->area[j - 1] * d->tanlat_on_R[j - 1] * vu[IDX(i, j)];
+                    ES(i, j, OR_UH) = ES(i, j, OR_UH) + (double)(cm2 * UU(OR_VH, i, j));
+                    ES(i, j, OR_VH) = ES(i, j, OR_VH) - (double)(cm2 * UU(OR_UH, i, j));
+                }
+
+                double max_speed = (double)rmax(s_max, -s_min);
+                if (max_speed > (double)EPS) {
+                    double cand = max_speed * (double)dx_cfl_half_inv1;
+                    max_dt_inv_work[i - 1] = (REAL)dmax((double)max_dt_inv_work[i - 1], cand);
+                }
+            }
+            for (int i = 1; i <= nx; i++) ES(i, j, OR_UH) = ES(i, j, OR_UH) + es_im1_work[i - 1];
+        }
+        REAL local_max = max_dt_inv_work[0];
+        for (int i = 1; i < nx; i++) local_max = rmax(local_max, max_dt_inv_work[i]);
+        #pragma omp critical
+        { max_dt_inv_global = rmax(max_dt_inv_global, local_max); }
+        grad_free(&ns_lower); grad_free(&ns); grad_free(&ew);
+        free(bed_j_minus_1); free(max_dt_inv_work); free(es_im1_work);
+    }
+    max_dt = (double)(ONE / max_dt_inv_global);
+    return max_dt;
+#undef FNS
+#undef FEW
+#undef ES
+#undef ESJM1
+}
+
+/* domain_mod.f90:1425-1559: depth/velocity, fluxes, boundary flux store */
+static double compute_fluxes(oracle_domain *d)
+{
+    const int nx = d->nx, ny = d->ny;
+    ORACLE_FN(compute_depth_and_velocity)(d);
+    double max_dt = ORACLE_FN(compute_fluxes_DE1_low_fr_diffusion)(d);
+    const size_t fns_plane = (size_t)nx * (size_t)(ny + 1);
+    (void)fns_plane;
+    int n_ext = d->exterior_cells_width;
+    REAL s;
+#define FNS1(i, j) d->flux_NS[(size_t)((i) - 1) + (size_t)((j) - 1) * (size_t)nx]
+#define FEW1(i, j) d->flux_EW[(size_t)((i) - 1) + (size_t)((j) - 1) * (size_t)(nx + 1)]
+    s = ZERO; for (int i = 1 + n_ext; i <= nx - n_ext; i++) s += FNS1(i, ny + 1 - n_ext);
+    d->boundary_flux_store[0] = (double)s;
+    s = ZERO; for (int j = 1 + n_ext; j <= ny - n_ext; j++) s += FEW1(nx + 1 - n_ext, j);
+    d->boundary_flux_store[1] = (double)s;
+    s = ZERO; for (int i = 1 + n_ext; i <= nx - n_ext; i++) s += FNS1(i, 1 + n_ext);
+    d->boundary_flux_store[2] = (double)(-s);
+    s = ZERO; for (int j = 1 + n_ext; j <= ny - n_ext; j++) s += FEW1(1 + n_ext, j);
+    d->boundary_flux_store[3] = (double)(-s);
+#undef FNS1
+#undef FEW1
+    return max_dt;
+}
+
+/* update_U_DE1_inner_include.f90:14-99 (manning: power -7/3; chezy: -2) */
+static void update_U(oracle_domain *d, REAL dt)
+{
+    const int nx = d->nx, ny = d->ny;
+    const size_t fns_plane = (size_t)nx * (size_t)(ny + 1);
+    const size_t few_plane = (size_t)(nx + 1) * (size_t)ny;
+    const size_t es_plane = (size_t)nx * (size_t)ny;
+    REAL *vu = d->velocity, *vv = d->velocity + (size_t)nx * ny;
+    const REAL friction_power_depth = d->friction_chezy ? (REAL)-2.0 : (REAL)-7.0 / (REAL)3.0;
+    d->dt_last_update = dt;
+    REAL dt_gravity = dt * GRAVITY;
+    #pragma omp parallel for schedule(static)
+    for (int j = 1; j <= ny; j++) {
+        REAL inv_cell_area_dt = dt / d->area[j - 1];
+        for (int i = 1; i <= nx; i++) {
+            for (int kk = 1; kk <= 3; kk++) {
+                REAL fn_hi = d->flux_NS[(size_t)(kk - 1) * fns_plane + (size_t)(i - 1) + (size_t)j * nx];
+                REAL fn_lo = d->flux_NS[(size_t)(kk - 1) * fns_plane + (size_t)(i - 1) + (size_t)(j - 1) * nx];
+                REAL fe_hi = d->flux_EW[(size_t)(kk - 1) * few_plane + (size_t)i + (size_t)(j - 1) * (nx + 1)];
+                REAL fe_lo = d->flux_EW[(size_t)(kk - 1) * few_plane + (size_t)(i - 1) + (size_t)(j - 1) * (nx + 1)];
+                UU(kk, i, j) = UU(kk, i, j) - inv_cell_area_dt * ((fn_hi - fn_lo) + (fe_hi - fe_lo));
+            }
+        }
+        for (int i = 1; i <= nx; i++) {
+            REAL depth = d->depth[IDX(i, j)];
+            if (UU(OR_STG, i, j) <= UU(OR_ELV, i, j) + MINIMUM_ALLOWED_DEPTH) {
+                UU(OR_UH, i, j) = ZERO;
+                UU(OR_VH, i, j) = ZERO;
+            } else {
+                REAL implicit_factor;
+                if (!d->nofriction) {
+                    REAL fs = d->manning_squared[IDX(i, j)] *
+                              (REAL)sqrt(vu[IDX(i, j)] * vu[IDX(i, j)] + vv[IDX(i, j)] * vv[IDX(i, j)]) *
+                              (REAL)RPOW(rmax(depth, MINIMUM_ALLOWED_DEPTH), friction_power_depth);
+                    implicit_factor = ONE / ((ONE + dt_gravity * rmax(depth, ZERO) * fs) +
+                                             dt * (REAL)d->linear_friction_coeff);
+                } else {
+                    implicit_factor = ONE;
+                }
+                double es_uh = d->explicit_source[(size_t)0 * es_plane + IDX(i, j)];
+                double es_vh = d->explicit_source[(size_t)1 * es_plane + IDX(i, j)];
+                double es_jm1 = d->explicit_source_VH_j_minus_1[(size_t)(i - 1) + (size_t)j * nx];
+                UU(OR_UH, i, j) = (REAL)((double)UU(OR_UH, i, j) + (double)inv_cell_area_dt * es_uh);
+                UU(OR_UH, i, j) = UU(OR_UH, i, j) * implicit_factor;
+                UU(OR_VH, i, j) = (REAL)((double)UU(OR_VH, i, j) + (double)inv_cell_area_dt * (es_vh + es_jm1));
+                UU(OR_VH, i, j) = UU(OR_VH, i, j) * implicit_factor;
+            }
+        }
+    }
+    d->time = d->time + (double)dt;
+    update_boundary(d);
+}
+
+/* timestepping_alternatives_include.f90:8-62 */
+static void one_euler_step(oracle_domain *d, double timestep, int has_ts)
+{
+    double ts = compute_fluxes(d);
+    d->max_dt = ts;
+    if (has_ts) ts = timestep;
+    update_U(d, (REAL)ts);
+    double tot = 0.0;
+    for (int k = 0; k < 4; k++) tot += d->boundary_flux_store[k];
+    d->boundary_flux_evolve_integral = d->boundary_flux_evolve_integral + (double)(REAL)ts * tot;
+}
+
+/* timestepping_alternatives_include.f90:64-146 */
+static void one_rk2_step(oracle_domain *d, double timestep, int has_ts)
+{
+    const int nx = d->nx, ny = d->ny;
+    const size_t plane = (size_t)nx * (size_t)ny;
+    double backup_time = d->time;
+    memcpy(d->backup_U, d->U, 3 * plane * sizeof(REAL));
+    double dt_first_step;
+    if (has_ts) { one_euler_step(d, timestep, 1); dt_first_step = (REAL)timestep; }
+    else { one_euler_step(d, 0.0, 0); dt_first_step = d->max_dt; }
+    double max_dt_store = d->max_dt;
+    one_euler_step(d, dt_first_step, 1);
+    for (size_t q = 0; q < 3 * plane; q++) d->U[q] = HALF * (d->U[q] + d->backup_U[q]);
+    d->time = backup_time + dt_first_step;
+    d->boundary_flux_evolve_integral = 0.5 * d->boundary_flux_evolve_integral;
+    d->max_dt = max_dt_store;
+}
+
+/* domain_mod.f90:1679-1813 */
+int ORACLE_FN(evolve_one_step)(oracle_domain *d, double dt, int has_dt)
+{
+    double time0 = d->time;
+    d->boundary_flux_evolve_integral = 0.0;
+    if (d->nsteps_advanced == 0) ORACLE_FN(update_max_quantities)(d);
+    switch (d->method) {
+    case OR_METHOD_RK2: one_rk2_step(d, dt, has_dt); break;
+    case OR_METHOD_EULER: one_euler_step(d, dt, has_dt); break;
+    case OR_METHOD_LINEAR:
+        if (!has_dt) return 2;
+        linear_leapfrog_step(d, (REAL)dt);
+        break;
+    default: return 3;
+    }
+    ORACLE_FN(update_max_quantities)(d);
+    d->evolve_step_dt = d->time - time0;
+    d->boundary_flux_time_integral += d->boundary_flux_evolve_integral;
+    d->nsteps_advanced += 1;
+    return 0;
+}

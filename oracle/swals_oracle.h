@@ -1,0 +1,139 @@
+/*
+ * swals_oracle.h -- TEST INFRASTRUCTURE ONLY.
+ *
+ * A plain-C, IEEE-strict restatement of the SWALS shallow-water time-step
+ * hot path (GeoscienceAustralia/ptha, propagation/SWALS/src/shallow_water).
+ * It is the checker for the CUDA implementation: only tests/, the smoke
+ * check and the CPU-baseline leg of the benchmark may load it.  Nothing in
+ * the product (ptha_b200/) links or calls it.
+ *
+ * Arrays follow the reference's Fortran column-major layout: U(i,j,k) with
+ * i fastest, 1-based indices in the code below; k = STG,UH,VH,ELV (1..4).
+ *
+ * Parity pinning: the reference cannot be compiled here (no Fortran
+ * compiler).  The restatement is pinned against the reference's own unit
+ * test known answers (MC limiter cases, spherical area values, point-gauge
+ * indexing, nested-comms linear-field exactness) and against conservation
+ * properties; see tests/test_oracle_golden.py.
+ *
+ * REAL is double unless compiled with -DORACLE_REAL32, mirroring the
+ * reference's -DREALFLOAT switch (global_mod.f90:16-34).  Variables that the
+ * reference declares real(force_double) stay double in both builds.
+ */
+#ifndef SWALS_ORACLE_H
+#define SWALS_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef ORACLE_REAL32
+typedef float REAL;
+#define ORACLE_FN(name) oracle32_##name
+#else
+typedef double REAL;
+#define ORACLE_FN(name) oracle64_##name
+#endif
+
+enum { OR_STG = 1, OR_UH = 2, OR_VH = 3, OR_ELV = 4 };
+
+/* timestepping_method codes (timestepping_metadata_mod.f90:135-232). */
+enum {
+    OR_METHOD_RK2 = 1,
+    OR_METHOD_RK2N = 2,
+    OR_METHOD_MIDPOINT = 3,
+    OR_METHOD_EULER = 4,
+    OR_METHOD_LINEAR = 5,
+    OR_METHOD_LEAPFROG_LINEAR_PLUS_NONLINEAR_FRICTION = 6,
+    OR_METHOD_CLIFFS = 7,
+    OR_METHOD_LEAPFROG_NONLINEAR = 8
+};
+
+/* Boundary condition kinds supported by the oracle (boundary_mod.f90). */
+enum {
+    OR_BC_NONE = 0,                               /* walls via elevation */
+    OR_BC_TRANSMISSIVE = 1,                       /* boundary_mod.f90:21-75 */
+    OR_BC_STAGE_TRANSMISSIVE_NORMAL_MOMENTUM = 2  /* boundary_mod.f90:78-163 */
+};
+
+/* Analytic boundary functions for OR_BC_STAGE_TRANSMISSIVE_NORMAL_MOMENTUM. */
+enum {
+    OR_BF_SOLITARY_WEST_WALLS = 1  /* solitary wave on the west edge, walls elsewhere */
+};
+
+typedef struct oracle_domain {
+    /* geometry (domain_mod.f90:137-160) */
+    int32_t nx, ny;
+    double lw[2];
+    double lower_left[2];
+    /* solver */
+    int32_t method;
+    int32_t spherical;           /* -DSPHERICAL */
+    int32_t coriolis;            /* CORIOLIS (spherical and not -DNOCORIOLIS) */
+    int32_t nofriction;          /* -DNOFRICTION */
+    int32_t truely_linear;       /* linear_solver_is_truely_linear */
+    int32_t friction_chezy;      /* friction_type == 'chezy' */
+    int32_t xL, xU, yL, yU;      /* 1-based active region */
+    int32_t exterior_cells_width;
+    int32_t boundary_exterior[4];/* N, E, S, W */
+    int32_t bc_kind;
+    int32_t bf_kind;
+    int32_t record_max_stage;
+    int32_t pad0;
+    double theta, cfl, msl_linear, linear_friction_coeff, maximum_timestep;
+    double bf_params[8];
+    /* state */
+    double time, max_dt, dt_last_update, evolve_step_dt;
+    int64_t nsteps_advanced;
+    int64_t negative_depth_fix_counter;
+    double boundary_flux_store[4];
+    double boundary_flux_evolve_integral;
+    double boundary_flux_time_integral;
+    /* arrays, owned by the caller (sizes in comments) */
+    REAL *U;            /* nx*ny*4 */
+    REAL *max_stage;    /* nx*ny */
+    REAL *manning_squared; /* nx*ny (rk2 family) */
+    REAL *x, *y;        /* nx, ny */
+    REAL *dxb;          /* distance_bottom_edge, ny+1 */
+    REAL *dyl;          /* distance_left_edge, nx+1 */
+    REAL *area;         /* area_cell_y, ny */
+    REAL *coriolis_c;   /* coriolis, ny */
+    REAL *coriolis_be;  /* coriolis_bottom_edge, ny+1 */
+    REAL *tanlat_on_R;  /* tanlat_on_radius_earth, ny */
+    /* rk2 work arrays */
+    REAL *depth;        /* nx*ny */
+    REAL *velocity;     /* nx*ny*2 (UH, VH slots) */
+    REAL *flux_NS;      /* nx*(ny+1)*3 */
+    REAL *flux_EW;      /* (nx+1)*ny*3 */
+    double *explicit_source;      /* nx*ny*2 (UH, VH) */
+    double *explicit_source_VH_j_minus_1; /* nx*(ny+1) */
+    REAL *backup_U;     /* nx*ny*3 */
+} oracle_domain;
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Defaults that allocate_quantities takes from timestepping metadata. */
+void ORACLE_FN(apply_method_defaults)(oracle_domain *d);
+/* Geometry arrays (domain_mod.f90:925-1014). */
+void ORACLE_FN(setup_geometry)(oracle_domain *d);
+/* domain%evolve_one_step(timestep) (domain_mod.f90:1679-1813). has_dt=0 means adaptive. */
+int  ORACLE_FN(evolve_one_step)(oracle_domain *d, double dt, int has_dt);
+/* Pieces used by tests directly. */
+void ORACLE_FN(update_max_quantities)(oracle_domain *d);
+double ORACLE_FN(linear_timestep_max)(const oracle_domain *d);
+double ORACLE_FN(nonlinear_stationary_timestep_max)(const oracle_domain *d);
+double ORACLE_FN(volume_interior)(const oracle_domain *d);
+void ORACLE_FN(compute_depth_and_velocity)(oracle_domain *d);
+double ORACLE_FN(compute_fluxes_DE1_low_fr_diffusion)(oracle_domain *d);
+void ORACLE_FN(limited_gradient_dx_vectorized)(const REAL *U_local, const REAL *U_lower,
+        const REAL *U_upper, const REAL *theta, REAL *gradient_dx, int32_t n);
+double ORACLE_FN(area_lonlat_rectangle)(double lon1, double lat1, double dlon, double dlat, int flat);
+void ORACLE_FN(gauge_site_index)(const double *xy, int32_t n, const double *ll,
+        const double *dx, const int32_t *nxy, int32_t *site_index);
+void ORACLE_FN(boundary_function)(const oracle_domain *d, double t, int32_t i, int32_t j, REAL *out4);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,336 @@
+// linear.cu -- truly-linear / not-truly-linear leapfrog step on sm_100a.
+//
+// Restates domain_mod_linear_solver_include.f90:58-571 (one_truely_linear_
+// leapfrog_step / one_not_truely_linear_leapfrog_step,
+// domain_mod_timestepping_alternatives_include.f90:339-387).
+//
+// The reference makes two sweeps over the grid (stage, then UH/VH) and uses
+// hand-made OpenMP chunking with thread-boundary snapshots so the Coriolis
+// averages see pre-update UH/VH without copying.  Here one fused pass reads
+// the old state once and writes the new state to a second buffer:
+//   - each CTA stages a tile of old UH/VH/ELV (plus a one-cell halo) in shared
+//     memory, recomputes the new stage on the tile plus its east/north halo,
+//     then applies the momentum update and writes STG/UH/VH and max_stage;
+//   - the ping-pong buffers make every old value available to the Coriolis
+//     averages, so no snapshots are needed.
+// Algorithmic traffic: read STG,UH,VH,ELV + write STG,UH,VH (7 planes), plus
+// max_stage read+write when recorded.  Halo re-reads hit L2.
+// A one-block edge kernel runs first: it applies the device boundary
+// function to the stage/elevation ring at time+dt/2 (boundary_mod.f90:78-163
+// staggered branch), forms the boundary flux sums (:126-205) and advances
+// domain%time.
+#include "swals_kernels.h"
+
+namespace swals {
+namespace {
+
+constexpr int LBX = 32;   // tile columns (one warp wide)
+constexpr int LBY = 16;   // tile rows
+constexpr int LTY = 8;    // thread rows; each thread handles LBY/LTY cells
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+template <typename R>
+struct LinArgs {
+    StepPlanes<R> p;
+    Metrics<R> m;
+    int xl, xu, yl, yu;
+    int bc_stage;
+    int bext[4];
+    R dt;
+    R msl;
+    int lin_fric;
+    R lin_fric_mult;
+};
+
+__device__ __forceinline__ bool on_bc_ring(int i, int r, int nx, int ny, const int bext[4])
+{
+    return (i == 0 && bext[3]) || (i == nx - 1 && bext[1]) || (r == 0 && bext[2]) || (r == ny - 1 && bext[0]);
+}
+
+template <typename R, bool CORIOLIS, bool TRUELY_LINEAR>
+__global__ void __launch_bounds__(LBX *LTY) linear_step_kernel(const LinArgs<R> a)
+{
+    __shared__ R s_uh[LBY + 1][LBX + 2];  // old UH: rows r0..r0+LBY, cols i0-1..i0+LBX (clamped)
+    __shared__ R s_vh[LBY + 2][LBX + 1];  // old VH: rows r0-1..r0+LBY, cols i0..i0+LBX (clamped)
+    __shared__ R s_sn[LBY + 1][LBX + 1];  // new STG: rows r0..r0+LBY, cols i0..i0+LBX
+    __shared__ R s_el[LBY + 1][LBX + 1];  // ELV on the same window as s_sn
+
+    const int nx = a.p.nx, ny = a.p.ny;
+    const int64_t P = a.p.pitch;
+    const int i0 = blockIdx.x * LBX, r0 = blockIdx.y * LBY;
+    const int tid = threadIdx.y * LBX + threadIdx.x;
+    constexpr int NT = LBX * LTY;
+
+    for (int q = tid; q < (LBY + 1) * (LBX + 2); q += NT) {
+        int rr = q / (LBX + 2), cc = q - rr * (LBX + 2);
+        int r = clampi(r0 + rr, 0, ny - 1), i = clampi(i0 - 1 + cc, 0, nx - 1);
+        s_uh[rr][cc] = a.p.uh[r * P + i];
+    }
+    for (int q = tid; q < (LBY + 2) * (LBX + 1); q += NT) {
+        int rr = q / (LBX + 1), cc = q - rr * (LBX + 1);
+        int r = clampi(r0 - 1 + rr, 0, ny - 1), i = clampi(i0 + cc, 0, nx - 1);
+        s_vh[rr][cc] = a.p.vh[r * P + i];
+    }
+    for (int q = tid; q < (LBY + 1) * (LBX + 1); q += NT) {
+        int rr = q / (LBX + 1), cc = q - rr * (LBX + 1);
+        int r = clampi(r0 + rr, 0, ny - 1), i = clampi(i0 + cc, 0, nx - 1);
+        s_el[rr][cc] = a.p.elv[r * P + i];
+    }
+    __syncthreads();
+
+    // New stage on the tile plus east/north halo (:92-115).
+    for (int q = tid; q < (LBY + 1) * (LBX + 1); q += NT) {
+        int rr = q / (LBX + 1), cc = q - rr * (LBX + 1);
+        int r = r0 + rr, i = i0 + cc;
+        R sn = R(0);
+        if (r < ny && i < nx) {
+            R s_old = a.p.stg[r * P + i];
+            bool interior = (i >= a.xl + 1) && (i <= a.xu - 1) && (r >= a.yl + 1) && (r <= a.yu - 1);
+            if (interior) {
+                R inv_cell_area_dt = a.dt / a.m.area[r];
+                R t1 = (s_uh[rr][cc + 1] - s_uh[rr][cc]) * a.m.dyl[i];
+                R t2 = s_vh[rr + 1][cc] * a.m.dxb[r + 1] - s_vh[rr][cc] * a.m.dxb[r];
+                sn = s_old - inv_cell_area_dt * (t1 + t2);
+            } else if (a.bc_stage && on_bc_ring(i, r, nx, ny, a.bext)) {
+                sn = a.p.stg_o[r * P + i];  // set by the edge kernel at time+dt/2
+            } else {
+                sn = s_old;
+            }
+        }
+        s_sn[rr][cc] = sn;
+    }
+    __syncthreads();
+
+    const R g = K<R>::gravity();
+    const R half = K<R>::half();
+    const R one = K<R>::one();
+    const R zero = K<R>::zero();
+    const R mad = K<R>::min_depth();
+#pragma unroll
+    for (int k = 0; k < LBY / LTY; k++) {
+        const int rr = threadIdx.y + k * LTY, cc = threadIdx.x;
+        const int r = r0 + rr, i = i0 + cc;
+        if (r >= ny || i >= nx) continue;
+        const int64_t o = r * P + i;
+        const R sn = s_sn[rr][cc];
+        a.p.stg_o[o] = sn;
+        if (a.p.max_stage && i >= a.xl && i <= a.xu && r >= a.yl && r <= a.yu) {
+            R mx = a.p.max_stage[o];
+            a.p.max_stage[o] = (sn > mx) ? sn : mx;
+        }
+        R uh = s_uh[rr][cc + 1];
+        R vh = s_vh[rr + 1][cc];
+        if (i >= a.xl && i <= a.xu - 1 && r >= a.yl && r <= a.yu - 1) {
+            const R inv_cell_area_dt_g = g * a.dt / a.m.area[r];
+            const R inv_cell_area_dt_vh_g = g * a.dt / (half * (a.m.area[r] + a.m.area[r + 1]));
+            const R e0 = s_el[rr][cc], e_e = s_el[rr][cc + 1], e_n = s_el[rr + 1][cc];
+            const R s_e = s_sn[rr][cc + 1], s_n = s_sn[rr + 1][cc];
+            R h_iph, h_jph, wet_iph, wet_jph;
+            if (TRUELY_LINEAR) {
+                bool wi = (e0 < -mad + a.msl) && (e_e < -mad + a.msl);
+                h_iph = wi ? (a.msl - half * (e_e + e0)) : zero;
+                bool wj = (e_n < -mad + a.msl) && (e0 < -mad + a.msl);
+                h_jph = wj ? (a.msl - half * (e_n + e0)) : zero;
+                wet_iph = one;
+                wet_jph = one;
+            } else {
+                bool wi = (sn - e0 > mad) && (s_e - e_e > mad);
+                h_iph = wi ? (half * ((s_e + sn) - (e_e + e0))) : zero;
+                bool wj = (s_n - e_n > mad) && (sn - e0 > mad);
+                h_jph = wj ? (half * ((s_n + sn) - (e_n + e0))) : zero;
+                wet_iph = (h_iph > zero) ? one : zero;
+                wet_jph = (h_jph > zero) ? one : zero;
+            }
+            const R dw_j = s_n - sn;
+            R uh_n = uh * wet_iph - inv_cell_area_dt_g * h_iph * (s_e - sn) * a.m.dyl[i + 1];
+            R vh_n = vh * wet_jph - inv_cell_area_dt_vh_g * h_jph * dw_j * a.m.dxb[r + 1];
+            if (CORIOLIS) {
+                // Pre-update 2-point averages (:409-428); rows/cols clamp like
+                // the reference's j=1 and max(xL-1,1) special cases.
+                const R vh_iph_jmh = half * (s_vh[rr][cc] + s_vh[rr][cc + 1]);
+                const R vh_iph_jph = half * (s_vh[rr + 1][cc] + s_vh[rr + 1][cc + 1]);
+                const R uh_i_j = half * (s_uh[rr][cc + 1] + s_uh[rr][cc]);
+                const R uh_i_jp1 = half * (s_uh[rr + 1][cc + 1] + s_uh[rr + 1][cc]);
+                const R dt_half_coriolis = a.dt * a.m.cor[r] * half * ((h_iph > zero) ? one : zero);
+                const R dt_half_coriolis_jph = a.dt * a.m.cor_be[r + 1] * half * ((h_jph > zero) ? one : zero);
+                uh_n = uh_n + dt_half_coriolis * (vh_iph_jmh + vh_iph_jph);
+                vh_n = vh_n - dt_half_coriolis_jph * (uh_i_j + uh_i_jp1);
+            }
+            if (a.lin_fric) {
+                uh_n = a.lin_fric_mult * uh_n;
+                vh_n = a.lin_fric_mult * vh_n;
+            }
+            uh = uh_n;
+            vh = vh_n;
+        }
+        a.p.uh_o[o] = uh;
+        a.p.vh_o[o] = vh;
+    }
+}
+
+// One block: boundary stage/elevation at time+dt/2, boundary flux sums,
+// time bookkeeping (:117-205, :571).
+template <typename R>
+__global__ void __launch_bounds__(512) linear_edge_kernel(const LinArgs<R> a, DevScalars *sc, int n_ext,
+                                                          BoundaryFn bf)
+{
+    const int nx = a.p.nx, ny = a.p.ny;
+    const int64_t P = a.p.pitch;
+    const double time0 = sc->time;
+    const double t_half = time0 + (double)(a.dt * K<R>::half());
+    if (a.bc_stage) {
+        const int nring = 2 * nx + 2 * ny;
+        for (int q = threadIdx.x; q < nring; q += blockDim.x) {
+            int i, r, side;
+            if (q < ny) { i = 0; r = q; side = 3; }
+            else if (q < 2 * ny) { i = nx - 1; r = q - ny; side = 1; }
+            else if (q < 2 * ny + nx) { i = q - 2 * ny; r = 0; side = 2; }
+            else { i = q - 2 * ny - nx; r = ny - 1; side = 0; }
+            if (!a.bext[side]) continue;
+            R stg, elv;
+            boundary_function<R>(bf, a.m.x, t_half, i, r, stg, elv);
+            a.p.stg_o[r * P + i] = stg;
+            a.p.elv[r * P + i] = elv;
+        }
+    }
+    // Boundary flux sums of the interior lines, using pre-update UH/VH.
+    __shared__ double red[4][32];
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int i = n_ext + threadIdx.x; i <= nx - n_ext - 1; i += blockDim.x) {
+        acc[0] += (double)a.p.vh[(int64_t)(ny - n_ext - 1) * P + i];
+        acc[2] += (double)a.p.vh[(int64_t)(n_ext - 1) * P + i];
+    }
+    for (int r = n_ext + threadIdx.x; r <= ny - n_ext - 1; r += blockDim.x) {
+        acc[1] += (double)a.p.uh[(int64_t)r * P + (nx - n_ext - 1)];
+        acc[3] += (double)a.p.uh[(int64_t)r * P + (n_ext - 1)];
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int k = 0; k < 4; k++) {
+        double v = acc[k];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) red[k][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s[4];
+        const int nw = blockDim.x >> 5;
+        for (int k = 0; k < 4; k++) {
+            double v = 0.0;
+            for (int w = 0; w < nw; w++) v += red[k][w];
+            s[k] = v;
+        }
+        sc->boundary_flux_store[0] = s[0] * (double)a.m.dxb[ny - n_ext];
+        sc->boundary_flux_store[1] = s[1] * (double)a.m.dyl[nx - n_ext];
+        sc->boundary_flux_store[2] = -(s[2] * (double)a.m.dxb[n_ext]);
+        sc->boundary_flux_store[3] = -(s[3] * (double)a.m.dyl[n_ext]);
+        double tot = 0.0;
+        for (int k = 0; k < 4; k++) tot += sc->boundary_flux_store[k];
+        sc->boundary_flux_evolve_integral = tot * (double)a.dt;
+        sc->boundary_flux_time_integral += sc->boundary_flux_evolve_integral;
+        sc->time0 = time0;
+        sc->time = t_half + (double)(K<R>::half() * a.dt);
+        sc->dt = (double)a.dt;
+        sc->dt_last_update = (double)a.dt;
+        sc->evolve_step_dt = sc->time - time0;
+        sc->nsteps_advanced += 1;
+    }
+}
+
+template <typename R>
+__global__ void max_stage_kernel(int nx, int ny, int64_t P, const R *stg, R *mx, int xl, int xu, int yl, int yu)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int r = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i < xl || i > xu || r < yl || r > yu || i >= nx || r >= ny) return;
+    int64_t o = r * P + i;
+    R s = stg[o], m = mx[o];
+    mx[o] = (s > m) ? s : m;
+}
+
+template <typename R>
+__global__ void gauge_kernel(int64_t P, const R *stg, const R *uh, const R *vh, const int *site_ij, int n,
+                             double *records, int capacity, DevScalars *sc)
+{
+    const int rec = sc->gauge_records;
+    for (int g = threadIdx.x; g < n; g += blockDim.x) {
+        if (rec < capacity) {
+            int i = site_ij[2 * g], r = site_ij[2 * g + 1];
+            int64_t o = (int64_t)r * P + i;
+            double *dst = records + ((int64_t)rec * n + g) * 3;
+            dst[0] = (double)stg[o];
+            dst[1] = (double)uh[o];
+            dst[2] = (double)vh[o];
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) sc->gauge_records = rec + 1;
+}
+
+}  // namespace
+
+template <typename R>
+cudaError_t launch_linear_step(const StepPlanes<R> &p, const Metrics<R> &m, const StepConfig &c, R dt,
+                               DevScalars *sc, cudaStream_t s, const LaunchHook &hook)
+{
+    LinArgs<R> a;
+    a.p = p;
+    a.m = m;
+    a.xl = c.xl; a.xu = c.xu; a.yl = c.yl; a.yu = c.yu;
+    a.bc_stage = (c.bc_kind == 2) ? 1 : 0;
+    for (int k = 0; k < 4; k++) a.bext[k] = c.bext[k];
+    a.dt = dt;
+    a.msl = R(c.msl_linear);
+    R lfc = R(c.linear_friction_coeff);
+    a.lin_fric = (lfc != R(0)) ? 1 : 0;
+    a.lin_fric_mult = a.lin_fric ? (R(1) / (R(1) + dt * lfc)) : R(0);
+
+    hook(CAT_LINEAR_EDGE, 0);
+    linear_edge_kernel<R><<<1, 512, 0, s>>>(a, sc, c.exterior_cells_width, c.bf);
+    hook(CAT_LINEAR_EDGE, 1);
+    dim3 block(LBX, LTY);
+    dim3 grid((p.nx + LBX - 1) / LBX, (p.ny + LBY - 1) / LBY);
+    const bool cor = c.coriolis != 0, tl = c.truely_linear != 0;
+    hook(CAT_LINEAR_MAIN, 0);
+    if (cor && tl) linear_step_kernel<R, true, true><<<grid, block, 0, s>>>(a);
+    else if (cor && !tl) linear_step_kernel<R, true, false><<<grid, block, 0, s>>>(a);
+    else if (!cor && tl) linear_step_kernel<R, false, true><<<grid, block, 0, s>>>(a);
+    else linear_step_kernel<R, false, false><<<grid, block, 0, s>>>(a);
+    hook(CAT_LINEAR_MAIN, 1);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_update_max_stage(int nx, int ny, int64_t pitch, const R *stg, R *max_stage, const StepConfig &c,
+                                    cudaStream_t s)
+{
+    dim3 block(32, 8);
+    dim3 grid((nx + 31) / 32, (ny + 7) / 8);
+    max_stage_kernel<R><<<grid, block, 0, s>>>(nx, ny, pitch, stg, max_stage, c.xl, c.xu, c.yl, c.yu);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_gauges(int64_t pitch, const R *stg, const R *uh, const R *vh, const int *site_ij, int n,
+                          double *records, int capacity, DevScalars *sc, cudaStream_t s)
+{
+    gauge_kernel<R><<<1, 256, 0, s>>>(pitch, stg, uh, vh, site_ij, n, records, capacity, sc);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_linear_step<double>(const StepPlanes<double> &, const Metrics<double> &,
+                                                const StepConfig &, double, DevScalars *, cudaStream_t,
+                                                const LaunchHook &);
+template cudaError_t launch_linear_step<float>(const StepPlanes<float> &, const Metrics<float> &,
+                                               const StepConfig &, float, DevScalars *, cudaStream_t,
+                                               const LaunchHook &);
+template cudaError_t launch_update_max_stage<double>(int, int, int64_t, const double *, double *,
+                                                     const StepConfig &, cudaStream_t);
+template cudaError_t launch_update_max_stage<float>(int, int, int64_t, const float *, float *,
+                                                    const StepConfig &, cudaStream_t);
+template cudaError_t launch_gauges<double>(int64_t, const double *, const double *, const double *, const int *,
+                                           int, double *, int, DevScalars *, cudaStream_t);
+template cudaError_t launch_gauges<float>(int64_t, const float *, const float *, const float *, const int *, int,
+                                          double *, int, DevScalars *, cudaStream_t);
+
+}  // namespace swals

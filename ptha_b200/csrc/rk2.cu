@@ -1,0 +1,822 @@
+// rk2.cu -- nonlinear finite-volume steps ('rk2', 'euler') on sm_100a.
+//
+// Restates, per Euler stage, in ONE fused kernel:
+//   compute_depth_and_velocity            domain_mod.f90:1360-1419
+//   compute_fluxes_DE1_low_fr_diffusion   compute_fluxes_alternatives_include.f90:25-36
+//     -> DE1_inner_include.f90:78-727 (NS/EW edge loops),
+//        :735-862 (theta wet/dry limiter + MC gradients),
+//        extrapolation_limiting_mod.f90:44-79 (MC limiter)
+//   update_U_manning / _chezy             update_U_DE1_inner_include.f90:14-99
+//   the CFL max-reduction                 DE1_inner_include.f90:426-430,712-727
+// and the rk2 driver (timestepping_alternatives_include.f90:64-146): stage 2
+// averages with the backed-up state in the same pass.
+//
+// Each CTA owns a 32x8 tile of cells.  It stages the tile plus a 2-cell cross
+// halo (the 5-point stencil of the limiter) in shared memory after the
+// depth/velocity fix-ups, computes the limited gradients, then every NS and
+// EW edge touching the tile (edges on tile borders are recomputed by both
+// neighbours, ~8% extra), then updates its cells.  Fluxes, depth, velocity
+// and explicit sources never reach HBM.  Edge loop bounds follow the
+// reference exactly: edges exist only for i=2..nx, j=2..ny (1-based); the
+// outer NS/EW gradients are zero; explicit_source of row 1 stays zero.
+// Arithmetic order mirrors the reference statement by statement and the
+// library is compiled without FMA contraction, so FP64 results equal the
+// IEEE-strict oracle except where a libm function (pow) differs.
+#include "swals_kernels.h"
+
+namespace swals {
+namespace {
+
+constexpr int TX = 32;
+constexpr int TY = 8;
+constexpr int NT = TX * TY;
+constexpr int CW = TX + 4;   // cell window columns (i0-2 .. i0+TX+1)
+constexpr int CH = TY + 4;   // cell window rows    (r0-2 .. r0+TY+1)
+
+enum { MODE_CFL = 0, MODE_STAGE1 = 1, MODE_STAGE2 = 2 };
+enum { FRIC_MANNING = 0, FRIC_CHEZY = 1, FRIC_NONE = 2 };
+
+template <typename R>
+struct Rk2Args {
+    int nx, ny;
+    int64_t P;
+    const R *stg, *uh, *vh;        // stage input (U0 for stage 1, U1 for stage 2)
+    const R *stg0, *uh0, *vh0;     // backup U0 (stage 2 average)
+    R *stg_o, *uh_o, *vh_o;        // stage output
+    const R *elv;
+    const R *nsq;                  // manning_squared
+    R *max_stage;
+    Metrics<R> m;
+    R theta, half_cfl;
+    R lin_fric;                    // linear_friction_coeff
+    double dt_fixed;               // used when dt_from_cfl == 0
+    int dt_from_cfl;               // stage dt = 1/max(1/maximum_timestep, CFL max) (adaptive)
+    double max_dt_inv_init;        // 1/maximum_timestep, rounded to R
+    int write_cfl;                 // accumulate the CFL max into sc
+    int n_ext;
+    int bc_ring;                   // a boundary routine rewrites the outer ring after this stage
+    int bext[4];
+    R *side;                       // stage-2 pre-average values of the outer two rings
+    double *lines;                 // flux_STG on the 4 boundary-flux lines: N[nx], E[ny], S[nx], W[ny]
+    DevScalars *sc;
+};
+
+template <typename R> struct Cell { R stg, dep, u, v, elv; };
+
+__device__ __forceinline__ void atomic_max_pos_double(unsigned long long *addr, double v)
+{
+    atomicMax(addr, (unsigned long long)__double_as_longlong(v));
+}
+
+// MC limiter, extrapolation_limiting_mod.f90:63-79 (sign(1,a) == copysign).
+template <typename R>
+__device__ __forceinline__ R mc_gradient(R local, R lower, R upper, R th)
+{
+    const R a = upper - local;
+    const R b = local - lower;
+    const R sa = copysign(R(1), a);
+    const R sb = copysign(R(1), b);
+    const R half_sasb = R(0.5) * (sa + sb);
+    const R d = rmin(R(fabs(a)), R(fabs(b))) * half_sasb * th;
+    const R e = R(0.5) * (a + b);
+    const R c = (d == R(0)) ? R(0) : e;
+    return (d > R(0)) ? rmin(c, d) : rmax(c, d);
+}
+
+// theta_wd of DE1_inner_include.f90:751-757 / :813-819.
+template <typename R>
+__device__ __forceinline__ R theta_wd(R d0, R d1, R d2, R theta)
+{
+    const R coef4 = R(1) / (K<R>::limiter_coef2() - K<R>::limiter_coef1());
+    const R mindep = rmin(rmin(d0, d1), d2) - K<R>::min_depth();
+    const R maxdep = rmax(rmax(d0, d1), d2) + K<R>::limiter_coef3() * K<R>::min_depth();
+    const R theta_local = coef4 * (mindep / maxdep - K<R>::limiter_coef1());
+    return rmax(theta * rmin(R(1), theta_local), R(0));
+}
+
+template <typename R> struct Grad { R ds, dd, du, dv; };
+
+template <typename R>
+struct EdgeRes {
+    R f[3];          // STG, UH, VH flux (already multiplied by edge length)
+    double es_pos;   // explicit-source contribution to the cell on the + side
+    double es_neg;   // contribution to the cell on the - side
+};
+
+// One Audusse/HLL edge of DE1_inner_include.f90 (:187-430 NS, :456-716 EW).
+// NS=true: normal velocity v, edge between (i,j-1) and (i,j).
+template <typename R, bool NS>
+__device__ __forceinline__ void edge_flux(const Cell<R> &cn, const Grad<R> &gn, const Cell<R> &cp, const Grad<R> &gp,
+                                          R edge_len, R dx_cfl_half_inv, EdgeRes<R> &out, double &cfl_cand)
+{
+    const R half = R(0.5);
+    const double half_gravity = (double)(half * K<R>::gravity());
+    const R EPS = R(1.0e-12);
+    const R EPS_gs = R(sqrt(K<R>::gravity() * K<R>::min_depth()));
+    const R beta = R(1.0);
+
+    R stage_neg = cn.stg + half * gn.ds;
+    R stage_pos = cp.stg - half * gp.ds;
+    double depth_neg = (double)(cn.dep + half * gn.dd);
+    double depth_pos = (double)(cp.dep - half * gp.dd);
+    R u_neg = cn.u + half * gn.du;
+    R u_pos = cp.u - half * gp.du;
+    R v_neg = cn.v + half * gn.dv;
+    R v_pos = cp.v - half * gp.dv;
+    double depth_neg_c = (double)cn.dep;
+    double depth_pos_c = (double)cp.dep;
+
+    R z_neg = R((double)stage_neg - depth_neg);
+    R z_pos = R((double)stage_pos - depth_pos);
+    R z_half = rmax(z_neg, z_pos);
+
+    R stage_neg_star = rmax(stage_neg, z_half);
+    double depth_neg_star = (double)(stage_neg_star - z_half);
+    if (depth_neg_star == 0.0) { u_neg = R(0); v_neg = R(0); }
+    R ud_neg = R((double)u_neg * depth_neg_star);
+    R vd_neg = R((double)v_neg * depth_neg_star);
+    R gs_neg = R(sqrt((double)K<R>::gravity() * depth_neg_star));
+
+    R stage_pos_star = rmax(stage_pos, z_half);
+    double depth_pos_star = (double)(stage_pos_star - z_half);
+    if (depth_pos_star == 0.0) { u_pos = R(0); v_pos = R(0); }
+    R ud_pos = R((double)u_pos * depth_pos_star);
+    R vd_pos = R((double)v_pos * depth_pos_star);
+    R gs_pos = R(sqrt((double)K<R>::gravity() * depth_pos_star));
+
+    const R vel_beta_neg = (NS ? v_neg : u_neg) * beta;
+    const R vel_beta_pos = (NS ? v_pos : u_pos) * beta;
+
+    const R s_max = rmax(rmax(vel_beta_neg + gs_neg, vel_beta_pos + gs_pos), R(0));
+    const R s_min = rmin(rmin(vel_beta_neg - gs_neg, vel_beta_pos - gs_pos), R(0));
+    const double denom = (double)(s_max - s_min);
+    double inv_denom;
+    if (denom > (double)EPS && (gs_pos > EPS_gs || gs_neg > EPS_gs))
+        inv_denom = (double)edge_len / denom;
+    else
+        inv_denom = 0.0;
+    const R sminsmax = s_min * s_max * R(1);
+    const R fr2num = ((v_neg * v_neg + v_pos * v_pos) + u_neg * u_neg) + u_pos * u_pos;
+    const R fr2den = (gs_neg * gs_neg + gs_pos * gs_pos) + R(1.0e-10);
+    const R fr2 = beta * R(sqrt(rmax(R(0.001), rmin(R(1), fr2num / fr2den))));
+
+    const R qn_neg = NS ? vd_neg : ud_neg, qn_pos = NS ? vd_pos : ud_pos;
+    const R qt_neg = NS ? ud_neg : vd_neg, qt_pos = NS ? ud_pos : vd_pos;
+    const R f_mass = R((double)((s_max * qn_neg - s_min * qn_pos) + sminsmax * (stage_pos_star - stage_neg_star)) *
+                       inv_denom);
+    const R f_norm = R((double)((s_max * qn_neg * vel_beta_neg - s_min * qn_pos * vel_beta_pos) +
+                                fr2 * sminsmax * (qn_pos - qn_neg)) * inv_denom);
+    const R f_tran = R((double)((s_max * qt_neg * vel_beta_neg - s_min * qt_pos * vel_beta_pos) +
+                                fr2 * sminsmax * (qt_pos - qt_neg)) * inv_denom);
+    out.f[0] = f_mass;
+    out.f[1] = NS ? f_tran : f_norm;
+    out.f[2] = NS ? f_norm : f_tran;
+
+    const double half_g_hh_edge = inv_denom * half_gravity *
+        ((double)s_max * depth_neg_star * depth_neg_star - (double)s_min * depth_pos_star * depth_pos_star);
+    const double bs_neg = half_gravity * ((depth_neg_star - depth_neg) * (depth_neg_star + depth_neg) -
+                                          (depth_neg + depth_neg_c) * (double)(z_neg - cn.elv));
+    out.es_neg = bs_neg * (double)edge_len - half_g_hh_edge;
+    const double bs_pos = half_gravity * ((depth_pos_star - depth_pos) * (depth_pos_star + depth_pos) -
+                                          (depth_pos + depth_pos_c) * (double)(z_pos - cp.elv));
+    out.es_pos = (0.0 - bs_pos * (double)edge_len) + half_g_hh_edge;
+
+    const double max_speed = (double)rmax(s_max, -s_min);
+    cfl_cand = (max_speed > (double)EPS) ? max_speed * (double)dx_cfl_half_inv : 0.0;
+}
+
+template <typename R>
+struct Smem {
+    Cell<R> cell[CH][CW];
+    Grad<R> gns[TY + 2][TX];     // NS gradients, rows r0-1 .. r0+TY, cols i0 .. i0+TX-1
+    Grad<R> gew[TY][TX + 2];     // EW gradients, rows r0 .. r0+TY-1, cols i0-1 .. i0+TX
+    EdgeRes<R> ens[TY + 1][TX];  // NS edges r0 .. r0+TY
+    EdgeRes<R> eew[TY][TX + 1];  // EW edges i0 .. i0+TX
+    double red[NT / 32];
+    long long negfix[NT / 32];
+};
+
+template <typename R, int MODE, bool SPH, bool COR, int FRIC>
+__global__ void __launch_bounds__(NT) rk2_stage_kernel(const Rk2Args<R> a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Smem<R> &S = *reinterpret_cast<Smem<R> *>(smem_raw);
+
+    const int nx = a.nx, ny = a.ny;
+    const int64_t P = a.P;
+    const int i0 = blockIdx.x * TX, r0 = blockIdx.y * TY;
+    const int tid = threadIdx.x;
+    const R mad = K<R>::min_depth();
+
+    // ---- Phase A: cells with the depth/velocity fix-ups (domain_mod.f90:1387-1412)
+    long long negfix = 0;
+    for (int q = tid; q < CH * CW; q += NT) {
+        const int rr = q / CW, cc = q - rr * CW;
+        const int r = r0 - 2 + rr, i = i0 - 2 + cc;
+        Cell<R> c;
+        c.stg = R(0); c.dep = R(0); c.u = R(0); c.v = R(0); c.elv = R(0);
+        if (r >= 0 && r < ny && i >= 0 && i < nx) {
+            const int64_t o = (int64_t)r * P + i;
+            R s = a.stg[o], e = a.elv[o];
+            R dep = s - e;
+            if (dep > mad) {
+                R depth_inv = R(1) / dep;
+                c.u = a.uh[o] * depth_inv;
+                c.v = a.vh[o] * depth_inv;
+            } else {
+                if (dep < R(0)) {
+                    dep = R(0);
+                    s = e;
+                    if (rr >= 2 && rr < 2 + TY && cc >= 2 && cc < 2 + TX) negfix += 1;
+                }
+            }
+            c.stg = s; c.dep = dep; c.elv = e;
+        }
+        S.cell[rr][cc] = c;
+    }
+    __syncthreads();
+
+    // ---- Phase B: limited gradients (DE1_inner_include.f90:735-862)
+    for (int q = tid; q < (TY + 2) * TX; q += NT) {
+        const int rr = q / TX, cc = q - rr * TX;        // cell (i0+cc, r0-1+rr)
+        const int r = r0 - 1 + rr, i = i0 + cc;
+        Grad<R> g; g.ds = R(0); g.dd = R(0); g.du = R(0); g.dv = R(0);
+        if (r > 0 && r < ny - 1 && i < nx) {
+            const Cell<R> &lo = S.cell[rr][cc + 2], &c = S.cell[rr + 1][cc + 2], &up = S.cell[rr + 2][cc + 2];
+            const R th = theta_wd<R>(lo.dep, c.dep, up.dep, a.theta);
+            g.ds = mc_gradient<R>(c.stg, lo.stg, up.stg, th);
+            g.dd = mc_gradient<R>(c.dep, lo.dep, up.dep, th);
+            g.du = mc_gradient<R>(c.u, lo.u, up.u, th);
+            g.dv = mc_gradient<R>(c.v, lo.v, up.v, th);
+        }
+        S.gns[rr][cc] = g;
+    }
+    for (int q = tid; q < TY * (TX + 2); q += NT) {
+        const int rr = q / (TX + 2), cc = q - rr * (TX + 2);  // cell (i0-1+cc, r0+rr)
+        const int r = r0 + rr, i = i0 - 1 + cc;
+        Grad<R> g; g.ds = R(0); g.dd = R(0); g.du = R(0); g.dv = R(0);
+        if (i > 0 && i < nx - 1 && r < ny) {
+            const Cell<R> &lo = S.cell[rr + 2][cc], &c = S.cell[rr + 2][cc + 1], &up = S.cell[rr + 2][cc + 2];
+            const R th = theta_wd<R>(lo.dep, c.dep, up.dep, a.theta);
+            g.ds = mc_gradient<R>(c.stg, lo.stg, up.stg, th);
+            g.dd = mc_gradient<R>(c.dep, lo.dep, up.dep, th);
+            g.du = mc_gradient<R>(c.u, lo.u, up.u, th);
+            g.dv = mc_gradient<R>(c.v, lo.v, up.v, th);
+        }
+        S.gew[rr][cc] = g;
+    }
+    __syncthreads();
+
+    // ---- Phase C: edges touching the tile
+    double cfl = 0.0;
+    const R inv2 = R(1) / (a.m.dyl[0] * a.half_cfl);  // dx_cfl_half_inv(2): NS edges
+    for (int q = tid; q < (TY + 1) * TX; q += NT) {
+        const int rr = q / TX, cc = q - rr * TX;        // edge between (i, r-1) and (i, r)
+        const int r = r0 + rr, i = i0 + cc;
+        EdgeRes<R> e;
+        e.f[0] = R(0); e.f[1] = R(0); e.f[2] = R(0); e.es_pos = 0.0; e.es_neg = 0.0;
+        if (r >= 1 && r <= ny - 1 && i >= 1 && i <= nx - 1) {
+            double cand;
+            edge_flux<R, true>(S.cell[rr + 1][cc + 2], S.gns[rr][cc], S.cell[rr + 2][cc + 2], S.gns[rr + 1][cc],
+                               a.m.dxb[r], inv2, e, cand);
+            cfl = fmax(cfl, cand);
+            if (MODE != MODE_CFL && a.lines) {
+                if (r == ny - a.n_ext && i >= a.n_ext && i <= nx - a.n_ext - 1) a.lines[i] = (double)e.f[0];
+                if (r == a.n_ext && i >= a.n_ext && i <= nx - a.n_ext - 1) a.lines[nx + ny + i] = (double)e.f[0];
+            }
+        }
+        if (MODE != MODE_CFL) S.ens[rr][cc] = e;
+    }
+    for (int q = tid; q < TY * (TX + 1); q += NT) {
+        const int rr = q / (TX + 1), cc = q - rr * (TX + 1);  // edge between (i-1, r) and (i, r)
+        const int r = r0 + rr, i = i0 + cc;
+        EdgeRes<R> e;
+        e.f[0] = R(0); e.f[1] = R(0); e.f[2] = R(0); e.es_pos = 0.0; e.es_neg = 0.0;
+        if (r >= 1 && r <= ny - 1 && i >= 1 && i <= nx - 1) {
+            const R inv1 = R(1) / (a.m.dxb[r] * a.half_cfl);  // dx_cfl_half_inv(1)
+            double cand;
+            edge_flux<R, false>(S.cell[rr + 2][cc + 1], S.gew[rr][cc], S.cell[rr + 2][cc + 2], S.gew[rr][cc + 1],
+                                a.m.dyl[i], inv1, e, cand);
+            cfl = fmax(cfl, cand);
+            if (MODE != MODE_CFL && a.lines) {
+                if (i == nx - a.n_ext && r >= a.n_ext && r <= ny - a.n_ext - 1) a.lines[nx + r] = (double)e.f[0];
+                if (i == a.n_ext && r >= a.n_ext && r <= ny - a.n_ext - 1) a.lines[2 * nx + ny + r] = (double)e.f[0];
+            }
+        }
+        if (MODE != MODE_CFL) S.eew[rr][cc] = e;
+    }
+
+    // Block max of the CFL candidates and the negative-depth count.
+    const int lane = tid & 31, warp = tid >> 5;
+    if (a.write_cfl || MODE == MODE_CFL) {
+        for (int o = 16; o > 0; o >>= 1) cfl = fmax(cfl, __shfl_down_sync(0xffffffffu, cfl, o));
+        if (lane == 0) S.red[warp] = cfl;
+    }
+    if (MODE != MODE_CFL) {
+        for (int o = 16; o > 0; o >>= 1) negfix += __shfl_down_sync(0xffffffffu, negfix, o);
+        if (lane == 0) S.negfix[warp] = negfix;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        if (a.write_cfl || MODE == MODE_CFL) {
+            double mx = S.red[0];
+            for (int w = 1; w < NT / 32; w++) mx = fmax(mx, S.red[w]);
+            if (mx > 0.0) atomic_max_pos_double(&a.sc->max_dt_inv_bits, mx);
+        }
+        if (MODE != MODE_CFL) {
+            long long n = 0;
+            for (int w = 0; w < NT / 32; w++) n += S.negfix[w];
+            if (n) atomicAdd((unsigned long long *)&a.sc->negative_depth_fix_counter, (unsigned long long)n);
+        }
+    }
+    if (MODE == MODE_CFL) return;
+
+    // ---- Phase D: update_U (update_U_DE1_inner_include.f90:38-96)
+    const int cc = tid & (TX - 1), rr = tid / TX;
+    const int i = i0 + cc, r = r0 + rr;
+    if (i >= nx || r >= ny) return;
+
+    R dt;
+    if (a.dt_from_cfl) {
+        // domain%max_dt of the first stage: 1/max(1/maximum_timestep, max speed/(dx cfl/2))
+        double bits_max = __longlong_as_double((long long)a.sc->max_dt_inv_bits);
+        R inv = R(fmax(a.max_dt_inv_init, bits_max));
+        dt = R(1) / inv;
+    } else {
+        dt = R(a.dt_fixed);
+    }
+
+    const int64_t o = (int64_t)r * P + i;
+    const Cell<R> &c = S.cell[rr + 2][cc + 2];
+    // Mutated U (compute_depth_and_velocity zeroes UH/VH where depth <= minimum_allowed_depth)
+    R U_stg = c.stg;
+    R Um_uh, Um_vh;  // U(i,j,UH/VH) after the fix-ups, before the update
+    if (c.dep > mad) { Um_uh = a.uh[o]; Um_vh = a.vh[o]; }
+    else { Um_uh = R(0); Um_vh = R(0); }
+    R U_uh = Um_uh, U_vh = Um_vh;
+
+    const R inv_cell_area_dt = dt / a.m.area[r];
+    const EdgeRes<R> &n_lo = S.ens[rr][cc], &n_hi = S.ens[rr + 1][cc];
+    const EdgeRes<R> &w_lo = S.eew[rr][cc], &w_hi = S.eew[rr][cc + 1];
+    U_stg = U_stg - inv_cell_area_dt * ((n_hi.f[0] - n_lo.f[0]) + (w_hi.f[0] - w_lo.f[0]));
+    U_uh = U_uh - inv_cell_area_dt * ((n_hi.f[1] - n_lo.f[1]) + (w_hi.f[1] - w_lo.f[1]));
+    U_vh = U_vh - inv_cell_area_dt * ((n_hi.f[2] - n_lo.f[2]) + (w_hi.f[2] - w_lo.f[2]));
+
+    // Explicit sources of cell (i, r), accumulated in the reference's order.
+    double es_uh = 0.0, es_vh = 0.0, es_jm1 = 0.0;
+    if (r >= 1) {
+        if (i >= 1) {
+            es_vh = n_lo.es_pos;   // NS loop (:403-409)
+            es_uh = w_lo.es_pos;   // EW loop (:649-654)
+            if (SPH) {
+                const double dep = (double)c.dep;
+                const double hg = (double)(R(0.5) * K<R>::gravity());
+                es_vh = es_vh + hg * dep * dep * (double)(a.m.dxb[r + 1] - a.m.dxb[r]);
+                if (COR) {
+                    const R cm = a.m.area[r] * a.m.cor[r];
+                    es_uh = es_uh + (double)(cm * Um_vh);
+                    es_vh = es_vh - (double)(cm * Um_uh);
+                }
+                const R cm2 = a.m.area[r] * a.m.tanlat[r] * c.u;
+                es_uh = es_uh + (double)(cm2 * Um_vh);
+                es_vh = es_vh - (double)(cm2 * Um_uh);
+            }
+        }
+        es_uh = es_uh + ((i + 1 <= nx - 1) ? w_hi.es_neg : 0.0);  // explicit_source_im1_work (:721)
+    }
+    if (r + 1 <= ny - 1 && i >= 1) es_jm1 = n_hi.es_neg;          // explicit_source_VH_j_minus_1(i, j+1)
+
+    if (U_stg <= c.elv + mad) {
+        U_uh = R(0);
+        U_vh = R(0);
+    } else {
+        R implicit_factor;
+        if (FRIC == FRIC_NONE) {
+            implicit_factor = R(1);
+        } else {
+            const R depth = c.dep;
+            const R power = (FRIC == FRIC_CHEZY) ? R(-2.0) : R(-7.0) / R(3.0);
+            const R fs = a.nsq[o] * R(sqrt(c.u * c.u + c.v * c.v)) * R(pow(rmax(depth, mad), power));
+            implicit_factor = R(1) / ((R(1) + dt * K<R>::gravity() * rmax(depth, R(0)) * fs) + dt * a.lin_fric);
+        }
+        U_uh = R((double)U_uh + (double)inv_cell_area_dt * es_uh);
+        U_uh = U_uh * implicit_factor;
+        U_vh = R((double)U_vh + (double)inv_cell_area_dt * (es_vh + es_jm1));
+        U_vh = U_vh * implicit_factor;
+    }
+
+    if (MODE == MODE_STAGE2) {
+        if (a.bc_ring) {
+            // Keep the pre-average outer two rings for the boundary kernel.
+            R *side = a.side;
+            const int cols[4] = {0, 1, nx - 2, nx - 1};
+            const int rows[4] = {0, 1, ny - 2, ny - 1};
+            for (int k = 0; k < 4; k++) {
+                if (i == cols[k]) {
+                    R *d = side + ((int64_t)k * ny + r) * 3;
+                    d[0] = U_stg; d[1] = U_uh; d[2] = U_vh;
+                }
+                if (r == rows[k]) {
+                    R *d = side + (int64_t)4 * ny * 3 + ((int64_t)k * nx + i) * 3;
+                    d[0] = U_stg; d[1] = U_uh; d[2] = U_vh;
+                }
+            }
+        }
+        U_stg = R(0.5) * (U_stg + a.stg0[o]);
+        U_uh = R(0.5) * (U_uh + a.uh0[o]);
+        U_vh = R(0.5) * (U_vh + a.vh0[o]);
+        if (a.max_stage) {
+            const bool ring = a.bc_ring && ((i == 0 && a.bext[3]) || (i == nx - 1 && a.bext[1]) ||
+                                            (r == 0 && a.bext[2]) || (r == ny - 1 && a.bext[0]));
+            if (!ring) {
+                R mx = a.max_stage[o];
+                a.max_stage[o] = (U_stg > mx) ? U_stg : mx;
+            }
+        }
+    }
+    a.stg_o[o] = U_stg;
+    a.uh_o[o] = U_uh;
+    a.vh_o[o] = U_vh;
+}
+
+
+// ---------------------------------------------------------------------------
+// Boundary routines on the non-staggered grid (boundary_mod.f90:21-75 and
+// :78-163).  One block: the west/east pass completes before the south/north
+// pass, as in the reference's two OpenMP loops (corner cells end with the
+// south/north values).
+//   STAGE_MODE 1: in place on the stage output (stage 1 of rk2, euler).
+//   STAGE_MODE 2: rk2 stage 2.  The stage kernel already wrote the averaged
+//                 state; here the outer ring is recomputed from the saved
+//                 pre-average values, the boundary values applied, and then
+//                 averaged with the backed-up U0 ring.
+template <typename R>
+struct BcArgs {
+    int nx, ny;
+    int64_t P;
+    int kind;               // SWALS_BC_*
+    int bext[4];            // N,E,S,W
+    BoundaryFn bf;
+    const R *x;
+    R *stg, *uh, *vh;       // stage output planes
+    const R *stg0, *uh0, *vh0;  // backup U0 (mode 2)
+    R *elv;
+    R *side;                // mode 2: saved outer two rings (updated in place)
+    R *max_stage;
+    int stage_mode;
+    int dt_from_cfl;
+    double dt_fixed;
+    double max_dt_inv_init;
+    int n_dt;               // boundary time = time0 + n_dt * dt
+    DevScalars *sc;
+};
+
+template <typename R>
+__device__ __forceinline__ R *side_ptr(const BcArgs<R> &a, int i, int r)
+{
+    const int nx = a.nx, ny = a.ny;
+    int k = -1;
+    if (i == 0) k = 0; else if (i == 1) k = 1; else if (i == nx - 1) k = 3; else if (i == nx - 2) k = 2;
+    if (k >= 0) return a.side + ((int64_t)k * ny + r) * 3;
+    if (r == 0) k = 0; else if (r == 1) k = 1; else if (r == ny - 1) k = 3; else k = 2;
+    return a.side + (int64_t)4 * ny * 3 + ((int64_t)k * nx + i) * 3;
+}
+
+template <typename R>
+__device__ __forceinline__ R bc_get(const BcArgs<R> &a, int i, int r, int v)
+{
+    if (a.stage_mode == 2) return side_ptr(a, i, r)[v];
+    const R *pl = (v == 0) ? a.stg : (v == 1) ? a.uh : a.vh;
+    return pl[(int64_t)r * a.P + i];
+}
+
+template <typename R>
+__device__ __forceinline__ void bc_set(const BcArgs<R> &a, int i, int r, R s, R u, R v)
+{
+    if (a.stage_mode == 2) {
+        R *d = side_ptr(a, i, r);
+        d[0] = s; d[1] = u; d[2] = v;
+        if (r == 0 || r == 1 || r == a.ny - 1 || r == a.ny - 2) {
+            // keep the row copy of corner-adjacent cells consistent too
+            int k = (r == 0) ? 0 : (r == 1) ? 1 : (r == a.ny - 1) ? 3 : 2;
+            R *d2 = a.side + (int64_t)4 * a.ny * 3 + ((int64_t)k * a.nx + i) * 3;
+            d2[0] = s; d2[1] = u; d2[2] = v;
+        }
+        return;
+    }
+    const int64_t o = (int64_t)r * a.P + i;
+    a.stg[o] = s; a.uh[o] = u; a.vh[o] = v;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(1024) rk2_boundary_kernel(const BcArgs<R> a)
+{
+    const int nx = a.nx, ny = a.ny;
+    const int64_t P = a.P;
+    double dtd;
+    if (a.dt_from_cfl) {
+        double bits_max = __longlong_as_double((long long)a.sc->max_dt_inv_bits);
+        R inv = R(fmax(a.max_dt_inv_init, bits_max));
+        dtd = (double)(R(1) / inv);
+    } else {
+        dtd = (double)R(a.dt_fixed);
+    }
+    double t = a.sc->time;
+    for (int k = 0; k < a.n_dt; k++) t = t + dtd;
+
+    // West / east pass
+    for (int r = threadIdx.x; r < ny; r += blockDim.x) {
+        for (int side = 0; side < 2; side++) {
+            const bool west = (side == 0);
+            if (!(west ? a.bext[3] : a.bext[1])) continue;
+            const int i = west ? 0 : nx - 1;
+            const int in = west ? 1 : nx - 2;
+            if (a.kind == 1) {  // transmissive: all four variables from the inner neighbour
+                a.elv[(int64_t)r * P + i] = a.elv[(int64_t)r * P + in];
+                bc_set(a, i, r, bc_get(a, in, r, 0), bc_get(a, in, r, 1), bc_get(a, in, r, 2));
+            } else {
+                R s, e;
+                boundary_function<R>(a.bf, a.x, t, i, r, s, e);
+                a.elv[(int64_t)r * P + i] = e;
+                bc_set(a, i, r, s, bc_get(a, in, r, 1), R(0));
+            }
+        }
+    }
+    __syncthreads();
+    // South / north pass
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+        for (int side = 0; side < 2; side++) {
+            const bool south = (side == 0);
+            if (!(south ? a.bext[2] : a.bext[0])) continue;
+            const int r = south ? 0 : ny - 1;
+            const int rn = south ? 1 : ny - 2;
+            if (a.kind == 1) {
+                a.elv[(int64_t)r * P + i] = a.elv[(int64_t)rn * P + i];
+                bc_set(a, i, r, bc_get(a, i, rn, 0), bc_get(a, i, rn, 1), bc_get(a, i, rn, 2));
+            } else {
+                R s, e;
+                boundary_function<R>(a.bf, a.x, t, i, r, s, e);
+                a.elv[(int64_t)r * P + i] = e;
+                bc_set(a, i, r, s, R(0), bc_get(a, i, rn, 2));
+            }
+        }
+    }
+    if (a.stage_mode != 2) return;
+    __syncthreads();
+    // rk2 average of the boundary ring and its max_stage.
+    const int nring = 2 * nx + 2 * ny;
+    for (int q = threadIdx.x; q < nring; q += blockDim.x) {
+        int i, r;
+        if (q < nx) { i = q; r = 0; }
+        else if (q < 2 * nx) { i = q - nx; r = ny - 1; }
+        else if (q < 2 * nx + ny) { i = 0; r = q - 2 * nx; }
+        else { i = nx - 1; r = q - 2 * nx - ny; }
+        const bool bc = (r == 0 && a.bext[2]) || (r == ny - 1 && a.bext[0]) || (i == 0 && a.bext[3]) ||
+                        (i == nx - 1 && a.bext[1]);
+        if (!bc) continue;
+        // Cells on both a row and a column of the ring appear twice; the
+        // values are identical so the duplicate write is harmless.
+        const R *d;
+        if ((r == 0 && a.bext[2]) || (r == ny - 1 && a.bext[0])) {
+            const int k = (r == 0) ? 0 : 3;
+            d = a.side + (int64_t)4 * ny * 3 + ((int64_t)k * nx + i) * 3;
+        } else {
+            const int k = (i == 0) ? 0 : 3;
+            d = a.side + ((int64_t)k * ny + r) * 3;
+        }
+        const int64_t o = (int64_t)r * P + i;
+        const R s = R(0.5) * (d[0] + a.stg0[o]);
+        a.stg[o] = s;
+        a.uh[o] = R(0.5) * (d[1] + a.uh0[o]);
+        a.vh[o] = R(0.5) * (d[2] + a.vh0[o]);
+        if (a.max_stage) {
+            R mx = a.max_stage[o];
+            a.max_stage[o] = (s > mx) ? s : mx;
+        }
+    }
+}
+
+// End of a step: domain%max_dt, time, boundary-flux integrals, counters
+// (timestepping_alternatives_include.f90:36-50,121-144; domain_mod.f90:1800-1810).
+template <typename R>
+__global__ void __launch_bounds__(1024) rk2_finalize_kernel(int nx, int ny, int n_ext, const double *lines1,
+                                                            const double *lines2, int euler_only, int dt_from_cfl,
+                                                            double dt_fixed, double max_dt_inv_init, DevScalars *sc)
+{
+    __shared__ double red[8][32];
+    double acc[8];
+    for (int k = 0; k < 8; k++) acc[k] = 0.0;
+    const int L = 2 * nx + 2 * ny;
+    for (int q = threadIdx.x; q < L; q += blockDim.x) {
+        int line, idx;
+        if (q < nx) { line = 0; idx = q; }
+        else if (q < nx + ny) { line = 1; idx = q - nx; }
+        else if (q < 2 * nx + ny) { line = 2; idx = q - nx - ny; }
+        else { line = 3; idx = q - 2 * nx - ny; }
+        const int lim = (line == 0 || line == 2) ? nx : ny;
+        if (idx < n_ext || idx > lim - n_ext - 1) continue;
+        acc[line] += lines1[q];
+        if (!euler_only) acc[4 + line] += lines2[q];
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int k = 0; k < 8; k++) {
+        double v = acc[k];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) red[k][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    const int nw = blockDim.x >> 5;
+    double s[8];
+    for (int k = 0; k < 8; k++) {
+        double v = 0.0;
+        for (int w = 0; w < nw; w++) v += red[k][w];
+        s[k] = v;
+    }
+    double bits_max = __longlong_as_double((long long)sc->max_dt_inv_bits);
+    R max_dt_inv = R(fmax(max_dt_inv_init, bits_max));
+    const double max_dt = (double)(R(1) / max_dt_inv);
+    const double dt = dt_from_cfl ? max_dt : (double)R(dt_fixed);
+    const double time0 = sc->time;
+    double store1[4] = {s[0], s[1], -s[2], -s[3]};
+    double store2[4] = {s[4], s[5], -s[6], -s[7]};
+    double tot1 = 0.0, tot2 = 0.0;
+    for (int k = 0; k < 4; k++) { tot1 += store1[k]; tot2 += store2[k]; }
+    double integral = 0.0 + dt * tot1;
+    if (!euler_only) {
+        integral = integral + dt * tot2;
+        integral = 0.5 * integral;
+        for (int k = 0; k < 4; k++) sc->boundary_flux_store[k] = store2[k];
+    } else {
+        for (int k = 0; k < 4; k++) sc->boundary_flux_store[k] = store1[k];
+    }
+    sc->boundary_flux_evolve_integral = integral;
+    sc->boundary_flux_time_integral += integral;
+    sc->max_dt = max_dt;
+    sc->dt = dt;
+    sc->dt_last_update = dt;
+    sc->time0 = time0;
+    sc->time = time0 + dt;
+    sc->evolve_step_dt = sc->time - time0;
+    sc->nsteps_advanced += 1;
+    sc->max_dt_inv_bits = 0ull;
+}
+
+template <typename R, int MODE, bool SPH, bool COR, int FRIC>
+cudaError_t launch_stage(const Rk2Args<R> &a, cudaStream_t s)
+{
+    static bool configured = false;
+    const size_t smem = sizeof(Smem<R>);
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(rk2_stage_kernel<R, MODE, SPH, COR, FRIC>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    dim3 grid((a.nx + TX - 1) / TX, (a.ny + TY - 1) / TY);
+    rk2_stage_kernel<R, MODE, SPH, COR, FRIC><<<grid, NT, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <typename R, int MODE>
+cudaError_t dispatch_stage(const Rk2Args<R> &a, const StepConfig &c, cudaStream_t s)
+{
+    const int fric = c.nofriction ? FRIC_NONE : (c.chezy ? FRIC_CHEZY : FRIC_MANNING);
+    if (c.spherical) {
+        if (c.coriolis) {
+            if (fric == FRIC_MANNING) return launch_stage<R, MODE, true, true, FRIC_MANNING>(a, s);
+            if (fric == FRIC_CHEZY) return launch_stage<R, MODE, true, true, FRIC_CHEZY>(a, s);
+            return launch_stage<R, MODE, true, true, FRIC_NONE>(a, s);
+        }
+        if (fric == FRIC_MANNING) return launch_stage<R, MODE, true, false, FRIC_MANNING>(a, s);
+        if (fric == FRIC_CHEZY) return launch_stage<R, MODE, true, false, FRIC_CHEZY>(a, s);
+        return launch_stage<R, MODE, true, false, FRIC_NONE>(a, s);
+    }
+    if (fric == FRIC_MANNING) return launch_stage<R, MODE, false, false, FRIC_MANNING>(a, s);
+    if (fric == FRIC_CHEZY) return launch_stage<R, MODE, false, false, FRIC_CHEZY>(a, s);
+    return launch_stage<R, MODE, false, false, FRIC_NONE>(a, s);
+}
+
+}  // namespace
+
+template <typename R>
+cudaError_t launch_rk2_step(R *const planes[3][3], int &cur, R *elv, R *max_stage, R *manning_sq, int nx, int ny,
+                            int64_t pitch, const Metrics<R> &m, const StepConfig &c, bool has_dt, double dt,
+                            bool euler_only, const Rk2Buffers &buf, DevScalars *sc, cudaStream_t s,
+                            const LaunchHook &hook)
+{
+    const int A = cur, B = (cur + 1) % 3, C = (cur + 2) % 3;
+    const bool bc = (c.bc_kind == 1 || c.bc_kind == 2);
+    double *lines1 = reinterpret_cast<double *>(buf.partials);
+    double *lines2 = lines1 + (2 * nx + 2 * ny);
+    const double max_dt_inv_init = (double)(R(1) / R(c.maximum_timestep));
+
+    Rk2Args<R> a;
+    a.nx = nx; a.ny = ny; a.P = pitch;
+    a.elv = elv; a.nsq = manning_sq; a.max_stage = nullptr; a.m = m;
+    a.theta = R(c.theta); a.half_cfl = R(0.5) * R(c.cfl);
+    a.lin_fric = R(c.linear_friction_coeff);
+    a.dt_fixed = dt;
+    a.max_dt_inv_init = max_dt_inv_init;
+    a.n_ext = c.exterior_cells_width;
+    a.bc_ring = 0;
+    for (int k = 0; k < 4; k++) a.bext[k] = c.bext[k];
+    a.side = reinterpret_cast<R *>(buf.side);
+    a.sc = sc;
+    a.stg0 = nullptr; a.uh0 = nullptr; a.vh0 = nullptr;
+    cudaError_t e;
+
+    if (!has_dt) {
+        // Adaptive: the CFL of U0 must be known before the first update.
+        Rk2Args<R> p = a;
+        p.stg = planes[A][0]; p.uh = planes[A][1]; p.vh = planes[A][2];
+        p.stg_o = nullptr; p.uh_o = nullptr; p.vh_o = nullptr;
+        p.dt_from_cfl = 0; p.write_cfl = 1; p.lines = nullptr;
+        hook(CAT_CFL, 0);
+        e = dispatch_stage<R, MODE_CFL>(p, c, s);
+        hook(CAT_CFL, 1);
+        if (e != cudaSuccess) return e;
+    }
+    // Stage 1: U0 -> B
+    a.stg = planes[A][0]; a.uh = planes[A][1]; a.vh = planes[A][2];
+    a.stg_o = planes[B][0]; a.uh_o = planes[B][1]; a.vh_o = planes[B][2];
+    a.dt_from_cfl = has_dt ? 0 : 1;
+    a.write_cfl = has_dt ? 1 : 0;
+    a.lines = lines1;
+    if (euler_only) a.max_stage = nullptr;
+    hook(CAT_STAGE1, 0);
+    e = dispatch_stage<R, MODE_STAGE1>(a, c, s);
+    hook(CAT_STAGE1, 1);
+    if (e != cudaSuccess) return e;
+
+    BcArgs<R> b;
+    b.nx = nx; b.ny = ny; b.P = pitch; b.kind = c.bc_kind;
+    for (int k = 0; k < 4; k++) b.bext[k] = c.bext[k];
+    b.bf = c.bf; b.x = m.x; b.elv = elv; b.side = a.side; b.max_stage = nullptr;
+    b.dt_from_cfl = a.dt_from_cfl; b.dt_fixed = dt; b.max_dt_inv_init = max_dt_inv_init; b.sc = sc;
+    b.stg0 = nullptr; b.uh0 = nullptr; b.vh0 = nullptr;
+    if (bc) {
+        b.stg = planes[B][0]; b.uh = planes[B][1]; b.vh = planes[B][2];
+        b.stage_mode = 1; b.n_dt = 1;
+        hook(CAT_BC1, 0);
+        rk2_boundary_kernel<R><<<1, 1024, 0, s>>>(b);
+        hook(CAT_BC1, 1);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    if (euler_only) {
+        if (max_stage) {
+            hook(CAT_MAXSTAGE, 0);
+            e = launch_update_max_stage<R>(nx, ny, pitch, planes[B][0], max_stage, c, s);
+            hook(CAT_MAXSTAGE, 1);
+            if (e != cudaSuccess) return e;
+        }
+        hook(CAT_FINALIZE, 0);
+        rk2_finalize_kernel<R><<<1, 1024, 0, s>>>(nx, ny, c.exterior_cells_width, lines1, lines2, 1,
+                                                  a.dt_from_cfl, dt, max_dt_inv_init, sc);
+        hook(CAT_FINALIZE, 1);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        cur = B;
+        return cudaSuccess;
+    }
+    // Stage 2: B -> C, averaged with U0 (A)
+    Rk2Args<R> a2 = a;
+    a2.stg = planes[B][0]; a2.uh = planes[B][1]; a2.vh = planes[B][2];
+    a2.stg0 = planes[A][0]; a2.uh0 = planes[A][1]; a2.vh0 = planes[A][2];
+    a2.stg_o = planes[C][0]; a2.uh_o = planes[C][1]; a2.vh_o = planes[C][2];
+    a2.dt_from_cfl = has_dt ? 0 : 1;
+    a2.write_cfl = 0;
+    a2.lines = lines2;
+    a2.bc_ring = bc ? 1 : 0;
+    a2.max_stage = max_stage;
+    hook(CAT_STAGE2, 0);
+    e = dispatch_stage<R, MODE_STAGE2>(a2, c, s);
+    hook(CAT_STAGE2, 1);
+    if (e != cudaSuccess) return e;
+    if (bc) {
+        b.stg = planes[C][0]; b.uh = planes[C][1]; b.vh = planes[C][2];
+        b.stg0 = planes[A][0]; b.uh0 = planes[A][1]; b.vh0 = planes[A][2];
+        b.stage_mode = 2; b.n_dt = 2; b.max_stage = max_stage;
+        hook(CAT_BC2, 0);
+        rk2_boundary_kernel<R><<<1, 1024, 0, s>>>(b);
+        hook(CAT_BC2, 1);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    hook(CAT_FINALIZE, 0);
+    rk2_finalize_kernel<R><<<1, 1024, 0, s>>>(nx, ny, c.exterior_cells_width, lines1, lines2, 0, a.dt_from_cfl,
+                                              dt, max_dt_inv_init, sc);
+    hook(CAT_FINALIZE, 1);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    cur = C;
+    return cudaSuccess;
+}
+
+template cudaError_t launch_rk2_step<double>(double *const[3][3], int &, double *, double *, double *, int, int,
+                                             int64_t, const Metrics<double> &, const StepConfig &, bool, double,
+                                             bool, const Rk2Buffers &, DevScalars *, cudaStream_t,
+                                             const LaunchHook &);
+template cudaError_t launch_rk2_step<float>(float *const[3][3], int &, float *, float *, float *, int, int,
+                                            int64_t, const Metrics<float> &, const StepConfig &, bool, double,
+                                            bool, const Rk2Buffers &, DevScalars *, cudaStream_t,
+                                            const LaunchHook &);
+
+}  // namespace swals

@@ -1,0 +1,101 @@
+// swals_common.cuh -- shared definitions for the sm_100a SWALS kernels.
+//
+// Device layout (one domain):
+//   STG, UH, VH, ELV planes, each ny rows of `pitch` elements, row j holding
+//   cells i = 0..nx-1 (the reference's U(i+1, j+1, k)); pitch is a multiple
+//   of 32 elements so every row starts on a 256-byte boundary (FP64) and
+//   every warp-wide row access is whole 128-byte sectors.
+//   State planes (STG, UH, VH) exist in 3 copies so a step reads one copy
+//   and writes another (no in-place races between CTAs); ELV, max_stage and
+//   manning_squared exist once.
+//   1-D metric arrays (dxb, dyl, area, coriolis, ...) hold the reference's
+//   Fortran arrays shifted to 0-based: dxb0[j] = distance_bottom_edge(j+1).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace swals {
+
+// global_mod.f90:37-55, domain_mod.f90:111-117, spherical_mod.f90:9-17.
+template <typename R> struct K {
+    static __host__ __device__ __forceinline__ R gravity() { return R(9.8); }
+    static __host__ __device__ __forceinline__ R half() { return R(0.5); }
+    static __host__ __device__ __forceinline__ R one() { return R(1.0); }
+    static __host__ __device__ __forceinline__ R zero() { return R(0.0); }
+    static __host__ __device__ __forceinline__ R min_depth() { return R(1.0e-05); }
+    static __host__ __device__ __forceinline__ R wall_elevation() { return R(1.0e+6); }
+    static __host__ __device__ __forceinline__ R limiter_coef1() { return R(0.1); }
+    static __host__ __device__ __forceinline__ R limiter_coef2() { return R(0.3); }
+    static __host__ __device__ __forceinline__ R limiter_coef3() { return R(100.0); }
+};
+
+template <typename R> __device__ __forceinline__ R rmin(R a, R b) { return (b < a) ? b : a; }
+template <typename R> __device__ __forceinline__ R rmax(R a, R b) { return (b > a) ? b : a; }
+
+// Metric arrays, 0-based copies of the Fortran arrays.
+template <typename R> struct Metrics {
+    const R *dxb;     // ny+1: distance_bottom_edge
+    const R *dyl;     // nx+1: distance_left_edge
+    const R *area;    // ny:   area_cell_y
+    const R *cor;     // ny:   coriolis
+    const R *cor_be;  // ny+1: coriolis_bottom_edge
+    const R *tanlat;  // ny:   tanlat_on_radius_earth
+    const R *x;       // nx
+    const R *y;       // ny
+};
+
+// Device-side scalar state of a domain (time, timestep, reductions).
+struct DevScalars {
+    double time;
+    double dt;                 // timestep used by the current step
+    double max_dt;             // domain%max_dt
+    unsigned long long max_dt_inv_bits;  // running max of 1/dt (positive doubles order as integers)
+    unsigned long long nonfinite;        // nonzero when a stability check found NaN/Inf
+    long long negative_depth_fix_counter;
+    long long nsteps_advanced;
+    double time0;              // time at the start of the current step
+    double boundary_flux_store[4];
+    double boundary_flux_evolve_integral;
+    double boundary_flux_time_integral;
+    double dt_last_update;
+    double evolve_step_dt;
+    int    gauge_records;      // number of gauge records written
+    int    pad;
+};
+
+// Boundary-function parameters (SWALS_BF_*), evaluated on the device.
+struct BoundaryFn {
+    int kind;
+    int pad;
+    double p[8];
+};
+
+__host__ __device__ inline int64_t round_up(int64_t a, int64_t b) { return (a + b - 1) / b * b; }
+
+// Analytic boundary_function values [stage, uh, vh, elev] at cell (i,j)
+// (0-based), time t.  i0/j0 tests use the 0-based cell index.
+template <typename R>
+__device__ __forceinline__ void boundary_function(const BoundaryFn &bf, const R *x, double t, int i, int j,
+                                                  R &stg, R &elv)
+{
+    (void)j;
+    if (bf.kind == 1) {  // SWALS_BF_SOLITARY_WEST_WALLS
+        R H = R(bf.p[0]), dep = R(bf.p[1]), x0 = R(bf.p[2]);
+        if (i == 0) {
+            R k = R(sqrt(R(3.0) * H / (R(4.0) * dep * dep * dep)));
+            R c = R(sqrt(K<R>::gravity() * (dep + H)));
+            R arg = k * (x[0] - x0 - c * R(t));
+            R ch = R(cosh(arg));
+            stg = H / (ch * ch);
+            elv = -dep;
+        } else {
+            stg = K<R>::wall_elevation();
+            elv = K<R>::wall_elevation();
+        }
+    } else {
+        stg = R(0);
+        elv = R(0);
+    }
+}
+
+}  // namespace swals

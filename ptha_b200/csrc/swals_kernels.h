@@ -1,0 +1,82 @@
+// swals_kernels.h -- host-side launch interface of the SWALS CUDA kernels
+// (internal to libswalsgpu; the public ABI is include/swals_gpu.h).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "swals_common.cuh"
+
+namespace swals {
+
+// Kernel categories for the per-launch timers (include/swals_gpu.h).
+enum LaunchCat {
+    CAT_CFL = 0, CAT_STAGE1 = 1, CAT_BC1 = 2, CAT_STAGE2 = 3, CAT_BC2 = 4, CAT_FINALIZE = 5,
+    CAT_LINEAR_EDGE = 6, CAT_LINEAR_MAIN = 7, CAT_GAUGES = 8, CAT_MAXSTAGE = 9, CAT_COUNT = 10
+};
+
+// Called before (phase 0) and after (phase 1) every kernel launch.
+struct LaunchHook {
+    void (*fn)(void *ctx, int cat, int phase) = nullptr;
+    void *ctx = nullptr;
+    void operator()(int cat, int phase) const { if (fn) fn(ctx, cat, phase); }
+};
+
+template <typename R>
+struct StepPlanes {
+    int nx, ny;
+    int64_t pitch;          // elements
+    const R *stg, *uh, *vh; // state read by the step
+    R *stg_o, *uh_o, *vh_o; // state written by the step
+    R *elv;
+    R *max_stage;           // may be null
+    R *manning_sq;          // rk2 family
+};
+
+struct StepConfig {
+    int xl, xu, yl, yu;     // 0-based inclusive active region (domain%xL-1 ...)
+    int bext[4];            // boundary_exterior N,E,S,W
+    int bc_kind;            // SWALS_BC_*
+    BoundaryFn bf;
+    int spherical, coriolis, nofriction, chezy, truely_linear;
+    double msl_linear, linear_friction_coeff, theta, cfl, maximum_timestep;
+    int exterior_cells_width;
+};
+
+// Linear leapfrog, one full step (domain_mod_linear_solver_include.f90:58-571).
+template <typename R>
+cudaError_t launch_linear_step(const StepPlanes<R> &p, const Metrics<R> &m, const StepConfig &c,
+                               R dt, DevScalars *sc, cudaStream_t s, const LaunchHook &hook);
+
+// max_stage = max(max_stage, STG) over the active region (domain_mod.f90:2243-2290).
+template <typename R>
+cudaError_t launch_update_max_stage(int nx, int ny, int64_t pitch, const R *stg, R *max_stage,
+                                    const StepConfig &c, cudaStream_t s);
+
+// Gauge sampling: append [STG,UH,VH] at sites (point_gauge_mod.f90:208-245).
+template <typename R>
+cudaError_t launch_gauges(int64_t pitch, const R *stg, const R *uh, const R *vh, const int *site_ij, int n,
+                          double *records, int capacity, DevScalars *sc, cudaStream_t s);
+
+// rk2 / euler (timestepping_alternatives_include.f90:8-146).
+struct Rk2Buffers {
+    void *side;            // ring buffer used when a boundary routine is active
+    void *partials;        // per-block partial sums (deterministic reductions)
+    int64_t partials_len;
+};
+
+template <typename R>
+cudaError_t launch_rk2_step(R *const planes[3][3], int &cur, R *elv, R *max_stage, R *manning_sq, int nx, int ny,
+                            int64_t pitch, const Metrics<R> &m, const StepConfig &c, bool has_dt, double dt,
+                            bool euler_only, const Rk2Buffers &buf, DevScalars *sc, cudaStream_t s,
+                            const LaunchHook &hook);
+
+// Reductions used by diagnostics.
+template <typename R>
+cudaError_t launch_volume_interior(int nx, int ny, int64_t pitch, const R *stg, const R *elv, const R *area,
+                                   int n_ext, double *row_sums, double *out, cudaStream_t s);
+template <typename R>
+cudaError_t launch_timestep_max(int nx, int ny, int64_t pitch, const R *stg, const R *elv, const R *dxb,
+                                const R *dyl, double msl, int linear, double cfl, double *block_min,
+                                int max_blocks, double *out, cudaStream_t s);
+
+}  // namespace swals
