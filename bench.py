@@ -34,8 +34,8 @@ if ROOT not in sys.path:
 
 METRIC = "cell-updates/s/GPU (fwd, batched, adjoint) at FP64-oracle tol; HBM % of peak"
 UNIT = "cell-updates/s"
-INNER = 2000          # model timesteps per bench step
-N = 2048
+INNER = 2000          # model timesteps per bench step (default)
+N = 2048              # grid cells per side (default)
 WORKLOAD = "rk2_beach_2048x2048_fp64_adaptive"
 # Algorithmic HBM bytes per cell for the fused FV stage kernel (FP64):
 #   stage 1 reads STG,UH,VH,ELV,n^2 and writes STG,UH,VH            = 8 planes
@@ -177,7 +177,11 @@ def run_ours(args, world, rank, local):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     from ptha_b200 import Domain, workloads
 
-    kw, U, gauges, nsq = workloads.rk2_beach(n=N)
+    global N, INNER
+    N, INNER = args.n, args.inner
+    kw, U, gauges, nsq = workloads.rk2_beach(n=N, dx=10.0 * 2048 / N, toe=17580.0 * N / 2048)
+    if args.real32:
+        kw["real_bytes"] = 4
     d = Domain(**kw, device=local)
     d.set_U(U)
     d.set_manning_squared(nsq)
@@ -192,6 +196,16 @@ def run_ours(args, world, rank, local):
     for _ in range(args.warmup):
         d.evolve_steps(INNER)
     d.synchronize()
+    if args.profile:
+        # Short untimed run for profilers: the warm-up above, then `steps`
+        # bench steps, nothing else.
+        for _ in range(args.steps):
+            d.evolve_steps(INNER)
+        d.synchronize()
+        if rank == 0:
+            print(json.dumps({"profile_run": True, "n": N, "inner": INNER, "launches": d.launch_count()}))
+        d.close()
+        return
 
     barrier()
     torch.cuda.synchronize()
@@ -229,16 +243,18 @@ def run_ours(args, world, rank, local):
     d.timers_enable(False)
     t1_ms, n1 = tm["fv_stage1"]
     t2_ms, n2 = tm["fv_stage2"]
-    bytes_kernel = cells * (BYTES_STAGE1 * n1 + BYTES_STAGE2 * n2)
+    es_scale = 0.5 if args.real32 else 1.0   # byte counts above are for 8-byte reals
+    bytes_kernel = cells * (BYTES_STAGE1 * n1 + BYTES_STAGE2 * n2) * es_scale
     achieved = bytes_kernel / ((t1_ms + t2_ms) / 1e3) / 1e9
     peak, peak_kind = hbm_peak()
     per_step_ms = {k: (v[0] / v[1] if v[1] else 0.0) for k, v in tm.items()}
 
     # End to end through the C ABI with host buffers: pinned H2D of the state,
     # INNER timesteps, D2H of the state, every step.
-    pin_in = torch.empty((4, N, N), dtype=torch.float64, pin_memory=True)
+    tdt = torch.float32 if args.real32 else torch.float64
+    pin_in = torch.empty((4, N, N), dtype=tdt, pin_memory=True)
     pin_in.copy_(torch.from_numpy(d.get_U()))
-    pin_out = torch.empty((4, N, N), dtype=torch.float64, pin_memory=True)
+    pin_out = torch.empty((4, N, N), dtype=tdt, pin_memory=True)
     h_in, h_out = pin_in.numpy(), pin_out.numpy()
     e2e_steps = 3
     barrier()
@@ -260,7 +276,7 @@ def run_ours(args, world, rank, local):
     d2h = int(h_out.nbytes)
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and N == 2048:
         try:
             cpu = cpu_baseline("rk2_beach", min_seconds=12.0)
         except Exception as ex:  # the baseline is reported, never required
@@ -270,8 +286,9 @@ def run_ours(args, world, rank, local):
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "nx": N, "ny": N, "timesteps_per_step": INNER,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.real32 else "f64", "data": "synthetic",
+            "config": {"workload": (f"rk2_beach_{N}x{N}_{'fp32' if args.real32 else 'fp64'}_adaptive"),
+                       "nx": N, "ny": N, "timesteps_per_step": INNER,
                        "timestepping_method": "rk2", "dt": "adaptive (CFL, cfl=0.99)", "theta": 1.6,
                        "manning_n": 0.025, "boundary": "solitary wave H/d=0.1 west, walls elsewhere",
                        "l2": "inputs larger than L2 (state 4x32 MB + manning 32 MB + max_stage 32 MB + "
@@ -282,7 +299,8 @@ def run_ours(args, world, rank, local):
                          "peak_source": peak_kind,
                          "bytes_per_cell": {"stage1": BYTES_STAGE1, "stage2": BYTES_STAGE2},
                          "traffic": profile_traffic("rk2_stage_kernel"),
-                         "step_effective_GBps": cells * BYTES_PER_CELL_UPDATE / (ms_max / args.steps / INNER / 1e3) / 1e9,
+                         "step_effective_GBps": cells * BYTES_PER_CELL_UPDATE * es_scale /
+                                                (ms_max / args.steps / INNER / 1e3) / 1e9,
                          "per_launch_ms": per_step_ms},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
@@ -305,8 +323,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--n", type=int, default=N, help="grid cells per side (default 2048)")
+    ap.add_argument("--inner", type=int, default=INNER, help="timesteps per bench step (default 2000)")
+    ap.add_argument("--real32", action="store_true", help="FP32 state (-DREALFLOAT analogue)")
+    ap.add_argument("--profile", action="store_true", help="short untimed run for ncu")
     args = ap.parse_args()
-    if args.warmup < 3:
+    if args.warmup < 3 and not args.profile:
         args.warmup = 3
     world, rank, local = dist_setup(args.gpus)
     if args.impl == "reference":

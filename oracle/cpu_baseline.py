@@ -13,7 +13,11 @@ import os
 import sys
 import time
 
-ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+# Run as a script, sys.path[0] is oracle/ itself, where `import oracle` would
+# find oracle/oracle.py instead of the package directory.
+sys.path = [p for p in sys.path if os.path.abspath(p or ".") != HERE]
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 

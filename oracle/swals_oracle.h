@@ -130,6 +130,7 @@ void ORACLE_FN(limited_gradient_dx_vectorized)(const REAL *U_local, const REAL *
 double ORACLE_FN(area_lonlat_rectangle)(double lon1, double lat1, double dlon, double dlat, int flat);
 void ORACLE_FN(gauge_site_index)(const double *xy, int32_t n, const double *ll,
         const double *dx, const int32_t *nxy, int32_t *site_index);
+double ORACLE_FN(pow_friction)(double x, int32_t chezy);
 void ORACLE_FN(boundary_function)(const oracle_domain *d, double t, int32_t i, int32_t j, REAL *out4);
 
 #ifdef __cplusplus

@@ -395,8 +395,8 @@ __global__ void __launch_bounds__(NT) rk2_stage_kernel(const Rk2Args<R> a)
             implicit_factor = R(1);
         } else {
             const R depth = c.dep;
-            const R power = (FRIC == FRIC_CHEZY) ? R(-2.0) : R(-7.0) / R(3.0);
-            const R fs = a.nsq[o] * R(sqrt(c.u * c.u + c.v * c.v)) * R(pow(rmax(depth, mad), power));
+            const R fs = a.nsq[o] * R(sqrt(c.u * c.u + c.v * c.v)) *
+                         R(pow_friction_cr<FRIC == FRIC_CHEZY>((double)rmax(depth, mad)));
             implicit_factor = R(1) / ((R(1) + dt * K<R>::gravity() * rmax(depth, R(0)) * fs) + dt * a.lin_fric);
         }
         U_uh = R((double)U_uh + (double)inv_cell_area_dt * es_uh);

@@ -32,6 +32,45 @@ template <typename R> struct K {
 template <typename R> __device__ __forceinline__ R rmin(R a, R b) { return (b < a) ? b : a; }
 template <typename R> __device__ __forceinline__ R rmax(R a, R b) { return (b > a) ? b : a; }
 
+// Correctly rounded friction power law pow(x, p), p = fl(-7/3) (Manning) or
+// -2 (Chezy), for x >= minimum_allowed_depth (update_U_DE1_inner_include.f90:
+// 72-75).  Double-double arithmetic: a Newton-corrected cube root, a
+// compensated reciprocal, and for fl(-7/3) the factor x**eps = 1 + eps*ln(x)
+// with eps = fl(-7/3) + 7/3.  Correct rounding makes the result independent
+// of any libm (the oracle uses the same definition; tests check both
+// against 300-bit arithmetic).
+struct DD { double hi, lo; };
+__device__ __forceinline__ DD dd_two_prod(double a, double b) { DD r; r.hi = a * b; r.lo = fma(a, b, -r.hi); return r; }
+__device__ __forceinline__ DD dd_fast_two_sum(double a, double b) { DD r; r.hi = a + b; r.lo = b - (r.hi - a); return r; }
+__device__ __forceinline__ DD dd_recip(DD p)
+{
+    const double y0 = 1.0 / p.hi;
+    DD t = dd_two_prod(p.hi, y0);
+    t.lo += p.lo * y0;
+    const double e = (1.0 - t.hi) - t.lo;
+    return dd_fast_two_sum(y0, y0 * e);
+}
+template <bool CHEZY>
+__device__ __forceinline__ double pow_friction_cr(double x)
+{
+    const DD x2 = dd_two_prod(x, x);
+    if (CHEZY) return dd_recip(x2).hi;
+    const double c0 = cbrt(x);
+    const DD s = dd_two_prod(c0, c0);
+    DD t = dd_two_prod(s.hi, c0);
+    t.lo += s.lo * c0;
+    const double r = (x - t.hi) - t.lo;
+    const DD c = dd_fast_two_sum(c0, r / (3.0 * c0 * c0));
+    DD p = dd_two_prod(x2.hi, c.hi);
+    p.lo += x2.hi * c.lo + x2.lo * c.hi;
+    p = dd_fast_two_sum(p.hi, p.lo);
+    const DD v = dd_recip(p);
+    const double q = 7.0 / 3.0;
+    const double eps = fma(-3.0, q, 7.0) / 3.0;
+    const double tl = eps * log(x);
+    return dd_fast_two_sum(v.hi, v.lo + v.hi * tl).hi;
+}
+
 // Metric arrays, 0-based copies of the Fortran arrays.
 template <typename R> struct Metrics {
     const R *dxb;     // ny+1: distance_bottom_edge

@@ -1,0 +1,27 @@
+"""The friction power law max(depth, mad)**p (update_U_DE1_inner_include.f90:
+72-75) is evaluated correctly rounded (p = fl(-7/3) for Manning, -2 for
+Chezy) so that oracle and GPU agree bit for bit whatever libm is present.
+Check the oracle's definition against 300-bit arithmetic."""
+import ctypes
+import random
+
+import mpmath
+import pytest
+
+from oracle import oracle as orc
+
+
+@pytest.mark.parametrize("chezy", [0, 1])
+def test_pow_friction_is_correctly_rounded(chezy):
+    lib = orc._load(False)
+    f = lib.oracle64_pow_friction
+    f.restype = ctypes.c_double
+    f.argtypes = [ctypes.c_double, ctypes.c_int32]
+    mpmath.mp.prec = 300
+    p = mpmath.mpf(-2.0 if chezy else -7.0 / 3.0)
+    rng = random.Random(1234 + chezy)
+    for k in range(20000):
+        u = rng.random()
+        x = 1e-5 * 10 ** (9 * u) if k % 2 else 1e-5 + 80 * u
+        want = float(mpmath.power(mpmath.mpf(x), p))
+        assert f(x, chezy) == want, (x, f(x, chezy), want)

@@ -30,6 +30,10 @@ def test_rk2_beach_solitary_wave(adaptive):
     _, errs = report(f"rk2 beach adaptive={adaptive}", g, o)
     for k in ("STG", "UH", "VH", "ELV"):
         assert errs[k] <= TOL64, errs
+    # Same operation order, no FMA contraction, correctly rounded pow:
+    # the FP64 state is expected to be bit-identical.
+    for k in ("STG", "UH", "VH", "ELV"):
+        assert errs[k + "_exact"] == 1.0, errs
     assert rel_err(g.max_stage(), o.max_stage, mask=water_mask(o.U[3])) <= TOL64
     st = g.state()
     assert st.time == pytest.approx(o.time, rel=1e-12)
