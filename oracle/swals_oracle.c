@@ -87,6 +87,52 @@ static double or_pow_friction(double x, int chezy)
 
 double ORACLE_FN(pow_friction)(double x, int32_t chezy) { return or_pow_friction(x, chezy); }
 
+/* Correctly rounded cosh for the analytic boundary functions, evaluated in
+ * double-double arithmetic exactly as the device library does (same
+ * operation sequence: a = k ln2 + r with a double-double ln2, exp(r) by the
+ * Horner form of its Taylor series to r^22/22!, exp(-|a|) by a compensated
+ * reciprocal), so oracle and GPU agree bit for bit whatever libm is present. */
+static or_dd or_two_sum(double a, double b) { or_dd r; r.hi = a + b; double bb = r.hi - a; r.lo = (a - (r.hi - bb)) + (b - bb); return r; }
+static or_dd or_dd_mul(or_dd a, or_dd b) { or_dd p = or_two_prod(a.hi, b.hi); p.lo += a.hi * b.lo + a.lo * b.hi; return or_fast_two_sum(p.hi, p.lo); }
+static or_dd or_dd_div_d(or_dd x, double n)
+{
+    double q1 = x.hi / n;
+    or_dd p = or_two_prod(q1, n);
+    double e = (((x.hi - p.hi) - p.lo) + x.lo) / n;
+    return or_fast_two_sum(q1, e);
+}
+static double or_cosh_cr(double a)
+{
+    double x = fabs(a);
+    if (x > 700.0) return x * 1.0e308;
+    const double ln2_hi = 6.93147180559945286227e-01, ln2_lo = 2.31904681384629955842e-17;
+    double k = rint(x * 1.44269504088896338700e+00);
+    or_dd p = or_two_prod(k, ln2_hi);
+    or_dd t = or_two_sum(x, -p.hi);
+    t.lo = (t.lo - p.lo) - k * ln2_lo;
+    or_dd r = or_fast_two_sum(t.hi, t.lo);
+    or_dd s; s.hi = 1.0; s.lo = 0.0;
+    for (int n = 22; n >= 1; n--) {
+        or_dd q = or_dd_div_d(or_dd_mul(r, s), (double)n);
+        or_dd u = or_two_sum(1.0, q.hi);
+        u.lo += q.lo;
+        s = or_fast_two_sum(u.hi, u.lo);
+    }
+    int ki = (int)k;
+    or_dd E; E.hi = ldexp(s.hi, ki); E.lo = ldexp(s.lo, ki);
+    double y0 = 1.0 / E.hi;
+    or_dd w = or_two_prod(E.hi, y0);
+    w.lo += E.lo * y0;
+    double e = (1.0 - w.hi) - w.lo;
+    or_dd inv = or_fast_two_sum(y0, y0 * e);
+    or_dd sum = or_two_sum(E.hi, inv.hi);
+    sum.lo += E.lo + inv.lo;
+    sum = or_fast_two_sum(sum.hi, sum.lo);
+    return 0.5 * sum.hi + 0.5 * sum.lo;
+}
+double ORACLE_FN(cosh_cr)(double a) { return or_cosh_cr(a); }
+
+
 static inline REAL rmin(REAL a, REAL b) { return (b < a) ? b : a; }
 static inline REAL rmax(REAL a, REAL b) { return (b > a) ? b : a; }
 static inline double dmin(double a, double b) { return (b < a) ? b : a; }
@@ -216,7 +262,7 @@ void ORACLE_FN(boundary_function)(const oracle_domain *d, double t, int32_t i, i
             REAL k = (REAL)sqrt((REAL)3.0 * H / ((REAL)4.0 * dep * dep * dep));
             REAL c = (REAL)sqrt(GRAVITY * (dep + H));
             REAL arg = k * (d->x[0] - x0 - c * (REAL)t);
-            REAL ch = (REAL)cosh(arg);
+            REAL ch = (REAL)or_cosh_cr((double)arg);
             out[0] = H / (ch * ch);
             out[1] = ZERO; out[2] = ZERO; out[3] = -dep;
         } else {

@@ -131,6 +131,7 @@ double ORACLE_FN(area_lonlat_rectangle)(double lon1, double lat1, double dlon, d
 void ORACLE_FN(gauge_site_index)(const double *xy, int32_t n, const double *ll,
         const double *dx, const int32_t *nxy, int32_t *site_index);
 double ORACLE_FN(pow_friction)(double x, int32_t chezy);
+double ORACLE_FN(cosh_cr)(double a);
 void ORACLE_FN(boundary_function)(const oracle_domain *d, double t, int32_t i, int32_t j, REAL *out4);
 
 #ifdef __cplusplus

@@ -79,6 +79,8 @@ bool is_staggered(int m) { return m == M_LINEAR || m == M_LF_LIN_NLFRIC || m == 
 
 }  // namespace
 
+void swals::set_last_error(const char *msg) { g_last_error = msg; }
+
 struct swals_domain {
     swals_domain_desc desc;
     int method = 0;

@@ -185,19 +185,65 @@ __device__ __forceinline__ void edge_flux(const Cell<R> &cn, const Grad<R> &gn, 
     cfl_cand = (max_speed > (double)EPS) ? max_speed * (double)dx_cfl_half_inv : 0.0;
 }
 
+// Structure-of-arrays shared-memory tiles (one array per field, so a warp's
+// accesses to one field are consecutive words).
+template <typename R, int H, int W>
+struct CellTile {
+    R stg[H][W], dep[H][W], u[H][W], v[H][W], elv[H][W];
+    __device__ __forceinline__ Cell<R> get(int r, int c) const
+    {
+        Cell<R> x;
+        x.stg = stg[r][c]; x.dep = dep[r][c]; x.u = u[r][c]; x.v = v[r][c]; x.elv = elv[r][c];
+        return x;
+    }
+    __device__ __forceinline__ void set(int r, int c, const Cell<R> &x)
+    {
+        stg[r][c] = x.stg; dep[r][c] = x.dep; u[r][c] = x.u; v[r][c] = x.v; elv[r][c] = x.elv;
+    }
+};
+template <typename R, int H, int W>
+struct GradTile {
+    R ds[H][W], dd[H][W], du[H][W], dv[H][W];
+    __device__ __forceinline__ Grad<R> get(int r, int c) const
+    {
+        Grad<R> g;
+        g.ds = ds[r][c]; g.dd = dd[r][c]; g.du = du[r][c]; g.dv = dv[r][c];
+        return g;
+    }
+    __device__ __forceinline__ void set(int r, int c, const Grad<R> &g)
+    {
+        ds[r][c] = g.ds; dd[r][c] = g.dd; du[r][c] = g.du; dv[r][c] = g.dv;
+    }
+};
+template <typename R, int H, int W>
+struct EdgeTile {
+    R f0[H][W], f1[H][W], f2[H][W];
+    double es_pos[H][W], es_neg[H][W];
+    __device__ __forceinline__ EdgeRes<R> get(int r, int c) const
+    {
+        EdgeRes<R> e;
+        e.f[0] = f0[r][c]; e.f[1] = f1[r][c]; e.f[2] = f2[r][c]; e.es_pos = es_pos[r][c]; e.es_neg = es_neg[r][c];
+        return e;
+    }
+    __device__ __forceinline__ void set(int r, int c, const EdgeRes<R> &e)
+    {
+        f0[r][c] = e.f[0]; f1[r][c] = e.f[1]; f2[r][c] = e.f[2]; es_pos[r][c] = e.es_pos; es_neg[r][c] = e.es_neg;
+    }
+};
+
 template <typename R>
 struct Smem {
-    Cell<R> cell[CH][CW];
-    Grad<R> gns[TY + 2][TX];     // NS gradients, rows r0-1 .. r0+TY, cols i0 .. i0+TX-1
-    Grad<R> gew[TY][TX + 2];     // EW gradients, rows r0 .. r0+TY-1, cols i0-1 .. i0+TX
-    EdgeRes<R> ens[TY + 1][TX];  // NS edges r0 .. r0+TY
-    EdgeRes<R> eew[TY][TX + 1];  // EW edges i0 .. i0+TX
+    CellTile<R, CH, CW> cell;
+    GradTile<R, TY + 2, TX> gns;     // NS gradients, rows r0-1 .. r0+TY, cols i0 .. i0+TX-1
+    GradTile<R, TY, TX + 2> gew;     // EW gradients, rows r0 .. r0+TY-1, cols i0-1 .. i0+TX
+    EdgeTile<R, TY + 1, TX> ens;     // NS edges r0 .. r0+TY
+    EdgeTile<R, TY, TX + 1> eew;     // EW edges i0 .. i0+TX
     double red[NT / 32];
     long long negfix[NT / 32];
 };
 
 template <typename R, int MODE, bool SPH, bool COR, int FRIC>
-__global__ void __launch_bounds__(NT) rk2_stage_kernel(const Rk2Args<R> a)
+__global__ void __launch_bounds__(NT, 3) rk2_stage_kernel(const Rk2Args<R> a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem<R> &S = *reinterpret_cast<Smem<R> *>(smem_raw);
@@ -232,7 +278,7 @@ __global__ void __launch_bounds__(NT) rk2_stage_kernel(const Rk2Args<R> a)
             }
             c.stg = s; c.dep = dep; c.elv = e;
         }
-        S.cell[rr][cc] = c;
+        S.cell.set(rr, cc, c);
     }
     __syncthreads();
 
@@ -242,28 +288,28 @@ __global__ void __launch_bounds__(NT) rk2_stage_kernel(const Rk2Args<R> a)
         const int r = r0 - 1 + rr, i = i0 + cc;
         Grad<R> g; g.ds = R(0); g.dd = R(0); g.du = R(0); g.dv = R(0);
         if (r > 0 && r < ny - 1 && i < nx) {
-            const Cell<R> &lo = S.cell[rr][cc + 2], &c = S.cell[rr + 1][cc + 2], &up = S.cell[rr + 2][cc + 2];
+            const Cell<R> lo = S.cell.get(rr, cc + 2), c = S.cell.get(rr + 1, cc + 2), up = S.cell.get(rr + 2, cc + 2);
             const R th = theta_wd<R>(lo.dep, c.dep, up.dep, a.theta);
             g.ds = mc_gradient<R>(c.stg, lo.stg, up.stg, th);
             g.dd = mc_gradient<R>(c.dep, lo.dep, up.dep, th);
             g.du = mc_gradient<R>(c.u, lo.u, up.u, th);
             g.dv = mc_gradient<R>(c.v, lo.v, up.v, th);
         }
-        S.gns[rr][cc] = g;
+        S.gns.set(rr, cc, g);
     }
     for (int q = tid; q < TY * (TX + 2); q += NT) {
         const int rr = q / (TX + 2), cc = q - rr * (TX + 2);  // cell (i0-1+cc, r0+rr)
         const int r = r0 + rr, i = i0 - 1 + cc;
         Grad<R> g; g.ds = R(0); g.dd = R(0); g.du = R(0); g.dv = R(0);
         if (i > 0 && i < nx - 1 && r < ny) {
-            const Cell<R> &lo = S.cell[rr + 2][cc], &c = S.cell[rr + 2][cc + 1], &up = S.cell[rr + 2][cc + 2];
+            const Cell<R> lo = S.cell.get(rr + 2, cc), c = S.cell.get(rr + 2, cc + 1), up = S.cell.get(rr + 2, cc + 2);
             const R th = theta_wd<R>(lo.dep, c.dep, up.dep, a.theta);
             g.ds = mc_gradient<R>(c.stg, lo.stg, up.stg, th);
             g.dd = mc_gradient<R>(c.dep, lo.dep, up.dep, th);
             g.du = mc_gradient<R>(c.u, lo.u, up.u, th);
             g.dv = mc_gradient<R>(c.v, lo.v, up.v, th);
         }
-        S.gew[rr][cc] = g;
+        S.gew.set(rr, cc, g);
     }
     __syncthreads();
 
@@ -277,7 +323,7 @@ __global__ void __launch_bounds__(NT) rk2_stage_kernel(const Rk2Args<R> a)
         e.f[0] = R(0); e.f[1] = R(0); e.f[2] = R(0); e.es_pos = 0.0; e.es_neg = 0.0;
         if (r >= 1 && r <= ny - 1 && i >= 1 && i <= nx - 1) {
             double cand;
-            edge_flux<R, true>(S.cell[rr + 1][cc + 2], S.gns[rr][cc], S.cell[rr + 2][cc + 2], S.gns[rr + 1][cc],
+            edge_flux<R, true>(S.cell.get(rr + 1, cc + 2), S.gns.get(rr, cc), S.cell.get(rr + 2, cc + 2), S.gns.get(rr + 1, cc),
                                a.m.dxb[r], inv2, e, cand);
             cfl = fmax(cfl, cand);
             if (MODE != MODE_CFL && a.lines) {
@@ -285,7 +331,7 @@ __global__ void __launch_bounds__(NT) rk2_stage_kernel(const Rk2Args<R> a)
                 if (r == a.n_ext && i >= a.n_ext && i <= nx - a.n_ext - 1) a.lines[nx + ny + i] = (double)e.f[0];
             }
         }
-        if (MODE != MODE_CFL) S.ens[rr][cc] = e;
+        if (MODE != MODE_CFL) S.ens.set(rr, cc, e);
     }
     for (int q = tid; q < TY * (TX + 1); q += NT) {
         const int rr = q / (TX + 1), cc = q - rr * (TX + 1);  // edge between (i-1, r) and (i, r)
@@ -295,7 +341,7 @@ __global__ void __launch_bounds__(NT) rk2_stage_kernel(const Rk2Args<R> a)
         if (r >= 1 && r <= ny - 1 && i >= 1 && i <= nx - 1) {
             const R inv1 = R(1) / (a.m.dxb[r] * a.half_cfl);  // dx_cfl_half_inv(1)
             double cand;
-            edge_flux<R, false>(S.cell[rr + 2][cc + 1], S.gew[rr][cc], S.cell[rr + 2][cc + 2], S.gew[rr][cc + 1],
+            edge_flux<R, false>(S.cell.get(rr + 2, cc + 1), S.gew.get(rr, cc), S.cell.get(rr + 2, cc + 2), S.gew.get(rr, cc + 1),
                                 a.m.dyl[i], inv1, e, cand);
             cfl = fmax(cfl, cand);
             if (MODE != MODE_CFL && a.lines) {
@@ -303,7 +349,7 @@ __global__ void __launch_bounds__(NT) rk2_stage_kernel(const Rk2Args<R> a)
                 if (i == a.n_ext && r >= a.n_ext && r <= ny - a.n_ext - 1) a.lines[2 * nx + ny + r] = (double)e.f[0];
             }
         }
-        if (MODE != MODE_CFL) S.eew[rr][cc] = e;
+        if (MODE != MODE_CFL) S.eew.set(rr, cc, e);
     }
 
     // Block max of the CFL candidates and the negative-depth count.
@@ -347,7 +393,7 @@ __global__ void __launch_bounds__(NT) rk2_stage_kernel(const Rk2Args<R> a)
     }
 
     const int64_t o = (int64_t)r * P + i;
-    const Cell<R> &c = S.cell[rr + 2][cc + 2];
+    const Cell<R> c = S.cell.get(rr + 2, cc + 2);
     // Mutated U (compute_depth_and_velocity zeroes UH/VH where depth <= minimum_allowed_depth)
     R U_stg = c.stg;
     R Um_uh, Um_vh;  // U(i,j,UH/VH) after the fix-ups, before the update
@@ -356,8 +402,8 @@ __global__ void __launch_bounds__(NT) rk2_stage_kernel(const Rk2Args<R> a)
     R U_uh = Um_uh, U_vh = Um_vh;
 
     const R inv_cell_area_dt = dt / a.m.area[r];
-    const EdgeRes<R> &n_lo = S.ens[rr][cc], &n_hi = S.ens[rr + 1][cc];
-    const EdgeRes<R> &w_lo = S.eew[rr][cc], &w_hi = S.eew[rr][cc + 1];
+    const EdgeRes<R> n_lo = S.ens.get(rr, cc), n_hi = S.ens.get(rr + 1, cc);
+    const EdgeRes<R> w_lo = S.eew.get(rr, cc), w_hi = S.eew.get(rr, cc + 1);
     U_stg = U_stg - inv_cell_area_dt * ((n_hi.f[0] - n_lo.f[0]) + (w_hi.f[0] - w_lo.f[0]));
     U_uh = U_uh - inv_cell_area_dt * ((n_hi.f[1] - n_lo.f[1]) + (w_hi.f[1] - w_lo.f[1]));
     U_vh = U_vh - inv_cell_area_dt * ((n_hi.f[2] - n_lo.f[2]) + (w_hi.f[2] - w_lo.f[2]));
@@ -670,6 +716,10 @@ cudaError_t launch_stage(const Rk2Args<R> &a, cudaStream_t s)
     if (!configured) {
         cudaError_t e = cudaFuncSetAttribute(rk2_stage_kernel<R, MODE, SPH, COR, FRIC>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        // Prefer shared memory over L1 so three CTAs fit per SM.
+        e = cudaFuncSetAttribute(rk2_stage_kernel<R, MODE, SPH, COR, FRIC>,
+                                 cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         if (e != cudaSuccess) return e;
         configured = true;
     }

@@ -71,6 +71,61 @@ __device__ __forceinline__ double pow_friction_cr(double x)
     return dd_fast_two_sum(v.hi, v.lo + v.hi * tl).hi;
 }
 
+// Correctly rounded cosh for the device boundary functions, in double-double
+// arithmetic: a = k ln2 + r with a double-double ln2 and |r| <= ln2/2,
+// exp(r) by the Horner form of its Taylor series to r^22/22!, exp(-|a|) by a
+// compensated reciprocal.  Only IEEE operations, fma, rint and ldexp are used,
+// so host and device evaluate it to the same bits.
+__host__ __device__ __forceinline__ DD dd_two_sum_hd(double a, double b)
+{
+    DD r; r.hi = a + b; const double bb = r.hi - a; r.lo = (a - (r.hi - bb)) + (b - bb); return r;
+}
+__host__ __device__ __forceinline__ DD dd_fts_hd(double a, double b) { DD r; r.hi = a + b; r.lo = b - (r.hi - a); return r; }
+__host__ __device__ __forceinline__ DD dd_tp_hd(double a, double b) { DD r; r.hi = a * b; r.lo = fma(a, b, -r.hi); return r; }
+__host__ __device__ __forceinline__ DD dd_mul_hd(DD a, DD b)
+{
+    DD p = dd_tp_hd(a.hi, b.hi);
+    p.lo += a.hi * b.lo + a.lo * b.hi;
+    return dd_fts_hd(p.hi, p.lo);
+}
+__host__ __device__ __forceinline__ DD dd_div_d_hd(DD x, double n)
+{
+    const double q1 = x.hi / n;
+    const DD p = dd_tp_hd(q1, n);
+    const double e = (((x.hi - p.hi) - p.lo) + x.lo) / n;
+    return dd_fts_hd(q1, e);
+}
+__host__ __device__ __forceinline__ double cosh_cr(double a)
+{
+    const double x = fabs(a);
+    if (x > 700.0) return x * 1.0e308;  // overflow to +inf, as cosh does
+    const double ln2_hi = 6.93147180559945286227e-01, ln2_lo = 2.31904681384629955842e-17;
+    const double k = rint(x * 1.44269504088896338700e+00);
+    const DD p = dd_tp_hd(k, ln2_hi);
+    DD t = dd_two_sum_hd(x, -p.hi);
+    t.lo = (t.lo - p.lo) - k * ln2_lo;
+    const DD r = dd_fts_hd(t.hi, t.lo);
+    DD s; s.hi = 1.0; s.lo = 0.0;
+    for (int n = 22; n >= 1; n--) {
+        DD q = dd_div_d_hd(dd_mul_hd(r, s), (double)n);
+        DD u = dd_two_sum_hd(1.0, q.hi);
+        u.lo += q.lo;
+        s = dd_fts_hd(u.hi, u.lo);
+    }
+    const int ki = (int)k;
+    DD E; E.hi = ldexp(s.hi, ki); E.lo = ldexp(s.lo, ki);
+    // 1/E
+    const double y0 = 1.0 / E.hi;
+    DD w = dd_tp_hd(E.hi, y0);
+    w.lo += E.lo * y0;
+    const double e = (1.0 - w.hi) - w.lo;
+    const DD inv = dd_fts_hd(y0, y0 * e);
+    DD sum = dd_two_sum_hd(E.hi, inv.hi);
+    sum.lo += E.lo + inv.lo;
+    sum = dd_fts_hd(sum.hi, sum.lo);
+    return 0.5 * sum.hi + 0.5 * sum.lo;
+}
+
 // Metric arrays, 0-based copies of the Fortran arrays.
 template <typename R> struct Metrics {
     const R *dxb;     // ny+1: distance_bottom_edge
@@ -124,7 +179,7 @@ __device__ __forceinline__ void boundary_function(const BoundaryFn &bf, const R 
             R k = R(sqrt(R(3.0) * H / (R(4.0) * dep * dep * dep)));
             R c = R(sqrt(K<R>::gravity() * (dep + H)));
             R arg = k * (x[0] - x0 - c * R(t));
-            R ch = R(cosh(arg));
+            R ch = R(cosh_cr((double)arg));
             stg = H / (ch * ch);
             elv = -dep;
         } else {

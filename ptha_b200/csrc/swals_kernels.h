@@ -8,6 +8,9 @@
 
 namespace swals {
 
+// Sets the message returned by swals_gpu_last_error (this thread).
+void set_last_error(const char *msg);
+
 // Kernel categories for the per-launch timers (include/swals_gpu.h).
 enum LaunchCat {
     CAT_CFL = 0, CAT_STAGE1 = 1, CAT_BC1 = 2, CAT_STAGE2 = 3, CAT_BC2 = 4, CAT_FINALIZE = 5,

@@ -25,3 +25,19 @@ def test_pow_friction_is_correctly_rounded(chezy):
         x = 1e-5 * 10 ** (9 * u) if k % 2 else 1e-5 + 80 * u
         want = float(mpmath.power(mpmath.mpf(x), p))
         assert f(x, chezy) == want, (x, f(x, chezy), want)
+
+
+def test_boundary_cosh_is_correctly_rounded():
+    """cosh of the device boundary functions (solitary wave sech^2) is the
+    correctly rounded value, so oracle and GPU give identical boundary stages."""
+    lib = orc._load(False)
+    f = lib.oracle64_cosh_cr
+    f.restype = ctypes.c_double
+    f.argtypes = [ctypes.c_double]
+    mpmath.mp.prec = 300
+    rng = random.Random(77)
+    for k in range(20000):
+        a = rng.uniform(-120.0, 120.0) if k % 2 else rng.uniform(-3.0, 3.0)
+        want = float(mpmath.cosh(mpmath.mpf(a)))
+        assert f(a) == want, (a, f(a), want)
+    assert f(0.0) == 1.0
