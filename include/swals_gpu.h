@@ -180,6 +180,26 @@ int swals_gpu_stream(swals_domain *d, void **stream_out);
 int swals_gpu_device_planes(swals_domain *d, void **stg, void **uh, void **vh, void **elv,
                             int64_t *pitch_elems);
 
+/* Allocation-free volume_interior.  This entry point has no counterpart in
+ * the reference.  It serves callers that cannot call cudaMalloc: code that
+ * runs while a CUDA graph is being captured, hosts whose device memory
+ * belongs to another allocator, loops that cannot take cudaMalloc's implicit
+ * device synchronisation.  The caller passes device pointers to its own STG
+ * and ELV planes (ny rows of pitch_elems elements, real_bytes 8 or 4), to
+ * area_cell_y (ny values, same type) and to one output double; the sum is
+ * written there, stream-ordered on `stream` (a cudaStream_t, NULL = legacy
+ * default stream), without synchronising.  Per-row scratch lives in a fixed
+ * device array of SWALS_NOALLOC_MAX_ROWS doubles that every GPU loading the
+ * library holds until exit; larger ny is rejected with SWALS_ERR_CAPACITY.
+ * The first call on each device looks up the array's device address (with
+ * that device current), so make that first call before any stream capture.
+ * All calls on a device share the scratch: calls that overlap on the GPU
+ * race.  Nothing is allocated or freed. */
+#define SWALS_NOALLOC_MAX_ROWS 65536
+int swals_gpu_volume_interior_noalloc(const void *stg, const void *elv, const void *area, int32_t nx, int32_t ny,
+                                      int64_t pitch_elems, int32_t real_bytes, int32_t exterior_cells_width,
+                                      double *out_device, void *stream);
+
 /* Last error message of this thread (util/stop_mod.f90 prints before stopping). */
 int swals_gpu_last_error(char *buf, size_t len);
 /* Library version string. */

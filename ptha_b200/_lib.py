@@ -33,7 +33,7 @@ EXPORTED = [
     "swals_gpu_volume_interior", "swals_gpu_gauges_setup", "swals_gpu_gauges_site_index",
     "swals_gpu_gauges_read", "swals_gpu_gauges_reset", "swals_gpu_timers_enable", "swals_gpu_timers_read",
     "swals_gpu_stream", "swals_gpu_device_planes", "swals_gpu_last_error", "swals_gpu_version",
-    "swals_gpu_launch_count",
+    "swals_gpu_launch_count", "swals_gpu_volume_interior_noalloc",
 ]
 TIMER_NAMES = ["cfl", "fv_stage1", "boundary1", "fv_stage2", "boundary2", "finalize", "leapfrog_edge",
                "leapfrog_step", "gauges", "max_stage"]
@@ -113,6 +113,7 @@ def lib():
                                     ctypes.POINTER(vp), ctypes.POINTER(i64)],
         "swals_gpu_last_error": [ctypes.c_char_p, ctypes.c_size_t],
         "swals_gpu_launch_count": [vp, ctypes.POINTER(i64)],
+        "swals_gpu_volume_interior_noalloc": [vp, vp, vp, i32, i32, i64, i32, i32, vp, vp],
     }
     for name, args in sig.items():
         f = getattr(L, name)
