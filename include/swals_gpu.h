@@ -200,6 +200,59 @@ int swals_gpu_volume_interior_noalloc(const void *stg, const void *elv, const vo
                                       int64_t pitch_elems, int32_t real_bytes, int32_t exterior_cells_width,
                                       double *out_device, void *stream);
 
+/* ---- batched linear leapfrog --------------------------------------------
+ * B independent initial conditions on one grid.  The reference has no
+ * batched form; a batch is B independent sequences of
+ * domain%evolve_one_step(dt) with timestepping_method='linear'
+ * (domain_mod_linear_solver_include.f90:58-571) that share geometry, ELV
+ * and options of `grid` (a 'linear' domain without a boundary routine, which
+ * must outlive the batch).  Each step is one kernel launch over all
+ * instances; evolve() replays steps from a CUDA graph. */
+typedef struct swals_batch swals_batch;  /* opaque */
+int swals_gpu_batch_create(swals_domain *grid, int32_t nbatch, int32_t record_max_stage, swals_batch **out);
+int swals_gpu_batch_destroy(swals_batch *b);
+/* count instances from `first`, each (nx,ny,3) column-major [STG,UH,VH]. */
+int swals_gpu_batch_upload_U(swals_batch *b, int32_t first, int32_t count, const void *U3);
+int swals_gpu_batch_download_U(swals_batch *b, int32_t first, int32_t count, void *U3);
+int swals_gpu_batch_download_max_stage(swals_batch *b, int32_t first, int32_t count, void *host);
+/* Device layout for callers that fill or read instances in place:
+ * instance b, variable v (0 STG, 1 UH, 2 VH), row j, column i is element
+ * b*instance_stride + v*plane + j*pitch + i of *stg0 (current buffer). */
+int swals_gpu_batch_device_state(swals_batch *b, void **stg0, int64_t *pitch_elems, int64_t *plane_elems,
+                                 int64_t *instance_stride_elems);
+/* Stage at gauge sites of every instance after every step; read returns
+ * records * nbatch * n values ordered [record][instance][gauge]. */
+int swals_gpu_batch_gauges_setup(swals_batch *b, const double *xy, int32_t n, int32_t capacity);
+int swals_gpu_batch_gauges_read(swals_batch *b, double *out, int32_t max_records, int32_t *n_records);
+int swals_gpu_batch_evolve(swals_batch *b, int32_t nsteps, double dt);
+int swals_gpu_batch_time(swals_batch *b, double *time, int64_t *nsteps);
+/* Autotuner: times every tile shape on this batch with state-preserving
+ * dt = 0 steps and keeps the fastest. */
+int swals_gpu_batch_tune(swals_batch *b, int32_t *cfg_out, double *ms_per_step_out);
+int swals_gpu_batch_set_tile_config(swals_batch *b, int32_t cfg);
+
+/* ---- discrete adjoint of the truly linear leapfrog -------------------------
+ * The reference has no adjoint.  For a 'linear' domain with
+ * linear_solver_is_truely_linear and no boundary routine, one step is a
+ * linear map x' = M x on x = (STG, UH, VH) with fixed dt.  With gauges set
+ * up (swals_gpu_gauges_setup), y_n = stage at the gauges after step n.
+ *
+ * adjoint_linear: given gauge_adjoint[n][g] = dL/dy_{n+1,g} for n < nsteps
+ * (nsteps x n_gauges, host, may be NULL) and an optional lambda_seed
+ * (dL/dx_nsteps as (nx,ny,3) column-major host array, may be NULL), writes
+ * dL/dx_0 into grad_U0 ((nx,ny,3) column-major host array).  The domain's
+ * state is not used or changed.
+ *
+ * misfit_gradient_linear: L = 1/2 sum_n sum_g (y_{n,g} - target[n][g])^2
+ * for n = 1..nsteps starting from the domain's current state (unchanged on
+ * return); forward keeping a checkpoint every `checkpoint_every` steps, then
+ * per segment recomputation and the adjoint sweep.  Writes L and
+ * dL/d(STG,UH,VH)_0. */
+int swals_gpu_adjoint_linear(swals_domain *d, int32_t nsteps, double timestep, const double *gauge_adjoint,
+                             const void *lambda_seed, void *grad_U0);
+int swals_gpu_misfit_gradient_linear(swals_domain *d, int32_t nsteps, double timestep, const double *target,
+                                     int32_t checkpoint_every, double *loss, void *grad_U0);
+
 /* Last error message of this thread (util/stop_mod.f90 prints before stopping). */
 int swals_gpu_last_error(char *buf, size_t len);
 /* Library version string. */

@@ -33,7 +33,11 @@ EXPORTED = [
     "swals_gpu_volume_interior", "swals_gpu_gauges_setup", "swals_gpu_gauges_site_index",
     "swals_gpu_gauges_read", "swals_gpu_gauges_reset", "swals_gpu_timers_enable", "swals_gpu_timers_read",
     "swals_gpu_stream", "swals_gpu_device_planes", "swals_gpu_last_error", "swals_gpu_version",
-    "swals_gpu_launch_count", "swals_gpu_volume_interior_noalloc",
+    "swals_gpu_launch_count",
+    "swals_gpu_batch_create", "swals_gpu_batch_destroy", "swals_gpu_batch_upload_U", "swals_gpu_batch_download_U",
+    "swals_gpu_batch_download_max_stage", "swals_gpu_batch_device_state", "swals_gpu_batch_gauges_setup",
+    "swals_gpu_batch_gauges_read", "swals_gpu_batch_evolve", "swals_gpu_batch_time", "swals_gpu_batch_tune",
+    "swals_gpu_batch_set_tile_config", "swals_gpu_adjoint_linear", "swals_gpu_misfit_gradient_linear", "swals_gpu_volume_interior_noalloc",
 ]
 TIMER_NAMES = ["cfl", "fv_stage1", "boundary1", "fv_stage2", "boundary2", "finalize", "leapfrog_edge",
                "leapfrog_step", "gauges", "max_stage"]
@@ -113,6 +117,21 @@ def lib():
                                     ctypes.POINTER(vp), ctypes.POINTER(i64)],
         "swals_gpu_last_error": [ctypes.c_char_p, ctypes.c_size_t],
         "swals_gpu_launch_count": [vp, ctypes.POINTER(i64)],
+        "swals_gpu_batch_create": [vp, i32, i32, ctypes.POINTER(vp)],
+        "swals_gpu_batch_destroy": [vp],
+        "swals_gpu_batch_upload_U": [vp, i32, i32, vp],
+        "swals_gpu_batch_download_U": [vp, i32, i32, vp],
+        "swals_gpu_batch_download_max_stage": [vp, i32, i32, vp],
+        "swals_gpu_batch_device_state": [vp, ctypes.POINTER(vp), ctypes.POINTER(i64), ctypes.POINTER(i64),
+                                         ctypes.POINTER(i64)],
+        "swals_gpu_batch_gauges_setup": [vp, vp, i32, i32],
+        "swals_gpu_batch_gauges_read": [vp, vp, i32, ctypes.POINTER(i32)],
+        "swals_gpu_batch_evolve": [vp, i32, dbl],
+        "swals_gpu_batch_time": [vp, ctypes.POINTER(dbl), ctypes.POINTER(i64)],
+        "swals_gpu_batch_tune": [vp, ctypes.POINTER(i32), ctypes.POINTER(dbl)],
+        "swals_gpu_batch_set_tile_config": [vp, i32],
+        "swals_gpu_adjoint_linear": [vp, i32, dbl, vp, vp, vp],
+        "swals_gpu_misfit_gradient_linear": [vp, i32, dbl, vp, i32, ctypes.POINTER(dbl), vp],
         "swals_gpu_volume_interior_noalloc": [vp, vp, vp, i32, i32, i64, i32, i32, vp, vp],
     }
     for name, args in sig.items():

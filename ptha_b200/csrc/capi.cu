@@ -6,8 +6,7 @@
 // state arrays U / max_U(:,:,1) / manning_squared, and the scalar state
 // (time, max_dt, nsteps_advanced, boundary-flux integrals).  The state lives
 // on the device; the host only keeps descriptors and the 1-D metrics.
-#include "swals_kernels.h"
-#include "../../include/swals_gpu.h"
+#include "domain_internal.h"
 
 #include <cfloat>
 #include <cmath>
@@ -80,45 +79,9 @@ bool is_staggered(int m) { return m == M_LINEAR || m == M_LF_LIN_NLFRIC || m == 
 }  // namespace
 
 void swals::set_last_error(const char *msg) { g_last_error = msg; }
+int swals::api_fail(int code, const char *msg) { g_last_error = msg; return code; }
+int swals::api_cuda_fail(cudaError_t e, const char *what) { return cuda_fail(e, what); }
 
-struct swals_domain {
-    swals_domain_desc desc;
-    int method = 0;
-    bool fp64 = true;
-    int nx = 0, ny = 0;
-    int64_t pitch = 0;
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    void *pool = nullptr;
-    size_t pool_bytes = 0;
-    void *planes[3][3] = {};
-    void *elv = nullptr, *max_stage = nullptr, *manning_sq = nullptr;
-    void *metric[8] = {};  // dxb, dyl, area, cor, cor_be, tanlat, x, y
-    std::vector<double> h_metric[8];
-    swals::DevScalars *sc = nullptr;
-    void *side = nullptr;
-    double *lines = nullptr;
-    double *scratch = nullptr;  // row sums / block minima
-    int64_t scratch_len = 0;
-    double *d_out = nullptr;    // small result slot
-    int cur = 0;
-    int64_t nsteps = 0;
-    swals::StepConfig cfg{};
-    // gauges
-    int n_gauges = 0, gauge_capacity = 0;
-    int *d_sites = nullptr;
-    double *d_records = nullptr;
-    std::vector<int> h_sites;
-    // launch accounting and per-kernel event timers
-    int64_t launches = 0;
-    bool timers_on = false;
-    std::vector<cudaEvent_t> ev_pool;
-    struct Pending { int cat; cudaEvent_t a, b; };
-    std::vector<Pending> pending;
-    cudaEvent_t open_ev[swals::CAT_COUNT] = {};
-    double tot_ms[swals::CAT_COUNT] = {};
-    int64_t counts[swals::CAT_COUNT] = {};
-};
 
 namespace {
 
@@ -189,20 +152,6 @@ int upload_metrics_t(swals_domain *d)
     return SWALS_OK;
 }
 
-template <typename R>
-swals::Metrics<R> metrics_of(swals_domain *d)
-{
-    swals::Metrics<R> m;
-    m.dxb = (const R *)d->metric[0];
-    m.dyl = (const R *)d->metric[1];
-    m.area = (const R *)d->metric[2];
-    m.cor = (const R *)d->metric[3];
-    m.cor_be = (const R *)d->metric[4];
-    m.tanlat = (const R *)d->metric[5];
-    m.x = (const R *)d->metric[6];
-    m.y = (const R *)d->metric[7];
-    return m;
-}
 
 template <typename R>
 __global__ void fill_kernel(R *p, int64_t n, R v)
@@ -254,7 +203,9 @@ void on_launch(void *ctx, int cat, int phase)
     else d->pending.push_back({cat, d->open_ev[cat], e});
 }
 
-swals::LaunchHook hook_of(swals_domain *d)
+}  // namespace
+
+swals::LaunchHook swals::hook_of(swals_domain *d)
 {
     swals::LaunchHook h;
     h.fn = on_launch;
@@ -262,13 +213,15 @@ swals::LaunchHook hook_of(swals_domain *d)
     return h;
 }
 
+namespace {
+
 template <typename R>
 int evolve_t(swals_domain *d, double timestep, int has_dt)
 {
     using namespace swals;
     const StepConfig &c = d->cfg;
-    const LaunchHook hook = hook_of(d);
-    Metrics<R> m = metrics_of<R>(d);
+    const LaunchHook hook = swals::hook_of(d);
+    Metrics<R> m = swals::metrics_of<R>(d);
     R *max_stage = d->desc.record_max_stage ? (R *)d->max_stage : nullptr;
     if (d->nsteps == 0 && max_stage) {
         hook(CAT_MAXSTAGE, 0);

@@ -1,0 +1,69 @@
+// domain_internal.h -- the device domain behind the C ABI, shared by the
+// entry-point files (capi.cu, batch.cu, adjoint.cu).  Internal to the library.
+#pragma once
+#include <vector>
+
+#include "swals_kernels.h"
+#include "../../include/swals_gpu.h"
+
+// Mirrors the parts of SWALS's domain_type (domain_mod.f90:137-507) the time
+// step touches: geometry, solver options, device planes and scalar state.
+struct swals_domain {
+    swals_domain_desc desc;
+    int method = 0;
+    bool fp64 = true;
+    int nx = 0, ny = 0;
+    int64_t pitch = 0;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    void *pool = nullptr;
+    size_t pool_bytes = 0;
+    void *planes[3][3] = {};
+    void *elv = nullptr, *max_stage = nullptr, *manning_sq = nullptr;
+    void *metric[8] = {};  // dxb, dyl, area, cor, cor_be, tanlat, x, y
+    std::vector<double> h_metric[8];
+    swals::DevScalars *sc = nullptr;
+    void *side = nullptr;
+    double *lines = nullptr;
+    double *scratch = nullptr;  // row sums / block minima
+    int64_t scratch_len = 0;
+    double *d_out = nullptr;    // small result slot
+    int cur = 0;
+    int64_t nsteps = 0;
+    swals::StepConfig cfg{};
+    // gauges
+    int n_gauges = 0, gauge_capacity = 0;
+    int *d_sites = nullptr;
+    double *d_records = nullptr;
+    std::vector<int> h_sites;
+    // launch accounting and per-kernel event timers
+    int64_t launches = 0;
+    bool timers_on = false;
+    std::vector<cudaEvent_t> ev_pool;
+    struct Pending { int cat; cudaEvent_t a, b; };
+    std::vector<Pending> pending;
+    cudaEvent_t open_ev[swals::CAT_COUNT] = {};
+    double tot_ms[swals::CAT_COUNT] = {};
+    int64_t counts[swals::CAT_COUNT] = {};
+};
+
+namespace swals {
+int api_fail(int code, const char *msg);
+int api_cuda_fail(cudaError_t e, const char *what);
+LaunchHook hook_of(swals_domain *d);
+
+template <typename R>
+inline Metrics<R> metrics_of(const swals_domain *d)
+{
+    Metrics<R> m;
+    m.dxb = (const R *)d->metric[0];
+    m.dyl = (const R *)d->metric[1];
+    m.area = (const R *)d->metric[2];
+    m.cor = (const R *)d->metric[3];
+    m.cor_be = (const R *)d->metric[4];
+    m.tanlat = (const R *)d->metric[5];
+    m.x = (const R *)d->metric[6];
+    m.y = (const R *)d->metric[7];
+    return m;
+}
+}  // namespace swals

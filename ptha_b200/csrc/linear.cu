@@ -25,14 +25,12 @@ namespace swals {
 namespace {
 
 constexpr int LBX = 32;   // tile columns (one warp wide)
-constexpr int LBY = 16;   // tile rows
-constexpr int LTY = 8;    // thread rows; each thread handles LBY/LTY cells
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
 template <typename R>
 struct LinArgs {
-    StepPlanes<R> p;
+    StepPlanes<R> p;        // planes of instance 0
     Metrics<R> m;
     int xl, xu, yl, yu;
     int bc_stage;
@@ -41,6 +39,9 @@ struct LinArgs {
     R msl;
     int lin_fric;
     R lin_fric_mult;
+    int nbatch;             // instances sharing ELV and the metrics (1 for a plain domain)
+    int64_t inst_stride;    // elements between consecutive instances' planes
+    int64_t max_stride;     // elements between consecutive instances' max_stage planes
 };
 
 __device__ __forceinline__ bool on_bc_ring(int i, int r, int nx, int ny, const int bext[4])
@@ -48,124 +49,154 @@ __device__ __forceinline__ bool on_bc_ring(int i, int r, int nx, int ny, const i
     return (i == 0 && bext[3]) || (i == nx - 1 && bext[1]) || (r == 0 && bext[2]) || (r == ny - 1 && bext[0]);
 }
 
-template <typename R, bool CORIOLIS, bool TRUELY_LINEAR>
-__global__ void __launch_bounds__(LBX *LTY) linear_step_kernel(const LinArgs<R> a)
+// One CTA: a 32 x BY tile (TYT thread rows, BY/TYT cells per thread) for IB
+// instances in turn.  ELV (and, for the truly linear solver, the face depths
+// that depend only on ELV) are staged once and reused by every instance.
+template <typename R, bool CORIOLIS, bool TRUELY_LINEAR, int BY, int TYT, int IB>
+__global__ void __launch_bounds__(LBX *TYT) linear_step_kernel(const LinArgs<R> a)
 {
-    __shared__ R s_uh[LBY + 1][LBX + 2];  // old UH: rows r0..r0+LBY, cols i0-1..i0+LBX (clamped)
-    __shared__ R s_vh[LBY + 2][LBX + 1];  // old VH: rows r0-1..r0+LBY, cols i0..i0+LBX (clamped)
-    __shared__ R s_sn[LBY + 1][LBX + 1];  // new STG: rows r0..r0+LBY, cols i0..i0+LBX
-    __shared__ R s_el[LBY + 1][LBX + 1];  // ELV on the same window as s_sn
+    constexpr int CPT = BY / TYT;
+    constexpr int NT = LBX * TYT;
+    __shared__ R s_uh[BY + 1][LBX + 2];  // old UH: rows r0..r0+BY, cols i0-1..i0+LBX (clamped)
+    __shared__ R s_vh[BY + 2][LBX + 1];  // old VH: rows r0-1..r0+BY, cols i0..i0+LBX (clamped)
+    __shared__ R s_sn[BY + 1][LBX + 1];  // new STG: rows r0..r0+BY, cols i0..i0+LBX
+    __shared__ R s_el[BY + 1][LBX + 1];  // ELV on the same window as s_sn
 
     const int nx = a.p.nx, ny = a.p.ny;
     const int64_t P = a.p.pitch;
-    const int i0 = blockIdx.x * LBX, r0 = blockIdx.y * LBY;
+    const int i0 = blockIdx.x * LBX, r0 = blockIdx.y * BY;
     const int tid = threadIdx.y * LBX + threadIdx.x;
-    constexpr int NT = LBX * LTY;
+    const R g = K<R>::gravity();
+    const R half = K<R>::half();
+    const R one = K<R>::one();
+    const R zero = K<R>::zero();
+    const R mad = K<R>::min_depth();
 
-    for (int q = tid; q < (LBY + 1) * (LBX + 2); q += NT) {
-        int rr = q / (LBX + 2), cc = q - rr * (LBX + 2);
-        int r = clampi(r0 + rr, 0, ny - 1), i = clampi(i0 - 1 + cc, 0, nx - 1);
-        s_uh[rr][cc] = a.p.uh[r * P + i];
-    }
-    for (int q = tid; q < (LBY + 2) * (LBX + 1); q += NT) {
-        int rr = q / (LBX + 1), cc = q - rr * (LBX + 1);
-        int r = clampi(r0 - 1 + rr, 0, ny - 1), i = clampi(i0 + cc, 0, nx - 1);
-        s_vh[rr][cc] = a.p.vh[r * P + i];
-    }
-    for (int q = tid; q < (LBY + 1) * (LBX + 1); q += NT) {
+    for (int q = tid; q < (BY + 1) * (LBX + 1); q += NT) {
         int rr = q / (LBX + 1), cc = q - rr * (LBX + 1);
         int r = clampi(r0 + rr, 0, ny - 1), i = clampi(i0 + cc, 0, nx - 1);
         s_el[rr][cc] = a.p.elv[r * P + i];
     }
     __syncthreads();
 
-    // New stage on the tile plus east/north halo (:92-115).
-    for (int q = tid; q < (LBY + 1) * (LBX + 1); q += NT) {
-        int rr = q / (LBX + 1), cc = q - rr * (LBX + 1);
-        int r = r0 + rr, i = i0 + cc;
-        R sn = R(0);
-        if (r < ny && i < nx) {
-            R s_old = a.p.stg[r * P + i];
-            bool interior = (i >= a.xl + 1) && (i <= a.xu - 1) && (r >= a.yl + 1) && (r <= a.yu - 1);
-            if (interior) {
-                R inv_cell_area_dt = a.dt / a.m.area[r];
-                R t1 = (s_uh[rr][cc + 1] - s_uh[rr][cc]) * a.m.dyl[i];
-                R t2 = s_vh[rr + 1][cc] * a.m.dxb[r + 1] - s_vh[rr][cc] * a.m.dxb[r];
-                sn = s_old - inv_cell_area_dt * (t1 + t2);
-            } else if (a.bc_stage && on_bc_ring(i, r, nx, ny, a.bext)) {
-                sn = a.p.stg_o[r * P + i];  // set by the edge kernel at time+dt/2
-            } else {
-                sn = s_old;
-            }
-        }
-        s_sn[rr][cc] = sn;
-    }
-    __syncthreads();
-
-    const R g = K<R>::gravity();
-    const R half = K<R>::half();
-    const R one = K<R>::one();
-    const R zero = K<R>::zero();
-    const R mad = K<R>::min_depth();
+    // Truly linear face depths h_{i+1/2}, h_{j+1/2} depend on ELV only (:353-370).
+    R h_iph_c[CPT], h_jph_c[CPT];
 #pragma unroll
-    for (int k = 0; k < LBY / LTY; k++) {
-        const int rr = threadIdx.y + k * LTY, cc = threadIdx.x;
-        const int r = r0 + rr, i = i0 + cc;
-        if (r >= ny || i >= nx) continue;
-        const int64_t o = r * P + i;
-        const R sn = s_sn[rr][cc];
-        a.p.stg_o[o] = sn;
-        if (a.p.max_stage && i >= a.xl && i <= a.xu && r >= a.yl && r <= a.yu) {
-            R mx = a.p.max_stage[o];
-            a.p.max_stage[o] = (sn > mx) ? sn : mx;
-        }
-        R uh = s_uh[rr][cc + 1];
-        R vh = s_vh[rr + 1][cc];
-        if (i >= a.xl && i <= a.xu - 1 && r >= a.yl && r <= a.yu - 1) {
-            const R inv_cell_area_dt_g = g * a.dt / a.m.area[r];
-            const R inv_cell_area_dt_vh_g = g * a.dt / (half * (a.m.area[r] + a.m.area[r + 1]));
+    for (int k = 0; k < CPT; k++) {
+        const int rr = threadIdx.y + k * TYT, cc = threadIdx.x;
+        h_iph_c[k] = zero;
+        h_jph_c[k] = zero;
+        if (TRUELY_LINEAR) {
             const R e0 = s_el[rr][cc], e_e = s_el[rr][cc + 1], e_n = s_el[rr + 1][cc];
-            const R s_e = s_sn[rr][cc + 1], s_n = s_sn[rr + 1][cc];
-            R h_iph, h_jph, wet_iph, wet_jph;
-            if (TRUELY_LINEAR) {
-                bool wi = (e0 < -mad + a.msl) && (e_e < -mad + a.msl);
-                h_iph = wi ? (a.msl - half * (e_e + e0)) : zero;
-                bool wj = (e_n < -mad + a.msl) && (e0 < -mad + a.msl);
-                h_jph = wj ? (a.msl - half * (e_n + e0)) : zero;
-                wet_iph = one;
-                wet_jph = one;
-            } else {
-                bool wi = (sn - e0 > mad) && (s_e - e_e > mad);
-                h_iph = wi ? (half * ((s_e + sn) - (e_e + e0))) : zero;
-                bool wj = (s_n - e_n > mad) && (sn - e0 > mad);
-                h_jph = wj ? (half * ((s_n + sn) - (e_n + e0))) : zero;
-                wet_iph = (h_iph > zero) ? one : zero;
-                wet_jph = (h_jph > zero) ? one : zero;
-            }
-            const R dw_j = s_n - sn;
-            R uh_n = uh * wet_iph - inv_cell_area_dt_g * h_iph * (s_e - sn) * a.m.dyl[i + 1];
-            R vh_n = vh * wet_jph - inv_cell_area_dt_vh_g * h_jph * dw_j * a.m.dxb[r + 1];
-            if (CORIOLIS) {
-                // Pre-update 2-point averages (:409-428); rows/cols clamp like
-                // the reference's j=1 and max(xL-1,1) special cases.
-                const R vh_iph_jmh = half * (s_vh[rr][cc] + s_vh[rr][cc + 1]);
-                const R vh_iph_jph = half * (s_vh[rr + 1][cc] + s_vh[rr + 1][cc + 1]);
-                const R uh_i_j = half * (s_uh[rr][cc + 1] + s_uh[rr][cc]);
-                const R uh_i_jp1 = half * (s_uh[rr + 1][cc + 1] + s_uh[rr + 1][cc]);
-                const R dt_half_coriolis = a.dt * a.m.cor[r] * half * ((h_iph > zero) ? one : zero);
-                const R dt_half_coriolis_jph = a.dt * a.m.cor_be[r + 1] * half * ((h_jph > zero) ? one : zero);
-                uh_n = uh_n + dt_half_coriolis * (vh_iph_jmh + vh_iph_jph);
-                vh_n = vh_n - dt_half_coriolis_jph * (uh_i_j + uh_i_jp1);
-            }
-            if (a.lin_fric) {
-                uh_n = a.lin_fric_mult * uh_n;
-                vh_n = a.lin_fric_mult * vh_n;
-            }
-            uh = uh_n;
-            vh = vh_n;
+            bool wi = (e0 < -mad + a.msl) && (e_e < -mad + a.msl);
+            h_iph_c[k] = wi ? (a.msl - half * (e_e + e0)) : zero;
+            bool wj = (e_n < -mad + a.msl) && (e0 < -mad + a.msl);
+            h_jph_c[k] = wj ? (a.msl - half * (e_n + e0)) : zero;
         }
-        a.p.uh_o[o] = uh;
-        a.p.vh_o[o] = vh;
+    }
+
+    for (int ib = 0; ib < IB; ib++) {
+        const int b = blockIdx.z * IB + ib;
+        if (b >= a.nbatch) break;  // uniform across the CTA
+        const int64_t io = (int64_t)b * a.inst_stride;
+        const R *stg = a.p.stg + io, *uhp = a.p.uh + io, *vhp = a.p.vh + io;
+        R *stg_o = a.p.stg_o + io, *uh_o = a.p.uh_o + io, *vh_o = a.p.vh_o + io;
+        R *max_stage = a.p.max_stage ? a.p.max_stage + (int64_t)b * a.max_stride : nullptr;
+        if (ib > 0) __syncthreads();  // the previous instance is done with the tiles
+
+        for (int q = tid; q < (BY + 1) * (LBX + 2); q += NT) {
+            int rr = q / (LBX + 2), cc = q - rr * (LBX + 2);
+            int r = clampi(r0 + rr, 0, ny - 1), i = clampi(i0 - 1 + cc, 0, nx - 1);
+            s_uh[rr][cc] = uhp[r * P + i];
+        }
+        for (int q = tid; q < (BY + 2) * (LBX + 1); q += NT) {
+            int rr = q / (LBX + 1), cc = q - rr * (LBX + 1);
+            int r = clampi(r0 - 1 + rr, 0, ny - 1), i = clampi(i0 + cc, 0, nx - 1);
+            s_vh[rr][cc] = vhp[r * P + i];
+        }
+        __syncthreads();
+
+        // New stage on the tile plus east/north halo (:92-115).
+        for (int q = tid; q < (BY + 1) * (LBX + 1); q += NT) {
+            int rr = q / (LBX + 1), cc = q - rr * (LBX + 1);
+            int r = r0 + rr, i = i0 + cc;
+            R sn = R(0);
+            if (r < ny && i < nx) {
+                R s_old = stg[r * P + i];
+                bool interior = (i >= a.xl + 1) && (i <= a.xu - 1) && (r >= a.yl + 1) && (r <= a.yu - 1);
+                if (interior) {
+                    R inv_cell_area_dt = a.dt / a.m.area[r];
+                    R t1 = (s_uh[rr][cc + 1] - s_uh[rr][cc]) * a.m.dyl[i];
+                    R t2 = s_vh[rr + 1][cc] * a.m.dxb[r + 1] - s_vh[rr][cc] * a.m.dxb[r];
+                    sn = s_old - inv_cell_area_dt * (t1 + t2);
+                } else if (a.bc_stage && on_bc_ring(i, r, nx, ny, a.bext)) {
+                    sn = stg_o[r * P + i];  // set by the edge kernel at time+dt/2
+                } else {
+                    sn = s_old;
+                }
+            }
+            s_sn[rr][cc] = sn;
+        }
+        __syncthreads();
+
+#pragma unroll
+        for (int k = 0; k < CPT; k++) {
+            const int rr = threadIdx.y + k * TYT, cc = threadIdx.x;
+            const int r = r0 + rr, i = i0 + cc;
+            if (r >= ny || i >= nx) continue;
+            const int64_t o = r * P + i;
+            const R sn = s_sn[rr][cc];
+            stg_o[o] = sn;
+            if (max_stage && i >= a.xl && i <= a.xu && r >= a.yl && r <= a.yu) {
+                R mx = max_stage[o];
+                max_stage[o] = (sn > mx) ? sn : mx;
+            }
+            R uh = s_uh[rr][cc + 1];
+            R vh = s_vh[rr + 1][cc];
+            if (i >= a.xl && i <= a.xu - 1 && r >= a.yl && r <= a.yu - 1) {
+                const R inv_cell_area_dt_g = g * a.dt / a.m.area[r];
+                const R inv_cell_area_dt_vh_g = g * a.dt / (half * (a.m.area[r] + a.m.area[r + 1]));
+                const R e0 = s_el[rr][cc], e_e = s_el[rr][cc + 1], e_n = s_el[rr + 1][cc];
+                const R s_e = s_sn[rr][cc + 1], s_n = s_sn[rr + 1][cc];
+                R h_iph, h_jph, wet_iph, wet_jph;
+                if (TRUELY_LINEAR) {
+                    h_iph = h_iph_c[k];
+                    h_jph = h_jph_c[k];
+                    wet_iph = one;
+                    wet_jph = one;
+                } else {
+                    bool wi = (sn - e0 > mad) && (s_e - e_e > mad);
+                    h_iph = wi ? (half * ((s_e + sn) - (e_e + e0))) : zero;
+                    bool wj = (s_n - e_n > mad) && (sn - e0 > mad);
+                    h_jph = wj ? (half * ((s_n + sn) - (e_n + e0))) : zero;
+                    wet_iph = (h_iph > zero) ? one : zero;
+                    wet_jph = (h_jph > zero) ? one : zero;
+                }
+                const R dw_j = s_n - sn;
+                R uh_n = uh * wet_iph - inv_cell_area_dt_g * h_iph * (s_e - sn) * a.m.dyl[i + 1];
+                R vh_n = vh * wet_jph - inv_cell_area_dt_vh_g * h_jph * dw_j * a.m.dxb[r + 1];
+                if (CORIOLIS) {
+                    // Pre-update 2-point averages (:409-428); rows/cols clamp like
+                    // the reference's j=1 and max(xL-1,1) special cases.
+                    const R vh_iph_jmh = half * (s_vh[rr][cc] + s_vh[rr][cc + 1]);
+                    const R vh_iph_jph = half * (s_vh[rr + 1][cc] + s_vh[rr + 1][cc + 1]);
+                    const R uh_i_j = half * (s_uh[rr][cc + 1] + s_uh[rr][cc]);
+                    const R uh_i_jp1 = half * (s_uh[rr + 1][cc + 1] + s_uh[rr + 1][cc]);
+                    const R dt_half_coriolis = a.dt * a.m.cor[r] * half * ((h_iph > zero) ? one : zero);
+                    const R dt_half_coriolis_jph = a.dt * a.m.cor_be[r + 1] * half * ((h_jph > zero) ? one : zero);
+                    uh_n = uh_n + dt_half_coriolis * (vh_iph_jmh + vh_iph_jph);
+                    vh_n = vh_n - dt_half_coriolis_jph * (uh_i_j + uh_i_jp1);
+                }
+                if (a.lin_fric) {
+                    uh_n = a.lin_fric_mult * uh_n;
+                    vh_n = a.lin_fric_mult * vh_n;
+                }
+                uh = uh_n;
+                vh = vh_n;
+            }
+            uh_o[o] = uh;
+            vh_o[o] = vh;
+        }
     }
 }
 
@@ -267,11 +298,72 @@ __global__ void gauge_kernel(int64_t P, const R *stg, const R *uh, const R *vh, 
     if (threadIdx.x == 0) sc->gauge_records = rec + 1;
 }
 
+template <typename R>
+__global__ void batch_gauge_kernel(int64_t P, const R *stg0, int64_t inst_stride, int nbatch, const int *site_ij,
+                                   int n, double *records, int rec)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n * nbatch) return;
+    const int b = q / n, gi = q - b * n;
+    const int i = site_ij[2 * gi], r = site_ij[2 * gi + 1];
+    records[((int64_t)rec * nbatch + b) * n + gi] = (double)stg0[(int64_t)b * inst_stride + (int64_t)r * P + i];
+}
+
 }  // namespace
 
 template <typename R>
-cudaError_t launch_linear_step(const StepPlanes<R> &p, const Metrics<R> &m, const StepConfig &c, R dt,
-                               DevScalars *sc, cudaStream_t s, const LaunchHook &hook)
+cudaError_t launch_batch_gauges(int64_t pitch, const R *stg0, int64_t inst_stride, int nbatch, const int *site_ij,
+                                int n, double *records, int rec, int capacity, cudaStream_t s)
+{
+    if (rec >= capacity || n <= 0) return cudaSuccess;
+    const int tot = n * nbatch;
+    batch_gauge_kernel<R><<<(tot + 255) / 256, 256, 0, s>>>(pitch, stg0, inst_stride, nbatch, site_ij, n, records,
+                                                            rec);
+    return cudaGetLastError();
+}
+template cudaError_t launch_batch_gauges<double>(int64_t, const double *, int64_t, int, const int *, int, double *,
+                                                 int, int, cudaStream_t);
+template cudaError_t launch_batch_gauges<float>(int64_t, const float *, int64_t, int, const int *, int, double *, int,
+                                                int, cudaStream_t);
+
+// Tile configurations (rows per tile, thread rows, instances per CTA); the
+// batched form's autotuner times each on the real problem.
+struct TileCfg { int by, tyt, ib; };
+constexpr TileCfg kTileCfgs[] = {{16, 8, 1}, {16, 8, 2}, {16, 8, 4}, {32, 8, 2}, {8, 8, 4}};
+constexpr int kNumTileCfgs = sizeof(kTileCfgs) / sizeof(kTileCfgs[0]);
+
+template <typename R, bool COR, bool TL, int BY, int TYT, int IB>
+void launch_cfg(const LinArgs<R> &a, cudaStream_t s)
+{
+    dim3 block(LBX, TYT);
+    dim3 grid((a.p.nx + LBX - 1) / LBX, (a.p.ny + BY - 1) / BY, (a.nbatch + IB - 1) / IB);
+    linear_step_kernel<R, COR, TL, BY, TYT, IB><<<grid, block, 0, s>>>(a);
+}
+
+template <typename R, bool COR, bool TL>
+void launch_tile(const LinArgs<R> &a, int cfg, cudaStream_t s)
+{
+    switch (cfg) {
+    case 1: launch_cfg<R, COR, TL, 16, 8, 2>(a, s); break;
+    case 2: launch_cfg<R, COR, TL, 16, 8, 4>(a, s); break;
+    case 3: launch_cfg<R, COR, TL, 32, 8, 2>(a, s); break;
+    case 4: launch_cfg<R, COR, TL, 8, 8, 4>(a, s); break;
+    default: launch_cfg<R, COR, TL, 16, 8, 1>(a, s); break;
+    }
+}
+
+template <typename R>
+void launch_main(const LinArgs<R> &a, const StepConfig &c, int cfg, cudaStream_t s)
+{
+    const bool cor = c.coriolis != 0, tl = c.truely_linear != 0;
+    if (cor && tl) launch_tile<R, true, true>(a, cfg, s);
+    else if (cor && !tl) launch_tile<R, true, false>(a, cfg, s);
+    else if (!cor && tl) launch_tile<R, false, true>(a, cfg, s);
+    else launch_tile<R, false, false>(a, cfg, s);
+}
+
+template <typename R>
+LinArgs<R> make_args(const StepPlanes<R> &p, const Metrics<R> &m, const StepConfig &c, R dt)
 {
     LinArgs<R> a;
     a.p = p;
@@ -284,21 +376,43 @@ cudaError_t launch_linear_step(const StepPlanes<R> &p, const Metrics<R> &m, cons
     R lfc = R(c.linear_friction_coeff);
     a.lin_fric = (lfc != R(0)) ? 1 : 0;
     a.lin_fric_mult = a.lin_fric ? (R(1) / (R(1) + dt * lfc)) : R(0);
+    a.nbatch = 1;
+    a.inst_stride = 0;
+    a.max_stride = 0;
+    return a;
+}
 
+template <typename R>
+cudaError_t launch_linear_step(const StepPlanes<R> &p, const Metrics<R> &m, const StepConfig &c, R dt,
+                               DevScalars *sc, cudaStream_t s, const LaunchHook &hook)
+{
+    LinArgs<R> a = make_args<R>(p, m, c, dt);
     hook(CAT_LINEAR_EDGE, 0);
     linear_edge_kernel<R><<<1, 512, 0, s>>>(a, sc, c.exterior_cells_width, c.bf);
     hook(CAT_LINEAR_EDGE, 1);
-    dim3 block(LBX, LTY);
-    dim3 grid((p.nx + LBX - 1) / LBX, (p.ny + LBY - 1) / LBY);
-    const bool cor = c.coriolis != 0, tl = c.truely_linear != 0;
     hook(CAT_LINEAR_MAIN, 0);
-    if (cor && tl) linear_step_kernel<R, true, true><<<grid, block, 0, s>>>(a);
-    else if (cor && !tl) linear_step_kernel<R, true, false><<<grid, block, 0, s>>>(a);
-    else if (!cor && tl) linear_step_kernel<R, false, true><<<grid, block, 0, s>>>(a);
-    else linear_step_kernel<R, false, false><<<grid, block, 0, s>>>(a);
+    launch_main<R>(a, c, 0, s);
     hook(CAT_LINEAR_MAIN, 1);
     return cudaGetLastError();
 }
+
+template <typename R>
+cudaError_t launch_linear_batch(const StepPlanes<R> &p0, int64_t inst_stride, int64_t max_stride, int nbatch,
+                                const Metrics<R> &m, const StepConfig &c, R dt, int tile_cfg, cudaStream_t s,
+                                const LaunchHook &hook)
+{
+    LinArgs<R> a = make_args<R>(p0, m, c, dt);
+    a.bc_stage = 0;
+    a.nbatch = nbatch;
+    a.inst_stride = inst_stride;
+    a.max_stride = max_stride;
+    hook(CAT_LINEAR_MAIN, 0);
+    launch_main<R>(a, c, tile_cfg, s);
+    hook(CAT_LINEAR_MAIN, 1);
+    return cudaGetLastError();
+}
+
+int linear_tile_config_count() { return kNumTileCfgs; }
 
 template <typename R>
 cudaError_t launch_update_max_stage(int nx, int ny, int64_t pitch, const R *stg, R *max_stage, const StepConfig &c,
@@ -324,6 +438,12 @@ template cudaError_t launch_linear_step<double>(const StepPlanes<double> &, cons
 template cudaError_t launch_linear_step<float>(const StepPlanes<float> &, const Metrics<float> &,
                                                const StepConfig &, float, DevScalars *, cudaStream_t,
                                                const LaunchHook &);
+template cudaError_t launch_linear_batch<double>(const StepPlanes<double> &, int64_t, int64_t, int,
+                                                 const Metrics<double> &, const StepConfig &, double, int,
+                                                 cudaStream_t, const LaunchHook &);
+template cudaError_t launch_linear_batch<float>(const StepPlanes<float> &, int64_t, int64_t, int,
+                                                const Metrics<float> &, const StepConfig &, float, int, cudaStream_t,
+                                                const LaunchHook &);
 template cudaError_t launch_update_max_stage<double>(int, int, int64_t, const double *, double *,
                                                      const StepConfig &, cudaStream_t);
 template cudaError_t launch_update_max_stage<float>(int, int, int64_t, const float *, float *,

@@ -50,6 +50,21 @@ template <typename R>
 cudaError_t launch_linear_step(const StepPlanes<R> &p, const Metrics<R> &m, const StepConfig &c,
                                R dt, DevScalars *sc, cudaStream_t s, const LaunchHook &hook);
 
+// Batched truly/not-truly linear leapfrog: `nbatch` instances whose planes
+// follow instance 0's at `inst_stride` elements, sharing ELV and metrics
+// (no boundary routine).  tile_cfg selects one of linear_tile_config_count()
+// tile shapes.
+template <typename R>
+cudaError_t launch_linear_batch(const StepPlanes<R> &p0, int64_t inst_stride, int64_t max_stride, int nbatch,
+                                const Metrics<R> &m, const StepConfig &c, R dt, int tile_cfg, cudaStream_t s,
+                                const LaunchHook &hook);
+int linear_tile_config_count();
+
+// Batched gauges: records[rec][b][g] = STG of instance b at gauge g.
+template <typename R>
+cudaError_t launch_batch_gauges(int64_t pitch, const R *stg0, int64_t inst_stride, int nbatch, const int *site_ij,
+                                int n, double *records, int rec, int capacity, cudaStream_t s);
+
 // max_stage = max(max_stage, STG) over the active region (domain_mod.f90:2243-2290).
 template <typename R>
 cudaError_t launch_update_max_stage(int nx, int ny, int64_t pitch, const R *stg, R *max_stage,

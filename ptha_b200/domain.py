@@ -220,6 +220,32 @@ class Domain:
         check(self._L.swals_gpu_gauges_read(self._h, _p(out), int(self._gauge_capacity), ctypes.byref(n)))
         return out[: n.value]
 
+    def gauges_reset(self):
+        check(self._L.swals_gpu_gauges_reset(self._h))
+
+    # ------------------------------------------------------------- adjoint
+    def adjoint_linear(self, nsteps, timestep, gauge_adjoint=None, lambda_seed=None):
+        """dL/d(STG,UH,VH) of the initial state, shape (3, ny, nx), given
+        gauge_adjoint[n, g] = dL/d(stage at gauge g after step n+1) and/or
+        lambda_seed = dL/d(state after the last step), shape (3, ny, nx)."""
+        out = np.empty((3, self.nx[1], self.nx[0]), dtype=self.dtype)
+        ga = None if gauge_adjoint is None else np.ascontiguousarray(gauge_adjoint, dtype=np.float64)
+        ls = None if lambda_seed is None else np.ascontiguousarray(lambda_seed, dtype=self.dtype)
+        check(self._L.swals_gpu_adjoint_linear(self._h, int(nsteps), float(timestep),
+                                               None if ga is None else _p(ga), None if ls is None else _p(ls),
+                                               _p(out)))
+        return out
+
+    def misfit_gradient(self, nsteps, timestep, target, checkpoint_every=50):
+        """(L, dL/d(STG,UH,VH)_0) for L = 1/2 sum (gauge stage - target)^2
+        over steps 1..nsteps from the current state (left unchanged)."""
+        target = np.ascontiguousarray(target, dtype=np.float64)
+        out = np.empty((3, self.nx[1], self.nx[0]), dtype=self.dtype)
+        loss = ctypes.c_double()
+        check(self._L.swals_gpu_misfit_gradient_linear(self._h, int(nsteps), float(timestep), _p(target),
+                                                       int(checkpoint_every), ctypes.byref(loss), _p(out)))
+        return loss.value, out
+
     def device_planes(self):
         ptrs = [ctypes.c_void_p() for _ in range(4)]
         pitch = ctypes.c_int64()
