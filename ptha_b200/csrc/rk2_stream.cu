@@ -1,0 +1,236 @@
+// rk2_stream.cu -- finite-volume stage kernel, register-streaming form.
+//
+// Same computation as the shared-memory tile kernel in rk2.cu (and the same
+// device functions: edge_flux, mc_gradient, theta_wd, fv_update), organised
+// for sm_100a's FP64 pipes instead of for shared memory:
+//   - each warp owns a strip of 28 columns (lanes 2..29; lanes 0,1,30,31
+//     carry the 2-cell x-halo) and marches down SH rows plus a 2-row halo at
+//     each end;
+//   - the three rows the north-south limiter needs (j-2, j-1, j), the
+//     north-south gradients of two rows and the south edge of the row being
+//     updated live in registers; east-west neighbours come from warp
+//     shuffles;
+//   - each cell's north-south edge, gradient and fix-ups are computed once
+//     (the tile kernel computes ~2.2 edges and ~2.3 gradients per cell) and
+//     there is no __syncthreads at all;
+//   - the next row's loads are issued before the current row is processed.
+#include "rk2_common.cuh"
+
+namespace swals {
+namespace {
+using namespace fv;
+
+constexpr int SLANES = 32;
+constexpr int SOUT = 28;    // output columns per warp
+constexpr int SWARPS = 4;   // warps per CTA
+constexpr unsigned FULL = 0xffffffffu;
+
+template <typename R> struct Raw { R s, uh, vh, e; };
+
+template <typename R>
+__device__ __forceinline__ Raw<R> load_raw(const Rk2Args<R> &a, int i, int r)
+{
+    Raw<R> x;
+    if (i >= 0 && i < a.nx && r >= 0 && r < a.ny) {
+        const int64_t o = (int64_t)r * a.P + i;
+        x.s = a.stg[o]; x.uh = a.uh[o]; x.vh = a.vh[o]; x.e = a.elv[o];
+    } else {
+        x.s = R(0); x.uh = R(0); x.vh = R(0); x.e = R(0);
+    }
+    return x;
+}
+
+// compute_depth_and_velocity for one cell (domain_mod.f90:1387-1412).
+template <typename R>
+__device__ __forceinline__ Cell<R> fix_up(const Raw<R> &x, bool valid, long long &negfix, bool count)
+{
+    Cell<R> c;
+    c.stg = R(0); c.dep = R(0); c.u = R(0); c.v = R(0); c.elv = R(0);
+    if (valid) {
+        R s = x.s;
+        const R e = x.e;
+        R dep = s - e;
+        if (dep > K<R>::min_depth()) {
+            const R depth_inv = R(1) / dep;
+            c.u = x.uh * depth_inv;
+            c.v = x.vh * depth_inv;
+        } else if (dep < R(0)) {
+            dep = R(0);
+            s = e;
+            if (count) negfix += 1;
+        }
+        c.stg = s; c.dep = dep; c.elv = e;
+    }
+    return c;
+}
+
+template <typename R> __device__ __forceinline__ R up1(R v) { return __shfl_up_sync(FULL, v, 1); }
+template <typename R> __device__ __forceinline__ R dn1(R v) { return __shfl_down_sync(FULL, v, 1); }
+
+template <typename R>
+__device__ __forceinline__ Cell<R> up1(const Cell<R> &c)
+{
+    Cell<R> x; x.stg = up1(c.stg); x.dep = up1(c.dep); x.u = up1(c.u); x.v = up1(c.v); x.elv = up1(c.elv); return x;
+}
+template <typename R>
+__device__ __forceinline__ Cell<R> dn1(const Cell<R> &c)
+{
+    Cell<R> x; x.stg = dn1(c.stg); x.dep = dn1(c.dep); x.u = dn1(c.u); x.v = dn1(c.v); x.elv = dn1(c.elv); return x;
+}
+
+template <typename R>
+__device__ __forceinline__ Grad<R> limited(const Cell<R> &lo, const Cell<R> &c, const Cell<R> &up, R theta)
+{
+    Grad<R> g;
+    const R th = theta_wd<R>(lo.dep, c.dep, up.dep, theta);
+    g.ds = mc_gradient<R>(c.stg, lo.stg, up.stg, th);
+    g.dd = mc_gradient<R>(c.dep, lo.dep, up.dep, th);
+    g.du = mc_gradient<R>(c.u, lo.u, up.u, th);
+    g.dv = mc_gradient<R>(c.v, lo.v, up.v, th);
+    return g;
+}
+
+template <typename R>
+__device__ __forceinline__ void zero_edge(EdgeRes<R> &e)
+{
+    e.f[0] = R(0); e.f[1] = R(0); e.f[2] = R(0); e.es_pos = 0.0; e.es_neg = 0.0;
+}
+
+template <typename R, int MODE, bool SPH, bool COR, int FRIC, int SH>
+__global__ void __launch_bounds__(SLANES *SWARPS) rk2_stream_kernel(const Rk2Args<R> a)
+{
+    const int lane = threadIdx.x & 31;
+    const int wid = blockIdx.x * SWARPS + (threadIdx.x >> 5);
+    const int nx = a.nx, ny = a.ny;
+    const int strips_x = (nx + SOUT - 1) / SOUT;
+    const int sx = wid % strips_x, sy = wid / strips_x;
+    const int ra = sy * SH;
+    if (ra >= ny) return;  // whole warp
+    const int rb = min(ra + SH, ny);
+    const int i = sx * SOUT - 2 + lane;
+    const bool col_valid = (i >= 0 && i < nx);
+    const bool out_lane = (lane >= 2 && lane <= 29 && i < nx);
+    const bool ew_lane = (lane >= 2 && lane <= 30);   // lanes whose west edge is fully determined
+
+    R dt = R(0);
+    if (MODE != MODE_CFL) dt = stage_dt<R>(a);
+    const R inv2 = R(1) / (a.m.dyl[0] * a.half_cfl);  // dx_cfl_half_inv(2): NS edges
+    double cfl = 0.0;
+    long long negfix = 0;
+
+    Cell<R> c0, c1, c2;
+    c0.stg = c0.dep = c0.u = c0.v = c0.elv = R(0);
+    c1 = c0; c2 = c0;
+    Grad<R> g1, g2;
+    g1.ds = g1.dd = g1.du = g1.dv = R(0);
+    g2 = g1;
+    EdgeRes<R> e_s;  // south edge of the row being updated
+    zero_edge(e_s);
+
+    Raw<R> nxt = load_raw<R>(a, i, ra - 2);
+    for (int r = ra - 2, k = 0; r <= rb + 1; r++, k++) {
+        const Raw<R> cur = nxt;
+        if (r + 1 <= rb + 1) nxt = load_raw<R>(a, i, r + 1);
+        c2 = c1;
+        c1 = c0;
+        c0 = fix_up<R>(cur, col_valid && r >= 0 && r < ny, negfix, out_lane && r >= ra && r < rb);
+        if (k < 2) continue;
+
+        // North-south gradient of row r-1 (DE1_inner_include.f90:746-781).
+        g2 = g1;
+        {
+            const int rg = r - 1;
+            if (col_valid && rg > 0 && rg < ny - 1) g1 = limited<R>(c2, c1, c0, a.theta);
+            else { g1.ds = R(0); g1.dd = R(0); g1.du = R(0); g1.dv = R(0); }
+        }
+        if (k < 3) continue;
+
+        // North-south edge between rows r-2 and r-1 (edge index r-1).
+        EdgeRes<R> e_n;
+        zero_edge(e_n);
+        {
+            const int e = r - 1;
+            if (e >= 1 && e <= ny - 1 && i >= 1 && i <= nx - 1) {
+                double cand;
+                edge_flux<R, true>(c2, g2, c1, g1, a.m.dxb[e], inv2, e_n, cand);
+                cfl = fmax(cfl, cand);
+                if (MODE != MODE_CFL && a.lines && i >= a.n_ext && i <= nx - a.n_ext - 1) {
+                    if (e == ny - a.n_ext) a.lines[i] = (double)e_n.f[0];
+                    if (e == a.n_ext) a.lines[nx + ny + i] = (double)e_n.f[0];
+                }
+            }
+        }
+        if (k < 4) { e_s = e_n; continue; }
+
+        // Row R = r-2: east-west gradient and west edge, then the update.
+        const int R_ = r - 2;
+        const Cell<R> cl = up1(c2), cr = dn1(c2);
+        Grad<R> gew;
+        if (col_valid && i > 0 && i < nx - 1) gew = limited<R>(cl, c2, cr, a.theta);
+        else { gew.ds = R(0); gew.dd = R(0); gew.du = R(0); gew.dv = R(0); }
+        Grad<R> gw;
+        gw.ds = up1(gew.ds); gw.dd = up1(gew.dd); gw.du = up1(gew.du); gw.dv = up1(gew.dv);
+        EdgeRes<R> e_w;
+        zero_edge(e_w);
+        if (ew_lane && i >= 1 && i <= nx - 1 && R_ >= 1 && R_ <= ny - 1) {
+            const R inv1 = R(1) / (a.m.dxb[R_] * a.half_cfl);  // dx_cfl_half_inv(1): EW edges
+            double cand;
+            edge_flux<R, false>(cl, gw, c2, gew, a.m.dyl[i], inv1, e_w, cand);
+            cfl = fmax(cfl, cand);
+            if (MODE != MODE_CFL && a.lines && R_ >= a.n_ext && R_ <= ny - a.n_ext - 1) {
+                if (i == nx - a.n_ext) a.lines[nx + R_] = (double)e_w.f[0];
+                if (i == a.n_ext) a.lines[2 * nx + ny + R_] = (double)e_w.f[0];
+            }
+        }
+        if (MODE != MODE_CFL) {
+            EdgeRes<R> e_e;
+            e_e.f[0] = dn1(e_w.f[0]); e_e.f[1] = dn1(e_w.f[1]); e_e.f[2] = dn1(e_w.f[2]);
+            e_e.es_neg = dn1(e_w.es_neg);
+            e_e.es_pos = 0.0;
+            if (out_lane) fv_update<R, MODE, SPH, COR, FRIC>(a, i, R_, c2, e_s, e_n, e_w, e_e, dt);
+        }
+        e_s = e_n;
+    }
+
+    // Warp reductions: CFL max and the negative-depth count.
+    if (a.write_cfl || MODE == MODE_CFL) {
+        for (int o = 16; o > 0; o >>= 1) cfl = fmax(cfl, __shfl_down_sync(FULL, cfl, o));
+        if (lane == 0 && cfl > 0.0) atomicMax(&a.sc->max_dt_inv_bits, (unsigned long long)__double_as_longlong(cfl));
+    }
+    if (MODE != MODE_CFL) {
+        for (int o = 16; o > 0; o >>= 1) negfix += __shfl_down_sync(FULL, negfix, o);
+        if (lane == 0 && negfix) atomicAdd((unsigned long long *)&a.sc->negative_depth_fix_counter,
+                                           (unsigned long long)negfix);
+    }
+}
+
+}  // namespace
+
+template <typename R, int MODE, bool SPH, bool COR, int FRIC>
+cudaError_t launch_stage_stream(const Rk2Args<R> &a, cudaStream_t s)
+{
+    constexpr int SH = 32;
+    const int strips_x = (a.nx + SOUT - 1) / SOUT;
+    const int strips_y = (a.ny + SH - 1) / SH;
+    const int warps = strips_x * strips_y;
+    const int blocks = (warps + SWARPS - 1) / SWARPS;
+    rk2_stream_kernel<R, MODE, SPH, COR, FRIC, SH><<<blocks, SLANES * SWARPS, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+#define SWALS_INST(R, MODE, SPH, COR, FRIC) \
+    template cudaError_t launch_stage_stream<R, MODE, SPH, COR, FRIC>(const fv::Rk2Args<R> &, cudaStream_t);
+#define SWALS_INST_F(R, MODE, SPH, COR) \
+    SWALS_INST(R, MODE, SPH, COR, fv::FRIC_MANNING) SWALS_INST(R, MODE, SPH, COR, fv::FRIC_CHEZY) \
+    SWALS_INST(R, MODE, SPH, COR, fv::FRIC_NONE)
+#define SWALS_INST_M(R, SPH, COR) \
+    SWALS_INST_F(R, fv::MODE_CFL, SPH, COR) SWALS_INST_F(R, fv::MODE_STAGE1, SPH, COR) \
+    SWALS_INST_F(R, fv::MODE_STAGE2, SPH, COR)
+SWALS_INST_M(double, false, false)
+SWALS_INST_M(double, true, false)
+SWALS_INST_M(double, true, true)
+SWALS_INST_M(float, false, false)
+SWALS_INST_M(float, true, false)
+SWALS_INST_M(float, true, true)
+
+}  // namespace swals

@@ -69,11 +69,14 @@ def test_misfit_gradient_vs_oracle_finite_differences():
     wet = np.argwhere(U[3] < -20.0)
     pick = wet[rng.choice(len(wet), 16, replace=False)]
     eps = 1e-6
+    # L is quadratic in eta0, so central differences have no truncation
+    # error; their round-off floor is about eps_mach * L / eps.
+    fd_floor = 10 * np.finfo(float).eps * max(loss, 1.0) / eps
     for j, i in pick:
         Up = U.copy(); Up[0, j, i] += eps
         Um = U.copy(); Um[0, j, i] -= eps
         fd = (oracle_loss(Up) - oracle_loss(Um)) / (2 * eps)
-        assert grad[0, j, i] == pytest.approx(fd, rel=1e-6, abs=1e-9), (i, j, grad[0, j, i], fd)
+        assert grad[0, j, i] == pytest.approx(fd, rel=1e-6, abs=fd_floor), (i, j, grad[0, j, i], fd)
 
 
 @pytest.mark.gpu
