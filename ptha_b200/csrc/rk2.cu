@@ -242,14 +242,18 @@ __global__ void __launch_bounds__(NT, 3) rk2_stage_kernel(const Rk2Args<R> a)
 
 // ---------------------------------------------------------------------------
 // Boundary routines on the non-staggered grid (boundary_mod.f90:21-75 and
-// :78-163).  One block: the west/east pass completes before the south/north
-// pass, as in the reference's two OpenMP loops (corner cells end with the
-// south/north values).
+// :78-163).  The reference applies them in two OpenMP loops: a west/east pass
+// over j, then a south/north pass over i, so a corner cell ends with its
+// south/north value, and that value reads the west/east result of the cell
+// next to it in the column.  Here one thread owns one ring cell; the corner
+// threads recompute that west/east value themselves instead of reading it,
+// so no thread reads a cell another thread writes and the kernel needs no
+// grid-wide ordering.
 //   STAGE_MODE 1: in place on the stage output (stage 1 of rk2, euler).
 //   STAGE_MODE 2: rk2 stage 2.  The stage kernel already wrote the averaged
-//                 state; here the outer ring is recomputed from the saved
-//                 pre-average values, the boundary values applied, and then
-//                 averaged with the backed-up U0 ring.
+//                 state; the ring's inputs are the pre-average values the
+//                 stage kernel saved in the side buffer, and the boundary
+//                 values are averaged with the backed-up U0 ring here.
 template <typename R>
 struct BcArgs {
     int nx, ny;
@@ -261,7 +265,7 @@ struct BcArgs {
     R *stg, *uh, *vh;       // stage output planes
     const R *stg0, *uh0, *vh0;  // backup U0 (mode 2)
     R *elv;
-    R *side;                // mode 2: saved outer two rings (updated in place)
+    const R *side;          // mode 2: saved pre-average outer two rings
     R *max_stage;
     int stage_mode;
     int dt_from_cfl;
@@ -271,48 +275,58 @@ struct BcArgs {
     DevScalars *sc;
 };
 
-template <typename R>
-__device__ __forceinline__ R *side_ptr(const BcArgs<R> &a, int i, int r)
-{
-    const int nx = a.nx, ny = a.ny;
-    int k = -1;
-    if (i == 0) k = 0; else if (i == 1) k = 1; else if (i == nx - 1) k = 3; else if (i == nx - 2) k = 2;
-    if (k >= 0) return a.side + ((int64_t)k * ny + r) * 3;
-    if (r == 0) k = 0; else if (r == 1) k = 1; else if (r == ny - 1) k = 3; else k = 2;
-    return a.side + (int64_t)4 * ny * 3 + ((int64_t)k * nx + i) * 3;
-}
+template <typename R> struct RingVal { R s, uh, vh, e; };
 
+// Stage-output value of a cell in the outer two rings or the interior
+// (mode 2 reads the saved pre-average copy; every cell of the outer two
+// rings has both a column and a row copy).
 template <typename R>
 __device__ __forceinline__ R bc_get(const BcArgs<R> &a, int i, int r, int v)
 {
-    if (a.stage_mode == 2) return side_ptr(a, i, r)[v];
+    if (a.stage_mode == 2) {
+        const int nx = a.nx, ny = a.ny;
+        int k = -1;
+        if (i == 0) k = 0; else if (i == 1) k = 1; else if (i == nx - 2) k = 2; else if (i == nx - 1) k = 3;
+        if (k >= 0) return a.side[((int64_t)k * ny + r) * 3 + v];
+        k = (r == 0) ? 0 : (r == 1) ? 1 : (r == ny - 1) ? 3 : 2;
+        return a.side[(int64_t)4 * ny * 3 + ((int64_t)k * nx + i) * 3 + v];
+    }
     const R *pl = (v == 0) ? a.stg : (v == 1) ? a.uh : a.vh;
     return pl[(int64_t)r * a.P + i];
 }
 
+// West/east pass value of ring cell (i, r), i in {0, nx-1}.
 template <typename R>
-__device__ __forceinline__ void bc_set(const BcArgs<R> &a, int i, int r, R s, R u, R v)
+__device__ __forceinline__ RingVal<R> we_value(const BcArgs<R> &a, int i, int r, double t)
 {
-    if (a.stage_mode == 2) {
-        R *d = side_ptr(a, i, r);
-        d[0] = s; d[1] = u; d[2] = v;
-        if (r == 0 || r == 1 || r == a.ny - 1 || r == a.ny - 2) {
-            // keep the row copy of corner-adjacent cells consistent too
-            int k = (r == 0) ? 0 : (r == 1) ? 1 : (r == a.ny - 1) ? 3 : 2;
-            R *d2 = a.side + (int64_t)4 * a.ny * 3 + ((int64_t)k * a.nx + i) * 3;
-            d2[0] = s; d2[1] = u; d2[2] = v;
-        }
-        return;
+    const int in = (i == 0) ? 1 : a.nx - 2;
+    RingVal<R> v;
+    if (a.kind == 1) {  // transmissive: all four variables from the inner neighbour
+        v.e = a.elv[(int64_t)r * a.P + in];
+        v.s = bc_get(a, in, r, 0); v.uh = bc_get(a, in, r, 1); v.vh = bc_get(a, in, r, 2);
+    } else {
+        boundary_function<R>(a.bf, a.x, t, i, r, v.s, v.e);
+        v.uh = bc_get(a, in, r, 1);
+        v.vh = R(0);
     }
-    const int64_t o = (int64_t)r * a.P + i;
-    a.stg[o] = s; a.uh[o] = u; a.vh[o] = v;
+    return v;
 }
 
 template <typename R>
-__global__ void __launch_bounds__(1024) rk2_boundary_kernel(const BcArgs<R> a)
+__global__ void __launch_bounds__(256) rk2_boundary_kernel(const BcArgs<R> a)
 {
     const int nx = a.nx, ny = a.ny;
-    const int64_t P = a.P;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    // Ring cells, each once: rows 0 and ny-1 in full, then columns 0 and
+    // nx-1 for rows 1..ny-2.
+    int i, r;
+    if (q < 2 * nx) { i = q % nx; r = (q < nx) ? 0 : ny - 1; }
+    else if (q < 2 * nx + 2 * (ny - 2)) { const int p = q - 2 * nx; r = 1 + p % (ny - 2); i = (p < ny - 2) ? 0 : nx - 1; }
+    else return;
+    const bool sn = (r == 0 && a.bext[2]) || (r == ny - 1 && a.bext[0]);
+    const bool we = (i == 0 && a.bext[3]) || (i == nx - 1 && a.bext[1]);
+    if (!sn && !we) return;
+
     double dtd;
     if (a.dt_from_cfl) {
         double bits_max = __longlong_as_double((long long)a.sc->max_dt_inv_bits);
@@ -324,76 +338,52 @@ __global__ void __launch_bounds__(1024) rk2_boundary_kernel(const BcArgs<R> a)
     double t = a.sc->time;
     for (int k = 0; k < a.n_dt; k++) t = t + dtd;
 
-    // West / east pass
-    for (int r = threadIdx.x; r < ny; r += blockDim.x) {
-        for (int side = 0; side < 2; side++) {
-            const bool west = (side == 0);
-            if (!(west ? a.bext[3] : a.bext[1])) continue;
-            const int i = west ? 0 : nx - 1;
-            const int in = west ? 1 : nx - 2;
-            if (a.kind == 1) {  // transmissive: all four variables from the inner neighbour
-                a.elv[(int64_t)r * P + i] = a.elv[(int64_t)r * P + in];
-                bc_set(a, i, r, bc_get(a, in, r, 0), bc_get(a, in, r, 1), bc_get(a, in, r, 2));
-            } else {
-                R s, e;
-                boundary_function<R>(a.bf, a.x, t, i, r, s, e);
-                a.elv[(int64_t)r * P + i] = e;
-                bc_set(a, i, r, s, bc_get(a, in, r, 1), R(0));
-            }
-        }
-    }
-    __syncthreads();
-    // South / north pass
-    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
-        for (int side = 0; side < 2; side++) {
-            const bool south = (side == 0);
-            if (!(south ? a.bext[2] : a.bext[0])) continue;
-            const int r = south ? 0 : ny - 1;
-            const int rn = south ? 1 : ny - 2;
-            if (a.kind == 1) {
-                a.elv[(int64_t)r * P + i] = a.elv[(int64_t)rn * P + i];
-                bc_set(a, i, r, bc_get(a, i, rn, 0), bc_get(a, i, rn, 1), bc_get(a, i, rn, 2));
-            } else {
-                R s, e;
-                boundary_function<R>(a.bf, a.x, t, i, r, s, e);
-                a.elv[(int64_t)r * P + i] = e;
-                bc_set(a, i, r, s, R(0), bc_get(a, i, rn, 2));
-            }
-        }
-    }
-    if (a.stage_mode != 2) return;
-    __syncthreads();
-    // rk2 average of the boundary ring and its max_stage.
-    const int nring = 2 * nx + 2 * ny;
-    for (int q = threadIdx.x; q < nring; q += blockDim.x) {
-        int i, r;
-        if (q < nx) { i = q; r = 0; }
-        else if (q < 2 * nx) { i = q - nx; r = ny - 1; }
-        else if (q < 2 * nx + ny) { i = 0; r = q - 2 * nx; }
-        else { i = nx - 1; r = q - 2 * nx - ny; }
-        const bool bc = (r == 0 && a.bext[2]) || (r == ny - 1 && a.bext[0]) || (i == 0 && a.bext[3]) ||
-                        (i == nx - 1 && a.bext[1]);
-        if (!bc) continue;
-        // Cells on both a row and a column of the ring appear twice; the
-        // values are identical so the duplicate write is harmless.
-        const R *d;
-        if ((r == 0 && a.bext[2]) || (r == ny - 1 && a.bext[0])) {
-            const int k = (r == 0) ? 0 : 3;
-            d = a.side + (int64_t)4 * ny * 3 + ((int64_t)k * nx + i) * 3;
+    RingVal<R> v;
+    if (sn) {
+        const int rn = (r == 0) ? 1 : ny - 2;
+        // The column neighbour after the west/east pass.
+        RingVal<R> nb;
+        const bool nb_we = (i == 0 && a.bext[3]) || (i == nx - 1 && a.bext[1]);
+        if (nb_we) {
+            nb = we_value<R>(a, i, rn, t);
         } else {
-            const int k = (i == 0) ? 0 : 3;
-            d = a.side + ((int64_t)k * ny + r) * 3;
+            nb.e = a.elv[(int64_t)rn * a.P + i];
+            nb.s = bc_get(a, i, rn, 0); nb.uh = bc_get(a, i, rn, 1); nb.vh = bc_get(a, i, rn, 2);
         }
-        const int64_t o = (int64_t)r * P + i;
-        const R s = R(0.5) * (d[0] + a.stg0[o]);
-        a.stg[o] = s;
-        a.uh[o] = R(0.5) * (d[1] + a.uh0[o]);
-        a.vh[o] = R(0.5) * (d[2] + a.vh0[o]);
-        if (a.max_stage) {
-            R mx = a.max_stage[o];
-            a.max_stage[o] = (s > mx) ? s : mx;
+        if (a.kind == 1) {
+            v = nb;
+        } else {
+            boundary_function<R>(a.bf, a.x, t, i, r, v.s, v.e);
+            v.uh = R(0);
+            v.vh = nb.vh;
         }
+    } else {
+        v = we_value<R>(a, i, r, t);
     }
+
+    const int64_t o = (int64_t)r * a.P + i;
+    a.elv[o] = v.e;
+    if (a.stage_mode != 2) {
+        a.stg[o] = v.s; a.uh[o] = v.uh; a.vh[o] = v.vh;
+        return;
+    }
+    // rk2 average of the ring cell and its max_stage.
+    const R s = R(0.5) * (v.s + a.stg0[o]);
+    a.stg[o] = s;
+    a.uh[o] = R(0.5) * (v.uh + a.uh0[o]);
+    a.vh[o] = R(0.5) * (v.vh + a.vh0[o]);
+    if (a.max_stage) {
+        R mx = a.max_stage[o];
+        a.max_stage[o] = (s > mx) ? s : mx;
+    }
+}
+
+template <typename R>
+cudaError_t launch_boundary(const BcArgs<R> &b, cudaStream_t s)
+{
+    const int n = 2 * b.nx + 2 * (b.ny - 2);
+    rk2_boundary_kernel<R><<<(n + 255) / 256, 256, 0, s>>>(b);
+    return cudaGetLastError();
 }
 
 // End of a step: domain%max_dt, time, boundary-flux integrals, counters
@@ -589,9 +579,9 @@ cudaError_t launch_rk2_step(R *const planes[3][3], int &cur, R *elv, R *max_stag
         b.stg = planes[B][0]; b.uh = planes[B][1]; b.vh = planes[B][2];
         b.stage_mode = 1; b.n_dt = 1;
         hook(CAT_BC1, 0);
-        rk2_boundary_kernel<R><<<1, 1024, 0, s>>>(b);
+        e = launch_boundary<R>(b, s);
         hook(CAT_BC1, 1);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if (e != cudaSuccess) return e;
     }
     if (euler_only) {
         if (max_stage) {
@@ -627,9 +617,9 @@ cudaError_t launch_rk2_step(R *const planes[3][3], int &cur, R *elv, R *max_stag
         b.stg0 = planes[A][0]; b.uh0 = planes[A][1]; b.vh0 = planes[A][2];
         b.stage_mode = 2; b.n_dt = 2; b.max_stage = max_stage;
         hook(CAT_BC2, 0);
-        rk2_boundary_kernel<R><<<1, 1024, 0, s>>>(b);
+        e = launch_boundary<R>(b, s);
         hook(CAT_BC2, 1);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if (e != cudaSuccess) return e;
     }
     hook(CAT_FINALIZE, 0);
     rk2_finalize_kernel<R><<<1, 1024, 0, s>>>(nx, ny, c.exterior_cells_width, lines1, lines2, 0, a.dt_from_cfl,
