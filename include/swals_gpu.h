@@ -253,6 +253,61 @@ int swals_gpu_adjoint_linear(swals_domain *d, int32_t nsteps, double timestep, c
 int swals_gpu_misfit_gradient_linear(swals_domain *d, int32_t nsteps, double timestep, const double *target,
                                      int32_t checkpoint_every, double *loss, void *grad_U0);
 
+/* ---- Multidomain nesting on one GPU -------------------------------------
+ * Replaces multidomain_type's evolve_one_step and halo exchange
+ * (multidomain_mod.f90:1081-1212, send_halos/recv_halos :2449-2565) for
+ * domains that share a device.  The tables are what the reference's setup
+ * (setup_multidomain_domains, multidomain_mod.f90:2781-3553) produces; the
+ * Python mirror ptha_b200/nesting.py builds them the same way. */
+typedef struct swals_multidomain swals_multidomain;
+
+/* A matched pair of a receive box of `receiver` and the send box of
+ * `sender` that feeds it (a recv_metadata row and its send_metadata row,
+ * multidomain_mod.f90:3170-3330).  Boxes are 1-based and inclusive:
+ * iL, iU, jL, jU.  All four variables STG..ELV are exchanged. */
+typedef struct swals_nest_exchange {
+    int32_t sender, receiver;   /* indices into the domain array */
+    int32_t send_box[4];
+    int32_t recv_box[4];
+} swals_nest_exchange;
+
+/* Create a multidomain over `ndomains` (<= 16) domains on one device, with
+ * all_dx (2 per domain: the cell sizes setup recorded before widening the
+ * domains, all_dx_md of multidomain_mod.f90:960-1060; NULL: lw/nx of each
+ * domain), each domain's timestepping_refinement_factor (NULL: all 1), the exchange
+ * table, and, when flux_correction is nonzero, each domain's
+ * priority_domain_index (nx*ny, column-major, 1-based domain indices;
+ * multidomain_mod.f90:2935-2960).  use_wetdry_limiting mirrors
+ * use_wetdry_limiting_nesting (:2663).  While the multidomain exists every
+ * domain launches on the first domain's stream; destroy it before its
+ * domains. */
+int swals_gpu_md_create(swals_domain *const *domains, int32_t ndomains, const double *all_dx,
+                        const int32_t *timestepping_refinement_factor, const swals_nest_exchange *exchanges,
+                        int32_t nexchanges, const int32_t *const *priority_domain_index,
+                        int32_t use_wetdry_limiting, int32_t flux_correction, swals_multidomain **out);
+int swals_gpu_md_destroy(swals_multidomain *md);
+/* evolve_multidomain_one_step_shallow_water (multidomain_mod.f90:1093-1212):
+ * every domain takes its refinement factor of sub-steps of dt/nt (fixed
+ * steps), then all halos are packed, unpacked and flux-corrected. */
+int swals_gpu_md_evolve_one_step(swals_multidomain *md, double dt);
+/* process_data_to_send for every exchange (nested_grid_comms_mod.f90:1387-2046). */
+int swals_gpu_md_send_halos(swals_multidomain *md);
+/* process_received_data for every exchange, then the staggered-grid fix-ups
+ * (nested_grid_comms_mod.f90:2048-2249; domain_mod.f90:3712-3893). */
+int swals_gpu_md_recv_halos(swals_multidomain *md);
+/* nesting_flux_correction_everywhere on every domain (domain_mod.f90:2766-3610). */
+int swals_gpu_md_flux_correction(swals_multidomain *md);
+/* Length of an exchange's buffer, and a copy of it (send_buffer). */
+int swals_gpu_md_buffer_size(swals_multidomain *md, int32_t exchange, int64_t *n);
+int swals_gpu_md_download_buffer(swals_multidomain *md, int32_t exchange, double *out, int64_t n);
+/* Flux integrals of an exchange: which = 0 send box, 1 receive box,
+ * 2 receive-box flux error; laid out edge by edge (N, S, E, W), then
+ * variable by variable (STG..ELV). */
+int swals_gpu_md_download_flux(swals_multidomain *md, int32_t exchange, int32_t which, double *out, int64_t n);
+int swals_gpu_md_time(swals_multidomain *md, double *time);
+int swals_gpu_md_synchronize(swals_multidomain *md);
+int swals_gpu_md_launch_count(swals_multidomain *md, int64_t *n);
+
 /* Last error message of this thread (util/stop_mod.f90 prints before stopping). */
 int swals_gpu_last_error(char *buf, size_t len);
 /* Library version string. */

@@ -66,6 +66,8 @@ class _OracleDomainC(ctypes.Structure):
         ("depth", ctypes.c_void_p), ("velocity", ctypes.c_void_p), ("flux_NS", ctypes.c_void_p),
         ("flux_EW", ctypes.c_void_p), ("explicit_source", ctypes.c_void_p),
         ("explicit_source_VH_j_minus_1", ctypes.c_void_p), ("backup_U", ctypes.c_void_p),
+        ("nest_nbox", ctypes.c_int32), ("pad1", ctypes.c_int32), ("nest_boxes", ctypes.c_void_p),
+        ("nest_offset", ctypes.c_void_p), ("nest_integral", ctypes.c_void_p),
     ]
 
 

@@ -396,6 +396,50 @@ double ORACLE_FN(volume_interior)(const oracle_domain *d)
 
 /* ------------------------------------------------------------------------ */
 /* Linear leapfrog: domain_mod_linear_solver_include.f90:58-571 */
+/* boundary_flux_integral_tstep (nested_grid_comms_mod.f90:2300-2469) for
+ * every nesting box of the domain.  flux_NS(i, j, kk) is at
+ * fNS[(kk-1)*ns_plane + (j-1)*nx + (i-1)] with j = 1..ns_ny (edge rows
+ * offset by ns_lower-1), flux_EW(i, j, kk) at
+ * fEW[(kk-1)*ew_plane + (j-1)*ew_nx + (i-1)] with i = 1..ew_nx; variables
+ * k1..k2 of the integrals are updated from flux variables k1..k2. */
+static void nest_flux_tstep(oracle_domain *d, double dt, const REAL *fNS, int ns_ny, size_t ns_plane, int ns_lower,
+                            const REAL *fEW, int ew_nx, size_t ew_plane, int ew_lower, int k1, int k2, int premult)
+{
+    const int nx = d->nx;
+    for (int b = 0; b < d->nest_nbox; b++) {
+        const int32_t *bx = d->nest_boxes + 4 * b;
+        const int iL = bx[0], iU = bx[1], jL = bx[2], jU = bx[3];
+        const int64_t bl = iU - iL + 1, bw = jU - jL + 1;
+        double *x = d->nest_integral + d->nest_offset[b];
+        /* NORTH (ns = jU + 1) and SOUTH (ns = jL) */
+        for (int e = 0; e < 2; e++) {
+            const int ns = (e == 0) ? jU + 1 : jL;
+            const int dns = ns_lower - 1;
+            if (!(ns - dns >= 1 && ns - dns <= ns_ny)) continue;
+            double *xe = x + ((e == 0) ? 0 : 4 * bl);
+            for (int k = k1; k <= k2; k++)
+                for (int m = iL; m <= iU; m++) {
+                    const REAL f = fNS[(size_t)(k - 1) * ns_plane + (size_t)(ns - dns - 1) * (size_t)nx + (size_t)(m - 1)];
+                    const REAL w = premult ? ONE : d->dxb[ns - 1];
+                    xe[(k - 1) * bl + (m - iL)] = xe[(k - 1) * bl + (m - iL)] + (double)(((REAL)dt * f) * w);
+                }
+        }
+        /* EAST (ns = iU + 1) and WEST (ns = iL) */
+        for (int e = 0; e < 2; e++) {
+            const int ns = (e == 0) ? iU + 1 : iL;
+            const int dns = ew_lower - 1;
+            if (!(ns - dns >= 1 && ns - dns <= ew_nx)) continue;
+            double *xe = x + 8 * bl + ((e == 0) ? 0 : 4 * bw);
+            for (int k = k1; k <= k2; k++)
+                for (int m = jL; m <= jU; m++) {
+                    const REAL f = fEW[(size_t)(k - 1) * ew_plane + (size_t)(m - 1) * (size_t)ew_nx + (size_t)(ns - dns - 1)];
+                    const REAL w = premult ? ONE : d->dyl[ns - 1];
+                    xe[(k - 1) * bw + (m - jL)] = xe[(k - 1) * bw + (m - jL)] + (double)(((REAL)dt * f) * w);
+                }
+        }
+    }
+}
+
 static void linear_leapfrog_step(oracle_domain *d, REAL dt)
 {
     const int nx = d->nx, ny = d->ny;
@@ -403,6 +447,13 @@ static void linear_leapfrog_step(oracle_domain *d, REAL dt)
     const int truely_linear = d->truely_linear;
     const REAL msl = (REAL)d->msl_linear;
     d->dt_last_update = dt;
+
+    /* Nesting flux integrals of the fluxes through the cell faces before the
+     * update (:71-77): flux_NS = U(:,:,VH), flux_EW = U(:,:,UH), lower index 2. */
+    if (d->nest_nbox > 0) {
+        const size_t plane = (size_t)nx * (size_t)ny;
+        nest_flux_tstep(d, (double)dt, d->U + 2 * plane, ny, plane, 2, d->U + plane, nx, plane, 2, 1, 1, 0);
+    }
 
     /* Stage update (:92-115) */
     #pragma omp parallel for schedule(static)
@@ -948,7 +999,15 @@ static void update_U(oracle_domain *d, REAL dt)
 }
 
 /* timestepping_alternatives_include.f90:8-62 */
-static void one_euler_step(oracle_domain *d, double timestep, int has_ts)
+static void nest_flux_tstep_fv(oracle_domain *d, double dt)
+{
+    if (d->nest_nbox <= 0) return;
+    const int nx = d->nx, ny = d->ny;
+    nest_flux_tstep(d, dt, d->flux_NS, ny + 1, (size_t)nx * (size_t)(ny + 1), 1, d->flux_EW, nx + 1,
+                    (size_t)(nx + 1) * (size_t)ny, 1, OR_STG, OR_VH, 1);
+}
+
+static void one_euler_step(oracle_domain *d, double timestep, int has_ts, int nesting_bf)
 {
     double ts = compute_fluxes(d);
     d->max_dt = ts;
@@ -957,6 +1016,7 @@ static void one_euler_step(oracle_domain *d, double timestep, int has_ts)
     double tot = 0.0;
     for (int k = 0; k < 4; k++) tot += d->boundary_flux_store[k];
     d->boundary_flux_evolve_integral = d->boundary_flux_evolve_integral + (double)(REAL)ts * tot;
+    if (nesting_bf) nest_flux_tstep_fv(d, (double)(REAL)ts);
 }
 
 /* timestepping_alternatives_include.f90:64-146 */
@@ -967,10 +1027,12 @@ static void one_rk2_step(oracle_domain *d, double timestep, int has_ts)
     double backup_time = d->time;
     memcpy(d->backup_U, d->U, 3 * plane * sizeof(REAL));
     double dt_first_step;
-    if (has_ts) { one_euler_step(d, timestep, 1); dt_first_step = (REAL)timestep; }
-    else { one_euler_step(d, 0.0, 0); dt_first_step = d->max_dt; }
+    if (has_ts) { one_euler_step(d, timestep, 1, 0); dt_first_step = (REAL)timestep; }
+    else { one_euler_step(d, 0.0, 0, 0); dt_first_step = d->max_dt; }
     double max_dt_store = d->max_dt;
-    one_euler_step(d, dt_first_step, 1);
+    nest_flux_tstep_fv(d, (double)(REAL)(dt_first_step * 0.5));
+    one_euler_step(d, dt_first_step, 1, 0);
+    nest_flux_tstep_fv(d, (double)(REAL)(dt_first_step * 0.5));
     for (size_t q = 0; q < 3 * plane; q++) d->U[q] = HALF * (d->U[q] + d->backup_U[q]);
     d->time = backup_time + dt_first_step;
     d->boundary_flux_evolve_integral = 0.5 * d->boundary_flux_evolve_integral;
@@ -985,7 +1047,7 @@ int ORACLE_FN(evolve_one_step)(oracle_domain *d, double dt, int has_dt)
     if (d->nsteps_advanced == 0) ORACLE_FN(update_max_quantities)(d);
     switch (d->method) {
     case OR_METHOD_RK2: one_rk2_step(d, dt, has_dt); break;
-    case OR_METHOD_EULER: one_euler_step(d, dt, has_dt); break;
+    case OR_METHOD_EULER: one_euler_step(d, dt, has_dt, 1); break;
     case OR_METHOD_LINEAR:
         if (!has_dt) return 2;
         linear_leapfrog_step(d, (REAL)dt);

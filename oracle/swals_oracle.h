@@ -106,7 +106,33 @@ typedef struct oracle_domain {
     double *explicit_source;      /* nx*ny*2 (UH, VH) */
     double *explicit_source_VH_j_minus_1; /* nx*(ny+1) */
     REAL *backup_U;     /* nx*ny*3 */
+    /* Nesting flux integrals (nested_grid_comms_mod.f90:2300-2469) of the
+     * boxes of this domain's send and recv comms.  Box b is (iL,iU,jL,jU),
+     * 1-based, at nest_boxes[4b..4b+3]; its integrals are the doubles at
+     * nest_integral + nest_offset[b], edge by edge (N, S, E, W) and within
+     * an edge variable by variable (STG..ELV), each of length iU-iL+1 (N, S)
+     * or jU-jL+1 (E, W). */
+    int32_t nest_nbox;
+    int32_t pad1;
+    const int32_t *nest_boxes;
+    const int64_t *nest_offset;
+    double *nest_integral;
 } oracle_domain;
+
+/* One side of a two_way_nesting_comms_type (nested_grid_comms_mod.f90:
+ * 120-255), as set up by initialise_two_way_nesting_comms (:257-658). */
+typedef struct oracle_nest_comm {
+    int32_t send_active, recv_active;
+    int32_t send_inds[6];        /* iL,iU,jL,jU,kL,kU */
+    int32_t recv_inds[6];
+    double cell_ratios[2];       /* my_dx / neighbour_dx */
+    int32_t my_domain_is_finer, equal_cell_ratios;
+    int32_t my_domain_staggered_grid, neighbour_domain_staggered_grid;
+    int32_t use_wetdry_limiting;
+    int32_t pad;
+    int64_t nsend, nsend_interior, send_flux_start, send_timeind;   /* 1-based indices */
+    int64_t nrecv, nrecv_interior, recv_flux_start, recv_timeind;
+} oracle_nest_comm;
 
 #ifdef __cplusplus
 extern "C" {
@@ -133,6 +159,21 @@ void ORACLE_FN(gauge_site_index)(const double *xy, int32_t n, const double *ll,
 double ORACLE_FN(pow_friction)(double x, int32_t chezy);
 double ORACLE_FN(cosh_cr)(double a);
 void ORACLE_FN(boundary_function)(const oracle_domain *d, double t, int32_t i, int32_t j, REAL *out4);
+
+/* Nesting (swals_nesting_oracle.c). */
+int  ORACLE_FN(nest_comm_init)(oracle_nest_comm *c, const double my_dx[2], const double neighbour_dx[2],
+                               const int32_t send_inds[6], const int32_t recv_inds[6], int32_t send_only,
+                               int32_t recv_only, int32_t use_wetdry_limiting, int32_t my_staggered,
+                               int32_t neighbour_staggered);
+void ORACLE_FN(nest_pack)(const oracle_nest_comm *c, const REAL *U, int32_t nx, int32_t ny,
+                          const double *send_integral, double time, int32_t has_time, REAL *send_buffer);
+void ORACLE_FN(nest_unpack)(const oracle_nest_comm *c, const REAL *recv_buffer, REAL *U, int32_t nx, int32_t ny,
+                            const double *recv_integral, double *recv_error, double *time_received);
+void ORACLE_FN(nest_recv_fixup)(oracle_domain *d, const int32_t recv_inds[4]);
+void ORACLE_FN(nest_flux_correction)(oracle_domain *d, int32_t ncomm, const int32_t *recv_boxes,
+                                     const int32_t *my_index, const int32_t *nbr_index, const double *recv_error,
+                                     const int64_t *error_offset, const int32_t *priority_index,
+                                     const double *all_dx, const int32_t *all_methods, double fraction_of);
 
 #ifdef __cplusplus
 }

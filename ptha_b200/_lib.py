@@ -37,7 +37,12 @@ EXPORTED = [
     "swals_gpu_batch_create", "swals_gpu_batch_destroy", "swals_gpu_batch_upload_U", "swals_gpu_batch_download_U",
     "swals_gpu_batch_download_max_stage", "swals_gpu_batch_device_state", "swals_gpu_batch_gauges_setup",
     "swals_gpu_batch_gauges_read", "swals_gpu_batch_evolve", "swals_gpu_batch_time", "swals_gpu_batch_tune",
-    "swals_gpu_batch_set_tile_config", "swals_gpu_adjoint_linear", "swals_gpu_misfit_gradient_linear", "swals_gpu_volume_interior_noalloc",
+    "swals_gpu_batch_set_tile_config", "swals_gpu_adjoint_linear", "swals_gpu_misfit_gradient_linear",
+    "swals_gpu_volume_interior_noalloc",
+    "swals_gpu_md_create", "swals_gpu_md_destroy", "swals_gpu_md_evolve_one_step", "swals_gpu_md_send_halos",
+    "swals_gpu_md_recv_halos", "swals_gpu_md_flux_correction", "swals_gpu_md_buffer_size",
+    "swals_gpu_md_download_buffer", "swals_gpu_md_download_flux", "swals_gpu_md_time", "swals_gpu_md_synchronize",
+    "swals_gpu_md_launch_count",
 ]
 TIMER_NAMES = ["cfl", "fv_stage1", "boundary1", "fv_stage2", "boundary2", "finalize", "leapfrog_edge",
                "leapfrog_step", "gauges", "max_stage"]
@@ -65,6 +70,11 @@ class DomainDesc(ctypes.Structure):
         ("has_host_boundary_subroutine", ctypes.c_int32), ("has_host_forcing_subroutine", ctypes.c_int32),
         ("device", ctypes.c_int32),
     ]
+
+
+class NestExchange(ctypes.Structure):
+    _fields_ = [("sender", ctypes.c_int32), ("receiver", ctypes.c_int32),
+                ("send_box", ctypes.c_int32 * 4), ("recv_box", ctypes.c_int32 * 4)]
 
 
 class DomainState(ctypes.Structure):
@@ -133,6 +143,14 @@ def lib():
         "swals_gpu_adjoint_linear": [vp, i32, dbl, vp, vp, vp],
         "swals_gpu_misfit_gradient_linear": [vp, i32, dbl, vp, i32, ctypes.POINTER(dbl), vp],
         "swals_gpu_volume_interior_noalloc": [vp, vp, vp, i32, i32, i64, i32, i32, vp, vp],
+        "swals_gpu_md_create": [vp, i32, vp, vp, vp, i32, vp, i32, i32, ctypes.POINTER(vp)],
+        "swals_gpu_md_destroy": [vp], "swals_gpu_md_evolve_one_step": [vp, dbl],
+        "swals_gpu_md_send_halos": [vp], "swals_gpu_md_recv_halos": [vp], "swals_gpu_md_flux_correction": [vp],
+        "swals_gpu_md_buffer_size": [vp, i32, ctypes.POINTER(i64)],
+        "swals_gpu_md_download_buffer": [vp, i32, vp, i64],
+        "swals_gpu_md_download_flux": [vp, i32, i32, vp, i64],
+        "swals_gpu_md_time": [vp, ctypes.POINTER(dbl)], "swals_gpu_md_synchronize": [vp],
+        "swals_gpu_md_launch_count": [vp, ctypes.POINTER(i64)],
     }
     for name, args in sig.items():
         f = getattr(L, name)

@@ -43,11 +43,6 @@ int cuda_fail(cudaError_t e, const char *what)
         if (_e != cudaSuccess) return cuda_fail(_e, #call);        \
     } while (0)
 
-// timestepping_metadata_mod.f90:135-232
-enum Method {
-    M_RK2 = 1, M_RK2N, M_MIDPOINT, M_EULER, M_LINEAR, M_LF_LIN_NLFRIC, M_CLIFFS, M_LF_NONLINEAR
-};
-
 int parse_method(const char *s, int *m, double *def_cfl, double *def_theta)
 {
     struct { const char *name; int m; double cfl; double theta; } tab[] = {

@@ -6,6 +6,11 @@
 #include "swals_kernels.h"
 #include "../../include/swals_gpu.h"
 
+// timestepping_method codes (timestepping_metadata_mod.f90:135-232).
+enum Method {
+    M_RK2 = 1, M_RK2N, M_MIDPOINT, M_EULER, M_LINEAR, M_LF_LIN_NLFRIC, M_CLIFFS, M_LF_NONLINEAR
+};
+
 // Mirrors the parts of SWALS's domain_type (domain_mod.f90:137-507) the time
 // step touches: geometry, solver options, device planes and scalar state.
 struct swals_domain {

@@ -1,0 +1,81 @@
+"""The nesting oracle against the reference's own nesting unit tests.
+
+* test_nested_grid_comms_mod (nested_grid_comms_mod.f90:2694-3056): for nest
+  ratios 1, 2, 3, 4, 5, 7, 101 -- cell ratios and fine/coarse roles, matching
+  send/receive buffer sizes, packed values inside [8, 32] (coarse) and
+  [8 - dx, 32 + dx] (fine, even ratios), exact preservation of a linear field
+  for odd ratios (relative 1e-14), and the time round trip.
+* test_multidomain_mod1's planar-field exchange (multidomain_mod.f90:
+  4089-4176): after send/recv every active cell of every domain holds the
+  plane of its priority domain, err^2 < spacing(1).
+"""
+import numpy as np
+import pytest
+
+from oracle.multidomain import OracleComm, OracleMultidomain
+from oracle.oracle import OracleDomain
+from ptha_b200 import nesting as nest
+
+from nest_cases import nested_comms_case, planar_values
+from test_nesting_metadata import four_domain_nest
+
+
+@pytest.mark.parametrize("r", [1, 2, 3, 4, 5, 7, 101])
+def test_nested_comms_known_answers(r):
+    c = nested_comms_case(r)
+    child = OracleComm(c["dx2"], c["dx1"], send_inds=list(c["child_send"]) + [1, 4],
+                       recv_inds=list(c["child_recv"]) + [1, 4], use_wetdry_limiting=False)
+    parent = OracleComm(c["dx1"], c["dx2"], send_inds=list(c["parent_send"]) + [1, 4],
+                        recv_inds=list(c["parent_recv"]) + [1, 4], use_wetdry_limiting=False)
+    assert np.allclose(child.c.cell_ratios[:], [1.0 / r] * 2, atol=1e-6)
+    assert np.allclose(parent.c.cell_ratios[:], [float(r)] * 2, atol=1e-6)
+    assert parent.c.nsend == child.c.nrecv
+    assert child.c.nsend == parent.c.nrecv
+    if r > 1:
+        assert not parent.c.my_domain_is_finer and child.c.my_domain_is_finer
+    U1, U2 = c["U1"].copy(), c["U2"].copy()
+    bp = parent.pack(U1).copy()
+    bc = child.pack(U2).copy()
+    err_tol = 1e-14
+    strd = 5
+    vals = bp[:parent.c.nsend_interior:strd]
+    assert vals.max() / 32.0 <= 1 + err_tol and vals.min() / 8.0 >= 1 - err_tol
+    off = c["dx2"][0] if r % 2 == 0 else 0.0
+    vals = bc[:child.c.nsend_interior]
+    assert vals.max() / (32.0 + off) <= 1 + err_tol and vals.min() / (8.0 - off) >= 1 - err_tol
+    parent.unpack(bc, U1)
+    child.unpack(bp, U2)
+    if r % 2 == 1:
+        for U, U0 in ((U1, c["U1"]), (U2, c["U2"])):
+            assert np.max(np.abs(U - U0) / U0) <= err_tol
+    # Time round trip
+    bp = parent.pack(U1, time=2.0).copy()
+    bc = child.pack(U2, time=3.0).copy()
+    assert parent.unpack(bc, U1) == 3.0
+    assert child.unpack(bp, U2) == 2.0
+
+
+def oracle_nest4():
+    specs = four_domain_nest()
+    ex = nest.setup_multidomain(specs, extra_halo_buffer=0, extra_cells_in_halo=0)
+    doms = [OracleDomain(s.nx[0], s.nx[1], s.lw, s.lower_left, timestepping_method=s.timestepping_method,
+                         boundary_exterior=tuple(not b for b in s.is_nesting_boundary)) for s in specs]
+    return specs, ex, doms
+
+
+def test_planar_field_exchange():
+    specs, ex, doms = oracle_nest4()
+    global_ll = specs[0].interior_bounding_box[0]
+    md = OracleMultidomain(doms, [s.timestepping_method for s in specs], [s.dx for s in specs], ex,
+                           use_wetdry_limiting=False, flux_correction=False)
+    for k, (s, d) in enumerate(zip(specs, doms)):
+        d.U[:] = planar_values(s, k + 1, global_ll)
+    for k in range(len(doms)):
+        md.send_halos(k)
+    md.recv_halos()
+    for k, (s, d) in enumerate(zip(specs, doms)):
+        active = nest._in_active_region(s.priority_domain_index, s.priority_domain_image, k + 1, 1,
+                                        s.nest_layer_width)
+        expect = planar_values(s, s.priority_domain_index.T.astype(np.float64), global_ll)
+        err = np.abs(d.U - expect)[:, active.T].max()
+        assert err * err <= np.spacing(1.0), (k, err)
