@@ -168,6 +168,7 @@ class OracleMultidomain:
                     self.recv[q].unpack(self.send[q].send_buffer, d.U)
             f = getattr(d.lib, d.pref + "nest_recv_fixup")
             f.restype = None
+            f.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
             for q, e in enumerate(self.exchanges):
                 if e.receiver == k:
                     f(ctypes.addressof(d.c), (ctypes.c_int32 * 4)(*e.recv_box))
