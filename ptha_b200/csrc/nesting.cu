@@ -699,7 +699,7 @@ int grid_for(int64_t items)
 struct HostCorr { int i, j; Corr c; };
 
 template <typename R>
-void build_corrections(const swals_multidomain *md, int dj, const int32_t *pind, std::vector<HostCorr> &out)
+int build_corrections(const swals_multidomain *md, int dj, const int32_t *pind, std::vector<HostCorr> &out)
 {
     const swals_domain *d = md->doms[dj];
     const int nx = d->nx, ny = d->ny;
@@ -755,6 +755,10 @@ void build_corrections(const swals_multidomain *md, int dj, const int32_t *pind,
                 }
                 if (!(out_index == myi))
                     if (dm != 0) sg = -sg;
+                const int lim = is_ew ? nx : ny;
+                if (p0 < 1 || p1 > lim)
+                    return fail(SWALS_ERR_INVALID_ARGUMENT,
+                                "domain %d: flux correction of receive box %zu reaches outside the domain", dj, x);
                 const int pp = is_ew ? P(p0, a) : P(a, p0);
                 if (myi != pp) sg = -sg;
                 R area_scale;
@@ -780,6 +784,7 @@ void build_corrections(const swals_multidomain *md, int dj, const int32_t *pind,
             }
         }
     }
+    return SWALS_OK;
 }
 
 static int integrals_scale(swals_multidomain *md, int k, double c)
@@ -971,8 +976,9 @@ int swals_gpu_md_create(swals_domain *const *domains, int32_t ndomains, const do
         pool_bytes += al((int64_t)sizeof(IBox) * std::max<size_t>(1, boxes[k].size()));
         if (md->flux_correction) {
             if (!priority_index[k]) return cleanup(fail(SWALS_ERR_INVALID_ARGUMENT, "priority index %d is NULL", k));
-            if (domains[k]->fp64) build_corrections<double>(md, k, priority_index[k], corr[k]);
-            else build_corrections<float>(md, k, priority_index[k], corr[k]);
+            const int rc = domains[k]->fp64 ? build_corrections<double>(md, k, priority_index[k], corr[k])
+                                            : build_corrections<float>(md, k, priority_index[k], corr[k]);
+            if (rc) return cleanup(rc);
             // Group by cell, keeping each cell's corrections in order.
             std::stable_sort(corr[k].begin(), corr[k].end(), [](const HostCorr &a, const HostCorr &b) {
                 return a.j != b.j ? a.j < b.j : a.i < b.i;

@@ -13,7 +13,10 @@
 //   - each cell's north-south edge, gradient and fix-ups are computed once
 //     (the tile kernel computes ~2.2 edges and ~2.3 gradients per cell) and
 //     there is no __syncthreads at all;
-//   - the next row's loads are issued before the current row is processed.
+//   - the next row's loads are issued before the current row is processed;
+//   - registers are capped for 4 CTAs (16 warps) per SM: the FP64 chains are
+//     latency-bound, and 16 warps beat 12 unspilled ones (measured 12% faster
+//     on the 2048x2048 beach, a few spilled values included).
 #include "rk2_common.cuh"
 
 namespace swals {
@@ -97,7 +100,7 @@ __device__ __forceinline__ void zero_edge(EdgeRes<R> &e)
 }
 
 template <typename R, int MODE, bool SPH, bool COR, int FRIC, int SH>
-__global__ void __launch_bounds__(SLANES *SWARPS) rk2_stream_kernel(const Rk2Args<R> a)
+__global__ void __launch_bounds__(SLANES *SWARPS, 4) rk2_stream_kernel(const Rk2Args<R> a)
 {
     const int lane = threadIdx.x & 31;
     const int wid = blockIdx.x * SWARPS + (threadIdx.x >> 5);

@@ -79,3 +79,43 @@ def test_planar_field_exchange():
         expect = planar_values(s, s.priority_domain_index.T.astype(np.float64), global_ll)
         err = np.abs(d.U - expect)[:, active.T].max()
         assert err * err <= np.spacing(1.0), (k, err)
+
+
+def _priority_volume(specs, doms):
+    """Water volume over each domain's priority cells."""
+    v = 0.0
+    for k, (s, d) in enumerate(zip(specs, doms)):
+        pr = (s.priority_domain_index.T == k + 1)
+        dep = d.U[0] - d.U[3]
+        v += float(np.sum((dep * d.area[:, None])[pr]))
+    return v
+
+
+@pytest.mark.parametrize("parent,child,nt,wetdry", [("linear", "rk2", 3, False), ("rk2", "rk2", 2, True)])
+def test_flux_correction_conserves_mass(parent, child, nt, wetdry):
+    """Flux correction makes the nested solution conserve mass to round-off
+    (the purpose of nesting_flux_correction_everywhere); without it the
+    coarse/fine flux mismatch leaks mass."""
+    from nest_cases import two_level_nest
+    from test_nesting_gpu import _ic
+    drift = {}
+    for fc in (False, True):
+        specs = two_level_nest(3, child, parent, nt)
+        ex = nest.setup_multidomain(specs)
+        doms = [OracleDomain(s.nx[0], s.nx[1], s.lw, s.lower_left, timestepping_method=s.timestepping_method,
+                             boundary_exterior=tuple(not b for b in s.is_nesting_boundary)) for s in specs]
+        md = OracleMultidomain(doms, [s.timestepping_method for s in specs], [s.dx for s in specs], ex,
+                               refinement=[s.timestepping_refinement_factor for s in specs],
+                               priority_index=[s.priority_domain_index for s in specs], flux_correction=fc)
+        for d, U in zip(doms, _ic(specs, wetdry)):
+            d.U[:] = U
+            d.manning_squared[:] = 0.025 ** 2
+        lim = [(d.linear_timestep_max() if s.timestepping_method == "linear" else d.nonlinear_stationary_timestep_max())
+               * s.timestepping_refinement_factor for s, d in zip(specs, doms)]
+        dt = 0.5 * min(lim)
+        v0 = _priority_volume(specs, doms)
+        for _ in range(10):
+            md.evolve_one_step(dt)
+        drift[fc] = abs(_priority_volume(specs, doms) - v0) / v0
+    assert drift[True] < 1e-13
+    assert drift[False] > 1e-8
