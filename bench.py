@@ -316,6 +316,300 @@ def run_ours(args, world, rank, local):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------------------
+# Secondary forms (`--workload linear|batched|adjoint`): one JSON line each,
+# for the evidence of the plain leapfrog roofline, the batched form against a
+# per-instance loop, and the adjoint's cost against a forward solve.
+
+def _event_ms(stream, fn):
+    import torch
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    fn()
+    b.record(stream)
+    b.synchronize()
+    return a.elapsed_time(b)
+
+
+def _dipoles(lon, lat, count, seed, band=((150.0, -40.0), (190.0, -10.0)), width_km=400.0):
+    """Compact dipole uplift patches in a band (uplift +/- A, extent L)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    LON, LAT = np.meshgrid(lon, lat)
+    (x0, y0), (x1, y1) = band
+    km_deg = 111.19
+    out = []
+    for _ in range(count):
+        t = rng.uniform(0.0, 1.0)
+        off = rng.uniform(-0.5, 0.5) * width_km / km_deg
+        cx = x0 + t * (x1 - x0) - off * (y1 - y0) / np.hypot(x1 - x0, y1 - y0)
+        cy = y0 + t * (y1 - y0) + off * (x1 - x0) / np.hypot(x1 - x0, y1 - y0)
+        L = rng.uniform(50.0, 200.0)
+        A = rng.uniform(0.5, 3.0)
+        ang = np.arctan2(y1 - y0, x1 - x0)
+        dx = (LON - cx) * km_deg * np.cos(np.deg2rad(cy))
+        dy = (LAT - cy) * km_deg
+        s_ = dx * np.cos(ang) + dy * np.sin(ang)
+        n_ = -dx * np.sin(ang) + dy * np.cos(ang)
+        sg = L / 6.0
+        eta = A * (np.exp(-((s_ - L / 4) ** 2 + n_ ** 2) / (2 * sg ** 2)) -
+                   np.exp(-((s_ + L / 4) ** 2 + n_ ** 2) / (2 * sg ** 2)))
+        out.append(eta)
+    return out
+
+
+def run_form(args, local):
+    import numpy as np
+    import torch
+    torch.cuda.set_device(local)
+    torch.zeros(1, device=f"cuda:{local}")
+    from ptha_b200 import Domain, workloads
+    peak, peak_kind = hbm_peak()
+    line = {"metric": METRIC, "unit": UNIT, "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
+            "vs_baseline": None}
+    if args.workload == "linear":
+        # The 400x400 Gaussian-basin configuration scaled up for the roofline
+        # sweep (dx 1 km, flat 4000 m, walls, CFL 0.7, FP64, max_stage on).
+        n = args.n if args.n != N else 8192
+        kw, U, gauges = workloads.linear_gaussian_basin(n=n)
+        d = Domain(**kw, device=local)
+        d.set_U(U)
+        dt = d.linear_timestep_max()
+        stream = torch.cuda.ExternalStream(d.stream(), device=f"cuda:{local}")
+        inner = max(1, args.inner if args.inner != INNER else 200)
+        for _ in range(args.warmup):
+            d.evolve_steps(inner, dt)
+        d.synchronize()
+        ms = _event_ms(stream, lambda: [d.evolve_steps(inner, dt) for _ in range(args.steps)])
+        value = n * n * inner * args.steps / (ms / 1e3)
+        d.timers_enable(True)
+        d.evolve_steps(50, dt)
+        tm = d.timers_read()
+        d.timers_enable(False)
+        t_ms, cnt = tm["leapfrog_step"]
+        achieved = n * n * 72.0 * cnt / (t_ms / 1e3) / 1e9
+        line.update({"workload": f"linear_gaussian_basin_{n}x{n}_fp64", "value": value, "steps": args.steps,
+                     "ms_per_step": ms / args.steps, "dtype": "f64",
+                     "config": {"workload": f"linear_gaussian_basin_{n}x{n}_fp64", "timesteps_per_step": inner,
+                                "dt": dt, "max_stage": True},
+                     "roofline": {"bound": "hbm", "kernel": "linear_step_kernel", "achieved": achieved,
+                                  "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                                  "bytes_per_cell": 72,
+                                  "per_launch_ms": {k: (v[0] / v[1] if v[1] else 0.0) for k, v in tm.items()}}})
+        d.close()
+    elif args.workload == "batched":
+        # Spherical 3600x2400 (1 arcmin) FP32, B dipole initial conditions,
+        # Coriolis on, fixed CFL-0.7 step: one batched launch per step
+        # against the same instances stepped one domain at a time.
+        from ptha_b200.batch import Batch
+        nxg, nyg = (3600, 2400) if args.n == N else (args.n * 3 // 2, args.n)
+        B = args.batch
+        dl = 1.0 / 60.0 * (3600 / nxg)
+        gkw, U0 = workloads.spherical_patch(nx=nxg, ny=nyg, dlon=dl, ll=(140.0, -45.0), seed=3)
+        grid = Domain(**gkw, timestepping_method="linear", real_bytes=4, device=local)
+        grid.set_U(U0)
+        dt = grid.linear_timestep_max()
+        lon = gkw["lower_left"][0] + (np.arange(nxg) + 0.5) * dl
+        lat = gkw["lower_left"][1] + (np.arange(nyg) + 0.5) * dl
+        wet = U0[3] < 0
+        b = Batch(grid, B)
+        etas = _dipoles(lon, lat, B, seed=4)
+        U3 = np.zeros((B, 3, nyg, nxg), np.float32)
+        for q, eta in enumerate(etas):
+            U3[q, 0] = np.where(wet, eta, 0.0)
+        b.set_U(U3)
+        del U3
+        cfg, _ = b.tune()
+        stream = torch.cuda.ExternalStream(grid.stream(), device=f"cuda:{local}")
+        inner = args.inner if args.inner != INNER else 50
+        b.evolve(inner, dt)
+        torch.cuda.synchronize()
+        ms_b = _event_ms(stream, lambda: [b.evolve(inner, dt) for _ in range(args.steps)])
+        v_batched = nxg * nyg * B * inner * args.steps / (ms_b / 1e3)
+        # Per-instance loop: each instance as its own domain step loop.
+        single = Domain(**gkw, timestepping_method="linear", real_bytes=4, device=local)
+        U = U0.astype(np.float32).copy()
+        U[0] = np.where(wet, etas[0], 0.0)
+        single.set_U(U)
+        single.evolve_steps(inner, dt)
+        single.synchronize()
+        s_stream = torch.cuda.ExternalStream(single.stream(), device=f"cuda:{local}")
+        ms_s = _event_ms(s_stream, lambda: [single.evolve_steps(inner, dt) for _ in range(args.steps)])
+        v_loop = nxg * nyg * inner * args.steps / (ms_s / 1e3)
+        bytes_cell = 32.0 + 4.0 / B
+        line.update({"workload": f"batched_linear_spherical_{nxg}x{nyg}_B{B}_fp32", "value": v_batched,
+                     "steps": args.steps, "ms_per_step": ms_b / args.steps, "dtype": "f32",
+                     "config": {"workload": f"batched_linear_spherical_{nxg}x{nyg}_B{B}_fp32", "batch": B,
+                                "timesteps_per_step": inner, "dt": dt, "coriolis": True, "tile_config": cfg},
+                     "per_instance_loop": {"value": v_loop, "ms_per_step_one_instance": ms_s / args.steps},
+                     "speedup_vs_loop": v_batched / v_loop,
+                     "roofline": {"bound": "hbm", "kernel": "linear_step_kernel (batched)",
+                                  "achieved": v_batched * bytes_cell / 1e9, "peak": peak, "unit": "GB/s",
+                                  "frac": v_batched * bytes_cell / 1e9 / peak, "peak_source": peak_kind,
+                                  "bytes_per_cell": bytes_cell}})
+        b.close()
+        single.close()
+        grid.close()
+    elif args.workload == "adjoint":
+        # Spherical 1200x800 (2 arcmin) FP64, 30 gauges, a hidden dipole's
+        # waveforms as the target, 2 h simulated, checkpoint every 50 steps.
+        nxg, nyg = (1200, 800) if args.n == N else (args.n * 3 // 2, args.n)
+        dl = 2.0 / 60.0 * (1200 / nxg)
+        gkw, U0 = workloads.spherical_patch(nx=nxg, ny=nyg, dlon=dl, ll=(150.0, -40.0), seed=6)
+        d = Domain(**gkw, timestepping_method="linear", device=local)
+        lon = gkw["lower_left"][0] + (np.arange(nxg) + 0.5) * dl
+        lat = gkw["lower_left"][1] + (np.arange(nyg) + 0.5) * dl
+        wet = U0[3] < 0
+        rng = np.random.default_rng(7)
+        wi = np.argwhere(wet)
+        pick = wi[rng.choice(len(wi), 30, replace=False)]
+        gauges = np.stack([lon[pick[:, 1]], lat[pick[:, 0]]], axis=1)
+        d.set_U(U0)
+        dt = d.linear_timestep_max()
+        nsteps = int(round(2 * 3600.0 / dt))
+        eta_t = _dipoles(lon, lat, 1, seed=8, band=((lon[0] + 5, lat[0] + 5), (lon[-1] - 5, lat[-1] - 5)))[0]
+        Ut = U0.copy()
+        Ut[0] = np.where(wet, eta_t, 0.0)
+        d.set_U(Ut)
+        d.gauges_setup(gauges, capacity=nsteps + 8)
+        stream = torch.cuda.ExternalStream(d.stream(), device=f"cuda:{local}")
+        d.evolve_steps(nsteps, dt)
+        target = d.gauges_read()[:nsteps, :, 0].copy()
+        Ui = U0.copy()
+        Ui[0] = 0.0
+        times_f, times_a = [], []
+        for _ in range(max(1, args.steps)):
+            d.set_U(Ui)
+            d.gauges_reset()
+            d.time = 0.0
+            d.synchronize()
+            times_f.append(_event_ms(stream, lambda: d.evolve_steps(nsteps, dt)))
+            d.set_U(Ui)
+            d.time = 0.0
+            d.synchronize()
+            t0 = time.perf_counter()
+            loss, grad = d.misfit_gradient(nsteps, dt, target, checkpoint_every=50)
+            times_a.append((time.perf_counter() - t0) * 1e3)
+        f_ms, a_ms = min(times_f), min(times_a)
+        line.update({"workload": f"adjoint_linear_spherical_{nxg}x{nyg}_fp64", "value": nxg * nyg * nsteps /
+                     (a_ms / 1e3), "steps": args.steps, "ms_per_step": a_ms, "dtype": "f64",
+                     "config": {"workload": f"adjoint_linear_spherical_{nxg}x{nyg}_fp64", "nsteps": nsteps,
+                                "dt": dt, "gauges": 30, "checkpoint_every": 50},
+                     "forward_ms": f_ms, "gradient_ms": a_ms, "gradient_over_forward": a_ms / f_ms,
+                     "loss": loss, "grad_norm": float(np.linalg.norm(grad[0]))})
+        d.close()
+    elif args.workload == "multidomain":
+        line.update(_run_multidomain(args, local, peak, peak_kind))
+    print(json.dumps(line), flush=True)
+
+
+def _coast_elevation(lon, lat, coasts):
+    """Deep ocean (-4000 m) shoaling over a 60 km shelf slope to -50 m, then a
+    1/40 coastal ramp to +10 m, for each straight coastline (lon0, lat0,
+    bearing of the seaward normal, (lon_min, lon_max, lat_min, lat_max) of
+    the region it shapes)."""
+    import numpy as np
+    km = 111.19
+    elv = np.full(np.broadcast(lon, lat).shape, -4000.0)
+    for (x0, y0, ang, box) in coasts:
+        inside = (lon >= box[0]) & (lon <= box[1]) & (lat >= box[2]) & (lat <= box[3])
+        # seaward distance (km) from the coastline
+        d = ((lon - x0) * np.cos(np.deg2rad(y0)) * np.cos(ang) + (lat - y0) * np.sin(ang)) * km
+        ramp = np.clip(-50.0 - (d * 1000.0) / 40.0, -50.0, 10.0)           # within ~2.4 km of the coast
+        shelf = np.clip(-50.0 - (d - 0.0) * (3950.0 / 60.0), -4000.0, -50.0)  # 60 km shelf slope
+        e = np.where(d <= 0.0, ramp, shelf)
+        elv = np.where(inside, np.maximum(elv, e), elv)
+    return elv
+
+
+def _run_multidomain(args, local, peak, peak_kind):
+    """Nested multidomain in the shape of the 5-domain configuration: a
+    coarse 'linear' FP32 band (4 arcmin, 5400x1800, 60S-60N), one ratio-3
+    'rk2' FP64 domain (900x900) and two ratio-9 'rk2' FP64 wet/dry domains
+    (1197x801 and 702x1098, the nearest sizes that are whole parent cells)
+    on synthetic coastal ramps; one dipole source; fixed md step from the
+    coarse domain's CFL, refinement factors from each domain's stationary
+    CFL; graph-captured md steps."""
+    import math
+    import numpy as np
+    import torch
+    from ptha_b200 import Multidomain, NestDomain
+    c = 1.0 / 15.0                     # coarse cell (degrees)
+    f3, f9 = c / 3.0, c / 9.0
+    specs = [
+        NestDomain((0.0, -60.0), (5400 * c, 1800 * c), (5400, 1800), "linear", 1),
+        NestDomain((140.0, -40.0), (900 * f3, 900 * f3), (900, 900), "rk2", 1),
+        NestDomain((141.0 + 2 * c, -39.0), (1197 * f9, 801 * f9), (1197, 801), "rk2", 1),
+        NestDomain((152.0, -35.0), (702 * f9, 1098 * f9), (702, 1098), "rk2", 1),
+    ]
+    coasts = [(141.0 + 2 * c + 1197 * f9 * 0.75, -39.0 + 801 * f9 * 0.5, 0.0,
+               (140.5, 151.0, -39.5, -32.5)),
+              (152.0 + 702 * f9 * 0.5, -35.0 + 1098 * f9 * 0.8, math.pi / 2,
+               (151.5, 157.7, -35.5, -26.3))]
+    # Refinement factors from the stationary CFL limits need the domains;
+    # set them up once with nt = 1, read the limits, then build the real nest.
+    kw = [dict(real_bytes=4, spherical=True), dict(spherical=True), dict(spherical=True), dict(spherical=True)]
+
+    def build(nts):
+        sp = [NestDomain(s.lower_left, s.lw, s.nx, s.timestepping_method, nt) for s, nt in zip(specs, nts)]
+        md = Multidomain(sp, domain_kwargs=kw, use_wetdry_limiting=True, flux_correction=True, device=local)
+        for k, (s, d) in enumerate(zip(sp, md.domains)):
+            lon, lat = s.x(), s.y()
+            LON, LAT = np.meshgrid(lon, lat)
+            elv = _coast_elevation(LON, LAT, coasts)
+            if k == 0:
+                elv[:2, :] = 100.0
+                elv[-2:, :] = 100.0
+                elv[:, :2] = 100.0
+                elv[:, -2:] = 100.0
+            eta = _dipoles(lon, lat, 1, seed=11, band=((144.0, -37.0), (150.0, -30.0)))[0]
+            U = np.zeros((4, s.nx[1], s.nx[0]))
+            U[3] = elv
+            U[0] = np.where(elv < 0, eta, elv)
+            d.set_U(U)
+            if d.timestepping_method == "rk2":
+                d.set_manning_squared(0.025 ** 2)
+        return sp, md
+
+    sp, md = build([1, 1, 1, 1])
+    dt = md.domains[0].linear_timestep_max()
+    lims = [d.stationary_timestep_max() if d.timestepping_method == "rk2" else dt for d in md.domains]
+    nts = [max(1, int(math.ceil(dt / l))) for l in lims]
+    md.close()
+    sp, md = build(nts)
+    cells = sum(s.nx[0] * s.nx[1] * nt for s, nt in zip(sp, nts))
+    stream = torch.cuda.ExternalStream(md.domains[0].stream(), device=f"cuda:{local}")
+    K = 3
+    for _ in range(args.warmup):
+        md.evolve_one_step(dt)
+    md.synchronize()
+    ms_plain = _event_ms(stream, lambda: [md.evolve_one_step(dt) for _ in range(K * 4)]) / (K * 4)
+    md.capture_graph(K, dt)
+    md.replay(1)
+    md.synchronize()
+    reps = max(1, args.inner if args.inner != INNER else 100)
+    l0 = md.launch_count()
+    ms = _event_ms(stream, lambda: md.replay(reps))
+    ms_step = ms / (reps * K)
+    value = cells / (ms_step / 1e3)
+    vols = [d.volume_interior() for d in md.domains]
+    out = {"workload": "nested_multidomain_4dom", "value": value, "steps": reps * K, "ms_per_step": ms_step,
+           "dtype": "f32 coarse / f64 fine",
+           "config": {"workload": "nested_multidomain_4dom",
+                      "domains": [{"nx": list(s.nx), "method": s.timestepping_method, "nt": nt,
+                                   "nest_layer_width": s.nest_layer_width} for s, nt in zip(sp, nts)],
+                      "md_dt": dt, "exchanges": len(md.exchanges), "flux_correction": True,
+                      "graph_steps": K, "sources": 1, "periodic": False},
+           "cell_updates_per_md_step": cells,
+           "ms_per_md_step_without_graph": ms_plain,
+           "graph_replay_speedup": ms_plain / ms_step,
+           "gpu_launches_per_md_step_graph": 1.0 / K,
+           "finite": bool(all(np.isfinite(v) for v in vols))}
+    md.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -327,12 +621,19 @@ def main():
     ap.add_argument("--inner", type=int, default=INNER, help="timesteps per bench step (default 2000)")
     ap.add_argument("--real32", action="store_true", help="FP32 state (-DREALFLOAT analogue)")
     ap.add_argument("--profile", action="store_true", help="short untimed run for ncu")
+    ap.add_argument("--workload", default="rk2", choices=["rk2", "linear", "batched", "adjoint", "multidomain"],
+                    help="rk2 (default, the headline) or a secondary form")
+    ap.add_argument("--batch", type=int, default=256, help="instances for --workload batched")
     args = ap.parse_args()
     if args.warmup < 3 and not args.profile:
         args.warmup = 3
     world, rank, local = dist_setup(args.gpus)
     if args.impl == "reference":
         run_reference(args, world, rank)
+        return
+    if args.workload != "rk2":
+        if rank == 0:
+            run_form(args, local)
         return
     run_ours(args, world, rank, local)
 

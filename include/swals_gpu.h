@@ -304,6 +304,12 @@ int swals_gpu_md_download_buffer(swals_multidomain *md, int32_t exchange, double
  * 2 receive-box flux error; laid out edge by edge (N, S, E, W), then
  * variable by variable (STG..ELV). */
 int swals_gpu_md_download_flux(swals_multidomain *md, int32_t exchange, int32_t which, double *out, int64_t n);
+/* Capture nsteps md steps of a fixed dt into a CUDA graph (nsteps must bring
+ * every domain back to its state buffer: a multiple of 3 always does), and
+ * replay it: every domain, sub-step and exchange of nsteps md steps in one
+ * graph launch.  The host time and step counts advance on replay. */
+int swals_gpu_md_capture_graph(swals_multidomain *md, int32_t nsteps, double dt);
+int swals_gpu_md_replay(swals_multidomain *md, int32_t nreplays);
 int swals_gpu_md_time(swals_multidomain *md, double *time);
 int swals_gpu_md_synchronize(swals_multidomain *md);
 int swals_gpu_md_launch_count(swals_multidomain *md, int64_t *n);

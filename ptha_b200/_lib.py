@@ -42,7 +42,7 @@ EXPORTED = [
     "swals_gpu_md_create", "swals_gpu_md_destroy", "swals_gpu_md_evolve_one_step", "swals_gpu_md_send_halos",
     "swals_gpu_md_recv_halos", "swals_gpu_md_flux_correction", "swals_gpu_md_buffer_size",
     "swals_gpu_md_download_buffer", "swals_gpu_md_download_flux", "swals_gpu_md_time", "swals_gpu_md_synchronize",
-    "swals_gpu_md_launch_count",
+    "swals_gpu_md_launch_count", "swals_gpu_md_capture_graph", "swals_gpu_md_replay",
 ]
 TIMER_NAMES = ["cfl", "fv_stage1", "boundary1", "fv_stage2", "boundary2", "finalize", "leapfrog_edge",
                "leapfrog_step", "gauges", "max_stage"]
@@ -151,6 +151,7 @@ def lib():
         "swals_gpu_md_download_flux": [vp, i32, i32, vp, i64],
         "swals_gpu_md_time": [vp, ctypes.POINTER(dbl)], "swals_gpu_md_synchronize": [vp],
         "swals_gpu_md_launch_count": [vp, ctypes.POINTER(i64)],
+        "swals_gpu_md_capture_graph": [vp, i32, dbl], "swals_gpu_md_replay": [vp, i32],
     }
     for name, args in sig.items():
         f = getattr(L, name)

@@ -439,7 +439,13 @@ __global__ void correction_kernel(DomPtr d, const int *cells, const int64_t *sta
 // ---------------------------------------------------------------------------
 // Nesting flux integrals.
 
-__global__ void set_time_kernel(DevScalars *sc, double t) { sc->time = t; }
+// Multidomain time on the device, so that a captured graph of md steps
+// replays correctly: t[1] = t[0] + dt at the start of a step (tend,
+// multidomain_mod.f90:1108), each domain's time = tend after its sub-steps
+// (:1152), t[0] = tend at the end.
+__global__ void md_time_begin_kernel(double *t, double dt) { t[1] = t[0] + dt; }
+__global__ void md_time_set_kernel(DevScalars *sc, const double *t) { sc->time = t[1]; }
+__global__ void md_time_end_kernel(double *t) { t[0] = t[1]; }
 
 __global__ void scale_kernel(double *x, int64_t n, double c)
 {
@@ -641,8 +647,13 @@ struct swals_multidomain {
     };
     std::vector<PerDom> per;
     bool flux_correction = true;
-    double time = 0.0;
+    double time = 0.0;       // host copy (advanced as steps are issued)
+    double *d_time = nullptr; // device copy: [0] md time, [1] tend of the step in flight
     int64_t launches = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    int graph_steps = 0;
+    double graph_dt = 0.0;
 };
 
 namespace {
@@ -962,7 +973,7 @@ int swals_gpu_md_create(swals_domain *const *domains, int32_t ndomains, const do
     std::vector<std::vector<HostCorr>> corr(ndomains);
     int64_t pool_bytes = 0;
     auto al = [](int64_t b) { return (b + 255) / 256 * 256; };
-    pool_bytes += al((int64_t)sizeof(Ex) * std::max<int64_t>(1, nex));
+    pool_bytes += al((int64_t)sizeof(Ex) * std::max<int64_t>(1, nex)) + al(2 * sizeof(double));
     pool_bytes += al(8 * std::max<int64_t>(1, md->n_buf)) + al(8 * std::max<int64_t>(1, md->n_int)) +
                   al(8 * std::max<int64_t>(1, md->n_err));
     for (int k = 0; k < ndomains; k++) {
@@ -999,6 +1010,7 @@ int swals_gpu_md_create(swals_domain *const *domains, int32_t ndomains, const do
     if (ce != cudaSuccess) return cleanup(fail(SWALS_ERR_OUT_OF_MEMORY, "multidomain pool of %lld bytes", (long long)pool_bytes));
     char *p = (char *)md->pool;
     md->d_ex = (Ex *)p; p += al((int64_t)sizeof(Ex) * std::max<int64_t>(1, nex));
+    md->d_time = (double *)p; p += al(2 * sizeof(double));
     md->d_buf = (double *)p; p += al(8 * std::max<int64_t>(1, md->n_buf));
     md->d_int = (double *)p; p += al(8 * std::max<int64_t>(1, md->n_int));
     md->d_err = (double *)p; p += al(8 * std::max<int64_t>(1, md->n_err));
@@ -1049,6 +1061,9 @@ int swals_gpu_md_create(swals_domain *const *domains, int32_t ndomains, const do
     swals_domain_state st;
     swals_gpu_get_state(domains[0], &st);
     md->time = st.time;
+    const double t2[2] = {st.time, st.time};
+    if ((ce = cudaMemcpy(md->d_time, t2, sizeof(t2), cudaMemcpyHostToDevice)) != cudaSuccess)
+        return cleanup(api_cuda_fail(ce, "upload time"));
     *out = md;
     return SWALS_OK;
 }
@@ -1057,6 +1072,8 @@ int swals_gpu_md_destroy(swals_multidomain *md)
 {
     if (!md) return SWALS_OK;
     cudaStreamSynchronize(md->stream);
+    if (md->graph_exec) cudaGraphExecDestroy(md->graph_exec);
+    if (md->graph) cudaGraphDestroy(md->graph);
     for (size_t k = 0; k < md->doms.size(); k++) md->doms[k]->stream = md->own_streams[k];
     if (md->pool) cudaFree(md->pool);
     delete md;
@@ -1119,6 +1136,8 @@ int swals_gpu_md_evolve_one_step(swals_multidomain *md, double dt)
     if (!(dt > 0.0)) return fail(SWALS_ERR_INVALID_ARGUMENT, "dt must be > 0");
     MDCK(cudaSetDevice(md->device));
     const double tend = md->time + dt;
+    md_time_begin_kernel<<<1, 1, 0, md->stream>>>(md->d_time, dt);
+    md->launches++;
     for (size_t k = 0; k < md->doms.size(); k++) {
         swals_domain *d = md->doms[k];
         int rc = integrals_scale(md, (int)k, 0.0);
@@ -1137,7 +1156,7 @@ int swals_gpu_md_evolve_one_step(swals_multidomain *md, double dt)
             if (rc) return rc;
         }
         // domains(j)%time = tend (multidomain_mod.f90:1152)
-        set_time_kernel<<<1, 1, 0, md->stream>>>(d->sc, tend);
+        md_time_set_kernel<<<1, 1, 0, md->stream>>>(d->sc, md->d_time);
         md->launches++;
         MDCK(cudaGetLastError());
     }
@@ -1147,7 +1166,72 @@ int swals_gpu_md_evolve_one_step(swals_multidomain *md, double dt)
     if (rc) return rc;
     rc = swals_gpu_md_flux_correction(md);
     if (rc) return rc;
+    md_time_end_kernel<<<1, 1, 0, md->stream>>>(md->d_time);
+    md->launches++;
+    MDCK(cudaGetLastError());
     md->time = tend;
+    return SWALS_OK;
+}
+
+int swals_gpu_md_capture_graph(swals_multidomain *md, int32_t nsteps, double dt)
+{
+    if (!md || nsteps < 1 || !(dt > 0.0)) return fail(SWALS_ERR_INVALID_ARGUMENT, "bad argument");
+    MDCK(cudaSetDevice(md->device));
+    // Every domain must come back to the same state buffer after the
+    // captured steps, so that the graph can be replayed as often as wanted.
+    std::vector<int> cur0;
+    for (swals_domain *d : md->doms) cur0.push_back(d->cur);
+    if (md->graph_exec) { cudaGraphExecDestroy(md->graph_exec); md->graph_exec = nullptr; }
+    if (md->graph) { cudaGraphDestroy(md->graph); md->graph = nullptr; }
+    MDCK(cudaStreamSynchronize(md->stream));
+    const double time0 = md->time;
+    const int64_t l0 = md->launches;
+    std::vector<int64_t> dl0;
+    for (swals_domain *d : md->doms) dl0.push_back(d->launches);
+    std::vector<int64_t> ns0;
+    for (swals_domain *d : md->doms) ns0.push_back(d->nsteps);
+    MDCK(cudaStreamBeginCapture(md->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = SWALS_OK;
+    for (int s = 0; s < nsteps && rc == SWALS_OK; s++) rc = swals_gpu_md_evolve_one_step(md, dt);
+    cudaGraph_t g = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(md->stream, &g);
+    // Capture records work without running it: restore the host bookkeeping.
+    md->time = time0;
+    md->launches = l0;
+    bool same = true;
+    for (size_t k = 0; k < md->doms.size(); k++) {
+        same &= (md->doms[k]->cur == cur0[k]);
+        md->doms[k]->cur = cur0[k];
+        md->doms[k]->launches = dl0[k];
+        md->doms[k]->nsteps = ns0[k];
+    }
+    if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+    if (ce != cudaSuccess) { if (g) cudaGraphDestroy(g); return api_cuda_fail(ce, "cudaStreamEndCapture"); }
+    if (!same) {
+        cudaGraphDestroy(g);
+        return fail(SWALS_ERR_INVALID_ARGUMENT,
+                    "%d md steps do not return every domain to its state buffer; capture a multiple of 3 steps",
+                    nsteps);
+    }
+    ce = cudaGraphInstantiate(&md->graph_exec, g, 0);
+    if (ce != cudaSuccess) { cudaGraphDestroy(g); return api_cuda_fail(ce, "cudaGraphInstantiate"); }
+    md->graph = g;
+    md->graph_steps = nsteps;
+    md->graph_dt = dt;
+    return SWALS_OK;
+}
+
+int swals_gpu_md_replay(swals_multidomain *md, int32_t nreplays)
+{
+    if (!md || nreplays < 0) return fail(SWALS_ERR_INVALID_ARGUMENT, "bad argument");
+    if (!md->graph_exec) return fail(SWALS_ERR_INVALID_ARGUMENT, "no captured graph");
+    MDCK(cudaSetDevice(md->device));
+    for (int r = 0; r < nreplays; r++) {
+        MDCK(cudaGraphLaunch(md->graph_exec, md->stream));
+        md->launches++;
+        md->time += md->graph_steps * md->graph_dt;
+        for (swals_domain *d : md->doms) d->nsteps += (int64_t)md->graph_steps;
+    }
     return SWALS_OK;
 }
 

@@ -67,6 +67,9 @@ __device__ __forceinline__ Cell<R> fix_up(const Raw<R> &x, bool valid, long long
     return c;
 }
 
+// Bring a line into L2 ahead of its use (no register is written).
+__device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 template <typename R> __device__ __forceinline__ R up1(R v) { return __shfl_up_sync(FULL, v, 1); }
 template <typename R> __device__ __forceinline__ R dn1(R v) { return __shfl_down_sync(FULL, v, 1); }
 
@@ -134,6 +137,18 @@ __global__ void __launch_bounds__(SLANES *SWARPS, 4) rk2_stream_kernel(const Rk2
     for (int r = ra - 2, k = 0; r <= rb + 1; r++, k++) {
         const Raw<R> cur = nxt;
         if (r + 1 <= rb + 1) nxt = load_raw<R>(a, i, r + 1);
+        // Inputs that only the update reads (friction coefficient, stage-2
+        // U0 and max_stage): start them towards L2 three rows early.
+        if (MODE != MODE_CFL && out_lane && r + 1 >= ra && r + 1 < rb) {
+            const int64_t o = (int64_t)(r + 1) * a.P + i;
+            if (FRIC != FRIC_NONE) prefetch_l2(a.nsq + o);
+            if (MODE == MODE_STAGE2) {
+                prefetch_l2(a.stg0 + o);
+                prefetch_l2(a.uh0 + o);
+                prefetch_l2(a.vh0 + o);
+                if (a.max_stage) prefetch_l2(a.max_stage + o);
+            }
+        }
         c2 = c1;
         c1 = c0;
         c0 = fix_up<R>(cur, col_valid && r >= 0 && r < ny, negfix, out_lane && r >= ra && r < rb);

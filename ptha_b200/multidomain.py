@@ -127,6 +127,13 @@ class Multidomain:
     def synchronize(self):
         check(self._L.swals_gpu_md_synchronize(self._md))
 
+    def capture_graph(self, nsteps: int, dt: float):
+        """Capture nsteps fixed-dt md steps (a multiple of 3) as one CUDA graph."""
+        check(self._L.swals_gpu_md_capture_graph(self._md, int(nsteps), float(dt)))
+
+    def replay(self, nreplays: int = 1):
+        check(self._L.swals_gpu_md_replay(self._md, int(nreplays)))
+
     def buffer(self, exchange: int) -> np.ndarray:
         n = ctypes.c_int64()
         check(self._L.swals_gpu_md_buffer_size(self._md, exchange, ctypes.byref(n)))

@@ -163,3 +163,30 @@ def test_rk2_wetdry_nest_steps():
     specs = two_level_nest(ratio=3, child_method="rk2", parent_method="rk2", child_nt=2)
     md, omd = _run_pair(specs, wetdry=True, nsteps=6)
     md.close()
+
+
+def test_md_graph_replay_matches_steps():
+    """Three md steps captured as one CUDA graph and replayed twice equal six
+    md steps issued one by one, bit for bit, including the domain times."""
+    res = []
+    for mode in ("steps", "graph"):
+        specs = two_level_nest(ratio=3, child_method="rk2", parent_method="linear")
+        md = Multidomain(specs, use_wetdry_limiting=True, flux_correction=True)
+        for d, U in zip(md.domains, _ic(specs, False)):
+            d.set_U(U)
+            if d.timestepping_method == "rk2":
+                d.set_manning_squared(0.025 ** 2)
+        dt = 10.0
+        if mode == "steps":
+            for _ in range(6):
+                md.evolve_one_step(dt)
+        else:
+            md.capture_graph(3, dt)
+            md.replay(2)
+        md.synchronize()
+        res.append(([d.get_U() for d in md.domains], [d.time for d in md.domains], md.time))
+        md.close()
+    for a, b in zip(res[0][0], res[1][0]):
+        np.testing.assert_array_equal(a, b)
+    assert res[0][1] == res[1][1]
+    assert res[0][2] == res[1][2] == pytest.approx(60.0)
