@@ -333,28 +333,37 @@ def _event_ms(stream, fn):
 
 
 def _dipoles(lon, lat, count, seed, band=((150.0, -40.0), (190.0, -10.0)), width_km=400.0):
-    """Compact dipole uplift patches in a band (uplift +/- A, extent L)."""
+    """Compact dipole uplift patches in a band: a random centre within
+    width_km of the band's axis, extent L in U[50, 200] km, amplitude A in
+    U[0.5, 3] m, eta = A [G(s - L/4, n) - G(s + L/4, n)] with Gaussians of
+    sigma L/6 in band-aligned coordinates; evaluated within 3L of the centre
+    (zero beyond)."""
     import numpy as np
     rng = np.random.default_rng(seed)
-    LON, LAT = np.meshgrid(lon, lat)
     (x0, y0), (x1, y1) = band
     km_deg = 111.19
+    ang = np.arctan2(y1 - y0, x1 - x0)
     out = []
     for _ in range(count):
         t = rng.uniform(0.0, 1.0)
         off = rng.uniform(-0.5, 0.5) * width_km / km_deg
-        cx = x0 + t * (x1 - x0) - off * (y1 - y0) / np.hypot(x1 - x0, y1 - y0)
-        cy = y0 + t * (y1 - y0) + off * (x1 - x0) / np.hypot(x1 - x0, y1 - y0)
+        cx = x0 + t * (x1 - x0) - off * np.sin(ang)
+        cy = y0 + t * (y1 - y0) + off * np.cos(ang)
         L = rng.uniform(50.0, 200.0)
         A = rng.uniform(0.5, 3.0)
-        ang = np.arctan2(y1 - y0, x1 - x0)
-        dx = (LON - cx) * km_deg * np.cos(np.deg2rad(cy))
-        dy = (LAT - cy) * km_deg
-        s_ = dx * np.cos(ang) + dy * np.sin(ang)
-        n_ = -dx * np.sin(ang) + dy * np.cos(ang)
-        sg = L / 6.0
-        eta = A * (np.exp(-((s_ - L / 4) ** 2 + n_ ** 2) / (2 * sg ** 2)) -
-                   np.exp(-((s_ + L / 4) ** 2 + n_ ** 2) / (2 * sg ** 2)))
+        eta = np.zeros((len(lat), len(lon)))
+        r_deg = 3.0 * L / km_deg
+        ii = np.flatnonzero(np.abs(lon - cx) <= r_deg / max(np.cos(np.deg2rad(cy)), 0.2))
+        jj = np.flatnonzero(np.abs(lat - cy) <= r_deg)
+        if len(ii) and len(jj):
+            LON, LAT = np.meshgrid(lon[ii], lat[jj])
+            dx = (LON - cx) * km_deg * np.cos(np.deg2rad(cy))
+            dy = (LAT - cy) * km_deg
+            s_ = dx * np.cos(ang) + dy * np.sin(ang)
+            n_ = -dx * np.sin(ang) + dy * np.cos(ang)
+            sg = L / 6.0
+            eta[np.ix_(jj, ii)] = A * (np.exp(-((s_ - L / 4) ** 2 + n_ ** 2) / (2 * sg ** 2)) -
+                                       np.exp(-((s_ + L / 4) ** 2 + n_ ** 2) / (2 * sg ** 2)))
         out.append(eta)
     return out
 
@@ -414,12 +423,19 @@ def run_form(args, local):
         lat = gkw["lower_left"][1] + (np.arange(nyg) + 0.5) * dl
         wet = U0[3] < 0
         b = Batch(grid, B)
-        etas = _dipoles(lon, lat, B, seed=4)
-        U3 = np.zeros((B, 3, nyg, nxg), np.float32)
-        for q, eta in enumerate(etas):
-            U3[q, 0] = np.where(wet, eta, 0.0)
-        b.set_U(U3)
-        del U3
+        chunk = 8
+        first_eta = None
+        rng_seeds = np.random.default_rng(4).integers(0, 2 ** 31, size=B)
+        for q0 in range(0, B, chunk):
+            cnt = min(chunk, B - q0)
+            U3 = np.zeros((cnt, 3, nyg, nxg), np.float32)
+            for t in range(cnt):
+                eta = _dipoles(lon, lat, 1, seed=int(rng_seeds[q0 + t]))[0]
+                U3[t, 0] = np.where(wet, eta, 0.0)
+                if first_eta is None:
+                    first_eta = U3[t, 0].copy()
+            b.set_U(U3, first=q0)
+            del U3
         cfg, _ = b.tune()
         stream = torch.cuda.ExternalStream(grid.stream(), device=f"cuda:{local}")
         inner = args.inner if args.inner != INNER else 50
@@ -430,7 +446,7 @@ def run_form(args, local):
         # Per-instance loop: each instance as its own domain step loop.
         single = Domain(**gkw, timestepping_method="linear", real_bytes=4, device=local)
         U = U0.astype(np.float32).copy()
-        U[0] = np.where(wet, etas[0], 0.0)
+        U[0] = first_eta
         single.set_U(U)
         single.evolve_steps(inner, dt)
         single.synchronize()
