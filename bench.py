@@ -294,11 +294,14 @@ def run_ours(args, world, rank, local):
                        "l2": "inputs larger than L2 (state 4x32 MB + manning 32 MB + max_stage 32 MB + "
                              "stage copies; ~0.7 GB streamed per timestep)",
                        "parallelism": f"replicas x{world}", "gauges": 9},
-            "roofline": {"bound": "hbm", "kernel": "rk2_stage_kernel (FV stage 1 + stage 2)",
+            "roofline": {"bound": "hbm", "kernel": "rk2_stream_kernel (FV stage 1 + stage 2)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": peak_kind,
                          "bytes_per_cell": {"stage1": BYTES_STAGE1, "stage2": BYTES_STAGE2},
-                         "traffic": profile_traffic("rk2_stage_kernel"),
+                         "algorithmic_bytes_per_launch_pair": cells * BYTES_PER_CELL_UPDATE * es_scale,
+                         "traffic": (profile_traffic("rk2_stream_kernel_pair") if N == 2048 and not args.real32
+                                     else None),
+                         "traffic_unit": "DRAM bytes of one stage-1 + one stage-2 launch (ncu, 2048x2048 FP64)",
                          "step_effective_GBps": cells * BYTES_PER_CELL_UPDATE * es_scale /
                                                 (ms_max / args.steps / INNER / 1e3) / 1e9,
                          "per_launch_ms": per_step_ms},
