@@ -19,6 +19,10 @@
 // function to the stage/elevation ring at time+dt/2 (boundary_mod.f90:78-163
 // staggered branch), forms the boundary flux sums (:126-205) and advances
 // domain%time.
+#include <algorithm>
+#include <cstdlib>
+#include <cstring>
+
 #include "swals_kernels.h"
 
 namespace swals {
@@ -200,6 +204,155 @@ __global__ void __launch_bounds__(LBX *TYT) linear_step_kernel(const LinArgs<R> 
     }
 }
 
+// Streaming form of the same step, for HBM-bound grids: a warp owns a strip
+// of 30 columns (lanes 1..30; lanes 0 and 31 carry the west and east
+// neighbour columns, clamped at the domain edge like the tile's halo) and
+// marches down SH rows.  Per row it loads STG, UH, VH and ELV once (the next
+// row's loads are in flight while the current row is computed), forms the
+// new stage of the next row and the momentum of the current row from
+// registers and shuffles, and writes the row: no shared memory, no block
+// barriers, and the three row-constant divisions are done once per row per
+// warp.  Every value is the same expression, in the same order, as in
+// linear_step_kernel.
+constexpr int SOUT = 30;
+
+template <typename R, bool CORIOLIS, bool TRUELY_LINEAR>
+__global__ void __launch_bounds__(128) linear_stream_kernel(const LinArgs<R> a, int SH, int nstrips, int total)
+{
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int b = blockIdx.x;  // instance: consecutive CTAs share ELV rows in L2
+    if (b >= a.nbatch) return;
+    const int nx = a.p.nx, ny = a.p.ny;
+    const int64_t P = a.p.pitch;
+    const int64_t io = (int64_t)b * a.inst_stride;
+    const R *stg = a.p.stg + io, *uhp = a.p.uh + io, *vhp = a.p.vh + io;
+    R *stg_o = a.p.stg_o + io, *uh_o = a.p.uh_o + io, *vh_o = a.p.vh_o + io;
+    R *max_stage = a.p.max_stage ? a.p.max_stage + (int64_t)b * a.max_stride : nullptr;
+    const R *elv = a.p.elv;
+    const R g = K<R>::gravity();
+    const R half = K<R>::half();
+    const R one = K<R>::one();
+    const R zero = K<R>::zero();
+    const R mad = K<R>::min_depth();
+
+    for (int w = blockIdx.y * 4 + (threadIdx.x >> 5); w < total; w += gridDim.y * 4) {
+        const int sx = w % nstrips, sy = w / nstrips;
+        const int ra = sy * SH;
+        const int rb = min(ra + SH, ny);
+        const int i = sx * SOUT - 1 + lane;
+        const int ic = clampi(i, 0, nx - 1);
+        const bool in_x = (i >= 0 && i < nx);
+        const bool out = (lane >= 1 && lane <= SOUT && i < nx);
+        const R dyl_i = a.m.dyl[ic];
+        const R dyl_ip1 = a.m.dyl[min(ic + 1, nx)];
+
+        // New stage of cell (i, r) from its row's loads (domain_mod_linear_solver_include.f90:92-115).
+        auto stage_new = [&](int r, R s_old, R uh_r, R uh_w, R vh_r, R vh_s) -> R {
+            R sn = R(0);
+            if (r < ny && in_x) {
+                const bool interior = (i >= a.xl + 1) && (i <= a.xu - 1) && (r >= a.yl + 1) && (r <= a.yu - 1);
+                if (interior) {
+                    const R inv_cell_area_dt = a.dt / a.m.area[r];
+                    const R t1 = (uh_r - uh_w) * dyl_i;
+                    const R t2 = vh_r * a.m.dxb[r + 1] - vh_s * a.m.dxb[r];
+                    sn = s_old - inv_cell_area_dt * (t1 + t2);
+                } else if (a.bc_stage && on_bc_ring(i, r, nx, ny, a.bext)) {
+                    sn = stg_o[(int64_t)r * P + i];
+                } else {
+                    sn = s_old;
+                }
+            }
+            return sn;
+        };
+        auto ld = [&](const R *p, int r) -> R { return p[(int64_t)clampi(r, 0, ny - 1) * P + ic]; };
+
+        // Prologue: VH of row ra-1, row ra, then row ra+1 in flight.
+        R vh_jm1 = ld(vhp, ra - 1);
+        R uh_j = ld(uhp, ra), vh_j = ld(vhp, ra), e_j = ld(elv, ra);
+        R st_j = (ra < ny && in_x) ? stg[(int64_t)ra * P + i] : R(0);
+        R sn_j;
+        {
+            const R uh_w = __shfl_up_sync(FULL, uh_j, 1);
+            sn_j = stage_new(ra, st_j, uh_j, uh_w, vh_j, vh_jm1);
+        }
+        R uh_n = ld(uhp, ra + 1), vh_n = ld(vhp, ra + 1), e_n = ld(elv, ra + 1);
+        R st_n = (ra + 1 < ny && in_x) ? stg[(int64_t)(ra + 1) * P + i] : R(0);
+
+        for (int j = ra; j < rb; j++) {
+            // Loads of row j+2 go out first.
+            const R uh_f = ld(uhp, j + 2), vh_f = ld(vhp, j + 2), e_f = ld(elv, j + 2);
+            const R st_f = (j + 2 < ny && in_x) ? stg[(int64_t)(j + 2) * P + i] : R(0);
+            R mx = R(0);
+            const bool in_ms = max_stage && out && i >= a.xl && i <= a.xu && j >= a.yl && j <= a.yu;
+            if (in_ms) mx = max_stage[(int64_t)j * P + i];
+
+            // New stage of row j+1.
+            const R uh_nw = __shfl_up_sync(FULL, uh_n, 1);
+            const R sn_n = stage_new(j + 1, st_n, uh_n, uh_nw, vh_n, vh_j);
+
+            // Momentum of row j (:225-567).
+            const R s_e = __shfl_down_sync(FULL, sn_j, 1);
+            const R e_e = __shfl_down_sync(FULL, e_j, 1);
+            const R uh_w = __shfl_up_sync(FULL, uh_j, 1);
+            const R vh_e = __shfl_down_sync(FULL, vh_j, 1);
+            const R vh_se = __shfl_down_sync(FULL, vh_jm1, 1);
+            if (out) {
+                const int64_t o = (int64_t)j * P + i;
+                stg_o[o] = sn_j;
+                if (in_ms) max_stage[o] = (sn_j > mx) ? sn_j : mx;
+                R uh = uh_j, vh = vh_j;
+                if (i >= a.xl && i <= a.xu - 1 && j >= a.yl && j <= a.yu - 1) {
+                    const R inv_cell_area_dt_g = g * a.dt / a.m.area[j];
+                    const R inv_cell_area_dt_vh_g = g * a.dt / (half * (a.m.area[j] + a.m.area[j + 1]));
+                    const R e0 = e_j;
+                    const R sn = sn_j, s_n = sn_n;
+                    R h_iph, h_jph, wet_iph, wet_jph;
+                    if (TRUELY_LINEAR) {
+                        const bool wi = (e0 < -mad + a.msl) && (e_e < -mad + a.msl);
+                        h_iph = wi ? (a.msl - half * (e_e + e0)) : zero;
+                        const bool wj = (e_n < -mad + a.msl) && (e0 < -mad + a.msl);
+                        h_jph = wj ? (a.msl - half * (e_n + e0)) : zero;
+                        wet_iph = one;
+                        wet_jph = one;
+                    } else {
+                        const bool wi = (sn - e0 > mad) && (s_e - e_e > mad);
+                        h_iph = wi ? (half * ((s_e + sn) - (e_e + e0))) : zero;
+                        const bool wj = (s_n - e_n > mad) && (sn - e0 > mad);
+                        h_jph = wj ? (half * ((s_n + sn) - (e_n + e0))) : zero;
+                        wet_iph = (h_iph > zero) ? one : zero;
+                        wet_jph = (h_jph > zero) ? one : zero;
+                    }
+                    const R dw_j = s_n - sn;
+                    R uh_new = uh * wet_iph - inv_cell_area_dt_g * h_iph * (s_e - sn) * dyl_ip1;
+                    R vh_new = vh * wet_jph - inv_cell_area_dt_vh_g * h_jph * dw_j * a.m.dxb[j + 1];
+                    if (CORIOLIS) {
+                        const R vh_iph_jmh = half * (vh_jm1 + vh_se);
+                        const R vh_iph_jph = half * (vh_j + vh_e);
+                        const R uh_i_j = half * (uh_j + uh_w);
+                        const R uh_i_jp1 = half * (uh_n + uh_nw);
+                        const R dt_half_coriolis = a.dt * a.m.cor[j] * half * ((h_iph > zero) ? one : zero);
+                        const R dt_half_coriolis_jph = a.dt * a.m.cor_be[j + 1] * half * ((h_jph > zero) ? one : zero);
+                        uh_new = uh_new + dt_half_coriolis * (vh_iph_jmh + vh_iph_jph);
+                        vh_new = vh_new - dt_half_coriolis_jph * (uh_i_j + uh_i_jp1);
+                    }
+                    if (a.lin_fric) {
+                        uh_new = a.lin_fric_mult * uh_new;
+                        vh_new = a.lin_fric_mult * vh_new;
+                    }
+                    uh = uh_new;
+                    vh = vh_new;
+                }
+                uh_o[o] = uh;
+                vh_o[o] = vh;
+            }
+            vh_jm1 = vh_j;
+            uh_j = uh_n; vh_j = vh_n; e_j = e_n; sn_j = sn_n;
+            uh_n = uh_f; vh_n = vh_f; e_n = e_f; st_n = st_f;
+        }
+    }
+}
+
 // One block: boundary stage/elevation at time+dt/2, boundary flux sums,
 // time bookkeeping (:117-205, :571).
 template <typename R>
@@ -328,9 +481,38 @@ template cudaError_t launch_batch_gauges<float>(int64_t, const float *, int64_t,
 
 // Tile configurations (rows per tile, thread rows, instances per CTA); the
 // batched form's autotuner times each on the real problem.
+// Configurations 0-4: shared-memory tiles (rows per CTA, thread rows,
+// instances per CTA); 5-7: streaming warps with 32, 64 or 128 rows per
+// segment; 8: streaming with the segment height chosen from the grid size.
+// Plain domains use STREAM_DEFAULT.
 struct TileCfg { int by, tyt, ib; };
 constexpr TileCfg kTileCfgs[] = {{16, 8, 1}, {16, 8, 2}, {16, 8, 4}, {32, 8, 2}, {8, 8, 4}};
-constexpr int kNumTileCfgs = sizeof(kTileCfgs) / sizeof(kTileCfgs[0]);
+constexpr int kStreamSH[] = {32, 64, 128, 0};
+constexpr int kNumTileCfgs = sizeof(kTileCfgs) / sizeof(kTileCfgs[0]) + sizeof(kStreamSH) / sizeof(kStreamSH[0]);
+constexpr int STREAM_DEFAULT = 8;
+
+// Rows per segment: the longest segment (up to 128 rows, which amortises the
+// two rows a segment reloads) that still gives every SM about 24 warps.
+inline int stream_rows(int nx, int ny, int nbatch)
+{
+    const int64_t nstrips = (nx + SOUT - 1) / SOUT;
+    const int64_t want = 148 * 24;
+    int sh = 128;
+    while (sh > 8 && (int64_t)nbatch * nstrips * ((ny + sh - 1) / sh) < want) sh /= 2;
+    return sh;
+}
+
+template <typename R, bool COR, bool TL>
+void launch_stream(const LinArgs<R> &a, int sh, cudaStream_t s)
+{
+    if (sh <= 0) sh = stream_rows(a.p.nx, a.p.ny, a.nbatch);
+    const int nstrips = (a.p.nx + SOUT - 1) / SOUT;
+    const int nseg = (a.p.ny + sh - 1) / sh;
+    const int total = nstrips * nseg;
+    const int gy = std::min((total + 3) / 4, 65535);
+    dim3 grid(a.nbatch, gy);
+    linear_stream_kernel<R, COR, TL><<<grid, 128, 0, s>>>(a, sh, nstrips, total);
+}
 
 template <typename R, bool COR, bool TL, int BY, int TYT, int IB>
 void launch_cfg(const LinArgs<R> &a, cudaStream_t s)
@@ -343,6 +525,11 @@ void launch_cfg(const LinArgs<R> &a, cudaStream_t s)
 template <typename R, bool COR, bool TL>
 void launch_tile(const LinArgs<R> &a, int cfg, cudaStream_t s)
 {
+    const int ntile = (int)(sizeof(kTileCfgs) / sizeof(kTileCfgs[0]));
+    if (cfg >= ntile) {
+        launch_stream<R, COR, TL>(a, kStreamSH[cfg - ntile], s);
+        return;
+    }
     switch (cfg) {
     case 1: launch_cfg<R, COR, TL, 16, 8, 2>(a, s); break;
     case 2: launch_cfg<R, COR, TL, 16, 8, 4>(a, s); break;
@@ -360,6 +547,18 @@ void launch_main(const LinArgs<R> &a, const StepConfig &c, int cfg, cudaStream_t
     else if (cor && !tl) launch_tile<R, true, false>(a, cfg, s);
     else if (!cor && tl) launch_tile<R, false, true>(a, cfg, s);
     else launch_tile<R, false, false>(a, cfg, s);
+}
+
+// Kernel of a plain (unbatched) step: the streaming form unless
+// SWALS_LINEAR_KERNEL=tile selects the shared-memory tile.
+int linear_kernel_config()
+{
+    static int cfg = -1;
+    if (cfg < 0) {
+        const char *e = getenv("SWALS_LINEAR_KERNEL");
+        cfg = (e && strcmp(e, "tile") == 0) ? 0 : STREAM_DEFAULT;
+    }
+    return cfg;
 }
 
 template <typename R>
@@ -391,7 +590,7 @@ cudaError_t launch_linear_step(const StepPlanes<R> &p, const Metrics<R> &m, cons
     linear_edge_kernel<R><<<1, 512, 0, s>>>(a, sc, c.exterior_cells_width, c.bf);
     hook(CAT_LINEAR_EDGE, 1);
     hook(CAT_LINEAR_MAIN, 0);
-    launch_main<R>(a, c, 0, s);
+    launch_main<R>(a, c, linear_kernel_config(), s);
     hook(CAT_LINEAR_MAIN, 1);
     return cudaGetLastError();
 }
