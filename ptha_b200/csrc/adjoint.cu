@@ -18,6 +18,8 @@
 // of the oracle's forward model and by the oracle forward as tangent linear.
 #include "domain_internal.h"
 
+#include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -161,6 +163,133 @@ __global__ void __launch_bounds__(ABX *ATY) linear_adjoint_kernel(const AdjArgs<
     }
 }
 
+// Streaming form of the same transpose (the forward's register-row design):
+// a warp owns 30 columns (lanes 1..30; lanes 0 and 31 carry the neighbour
+// columns) and marches down SH rows.  Rows r+2 and r+3 are in flight while
+// row r is produced: row r+1's face coefficients and total stage adjoint are
+// formed from rows r+1 and r+2, then row r's outputs from rows r-1..r+1.
+// Values outside the domain are zero, as in the tile kernel, and every
+// expression keeps the tile kernel's order.  With `resid` set, the gauge
+// adjoint of this step (lambda_STG(site) += resid[g], gauges in order) is
+// added where lambda_STG is loaded, so no separate injection launch is needed.
+constexpr int AOUT = 30;
+
+template <typename R>
+struct ARow { R ls, lu, lv, e, ee; };  // ee: ELV one column east
+
+template <typename R>
+struct ACoef { R aU, aV, cU, cV; };
+
+template <typename R, bool COR>
+__global__ void __launch_bounds__(128) linear_adjoint_stream_kernel(const AdjArgs<R> a, int SH, int nstrips, int total,
+                                                                    const int *sites, int ng, const double *resid)
+{
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int nx = a.nx, ny = a.ny;
+    const int64_t P = a.P;
+    const R g = swals::K<R>::gravity(), half = R(0.5), mad = swals::K<R>::min_depth(), zero = R(0), one = R(1);
+
+    for (int w = blockIdx.x * 4 + (threadIdx.x >> 5); w < total; w += gridDim.x * 4) {
+        const int sx = w % nstrips, sy = w / nstrips;
+        const int ra = sy * SH, rb = min(ra + SH, ny);
+        const int i = sx * AOUT - 1 + lane;
+        const bool in_x = (i >= 0 && i < nx);
+        const bool out = (lane >= 1 && lane <= AOUT && i < nx);
+
+        auto load = [&](int r) -> ARow<R> {
+            ARow<R> v;
+            v.ls = v.lu = v.lv = v.e = v.ee = zero;
+            if (in_x && r >= 0 && r < ny) {
+                const int64_t o = (int64_t)r * P + i;
+                v.ls = a.ls[o]; v.lu = a.lu[o]; v.lv = a.lv[o]; v.e = a.elv[o];
+                if (i + 1 < nx) v.ee = a.elv[o + 1];
+                if (resid)
+                    for (int q = 0; q < ng; q++)
+                        if (sites[2 * q] == i && sites[2 * q + 1] == r) v.ls = v.ls + R(resid[q]);
+            }
+            return v;
+        };
+        // Face coefficients of row r from its ELV and the ELV of row r+1 (zero outside IM).
+        auto coef = [&](int r, R e0, R e_e, R e_n) -> ACoef<R> {
+            ACoef<R> c;
+            c.aU = c.aV = c.cU = c.cV = zero;
+            if (in_x && r >= 0 && r < ny && in_im(i, r, a.xl, a.xu, a.yl, a.yu)) {
+                const bool wi = (e0 < -mad + a.msl) && (e_e < -mad + a.msl);
+                const R hU = wi ? (a.msl - half * (e_e + e0)) : zero;
+                const bool wj = (e_n < -mad + a.msl) && (e0 < -mad + a.msl);
+                const R hV = wj ? (a.msl - half * (e_n + e0)) : zero;
+                const R gU = g * a.dt / a.m.area[r];
+                const R gV = g * a.dt / (half * (a.m.area[r] + a.m.area[r + 1]));
+                c.aU = a.mult * (gU * hU * a.m.dyl[i + 1]);
+                c.aV = a.mult * (gV * hV * a.m.dxb[r + 1]);
+                if (COR) {
+                    c.cU = a.mult * (a.dt * a.m.cor[r] * half * ((hU > zero) ? one : zero)) * half;
+                    c.cV = a.mult * (a.dt * a.m.cor_be[r + 1] * half * ((hV > zero) ? one : zero)) * half;
+                }
+            }
+            return c;
+        };
+        // Total stage adjoint of row r from rows r (value, coefficients) and r-1.
+        auto lst_of = [&](const ARow<R> &v, const ACoef<R> &c, R aV_s, R lv_s) -> R {
+            const R pw = __shfl_up_sync(FULL, c.aU * v.lu, 1);
+            return v.ls + c.aU * v.lu + c.aV * v.lv - pw - aV_s * lv_s;
+        };
+
+        // Prologue: rows ra-1 .. ra+2 loaded, coefficients of rows ra-1 and ra,
+        // total stage adjoint of row ra.
+        ARow<R> vm = load(ra - 1), v0 = load(ra), v1 = load(ra + 1), v2 = load(ra + 2);
+        ACoef<R> cm = coef(ra - 1, vm.e, vm.ee, v0.e);
+        ACoef<R> c0 = coef(ra, v0.e, v0.ee, v1.e);
+        R lst0 = lst_of(v0, c0, cm.aV, vm.lv);
+
+        for (int r = ra; r < rb; r++) {
+            const ARow<R> v3 = load(r + 3);
+            const ACoef<R> c1 = coef(r + 1, v1.e, v1.ee, v2.e);
+            const R lst1 = lst_of(v1, c1, c0.aV, v0.lv);
+
+            const R lst_e = __shfl_down_sync(FULL, lst0, 1);
+            const R cvlv_e0 = __shfl_down_sync(FULL, c0.cV * v0.lv, 1);   // (cV*1)*lV at (i+1, r)
+            const R cvlv_em = __shfl_down_sync(FULL, cm.cV * vm.lv, 1);   // at (i+1, r-1)
+            const R culu_w0 = __shfl_up_sync(FULL, c0.cU * v0.lu, 1);     // at (i-1, r)
+            const R culu_w1 = __shfl_up_sync(FULL, c1.cU * v1.lu, 1);     // at (i-1, r+1)
+            if (out) {
+                const R idm = in_im(i, r, a.xl, a.xu, a.yl, a.yu) ? a.mult : one;
+                R lU = idm * v0.lu;
+                R lV = idm * v0.lv;
+                if (COR) {
+                    // U'(i',r') and V'(i',r') terms in the tile kernel's order;
+                    // (c * cnt) * l with cnt in {1, 2} equals cnt * (c * l).
+                    const R cnt_i = R(1) + R((i == 0) ? 1 : 0);
+                    lU = lU - c0.cV * cnt_i * v0.lv;
+                    lU = lU - cvlv_e0;
+                    lU = lU - cm.cV * cnt_i * vm.lv;
+                    lU = lU - cvlv_em;
+                    const R cnt_r = R(1) + R((r == 0) ? 1 : 0);
+                    lV = lV + cnt_r * culu_w0;
+                    lV = lV + c0.cU * cnt_r * v0.lu;
+                    lV = lV + culu_w1;
+                    lV = lV + c1.cU * R(1) * v1.lu;
+                }
+                const R c_r = a.dt / a.m.area[r];
+                if (in_is(i, r, a.xl, a.xu, a.yl, a.yu)) {
+                    lU = lU - c_r * a.m.dyl[i] * lst0;
+                    lV = lV - c_r * a.m.dxb[r + 1] * lst0;
+                }
+                if (in_is(i + 1, r, a.xl, a.xu, a.yl, a.yu)) lU = lU + c_r * a.m.dyl[i + 1] * lst_e;
+                if (in_is(i, r + 1, a.xl, a.xu, a.yl, a.yu)) lV = lV + (a.dt / a.m.area[r + 1]) * a.m.dxb[r + 1] * lst1;
+                const int64_t o = (int64_t)r * P + i;
+                a.ls_o[o] = lst0;
+                a.lu_o[o] = lU;
+                a.lv_o[o] = lV;
+            }
+            vm = v0; v0 = v1; v1 = v2; v2 = v3;
+            cm = c0; c0 = c1;
+            lst0 = lst1;
+        }
+    }
+}
+
 // lambda_STG(site) += weight * gauge adjoint, one thread (sites may repeat).
 template <typename R>
 __global__ void inject_kernel(R *ls, int64_t P, const int *site_ij, int n, const double *gadj)
@@ -172,32 +301,22 @@ __global__ void inject_kernel(R *ls, int64_t P, const int *site_ij, int n, const
     }
 }
 
-// Residual of the recorded gauge stage against a target: out[g] = y[g] - d[g].
-__global__ void residual_kernel(const double *records3, const double *target, int n, double *out, double *loss)
+// Kernel choice: streaming unless SWALS_ADJOINT_KERNEL=tile.
+bool adjoint_tile()
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    double acc = 0.0;
-    for (int g = 0; g < n; g++) {
-        const double rsd = records3[3 * g] - target[g];
-        out[g] = rsd;
-        acc += rsd * rsd;
+    static int t = -1;
+    if (t < 0) {
+        const char *e = getenv("SWALS_ADJOINT_KERNEL");
+        t = (e && strcmp(e, "tile") == 0) ? 1 : 0;
     }
-    *loss += 0.5 * acc;
+    return t == 1;
 }
 
+// One adjoint step lambda_out = M^T (lambda_in + C^T resid): with `resid`
+// (n gauges at `sites`) the injection is fused into the streaming kernel.
 template <typename R>
-struct Work {
-    swals_domain *d;
-    int64_t plane;
-    R *lam[2][3];
-    R *x[2][3];
-    swals::DevScalars *sc;
-    int *sites;
-    double *records, *gadj, *loss;
-};
-
-template <typename R>
-cudaError_t adjoint_step(swals_domain *d, R *const in[3], R *const out[3], double dt)
+cudaError_t adjoint_step(swals_domain *d, R *const in[3], R *const out[3], double dt, const int *sites = nullptr,
+                         int ng = 0, const double *resid = nullptr)
 {
     AdjArgs<R> a;
     a.nx = d->nx; a.ny = d->ny; a.P = d->pitch;
@@ -210,27 +329,48 @@ cudaError_t adjoint_step(swals_domain *d, R *const in[3], R *const out[3], doubl
     a.msl = R(d->cfg.msl_linear);
     const R lfc = R(d->cfg.linear_friction_coeff);
     a.mult = (lfc != R(0)) ? (R(1) / (R(1) + a.dt * lfc)) : R(1);
-    dim3 block(ABX, ATY), grid((d->nx + ABX - 1) / ABX, (d->ny + ABY - 1) / ABY);
     swals::LaunchHook hook = swals::hook_of(d);
+    if (adjoint_tile()) {
+        if (resid && ng > 0) {
+            inject_kernel<R><<<1, 32, 0, d->stream>>>(const_cast<R *>(in[0]), d->pitch, sites, ng, resid);
+            d->launches++;
+        }
+        dim3 block(ABX, ATY), grid((d->nx + ABX - 1) / ABX, (d->ny + ABY - 1) / ABY);
+        hook(swals::CAT_LINEAR_MAIN, 0);
+        if (d->cfg.coriolis) linear_adjoint_kernel<R, true><<<grid, block, 0, d->stream>>>(a);
+        else linear_adjoint_kernel<R, false><<<grid, block, 0, d->stream>>>(a);
+        hook(swals::CAT_LINEAR_MAIN, 1);
+        return cudaGetLastError();
+    }
+    // Rows per segment: up to 128, while every SM still gets about 24 warps.
+    const int nstrips = (d->nx + AOUT - 1) / AOUT;
+    int sh = 128;
+    while (sh > 8 && (int64_t)nstrips * ((d->ny + sh - 1) / sh) < 148 * 24) sh /= 2;
+    const int total = nstrips * ((d->ny + sh - 1) / sh);
+    const int gx = std::min((total + 3) / 4, 1 << 20);
     hook(swals::CAT_LINEAR_MAIN, 0);
-    if (d->cfg.coriolis) linear_adjoint_kernel<R, true><<<grid, block, 0, d->stream>>>(a);
-    else linear_adjoint_kernel<R, false><<<grid, block, 0, d->stream>>>(a);
+    if (d->cfg.coriolis)
+        linear_adjoint_stream_kernel<R, true><<<gx, 128, 0, d->stream>>>(a, sh, nstrips, total, sites, ng, resid);
+    else
+        linear_adjoint_stream_kernel<R, false><<<gx, 128, 0, d->stream>>>(a, sh, nstrips, total, sites, ng, resid);
     hook(swals::CAT_LINEAR_MAIN, 1);
     return cudaGetLastError();
 }
 
-template <typename R>
-cudaError_t forward_step(swals_domain *d, R *const in[3], R *const out[3], double dt, swals::DevScalars *sc)
+// The domain's adjoint scratch, grown to at least `need` bytes.
+cudaError_t workspace(swals_domain *d, size_t need, void **out)
 {
-    swals::StepPlanes<R> p;
-    p.nx = d->nx; p.ny = d->ny; p.pitch = d->pitch;
-    p.stg = in[0]; p.uh = in[1]; p.vh = in[2];
-    p.stg_o = out[0]; p.uh_o = out[1]; p.vh_o = out[2];
-    p.elv = (R *)d->elv;
-    p.max_stage = nullptr;
-    p.manning_sq = nullptr;
-    return swals::launch_linear_step<R>(p, swals::metrics_of<R>(d), d->cfg, R(dt), sc, d->stream,
-                                        swals::hook_of(d));
+    if (d->ws_bytes < need) {
+        cudaStreamSynchronize(d->stream);
+        if (d->ws) cudaFree(d->ws);
+        d->ws = nullptr;
+        d->ws_bytes = 0;
+        cudaError_t e = cudaMalloc(&d->ws, need);
+        if (e != cudaSuccess) return e;
+        d->ws_bytes = need;
+    }
+    *out = d->ws;
+    return cudaSuccess;
 }
 
 int check_adjoint_domain(swals_domain *d)
@@ -274,7 +414,7 @@ int adjoint_sweep(swals_domain *d, int nsteps, double dt, const double *gadj_hos
     const int ng = d->n_gauges > 0 ? d->n_gauges : (int)(d->h_sites.size() / 2);
     void *buf = nullptr;
     const size_t need = 6 * plane * es + sizeof(double) * (size_t)nsteps * (ng > 0 ? ng : 1) + 2 * sizeof(int) * (ng + 1);
-    cudaError_t e = cudaMalloc(&buf, need);
+    cudaError_t e = workspace(d, need, &buf);
     if (e != cudaSuccess) return swals::api_cuda_fail(e, "adjoint workspace");
     R *lam[2][3];
     for (int b = 0; b < 2; b++)
@@ -295,11 +435,9 @@ int adjoint_sweep(swals_domain *d, int nsteps, double dt, const double *gadj_hos
         rc = copy_plane3(d, dst, (void *)lambda_seed_host, true);
     }
     for (int n = nsteps; n >= 1 && rc == SWALS_OK; n--) {
-        if (ng > 0 && gadj_host) {
-            inject_kernel<R><<<1, 32, 0, d->stream>>>(lam[cur][0], d->pitch, d_sites, ng, d_g + (size_t)(n - 1) * ng);
-            d->launches++;
-        }
-        e = adjoint_step<R>(d, lam[cur], lam[1 - cur], dt);
+        const bool inj = ng > 0 && gadj_host;
+        e = adjoint_step<R>(d, lam[cur], lam[1 - cur], dt, inj ? d_sites : nullptr, inj ? ng : 0,
+                            inj ? d_g + (size_t)(n - 1) * ng : nullptr);
         if (e != cudaSuccess) rc = swals::api_cuda_fail(e, "adjoint step");
         cur = 1 - cur;
     }
@@ -308,14 +446,59 @@ int adjoint_sweep(swals_domain *d, int nsteps, double dt, const double *gadj_hos
         rc = copy_plane3(d, src, grad_host, false);
     }
     cudaStreamSynchronize(d->stream);
-    cudaFree(buf);
     return rc;
 }
 
-// Misfit gradient with checkpointing: forward from the domain's current
-// state keeping a copy every K steps (and nothing else), then for each
-// segment from the last: recompute its forward steps from the checkpoint to
-// get the gauge residuals, and run the adjoint back through it.
+// One interior update x' = M x of the forward (no boundary routine, bookkeeping
+// or max_stage, which the misfit does not involve), optionally recording the
+// new stage at the gauges into rec.
+template <typename R>
+cudaError_t map_step(swals_domain *d, R *const in[3], R *const out[3], double dt, const int *sites, int ng,
+                     double *rec)
+{
+    swals::StepPlanes<R> p;
+    p.nx = d->nx; p.ny = d->ny; p.pitch = d->pitch;
+    p.stg = in[0]; p.uh = in[1]; p.vh = in[2];
+    p.stg_o = out[0]; p.uh_o = out[1]; p.vh_o = out[2];
+    p.elv = (R *)d->elv;
+    p.max_stage = nullptr;
+    p.manning_sq = nullptr;
+    return swals::launch_linear_map<R>(p, swals::metrics_of<R>(d), d->cfg, R(dt), sites, ng, rec, d->stream,
+                                       swals::hook_of(d));
+}
+
+// Residuals of `count` recorded steps against the target, and each step's
+// half squared misfit (the loss is summed over steps in forward order at
+// the end, so it does not depend on the checkpoint spacing).
+__global__ void segment_residual_kernel(const double *rec, const double *target, int count, int ng, double *resid,
+                                        double *step_half)
+{
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        for (int q = 0; q < ng; q++) {
+            const double rsd = rec[(size_t)t * ng + q] - target[(size_t)t * ng + q];
+            resid[(size_t)t * ng + q] = rsd;
+            acc += rsd * rsd;
+        }
+        step_half[t] = 0.5 * acc;
+    }
+}
+
+__global__ void loss_sum_kernel(const double *step_half, int n, double *loss)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double l = 0.0;
+    for (int k = 0; k < n; k++) l += step_half[k];
+    *loss = l;
+}
+
+// Misfit gradient with checkpointing: a forward sweep from the domain's
+// current state keeps a copy of the state every K steps (and nothing else);
+// then, for each segment from the last, the segment's forward steps are
+// recomputed from its checkpoint, recording the gauge stage, the segment's
+// residuals are formed, and the adjoint runs back through the segment with
+// the residuals injected as it goes.  Per timestep that is one forward map,
+// one recomputed forward map and one adjoint launch.
 template <typename R>
 int misfit_gradient(swals_domain *d, int nsteps, double dt, const double *target_host, int K, double *loss_out,
                     void *grad_host)
@@ -326,10 +509,10 @@ int misfit_gradient(swals_domain *d, int nsteps, double dt, const double *target
     const size_t es = sizeof(R);
     const int nseg = (nsteps + K - 1) / K;
     size_t need = (size_t)(6 + 6 + 3 * nseg) * plane * es;          // lambda x2, state x2, checkpoints
-    need += sizeof(double) * ((size_t)nsteps * ng + (size_t)K * ng * 3 + (size_t)ng + 8);
-    need += sizeof(int) * 2 * (size_t)ng + sizeof(swals::DevScalars) + 1024;
+    need += sizeof(double) * ((size_t)nsteps * ng + 2 * (size_t)K * ng + (size_t)nsteps + 8);
+    need += sizeof(int) * 2 * (size_t)ng + 1024;
     void *buf = nullptr;
-    cudaError_t e = cudaMalloc(&buf, need);
+    cudaError_t e = workspace(d, need, &buf);
     if (e != cudaSuccess) return swals::api_cuda_fail(e, "misfit-gradient workspace");
     char *p = (char *)buf;
     R *lam[2][3], *x[2][3];
@@ -339,60 +522,114 @@ int misfit_gradient(swals_domain *d, int nsteps, double dt, const double *target
         for (int v = 0; v < 3; v++) { x[b][v] = (R *)p; p += plane * es; }
     R *ckpt = (R *)p; p += (size_t)3 * nseg * plane * es;
     double *d_target = (double *)p; p += sizeof(double) * (size_t)nsteps * ng;
-    double *d_rec = (double *)p; p += sizeof(double) * (size_t)K * ng * 3;
-    double *d_resid = (double *)p; p += sizeof(double) * (size_t)ng;
+    double *d_rec = (double *)p; p += sizeof(double) * (size_t)K * ng;
+    double *d_resid = (double *)p; p += sizeof(double) * (size_t)K * ng;
+    double *d_half = (double *)p; p += sizeof(double) * (size_t)nsteps;
     double *d_loss = (double *)p; p += sizeof(double) * 8;
-    int *d_sites = (int *)p; p += sizeof(int) * 2 * (size_t)ng;
-    p = (char *)(((uintptr_t)p + 255) & ~(uintptr_t)255);
-    swals::DevScalars *sc = (swals::DevScalars *)p;
+    int *d_sites = (int *)p;
 
     int rc = SWALS_OK;
     auto ck = [&](cudaError_t err, const char *w) { if (err != cudaSuccess && rc == SWALS_OK) rc = swals::api_cuda_fail(err, w); };
-    ck(cudaMemsetAsync(buf, 0, need, d->stream), "memset");
+    ck(cudaMemsetAsync(lam[0][0], 0, 3 * plane * es, d->stream), "memset");
     ck(cudaMemcpyAsync(d_target, target_host, sizeof(double) * (size_t)nsteps * ng, cudaMemcpyHostToDevice, d->stream),
        "target upload");
     ck(cudaMemcpyAsync(d_sites, d->h_sites.data(), sizeof(int) * 2 * ng, cudaMemcpyHostToDevice, d->stream), "sites");
-    // x_0 = the domain's current state
     for (int v = 0; v < 3; v++)
         ck(cudaMemcpyAsync(x[0][v], d->planes[d->cur][v], plane * es, cudaMemcpyDeviceToDevice, d->stream), "x0");
 
-    // Forward with checkpoints (loss accumulated on the device).
+    // The three per-segment step sequences.  For an even K a full segment
+    // leaves the buffer parity unchanged, so each sequence is captured once
+    // as a CUDA graph and replayed for every full segment.
+    auto fwd_seq = [&](int count) {   // x[0] -> x[0] after an even count
+        int c = 0;
+        for (int n = 0; n < count; n++) {
+            ck(map_step<R>(d, x[c], x[1 - c], dt, nullptr, 0, nullptr), "forward");
+            c = 1 - c;
+        }
+        return c;
+    };
+    auto rec_seq = [&](int count) {   // recompute, recording the gauge stage
+        int c = 0;
+        for (int n = 0; n < count; n++) {
+            ck(map_step<R>(d, x[c], x[1 - c], dt, d_sites, ng, d_rec + (size_t)n * ng), "recompute");
+            c = 1 - c;
+        }
+        return c;
+    };
+    auto adj_seq = [&](int count, int lc) {   // adjoint back through `count` steps
+        for (int t = count; t > 0; t--) {
+            ck(adjoint_step<R>(d, lam[lc], lam[1 - lc], dt, d_sites, ng, d_resid + (size_t)(t - 1) * ng),
+               "adjoint");
+            lc = 1 - lc;
+        }
+        return lc;
+    };
+    const bool graphs = (K % 2 == 0) && K <= nsteps && !d->timers_on;
+    if (graphs && (d->adj_K != K || d->adj_ng != ng || d->adj_dt != dt || d->adj_ws != d->ws || !d->adj_graph[0])) {
+        for (auto &g : d->adj_graph)
+            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+        d->adj_K = 0;
+        const int64_t l0 = d->launches;
+        for (int q = 0; q < 4 && rc == SWALS_OK; q++) {
+            ck(cudaStreamBeginCapture(d->stream, cudaStreamCaptureModeThreadLocal), "capture");
+            if (q == 0) fwd_seq(K);
+            else if (q == 1) rec_seq(K);
+            else adj_seq(K, q - 2);
+            cudaGraph_t gr = nullptr;
+            ck(cudaStreamEndCapture(d->stream, &gr), "end capture");
+            if (gr) {
+                ck(cudaGraphInstantiate(&d->adj_graph[q], gr, 0), "instantiate");
+                cudaGraphDestroy(gr);
+            }
+        }
+        d->launches = l0;
+        if (rc == SWALS_OK) { d->adj_K = K; d->adj_ng = ng; d->adj_dt = dt; d->adj_ws = d->ws; }
+    }
+
+    // Forward sweep with checkpoints (every segment starts in x[0]).
     int cur = 0;
-    for (int n = 0; n < nsteps && rc == SWALS_OK; n++) {
-        if (n % K == 0)
-            for (int v = 0; v < 3; v++)
-                ck(cudaMemcpyAsync(ckpt + ((size_t)(n / K) * 3 + v) * plane, x[cur][v], plane * es,
-                                   cudaMemcpyDeviceToDevice, d->stream), "checkpoint");
-        ck(forward_step<R>(d, x[cur], x[1 - cur], dt, sc), "forward");
-        cur = 1 - cur;
-        ck(cudaMemsetAsync(&sc->gauge_records, 0, sizeof(int), d->stream), "rec reset");
-        ck(swals::launch_gauges<R>(d->pitch, x[cur][0], x[cur][1], x[cur][2], d_sites, ng, d_rec, 1, sc, d->stream),
-           "gauges");
-        residual_kernel<<<1, 32, 0, d->stream>>>(d_rec, d_target + (size_t)n * ng, ng, d_resid, d_loss);
+    for (int sgm = 0; sgm < nseg && rc == SWALS_OK; sgm++) {
+        const int n0 = sgm * K, cnt = (n0 + K < nsteps) ? K : nsteps - n0;
+        for (int v = 0; v < 3; v++)
+            ck(cudaMemcpyAsync(ckpt + ((size_t)sgm * 3 + v) * plane, x[cur][v], plane * es, cudaMemcpyDeviceToDevice,
+                               d->stream), "checkpoint");
+        if (graphs && cnt == K && cur == 0) {
+            ck(cudaGraphLaunch(d->adj_graph[0], d->stream), "forward graph");
+            d->launches += K;
+        } else {
+            // A last, shorter segment (no state is needed after it).
+            int c = cur;
+            for (int n = 0; n < cnt; n++) {
+                ck(map_step<R>(d, x[c], x[1 - c], dt, nullptr, 0, nullptr), "forward");
+                c = 1 - c;
+            }
+            cur = c;
+        }
     }
     // Backward, segment by segment from the last.
     int lc = 0;
-    for (int s = nseg - 1; s >= 0 && rc == SWALS_OK; s--) {
-        const int n0 = s * K, n1 = (n0 + K < nsteps) ? n0 + K : nsteps;
+    for (int sgm = nseg - 1; sgm >= 0 && rc == SWALS_OK; sgm--) {
+        const int n0 = sgm * K, n1 = (n0 + K < nsteps) ? n0 + K : nsteps;
+        const int cnt = n1 - n0;
         for (int v = 0; v < 3; v++)
-            ck(cudaMemcpyAsync(x[0][v], ckpt + ((size_t)s * 3 + v) * plane, plane * es, cudaMemcpyDeviceToDevice,
+            ck(cudaMemcpyAsync(x[0][v], ckpt + ((size_t)sgm * 3 + v) * plane, plane * es, cudaMemcpyDeviceToDevice,
                                d->stream), "restore");
-        ck(cudaMemsetAsync(&sc->gauge_records, 0, sizeof(int), d->stream), "rec reset");
-        int xc = 0;
-        for (int n = n0; n < n1; n++) {   // recompute the segment, recording gauges
-            ck(forward_step<R>(d, x[xc], x[1 - xc], dt, sc), "recompute");
-            xc = 1 - xc;
-            ck(swals::launch_gauges<R>(d->pitch, x[xc][0], x[xc][1], x[xc][2], d_sites, ng, d_rec, K, sc,
-                                       d->stream), "gauges");
+        if (graphs && cnt == K) {
+            ck(cudaGraphLaunch(d->adj_graph[1], d->stream), "recompute graph");
+            d->launches += K;
+        } else {
+            rec_seq(cnt);
         }
-        for (int n = n1; n > n0; n--) {   // adjoint back through the segment
-            residual_kernel<<<1, 32, 0, d->stream>>>(d_rec + (size_t)(n - 1 - n0) * ng * 3, d_target + (size_t)(n - 1) * ng,
-                                                     ng, d_resid, d_loss + 1);
-            inject_kernel<R><<<1, 32, 0, d->stream>>>(lam[lc][0], d->pitch, d_sites, ng, d_resid);
-            ck(adjoint_step<R>(d, lam[lc], lam[1 - lc], dt), "adjoint");
-            lc = 1 - lc;
+        segment_residual_kernel<<<1, 128, 0, d->stream>>>(d_rec, d_target + (size_t)n0 * ng, cnt, ng, d_resid,
+                                                          d_half + n0);
+        if (graphs && cnt == K) {
+            ck(cudaGraphLaunch(d->adj_graph[2 + lc], d->stream), "adjoint graph");
+            d->launches += K;
+        } else {
+            lc = adj_seq(cnt, lc);
         }
     }
+    loss_sum_kernel<<<1, 32, 0, d->stream>>>(d_half, nsteps, d_loss);
     double loss = 0.0;
     ck(cudaMemcpyAsync(&loss, d_loss, sizeof(double), cudaMemcpyDeviceToHost, d->stream), "loss");
     if (rc == SWALS_OK) {
@@ -400,7 +637,6 @@ int misfit_gradient(swals_domain *d, int nsteps, double dt, const double *target
         rc = copy_plane3(d, src, grad_host, false);
     }
     cudaStreamSynchronize(d->stream);
-    cudaFree(buf);
     if (loss_out) *loss_out = loss;
     return rc;
 }

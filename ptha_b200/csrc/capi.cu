@@ -436,6 +436,12 @@ int swals_gpu_domain_create(const swals_domain_desc *desc, swals_domain **out)
     return SWALS_OK;
 }
 
+static void drop_step_graph(swals_domain *d)
+{
+    if (d->step_graph) cudaGraphExecDestroy(d->step_graph);
+    d->step_graph = nullptr;
+}
+
 int swals_gpu_domain_destroy(swals_domain *d)
 {
     if (!d) return SWALS_OK;
@@ -444,6 +450,10 @@ int swals_gpu_domain_destroy(swals_domain *d)
     for (auto e : d->ev_pool) cudaEventDestroy(e);
     if (d->d_sites) cudaFree(d->d_sites);
     if (d->d_records) cudaFree(d->d_records);
+    if (d->ws) cudaFree(d->ws);
+    drop_step_graph(d);
+    for (auto &g : d->adj_graph)
+        if (g) cudaGraphExecDestroy(g);
     cudaFree(d->pool);
     cudaStreamDestroy(d->stream);
     delete d;
@@ -536,14 +546,67 @@ int swals_gpu_evolve_one_step(swals_domain *d, double timestep, int32_t has_time
     return d->fp64 ? evolve_t<double>(d, timestep, has_timestep) : evolve_t<float>(d, timestep, has_timestep);
 }
 
+// nsteps calls of evolve_one_step.  Long runs replay a CUDA graph of
+// GRAPH_STEPS steps (a multiple of 3, so every method's state-buffer
+// rotation returns to where it started): the sequence of launches is the
+// same, without the per-launch host cost.  Timed (timers on) and first
+// steps run one by one.
+static constexpr int GRAPH_STEPS = 6;
+
 int swals_gpu_evolve_steps(swals_domain *d, int32_t nsteps, double timestep, int32_t has_timestep)
 {
     if (!d || nsteps < 0) return fail(SWALS_ERR_INVALID_ARGUMENT, "bad argument");
-    for (int s = 0; s < nsteps; s++) {
-        int rc = swals_gpu_evolve_one_step(d, timestep, has_timestep);
+    int done = 0;
+    auto eager = [&](int n) {
+        for (int s = 0; s < n; s++) {
+            int rc = swals_gpu_evolve_one_step(d, timestep, has_timestep);
+            if (rc) return rc;
+        }
+        return (int)SWALS_OK;
+    };
+    if (d->nsteps == 0 && nsteps > 0) {
+        int rc = eager(1);
         if (rc) return rc;
+        done = 1;
     }
-    return SWALS_OK;
+    const bool use_graph = !d->timers_on && (nsteps - done) >= 2 * GRAPH_STEPS;
+    if (use_graph) {
+        const bool same = d->step_graph && d->graph_dt == timestep && d->graph_has_dt == (has_timestep != 0) &&
+                          d->graph_stream == d->stream && d->graph_gauges == d->n_gauges;
+        if (!same) {
+            drop_step_graph(d);
+            const int cur0 = d->cur;
+            const int64_t n0 = d->nsteps, l0 = d->launches;
+            CK(cudaStreamBeginCapture(d->stream, cudaStreamCaptureModeThreadLocal));
+            int rc = SWALS_OK;
+            for (int s = 0; s < GRAPH_STEPS && rc == SWALS_OK; s++)
+                rc = d->fp64 ? evolve_t<double>(d, timestep, has_timestep) : evolve_t<float>(d, timestep, has_timestep);
+            cudaGraph_t g = nullptr;
+            cudaError_t ce = cudaStreamEndCapture(d->stream, &g);
+            const bool back = (d->cur == cur0);
+            d->graph_launches = d->launches - l0;
+            d->cur = cur0;
+            d->nsteps = n0;
+            d->launches = l0;
+            if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+            if (ce != cudaSuccess) { if (g) cudaGraphDestroy(g); return cuda_fail(ce, "cudaStreamEndCapture"); }
+            if (!back) { cudaGraphDestroy(g); return eager(nsteps - done); }
+            ce = cudaGraphInstantiate(&d->step_graph, g, 0);
+            cudaGraphDestroy(g);
+            if (ce != cudaSuccess) return cuda_fail(ce, "cudaGraphInstantiate");
+            d->graph_dt = timestep;
+            d->graph_has_dt = has_timestep != 0;
+            d->graph_stream = d->stream;
+            d->graph_gauges = d->n_gauges;
+        }
+        while (nsteps - done >= GRAPH_STEPS) {
+            CK(cudaGraphLaunch(d->step_graph, d->stream));
+            d->nsteps += GRAPH_STEPS;
+            d->launches += d->graph_launches;
+            done += GRAPH_STEPS;
+        }
+    }
+    return eager(nsteps - done);
 }
 
 int swals_gpu_get_state(swals_domain *d, swals_domain_state *st)
@@ -645,6 +708,8 @@ int swals_gpu_volume_interior(swals_domain *d, double *out)
 int swals_gpu_gauges_setup(swals_domain *d, const double *xy, int32_t n, int32_t capacity)
 {
     if (!d || (n > 0 && !xy) || n < 0 || capacity < 0) return fail(SWALS_ERR_INVALID_ARGUMENT, "bad argument");
+    cudaStreamSynchronize(d->stream);
+    drop_step_graph(d);  // it holds the old gauge buffers
     if (d->d_sites) { cudaFree(d->d_sites); d->d_sites = nullptr; }
     if (d->d_records) { cudaFree(d->d_records); d->d_records = nullptr; }
     d->n_gauges = 0;

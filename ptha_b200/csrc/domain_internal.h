@@ -43,6 +43,22 @@ struct swals_domain {
     std::vector<int> h_sites;
     // launch accounting and per-kernel event timers
     int64_t launches = 0;
+    // Replayed graph of a few steps for evolve_steps.
+    cudaGraphExec_t step_graph = nullptr;
+    double graph_dt = 0.0;
+    bool graph_has_dt = false;
+    cudaStream_t graph_stream = nullptr;
+    int graph_gauges = -1;
+    int64_t graph_launches = 0;
+    // misfit_gradient's replayed graphs (segments of K steps), valid for
+    // (adj_K, adj_ng, adj_dt, ws).
+    cudaGraphExec_t adj_graph[4] = {};   // forward, recompute, adjoint from lambda 0, from lambda 1
+    int adj_K = 0, adj_ng = 0;
+    double adj_dt = 0.0;
+    void *adj_ws = nullptr;
+    // Scratch of the adjoint entry points, kept between calls (grown on demand).
+    void *ws = nullptr;
+    size_t ws_bytes = 0;
     bool timers_on = false;
     std::vector<cudaEvent_t> ev_pool;
     struct Pending { int cat; cudaEvent_t a, b; };

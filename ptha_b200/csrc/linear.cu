@@ -46,6 +46,11 @@ struct LinArgs {
     int nbatch;             // instances sharing ELV and the metrics (1 for a plain domain)
     int64_t inst_stride;    // elements between consecutive instances' planes
     int64_t max_stride;     // elements between consecutive instances' max_stage planes
+    // Optional gauge sampling fused into the streaming kernel: rec[g] = new
+    // stage at site g (0-based i, j pairs).
+    const int *sites;
+    int n_sites;
+    double *rec;
 };
 
 __device__ __forceinline__ bool on_bc_ring(int i, int r, int nx, int ny, const int bext[4])
@@ -215,9 +220,12 @@ __global__ void __launch_bounds__(LBX *TYT) linear_step_kernel(const LinArgs<R> 
 // warp.  Every value is the same expression, in the same order, as in
 // linear_step_kernel.
 constexpr int SOUT = 30;
+#ifndef LIN_MINB
+#define LIN_MINB 8
+#endif
 
-template <typename R, bool CORIOLIS, bool TRUELY_LINEAR>
-__global__ void __launch_bounds__(128) linear_stream_kernel(const LinArgs<R> a, int SH, int nstrips, int total)
+template <typename R, bool CORIOLIS, bool TRUELY_LINEAR, bool GAUGES = false>
+__global__ void __launch_bounds__(128, LIN_MINB) linear_stream_kernel(const LinArgs<R> a, int SH, int nstrips, int total)
 {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
@@ -300,6 +308,9 @@ __global__ void __launch_bounds__(128) linear_stream_kernel(const LinArgs<R> a, 
             if (out) {
                 const int64_t o = (int64_t)j * P + i;
                 stg_o[o] = sn_j;
+                if (GAUGES)
+                    for (int q = 0; q < a.n_sites; q++)
+                        if (a.sites[2 * q] == i && a.sites[2 * q + 1] == j) a.rec[q] = (double)sn_j;
                 if (in_ms) max_stage[o] = (sn_j > mx) ? sn_j : mx;
                 R uh = uh_j, vh = vh_j;
                 if (i >= a.xl && i <= a.xu - 1 && j >= a.yl && j <= a.yu - 1) {
@@ -350,6 +361,188 @@ __global__ void __launch_bounds__(128) linear_stream_kernel(const LinArgs<R> a, 
             uh_j = uh_n; vh_j = vh_n; e_j = e_n; sn_j = sn_n;
             uh_n = uh_f; vh_n = vh_f; e_n = e_f; st_n = st_f;
         }
+    }
+}
+
+// The streaming step with its row loads staged through shared memory by
+// asynchronous copies (cp.async), so that AD rows per warp are in flight
+// without holding them in registers: each lane copies its own element of
+// UH, VH, STG, ELV and max_stage for a row into a per-warp ring of AD slots
+// and reads it back when the row is consumed; no other lane touches it, so
+// only the per-thread group waits are needed.  The arithmetic is
+// linear_stream_kernel's.
+constexpr int AD = 4;   // ring slots per warp (AD-1 rows in flight)
+
+__device__ __forceinline__ void cp_async_elem(void *smem, const void *gmem, int bytes, bool valid)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    const int src = valid ? bytes : 0;   // 0: zero-fill, nothing read
+    if (bytes == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(src));
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(sa), "l"(gmem), "r"(src));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+template <typename R, bool CORIOLIS, bool TRUELY_LINEAR, bool GAUGES = false>
+__global__ void __launch_bounds__(128, LIN_MINB) linear_async_kernel(const LinArgs<R> a, int SH, int nstrips, int total)
+{
+    __shared__ R ring[4][AD][5][32];   // [warp][slot][UH, VH, STG, ELV, max_stage][lane]
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int b = blockIdx.x;
+    if (b >= a.nbatch) return;
+    const int nx = a.p.nx, ny = a.p.ny;
+    const int64_t P = a.p.pitch;
+    const int64_t io = (int64_t)b * a.inst_stride;
+    const R *stg = a.p.stg + io, *uhp = a.p.uh + io, *vhp = a.p.vh + io;
+    R *stg_o = a.p.stg_o + io, *uh_o = a.p.uh_o + io, *vh_o = a.p.vh_o + io;
+    R *max_stage = a.p.max_stage ? a.p.max_stage + (int64_t)b * a.max_stride : nullptr;
+    const R *elv = a.p.elv;
+    const R g = K<R>::gravity();
+    const R half = K<R>::half();
+    const R one = K<R>::one();
+    const R zero = K<R>::zero();
+    const R mad = K<R>::min_depth();
+    R (*rg)[5][32] = ring[wib];
+
+    for (int w = blockIdx.y * 4 + wib; w < total; w += gridDim.y * 4) {
+        const int sx = w % nstrips, sy = w / nstrips;
+        const int ra = sy * SH;
+        const int rb = min(ra + SH, ny);
+        const int i = sx * SOUT - 1 + lane;
+        const int ic = clampi(i, 0, nx - 1);
+        const bool in_x = (i >= 0 && i < nx);
+        const bool out = (lane >= 1 && lane <= SOUT && i < nx);
+        const R dyl_i = a.m.dyl[ic];
+        const R dyl_ip1 = a.m.dyl[min(ic + 1, nx)];
+        // Row k of the segment's sequence is row ra - 1 + k, k = 0 .. rb - ra + 1.
+        const int nrow = rb - ra + 2;
+        auto issue = [&](int k) {
+            if (k < nrow) {
+                const int q = ra - 1 + k;
+                const int qc = clampi(q, 0, ny - 1);
+                const int slot = k % AD;
+                const int64_t oc = (int64_t)qc * P + ic;
+                cp_async_elem(&rg[slot][0][lane], uhp + oc, sizeof(R), true);
+                cp_async_elem(&rg[slot][1][lane], vhp + oc, sizeof(R), true);
+                const bool sv = (q >= 0 && q < ny && in_x);
+                cp_async_elem(&rg[slot][2][lane], stg + oc, sizeof(R), sv);
+                cp_async_elem(&rg[slot][3][lane], elv + oc, sizeof(R), true);
+                const bool mv = max_stage && out && i >= a.xl && i <= a.xu && q >= a.yl && q <= a.yu && q >= ra && q < rb;
+                cp_async_elem(&rg[slot][4][lane], (max_stage ? max_stage : stg) + oc, sizeof(R), mv);
+            }
+            cp_async_commit();
+        };
+        auto stage_new = [&](int r, R s_old, R uh_r, R uh_w, R vh_r, R vh_s) -> R {
+            R sn = R(0);
+            if (r < ny && in_x) {
+                const bool interior = (i >= a.xl + 1) && (i <= a.xu - 1) && (r >= a.yl + 1) && (r <= a.yu - 1);
+                if (interior) {
+                    const R inv_cell_area_dt = a.dt / a.m.area[r];
+                    const R t1 = (uh_r - uh_w) * dyl_i;
+                    const R t2 = vh_r * a.m.dxb[r + 1] - vh_s * a.m.dxb[r];
+                    sn = s_old - inv_cell_area_dt * (t1 + t2);
+                } else if (a.bc_stage && on_bc_ring(i, r, nx, ny, a.bext)) {
+                    sn = stg_o[(int64_t)r * P + i];
+                } else {
+                    sn = s_old;
+                }
+            }
+            return sn;
+        };
+
+        __syncwarp();  // the previous segment's reads of the ring are done
+        for (int k = 0; k < AD - 1; k++) issue(k);
+        // k = 0: row ra-1 (VH only)
+        cp_async_wait<AD - 2>();
+        R vh_jm1 = rg[0][1][lane];
+        issue(AD - 1);
+        // k = 1: row ra
+        cp_async_wait<AD - 2>();
+        R uh_j = rg[1][0][lane], vh_j = rg[1][1][lane], st_j = rg[1][2][lane], e_j = rg[1][3][lane];
+        R mx = rg[1][4][lane];
+        issue(AD);
+        R sn_j;
+        {
+            const R uh_w = __shfl_up_sync(FULL, uh_j, 1);
+            sn_j = stage_new(ra, st_j, uh_j, uh_w, vh_j, vh_jm1);
+        }
+        for (int j = ra; j < rb; j++) {
+            const int k = j - ra + 2;  // row j+1
+            cp_async_wait<AD - 2>();
+            const int slot = k % AD;
+            const R uh_n = rg[slot][0][lane], vh_n = rg[slot][1][lane], st_n = rg[slot][2][lane];
+            const R e_n = rg[slot][3][lane], mx_n = rg[slot][4][lane];
+            issue(k + AD - 1);
+            const bool in_ms = max_stage && out && i >= a.xl && i <= a.xu && j >= a.yl && j <= a.yu;
+
+            const R uh_nw = __shfl_up_sync(FULL, uh_n, 1);
+            const R sn_n = stage_new(j + 1, st_n, uh_n, uh_nw, vh_n, vh_j);
+
+            const R s_e = __shfl_down_sync(FULL, sn_j, 1);
+            const R e_e = __shfl_down_sync(FULL, e_j, 1);
+            const R uh_w = __shfl_up_sync(FULL, uh_j, 1);
+            const R vh_e = __shfl_down_sync(FULL, vh_j, 1);
+            const R vh_se = __shfl_down_sync(FULL, vh_jm1, 1);
+            if (out) {
+                const int64_t o = (int64_t)j * P + i;
+                stg_o[o] = sn_j;
+                if (GAUGES)
+                    for (int q = 0; q < a.n_sites; q++)
+                        if (a.sites[2 * q] == i && a.sites[2 * q + 1] == j) a.rec[q] = (double)sn_j;
+                if (in_ms) max_stage[o] = (sn_j > mx) ? sn_j : mx;
+                R uh = uh_j, vh = vh_j;
+                if (i >= a.xl && i <= a.xu - 1 && j >= a.yl && j <= a.yu - 1) {
+                    const R inv_cell_area_dt_g = g * a.dt / a.m.area[j];
+                    const R inv_cell_area_dt_vh_g = g * a.dt / (half * (a.m.area[j] + a.m.area[j + 1]));
+                    const R e0 = e_j;
+                    const R sn = sn_j, s_n = sn_n;
+                    R h_iph, h_jph, wet_iph, wet_jph;
+                    if (TRUELY_LINEAR) {
+                        const bool wi = (e0 < -mad + a.msl) && (e_e < -mad + a.msl);
+                        h_iph = wi ? (a.msl - half * (e_e + e0)) : zero;
+                        const bool wj = (e_n < -mad + a.msl) && (e0 < -mad + a.msl);
+                        h_jph = wj ? (a.msl - half * (e_n + e0)) : zero;
+                        wet_iph = one;
+                        wet_jph = one;
+                    } else {
+                        const bool wi = (sn - e0 > mad) && (s_e - e_e > mad);
+                        h_iph = wi ? (half * ((s_e + sn) - (e_e + e0))) : zero;
+                        const bool wj = (s_n - e_n > mad) && (sn - e0 > mad);
+                        h_jph = wj ? (half * ((s_n + sn) - (e_n + e0))) : zero;
+                        wet_iph = (h_iph > zero) ? one : zero;
+                        wet_jph = (h_jph > zero) ? one : zero;
+                    }
+                    const R dw_j = s_n - sn;
+                    R uh_new = uh * wet_iph - inv_cell_area_dt_g * h_iph * (s_e - sn) * dyl_ip1;
+                    R vh_new = vh * wet_jph - inv_cell_area_dt_vh_g * h_jph * dw_j * a.m.dxb[j + 1];
+                    if (CORIOLIS) {
+                        const R vh_iph_jmh = half * (vh_jm1 + vh_se);
+                        const R vh_iph_jph = half * (vh_j + vh_e);
+                        const R uh_i_j = half * (uh_j + uh_w);
+                        const R uh_i_jp1 = half * (uh_n + uh_nw);
+                        const R dt_half_coriolis = a.dt * a.m.cor[j] * half * ((h_iph > zero) ? one : zero);
+                        const R dt_half_coriolis_jph = a.dt * a.m.cor_be[j + 1] * half * ((h_jph > zero) ? one : zero);
+                        uh_new = uh_new + dt_half_coriolis * (vh_iph_jmh + vh_iph_jph);
+                        vh_new = vh_new - dt_half_coriolis_jph * (uh_i_j + uh_i_jp1);
+                    }
+                    if (a.lin_fric) {
+                        uh_new = a.lin_fric_mult * uh_new;
+                        vh_new = a.lin_fric_mult * vh_new;
+                    }
+                    uh = uh_new;
+                    vh = vh_new;
+                }
+                uh_o[o] = uh;
+                vh_o[o] = vh;
+            }
+            vh_jm1 = vh_j;
+            uh_j = uh_n; vh_j = vh_n; e_j = e_n; sn_j = sn_n; mx = mx_n;
+        }
+        cp_async_wait<0>();
     }
 }
 
@@ -483,22 +676,28 @@ template cudaError_t launch_batch_gauges<float>(int64_t, const float *, int64_t,
 // batched form's autotuner times each on the real problem.
 // Configurations 0-4: shared-memory tiles (rows per CTA, thread rows,
 // instances per CTA); 5-7: streaming warps with 32, 64 or 128 rows per
-// segment; 8: streaming with the segment height chosen from the grid size.
-// Plain domains use STREAM_DEFAULT.
+// segment; 8: streaming with the segment height chosen from the grid size;
+// 9-10: cp.async-pipelined streaming, 64 rows or chosen.  Plain domains use
+// ASYNC_DEFAULT.
 struct TileCfg { int by, tyt, ib; };
 constexpr TileCfg kTileCfgs[] = {{16, 8, 1}, {16, 8, 2}, {16, 8, 4}, {32, 8, 2}, {8, 8, 4}};
 constexpr int kStreamSH[] = {32, 64, 128, 0};
-constexpr int kNumTileCfgs = sizeof(kTileCfgs) / sizeof(kTileCfgs[0]) + sizeof(kStreamSH) / sizeof(kStreamSH[0]);
+constexpr int kAsyncSH[] = {64, 0};
+constexpr int kNumTileCfgs = sizeof(kTileCfgs) / sizeof(kTileCfgs[0]) + sizeof(kStreamSH) / sizeof(kStreamSH[0]) +
+                             sizeof(kAsyncSH) / sizeof(kAsyncSH[0]);
 constexpr int STREAM_DEFAULT = 8;
+constexpr int ASYNC_DEFAULT = 10;
 
 // Rows per segment: the longest segment (up to 128 rows, which amortises the
 // two rows a segment reloads) that still gives every SM about 24 warps.
 inline int stream_rows(int nx, int ny, int nbatch)
 {
+    // At least four waves of 20 warps per SM (so the last, partial wave is a
+    // small part of the launch), but no segment under 16 rows.
     const int64_t nstrips = (nx + SOUT - 1) / SOUT;
-    const int64_t want = 148 * 24;
+    const int64_t want = 148 * 20 * 4;
     int sh = 128;
-    while (sh > 8 && (int64_t)nbatch * nstrips * ((ny + sh - 1) / sh) < want) sh /= 2;
+    while (sh > 16 && (int64_t)nbatch * nstrips * ((ny + sh - 1) / sh) < want) sh /= 2;
     return sh;
 }
 
@@ -511,7 +710,10 @@ void launch_stream(const LinArgs<R> &a, int sh, cudaStream_t s)
     const int total = nstrips * nseg;
     const int gy = std::min((total + 3) / 4, 65535);
     dim3 grid(a.nbatch, gy);
-    linear_stream_kernel<R, COR, TL><<<grid, 128, 0, s>>>(a, sh, nstrips, total);
+    if (a.rec && a.n_sites > 0)
+        linear_stream_kernel<R, COR, TL, true><<<grid, 128, 0, s>>>(a, sh, nstrips, total);
+    else
+        linear_stream_kernel<R, COR, TL, false><<<grid, 128, 0, s>>>(a, sh, nstrips, total);
 }
 
 template <typename R, bool COR, bool TL, int BY, int TYT, int IB>
@@ -523,9 +725,29 @@ void launch_cfg(const LinArgs<R> &a, cudaStream_t s)
 }
 
 template <typename R, bool COR, bool TL>
+void launch_async(const LinArgs<R> &a, int sh, cudaStream_t s)
+{
+    if (sh <= 0) sh = stream_rows(a.p.nx, a.p.ny, a.nbatch);
+    const int nstrips = (a.p.nx + SOUT - 1) / SOUT;
+    const int nseg = (a.p.ny + sh - 1) / sh;
+    const int total = nstrips * nseg;
+    const int gy = std::min((total + 3) / 4, 65535);
+    dim3 grid(a.nbatch, gy);
+    if (a.rec && a.n_sites > 0)
+        linear_async_kernel<R, COR, TL, true><<<grid, 128, 0, s>>>(a, sh, nstrips, total);
+    else
+        linear_async_kernel<R, COR, TL, false><<<grid, 128, 0, s>>>(a, sh, nstrips, total);
+}
+
+template <typename R, bool COR, bool TL>
 void launch_tile(const LinArgs<R> &a, int cfg, cudaStream_t s)
 {
     const int ntile = (int)(sizeof(kTileCfgs) / sizeof(kTileCfgs[0]));
+    const int nstream = (int)(sizeof(kStreamSH) / sizeof(kStreamSH[0]));
+    if (cfg >= ntile + nstream) {
+        launch_async<R, COR, TL>(a, kAsyncSH[cfg - ntile - nstream], s);
+        return;
+    }
     if (cfg >= ntile) {
         launch_stream<R, COR, TL>(a, kStreamSH[cfg - ntile], s);
         return;
@@ -549,14 +771,14 @@ void launch_main(const LinArgs<R> &a, const StepConfig &c, int cfg, cudaStream_t
     else launch_tile<R, false, false>(a, cfg, s);
 }
 
-// Kernel of a plain (unbatched) step: the streaming form unless
-// SWALS_LINEAR_KERNEL=tile selects the shared-memory tile.
+// Kernel of a plain (unbatched) step: the cp.async-pipelined streaming form
+// unless SWALS_LINEAR_KERNEL selects "stream" (registers only) or "tile".
 int linear_kernel_config()
 {
     static int cfg = -1;
     if (cfg < 0) {
         const char *e = getenv("SWALS_LINEAR_KERNEL");
-        cfg = (e && strcmp(e, "tile") == 0) ? 0 : STREAM_DEFAULT;
+        cfg = (e && strcmp(e, "tile") == 0) ? 0 : (e && strcmp(e, "stream") == 0) ? STREAM_DEFAULT : ASYNC_DEFAULT;
     }
     return cfg;
 }
@@ -578,6 +800,9 @@ LinArgs<R> make_args(const StepPlanes<R> &p, const Metrics<R> &m, const StepConf
     a.nbatch = 1;
     a.inst_stride = 0;
     a.max_stride = 0;
+    a.sites = nullptr;
+    a.n_sites = 0;
+    a.rec = nullptr;
     return a;
 }
 
@@ -591,6 +816,25 @@ cudaError_t launch_linear_step(const StepPlanes<R> &p, const Metrics<R> &m, cons
     hook(CAT_LINEAR_EDGE, 1);
     hook(CAT_LINEAR_MAIN, 0);
     launch_main<R>(a, c, linear_kernel_config(), s);
+    hook(CAT_LINEAR_MAIN, 1);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_linear_map(const StepPlanes<R> &p, const Metrics<R> &m, const StepConfig &c, R dt,
+                              const int *sites, int n_sites, double *rec, cudaStream_t s, const LaunchHook &hook)
+{
+    LinArgs<R> a = make_args<R>(p, m, c, dt);
+    a.bc_stage = 0;
+    a.sites = sites;
+    a.n_sites = n_sites;
+    a.rec = rec;
+    hook(CAT_LINEAR_MAIN, 0);
+    const bool cor = c.coriolis != 0, tl = c.truely_linear != 0;
+    if (cor && tl) launch_async<R, true, true>(a, 0, s);
+    else if (cor && !tl) launch_async<R, true, false>(a, 0, s);
+    else if (!cor && tl) launch_async<R, false, true>(a, 0, s);
+    else launch_async<R, false, false>(a, 0, s);
     hook(CAT_LINEAR_MAIN, 1);
     return cudaGetLastError();
 }
@@ -637,6 +881,11 @@ template cudaError_t launch_linear_step<double>(const StepPlanes<double> &, cons
 template cudaError_t launch_linear_step<float>(const StepPlanes<float> &, const Metrics<float> &,
                                                const StepConfig &, float, DevScalars *, cudaStream_t,
                                                const LaunchHook &);
+template cudaError_t launch_linear_map<double>(const StepPlanes<double> &, const Metrics<double> &,
+                                               const StepConfig &, double, const int *, int, double *, cudaStream_t,
+                                               const LaunchHook &);
+template cudaError_t launch_linear_map<float>(const StepPlanes<float> &, const Metrics<float> &, const StepConfig &,
+                                              float, const int *, int, double *, cudaStream_t, const LaunchHook &);
 template cudaError_t launch_linear_batch<double>(const StepPlanes<double> &, int64_t, int64_t, int,
                                                  const Metrics<double> &, const StepConfig &, double, int,
                                                  cudaStream_t, const LaunchHook &);

@@ -50,6 +50,14 @@ template <typename R>
 cudaError_t launch_linear_step(const StepPlanes<R> &p, const Metrics<R> &m, const StepConfig &c,
                                R dt, DevScalars *sc, cudaStream_t s, const LaunchHook &hook);
 
+// The leapfrog's interior update alone (no boundary routine, boundary-flux
+// sums, time or max_stage): the linear map x' = M x that the adjoint
+// differentiates.  With n_sites > 0 the new stage at the sites (0-based i, j
+// pairs) is written to rec.
+template <typename R>
+cudaError_t launch_linear_map(const StepPlanes<R> &p, const Metrics<R> &m, const StepConfig &c, R dt,
+                              const int *sites, int n_sites, double *rec, cudaStream_t s, const LaunchHook &hook);
+
 // Batched truly/not-truly linear leapfrog: `nbatch` instances whose planes
 // follow instance 0's at `inst_stride` elements, sharing ELV and metrics
 // (no boundary routine).  tile_cfg selects one of linear_tile_config_count()
