@@ -196,6 +196,9 @@ __global__ void __launch_bounds__(128) linear_adjoint_stream_kernel(const AdjArg
         const int i = sx * AOUT - 1 + lane;
         const bool in_x = (i >= 0 && i < nx);
         const bool out = (lane >= 1 && lane <= AOUT && i < nx);
+        // Gauges whose adjoint is injected into the rows this warp loads.
+        const unsigned long long gmask =
+            resid ? swals::gauges_in(sites, ng, sx * AOUT - 1, sx * AOUT + AOUT, ra - 1, rb + 2) : 0ull;
 
         auto load = [&](int r) -> ARow<R> {
             ARow<R> v;
@@ -204,9 +207,17 @@ __global__ void __launch_bounds__(128) linear_adjoint_stream_kernel(const AdjArg
                 const int64_t o = (int64_t)r * P + i;
                 v.ls = a.ls[o]; v.lu = a.lu[o]; v.lv = a.lv[o]; v.e = a.elv[o];
                 if (i + 1 < nx) v.ee = a.elv[o + 1];
-                if (resid)
-                    for (int q = 0; q < ng; q++)
-                        if (sites[2 * q] == i && sites[2 * q + 1] == r) v.ls = v.ls + R(resid[q]);
+                if (gmask) {
+                    if (ng > 64) {
+                        for (int q = 0; q < ng; q++)
+                            if (sites[2 * q] == i && sites[2 * q + 1] == r) v.ls = v.ls + R(resid[q]);
+                    } else {
+                        for (unsigned long long m = gmask; m; m &= m - 1) {
+                            const int q = __ffsll((long long)m) - 1;
+                            if (sites[2 * q] == i && sites[2 * q + 1] == r) v.ls = v.ls + R(resid[q]);
+                        }
+                    }
+                }
             }
             return v;
         };

@@ -234,7 +234,12 @@ int evolve_t(swals_domain *d, double timestep, int has_dt)
         p.stg = (const R *)d->planes[in][0]; p.uh = (const R *)d->planes[in][1]; p.vh = (const R *)d->planes[in][2];
         p.stg_o = (R *)d->planes[out][0]; p.uh_o = (R *)d->planes[out][1]; p.vh_o = (R *)d->planes[out][2];
         p.elv = (R *)d->elv; p.max_stage = max_stage; p.manning_sq = (R *)d->manning_sq;
-        e = launch_linear_step<R>(p, m, c, R(timestep), d->sc, d->stream, hook);
+        if (!d->aux.stream) {
+            cudaStreamCreateWithFlags(&d->aux.stream, cudaStreamNonBlocking);
+            cudaEventCreateWithFlags(&d->aux.fork, cudaEventDisableTiming);
+            cudaEventCreateWithFlags(&d->aux.join, cudaEventDisableTiming);
+        }
+        e = launch_linear_step<R>(p, m, c, R(timestep), d->sc, d->stream, hook, d->timers_on ? nullptr : &d->aux);
         if (e != cudaSuccess) return cuda_fail(e, "linear leapfrog step");
         d->cur = out;
     } else if (d->method == M_RK2 || d->method == M_EULER) {
@@ -454,6 +459,12 @@ int swals_gpu_domain_destroy(swals_domain *d)
     drop_step_graph(d);
     for (auto &g : d->adj_graph)
         if (g) cudaGraphExecDestroy(g);
+    if (d->aux.stream) {
+        cudaStreamSynchronize(d->aux.stream);
+        cudaStreamDestroy(d->aux.stream);
+        cudaEventDestroy(d->aux.fork);
+        cudaEventDestroy(d->aux.join);
+    }
     cudaFree(d->pool);
     cudaStreamDestroy(d->stream);
     delete d;

@@ -43,6 +43,8 @@ struct swals_domain {
     std::vector<int> h_sites;
     // launch accounting and per-kernel event timers
     int64_t launches = 0;
+    // Side stream for the leapfrog's bookkeeping kernel.
+    swals::AuxStream aux;
     // Replayed graph of a few steps for evolve_steps.
     cudaGraphExec_t step_graph = nullptr;
     double graph_dt = 0.0;

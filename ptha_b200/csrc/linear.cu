@@ -254,6 +254,8 @@ __global__ void __launch_bounds__(128, LIN_MINB) linear_stream_kernel(const LinA
         const bool out = (lane >= 1 && lane <= SOUT && i < nx);
         const R dyl_i = a.m.dyl[ic];
         const R dyl_ip1 = a.m.dyl[min(ic + 1, nx)];
+        const unsigned long long gmask =
+            GAUGES ? gauges_in(a.sites, a.n_sites, sx * SOUT, sx * SOUT + SOUT - 1, ra, rb - 1) : 0ull;
 
         // New stage of cell (i, r) from its row's loads (domain_mod_linear_solver_include.f90:92-115).
         auto stage_new = [&](int r, R s_old, R uh_r, R uh_w, R vh_r, R vh_s) -> R {
@@ -308,9 +310,17 @@ __global__ void __launch_bounds__(128, LIN_MINB) linear_stream_kernel(const LinA
             if (out) {
                 const int64_t o = (int64_t)j * P + i;
                 stg_o[o] = sn_j;
-                if (GAUGES)
-                    for (int q = 0; q < a.n_sites; q++)
-                        if (a.sites[2 * q] == i && a.sites[2 * q + 1] == j) a.rec[q] = (double)sn_j;
+                if (GAUGES && gmask) {
+                    if (a.n_sites > 64) {
+                        for (int q = 0; q < a.n_sites; q++)
+                            if (a.sites[2 * q] == i && a.sites[2 * q + 1] == j) a.rec[q] = (double)sn_j;
+                    } else {
+                        for (unsigned long long m = gmask; m; m &= m - 1) {
+                            const int q = __ffsll((long long)m) - 1;
+                            if (a.sites[2 * q] == i && a.sites[2 * q + 1] == j) a.rec[q] = (double)sn_j;
+                        }
+                    }
+                }
                 if (in_ms) max_stage[o] = (sn_j > mx) ? sn_j : mx;
                 R uh = uh_j, vh = vh_j;
                 if (i >= a.xl && i <= a.xu - 1 && j >= a.yl && j <= a.yu - 1) {
@@ -418,6 +428,8 @@ __global__ void __launch_bounds__(128, LIN_MINB) linear_async_kernel(const LinAr
         const bool out = (lane >= 1 && lane <= SOUT && i < nx);
         const R dyl_i = a.m.dyl[ic];
         const R dyl_ip1 = a.m.dyl[min(ic + 1, nx)];
+        const unsigned long long gmask =
+            GAUGES ? gauges_in(a.sites, a.n_sites, sx * SOUT, sx * SOUT + SOUT - 1, ra, rb - 1) : 0ull;
         // Row k of the segment's sequence is row ra - 1 + k, k = 0 .. rb - ra + 1.
         const int nrow = rb - ra + 2;
         auto issue = [&](int k) {
@@ -490,9 +502,17 @@ __global__ void __launch_bounds__(128, LIN_MINB) linear_async_kernel(const LinAr
             if (out) {
                 const int64_t o = (int64_t)j * P + i;
                 stg_o[o] = sn_j;
-                if (GAUGES)
-                    for (int q = 0; q < a.n_sites; q++)
-                        if (a.sites[2 * q] == i && a.sites[2 * q + 1] == j) a.rec[q] = (double)sn_j;
+                if (GAUGES && gmask) {
+                    if (a.n_sites > 64) {
+                        for (int q = 0; q < a.n_sites; q++)
+                            if (a.sites[2 * q] == i && a.sites[2 * q + 1] == j) a.rec[q] = (double)sn_j;
+                    } else {
+                        for (unsigned long long m = gmask; m; m &= m - 1) {
+                            const int q = __ffsll((long long)m) - 1;
+                            if (a.sites[2 * q] == i && a.sites[2 * q + 1] == j) a.rec[q] = (double)sn_j;
+                        }
+                    }
+                }
                 if (in_ms) max_stage[o] = (sn_j > mx) ? sn_j : mx;
                 R uh = uh_j, vh = vh_j;
                 if (i >= a.xl && i <= a.xu - 1 && j >= a.yl && j <= a.yu - 1) {
@@ -808,9 +828,27 @@ LinArgs<R> make_args(const StepPlanes<R> &p, const Metrics<R> &m, const StepConf
 
 template <typename R>
 cudaError_t launch_linear_step(const StepPlanes<R> &p, const Metrics<R> &m, const StepConfig &c, R dt,
-                               DevScalars *sc, cudaStream_t s, const LaunchHook &hook)
+                               DevScalars *sc, cudaStream_t s, const LaunchHook &hook, const AuxStream *aux)
 {
     LinArgs<R> a = make_args<R>(p, m, c, dt);
+    const bool side = aux && aux->stream && !a.bc_stage;
+    if (side) {
+        // Bookkeeping beside the main kernel: it reads the input planes and
+        // writes only the scalars; the main stream waits for it at the end.
+        // (The caller passes `aux` only when the per-launch timers are off;
+        // the hook then only counts launches.)
+        cudaEventRecord(aux->fork, s);
+        cudaStreamWaitEvent(aux->stream, aux->fork, 0);
+        hook(CAT_LINEAR_EDGE, 0);
+        linear_edge_kernel<R><<<1, 512, 0, aux->stream>>>(a, sc, c.exterior_cells_width, c.bf);
+        hook(CAT_LINEAR_EDGE, 1);
+        cudaEventRecord(aux->join, aux->stream);
+        hook(CAT_LINEAR_MAIN, 0);
+        launch_main<R>(a, c, linear_kernel_config(), s);
+        hook(CAT_LINEAR_MAIN, 1);
+        cudaStreamWaitEvent(s, aux->join, 0);
+        return cudaGetLastError();
+    }
     hook(CAT_LINEAR_EDGE, 0);
     linear_edge_kernel<R><<<1, 512, 0, s>>>(a, sc, c.exterior_cells_width, c.bf);
     hook(CAT_LINEAR_EDGE, 1);
@@ -877,10 +915,10 @@ cudaError_t launch_gauges(int64_t pitch, const R *stg, const R *uh, const R *vh,
 
 template cudaError_t launch_linear_step<double>(const StepPlanes<double> &, const Metrics<double> &,
                                                 const StepConfig &, double, DevScalars *, cudaStream_t,
-                                                const LaunchHook &);
+                                                const LaunchHook &, const AuxStream *);
 template cudaError_t launch_linear_step<float>(const StepPlanes<float> &, const Metrics<float> &,
                                                const StepConfig &, float, DevScalars *, cudaStream_t,
-                                               const LaunchHook &);
+                                               const LaunchHook &, const AuxStream *);
 template cudaError_t launch_linear_map<double>(const StepPlanes<double> &, const Metrics<double> &,
                                                const StepConfig &, double, const int *, int, double *, cudaStream_t,
                                                const LaunchHook &);

@@ -45,10 +45,33 @@ struct StepConfig {
     int exterior_cells_width;
 };
 
+// Gauges (0-based i, j site pairs) inside the window [i0, i1] x [r0, r1]:
+// bit q set for gauge q.  Streaming kernels compute it once per warp segment
+// so the per-row check costs nothing where there is no gauge.  With more than
+// 64 gauges every bit is set and the callers test each gauge.
+__device__ __forceinline__ unsigned long long gauges_in(const int *sites, int n, int i0, int i1, int r0, int r1)
+{
+    if (n > 64) return ~0ull;
+    unsigned long long m = 0ull;
+    for (int q = 0; q < n; q++) {
+        const int gi = sites[2 * q], gj = sites[2 * q + 1];
+        if (gi >= i0 && gi <= i1 && gj >= r0 && gj <= r1) m |= 1ull << q;
+    }
+    return m;
+}
+
 // Linear leapfrog, one full step (domain_mod_linear_solver_include.f90:58-571).
+// With an auxiliary stream and two events, the one-block bookkeeping kernel
+// (boundary-flux sums, time) runs beside the main kernel when no boundary
+// routine writes the stage ring (the two then touch disjoint data).
+struct AuxStream {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+};
 template <typename R>
 cudaError_t launch_linear_step(const StepPlanes<R> &p, const Metrics<R> &m, const StepConfig &c,
-                               R dt, DevScalars *sc, cudaStream_t s, const LaunchHook &hook);
+                               R dt, DevScalars *sc, cudaStream_t s, const LaunchHook &hook,
+                               const AuxStream *aux = nullptr);
 
 // The leapfrog's interior update alone (no boundary routine, boundary-flux
 // sums, time or max_stage): the linear map x' = M x that the adjoint
