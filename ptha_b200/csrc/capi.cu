@@ -250,6 +250,7 @@ int evolve_t(swals_domain *d, double timestep, int has_dt)
         buf.side = d->side;
         buf.partials = d->lines;
         buf.partials_len = 2 * (2 * d->nx + 2 * d->ny);
+        buf.edges = d->edges;
         e = launch_rk2_step<R>(pl, d->cur, (R *)d->elv, max_stage, (R *)d->manning_sq, d->nx, d->ny, d->pitch, m, c,
                                has_dt != 0, timestep, d->method == M_EULER, buf, d->sc, d->stream, hook);
         if (e != cudaSuccess) return cuda_fail(e, "finite-volume step");
@@ -395,6 +396,10 @@ int swals_gpu_domain_create(const swals_domain_desc *desc, swals_domain **out)
     d->scratch_len = (nx > ny ? nx : ny) + 4096;
     const size_t scratch_bytes = al((size_t)d->scratch_len * sizeof(double));
     total += side_bytes + lines_bytes + scratch_bytes + al(64);
+    // Stored stage-1 edge results of adaptive finite-volume steps.
+    const size_t edge_bytes = (d->method == M_RK2 || d->method == M_EULER)
+                                  ? al((size_t)swals::rk2_edge_bytes(d->pitch, ny, (int)es)) : 0;
+    total += edge_bytes;
     e = cudaMalloc(&d->pool, total);
     if (e != cudaSuccess) {
         cudaStreamDestroy(d->stream);
@@ -414,6 +419,7 @@ int swals_gpu_domain_create(const swals_domain_desc *desc, swals_domain **out)
     d->lines = (double *)p; p += lines_bytes;
     d->scratch = (double *)p; p += scratch_bytes;
     d->d_out = (double *)p; p += al(64);
+    d->edges = edge_bytes ? (void *)p : nullptr; p += edge_bytes;
 
     int rc = SWALS_OK;
     if ((e = cudaMemsetAsync(d->pool, 0, total, d->stream)) != cudaSuccess) rc = cuda_fail(e, "memset");

@@ -498,6 +498,101 @@ cudaError_t launch_stage_any(const Rk2Args<R> &a, cudaStream_t s)
     return launch_stage<R, MODE, SPH, COR, FRIC>(a, s);
 }
 
+// Stage-1 update of an adaptive step from the edge results the flux pass
+// stored: the same per-cell fix-ups and fv_update as the stage kernels, one
+// thread per cell.
+template <typename R, bool SPH, bool COR, int FRIC>
+__global__ void __launch_bounds__(256) rk2_update_kernel(const Rk2Args<R> a)
+{
+    const int i = blockIdx.x * 32 + threadIdx.x;
+    const int r = blockIdx.y * 8 + threadIdx.y;
+    const int nx = a.nx, ny = a.ny;
+    long long negfix = 0;
+    if (i < nx && r < ny) {
+        const int64_t o = (int64_t)r * a.P + i;
+        // compute_depth_and_velocity (domain_mod.f90:1387-1412)
+        Cell<R> c;
+        R sv = a.stg[o];
+        const R ev = a.elv[o];
+        R dep = sv - ev;
+        c.u = R(0); c.v = R(0);
+        if (dep > K<R>::min_depth()) {
+            const R depth_inv = R(1) / dep;
+            c.u = a.uh[o] * depth_inv;
+            c.v = a.vh[o] * depth_inv;
+        } else if (dep < R(0)) {
+            dep = R(0);
+            sv = ev;
+            negfix = 1;
+        }
+        c.stg = sv; c.dep = dep; c.elv = ev;
+        const EdgePlanes<R> &ep = a.ep;
+        EdgeRes<R> n_lo, n_hi, w_lo, w_hi;
+        n_lo.f[0] = ep.sf[0][o]; n_lo.f[1] = ep.sf[1][o]; n_lo.f[2] = ep.sf[2][o];
+        n_lo.es_pos = ep.s_pos[o]; n_lo.es_neg = 0.0;
+        w_lo.f[0] = ep.wf[0][o]; w_lo.f[1] = ep.wf[1][o]; w_lo.f[2] = ep.wf[2][o];
+        w_lo.es_pos = ep.w_pos[o]; w_lo.es_neg = 0.0;
+        if (r + 1 < ny) {
+            const int64_t on = o + a.P;
+            n_hi.f[0] = ep.sf[0][on]; n_hi.f[1] = ep.sf[1][on]; n_hi.f[2] = ep.sf[2][on];
+            n_hi.es_neg = ep.s_neg[on];
+        } else {
+            n_hi.f[0] = n_hi.f[1] = n_hi.f[2] = R(0);
+            n_hi.es_neg = 0.0;
+        }
+        n_hi.es_pos = 0.0;
+        if (i + 1 < nx) {
+            w_hi.f[0] = ep.wf[0][o + 1]; w_hi.f[1] = ep.wf[1][o + 1]; w_hi.f[2] = ep.wf[2][o + 1];
+            w_hi.es_neg = ep.w_neg[o + 1];
+        } else {
+            w_hi.f[0] = w_hi.f[1] = w_hi.f[2] = R(0);
+            w_hi.es_neg = 0.0;
+        }
+        w_hi.es_pos = 0.0;
+        fv_update<R, MODE_STAGE1, SPH, COR, FRIC>(a, i, r, c, n_lo, n_hi, w_lo, w_hi, stage_dt<R>(a));
+    }
+    for (int off = 16; off > 0; off >>= 1) negfix += __shfl_down_sync(0xffffffffu, negfix, off);
+    if ((threadIdx.x & 31) == 0 && negfix)
+        atomicAdd((unsigned long long *)&a.sc->negative_depth_fix_counter, (unsigned long long)negfix);
+}
+
+template <typename R, bool SPH, bool COR, int FRIC>
+cudaError_t launch_flux_pass(const Rk2Args<R> &a, cudaStream_t s)
+{
+    return launch_stage_stream<R, MODE_FLUX, SPH, COR, FRIC>(a, s);
+}
+
+template <typename R, bool SPH, bool COR, int FRIC>
+cudaError_t launch_update(const Rk2Args<R> &a, cudaStream_t s)
+{
+    dim3 block(32, 8), grid((a.nx + 31) / 32, (a.ny + 7) / 8);
+    rk2_update_kernel<R, SPH, COR, FRIC><<<grid, block, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+// Run F<R, SPH, COR, FRIC>(a, s) for the step configuration.
+#define SWALS_DISPATCH_FV(FN)                                                                          \
+    const int fric = c.nofriction ? FRIC_NONE : (c.chezy ? FRIC_CHEZY : FRIC_MANNING);                 \
+    if (c.spherical) {                                                                                 \
+        if (c.coriolis) {                                                                              \
+            if (fric == FRIC_MANNING) return FN<R, true, true, FRIC_MANNING>(a, s);                    \
+            if (fric == FRIC_CHEZY) return FN<R, true, true, FRIC_CHEZY>(a, s);                        \
+            return FN<R, true, true, FRIC_NONE>(a, s);                                                 \
+        }                                                                                              \
+        if (fric == FRIC_MANNING) return FN<R, true, false, FRIC_MANNING>(a, s);                       \
+        if (fric == FRIC_CHEZY) return FN<R, true, false, FRIC_CHEZY>(a, s);                           \
+        return FN<R, true, false, FRIC_NONE>(a, s);                                                    \
+    }                                                                                                  \
+    if (fric == FRIC_MANNING) return FN<R, false, false, FRIC_MANNING>(a, s);                          \
+    if (fric == FRIC_CHEZY) return FN<R, false, false, FRIC_CHEZY>(a, s);                              \
+    return FN<R, false, false, FRIC_NONE>(a, s);
+
+template <typename R>
+cudaError_t dispatch_flux(const Rk2Args<R> &a, const StepConfig &c, cudaStream_t s) { SWALS_DISPATCH_FV(launch_flux_pass) }
+
+template <typename R>
+cudaError_t dispatch_update(const Rk2Args<R> &a, const StepConfig &c, cudaStream_t s) { SWALS_DISPATCH_FV(launch_update) }
+
 template <typename R, int MODE>
 cudaError_t dispatch_stage(const Rk2Args<R> &a, const StepConfig &c, cudaStream_t s)
 {
@@ -544,9 +639,31 @@ cudaError_t launch_rk2_step(R *const planes[3][3], int &cur, R *elv, R *max_stag
     a.side = reinterpret_cast<R *>(buf.side);
     a.sc = sc;
     a.stg0 = nullptr; a.uh0 = nullptr; a.vh0 = nullptr;
+    a.ep = EdgePlanes<R>{};
     cudaError_t e;
 
-    if (!has_dt) {
+    // With stored edges, an adaptive stage 1 is a flux pass (edges, CFL
+    // maximum and boundary-flux lines of U0) and an update once dt is known;
+    // otherwise a CFL pass (adaptive only) and the fused stage kernel.
+    const bool stored = !has_dt && buf.edges && use_stream_kernel();
+    if (stored) {
+        char *q = reinterpret_cast<char *>(buf.edges);
+        const int64_t plane = pitch * (int64_t)ny;
+        auto take_r = [&]() { R *p = reinterpret_cast<R *>(q); q += plane * sizeof(R); return p; };
+        auto take_d = [&]() { double *p = reinterpret_cast<double *>(q); q += plane * sizeof(double); return p; };
+        // doubles first (8-byte alignment whatever R is)
+        a.ep.s_pos = take_d(); a.ep.s_neg = take_d(); a.ep.w_pos = take_d(); a.ep.w_neg = take_d();
+        for (int k = 0; k < 3; k++) a.ep.sf[k] = take_r();
+        for (int k = 0; k < 3; k++) a.ep.wf[k] = take_r();
+        Rk2Args<R> p = a;
+        p.stg = planes[A][0]; p.uh = planes[A][1]; p.vh = planes[A][2];
+        p.stg_o = nullptr; p.uh_o = nullptr; p.vh_o = nullptr;
+        p.dt_from_cfl = 0; p.write_cfl = 1; p.lines = lines1;
+        hook(CAT_CFL, 0);
+        e = dispatch_flux<R>(p, c, s);
+        hook(CAT_CFL, 1);
+        if (e != cudaSuccess) return e;
+    } else if (!has_dt) {
         // Adaptive: the CFL of U0 must be known before the first update.
         Rk2Args<R> p = a;
         p.stg = planes[A][0]; p.uh = planes[A][1]; p.vh = planes[A][2];
@@ -565,7 +682,7 @@ cudaError_t launch_rk2_step(R *const planes[3][3], int &cur, R *elv, R *max_stag
     a.lines = lines1;
     if (euler_only) a.max_stage = nullptr;
     hook(CAT_STAGE1, 0);
-    e = dispatch_stage<R, MODE_STAGE1>(a, c, s);
+    e = stored ? dispatch_update<R>(a, c, s) : dispatch_stage<R, MODE_STAGE1>(a, c, s);
     hook(CAT_STAGE1, 1);
     if (e != cudaSuccess) return e;
 

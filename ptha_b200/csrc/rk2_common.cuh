@@ -6,7 +6,21 @@
 namespace swals {
 namespace fv {
 
-enum { MODE_CFL = 0, MODE_STAGE1 = 1, MODE_STAGE2 = 2 };
+// MODE_FLUX: the CFL pass of an adaptive step that also stores every
+// cell's south and west edge results (EdgePlanes) for the stage-1 update.
+enum { MODE_CFL = 0, MODE_STAGE1 = 1, MODE_STAGE2 = 2, MODE_FLUX = 3 };
+
+// Stored edge results of a stage: for cell (i, j), its south edge (between
+// rows j-1 and j) and its west edge (between columns i-1 and i): the three
+// fluxes (already multiplied by the edge length) and the explicit-source
+// contributions to the + and - side cells.
+template <typename R>
+struct EdgePlanes {
+    R *sf[3];
+    double *s_pos, *s_neg;
+    R *wf[3];
+    double *w_pos, *w_neg;
+};
 enum { FRIC_MANNING = 0, FRIC_CHEZY = 1, FRIC_NONE = 2 };
 
 template <typename R>
@@ -32,6 +46,7 @@ struct Rk2Args {
     R *side;                       // stage-2 pre-average values of the outer two rings
     double *lines;                 // flux_STG on the 4 boundary-flux lines: N[nx], E[ny], S[nx], W[ny]
     DevScalars *sc;
+    EdgePlanes<R> ep;              // MODE_FLUX output / stage-1 update input
 };
 
 template <typename R> struct Cell { R stg, dep, u, v, elv; };

@@ -119,7 +119,7 @@ __global__ void __launch_bounds__(SLANES *SWARPS, 4) rk2_stream_kernel(const Rk2
     const bool ew_lane = (lane >= 2 && lane <= 30);   // lanes whose west edge is fully determined
 
     R dt = R(0);
-    if (MODE != MODE_CFL) dt = stage_dt<R>(a);
+    if (MODE == MODE_STAGE1 || MODE == MODE_STAGE2) dt = stage_dt<R>(a);
     const R inv2 = R(1) / (a.m.dyl[0] * a.half_cfl);  // dx_cfl_half_inv(2): NS edges
     double cfl = 0.0;
     long long negfix = 0;
@@ -139,7 +139,7 @@ __global__ void __launch_bounds__(SLANES *SWARPS, 4) rk2_stream_kernel(const Rk2
         if (r + 1 <= rb + 1) nxt = load_raw<R>(a, i, r + 1);
         // Inputs that only the update reads (friction coefficient, stage-2
         // U0 and max_stage): start them towards L2 three rows early.
-        if (MODE != MODE_CFL && out_lane && r + 1 >= ra && r + 1 < rb) {
+        if ((MODE == MODE_STAGE1 || MODE == MODE_STAGE2) && out_lane && r + 1 >= ra && r + 1 < rb) {
             const int64_t o = (int64_t)(r + 1) * a.P + i;
             if (FRIC != FRIC_NONE) prefetch_l2(a.nsq + o);
             if (MODE == MODE_STAGE2) {
@@ -151,7 +151,8 @@ __global__ void __launch_bounds__(SLANES *SWARPS, 4) rk2_stream_kernel(const Rk2
         }
         c2 = c1;
         c1 = c0;
-        c0 = fix_up<R>(cur, col_valid && r >= 0 && r < ny, negfix, out_lane && r >= ra && r < rb);
+        c0 = fix_up<R>(cur, col_valid && r >= 0 && r < ny, negfix,
+                       (MODE == MODE_STAGE1 || MODE == MODE_STAGE2) && out_lane && r >= ra && r < rb);
         if (k < 2) continue;
 
         // North-south gradient of row r-1 (DE1_inner_include.f90:746-781).
@@ -178,6 +179,12 @@ __global__ void __launch_bounds__(SLANES *SWARPS, 4) rk2_stream_kernel(const Rk2
                 }
             }
         }
+        if (MODE == MODE_FLUX && out_lane && r - 1 >= ra && r - 1 < rb) {
+            // The south edge of row r-1 for the stage-1 update.
+            const int64_t o = (int64_t)(r - 1) * a.P + i;
+            a.ep.sf[0][o] = e_n.f[0]; a.ep.sf[1][o] = e_n.f[1]; a.ep.sf[2][o] = e_n.f[2];
+            a.ep.s_pos[o] = e_n.es_pos; a.ep.s_neg[o] = e_n.es_neg;
+        }
         if (k < 4) { e_s = e_n; continue; }
 
         // Row R = r-2: east-west gradient and west edge, then the update.
@@ -200,7 +207,13 @@ __global__ void __launch_bounds__(SLANES *SWARPS, 4) rk2_stream_kernel(const Rk2
                 if (i == a.n_ext) a.lines[2 * nx + ny + R_] = (double)e_w.f[0];
             }
         }
-        if (MODE != MODE_CFL) {
+        if (MODE == MODE_FLUX && out_lane) {
+            // The west edge of row R_.
+            const int64_t o = (int64_t)R_ * a.P + i;
+            a.ep.wf[0][o] = e_w.f[0]; a.ep.wf[1][o] = e_w.f[1]; a.ep.wf[2][o] = e_w.f[2];
+            a.ep.w_pos[o] = e_w.es_pos; a.ep.w_neg[o] = e_w.es_neg;
+        }
+        if (MODE == MODE_STAGE1 || MODE == MODE_STAGE2) {
             EdgeRes<R> e_e;
             e_e.f[0] = dn1(e_w.f[0]); e_e.f[1] = dn1(e_w.f[1]); e_e.f[2] = dn1(e_w.f[2]);
             e_e.es_neg = dn1(e_w.es_neg);
@@ -211,11 +224,11 @@ __global__ void __launch_bounds__(SLANES *SWARPS, 4) rk2_stream_kernel(const Rk2
     }
 
     // Warp reductions: CFL max and the negative-depth count.
-    if (a.write_cfl || MODE == MODE_CFL) {
+    if (a.write_cfl || MODE == MODE_CFL || MODE == MODE_FLUX) {
         for (int o = 16; o > 0; o >>= 1) cfl = fmax(cfl, __shfl_down_sync(FULL, cfl, o));
         if (lane == 0 && cfl > 0.0) atomicMax(&a.sc->max_dt_inv_bits, (unsigned long long)__double_as_longlong(cfl));
     }
-    if (MODE != MODE_CFL) {
+    if (MODE == MODE_STAGE1 || MODE == MODE_STAGE2) {
         for (int o = 16; o > 0; o >>= 1) negfix += __shfl_down_sync(FULL, negfix, o);
         if (lane == 0 && negfix) atomicAdd((unsigned long long *)&a.sc->negative_depth_fix_counter,
                                            (unsigned long long)negfix);
@@ -243,6 +256,7 @@ cudaError_t launch_stage_stream(const Rk2Args<R> &a, cudaStream_t s)
     SWALS_INST(R, MODE, SPH, COR, fv::FRIC_NONE)
 #define SWALS_INST_M(R, SPH, COR) \
     SWALS_INST_F(R, fv::MODE_CFL, SPH, COR) SWALS_INST_F(R, fv::MODE_STAGE1, SPH, COR) \
+    SWALS_INST_F(R, fv::MODE_FLUX, SPH, COR) \
     SWALS_INST_F(R, fv::MODE_STAGE2, SPH, COR)
 SWALS_INST_M(double, false, false)
 SWALS_INST_M(double, true, false)

@@ -111,7 +111,15 @@ struct Rk2Buffers {
     void *side;            // ring buffer used when a boundary routine is active
     void *partials;        // per-block partial sums (deterministic reductions)
     int64_t partials_len;
+    void *edges = nullptr; // stored stage-1 edge results (adaptive steps), or null
 };
+
+// Bytes of the stored stage-1 edge results of a pitch x ny grid: per cell
+// the south and west edges' three fluxes (real) and two sources (double).
+inline int64_t rk2_edge_bytes(int64_t pitch, int ny, int real_bytes)
+{
+    return 2 * (3 * (int64_t)real_bytes + 2 * 8) * pitch * (int64_t)ny + 512;
+}
 
 template <typename R>
 cudaError_t launch_rk2_step(R *const planes[3][3], int &cur, R *elv, R *max_stage, R *manning_sq, int nx, int ny,
