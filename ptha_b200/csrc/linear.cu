@@ -803,6 +803,19 @@ int linear_kernel_config()
     return cfg;
 }
 
+// Plain-step kernel for a grid: small grids (up to 0.7 M cells; L2-resident,
+// a few hundred warp strips) run faster as shared-memory tiles, whose rows
+// are all loaded at once, than as streaming warps that march down their rows
+// (measured crossover between 800^2 and 1200^2 FP64).  An explicit
+// SWALS_LINEAR_KERNEL choice wins.
+int plain_config(int nx, int ny)
+{
+    const char *e = getenv("SWALS_LINEAR_KERNEL");
+    if (e && *e) return linear_kernel_config();
+    if ((int64_t)nx * ny <= 700000) return 0;
+    return linear_kernel_config();
+}
+
 template <typename R>
 LinArgs<R> make_args(const StepPlanes<R> &p, const Metrics<R> &m, const StepConfig &c, R dt)
 {
@@ -844,7 +857,7 @@ cudaError_t launch_linear_step(const StepPlanes<R> &p, const Metrics<R> &m, cons
         hook(CAT_LINEAR_EDGE, 1);
         cudaEventRecord(aux->join, aux->stream);
         hook(CAT_LINEAR_MAIN, 0);
-        launch_main<R>(a, c, linear_kernel_config(), s);
+        launch_main<R>(a, c, plain_config(p.nx, p.ny), s);
         hook(CAT_LINEAR_MAIN, 1);
         cudaStreamWaitEvent(s, aux->join, 0);
         return cudaGetLastError();
@@ -853,7 +866,7 @@ cudaError_t launch_linear_step(const StepPlanes<R> &p, const Metrics<R> &m, cons
     linear_edge_kernel<R><<<1, 512, 0, s>>>(a, sc, c.exterior_cells_width, c.bf);
     hook(CAT_LINEAR_EDGE, 1);
     hook(CAT_LINEAR_MAIN, 0);
-    launch_main<R>(a, c, linear_kernel_config(), s);
+    launch_main<R>(a, c, plain_config(p.nx, p.ny), s);
     hook(CAT_LINEAR_MAIN, 1);
     return cudaGetLastError();
 }
