@@ -314,6 +314,22 @@ int swals_gpu_md_time(swals_multidomain *md, double *time);
 int swals_gpu_md_synchronize(swals_multidomain *md);
 int swals_gpu_md_launch_count(swals_multidomain *md, int64_t *n);
 
+/* ---- Domain diagnostics ------------------------------------------------ */
+typedef struct swals_domain_stats {
+    double maxstage, maxspeed, minstage, minspeed;
+    double energy_potential_on_rho, energy_kinetic_on_rho, energy_total_on_rho;
+} swals_domain_stats;
+/* The cells a nested domain owns (is_priority_domain_not_periodic,
+ * multidomain_mod.f90:2960-2966): mask[i + nx*j] != 0, 0-based; NULL: all
+ * cells.  Used by swals_gpu_domain_statistics. */
+int swals_gpu_set_priority_mask(swals_domain *d, const uint8_t *mask);
+/* compute_domain_statistics_new (domain_mod.f90:683-849): over the cells
+ * exterior_cells_width+1 .. n-exterior_cells_width that the priority mask
+ * keeps, the max/min stage and speed of wet cells and the potential and
+ * kinetic energy per unit density (row sums reduced by warps, rows added in
+ * order). */
+int swals_gpu_domain_statistics(swals_domain *d, swals_domain_stats *out);
+
 /* Last error message of this thread (util/stop_mod.f90 prints before stopping). */
 int swals_gpu_last_error(char *buf, size_t len);
 /* Library version string. */

@@ -169,6 +169,17 @@ class OracleDomain:
         f.argtypes = [ctypes.c_void_p]
         return f(ctypes.addressof(self.c))
 
+    def domain_statistics(self, mask=None):
+        """compute_domain_statistics_new: (maxstage, maxspeed, minstage,
+        minspeed, E_potential, E_kinetic, E_total); mask (ny, nx) of the
+        domain's own priority cells, or None."""
+        f = self._fn("domain_statistics")
+        f.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        out = np.zeros(7)
+        m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
+        f(ctypes.addressof(self.c), None if m is None else _ptr(m), _ptr(out))
+        return tuple(out)
+
     @property
     def time(self):
         return self.c.time

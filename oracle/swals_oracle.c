@@ -1060,3 +1060,75 @@ int ORACLE_FN(evolve_one_step)(oracle_domain *d, double dt, int has_dt)
     d->nsteps_advanced += 1;
     return 0;
 }
+
+#ifdef ORACLE_REAL32
+#define FLT_MAX_R FLT_MAX
+#else
+#define FLT_MAX_R DBL_MAX
+#endif
+
+/* compute_domain_statistics_new (domain_mod.f90:683-849): max/min stage and
+ * speed over wet cells and the potential / kinetic energy per density, over
+ * the cells ecw+1..n-ecw of each direction that `mask` (nx*ny, i fastest;
+ * NULL = all) marks as the domain's own priority cells.  out = {maxstage,
+ * maxspeed, minstage, minspeed, E_potential, E_kinetic, E_total}. */
+void ORACLE_FN(domain_statistics)(const oracle_domain *d, const uint8_t *mask, double *out)
+{
+    const int nx = d->nx, ny = d->ny, ecw = d->exterior_cells_width;
+    const REAL mad = MINIMUM_ALLOWED_DEPTH;
+    const int staggered = is_staggered(d);
+    const int tl = staggered && d->truely_linear &&
+                   (d->method == OR_METHOD_LINEAR || d->method == OR_METHOD_LEAPFROG_LINEAR_PLUS_NONLINEAR_FRICTION);
+    const REAL msl = (REAL)d->msl_linear;
+    REAL maxstage = -FLT_MAX_R, minstage = FLT_MAX_R, maxspeed = ZERO, minspeed = FLT_MAX_R;
+    double pe_tot = 0.0, ke_tot = 0.0;
+    for (int j = 1 + ecw; j <= ny - ecw; j++) {
+        double pe = 0.0, ke = 0.0;
+        for (int i = 1 + ecw; i <= nx - ecw; i++) {
+            if (mask && !mask[(size_t)(j - 1) * nx + (i - 1)]) continue;
+            const REAL s = UU(OR_STG, i, j), e = UU(OR_ELV, i, j);
+            const int wet = tl ? (msl > e + mad) : (s > e + mad);
+            const double w0 = (double)s + (double)e, d1 = (double)s - (double)e;
+            const double e_flow = wet ? w0 * d1 : 0.0;
+            const double w2 = (double)msl + (double)e, d3 = (double)msl - (double)e;
+            const double e_const = (msl > e + mad) ? w2 * d3 : 0.0;
+            pe = pe + (double)(d->area[j - 1] * GRAVITY * HALF) * (e_flow - e_const);
+            if (!wet) continue;
+            maxstage = (s > maxstage) ? s : maxstage;
+            minstage = (s < minstage) ? s : minstage;
+            REAL speed_sq;
+            if (staggered) {
+                REAL dE, dN;
+                if (tl) {
+                    dE = HALF * ((msl - UU(OR_ELV, i, j)) + (msl - UU(OR_ELV, i + 1, j)));
+                    dN = HALF * ((msl - UU(OR_ELV, i, j)) + (msl - UU(OR_ELV, i, j + 1)));
+                } else {
+                    dE = HALF * ((UU(OR_STG, i, j) - UU(OR_ELV, i, j)) + (UU(OR_STG, i + 1, j) - UU(OR_ELV, i + 1, j)));
+                    dN = HALF * ((UU(OR_STG, i, j) - UU(OR_ELV, i, j)) + (UU(OR_STG, i, j + 1) - UU(OR_ELV, i, j + 1)));
+                }
+                const REAL dEi = (dE > mad) ? ONE / dE : ZERO;
+                const REAL dNi = (dN > mad) ? ONE / dN : ZERO;
+                const REAL uh = UU(OR_UH, i, j), vh = UU(OR_VH, i, j);
+                speed_sq = uh * uh * (dEi * dEi) + vh * vh * (dNi * dNi);
+                ke = ke + (double)(HALF * (d->area[j - 1] * uh * uh * dEi +
+                                           HALF * (d->area[j - 1] + d->area[j]) * vh * vh * dNi));
+            } else {
+                const REAL dc = s - e;
+                const REAL uh = UU(OR_UH, i, j), vh = UU(OR_VH, i, j);
+                speed_sq = (uh * uh + vh * vh) / (dc * dc);
+                ke = ke + (double)(d->area[j - 1] * HALF * dc * speed_sq);
+            }
+            maxspeed = (speed_sq > maxspeed) ? speed_sq : maxspeed;
+            minspeed = (speed_sq < minspeed) ? speed_sq : minspeed;
+        }
+        pe_tot = pe_tot + pe;
+        ke_tot = ke_tot + ke;
+    }
+    out[0] = (double)maxstage;
+    out[1] = (double)(REAL)sqrt((double)maxspeed);
+    out[2] = (double)minstage;
+    out[3] = (double)(REAL)sqrt((double)minspeed);
+    out[4] = pe_tot;
+    out[5] = ke_tot;
+    out[6] = ke_tot + pe_tot;
+}

@@ -160,6 +160,8 @@ double ORACLE_FN(pow_friction)(double x, int32_t chezy);
 double ORACLE_FN(cosh_cr)(double a);
 void ORACLE_FN(boundary_function)(const oracle_domain *d, double t, int32_t i, int32_t j, REAL *out4);
 
+void ORACLE_FN(domain_statistics)(const oracle_domain *d, const uint8_t *mask, double *out);
+
 /* Nesting (swals_nesting_oracle.c). */
 int  ORACLE_FN(nest_comm_init)(oracle_nest_comm *c, const double my_dx[2], const double neighbour_dx[2],
                                const int32_t send_inds[6], const int32_t recv_inds[6], int32_t send_only,

@@ -462,6 +462,8 @@ int swals_gpu_domain_destroy(swals_domain *d)
     if (d->d_sites) cudaFree(d->d_sites);
     if (d->d_records) cudaFree(d->d_records);
     if (d->ws) cudaFree(d->ws);
+    if (d->prio_mask) cudaFree(d->prio_mask);
+    if (d->stats_buf) cudaFree(d->stats_buf);
     drop_step_graph(d);
     for (auto &g : d->adj_graph)
         if (g) cudaGraphExecDestroy(g);
@@ -700,6 +702,49 @@ int swals_gpu_stationary_timestep_max(swals_domain *d, double *out)
     if (d->method == M_RK2N) *out = *out * 0.5 * (5 - 1.0);
     else if (d->method == M_CLIFFS) (void)0;
     else *out = *out * 0.5;
+    return SWALS_OK;
+}
+
+int swals_gpu_set_priority_mask(swals_domain *d, const uint8_t *mask)
+{
+    if (!d) return fail(SWALS_ERR_INVALID_ARGUMENT, "NULL domain");
+    CK(cudaStreamSynchronize(d->stream));
+    if (!mask) {
+        if (d->prio_mask) cudaFree(d->prio_mask);
+        d->prio_mask = nullptr;
+        return SWALS_OK;
+    }
+    const size_t n = (size_t)d->nx * d->ny;
+    if (!d->prio_mask) CK(cudaMalloc(&d->prio_mask, n));
+    CK(cudaMemcpy(d->prio_mask, mask, n, cudaMemcpyHostToDevice));
+    return SWALS_OK;
+}
+
+int swals_gpu_domain_statistics(swals_domain *d, swals_domain_stats *out)
+{
+    if (!d || !out) return fail(SWALS_ERR_INVALID_ARGUMENT, "bad argument");
+    if (!d->stats_buf) CK(cudaMalloc(&d->stats_buf, sizeof(double) * (6 * (size_t)d->ny + 8)));
+    const int ecw = d->desc.exterior_cells_width;
+    const int staggered = (d->method == M_LINEAR) ? 1 : 0;
+    const int tl = staggered && d->desc.linear_solver_is_truely_linear;
+    double *o7 = d->stats_buf + 6 * (size_t)d->ny;
+    cudaError_t e;
+    if (d->fp64)
+        e = swals::launch_domain_statistics<double>(
+            d->nx, d->ny, d->pitch, (const double *)d->planes[d->cur][0], (const double *)d->planes[d->cur][1],
+            (const double *)d->planes[d->cur][2], (const double *)d->elv, (const double *)d->metric[2], d->prio_mask,
+            ecw, staggered, tl, d->desc.msl_linear, d->stats_buf, o7, d->stream);
+    else
+        e = swals::launch_domain_statistics<float>(
+            d->nx, d->ny, d->pitch, (const float *)d->planes[d->cur][0], (const float *)d->planes[d->cur][1],
+            (const float *)d->planes[d->cur][2], (const float *)d->elv, (const float *)d->metric[2], d->prio_mask,
+            ecw, staggered, tl, d->desc.msl_linear, d->stats_buf, o7, d->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "domain statistics");
+    double h[7];
+    CK(cudaMemcpyAsync(h, o7, sizeof(h), cudaMemcpyDeviceToHost, d->stream));
+    CK(cudaStreamSynchronize(d->stream));
+    out->maxstage = h[0]; out->maxspeed = h[1]; out->minstage = h[2]; out->minspeed = h[3];
+    out->energy_potential_on_rho = h[4]; out->energy_kinetic_on_rho = h[5]; out->energy_total_on_rho = h[6];
     return SWALS_OK;
 }
 

@@ -44,6 +44,10 @@ struct swals_domain {
     std::vector<int> h_sites;
     // launch accounting and per-kernel event timers
     int64_t launches = 0;
+    // Diagnostics: the domain's own priority cells (nx*ny bytes, i fastest)
+    // and the statistics scratch.
+    uint8_t *prio_mask = nullptr;
+    double *stats_buf = nullptr;
     // Side stream for the leapfrog's bookkeeping kernel.
     swals::AuxStream aux;
     // Replayed graph of a few steps for evolve_steps.

@@ -24,6 +24,8 @@ template <typename R> struct K {
     static __host__ __device__ __forceinline__ R zero() { return R(0.0); }
     static __host__ __device__ __forceinline__ R min_depth() { return R(1.0e-05); }
     static __host__ __device__ __forceinline__ R wall_elevation() { return R(1.0e+6); }
+    // HUGE(1.0_dp) of the state precision.
+    static __host__ __device__ __forceinline__ R huge() { return sizeof(R) == 8 ? R(1.7976931348623157e308) : R(3.4028234663852886e38f); }
     static __host__ __device__ __forceinline__ R limiter_coef1() { return R(0.1); }
     static __host__ __device__ __forceinline__ R limiter_coef2() { return R(0.3); }
     static __host__ __device__ __forceinline__ R limiter_coef3() { return R(100.0); }

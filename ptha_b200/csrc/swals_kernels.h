@@ -45,6 +45,13 @@ struct StepConfig {
     int exterior_cells_width;
 };
 
+// compute_domain_statistics_new: rows6 is 6*ny doubles of scratch; out7 (device)
+// receives {maxstage, maxspeed, minstage, minspeed, E_pot, E_kin, E_total}.
+template <typename R>
+cudaError_t launch_domain_statistics(int nx, int ny, int64_t P, const R *stg, const R *uh, const R *vh, const R *elv,
+                                     const R *area, const uint8_t *mask, int ecw, int staggered, int tl, double msl,
+                                     double *rows6, double *out7, cudaStream_t s);
+
 // Gauges (0-based i, j site pairs) inside the window [i0, i1] x [r0, r1]:
 // bit q set for gauge q.  Streaming kernels compute it once per warp segment
 // so the per-row check costs nothing where there is no gauge.  With more than

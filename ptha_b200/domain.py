@@ -203,6 +203,23 @@ class Domain:
         return self._scalar(self._L.swals_gpu_volume_interior)
 
     # --------------------------------------------------------------- gauges
+    def set_priority_mask(self, mask=None):
+        """The cells this domain owns in a multidomain, (ny, nx) booleans, or None."""
+        if mask is None:
+            check(self._L.swals_gpu_set_priority_mask(self._h, None))
+            return
+        m = np.ascontiguousarray(np.asarray(mask).astype(np.uint8).reshape(self.nx[1], self.nx[0]))
+        check(self._L.swals_gpu_set_priority_mask(self._h, _p(m)))
+
+    def compute_domain_statistics(self):
+        """compute_domain_statistics_new: dict of maxstage, maxspeed, minstage,
+        minspeed, energy_potential_on_rho, energy_kinetic_on_rho, energy_total_on_rho."""
+        out = (ctypes.c_double * 7)()
+        check(self._L.swals_gpu_domain_statistics(self._h, out))
+        keys = ["maxstage", "maxspeed", "minstage", "minspeed", "energy_potential_on_rho",
+                "energy_kinetic_on_rho", "energy_total_on_rho"]
+        return dict(zip(keys, list(out)))
+
     def gauges_setup(self, xy, capacity):
         xy = np.ascontiguousarray(xy, dtype=np.float64).reshape(-1, 2)
         self._n_gauges = xy.shape[0]
