@@ -329,6 +329,9 @@ int swals_gpu_set_priority_mask(swals_domain *d, const uint8_t *mask);
  * kinetic energy per unit density (row sums reduced by warps, rows added in
  * order). */
 int swals_gpu_domain_statistics(swals_domain *d, swals_domain_stats *out);
+/* volume_in_priority_domain (domain_mod.f90:1851-1889): volume_interior over
+ * the cells the priority mask keeps (all cells without a mask). */
+int swals_gpu_volume_in_priority_domain(swals_domain *d, double *out);
 
 /* Last error message of this thread (util/stop_mod.f90 prints before stopping). */
 int swals_gpu_last_error(char *buf, size_t len);

@@ -169,6 +169,13 @@ class OracleDomain:
         f.argtypes = [ctypes.c_void_p]
         return f(ctypes.addressof(self.c))
 
+    def volume_in_priority_domain(self, mask=None):
+        """volume_interior over the cells of mask (ny, nx), or all cells."""
+        f = self._fn("volume_in_priority_domain", ctypes.c_double)
+        f.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
+        return f(ctypes.addressof(self.c), None if m is None else _ptr(m))
+
     def domain_statistics(self, mask=None):
         """compute_domain_statistics_new: (maxstage, maxspeed, minstage,
         minspeed, E_potential, E_kinetic, E_total); mask (ny, nx) of the

@@ -394,6 +394,25 @@ double ORACLE_FN(volume_interior)(const oracle_domain *d)
     return vol;
 }
 
+/* volume_in_priority_domain (domain_mod.f90:1851-1889): the interior volume
+ * over the cells of the domain's priority mask (mask (ny, nx) row-major,
+ * 1 = the domain's own priority cell; NULL = every cell). */
+double ORACLE_FN(volume_in_priority_domain)(const oracle_domain *d, const uint8_t *mask)
+{
+    const int nx = d->nx, ny = d->ny;
+    int n_ext = d->exterior_cells_width;
+    double vol = 0.0;
+    for (int j = 1 + n_ext; j <= ny - n_ext; j++) {
+        double local_sum = 0.0;
+        for (int i = 1 + n_ext; i <= nx - n_ext; i++) {
+            if (mask && !mask[(size_t)(j - 1) * nx + (i - 1)]) continue;
+            local_sum += (double)UU(OR_STG, i, j) - (double)UU(OR_ELV, i, j);
+        }
+        vol = vol + (double)((double)d->area[j - 1] * local_sum);
+    }
+    return vol;
+}
+
 /* ------------------------------------------------------------------------ */
 /* Linear leapfrog: domain_mod_linear_solver_include.f90:58-571 */
 /* boundary_flux_integral_tstep (nested_grid_comms_mod.f90:2300-2469) for

@@ -149,6 +149,7 @@ void ORACLE_FN(update_max_quantities)(oracle_domain *d);
 double ORACLE_FN(linear_timestep_max)(const oracle_domain *d);
 double ORACLE_FN(nonlinear_stationary_timestep_max)(const oracle_domain *d);
 double ORACLE_FN(volume_interior)(const oracle_domain *d);
+double ORACLE_FN(volume_in_priority_domain)(const oracle_domain *d, const uint8_t *mask);
 void ORACLE_FN(compute_depth_and_velocity)(oracle_domain *d);
 double ORACLE_FN(compute_fluxes_DE1_low_fr_diffusion)(oracle_domain *d);
 void ORACLE_FN(limited_gradient_dx_vectorized)(const REAL *U_local, const REAL *U_lower,

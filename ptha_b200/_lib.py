@@ -43,7 +43,7 @@ EXPORTED = [
     "swals_gpu_md_recv_halos", "swals_gpu_md_flux_correction", "swals_gpu_md_buffer_size",
     "swals_gpu_md_download_buffer", "swals_gpu_md_download_flux", "swals_gpu_md_time", "swals_gpu_md_synchronize",
     "swals_gpu_md_launch_count", "swals_gpu_md_capture_graph", "swals_gpu_md_replay",
-    "swals_gpu_set_priority_mask", "swals_gpu_domain_statistics",
+    "swals_gpu_set_priority_mask", "swals_gpu_domain_statistics", "swals_gpu_volume_in_priority_domain",
 ]
 TIMER_NAMES = ["cfl", "fv_stage1", "boundary1", "fv_stage2", "boundary2", "finalize", "leapfrog_edge",
                "leapfrog_step", "gauges", "max_stage"]
@@ -154,6 +154,7 @@ def lib():
         "swals_gpu_md_launch_count": [vp, ctypes.POINTER(i64)],
         "swals_gpu_md_capture_graph": [vp, i32, dbl], "swals_gpu_md_replay": [vp, i32],
         "swals_gpu_set_priority_mask": [vp, vp], "swals_gpu_domain_statistics": [vp, vp],
+        "swals_gpu_volume_in_priority_domain": [vp, ctypes.POINTER(dbl)],
     }
     for name, args in sig.items():
         f = getattr(L, name)

@@ -748,7 +748,7 @@ int swals_gpu_domain_statistics(swals_domain *d, swals_domain_stats *out)
     return SWALS_OK;
 }
 
-int swals_gpu_volume_interior(swals_domain *d, double *out)
+static int volume_impl(swals_domain *d, double *out, const uint8_t *mask)
 {
     if (!d || !out) return fail(SWALS_ERR_INVALID_ARGUMENT, "NULL argument");
     cudaError_t e;
@@ -756,15 +756,23 @@ int swals_gpu_volume_interior(swals_domain *d, double *out)
     if (d->fp64)
         e = swals::launch_volume_interior<double>(d->nx, d->ny, d->pitch, (const double *)d->planes[d->cur][0],
                                                   (const double *)d->elv, (const double *)d->metric[2], n_ext,
-                                                  d->scratch, d->d_out, d->stream);
+                                                  d->scratch, d->d_out, d->stream, mask);
     else
         e = swals::launch_volume_interior<float>(d->nx, d->ny, d->pitch, (const float *)d->planes[d->cur][0],
                                                  (const float *)d->elv, (const float *)d->metric[2], n_ext,
-                                                 d->scratch, d->d_out, d->stream);
+                                                 d->scratch, d->d_out, d->stream, mask);
     if (e != cudaSuccess) return cuda_fail(e, "volume_interior");
     CK(cudaMemcpyAsync(out, d->d_out, sizeof(double), cudaMemcpyDeviceToHost, d->stream));
     CK(cudaStreamSynchronize(d->stream));
     return SWALS_OK;
+}
+
+int swals_gpu_volume_interior(swals_domain *d, double *out) { return volume_impl(d, out, nullptr); }
+
+int swals_gpu_volume_in_priority_domain(swals_domain *d, double *out)
+{
+    if (!d) return fail(SWALS_ERR_INVALID_ARGUMENT, "NULL domain");
+    return volume_impl(d, out, d->prio_mask);
 }
 
 int swals_gpu_gauges_setup(swals_domain *d, const double *xy, int32_t n, int32_t capacity)

@@ -10,7 +10,8 @@ namespace {
 // One warp per row: fixed-order warp tree of (double)STG - (double)ELV, then
 // one thread adds area(j) * row sum in row order (deterministic).
 template <typename R>
-__global__ void row_volume_kernel(int nx, int ny, int64_t P, const R *stg, const R *elv, int n_ext, double *row_sums)
+__global__ void row_volume_kernel(int nx, int ny, int64_t P, const R *stg, const R *elv, int n_ext, double *row_sums,
+                                  const uint8_t *mask)
 {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -18,6 +19,7 @@ __global__ void row_volume_kernel(int nx, int ny, int64_t P, const R *stg, const
     if (r > ny - n_ext - 1) return;
     double acc = 0.0;
     for (int i = n_ext + lane; i <= nx - n_ext - 1; i += 32) {
+        if (mask && !mask[(int64_t)r * nx + i]) continue;   // volume_in_priority_domain's mask
         const int64_t o = (int64_t)r * P + i;
         acc += (double)stg[o] - (double)elv[o];
     }
@@ -190,13 +192,13 @@ template cudaError_t launch_domain_statistics<float>(int, int, int64_t, const fl
 
 template <typename R>
 cudaError_t launch_volume_interior(int nx, int ny, int64_t pitch, const R *stg, const R *elv, const R *area,
-                                   int n_ext, double *row_sums, double *out, cudaStream_t s)
+                                   int n_ext, double *row_sums, double *out, cudaStream_t s, const uint8_t *mask)
 {
     const int rows = ny - 2 * n_ext;
     if (rows > 0) {
         const int threads = 256;
         const int blocks = (rows * 32 + threads - 1) / threads;
-        row_volume_kernel<R><<<blocks, threads, 0, s>>>(nx, ny, pitch, stg, elv, n_ext, row_sums);
+        row_volume_kernel<R><<<blocks, threads, 0, s>>>(nx, ny, pitch, stg, elv, n_ext, row_sums, mask);
     }
     volume_total_kernel<R><<<1, 32, 0, s>>>(ny, n_ext, area, row_sums, out);
     return cudaGetLastError();
@@ -216,9 +218,10 @@ cudaError_t launch_timestep_max(int nx, int ny, int64_t pitch, const R *stg, con
 }
 
 template cudaError_t launch_volume_interior<double>(int, int, int64_t, const double *, const double *,
-                                                    const double *, int, double *, double *, cudaStream_t);
+                                                    const double *, int, double *, double *, cudaStream_t,
+                                                    const uint8_t *);
 template cudaError_t launch_volume_interior<float>(int, int, int64_t, const float *, const float *, const float *,
-                                                   int, double *, double *, cudaStream_t);
+                                                   int, double *, double *, cudaStream_t, const uint8_t *);
 template cudaError_t launch_timestep_max<double>(int, int, int64_t, const double *, const double *, const double *,
                                                  const double *, double, int, double, double *, int, double *,
                                                  cudaStream_t);

@@ -137,7 +137,8 @@ cudaError_t launch_rk2_step(R *const planes[3][3], int &cur, R *elv, R *max_stag
 // Reductions used by diagnostics.
 template <typename R>
 cudaError_t launch_volume_interior(int nx, int ny, int64_t pitch, const R *stg, const R *elv, const R *area,
-                                   int n_ext, double *row_sums, double *out, cudaStream_t s);
+                                   int n_ext, double *row_sums, double *out, cudaStream_t s,
+                                   const uint8_t *mask = nullptr);
 template <typename R>
 cudaError_t launch_timestep_max(int nx, int ny, int64_t pitch, const R *stg, const R *elv, const R *dxb,
                                 const R *dyl, double msl, int linear, double cfl, double *block_min,

@@ -211,6 +211,10 @@ class Domain:
         m = np.ascontiguousarray(np.asarray(mask).astype(np.uint8).reshape(self.nx[1], self.nx[0]))
         check(self._L.swals_gpu_set_priority_mask(self._h, _p(m)))
 
+    def volume_in_priority_domain(self):
+        """volume_interior over the cells set_priority_mask kept."""
+        return self._scalar(self._L.swals_gpu_volume_in_priority_domain)
+
     def compute_domain_statistics(self):
         """compute_domain_statistics_new: dict of maxstage, maxspeed, minstage,
         minspeed, energy_potential_on_rho, energy_kinetic_on_rho, energy_total_on_rho."""

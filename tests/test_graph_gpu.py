@@ -15,7 +15,10 @@ def _linear():
 
 
 def _rk2():
-    kw, U, gauges, nsq = workloads.rk2_beach(n=96, dx=10.0 * 2048 / 96, toe=17580.0 * 96 / 2048)
+    kw, U, _, nsq = workloads.rk2_beach(n=96, dx=10.0 * 2048 / 96, toe=17580.0 * 96 / 2048)
+    lw = kw["lw"]
+    g = [0.25, 0.5, 0.75]
+    gauges = [[fx * lw[0], fy * lw[1]] for fy in g for fx in g]
     return kw, U, gauges, nsq
 
 

@@ -190,3 +190,33 @@ def test_md_graph_replay_matches_steps():
         np.testing.assert_array_equal(a, b)
     assert res[0][1] == res[1][1]
     assert res[0][2] == res[1][2] == pytest.approx(60.0)
+
+
+def test_mixed_precision_nest_close_to_fp64():
+    """An FP32 'linear' parent with an FP64 'rk2' child (the precisions of
+    the nested configuration) stays within FP32 round-off of the all-FP64
+    oracle over several md steps."""
+    specs = two_level_nest(ratio=3, child_method="rk2", parent_method="linear")
+    kw = [dict(real_bytes=4), dict(real_bytes=8)]
+    md = Multidomain(specs, domain_kwargs=kw, use_wetdry_limiting=True, flux_correction=True)
+    odoms = [OracleDomain(s.nx[0], s.nx[1], s.lw, s.lower_left, timestepping_method=s.timestepping_method,
+                          boundary_exterior=tuple(not b for b in s.is_nesting_boundary)) for s in specs]
+    omd = OracleMultidomain(odoms, [s.timestepping_method for s in specs], [s.dx for s in specs], md.exchanges,
+                            refinement=[s.timestepping_refinement_factor for s in specs],
+                            priority_index=[s.priority_domain_index for s in specs], flux_correction=True)
+    for d, od, U in zip(md.domains, odoms, _ic(specs, False)):
+        d.set_U(U)
+        od.U[:] = U
+        if d.timestepping_method == "rk2":
+            d.set_manning_squared(0.025 ** 2)
+            od.manning_squared[:] = 0.025 ** 2
+    dt = 10.0
+    for _ in range(8):
+        md.evolve_one_step(dt)
+        omd.evolve_one_step(dt)
+    for k, (d, od) in enumerate(zip(md.domains, odoms)):
+        U = d.get_U().astype(np.float64)
+        wet = od.U[3] < 0
+        err = np.abs(U[0] - od.U[0])[wet].max()
+        assert err <= 2e-5 * max(1.0, np.abs(od.U[0][wet]).max()), (k, err)
+    md.close()

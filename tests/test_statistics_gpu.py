@@ -1,7 +1,7 @@
-"""compute_domain_statistics_new on the GPU against the oracle: max/min
-stage and speed equal exactly (order-free), the energies within 1e-12
-relative (the GPU adds each row's terms in a warp tree, the reference in
-column order)."""
+"""compute_domain_statistics_new and volume_in_priority_domain on the GPU
+against the oracle: max/min stage and speed equal exactly (order-free), the
+energies and the volume within 1e-12 relative (the GPU adds each row's terms
+in a warp tree, the reference in column order)."""
 import numpy as np
 import pytest
 
@@ -23,6 +23,9 @@ def _check(g, o, mask=None):
         assert s[k] == ref, (k, s[k], ref)
     for k, ref in zip(keys[4:], r[4:]):
         assert s[k] == pytest.approx(ref, rel=1e-12, abs=1e-9 * max(1.0, abs(r[6]))), (k, s[k], ref)
+    # volume_in_priority_domain: row sums in a warp tree vs column order.
+    v = g.volume_in_priority_domain()
+    assert v == pytest.approx(o.volume_in_priority_domain(mask), rel=1e-12, abs=1e-12 * abs(o.volume_interior()))
 
 
 def test_linear_statistics():
