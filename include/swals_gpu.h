@@ -50,6 +50,9 @@ extern "C" {
 #define SWALS_BC_NONE                              0 /* walls via high elevation, no routine */
 #define SWALS_BC_TRANSMISSIVE                      1 /* transmissive_boundary, boundary_mod.f90:21-75 */
 #define SWALS_BC_STAGE_TRANSMISSIVE_NORMAL_MOMENTUM 2 /* boundary_mod.f90:78-163 */
+#define SWALS_BC_FLATHER                           3 /* flather_boundary, boundary_mod.f90:502-730; the
+                                                        'outside' state from boundary_function_kind,
+                                                        or stage max(msl_linear, elev) at rest (SWALS_BF_NONE) */
 
 /* Device-native boundary_function kinds (domain_mod.f90:594-633 interface). */
 #define SWALS_BF_NONE                   0

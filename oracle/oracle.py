@@ -22,7 +22,7 @@ METHODS = {
     "rk2": 1, "rk2n": 2, "midpoint": 3, "euler": 4, "linear": 5,
     "leapfrog_linear_plus_nonlinear_friction": 6, "cliffs": 7, "leapfrog_nonlinear": 8,
 }
-BC_NONE, BC_TRANSMISSIVE, BC_STAGE_TRANSMISSIVE_NORMAL_MOMENTUM = 0, 1, 2
+BC_NONE, BC_TRANSMISSIVE, BC_STAGE_TRANSMISSIVE_NORMAL_MOMENTUM, BC_FLATHER = 0, 1, 2, 3
 BF_SOLITARY_WEST_WALLS = 1
 NEG_HUGE = -np.finfo(np.float64).max
 

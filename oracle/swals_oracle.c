@@ -279,6 +279,55 @@ static int is_staggered(const oracle_domain *d)
            d->method == OR_METHOD_LEAPFROG_NONLINEAR;
 }
 
+/* flather_boundary (boundary_mod.f90:502-730) at ring cell (i, j), 1-based,
+ * whose inner neighbour is (ii, jj).  ew: 1 on the west/east edges (normal
+ * momentum UH), 0 on the south/north edges (VH); sg: +1 on west/south,
+ * -1 on east/north.  The 'outside' state is the boundary function's, or
+ * stage max(msl_linear, elevation) at rest without one. */
+static void flather_cell(oracle_domain *d, int i, int j, int ii, int jj, int ew, int sg)
+{
+    const int nx = d->nx, ny = d->ny;
+    (void)ny;
+    const int kn = ew ? OR_UH : OR_VH, kt = ew ? OR_VH : OR_UH;
+    REAL depth_inside = UU(OR_STG, ii, jj) - UU(OR_ELV, ii, jj);
+    REAL stage_outside, u_outside, depth_outside;
+    if (d->bf_kind == OR_BF_NONE) {
+        REAL msl = (REAL)d->msl_linear, e = UU(OR_ELV, i, j);
+        stage_outside = (msl > e) ? msl : e;
+        u_outside = ZERO;
+        depth_outside = stage_outside - UU(OR_ELV, i, j);
+    } else {
+        REAL bt[4];
+        ORACLE_FN(boundary_function)(d, d->time, i, j, bt);
+        stage_outside = bt[0];
+        depth_outside = bt[0] - bt[3];
+        if (depth_outside <= MINIMUM_ALLOWED_DEPTH) u_outside = ZERO;
+        else u_outside = bt[ew ? 1 : 2] / depth_outside;
+    }
+    if (depth_inside > MINIMUM_ALLOWED_DEPTH && depth_outside > MINIMUM_ALLOWED_DEPTH) {
+        REAL depth_inside_inv = ONE / depth_inside;
+        REAL sqrt_g_on_di = (REAL)sqrt(GRAVITY * depth_inside_inv);
+        REAL w1, w2, w3;
+        if (sg > 0) {
+            w1 = u_outside + sqrt_g_on_di * stage_outside;
+            w2 = (UU(kn, ii, jj) < ZERO) ? UU(kt, ii, jj) * depth_inside_inv : ZERO;
+            w3 = UU(kn, ii, jj) * depth_inside_inv - sqrt_g_on_di * UU(OR_STG, ii, jj);
+            UU(OR_STG, i, j) = (-w3 + w1) / ((REAL)2.0 * sqrt_g_on_di);
+        } else {
+            w1 = u_outside - sqrt_g_on_di * stage_outside;
+            w2 = (UU(kn, ii, jj) > ZERO) ? UU(kt, ii, jj) * depth_inside_inv : ZERO;
+            w3 = UU(kn, ii, jj) * depth_inside_inv + sqrt_g_on_di * UU(OR_STG, ii, jj);
+            UU(OR_STG, i, j) = (w3 - w1) / ((REAL)2.0 * sqrt_g_on_di);
+        }
+        UU(kn, i, j) = (w3 + w1) * HALF * depth_inside;
+        UU(kt, i, j) = w2 * depth_inside;
+    } else {
+        UU(OR_STG, i, j) = stage_outside;
+        UU(OR_UH, i, j) = ZERO;
+        UU(OR_VH, i, j) = ZERO;
+    }
+}
+
 static void update_boundary(oracle_domain *d)
 {
     const int nx = d->nx, ny = d->ny;
@@ -294,6 +343,16 @@ static void update_boundary(oracle_domain *d)
                 if (d->boundary_exterior[2]) UU(k, i, 1) = UU(k, i, 2);
                 if (d->boundary_exterior[0]) UU(k, i, ny) = UU(k, i, ny - 1);
             }
+    } else if (d->bc_kind == OR_BC_FLATHER) {
+        /* West/east over every row, then south/north over every column. */
+        for (int j = 1; j <= ny; j++) {
+            if (d->boundary_exterior[3]) flather_cell(d, 1, j, 2, j, 1, 1);
+            if (d->boundary_exterior[1]) flather_cell(d, nx, j, nx - 1, j, 1, -1);
+        }
+        for (int i = 1; i <= nx; i++) {
+            if (d->boundary_exterior[2]) flather_cell(d, i, 1, i, 2, 0, 1);
+            if (d->boundary_exterior[0]) flather_cell(d, i, ny, i, ny - 1, 0, -1);
+        }
     } else if (d->bc_kind == OR_BC_STAGE_TRANSMISSIVE_NORMAL_MOMENTUM) {
         /* boundary_mod.f90:94-161 */
         int stag = is_staggered(d);

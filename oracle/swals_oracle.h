@@ -51,11 +51,14 @@ enum {
 enum {
     OR_BC_NONE = 0,                               /* walls via elevation */
     OR_BC_TRANSMISSIVE = 1,                       /* boundary_mod.f90:21-75 */
-    OR_BC_STAGE_TRANSMISSIVE_NORMAL_MOMENTUM = 2  /* boundary_mod.f90:78-163 */
+    OR_BC_STAGE_TRANSMISSIVE_NORMAL_MOMENTUM = 2, /* boundary_mod.f90:78-163 */
+    OR_BC_FLATHER = 3                             /* boundary_mod.f90:502-730 */
 };
 
-/* Analytic boundary functions for OR_BC_STAGE_TRANSMISSIVE_NORMAL_MOMENTUM. */
+/* Analytic boundary functions (domain%boundary_function) for
+ * OR_BC_STAGE_TRANSMISSIVE_NORMAL_MOMENTUM and OR_BC_FLATHER. */
 enum {
+    OR_BF_NONE = 0,                /* not associated */
     OR_BF_SOLITARY_WEST_WALLS = 1  /* solitary wave on the west edge, walls elsewhere */
 };
 

@@ -18,7 +18,7 @@ ERRORS = {
     7: "SWALS_ERR_TIMESTEP_REQUIRED", 8: "SWALS_ERR_OUT_OF_MEMORY", 9: "SWALS_ERR_NO_DEVICE",
     10: "SWALS_ERR_CAPACITY",
 }
-BC_NONE, BC_TRANSMISSIVE, BC_STAGE_TRANSMISSIVE_NORMAL_MOMENTUM = 0, 1, 2
+BC_NONE, BC_TRANSMISSIVE, BC_STAGE_TRANSMISSIVE_NORMAL_MOMENTUM, BC_FLATHER = 0, 1, 2, 3
 BF_NONE, BF_SOLITARY_WEST_WALLS = 0, 1
 FRICTION_MANNING, FRICTION_CHEZY = 0, 1
 

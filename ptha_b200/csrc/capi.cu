@@ -325,8 +325,12 @@ int swals_gpu_domain_create(const swals_domain_desc *desc, swals_domain **out)
         return fail(SWALS_ERR_INVALID_ARGUMENT, "real_bytes must be 4 or 8");
     if (desc->coriolis && !desc->spherical)
         return fail(SWALS_ERR_INVALID_ARGUMENT, "Cannot define preprocessing flag CORIOLIS without also defining SPHERICAL");
-    if (desc->boundary_kind < 0 || desc->boundary_kind > 2)
+    if (desc->boundary_kind < 0 || desc->boundary_kind > 3)
         return fail(SWALS_ERR_INVALID_ARGUMENT, "unknown boundary_kind %d", desc->boundary_kind);
+    if (desc->boundary_function_kind < 0 || desc->boundary_function_kind > 1)
+        return fail(SWALS_ERR_UNSUPPORTED_CALLBACK, "unknown boundary_function_kind %d", desc->boundary_function_kind);
+    if (method == M_LINEAR && desc->boundary_kind == SWALS_BC_FLATHER && desc->exterior_cells_width == 1)
+        return fail(SWALS_ERR_UNSUPPORTED, "flather_boundary with the linear solver needs exterior_cells_width >= 2");
     if (method == M_LINEAR && desc->boundary_kind == SWALS_BC_TRANSMISSIVE)
         return fail(SWALS_ERR_UNSUPPORTED, "transmissive_boundary with the staggered linear solver is not implemented");
     if (desc->boundary_kind == SWALS_BC_STAGE_TRANSMISSIVE_NORMAL_MOMENTUM && desc->boundary_function_kind != 1)
@@ -420,6 +424,7 @@ int swals_gpu_domain_create(const swals_domain_desc *desc, swals_domain **out)
     d->scratch = (double *)p; p += scratch_bytes;
     d->d_out = (double *)p; p += al(64);
     d->edges = edge_bytes ? (void *)p : nullptr; p += edge_bytes;
+    d->cfg.ring = d->side;   // the staggered solver's Flather ring buffer (the side buffer is for FV stages)
 
     int rc = SWALS_OK;
     if ((e = cudaMemsetAsync(d->pool, 0, total, d->stream)) != cudaSuccess) rc = cuda_fail(e, "memset");

@@ -37,7 +37,8 @@ struct LinArgs {
     StepPlanes<R> p;        // planes of instance 0
     Metrics<R> m;
     int xl, xu, yl, yu;
-    int bc_stage;
+    int bc_stage;           // the ring stage is in stg_o before the step kernel runs
+    int bc_fn_ring;         // the edge kernel writes it from the boundary function
     int bext[4];
     R dt;
     R msl;
@@ -576,7 +577,7 @@ __global__ void __launch_bounds__(512) linear_edge_kernel(const LinArgs<R> a, De
     const int64_t P = a.p.pitch;
     const double time0 = sc->time;
     const double t_half = time0 + (double)(a.dt * K<R>::half());
-    if (a.bc_stage) {
+    if (a.bc_fn_ring) {
         const int nring = 2 * nx + 2 * ny;
         for (int q = threadIdx.x; q < nring; q += blockDim.x) {
             int i, r, side;
@@ -632,6 +633,176 @@ __global__ void __launch_bounds__(512) linear_edge_kernel(const LinArgs<R> a, De
         sc->evolve_step_dt = sc->time - time0;
         sc->nsteps_advanced += 1;
     }
+}
+
+// ---------------------------------------------------------------------------
+// flather_boundary on the staggered grid (boundary_mod.f90:502-730, called
+// between the stage and the momentum sweep, linear_solver_include.f90:122).
+// The fused step kernels read the old momenta once for both sweeps, but the
+// momentum sweep has to see the ring's momenta as the boundary routine left
+// them.  So with Flather a step is three launches:
+//   1. linear_flather_ring_kernel: the ring values from the inner cells'
+//      swept stage (recomputed with the sweep's own expression) and old
+//      momenta; the ring stage goes to the output stage plane, where the step
+//      kernel keeps it as it does for a stage boundary, and the ring momenta
+//      to a ring buffer;
+//   2. the step kernel, unchanged;
+//   3. linear_flather_fix_kernel: the momentum update of the outer two rings
+//      -- the only cells whose update reads a ring momentum (own value or a
+//      Coriolis average) -- again, from the new stage and the ring buffer.
+// Ring cell q: rows 0 and ny-1 in full (q < 2 nx), then columns 0 and nx-1 of
+// rows 1 .. ny-2.
+__device__ __forceinline__ int ring_index(int i, int r, int nx, int ny)
+{
+    if (r == 0) return i;
+    if (r == ny - 1) return nx + i;
+    return 2 * nx + ((i == 0) ? (r - 1) : (ny - 2) + (r - 1));
+}
+
+// Stage of cell (i, r) after the stage sweep (:92-115).
+template <typename R>
+__device__ __forceinline__ R swept_stage(const LinArgs<R> &a, int i, int r)
+{
+    const int64_t P = a.p.pitch;
+    const int64_t o = (int64_t)r * P + i;
+    const R s_old = a.p.stg[o];
+    const bool interior = (i >= a.xl + 1) && (i <= a.xu - 1) && (r >= a.yl + 1) && (r <= a.yu - 1);
+    if (!interior) return s_old;
+    const R inv_cell_area_dt = a.dt / a.m.area[r];
+    const R t1 = (a.p.uh[o] - a.p.uh[o - 1]) * a.m.dyl[i];
+    const R t2 = a.p.vh[o] * a.m.dxb[r + 1] - a.p.vh[o - P] * a.m.dxb[r];
+    return s_old - inv_cell_area_dt * (t1 + t2);
+}
+
+template <typename R> struct LinRing { R s, uh, vh; };
+
+// West/east pass value of ring cell (i, r), i in {0, nx-1}.
+template <typename R>
+__device__ __forceinline__ LinRing<R> flather_we(const LinArgs<R> &a, const BoundaryFn &bf, double t, int i, int r)
+{
+    const int in = (i == 0) ? 1 : a.p.nx - 2;
+    const int64_t ro = (int64_t)r * a.p.pitch;
+    LinRing<R> v;
+    flather_cell<R>(bf, a.m.x, t, i, r, a.msl, i == 0, swept_stage(a, in, r), a.p.uh[ro + in], a.p.vh[ro + in],
+                    a.p.elv[ro + in], a.p.elv[ro + i], v.s, v.uh, v.vh);
+    return v;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) linear_flather_ring_kernel(const LinArgs<R> a, const DevScalars *sc,
+                                                                  BoundaryFn bf, R *ring)
+{
+    const int nx = a.p.nx, ny = a.p.ny;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    int i, r;
+    if (q < 2 * nx) { i = q % nx; r = (q < nx) ? 0 : ny - 1; }
+    else if (q < 2 * nx + 2 * (ny - 2)) { const int p = q - 2 * nx; r = 1 + p % (ny - 2); i = (p < ny - 2) ? 0 : nx - 1; }
+    else return;
+    const bool sn = (r == 0 && a.bext[2]) || (r == ny - 1 && a.bext[0]);
+    const bool we = (i == 0 && a.bext[3]) || (i == nx - 1 && a.bext[1]);
+    if (!sn && !we) return;
+    // domain%time after the stage sweep, as linear_edge_kernel forms it.
+    const double t = sc->time + (double)(a.dt * K<R>::half());
+    const int64_t P = a.p.pitch;
+    LinRing<R> v;
+    if (sn) {
+        // South/north pass: reads the column neighbour after the west/east pass.
+        const int rn = (r == 0) ? 1 : ny - 2;
+        LinRing<R> nb;
+        if (we) {
+            nb = flather_we<R>(a, bf, t, i, rn);
+        } else {
+            nb.s = swept_stage(a, i, rn);
+            nb.uh = a.p.uh[(int64_t)rn * P + i];
+            nb.vh = a.p.vh[(int64_t)rn * P + i];
+        }
+        flather_cell<R>(bf, a.m.x, t, i, r, a.msl, r == 0, nb.s, nb.vh, nb.uh, a.p.elv[(int64_t)rn * P + i],
+                        a.p.elv[(int64_t)r * P + i], v.s, v.vh, v.uh);
+    } else {
+        v = flather_we<R>(a, bf, t, i, r);
+    }
+    a.p.stg_o[(int64_t)r * P + i] = v.s;
+    ring[2 * q] = v.uh;
+    ring[2 * q + 1] = v.vh;
+}
+
+template <typename R, bool CORIOLIS, bool TRUELY_LINEAR>
+__global__ void __launch_bounds__(256) linear_flather_fix_kernel(const LinArgs<R> a, const R *ring)
+{
+    const int nx = a.p.nx, ny = a.p.ny;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    // Rows 0, 1, ny-2, ny-1 in full, then columns 0, 1, nx-2, nx-1 of rows 2 .. ny-3.
+    int i, r;
+    if (q < 4 * nx) {
+        const int k = q / nx;
+        i = q - k * nx;
+        r = (k < 2) ? k : ny - 4 + k;
+    } else if (q < 4 * nx + 4 * (ny - 4)) {
+        const int p = q - 4 * nx;
+        const int k = p / (ny - 4);
+        r = 2 + (p - k * (ny - 4));
+        i = (k < 2) ? k : nx - 4 + k;
+    } else {
+        return;
+    }
+    const int64_t P = a.p.pitch;
+    const R g = K<R>::gravity(), half = K<R>::half(), one = K<R>::one(), zero = K<R>::zero();
+    const R mad = K<R>::min_depth();
+    // Momenta as the boundary routine left them.
+    auto uhb = [&](int ii, int rr) -> R {
+        return on_bc_ring(ii, rr, nx, ny, a.bext) ? ring[2 * ring_index(ii, rr, nx, ny)]
+                                                  : a.p.uh[(int64_t)rr * P + ii];
+    };
+    auto vhb = [&](int ii, int rr) -> R {
+        return on_bc_ring(ii, rr, nx, ny, a.bext) ? ring[2 * ring_index(ii, rr, nx, ny) + 1]
+                                                  : a.p.vh[(int64_t)rr * P + ii];
+    };
+    const int64_t o = (int64_t)r * P + i;
+    R uh = uhb(i, r), vh = vhb(i, r);
+    if (i >= a.xl && i <= a.xu - 1 && r >= a.yl && r <= a.yu - 1) {
+        const R inv_cell_area_dt_g = g * a.dt / a.m.area[r];
+        const R inv_cell_area_dt_vh_g = g * a.dt / (half * (a.m.area[r] + a.m.area[r + 1]));
+        const R e0 = a.p.elv[o], e_e = a.p.elv[o + 1], e_n = a.p.elv[o + P];
+        const R sn = a.p.stg_o[o], s_e = a.p.stg_o[o + 1], s_n = a.p.stg_o[o + P];
+        R h_iph, h_jph, wet_iph, wet_jph;
+        if (TRUELY_LINEAR) {
+            const bool wi = (e0 < -mad + a.msl) && (e_e < -mad + a.msl);
+            h_iph = wi ? (a.msl - half * (e_e + e0)) : zero;
+            const bool wj = (e_n < -mad + a.msl) && (e0 < -mad + a.msl);
+            h_jph = wj ? (a.msl - half * (e_n + e0)) : zero;
+            wet_iph = one;
+            wet_jph = one;
+        } else {
+            const bool wi = (sn - e0 > mad) && (s_e - e_e > mad);
+            h_iph = wi ? (half * ((s_e + sn) - (e_e + e0))) : zero;
+            const bool wj = (s_n - e_n > mad) && (sn - e0 > mad);
+            h_jph = wj ? (half * ((s_n + sn) - (e_n + e0))) : zero;
+            wet_iph = (h_iph > zero) ? one : zero;
+            wet_jph = (h_jph > zero) ? one : zero;
+        }
+        const R dw_j = s_n - sn;
+        R uh_new = uh * wet_iph - inv_cell_area_dt_g * h_iph * (s_e - sn) * a.m.dyl[i + 1];
+        R vh_new = vh * wet_jph - inv_cell_area_dt_vh_g * h_jph * dw_j * a.m.dxb[r + 1];
+        if (CORIOLIS) {
+            const int rm = (r > 0) ? r - 1 : 0, im = (i > 0) ? i - 1 : 0;
+            const R vh_iph_jmh = half * (vhb(i, rm) + vhb(i + 1, rm));
+            const R vh_iph_jph = half * (vh + vhb(i + 1, r));
+            const R uh_i_j = half * (uh + uhb(im, r));
+            const R uh_i_jp1 = half * (uhb(i, r + 1) + uhb(im, r + 1));
+            const R dt_half_coriolis = a.dt * a.m.cor[r] * half * ((h_iph > zero) ? one : zero);
+            const R dt_half_coriolis_jph = a.dt * a.m.cor_be[r + 1] * half * ((h_jph > zero) ? one : zero);
+            uh_new = uh_new + dt_half_coriolis * (vh_iph_jmh + vh_iph_jph);
+            vh_new = vh_new - dt_half_coriolis_jph * (uh_i_j + uh_i_jp1);
+        }
+        if (a.lin_fric) {
+            uh_new = a.lin_fric_mult * uh_new;
+            vh_new = a.lin_fric_mult * vh_new;
+        }
+        uh = uh_new;
+        vh = vh_new;
+    }
+    a.p.uh_o[o] = uh;
+    a.p.vh_o[o] = vh;
 }
 
 template <typename R>
@@ -823,7 +994,11 @@ LinArgs<R> make_args(const StepPlanes<R> &p, const Metrics<R> &m, const StepConf
     a.p = p;
     a.m = m;
     a.xl = c.xl; a.xu = c.xu; a.yl = c.yl; a.yu = c.yu;
-    a.bc_stage = (c.bc_kind == 2) ? 1 : 0;
+    // Ring stage set before the step kernel: from the boundary function by
+    // the edge kernel (SWALS_BC_STAGE_TRANSMISSIVE_NORMAL_MOMENTUM), or by the
+    // Flather ring kernel.
+    a.bc_stage = (c.bc_kind == 2 || c.bc_kind == 3) ? 1 : 0;
+    a.bc_fn_ring = (c.bc_kind == 2) ? 1 : 0;
     for (int k = 0; k < 4; k++) a.bext[k] = c.bext[k];
     a.dt = dt;
     a.msl = R(c.msl_linear);
@@ -862,12 +1037,32 @@ cudaError_t launch_linear_step(const StepPlanes<R> &p, const Metrics<R> &m, cons
         cudaStreamWaitEvent(s, aux->join, 0);
         return cudaGetLastError();
     }
+    const bool flather = (c.bc_kind == 3);
+    R *ring = (R *)c.ring;
+    if (flather) {
+        // Before the edge kernel: it reads domain%time before the step.
+        hook(CAT_LINEAR_EDGE, 0);
+        const int n = 2 * p.nx + 2 * (p.ny - 2);
+        linear_flather_ring_kernel<R><<<(n + 255) / 256, 256, 0, s>>>(a, sc, c.bf, ring);
+        hook(CAT_LINEAR_EDGE, 1);
+    }
     hook(CAT_LINEAR_EDGE, 0);
     linear_edge_kernel<R><<<1, 512, 0, s>>>(a, sc, c.exterior_cells_width, c.bf);
     hook(CAT_LINEAR_EDGE, 1);
     hook(CAT_LINEAR_MAIN, 0);
     launch_main<R>(a, c, plain_config(p.nx, p.ny), s);
     hook(CAT_LINEAR_MAIN, 1);
+    if (flather) {
+        hook(CAT_LINEAR_EDGE, 0);
+        const int n = 4 * p.nx + 4 * (p.ny - 4);
+        const int blocks = (n + 255) / 256;
+        const bool cor = c.coriolis != 0, tl = c.truely_linear != 0;
+        if (cor && tl) linear_flather_fix_kernel<R, true, true><<<blocks, 256, 0, s>>>(a, ring);
+        else if (cor && !tl) linear_flather_fix_kernel<R, true, false><<<blocks, 256, 0, s>>>(a, ring);
+        else if (!cor && tl) linear_flather_fix_kernel<R, false, true><<<blocks, 256, 0, s>>>(a, ring);
+        else linear_flather_fix_kernel<R, false, false><<<blocks, 256, 0, s>>>(a, ring);
+        hook(CAT_LINEAR_EDGE, 1);
+    }
     return cudaGetLastError();
 }
 
@@ -877,6 +1072,7 @@ cudaError_t launch_linear_map(const StepPlanes<R> &p, const Metrics<R> &m, const
 {
     LinArgs<R> a = make_args<R>(p, m, c, dt);
     a.bc_stage = 0;
+    a.bc_fn_ring = 0;
     a.sites = sites;
     a.n_sites = n_sites;
     a.rec = rec;
@@ -897,6 +1093,7 @@ cudaError_t launch_linear_batch(const StepPlanes<R> &p0, int64_t inst_stride, in
 {
     LinArgs<R> a = make_args<R>(p0, m, c, dt);
     a.bc_stage = 0;
+    a.bc_fn_ring = 0;
     a.nbatch = nbatch;
     a.inst_stride = inst_stride;
     a.max_stride = max_stride;

@@ -261,6 +261,7 @@ struct BcArgs {
     int kind;               // SWALS_BC_*
     int bext[4];            // N,E,S,W
     BoundaryFn bf;
+    R msl;                  // msl_linear (flather's default outside stage)
     const R *x;
     R *stg, *uh, *vh;       // stage output planes
     const R *stg0, *uh0, *vh0;  // backup U0 (mode 2)
@@ -304,6 +305,10 @@ __device__ __forceinline__ RingVal<R> we_value(const BcArgs<R> &a, int i, int r,
     if (a.kind == 1) {  // transmissive: all four variables from the inner neighbour
         v.e = a.elv[(int64_t)r * a.P + in];
         v.s = bc_get(a, in, r, 0); v.uh = bc_get(a, in, r, 1); v.vh = bc_get(a, in, r, 2);
+    } else if (a.kind == 3) {  // flather: normal momentum UH
+        v.e = a.elv[(int64_t)r * a.P + i];
+        flather_cell<R>(a.bf, a.x, t, i, r, a.msl, i == 0, bc_get(a, in, r, 0), bc_get(a, in, r, 1),
+                        bc_get(a, in, r, 2), a.elv[(int64_t)r * a.P + in], v.e, v.s, v.uh, v.vh);
     } else {
         boundary_function<R>(a.bf, a.x, t, i, r, v.s, v.e);
         v.uh = bc_get(a, in, r, 1);
@@ -352,6 +357,9 @@ __global__ void __launch_bounds__(256) rk2_boundary_kernel(const BcArgs<R> a)
         }
         if (a.kind == 1) {
             v = nb;
+        } else if (a.kind == 3) {  // flather: normal momentum VH
+            v.e = a.elv[(int64_t)r * a.P + i];
+            flather_cell<R>(a.bf, a.x, t, i, r, a.msl, r == 0, nb.s, nb.vh, nb.uh, nb.e, v.e, v.s, v.vh, v.uh);
         } else {
             boundary_function<R>(a.bf, a.x, t, i, r, v.s, v.e);
             v.uh = R(0);
@@ -621,7 +629,7 @@ cudaError_t launch_rk2_step(R *const planes[3][3], int &cur, R *elv, R *max_stag
                             const LaunchHook &hook)
 {
     const int A = cur, B = (cur + 1) % 3, C = (cur + 2) % 3;
-    const bool bc = (c.bc_kind == 1 || c.bc_kind == 2);
+    const bool bc = (c.bc_kind == 1 || c.bc_kind == 2 || c.bc_kind == 3);
     double *lines1 = reinterpret_cast<double *>(buf.partials);
     double *lines2 = lines1 + (2 * nx + 2 * ny);
     const double max_dt_inv_init = (double)(R(1) / R(c.maximum_timestep));
@@ -689,7 +697,7 @@ cudaError_t launch_rk2_step(R *const planes[3][3], int &cur, R *elv, R *max_stag
     BcArgs<R> b;
     b.nx = nx; b.ny = ny; b.P = pitch; b.kind = c.bc_kind;
     for (int k = 0; k < 4; k++) b.bext[k] = c.bext[k];
-    b.bf = c.bf; b.x = m.x; b.elv = elv; b.side = a.side; b.max_stage = nullptr;
+    b.bf = c.bf; b.msl = R(c.msl_linear); b.x = m.x; b.elv = elv; b.side = a.side; b.max_stage = nullptr;
     b.dt_from_cfl = a.dt_from_cfl; b.dt_fixed = dt; b.max_dt_inv_init = max_dt_inv_init; b.sc = sc;
     b.stg0 = nullptr; b.uh0 = nullptr; b.vh0 = nullptr;
     if (bc) {

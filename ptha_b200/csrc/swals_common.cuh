@@ -194,4 +194,53 @@ __device__ __forceinline__ void boundary_function(const BoundaryFn &bf, const R 
     }
 }
 
+// flather_boundary (boundary_mod.f90:502-730) for one ring cell (i, j),
+// 0-based.  The inner neighbour holds stage s_in, elevation e_in, normal
+// momentum qn_in (UH on the west/east edges, VH on the south/north edges) and
+// transverse momentum qt_in; e is the ring cell's elevation.  lo: the west or
+// south edge (inflow has positive normal velocity).  The 'outside' state is
+// the boundary function's (whose momenta are zero for the device kinds), or
+// at rest at stage max(msl_linear, e) without one.  Returns the ring cell's
+// stage, normal and transverse momentum; its elevation is unchanged.
+template <typename R>
+__device__ __forceinline__ void flather_cell(const BoundaryFn &bf, const R *x, double t, int i, int j, R msl, bool lo,
+                                             R s_in, R qn_in, R qt_in, R e_in, R e, R &s_out, R &qn_out, R &qt_out)
+{
+    const R mad = K<R>::min_depth();
+    const R depth_inside = s_in - e_in;
+    R stage_outside, depth_outside;
+    const R u_outside = R(0);
+    if (bf.kind == 0) {
+        stage_outside = (msl > e) ? msl : e;
+        depth_outside = stage_outside - e;
+    } else {
+        R bs, be;
+        boundary_function<R>(bf, x, t, i, j, bs, be);
+        stage_outside = bs;
+        depth_outside = bs - be;
+    }
+    if (depth_inside > mad && depth_outside > mad) {
+        const R depth_inside_inv = R(1) / depth_inside;
+        const R sqrt_g_on_di = sqrt(K<R>::gravity() * depth_inside_inv);
+        R w1, w2, w3;
+        if (lo) {
+            w1 = u_outside + sqrt_g_on_di * stage_outside;
+            w2 = (qn_in < R(0)) ? qt_in * depth_inside_inv : R(0);
+            w3 = qn_in * depth_inside_inv - sqrt_g_on_di * s_in;
+            s_out = (-w3 + w1) / (R(2) * sqrt_g_on_di);
+        } else {
+            w1 = u_outside - sqrt_g_on_di * stage_outside;
+            w2 = (qn_in > R(0)) ? qt_in * depth_inside_inv : R(0);
+            w3 = qn_in * depth_inside_inv + sqrt_g_on_di * s_in;
+            s_out = (w3 - w1) / (R(2) * sqrt_g_on_di);
+        }
+        qn_out = (w3 + w1) * K<R>::half() * depth_inside;
+        qt_out = w2 * depth_inside;
+    } else {
+        s_out = stage_outside;
+        qn_out = R(0);
+        qt_out = R(0);
+    }
+}
+
 }  // namespace swals

@@ -43,6 +43,7 @@ struct StepConfig {
     int spherical, coriolis, nofriction, chezy, truely_linear;
     double msl_linear, linear_friction_coeff, theta, cfl, maximum_timestep;
     int exterior_cells_width;
+    void *ring;             // linear + Flather: 2 (nx + ny - 2) x 2 reals of ring momenta
 };
 
 // compute_domain_statistics_new: rows6 is 6*ny doubles of scratch; out7 (device)
