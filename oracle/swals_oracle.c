@@ -1117,6 +1117,66 @@ static void one_rk2_step(oracle_domain *d, double timestep, int has_ts)
     d->max_dt = max_dt_store;
 }
 
+/* one_rk2n_step (timestepping_alternatives_include.f90:149-270) with
+ * n = rk2n_n_value = 5 (domain_mod.f90:90): n-1 Euler steps of the first
+ * step's dt, the last shortened to (n-1)/n of it, plus 1/n of the change
+ * over the first n-2 steps subtracted back. */
+static void one_rk2n_step(oracle_domain *d, double timestep, int has_ts)
+{
+    const int nx = d->nx, ny = d->ny;
+    const size_t plane = (size_t)nx * (size_t)ny;
+    const int n = 5;
+    const REAL n_inverse = ONE / (ONE * (REAL)n);
+    double backup_time = d->time;
+    memcpy(d->backup_U, d->U, 3 * plane * sizeof(REAL));
+    REAL dt_first_step;
+    if (has_ts) {
+        dt_first_step = (REAL)timestep / ((REAL)n - (REAL)1.0);
+        one_euler_step(d, (double)dt_first_step, 1, 0);
+    } else {
+        one_euler_step(d, 0.0, 0, 0);
+        dt_first_step = (REAL)d->max_dt;
+    }
+    const REAL rescaled = dt_first_step * ((REAL)n - (REAL)1.0) * n_inverse;
+    nest_flux_tstep_fv(d, (double)rescaled);
+    double max_dt_store = d->max_dt;
+    for (int j = 2; j <= n - 1; j++) {
+        one_euler_step(d, (double)dt_first_step, 1, 0);
+        nest_flux_tstep_fv(d, (double)rescaled);
+    }
+    for (size_t q = 0; q < 3 * plane; q++) d->backup_U[q] = (d->backup_U[q] - d->U[q]) * n_inverse;
+    d->boundary_flux_evolve_integral = d->boundary_flux_evolve_integral * (double)((REAL)n - (REAL)1.0) *
+                                       (double)n_inverse;
+    const REAL reduced_dt = (ONE * (REAL)n - ONE) * n_inverse * dt_first_step;
+    one_euler_step(d, (double)reduced_dt, 1, 1);
+    for (size_t q = 0; q < 3 * plane; q++) d->U[q] = d->U[q] + d->backup_U[q];
+    d->time = backup_time + (double)(dt_first_step * (REAL)(n - 1));
+    d->max_dt = max_dt_store;
+}
+
+/* one_midpoint_step (timestepping_alternatives_include.f90:273-337): a half
+ * step to the midpoint, then the full step from the backed-up state with the
+ * midpoint's fluxes, depth and velocity. */
+static void one_midpoint_step(oracle_domain *d, double timestep, int has_ts)
+{
+    const int nx = d->nx, ny = d->ny;
+    const size_t plane = (size_t)nx * (size_t)ny;
+    double backup_time = d->time;
+    memcpy(d->backup_U, d->U, 3 * plane * sizeof(REAL));
+    REAL dt_first_step = (REAL)compute_fluxes(d);
+    d->max_dt = (double)dt_first_step;
+    if (has_ts) dt_first_step = (REAL)timestep;
+    update_U(d, dt_first_step * HALF);
+    compute_fluxes(d);
+    memcpy(d->U, d->backup_U, 3 * plane * sizeof(REAL));
+    d->time = backup_time;
+    update_U(d, dt_first_step);
+    nest_flux_tstep_fv(d, (double)dt_first_step);
+    double tot = 0.0;
+    for (int k = 0; k < 4; k++) tot += d->boundary_flux_store[k];
+    d->boundary_flux_evolve_integral = tot * (double)dt_first_step;
+}
+
 /* domain_mod.f90:1679-1813 */
 int ORACLE_FN(evolve_one_step)(oracle_domain *d, double dt, int has_dt)
 {
@@ -1126,6 +1186,8 @@ int ORACLE_FN(evolve_one_step)(oracle_domain *d, double dt, int has_dt)
     switch (d->method) {
     case OR_METHOD_RK2: one_rk2_step(d, dt, has_dt); break;
     case OR_METHOD_EULER: one_euler_step(d, dt, has_dt, 1); break;
+    case OR_METHOD_RK2N: one_rk2n_step(d, dt, has_dt); break;
+    case OR_METHOD_MIDPOINT: one_midpoint_step(d, dt, has_dt); break;
     case OR_METHOD_LINEAR:
         if (!has_dt) return 2;
         linear_leapfrog_step(d, (REAL)dt);

@@ -242,17 +242,24 @@ int evolve_t(swals_domain *d, double timestep, int has_dt)
         e = launch_linear_step<R>(p, m, c, R(timestep), d->sc, d->stream, hook, d->timers_on ? nullptr : &d->aux);
         if (e != cudaSuccess) return cuda_fail(e, "linear leapfrog step");
         d->cur = out;
-    } else if (d->method == M_RK2 || d->method == M_EULER) {
+    } else if (d->method == M_RK2 || d->method == M_EULER || d->method == M_MIDPOINT || d->method == M_RK2N) {
         R *pl[3][3];
         for (int b = 0; b < 3; b++)
             for (int v = 0; v < 3; v++) pl[b][v] = (R *)d->planes[b][v];
         Rk2Buffers buf;
         buf.side = d->side;
         buf.partials = d->lines;
-        buf.partials_len = 2 * (2 * d->nx + 2 * d->ny);
+        buf.partials_len = 4 * (2 * d->nx + 2 * d->ny);
         buf.edges = d->edges;
-        e = launch_rk2_step<R>(pl, d->cur, (R *)d->elv, max_stage, (R *)d->manning_sq, d->nx, d->ny, d->pitch, m, c,
-                               has_dt != 0, timestep, d->method == M_EULER, buf, d->sc, d->stream, hook);
+        if (d->method == M_MIDPOINT)
+            e = launch_midpoint_step<R>(pl, d->cur, (R *)d->elv, max_stage, (R *)d->manning_sq, d->nx, d->ny,
+                                        d->pitch, m, c, has_dt != 0, timestep, buf, d->sc, d->stream, hook);
+        else if (d->method == M_RK2N)
+            e = launch_rk2n_step<R>(pl, d->cur, (R *)d->elv, max_stage, (R *)d->manning_sq, d->nx, d->ny, d->pitch,
+                                    m, c, has_dt != 0, timestep, buf, d->sc, d->stream, hook);
+        else
+            e = launch_rk2_step<R>(pl, d->cur, (R *)d->elv, max_stage, (R *)d->manning_sq, d->nx, d->ny, d->pitch,
+                                   m, c, has_dt != 0, timestep, d->method == M_EULER, buf, d->sc, d->stream, hook);
         if (e != cudaSuccess) return cuda_fail(e, "finite-volume step");
     } else {
         return fail(SWALS_ERR_UNSUPPORTED, "timestepping_method '%s' is not implemented on the GPU path",
@@ -316,7 +323,7 @@ int swals_gpu_domain_create(const swals_domain_desc *desc, swals_domain **out)
     double def_cfl, def_theta;
     if (!parse_method(desc->timestepping_method, &method, &def_cfl, &def_theta))
         return fail(SWALS_ERR_UNKNOWN_METHOD, "timestepping_method: %s not recognized", desc->timestepping_method);
-    if (!(method == M_LINEAR || method == M_RK2 || method == M_EULER))
+    if (!(method == M_LINEAR || method == M_RK2 || method == M_EULER || method == M_MIDPOINT || method == M_RK2N))
         return fail(SWALS_ERR_UNSUPPORTED, "timestepping_method '%s' is not implemented on the GPU path",
                     desc->timestepping_method);
     const int nx = desc->nx[0], ny = desc->nx[1];
@@ -396,12 +403,13 @@ int swals_gpu_domain_create(const swals_domain_desc *desc, swals_domain **out)
     for (int k = 0; k < 8; k++) total += al(metric_elems[k] * es);
     total += al(sizeof(swals::DevScalars));
     const size_t side_bytes = al((size_t)(4 * ny + 4 * nx) * 3 * es);
-    const size_t lines_bytes = al((size_t)2 * (2 * nx + 2 * ny) * sizeof(double));
+    const size_t lines_bytes = al((size_t)4 * (2 * nx + 2 * ny) * sizeof(double));   // 4 flux evaluations (rk2n)
     d->scratch_len = (nx > ny ? nx : ny) + 4096;
     const size_t scratch_bytes = al((size_t)d->scratch_len * sizeof(double));
     total += side_bytes + lines_bytes + scratch_bytes + al(64);
     // Stored stage-1 edge results of adaptive finite-volume steps.
-    const size_t edge_bytes = (d->method == M_RK2 || d->method == M_EULER)
+    const size_t edge_bytes = (d->method == M_RK2 || d->method == M_EULER || d->method == M_MIDPOINT ||
+                               d->method == M_RK2N)
                                   ? al((size_t)swals::rk2_edge_bytes(d->pitch, ny, (int)es)) : 0;
     total += edge_bytes;
     e = cudaMalloc(&d->pool, total);

@@ -272,7 +272,8 @@ struct BcArgs {
     int dt_from_cfl;
     double dt_fixed;
     double max_dt_inv_init;
-    int n_dt;               // boundary time = time0 + n_dt * dt
+    int n_dt;               // boundary time = time0 + n_dt * dt (n_dt additions) ...
+    R dt_extra;             // ... + dt * dt_extra when nonzero (midpoint half step, rk2n last step)
     DevScalars *sc;
 };
 
@@ -342,6 +343,7 @@ __global__ void __launch_bounds__(256) rk2_boundary_kernel(const BcArgs<R> a)
     }
     double t = a.sc->time;
     for (int k = 0; k < a.n_dt; k++) t = t + dtd;
+    if (a.dt_extra != R(0)) t = t + (double)(R(dtd) * a.dt_extra);
 
     RingVal<R> v;
     if (sn) {
@@ -396,14 +398,22 @@ cudaError_t launch_boundary(const BcArgs<R> &b, cudaStream_t s)
 
 // End of a step: domain%max_dt, time, boundary-flux integrals, counters
 // (timestepping_alternatives_include.f90:36-50,121-144; domain_mod.f90:1800-1810).
+// kind: FIN_RK2 (two Euler stages averaged), FIN_EULER, FIN_MIDPOINT (the
+// store of the midpoint's fluxes), FIN_RK2N (n-1 = 4 Euler steps,
+// timestepping_alternatives_include.f90:149-270).  `lines` holds one set of
+// 2 nx + 2 ny boundary-flux line values per flux evaluation.
+enum { FIN_RK2 = 0, FIN_EULER = 1, FIN_MIDPOINT = 2, FIN_RK2N = 3 };
+constexpr int RK2N_N = 5;   // rk2n_n_value (domain_mod.f90:90)
+
 template <typename R>
-__global__ void __launch_bounds__(1024) rk2_finalize_kernel(int nx, int ny, int n_ext, const double *lines1,
-                                                            const double *lines2, int euler_only, int dt_from_cfl,
-                                                            double dt_fixed, double max_dt_inv_init, DevScalars *sc)
+__global__ void __launch_bounds__(1024) rk2_finalize_kernel(int nx, int ny, int n_ext, const double *lines, int kind,
+                                                            int dt_from_cfl, double dt_fixed, double max_dt_inv_init,
+                                                            DevScalars *sc)
 {
-    __shared__ double red[8][32];
-    double acc[8];
-    for (int k = 0; k < 8; k++) acc[k] = 0.0;
+    __shared__ double red[16][32];
+    double acc[16];
+    for (int k = 0; k < 16; k++) acc[k] = 0.0;
+    const int nsets = (kind == FIN_EULER) ? 1 : (kind == FIN_RK2N) ? 4 : 2;
     const int L = 2 * nx + 2 * ny;
     for (int q = threadIdx.x; q < L; q += blockDim.x) {
         int line, idx;
@@ -413,11 +423,10 @@ __global__ void __launch_bounds__(1024) rk2_finalize_kernel(int nx, int ny, int 
         else { line = 3; idx = q - 2 * nx - ny; }
         const int lim = (line == 0 || line == 2) ? nx : ny;
         if (idx < n_ext || idx > lim - n_ext - 1) continue;
-        acc[line] += lines1[q];
-        if (!euler_only) acc[4 + line] += lines2[q];
+        for (int k = 0; k < nsets; k++) acc[4 * k + line] += lines[(int64_t)k * L + q];
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int k = 0; k < 8; k++) {
+    for (int k = 0; k < 4 * nsets; k++) {
         double v = acc[k];
         for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
         if (lane == 0) red[k][warp] = v;
@@ -425,8 +434,8 @@ __global__ void __launch_bounds__(1024) rk2_finalize_kernel(int nx, int ny, int 
     __syncthreads();
     if (threadIdx.x != 0) return;
     const int nw = blockDim.x >> 5;
-    double s[8];
-    for (int k = 0; k < 8; k++) {
+    double s[16];
+    for (int k = 0; k < 4 * nsets; k++) {
         double v = 0.0;
         for (int w = 0; w < nw; w++) v += red[k][w];
         s[k] = v;
@@ -436,25 +445,45 @@ __global__ void __launch_bounds__(1024) rk2_finalize_kernel(int nx, int ny, int 
     const double max_dt = (double)(R(1) / max_dt_inv);
     const double dt = dt_from_cfl ? max_dt : (double)R(dt_fixed);
     const double time0 = sc->time;
-    double store1[4] = {s[0], s[1], -s[2], -s[3]};
-    double store2[4] = {s[4], s[5], -s[6], -s[7]};
-    double tot1 = 0.0, tot2 = 0.0;
-    for (int k = 0; k < 4; k++) { tot1 += store1[k]; tot2 += store2[k]; }
-    double integral = 0.0 + dt * tot1;
-    if (!euler_only) {
-        integral = integral + dt * tot2;
-        integral = 0.5 * integral;
-        for (int k = 0; k < 4; k++) sc->boundary_flux_store[k] = store2[k];
-    } else {
-        for (int k = 0; k < 4; k++) sc->boundary_flux_store[k] = store1[k];
+    double store[4][4], tot[4];
+    for (int q = 0; q < nsets; q++) {
+        store[q][0] = s[4 * q]; store[q][1] = s[4 * q + 1]; store[q][2] = -s[4 * q + 2]; store[q][3] = -s[4 * q + 3];
+        tot[q] = 0.0;
+        for (int k = 0; k < 4; k++) tot[q] += store[q][k];
     }
+    double integral;
+    double dt_last = dt;
+    double t_end = time0 + dt;
+    int last = 0;
+    if (kind == FIN_RK2) {
+        integral = 0.0 + dt * tot[0];
+        integral = integral + dt * tot[1];
+        integral = 0.5 * integral;
+        last = 1;
+    } else if (kind == FIN_EULER) {
+        integral = 0.0 + dt * tot[0];
+    } else if (kind == FIN_MIDPOINT) {
+        integral = tot[1] * dt;
+        last = 1;
+    } else {
+        const R n_inverse = R(1) / (R(1) * R(RK2N_N));
+        integral = 0.0;
+        for (int q = 0; q < RK2N_N - 2; q++) integral = integral + dt * tot[q];
+        integral = integral * (double)(R(RK2N_N) - R(1)) * (double)n_inverse;
+        const R reduced_dt = (R(1) * R(RK2N_N) - R(1)) * n_inverse * R(dt);
+        integral = integral + (double)reduced_dt * tot[3];
+        dt_last = (double)reduced_dt;
+        t_end = time0 + (double)(R(dt) * R(RK2N_N - 1));
+        last = 3;
+    }
+    for (int k = 0; k < 4; k++) sc->boundary_flux_store[k] = store[last][k];
     sc->boundary_flux_evolve_integral = integral;
     sc->boundary_flux_time_integral += integral;
     sc->max_dt = max_dt;
     sc->dt = dt;
-    sc->dt_last_update = dt;
+    sc->dt_last_update = dt_last;
     sc->time0 = time0;
-    sc->time = time0 + dt;
+    sc->time = t_end;
     sc->evolve_step_dt = sc->time - time0;
     sc->nsteps_advanced += 1;
     sc->max_dt_inv_bits = 0ull;
@@ -622,25 +651,20 @@ cudaError_t dispatch_stage(const Rk2Args<R> &a, const StepConfig &c, cudaStream_
 
 }  // namespace
 
-template <typename R>
-cudaError_t launch_rk2_step(R *const planes[3][3], int &cur, R *elv, R *max_stage, R *manning_sq, int nx, int ny,
-                            int64_t pitch, const Metrics<R> &m, const StepConfig &c, bool has_dt, double dt,
-                            bool euler_only, const Rk2Buffers &buf, DevScalars *sc, cudaStream_t s,
-                            const LaunchHook &hook)
-{
-    const int A = cur, B = (cur + 1) % 3, C = (cur + 2) % 3;
-    const bool bc = (c.bc_kind == 1 || c.bc_kind == 2 || c.bc_kind == 3);
-    double *lines1 = reinterpret_cast<double *>(buf.partials);
-    double *lines2 = lines1 + (2 * nx + 2 * ny);
-    const double max_dt_inv_init = (double)(R(1) / R(c.maximum_timestep));
+namespace {
 
+// Stage arguments common to every stage of a finite-volume step.
+template <typename R>
+Rk2Args<R> fv_args(int nx, int ny, int64_t pitch, R *elv, R *manning_sq, const Metrics<R> &m, const StepConfig &c,
+                   double dt, const Rk2Buffers &buf, DevScalars *sc)
+{
     Rk2Args<R> a;
     a.nx = nx; a.ny = ny; a.P = pitch;
     a.elv = elv; a.nsq = manning_sq; a.max_stage = nullptr; a.m = m;
     a.theta = R(c.theta); a.half_cfl = R(0.5) * R(c.cfl);
     a.lin_fric = R(c.linear_friction_coeff);
     a.dt_fixed = dt;
-    a.max_dt_inv_init = max_dt_inv_init;
+    a.max_dt_inv_init = (double)(R(1) / R(c.maximum_timestep));
     a.n_ext = c.exterior_cells_width;
     a.bc_ring = 0;
     for (int k = 0; k < 4; k++) a.bext[k] = c.bext[k];
@@ -648,15 +672,46 @@ cudaError_t launch_rk2_step(R *const planes[3][3], int &cur, R *elv, R *max_stag
     a.sc = sc;
     a.stg0 = nullptr; a.uh0 = nullptr; a.vh0 = nullptr;
     a.ep = EdgePlanes<R>{};
-    cudaError_t e;
+    a.dt_scale = R(1);
+    a.base0 = 0;
+    a.lines = nullptr;
+    a.write_cfl = 0;
+    a.dt_from_cfl = 0;
+    return a;
+}
 
-    // With stored edges, an adaptive stage 1 is a flux pass (edges, CFL
-    // maximum and boundary-flux lines of U0) and an update once dt is known;
-    // otherwise a CFL pass (adaptive only) and the fused stage kernel.
+// Boundary-kernel arguments of a step.
+template <typename R>
+BcArgs<R> bc_args(const Rk2Args<R> &a, const StepConfig &c, double dt)
+{
+    BcArgs<R> b;
+    b.nx = a.nx; b.ny = a.ny; b.P = a.P; b.kind = c.bc_kind;
+    for (int k = 0; k < 4; k++) b.bext[k] = c.bext[k];
+    b.bf = c.bf; b.msl = R(c.msl_linear); b.x = a.m.x; b.elv = const_cast<R *>(a.elv); b.side = a.side;
+    b.max_stage = nullptr;
+    b.dt_extra = R(0);
+    b.dt_from_cfl = a.dt_from_cfl; b.dt_fixed = dt; b.max_dt_inv_init = a.max_dt_inv_init; b.sc = a.sc;
+    b.stg0 = nullptr; b.uh0 = nullptr; b.vh0 = nullptr;
+    b.n_dt = 1;
+    b.stage_mode = 1;
+    return b;
+}
+
+// The first flux evaluation of a step, from planes[A] into planes[B]
+// (one_euler_step's compute_fluxes + update_U): with stored edges and an
+// adaptive dt, a flux pass (edges, CFL maximum, boundary-flux lines) and an
+// update once dt is known; otherwise a CFL pass (adaptive only) and the fused
+// stage kernel.  `a` carries dt_scale and max_stage; returns with a's planes
+// and dt flags set as the stage used them.
+template <typename R>
+cudaError_t first_stage(Rk2Args<R> &a, R *const planes[3][3], int A, int B, bool has_dt, const Rk2Buffers &buf,
+                        double *lines, const StepConfig &c, cudaStream_t s, const LaunchHook &hook)
+{
+    cudaError_t e;
     const bool stored = !has_dt && buf.edges && use_stream_kernel();
     if (stored) {
         char *q = reinterpret_cast<char *>(buf.edges);
-        const int64_t plane = pitch * (int64_t)ny;
+        const int64_t plane = a.P * (int64_t)a.ny;
         auto take_r = [&]() { R *p = reinterpret_cast<R *>(q); q += plane * sizeof(R); return p; };
         auto take_d = [&]() { double *p = reinterpret_cast<double *>(q); q += plane * sizeof(double); return p; };
         // doubles first (8-byte alignment whatever R is)
@@ -666,7 +721,7 @@ cudaError_t launch_rk2_step(R *const planes[3][3], int &cur, R *elv, R *max_stag
         Rk2Args<R> p = a;
         p.stg = planes[A][0]; p.uh = planes[A][1]; p.vh = planes[A][2];
         p.stg_o = nullptr; p.uh_o = nullptr; p.vh_o = nullptr;
-        p.dt_from_cfl = 0; p.write_cfl = 1; p.lines = lines1;
+        p.dt_from_cfl = 0; p.write_cfl = 1; p.lines = lines;
         hook(CAT_CFL, 0);
         e = dispatch_flux<R>(p, c, s);
         hook(CAT_CFL, 1);
@@ -682,24 +737,57 @@ cudaError_t launch_rk2_step(R *const planes[3][3], int &cur, R *elv, R *max_stag
         hook(CAT_CFL, 1);
         if (e != cudaSuccess) return e;
     }
-    // Stage 1: U0 -> B
     a.stg = planes[A][0]; a.uh = planes[A][1]; a.vh = planes[A][2];
     a.stg_o = planes[B][0]; a.uh_o = planes[B][1]; a.vh_o = planes[B][2];
     a.dt_from_cfl = has_dt ? 0 : 1;
     a.write_cfl = has_dt ? 1 : 0;
-    a.lines = lines1;
-    if (euler_only) a.max_stage = nullptr;
+    a.lines = lines;
     hook(CAT_STAGE1, 0);
     e = stored ? dispatch_update<R>(a, c, s) : dispatch_stage<R, MODE_STAGE1>(a, c, s);
     hook(CAT_STAGE1, 1);
+    return e;
+}
+
+// A later Euler stage with the first stage's dt (rk2 / rk2n sub-steps,
+// midpoint full step): planes[in] -> planes[out], no CFL accumulation.
+template <typename R>
+cudaError_t later_stage(Rk2Args<R> a, R *const planes[3][3], int in, int out, bool has_dt, double *lines,
+                        const StepConfig &c, cudaStream_t s, const LaunchHook &hook, int cat)
+{
+    a.stg = planes[in][0]; a.uh = planes[in][1]; a.vh = planes[in][2];
+    a.stg_o = planes[out][0]; a.uh_o = planes[out][1]; a.vh_o = planes[out][2];
+    a.dt_from_cfl = has_dt ? 0 : 1;
+    a.write_cfl = 0;
+    a.lines = lines;
+    hook(cat, 0);
+    cudaError_t e = dispatch_stage<R, MODE_STAGE1>(a, c, s);
+    hook(cat, 1);
+    return e;
+}
+
+bool has_bc(const StepConfig &c) { return c.bc_kind == 1 || c.bc_kind == 2 || c.bc_kind == 3; }
+
+}  // namespace
+
+template <typename R>
+cudaError_t launch_rk2_step(R *const planes[3][3], int &cur, R *elv, R *max_stage, R *manning_sq, int nx, int ny,
+                            int64_t pitch, const Metrics<R> &m, const StepConfig &c, bool has_dt, double dt,
+                            bool euler_only, const Rk2Buffers &buf, DevScalars *sc, cudaStream_t s,
+                            const LaunchHook &hook)
+{
+    const int A = cur, B = (cur + 1) % 3, C = (cur + 2) % 3;
+    const bool bc = has_bc(c);
+    double *lines1 = reinterpret_cast<double *>(buf.partials);
+    double *lines2 = lines1 + (2 * nx + 2 * ny);
+    const double max_dt_inv_init = (double)(R(1) / R(c.maximum_timestep));
+    cudaError_t e;
+
+    // Stage 1: U0 -> B
+    Rk2Args<R> a = fv_args<R>(nx, ny, pitch, elv, manning_sq, m, c, dt, buf, sc);
+    e = first_stage<R>(a, planes, A, B, has_dt, buf, lines1, c, s, hook);
     if (e != cudaSuccess) return e;
 
-    BcArgs<R> b;
-    b.nx = nx; b.ny = ny; b.P = pitch; b.kind = c.bc_kind;
-    for (int k = 0; k < 4; k++) b.bext[k] = c.bext[k];
-    b.bf = c.bf; b.msl = R(c.msl_linear); b.x = m.x; b.elv = elv; b.side = a.side; b.max_stage = nullptr;
-    b.dt_from_cfl = a.dt_from_cfl; b.dt_fixed = dt; b.max_dt_inv_init = max_dt_inv_init; b.sc = sc;
-    b.stg0 = nullptr; b.uh0 = nullptr; b.vh0 = nullptr;
+    BcArgs<R> b = bc_args<R>(a, c, dt);
     if (bc) {
         b.stg = planes[B][0]; b.uh = planes[B][1]; b.vh = planes[B][2];
         b.stage_mode = 1; b.n_dt = 1;
@@ -716,7 +804,7 @@ cudaError_t launch_rk2_step(R *const planes[3][3], int &cur, R *elv, R *max_stag
             if (e != cudaSuccess) return e;
         }
         hook(CAT_FINALIZE, 0);
-        rk2_finalize_kernel<R><<<1, 1024, 0, s>>>(nx, ny, c.exterior_cells_width, lines1, lines2, 1,
+        rk2_finalize_kernel<R><<<1, 1024, 0, s>>>(nx, ny, c.exterior_cells_width, lines1, FIN_EULER,
                                                   a.dt_from_cfl, dt, max_dt_inv_init, sc);
         hook(CAT_FINALIZE, 1);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -747,13 +835,181 @@ cudaError_t launch_rk2_step(R *const planes[3][3], int &cur, R *elv, R *max_stag
         if (e != cudaSuccess) return e;
     }
     hook(CAT_FINALIZE, 0);
-    rk2_finalize_kernel<R><<<1, 1024, 0, s>>>(nx, ny, c.exterior_cells_width, lines1, lines2, 0, a.dt_from_cfl,
+    rk2_finalize_kernel<R><<<1, 1024, 0, s>>>(nx, ny, c.exterior_cells_width, lines1, FIN_RK2, a.dt_from_cfl,
                                               dt, max_dt_inv_init, sc);
     hook(CAT_FINALIZE, 1);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     cur = C;
     return cudaSuccess;
 }
+
+namespace {
+
+// rk2n: backup_U = (backup_U - U) / n (timestepping_alternatives_include.f90:211-220).
+template <typename R>
+__global__ void rk2n_backup_kernel(int nx, int ny, int64_t P, R *b0, R *b1, R *b2, const R *u0, const R *u1,
+                                   const R *u2, R n_inverse)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, r = blockIdx.y;
+    if (i >= nx) return;
+    const int64_t o = (int64_t)r * P + i;
+    b0[o] = (b0[o] - u0[o]) * n_inverse;
+    b1[o] = (b1[o] - u1[o]) * n_inverse;
+    b2[o] = (b2[o] - u2[o]) * n_inverse;
+}
+
+// rk2n: U = U + backup_U (:237-247), then update_max_quantities (max_stage
+// over the active region, dry cells included).
+template <typename R>
+__global__ void rk2n_final_kernel(int nx, int ny, int64_t P, R *u0, R *u1, R *u2, const R *b0, const R *b1,
+                                  const R *b2, R *max_stage, int xl, int xu, int yl, int yu)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, r = blockIdx.y;
+    if (i >= nx) return;
+    const int64_t o = (int64_t)r * P + i;
+    const R st = u0[o] + b0[o];
+    u0[o] = st;
+    u1[o] = u1[o] + b1[o];
+    u2[o] = u2[o] + b2[o];
+    if (max_stage && i >= xl && i <= xu && r >= yl && r <= yu) {
+        const R mx = max_stage[o];
+        max_stage[o] = (st > mx) ? st : mx;
+    }
+}
+
+}  // namespace
+
+// one_midpoint_step (timestepping_alternatives_include.f90:273-337):
+// U0 (A) -> the midpoint state (B) with dt/2, then the full step of U0 with
+// the midpoint's fluxes, depth and velocity (C).
+template <typename R>
+cudaError_t launch_midpoint_step(R *const planes[3][3], int &cur, R *elv, R *max_stage, R *manning_sq, int nx, int ny,
+                                 int64_t pitch, const Metrics<R> &m, const StepConfig &c, bool has_dt, double dt,
+                                 const Rk2Buffers &buf, DevScalars *sc, cudaStream_t s, const LaunchHook &hook)
+{
+    const int A = cur, B = (cur + 1) % 3, C = (cur + 2) % 3;
+    const bool bc = has_bc(c);
+    double *lines1 = reinterpret_cast<double *>(buf.partials);
+    double *lines2 = lines1 + (2 * nx + 2 * ny);
+    cudaError_t e;
+
+    Rk2Args<R> a = fv_args<R>(nx, ny, pitch, elv, manning_sq, m, c, dt, buf, sc);
+    a.dt_scale = K<R>::half();
+    e = first_stage<R>(a, planes, A, B, has_dt, buf, lines1, c, s, hook);
+    if (e != cudaSuccess) return e;
+    BcArgs<R> b = bc_args<R>(a, c, dt);
+    if (bc) {
+        // update_U(dt/2) ends with update_boundary at time + dt/2
+        b.stg = planes[B][0]; b.uh = planes[B][1]; b.vh = planes[B][2];
+        b.n_dt = 0; b.dt_extra = K<R>::half();
+        hook(CAT_BC1, 0);
+        e = launch_boundary<R>(b, s);
+        hook(CAT_BC1, 1);
+        if (e != cudaSuccess) return e;
+    }
+    Rk2Args<R> a2 = a;
+    a2.dt_scale = R(1);
+    a2.base0 = 1;
+    a2.stg0 = planes[A][0]; a2.uh0 = planes[A][1]; a2.vh0 = planes[A][2];
+    e = later_stage<R>(a2, planes, B, C, has_dt, lines2, c, s, hook, CAT_STAGE2);
+    if (e != cudaSuccess) return e;
+    if (bc) {
+        b.stg = planes[C][0]; b.uh = planes[C][1]; b.vh = planes[C][2];
+        b.n_dt = 1; b.dt_extra = R(0);
+        hook(CAT_BC2, 0);
+        e = launch_boundary<R>(b, s);
+        hook(CAT_BC2, 1);
+        if (e != cudaSuccess) return e;
+    }
+    if (max_stage) {
+        hook(CAT_MAXSTAGE, 0);
+        e = launch_update_max_stage<R>(nx, ny, pitch, planes[C][0], max_stage, c, s);
+        hook(CAT_MAXSTAGE, 1);
+        if (e != cudaSuccess) return e;
+    }
+    hook(CAT_FINALIZE, 0);
+    rk2_finalize_kernel<R><<<1, 1024, 0, s>>>(nx, ny, c.exterior_cells_width, lines1, FIN_MIDPOINT,
+                                              has_dt ? 0 : 1, dt, a.max_dt_inv_init, sc);
+    hook(CAT_FINALIZE, 1);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    cur = C;
+    return cudaSuccess;
+}
+
+// one_rk2n_step (timestepping_alternatives_include.f90:149-270) with n = 5:
+// A holds the backup; Euler steps A -> B -> C -> B, backup = (backup - U)/n,
+// the last step B -> C with (n-1)/n of dt, and U = C + backup.  `dt` is the
+// caller's timestep (n-1 sub-steps of dt/(n-1)).
+template <typename R>
+cudaError_t launch_rk2n_step(R *const planes[3][3], int &cur, R *elv, R *max_stage, R *manning_sq, int nx, int ny,
+                             int64_t pitch, const Metrics<R> &m, const StepConfig &c, bool has_dt, double dt,
+                             const Rk2Buffers &buf, DevScalars *sc, cudaStream_t s, const LaunchHook &hook)
+{
+    const int A = cur, B = (cur + 1) % 3, C = (cur + 2) % 3;
+    const bool bc = has_bc(c);
+    const int L = 2 * nx + 2 * ny;
+    double *lines = reinterpret_cast<double *>(buf.partials);
+    const R n_inverse = R(1) / (R(1) * R(RK2N_N));
+    // dt_first_step = timestep / (n - 1)
+    const double dt_sub = has_dt ? (double)(R(dt) / (R(RK2N_N) - R(1))) : 0.0;
+    cudaError_t e;
+
+    Rk2Args<R> a = fv_args<R>(nx, ny, pitch, elv, manning_sq, m, c, dt_sub, buf, sc);
+    e = first_stage<R>(a, planes, A, B, has_dt, buf, lines, c, s, hook);
+    if (e != cudaSuccess) return e;
+    BcArgs<R> b = bc_args<R>(a, c, dt_sub);
+    auto boundary = [&](int P_, int n_dt, R extra) -> cudaError_t {
+        if (!bc) return cudaSuccess;
+        b.stg = planes[P_][0]; b.uh = planes[P_][1]; b.vh = planes[P_][2];
+        b.n_dt = n_dt; b.dt_extra = extra;
+        hook(CAT_BC1, 0);
+        cudaError_t r = launch_boundary<R>(b, s);
+        hook(CAT_BC1, 1);
+        return r;
+    };
+    if ((e = boundary(B, 1, R(0))) != cudaSuccess) return e;
+    // sub-steps 2 .. n-1
+    const int seq[3] = {B, C, B};
+    for (int k = 1; k < RK2N_N - 2; k++) {
+        e = later_stage<R>(a, planes, seq[k - 1], seq[k], has_dt, lines + (int64_t)k * L, c, s, hook, CAT_STAGE2);
+        if (e != cudaSuccess) return e;
+        if ((e = boundary(seq[k], k + 1, R(0))) != cudaSuccess) return e;
+    }
+    const dim3 eg((nx + 255) / 256, ny);
+    hook(CAT_FINALIZE, 0);
+    rk2n_backup_kernel<R><<<eg, 256, 0, s>>>(nx, ny, pitch, planes[A][0], planes[A][1], planes[A][2], planes[B][0],
+                                            planes[B][1], planes[B][2], n_inverse);
+    hook(CAT_FINALIZE, 1);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    // the last sub-step, (n-1)/n of dt
+    Rk2Args<R> a4 = a;
+    a4.dt_scale = (R(1) * R(RK2N_N) - R(1)) * n_inverse;
+    e = later_stage<R>(a4, planes, B, C, has_dt, lines + 3 * (int64_t)L, c, s, hook, CAT_STAGE2);
+    if (e != cudaSuccess) return e;
+    if ((e = boundary(C, RK2N_N - 2, a4.dt_scale)) != cudaSuccess) return e;
+    hook(CAT_MAXSTAGE, 0);
+    rk2n_final_kernel<R><<<eg, 256, 0, s>>>(nx, ny, pitch, planes[C][0], planes[C][1], planes[C][2], planes[A][0],
+                                           planes[A][1], planes[A][2], max_stage, c.xl, c.xu, c.yl, c.yu);
+    hook(CAT_MAXSTAGE, 1);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    hook(CAT_FINALIZE, 0);
+    rk2_finalize_kernel<R><<<1, 1024, 0, s>>>(nx, ny, c.exterior_cells_width, lines, FIN_RK2N, has_dt ? 0 : 1,
+                                              dt_sub, a.max_dt_inv_init, sc);
+    hook(CAT_FINALIZE, 1);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    cur = C;
+    return cudaSuccess;
+}
+
+#define SWALS_INST_FV_STEPS(R)                                                                                      \
+    template cudaError_t launch_midpoint_step<R>(R *const[3][3], int &, R *, R *, R *, int, int, int64_t,           \
+                                                 const Metrics<R> &, const StepConfig &, bool, double,              \
+                                                 const Rk2Buffers &, DevScalars *, cudaStream_t, const LaunchHook &); \
+    template cudaError_t launch_rk2n_step<R>(R *const[3][3], int &, R *, R *, R *, int, int, int64_t,               \
+                                             const Metrics<R> &, const StepConfig &, bool, double,                  \
+                                             const Rk2Buffers &, DevScalars *, cudaStream_t, const LaunchHook &);
+SWALS_INST_FV_STEPS(double)
+SWALS_INST_FV_STEPS(float)
 
 template cudaError_t launch_rk2_step<double>(double *const[3][3], int &, double *, double *, double *, int, int,
                                              int64_t, const Metrics<double> &, const StepConfig &, bool, double,

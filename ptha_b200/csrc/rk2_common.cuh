@@ -47,6 +47,8 @@ struct Rk2Args {
     double *lines;                 // flux_STG on the 4 boundary-flux lines: N[nx], E[ny], S[nx], W[ny]
     DevScalars *sc;
     EdgePlanes<R> ep;              // MODE_FLUX output / stage-1 update input
+    R dt_scale;                    // the stage's dt times this (midpoint half step, rk2n last step; else 1)
+    int base0;                     // stage 1 updates U0 (stg0..) with this state's fluxes (midpoint)
 };
 
 template <typename R> struct Cell { R stg, dep, u, v, elv; };
@@ -183,9 +185,9 @@ __device__ __forceinline__ R stage_dt(const Rk2Args<R> &a)
     if (a.dt_from_cfl) {
         const double bits_max = __longlong_as_double((long long)a.sc->max_dt_inv_bits);
         const R inv = R(fmax(a.max_dt_inv_init, bits_max));
-        return R(1) / inv;
+        return (R(1) / inv) * a.dt_scale;
     }
-    return R(a.dt_fixed);
+    return R(a.dt_fixed) * a.dt_scale;
 }
 
 // update_U for cell (i, r) (update_U_DE1_inner_include.f90:38-96) from its
@@ -206,6 +208,11 @@ __device__ __forceinline__ void fv_update(const Rk2Args<R> &a, int i, int r, con
     if (c.dep > mad) { Um_uh = a.uh[o]; Um_vh = a.vh[o]; }
     else { Um_uh = R(0); Um_vh = R(0); }
     R U_uh = Um_uh, U_vh = Um_vh;
+    if (MODE == MODE_STAGE1 && a.base0) {
+        // one_midpoint_step's full step: U was reset to the backup, and
+        // update_U applies the midpoint's fluxes to it.
+        U_stg = a.stg0[o]; U_uh = a.uh0[o]; U_vh = a.vh0[o];
+    }
 
     const R inv_cell_area_dt = dt / a.m.area[r];
     U_stg = U_stg - inv_cell_area_dt * ((n_hi.f[0] - n_lo.f[0]) + (w_hi.f[0] - w_lo.f[0]));

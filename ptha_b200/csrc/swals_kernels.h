@@ -134,6 +134,16 @@ cudaError_t launch_rk2_step(R *const planes[3][3], int &cur, R *elv, R *max_stag
                             int64_t pitch, const Metrics<R> &m, const StepConfig &c, bool has_dt, double dt,
                             bool euler_only, const Rk2Buffers &buf, DevScalars *sc, cudaStream_t s,
                             const LaunchHook &hook);
+// one_midpoint_step / one_rk2n_step (timestepping_alternatives_include.f90:
+// 149-337) on the same stage kernels; the same arguments as launch_rk2_step.
+template <typename R>
+cudaError_t launch_midpoint_step(R *const planes[3][3], int &cur, R *elv, R *max_stage, R *manning_sq, int nx, int ny,
+                                 int64_t pitch, const Metrics<R> &m, const StepConfig &c, bool has_dt, double dt,
+                                 const Rk2Buffers &buf, DevScalars *sc, cudaStream_t s, const LaunchHook &hook);
+template <typename R>
+cudaError_t launch_rk2n_step(R *const planes[3][3], int &cur, R *elv, R *max_stage, R *manning_sq, int nx, int ny,
+                             int64_t pitch, const Metrics<R> &m, const StepConfig &c, bool has_dt, double dt,
+                             const Rk2Buffers &buf, DevScalars *sc, cudaStream_t s, const LaunchHook &hook);
 
 // Reductions used by diagnostics.
 template <typename R>

@@ -37,7 +37,7 @@ class Domain:
                  linear_solver_is_truely_linear=True, friction_type="manning", linear_friction_coeff=0.0,
                  maximum_timestep=1.0e20, boundary_exterior=(True, True, True, True),
                  boundary_kind=_lib.BC_NONE, boundary_function_kind=_lib.BF_NONE, boundary_function_params=(),
-                 record_max_stage=True, xL=0, xU=0, yL=0, yU=0, boundary_subroutine=None,
+                 record_max_stage=True, xL=0, xU=0, yL=0, yU=0, exterior_cells_width=2, boundary_subroutine=None,
                  forcing_subroutine=None, device=-1):
         L = _lib.lib()
         self._L = L
@@ -62,6 +62,7 @@ class Domain:
         for k in range(4):
             d.boundary_exterior[k] = int(bool(boundary_exterior[k]))
         d.boundary_kind = int(boundary_kind)
+        d.exterior_cells_width = int(exterior_cells_width)
         d.boundary_function_kind = int(boundary_function_kind)
         for k, v in enumerate(boundary_function_params):
             d.boundary_function_params[k] = float(v)

@@ -53,8 +53,7 @@ def test_unknown_method_is_rejected():
     assert e.value.code == 2 and "not recognized" in str(e.value)
 
 
-@pytest.mark.parametrize("m", ["rk2n", "midpoint", "cliffs", "leapfrog_nonlinear",
-                               "leapfrog_linear_plus_nonlinear_friction"])
+@pytest.mark.parametrize("m", ["cliffs", "leapfrog_nonlinear", "leapfrog_linear_plus_nonlinear_friction"])
 def test_valid_but_unimplemented_methods(m):
     with pytest.raises(SwalsError) as e:
         _create(timestepping_method=m)
@@ -93,3 +92,21 @@ def test_no_cpu_fallback():
     with pytest.raises(SwalsError) as e:
         _create()
     assert e.value.code == 9
+
+
+def test_boundary_kind_checks():
+    import torch
+    # Flather is a known kind: on a CPU box only the missing device stops it.
+    if not torch.cuda.is_available():
+        with pytest.raises(SwalsError) as e:
+            _create(boundary_kind=_lib.BC_FLATHER)
+        assert e.value.code == 9
+    with pytest.raises(SwalsError) as e:
+        _create(boundary_kind=4)
+    assert e.value.code == 1
+    with pytest.raises(SwalsError) as e:
+        _create(boundary_kind=_lib.BC_FLATHER, boundary_function_kind=7)
+    assert e.value.code == 6
+    with pytest.raises(SwalsError) as e:
+        _create(boundary_kind=_lib.BC_FLATHER, exterior_cells_width=1)
+    assert e.value.code == 3
