@@ -249,7 +249,7 @@ int evolve_t(swals_domain *d, double timestep, int has_dt)
         Rk2Buffers buf;
         buf.side = d->side;
         buf.partials = d->lines;
-        buf.partials_len = 4 * (2 * d->nx + 2 * d->ny);
+        buf.partials_len = 5 * (2 * d->nx + 2 * d->ny);
         buf.edges = d->edges;
         if (d->method == M_MIDPOINT)
             e = launch_midpoint_step<R>(pl, d->cur, (R *)d->elv, max_stage, (R *)d->manning_sq, d->nx, d->ny,
@@ -403,7 +403,7 @@ int swals_gpu_domain_create(const swals_domain_desc *desc, swals_domain **out)
     for (int k = 0; k < 8; k++) total += al(metric_elems[k] * es);
     total += al(sizeof(swals::DevScalars));
     const size_t side_bytes = al((size_t)(4 * ny + 4 * nx) * 3 * es);
-    const size_t lines_bytes = al((size_t)4 * (2 * nx + 2 * ny) * sizeof(double));   // 4 flux evaluations (rk2n)
+    const size_t lines_bytes = al((size_t)5 * (2 * nx + 2 * ny) * sizeof(double));   // 5 flux evaluations (rk2n)
     d->scratch_len = (nx > ny ? nx : ny) + 4096;
     const size_t scratch_bytes = al((size_t)d->scratch_len * sizeof(double));
     total += side_bytes + lines_bytes + scratch_bytes + al(64);

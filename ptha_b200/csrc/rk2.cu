@@ -399,8 +399,8 @@ cudaError_t launch_boundary(const BcArgs<R> &b, cudaStream_t s)
 // End of a step: domain%max_dt, time, boundary-flux integrals, counters
 // (timestepping_alternatives_include.f90:36-50,121-144; domain_mod.f90:1800-1810).
 // kind: FIN_RK2 (two Euler stages averaged), FIN_EULER, FIN_MIDPOINT (the
-// store of the midpoint's fluxes), FIN_RK2N (n-1 = 4 Euler steps,
-// timestepping_alternatives_include.f90:149-270).  `lines` holds one set of
+// store of the midpoint's fluxes), FIN_RK2N (n = 5 Euler steps, the last
+// one shortened, timestepping_alternatives_include.f90:149-270).  `lines` holds one set of
 // 2 nx + 2 ny boundary-flux line values per flux evaluation.
 enum { FIN_RK2 = 0, FIN_EULER = 1, FIN_MIDPOINT = 2, FIN_RK2N = 3 };
 constexpr int RK2N_N = 5;   // rk2n_n_value (domain_mod.f90:90)
@@ -410,10 +410,10 @@ __global__ void __launch_bounds__(1024) rk2_finalize_kernel(int nx, int ny, int 
                                                             int dt_from_cfl, double dt_fixed, double max_dt_inv_init,
                                                             DevScalars *sc)
 {
-    __shared__ double red[16][32];
-    double acc[16];
-    for (int k = 0; k < 16; k++) acc[k] = 0.0;
-    const int nsets = (kind == FIN_EULER) ? 1 : (kind == FIN_RK2N) ? 4 : 2;
+    __shared__ double red[4 * RK2N_N][32];
+    double acc[4 * RK2N_N];
+    for (int k = 0; k < 4 * RK2N_N; k++) acc[k] = 0.0;
+    const int nsets = (kind == FIN_EULER) ? 1 : (kind == FIN_RK2N) ? RK2N_N : 2;
     const int L = 2 * nx + 2 * ny;
     for (int q = threadIdx.x; q < L; q += blockDim.x) {
         int line, idx;
@@ -434,7 +434,7 @@ __global__ void __launch_bounds__(1024) rk2_finalize_kernel(int nx, int ny, int 
     __syncthreads();
     if (threadIdx.x != 0) return;
     const int nw = blockDim.x >> 5;
-    double s[16];
+    double s[4 * RK2N_N];
     for (int k = 0; k < 4 * nsets; k++) {
         double v = 0.0;
         for (int w = 0; w < nw; w++) v += red[k][w];
@@ -445,7 +445,7 @@ __global__ void __launch_bounds__(1024) rk2_finalize_kernel(int nx, int ny, int 
     const double max_dt = (double)(R(1) / max_dt_inv);
     const double dt = dt_from_cfl ? max_dt : (double)R(dt_fixed);
     const double time0 = sc->time;
-    double store[4][4], tot[4];
+    double store[RK2N_N][4], tot[RK2N_N];
     for (int q = 0; q < nsets; q++) {
         store[q][0] = s[4 * q]; store[q][1] = s[4 * q + 1]; store[q][2] = -s[4 * q + 2]; store[q][3] = -s[4 * q + 3];
         tot[q] = 0.0;
@@ -468,13 +468,13 @@ __global__ void __launch_bounds__(1024) rk2_finalize_kernel(int nx, int ny, int 
     } else {
         const R n_inverse = R(1) / (R(1) * R(RK2N_N));
         integral = 0.0;
-        for (int q = 0; q < RK2N_N - 2; q++) integral = integral + dt * tot[q];
+        for (int q = 0; q < RK2N_N - 1; q++) integral = integral + dt * tot[q];
         integral = integral * (double)(R(RK2N_N) - R(1)) * (double)n_inverse;
         const R reduced_dt = (R(1) * R(RK2N_N) - R(1)) * n_inverse * R(dt);
-        integral = integral + (double)reduced_dt * tot[3];
+        integral = integral + (double)reduced_dt * tot[RK2N_N - 1];
         dt_last = (double)reduced_dt;
         t_end = time0 + (double)(R(dt) * R(RK2N_N - 1));
-        last = 3;
+        last = RK2N_N - 1;
     }
     for (int k = 0; k < 4; k++) sc->boundary_flux_store[k] = store[last][k];
     sc->boundary_flux_evolve_integral = integral;
@@ -937,9 +937,9 @@ cudaError_t launch_midpoint_step(R *const planes[3][3], int &cur, R *elv, R *max
 }
 
 // one_rk2n_step (timestepping_alternatives_include.f90:149-270) with n = 5:
-// A holds the backup; Euler steps A -> B -> C -> B, backup = (backup - U)/n,
-// the last step B -> C with (n-1)/n of dt, and U = C + backup.  `dt` is the
-// caller's timestep (n-1 sub-steps of dt/(n-1)).
+// A holds the backup; n-1 Euler steps A -> B -> C -> B -> C, backup =
+// (backup - U)/n, a last step C -> B with (n-1)/n of dt, and U = B + backup.
+// `dt` is the caller's timestep (n-1 sub-steps of dt/(n-1)).
 template <typename R>
 cudaError_t launch_rk2n_step(R *const planes[3][3], int &cur, R *elv, R *max_stage, R *manning_sq, int nx, int ny,
                              int64_t pitch, const Metrics<R> &m, const StepConfig &c, bool has_dt, double dt,
@@ -969,27 +969,29 @@ cudaError_t launch_rk2n_step(R *const planes[3][3], int &cur, R *elv, R *max_sta
     };
     if ((e = boundary(B, 1, R(0))) != cudaSuccess) return e;
     // sub-steps 2 .. n-1
-    const int seq[3] = {B, C, B};
-    for (int k = 1; k < RK2N_N - 2; k++) {
+    const int seq[RK2N_N] = {B, C, B, C, B};
+    for (int k = 1; k < RK2N_N - 1; k++) {
         e = later_stage<R>(a, planes, seq[k - 1], seq[k], has_dt, lines + (int64_t)k * L, c, s, hook, CAT_STAGE2);
         if (e != cudaSuccess) return e;
         if ((e = boundary(seq[k], k + 1, R(0))) != cudaSuccess) return e;
     }
+    const int U4 = seq[RK2N_N - 2], U5 = seq[RK2N_N - 1];
     const dim3 eg((nx + 255) / 256, ny);
     hook(CAT_FINALIZE, 0);
-    rk2n_backup_kernel<R><<<eg, 256, 0, s>>>(nx, ny, pitch, planes[A][0], planes[A][1], planes[A][2], planes[B][0],
-                                            planes[B][1], planes[B][2], n_inverse);
+    rk2n_backup_kernel<R><<<eg, 256, 0, s>>>(nx, ny, pitch, planes[A][0], planes[A][1], planes[A][2], planes[U4][0],
+                                            planes[U4][1], planes[U4][2], n_inverse);
     hook(CAT_FINALIZE, 1);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     // the last sub-step, (n-1)/n of dt
-    Rk2Args<R> a4 = a;
-    a4.dt_scale = (R(1) * R(RK2N_N) - R(1)) * n_inverse;
-    e = later_stage<R>(a4, planes, B, C, has_dt, lines + 3 * (int64_t)L, c, s, hook, CAT_STAGE2);
+    Rk2Args<R> a5 = a;
+    a5.dt_scale = (R(1) * R(RK2N_N) - R(1)) * n_inverse;
+    e = later_stage<R>(a5, planes, U4, U5, has_dt, lines + (int64_t)(RK2N_N - 1) * L, c, s, hook, CAT_STAGE2);
     if (e != cudaSuccess) return e;
-    if ((e = boundary(C, RK2N_N - 2, a4.dt_scale)) != cudaSuccess) return e;
+    if ((e = boundary(U5, RK2N_N - 1, a5.dt_scale)) != cudaSuccess) return e;
     hook(CAT_MAXSTAGE, 0);
-    rk2n_final_kernel<R><<<eg, 256, 0, s>>>(nx, ny, pitch, planes[C][0], planes[C][1], planes[C][2], planes[A][0],
-                                           planes[A][1], planes[A][2], max_stage, c.xl, c.xu, c.yl, c.yu);
+    rk2n_final_kernel<R><<<eg, 256, 0, s>>>(nx, ny, pitch, planes[U5][0], planes[U5][1], planes[U5][2],
+                                           planes[A][0], planes[A][1], planes[A][2], max_stage, c.xl, c.xu, c.yl,
+                                           c.yu);
     hook(CAT_MAXSTAGE, 1);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     hook(CAT_FINALIZE, 0);
@@ -997,7 +999,7 @@ cudaError_t launch_rk2n_step(R *const planes[3][3], int &cur, R *elv, R *max_sta
                                               dt_sub, a.max_dt_inv_init, sc);
     hook(CAT_FINALIZE, 1);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    cur = C;
+    cur = U5;
     return cudaSuccess;
 }
 
