@@ -89,6 +89,10 @@ typedef struct swals_domain_desc {
     int32_t has_host_boundary_subroutine; /* nonzero: a host callback was set -> rejected */
     int32_t has_host_forcing_subroutine;  /* nonzero: a host callback was set -> rejected */
     int32_t device;                 /* CUDA device ordinal; -1 = the calling thread's current device */
+    char    compute_fluxes_inner_method[64]; /* domain%compute_fluxes_inner_method (default
+                                        'DE1_low_fr_diffusion'; also 'DE1', 'DE1_upwind_transverse',
+                                        'DE1_low_fr_diffusion_upwind_transverse',
+                                        compute_fluxes_alternatives_include.f90:11-64) */
 } swals_domain_desc;
 
 typedef struct swals_domain_state {

@@ -18,6 +18,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 
+# compute_fluxes_inner_method -> flux_variant bits (1: fr2 = 1, 2: upwind transverse momentum)
+FLUX_VARIANTS = {"DE1_low_fr_diffusion": 0, "DE1": 1, "DE1_upwind_transverse": 3,
+                 "DE1_low_fr_diffusion_upwind_transverse": 2}
 METHODS = {
     "rk2": 1, "rk2n": 2, "midpoint": 3, "euler": 4, "linear": 5,
     "leapfrog_linear_plus_nonlinear_friction": 6, "cliffs": 7, "leapfrog_nonlinear": 8,
@@ -49,7 +52,7 @@ class _OracleDomainC(ctypes.Structure):
         ("xL", ctypes.c_int32), ("xU", ctypes.c_int32), ("yL", ctypes.c_int32), ("yU", ctypes.c_int32),
         ("exterior_cells_width", ctypes.c_int32), ("boundary_exterior", ctypes.c_int32 * 4),
         ("bc_kind", ctypes.c_int32), ("bf_kind", ctypes.c_int32), ("record_max_stage", ctypes.c_int32),
-        ("pad0", ctypes.c_int32),
+        ("flux_variant", ctypes.c_int32),
         ("theta", ctypes.c_double), ("cfl", ctypes.c_double), ("msl_linear", ctypes.c_double),
         ("linear_friction_coeff", ctypes.c_double), ("maximum_timestep", ctypes.c_double),
         ("bf_params", ctypes.c_double * 8),
@@ -84,7 +87,7 @@ class OracleDomain:
                  linear_friction_coeff=0.0, maximum_timestep=1.0e20,
                  boundary_exterior=(True, True, True, True), bc_kind=BC_NONE,
                  bf_kind=0, bf_params=(), record_max_stage=True, real32=False,
-                 xL=0, xU=0, yL=0, yU=0):
+                 xL=0, xU=0, yL=0, yU=0, compute_fluxes_inner_method="DE1_low_fr_diffusion"):
         self.real32 = real32
         self.dtype = np.float32 if real32 else np.float64
         self.lib = _load(real32)
@@ -107,6 +110,7 @@ class OracleDomain:
         for k, v in enumerate(bf_params):
             c.bf_params[k] = v
         c.record_max_stage = int(record_max_stage)
+        c.flux_variant = FLUX_VARIANTS[compute_fluxes_inner_method]
         c.theta = NEG_HUGE if theta is None else theta
         c.cfl = NEG_HUGE if cfl is None else cfl
         c.msl_linear = msl_linear

@@ -869,12 +869,18 @@ double ORACLE_FN(compute_fluxes_DE1_low_fr_diffusion)(oracle_domain *d)
                 REAL sminsmax = s_min * s_max * ONE;
                 REAL fr2num = ((v_neg * v_neg + v_pos * v_pos) + u_neg * u_neg) + u_pos * u_pos;
                 REAL fr2den = ((gs_neg * gs_neg + gs_pos * gs_pos) + (REAL)1.0e-10);
-                REAL fr2 = ADVECTION_BETA * (REAL)sqrt(rmax((REAL)0.001, rmin(ONE, fr2num / fr2den)));
+                /* reduced_momentum_diffusion (DE1_low_fr_diffusion variants), else 1 */
+                REAL fr2 = (d->flux_variant & OR_FLUX_PLAIN_DIFFUSION)
+                               ? ONE
+                               : ADVECTION_BETA * (REAL)sqrt(rmax((REAL)0.001, rmin(ONE, fr2num / fr2den)));
 
                 FNS(i, j, OR_STG) = (REAL)((double)((s_max * vd_neg - s_min * vd_pos) +
                                                      sminsmax * (stage_pos_star - stage_neg_star)) * inv_denom);
-                FNS(i, j, OR_UH) = (REAL)((double)((s_max * ud_neg * vel_beta_neg - s_min * ud_pos * vel_beta_pos) +
-                                                    fr2 * sminsmax * (ud_pos - ud_neg)) * inv_denom);
+                if (d->flux_variant & OR_FLUX_UPWIND_TRANSVERSE)
+                    FNS(i, j, OR_UH) = ADVECTION_BETA * ((FNS(i, j, OR_STG) > ZERO) ? u_neg : u_pos) * FNS(i, j, OR_STG);
+                else
+                    FNS(i, j, OR_UH) = (REAL)((double)((s_max * ud_neg * vel_beta_neg - s_min * ud_pos * vel_beta_pos) +
+                                                        fr2 * sminsmax * (ud_pos - ud_neg)) * inv_denom);
                 FNS(i, j, OR_VH) = (REAL)((double)((s_max * vd_neg * vel_beta_neg - s_min * vd_pos * vel_beta_pos) +
                                                     fr2 * sminsmax * (vd_pos - vd_neg)) * inv_denom);
 
@@ -942,14 +948,19 @@ double ORACLE_FN(compute_fluxes_DE1_low_fr_diffusion)(oracle_domain *d)
                 REAL sminsmax = s_min * s_max * ONE;
                 REAL fr2num = ((v_neg * v_neg + v_pos * v_pos) + u_neg * u_neg) + u_pos * u_pos;
                 REAL fr2den = ((gs_neg * gs_neg + gs_pos * gs_pos) + (REAL)1.0e-10);
-                REAL fr2 = ADVECTION_BETA * (REAL)sqrt(rmax((REAL)0.001, rmin(ONE, fr2num / fr2den)));
+                REAL fr2 = (d->flux_variant & OR_FLUX_PLAIN_DIFFUSION)
+                               ? ONE
+                               : ADVECTION_BETA * (REAL)sqrt(rmax((REAL)0.001, rmin(ONE, fr2num / fr2den)));
 
                 FEW(i, j, OR_STG) = (REAL)((double)((s_max * ud_neg - s_min * ud_pos) +
                                                      sminsmax * (stage_pos_star - stage_neg_star)) * inv_denom);
                 FEW(i, j, OR_UH) = (REAL)((double)((s_max * ud_neg * vel_beta_neg - s_min * ud_pos * vel_beta_pos) +
                                                     fr2 * sminsmax * (ud_pos - ud_neg)) * inv_denom);
-                FEW(i, j, OR_VH) = (REAL)((double)((s_max * vd_neg * vel_beta_neg - s_min * vd_pos * vel_beta_pos) +
-                                                    fr2 * sminsmax * (vd_pos - vd_neg)) * inv_denom);
+                if (d->flux_variant & OR_FLUX_UPWIND_TRANSVERSE)
+                    FEW(i, j, OR_VH) = ADVECTION_BETA * ((FEW(i, j, OR_STG) > ZERO) ? v_neg : v_pos) * FEW(i, j, OR_STG);
+                else
+                    FEW(i, j, OR_VH) = (REAL)((double)((s_max * vd_neg * vel_beta_neg - s_min * vd_pos * vel_beta_pos) +
+                                                        fr2 * sminsmax * (vd_pos - vd_neg)) * inv_denom);
 
                 double half_g_hh_edge = inv_denom * half_gravity *
                     ((double)s_max * depth_neg_star * depth_neg_star - (double)s_min * depth_pos_star * depth_pos_star);

@@ -55,6 +55,15 @@ enum {
     OR_BC_FLATHER = 3                             /* boundary_mod.f90:502-730 */
 };
 
+/* compute_fluxes_inner_method (compute_fluxes_alternatives_include.f90:11-64):
+ * 'DE1_low_fr_diffusion' = 0, 'DE1' = PLAIN_DIFFUSION,
+ * 'DE1_upwind_transverse' = PLAIN_DIFFUSION | UPWIND_TRANSVERSE,
+ * 'DE1_low_fr_diffusion_upwind_transverse' = UPWIND_TRANSVERSE. */
+enum {
+    OR_FLUX_PLAIN_DIFFUSION = 1,   /* reduced_momentum_diffusion = .false. */
+    OR_FLUX_UPWIND_TRANSVERSE = 2  /* upwind_transverse_momentum = .true. */
+};
+
 /* Analytic boundary functions (domain%boundary_function) for
  * OR_BC_STAGE_TRANSMISSIVE_NORMAL_MOMENTUM and OR_BC_FLATHER. */
 enum {
@@ -80,7 +89,7 @@ typedef struct oracle_domain {
     int32_t bc_kind;
     int32_t bf_kind;
     int32_t record_max_stage;
-    int32_t pad0;
+    int32_t flux_variant;        /* compute_fluxes_inner_method: OR_FLUX_* bits, 0 = 'DE1_low_fr_diffusion' */
     double theta, cfl, msl_linear, linear_friction_coeff, maximum_timestep;
     double bf_params[8];
     /* state */

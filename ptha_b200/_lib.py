@@ -69,7 +69,7 @@ class DomainDesc(ctypes.Structure):
         ("boundary_function_kind", ctypes.c_int32), ("boundary_function_params", ctypes.c_double * 8),
         ("record_max_stage", ctypes.c_int32), ("exterior_cells_width", ctypes.c_int32),
         ("has_host_boundary_subroutine", ctypes.c_int32), ("has_host_forcing_subroutine", ctypes.c_int32),
-        ("device", ctypes.c_int32),
+        ("device", ctypes.c_int32), ("compute_fluxes_inner_method", ctypes.c_char * 64),
     ]
 
 

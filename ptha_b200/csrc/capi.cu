@@ -69,6 +69,19 @@ int parse_method(const char *s, int *m, double *def_cfl, double *def_theta)
     return 0;
 }
 
+// domain%compute_fluxes_inner_method (domain_mod.f90:1448-1484) -> fv::FLUX_*
+// bits; empty = the default 'DE1_low_fr_diffusion'.  -1: not implemented.
+int parse_flux_method(const char *s, size_t cap)
+{
+    std::string name(s, strnlen(s, cap));
+    while (!name.empty() && name.back() == ' ') name.pop_back();
+    if (name.empty() || name == "DE1_low_fr_diffusion") return 0;
+    if (name == "DE1") return swals::FLUX_PLAIN_DIFFUSION;
+    if (name == "DE1_upwind_transverse") return swals::FLUX_PLAIN_DIFFUSION | swals::FLUX_UPWIND_TRANSVERSE;
+    if (name == "DE1_low_fr_diffusion_upwind_transverse") return swals::FLUX_UPWIND_TRANSVERSE;
+    return -1;
+}
+
 bool is_staggered(int m) { return m == M_LINEAR || m == M_LF_LIN_NLFRIC || m == M_LF_NONLINEAR; }
 
 }  // namespace
@@ -309,6 +322,8 @@ int swals_gpu_desc_init(swals_domain_desc *desc)
     desc->record_max_stage = 1;
     desc->exterior_cells_width = 2;
     desc->device = -1;
+    snprintf(desc->compute_fluxes_inner_method, sizeof(desc->compute_fluxes_inner_method), "%s",
+             "DE1_low_fr_diffusion");
     return SWALS_OK;
 }
 
@@ -332,6 +347,11 @@ int swals_gpu_domain_create(const swals_domain_desc *desc, swals_domain **out)
         return fail(SWALS_ERR_INVALID_ARGUMENT, "real_bytes must be 4 or 8");
     if (desc->coriolis && !desc->spherical)
         return fail(SWALS_ERR_INVALID_ARGUMENT, "Cannot define preprocessing flag CORIOLIS without also defining SPHERICAL");
+    const int flux_variant = parse_flux_method(desc->compute_fluxes_inner_method,
+                                               sizeof(desc->compute_fluxes_inner_method));
+    if (flux_variant < 0)
+        return fail(SWALS_ERR_UNSUPPORTED, "compute_fluxes_inner_method '%.64s' is not implemented on the GPU path",
+                    desc->compute_fluxes_inner_method);
     if (desc->boundary_kind < 0 || desc->boundary_kind > 3)
         return fail(SWALS_ERR_INVALID_ARGUMENT, "unknown boundary_kind %d", desc->boundary_kind);
     if (desc->boundary_function_kind < 0 || desc->boundary_function_kind > 1)
@@ -373,6 +393,7 @@ int swals_gpu_domain_create(const swals_domain_desc *desc, swals_domain **out)
     c.yu = (desc->yU > 0 ? desc->yU : ny) - 1;
     for (int k = 0; k < 4; k++) c.bext[k] = desc->boundary_exterior[k] ? 1 : 0;
     c.bc_kind = desc->boundary_kind;
+    c.flux_variant = flux_variant;
     c.bf.kind = desc->boundary_function_kind;
     for (int k = 0; k < 8; k++) c.bf.p[k] = desc->boundary_function_params[k];
     c.spherical = desc->spherical;

@@ -536,7 +536,7 @@ __device__ __forceinline__ fv::Grad<R> fv_grad(const fv::Cell<R> &lo, const fv::
 // flux_EW; zero where the reference never computes an edge.
 template <typename R, bool NS>
 __device__ void fv_edge(const R *stg, const R *uh, const R *vh, const R *elv, int64_t P, int nx, int ny,
-                        const Metrics<R> &m, R theta, int i0, int e0, R out[3])
+                        const Metrics<R> &m, R theta, int variant, int i0, int e0, R out[3])
 {
     out[0] = out[1] = out[2] = R(0);
     fv::Cell<R> c[4];
@@ -553,7 +553,7 @@ __device__ void fv_edge(const R *stg, const R *uh, const R *vh, const R *elv, in
         gh = (e0 > 0 && e0 < ny - 1) ? fv_grad<R>(c[1], c[2], c[3], theta) : zero;
         fv::EdgeRes<R> res;
         double cand;
-        fv::edge_flux<R, true>(c[1], gl, c[2], gh, m.dxb[e0], R(1), res, cand);
+        fv::edge_flux<R, true>(c[1], gl, c[2], gh, m.dxb[e0], R(1), res, cand, variant);
         out[0] = res.f[0]; out[1] = res.f[1]; out[2] = res.f[2];
     } else {
         // EW edge at 0-based column e0 (west face of column e0), row i0.
@@ -566,7 +566,7 @@ __device__ void fv_edge(const R *stg, const R *uh, const R *vh, const R *elv, in
         gh = (e0 > 0 && e0 < nx - 1) ? fv_grad<R>(c[1], c[2], c[3], theta) : zero;
         fv::EdgeRes<R> res;
         double cand;
-        fv::edge_flux<R, false>(c[1], gl, c[2], gh, m.dyl[e0], R(1), res, cand);
+        fv::edge_flux<R, false>(c[1], gl, c[2], gh, m.dyl[e0], R(1), res, cand, variant);
         out[0] = res.f[0]; out[1] = res.f[1]; out[2] = res.f[2];
     }
 }
@@ -574,7 +574,7 @@ __device__ void fv_edge(const R *stg, const R *uh, const R *vh, const R *elv, in
 // Finite-volume step: for each stage input S (U0, then U1 for rk2), add
 // dts * flux(S) to STG..VH (timestepping_alternatives_include.f90:50-59, 95-118).
 template <typename R>
-__global__ void integral_fv_kernel(DomPtr d, Metrics<R> m, R theta, const R *s1, const R *u1, const R *v1, const R *s2,
+__global__ void integral_fv_kernel(DomPtr d, Metrics<R> m, R theta, int variant, const R *s1, const R *u1, const R *v1, const R *s2,
                                    const R *u2, const R *v2, const IBox *bx, int nbox, int64_t nitems, double *ints,
                                    R dts, int nstage)
 {
@@ -593,8 +593,8 @@ __global__ void integral_fv_kernel(DomPtr d, Metrics<R> m, R theta, const R *s1,
             const int mcol = B.b[0] + (int)(p % bl);
             const int ns = (e == 0) ? B.b[3] + 1 : B.b[2];
             if (!(ns >= 1 && ns <= d.ny + 1)) continue;
-            fv_edge<R, true>(s1, u1, v1, elv, d.P, d.nx, d.ny, m, theta, mcol - 1, ns - 1, f[0]);
-            if (nstage > 1) fv_edge<R, true>(s2, u2, v2, elv, d.P, d.nx, d.ny, m, theta, mcol - 1, ns - 1, f[1]);
+            fv_edge<R, true>(s1, u1, v1, elv, d.P, d.nx, d.ny, m, theta, variant, mcol - 1, ns - 1, f[0]);
+            if (nstage > 1) fv_edge<R, true>(s2, u2, v2, elv, d.P, d.nx, d.ny, m, theta, variant, mcol - 1, ns - 1, f[1]);
             xe = x + e * 4 * bl + (mcol - B.b[0]);
             len = bl;
         } else {
@@ -603,8 +603,8 @@ __global__ void integral_fv_kernel(DomPtr d, Metrics<R> m, R theta, const R *s1,
             const int mrow = B.b[2] + (int)(p % bw);
             const int ns = (e == 0) ? B.b[1] + 1 : B.b[0];
             if (!(ns >= 1 && ns <= d.nx + 1)) continue;
-            fv_edge<R, false>(s1, u1, v1, elv, d.P, d.nx, d.ny, m, theta, mrow - 1, ns - 1, f[0]);
-            if (nstage > 1) fv_edge<R, false>(s2, u2, v2, elv, d.P, d.nx, d.ny, m, theta, mrow - 1, ns - 1, f[1]);
+            fv_edge<R, false>(s1, u1, v1, elv, d.P, d.nx, d.ny, m, theta, variant, mrow - 1, ns - 1, f[0]);
+            if (nstage > 1) fv_edge<R, false>(s2, u2, v2, elv, d.P, d.nx, d.ny, m, theta, variant, mrow - 1, ns - 1, f[1]);
             xe = x + 8 * bl + e * 4 * bw + (mrow - B.b[2]);
             len = bw;
         }
@@ -835,7 +835,7 @@ static int integral_step(swals_multidomain *md, int k, int phase, int A, double 
         const bool euler = (d->method == M_EULER);
         const R dts = euler ? R(dt_local) : R(R(dt_local) * R(0.5));
         integral_fv_kernel<R><<<grid_for(pd.nitems), 256, 0, md->stream>>>(
-            p, m, R(d->cfg.theta), (const R *)d->planes[A][0], (const R *)d->planes[A][1], (const R *)d->planes[A][2],
+            p, m, R(d->cfg.theta), d->cfg.flux_variant, (const R *)d->planes[A][0], (const R *)d->planes[A][1], (const R *)d->planes[A][2],
             (const R *)d->planes[B][0], (const R *)d->planes[B][1], (const R *)d->planes[B][2], pd.d_box, pd.nbox,
             pd.nitems, md->d_int, dts, euler ? 1 : 2);
     }

@@ -176,7 +176,7 @@ __global__ void __launch_bounds__(NT, 3) rk2_stage_kernel(const Rk2Args<R> a)
         if (r >= 1 && r <= ny - 1 && i >= 1 && i <= nx - 1) {
             double cand;
             edge_flux<R, true>(S.cell.get(rr + 1, cc + 2), S.gns.get(rr, cc), S.cell.get(rr + 2, cc + 2), S.gns.get(rr + 1, cc),
-                               a.m.dxb[r], inv2, e, cand);
+                               a.m.dxb[r], inv2, e, cand, a.flux_variant);
             cfl = fmax(cfl, cand);
             if (MODE != MODE_CFL && a.lines) {
                 if (r == ny - a.n_ext && i >= a.n_ext && i <= nx - a.n_ext - 1) a.lines[i] = (double)e.f[0];
@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(NT, 3) rk2_stage_kernel(const Rk2Args<R> a)
             const R inv1 = R(1) / (a.m.dxb[r] * a.half_cfl);  // dx_cfl_half_inv(1)
             double cand;
             edge_flux<R, false>(S.cell.get(rr + 2, cc + 1), S.gew.get(rr, cc), S.cell.get(rr + 2, cc + 2), S.gew.get(rr, cc + 1),
-                                a.m.dyl[i], inv1, e, cand);
+                                a.m.dyl[i], inv1, e, cand, a.flux_variant);
             cfl = fmax(cfl, cand);
             if (MODE != MODE_CFL && a.lines) {
                 if (i == nx - a.n_ext && r >= a.n_ext && r <= ny - a.n_ext - 1) a.lines[nx + r] = (double)e.f[0];
@@ -405,15 +405,16 @@ cudaError_t launch_boundary(const BcArgs<R> &b, cudaStream_t s)
 enum { FIN_RK2 = 0, FIN_EULER = 1, FIN_MIDPOINT = 2, FIN_RK2N = 3 };
 constexpr int RK2N_N = 5;   // rk2n_n_value (domain_mod.f90:90)
 
-template <typename R>
-__global__ void __launch_bounds__(1024) rk2_finalize_kernel(int nx, int ny, int n_ext, const double *lines, int kind,
+template <typename R, int KIND>
+__global__ void __launch_bounds__(1024) rk2_finalize_kernel(int nx, int ny, int n_ext, const double *lines,
                                                             int dt_from_cfl, double dt_fixed, double max_dt_inv_init,
                                                             DevScalars *sc)
 {
-    __shared__ double red[4 * RK2N_N][32];
-    double acc[4 * RK2N_N];
-    for (int k = 0; k < 4 * RK2N_N; k++) acc[k] = 0.0;
-    const int nsets = (kind == FIN_EULER) ? 1 : (kind == FIN_RK2N) ? RK2N_N : 2;
+    constexpr int NSETS = (KIND == FIN_EULER) ? 1 : (KIND == FIN_RK2N) ? RK2N_N : 2;
+    __shared__ double red[4 * NSETS][32];
+    double acc[4 * NSETS];
+#pragma unroll
+    for (int k = 0; k < 4 * NSETS; k++) acc[k] = 0.0;
     const int L = 2 * nx + 2 * ny;
     for (int q = threadIdx.x; q < L; q += blockDim.x) {
         int line, idx;
@@ -423,10 +424,17 @@ __global__ void __launch_bounds__(1024) rk2_finalize_kernel(int nx, int ny, int 
         else { line = 3; idx = q - 2 * nx - ny; }
         const int lim = (line == 0 || line == 2) ? nx : ny;
         if (idx < n_ext || idx > lim - n_ext - 1) continue;
-        for (int k = 0; k < nsets; k++) acc[4 * k + line] += lines[(int64_t)k * L + q];
+#pragma unroll
+        for (int k = 0; k < NSETS; k++) {
+            const double v = lines[(int64_t)k * L + q];
+#pragma unroll
+            for (int l = 0; l < 4; l++)
+                if (line == l) acc[4 * k + l] += v;
+        }
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int k = 0; k < 4 * nsets; k++) {
+#pragma unroll
+    for (int k = 0; k < 4 * NSETS; k++) {
         double v = acc[k];
         for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
         if (lane == 0) red[k][warp] = v;
@@ -434,8 +442,8 @@ __global__ void __launch_bounds__(1024) rk2_finalize_kernel(int nx, int ny, int 
     __syncthreads();
     if (threadIdx.x != 0) return;
     const int nw = blockDim.x >> 5;
-    double s[4 * RK2N_N];
-    for (int k = 0; k < 4 * nsets; k++) {
+    double s[4 * NSETS];
+    for (int k = 0; k < 4 * NSETS; k++) {
         double v = 0.0;
         for (int w = 0; w < nw; w++) v += red[k][w];
         s[k] = v;
@@ -445,8 +453,8 @@ __global__ void __launch_bounds__(1024) rk2_finalize_kernel(int nx, int ny, int 
     const double max_dt = (double)(R(1) / max_dt_inv);
     const double dt = dt_from_cfl ? max_dt : (double)R(dt_fixed);
     const double time0 = sc->time;
-    double store[RK2N_N][4], tot[RK2N_N];
-    for (int q = 0; q < nsets; q++) {
+    double store[NSETS][4], tot[NSETS];
+    for (int q = 0; q < NSETS; q++) {
         store[q][0] = s[4 * q]; store[q][1] = s[4 * q + 1]; store[q][2] = -s[4 * q + 2]; store[q][3] = -s[4 * q + 3];
         tot[q] = 0.0;
         for (int k = 0; k < 4; k++) tot[q] += store[q][k];
@@ -455,26 +463,26 @@ __global__ void __launch_bounds__(1024) rk2_finalize_kernel(int nx, int ny, int 
     double dt_last = dt;
     double t_end = time0 + dt;
     int last = 0;
-    if (kind == FIN_RK2) {
+    if (KIND == FIN_RK2) {
         integral = 0.0 + dt * tot[0];
         integral = integral + dt * tot[1];
         integral = 0.5 * integral;
         last = 1;
-    } else if (kind == FIN_EULER) {
+    } else if (KIND == FIN_EULER) {
         integral = 0.0 + dt * tot[0];
-    } else if (kind == FIN_MIDPOINT) {
+    } else if (KIND == FIN_MIDPOINT) {
         integral = tot[1] * dt;
         last = 1;
     } else {
         const R n_inverse = R(1) / (R(1) * R(RK2N_N));
         integral = 0.0;
-        for (int q = 0; q < RK2N_N - 1; q++) integral = integral + dt * tot[q];
+        for (int q = 0; q < NSETS - 1; q++) integral = integral + dt * tot[q];
         integral = integral * (double)(R(RK2N_N) - R(1)) * (double)n_inverse;
         const R reduced_dt = (R(1) * R(RK2N_N) - R(1)) * n_inverse * R(dt);
-        integral = integral + (double)reduced_dt * tot[RK2N_N - 1];
+        integral = integral + (double)reduced_dt * tot[NSETS - 1];
         dt_last = (double)reduced_dt;
         t_end = time0 + (double)(R(dt) * R(RK2N_N - 1));
-        last = RK2N_N - 1;
+        last = NSETS - 1;
     }
     for (int k = 0; k < 4; k++) sc->boundary_flux_store[k] = store[last][k];
     sc->boundary_flux_evolve_integral = integral;
@@ -672,6 +680,7 @@ Rk2Args<R> fv_args(int nx, int ny, int64_t pitch, R *elv, R *manning_sq, const M
     a.sc = sc;
     a.stg0 = nullptr; a.uh0 = nullptr; a.vh0 = nullptr;
     a.ep = EdgePlanes<R>{};
+    a.flux_variant = c.flux_variant;
     a.dt_scale = R(1);
     a.base0 = 0;
     a.lines = nullptr;
@@ -804,8 +813,8 @@ cudaError_t launch_rk2_step(R *const planes[3][3], int &cur, R *elv, R *max_stag
             if (e != cudaSuccess) return e;
         }
         hook(CAT_FINALIZE, 0);
-        rk2_finalize_kernel<R><<<1, 1024, 0, s>>>(nx, ny, c.exterior_cells_width, lines1, FIN_EULER,
-                                                  a.dt_from_cfl, dt, max_dt_inv_init, sc);
+        rk2_finalize_kernel<R, FIN_EULER><<<1, 1024, 0, s>>>(nx, ny, c.exterior_cells_width, lines1,
+                                                             a.dt_from_cfl, dt, max_dt_inv_init, sc);
         hook(CAT_FINALIZE, 1);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         cur = B;
@@ -835,7 +844,7 @@ cudaError_t launch_rk2_step(R *const planes[3][3], int &cur, R *elv, R *max_stag
         if (e != cudaSuccess) return e;
     }
     hook(CAT_FINALIZE, 0);
-    rk2_finalize_kernel<R><<<1, 1024, 0, s>>>(nx, ny, c.exterior_cells_width, lines1, FIN_RK2, a.dt_from_cfl,
+    rk2_finalize_kernel<R, FIN_RK2><<<1, 1024, 0, s>>>(nx, ny, c.exterior_cells_width, lines1, a.dt_from_cfl,
                                               dt, max_dt_inv_init, sc);
     hook(CAT_FINALIZE, 1);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -928,8 +937,8 @@ cudaError_t launch_midpoint_step(R *const planes[3][3], int &cur, R *elv, R *max
         if (e != cudaSuccess) return e;
     }
     hook(CAT_FINALIZE, 0);
-    rk2_finalize_kernel<R><<<1, 1024, 0, s>>>(nx, ny, c.exterior_cells_width, lines1, FIN_MIDPOINT,
-                                              has_dt ? 0 : 1, dt, a.max_dt_inv_init, sc);
+    rk2_finalize_kernel<R, FIN_MIDPOINT><<<1, 1024, 0, s>>>(nx, ny, c.exterior_cells_width, lines1,
+                                                            has_dt ? 0 : 1, dt, a.max_dt_inv_init, sc);
     hook(CAT_FINALIZE, 1);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     cur = C;
@@ -995,7 +1004,7 @@ cudaError_t launch_rk2n_step(R *const planes[3][3], int &cur, R *elv, R *max_sta
     hook(CAT_MAXSTAGE, 1);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     hook(CAT_FINALIZE, 0);
-    rk2_finalize_kernel<R><<<1, 1024, 0, s>>>(nx, ny, c.exterior_cells_width, lines, FIN_RK2N, has_dt ? 0 : 1,
+    rk2_finalize_kernel<R, FIN_RK2N><<<1, 1024, 0, s>>>(nx, ny, c.exterior_cells_width, lines, has_dt ? 0 : 1,
                                               dt_sub, a.max_dt_inv_init, sc);
     hook(CAT_FINALIZE, 1);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;

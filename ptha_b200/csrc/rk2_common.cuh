@@ -47,6 +47,7 @@ struct Rk2Args {
     double *lines;                 // flux_STG on the 4 boundary-flux lines: N[nx], E[ny], S[nx], W[ny]
     DevScalars *sc;
     EdgePlanes<R> ep;              // MODE_FLUX output / stage-1 update input
+    int flux_variant;              // FLUX_* bits (compute_fluxes_inner_method)
     R dt_scale;                    // the stage's dt times this (midpoint half step, rk2n last step; else 1)
     int base0;                     // stage 1 updates U0 (stg0..) with this state's fluxes (midpoint)
 };
@@ -95,9 +96,12 @@ struct EdgeRes {
 
 // One Audusse/HLL edge of DE1_inner_include.f90 (:187-430 NS, :456-716 EW).
 // NS=true: normal velocity v, edge between (i,j-1) and (i,j).
+// variant: compute_fluxes_inner_method as FLUX_* bits (swals_kernels.h);
+// 0 is the default 'DE1_low_fr_diffusion'.
 template <typename R, bool NS>
 __device__ __forceinline__ void edge_flux(const Cell<R> &cn, const Grad<R> &gn, const Cell<R> &cp, const Grad<R> &gp,
-                                          R edge_len, R dx_cfl_half_inv, EdgeRes<R> &out, double &cfl_cand)
+                                          R edge_len, R dx_cfl_half_inv, EdgeRes<R> &out, double &cfl_cand,
+                                          int variant = 0)
 {
     const R half = R(0.5);
     const double half_gravity = (double)(half * K<R>::gravity());
@@ -148,7 +152,8 @@ __device__ __forceinline__ void edge_flux(const Cell<R> &cn, const Grad<R> &gn, 
     const R sminsmax = s_min * s_max * R(1);
     const R fr2num = ((v_neg * v_neg + v_pos * v_pos) + u_neg * u_neg) + u_pos * u_pos;
     const R fr2den = (gs_neg * gs_neg + gs_pos * gs_pos) + R(1.0e-10);
-    const R fr2 = beta * R(sqrt(rmax(R(0.001), rmin(R(1), fr2num / fr2den))));
+    // reduced_momentum_diffusion (the low_fr_diffusion variants), else 1
+    const R fr2 = (variant & FLUX_PLAIN_DIFFUSION) ? R(1) : beta * R(sqrt(rmax(R(0.001), rmin(R(1), fr2num / fr2den))));
 
     const R qn_neg = NS ? vd_neg : ud_neg, qn_pos = NS ? vd_pos : ud_pos;
     const R qt_neg = NS ? ud_neg : vd_neg, qt_pos = NS ? ud_pos : vd_pos;
@@ -156,8 +161,12 @@ __device__ __forceinline__ void edge_flux(const Cell<R> &cn, const Grad<R> &gn, 
                        inv_denom);
     const R f_norm = R((double)((s_max * qn_neg * vel_beta_neg - s_min * qn_pos * vel_beta_pos) +
                                 fr2 * sminsmax * (qn_pos - qn_neg)) * inv_denom);
-    const R f_tran = R((double)((s_max * qt_neg * vel_beta_neg - s_min * qt_pos * vel_beta_pos) +
-                                fr2 * sminsmax * (qt_pos - qt_neg)) * inv_denom);
+    R f_tran;
+    if (variant & FLUX_UPWIND_TRANSVERSE)   // upwind_transverse_momentum: the transverse velocity upwind of the mass flux
+        f_tran = beta * ((f_mass > R(0)) ? (NS ? u_neg : v_neg) : (NS ? u_pos : v_pos)) * f_mass;
+    else
+        f_tran = R((double)((s_max * qt_neg * vel_beta_neg - s_min * qt_pos * vel_beta_pos) +
+                            fr2 * sminsmax * (qt_pos - qt_neg)) * inv_denom);
     out.f[0] = f_mass;
     out.f[1] = NS ? f_tran : f_norm;
     out.f[2] = NS ? f_norm : f_tran;

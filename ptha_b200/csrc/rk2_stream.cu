@@ -171,7 +171,7 @@ __global__ void __launch_bounds__(SLANES *SWARPS, 4) rk2_stream_kernel(const Rk2
             const int e = r - 1;
             if (e >= 1 && e <= ny - 1 && i >= 1 && i <= nx - 1) {
                 double cand;
-                edge_flux<R, true>(c2, g2, c1, g1, a.m.dxb[e], inv2, e_n, cand);
+                edge_flux<R, true>(c2, g2, c1, g1, a.m.dxb[e], inv2, e_n, cand, a.flux_variant);
                 cfl = fmax(cfl, cand);
                 if (MODE != MODE_CFL && a.lines && i >= a.n_ext && i <= nx - a.n_ext - 1) {
                     if (e == ny - a.n_ext) a.lines[i] = (double)e_n.f[0];
@@ -200,7 +200,7 @@ __global__ void __launch_bounds__(SLANES *SWARPS, 4) rk2_stream_kernel(const Rk2
         if (ew_lane && i >= 1 && i <= nx - 1 && R_ >= 1 && R_ <= ny - 1) {
             const R inv1 = R(1) / (a.m.dxb[R_] * a.half_cfl);  // dx_cfl_half_inv(1): EW edges
             double cand;
-            edge_flux<R, false>(cl, gw, c2, gew, a.m.dyl[i], inv1, e_w, cand);
+            edge_flux<R, false>(cl, gw, c2, gew, a.m.dyl[i], inv1, e_w, cand, a.flux_variant);
             cfl = fmax(cfl, cand);
             if (MODE != MODE_CFL && a.lines && R_ >= a.n_ext && R_ <= ny - a.n_ext - 1) {
                 if (i == nx - a.n_ext) a.lines[nx + R_] = (double)e_w.f[0];

@@ -35,6 +35,15 @@ struct StepPlanes {
     R *manning_sq;          // rk2 family
 };
 
+// compute_fluxes_inner_method (compute_fluxes_alternatives_include.f90:11-64)
+// as bits: 'DE1_low_fr_diffusion' 0, 'DE1' PLAIN_DIFFUSION,
+// 'DE1_upwind_transverse' both, 'DE1_low_fr_diffusion_upwind_transverse'
+// UPWIND_TRANSVERSE.
+enum {
+    FLUX_PLAIN_DIFFUSION = 1,    // reduced_momentum_diffusion = .false. (fr2 = 1)
+    FLUX_UPWIND_TRANSVERSE = 2   // upwind_transverse_momentum = .true.
+};
+
 struct StepConfig {
     int xl, xu, yl, yu;     // 0-based inclusive active region (domain%xL-1 ...)
     int bext[4];            // boundary_exterior N,E,S,W
@@ -43,6 +52,7 @@ struct StepConfig {
     int spherical, coriolis, nofriction, chezy, truely_linear;
     double msl_linear, linear_friction_coeff, theta, cfl, maximum_timestep;
     int exterior_cells_width;
+    int flux_variant;       // compute_fluxes_inner_method as fv::FLUX_* bits
     void *ring;             // linear + Flather: 2 (nx + ny - 2) x 2 reals of ring momenta
 };
 

@@ -38,7 +38,7 @@ class Domain:
                  maximum_timestep=1.0e20, boundary_exterior=(True, True, True, True),
                  boundary_kind=_lib.BC_NONE, boundary_function_kind=_lib.BF_NONE, boundary_function_params=(),
                  record_max_stage=True, xL=0, xU=0, yL=0, yU=0, exterior_cells_width=2, boundary_subroutine=None,
-                 forcing_subroutine=None, device=-1):
+                 forcing_subroutine=None, device=-1, compute_fluxes_inner_method="DE1_low_fr_diffusion"):
         L = _lib.lib()
         self._L = L
         d = _lib.DomainDesc()
@@ -63,6 +63,7 @@ class Domain:
             d.boundary_exterior[k] = int(bool(boundary_exterior[k]))
         d.boundary_kind = int(boundary_kind)
         d.exterior_cells_width = int(exterior_cells_width)
+        d.compute_fluxes_inner_method = compute_fluxes_inner_method.encode()
         d.boundary_function_kind = int(boundary_function_kind)
         for k, v in enumerate(boundary_function_params):
             d.boundary_function_params[k] = float(v)

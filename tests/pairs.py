@@ -19,6 +19,7 @@ def oracle_from_kw(kw, real32=False):
         bc_kind=kw.get("boundary_kind", 0), bf_kind=kw.get("boundary_function_kind", 0),
         bf_params=kw.get("boundary_function_params", ()),
         xL=kw.get("xL", 0), xU=kw.get("xU", 0), yL=kw.get("yL", 0), yU=kw.get("yU", 0),
+        compute_fluxes_inner_method=kw.get("compute_fluxes_inner_method", "DE1_low_fr_diffusion"),
         real32=real32)
 
 

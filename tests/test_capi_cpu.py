@@ -110,3 +110,9 @@ def test_boundary_kind_checks():
     with pytest.raises(SwalsError) as e:
         _create(boundary_kind=_lib.BC_FLATHER, exterior_cells_width=1)
     assert e.value.code == 3
+
+
+def test_flux_method_checks():
+    with pytest.raises(SwalsError) as e:
+        _create(timestepping_method="rk2", compute_fluxes_inner_method="EEC")
+    assert e.value.code == 3

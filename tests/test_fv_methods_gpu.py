@@ -69,3 +69,33 @@ def test_graph_replay_rk2n():
     b.evolve_steps(13)
     np.testing.assert_array_equal(a.get_U(), b.get_U())
     assert a.state().time == b.state().time
+
+
+@pytest.mark.parametrize("flux", ["DE1", "DE1_upwind_transverse", "DE1_low_fr_diffusion_upwind_transverse"])
+def test_compute_fluxes_inner_methods(flux):
+    """The other DE1 flux variants (compute_fluxes_alternatives_include.f90:
+    11-64): plain HLL momentum diffusion, and/or upwind transverse momentum."""
+    kw, U, _, nsq = workloads.rk2_beach(n=96, dx=10.0 * 2048 / 96, toe=17580.0 * 96 / 2048)
+    kw = dict(kw)
+    kw["compute_fluxes_inner_method"] = flux
+    g, o = make_pair(kw, U, manning_sq=nsq)
+    for _ in range(250):
+        g.evolve_one_step()
+        o.evolve_one_step()
+    _check(g, o, f"rk2 {flux}")
+
+
+@pytest.mark.parametrize("flux", ["DE1_upwind_transverse", "DE1_low_fr_diffusion_upwind_transverse"])
+def test_upwind_transverse_spherical_coriolis(flux):
+    kw, U = workloads.spherical_patch(nx=100, ny=70)
+    kw = dict(kw)
+    kw.update(timestepping_method="rk2", coriolis=True, compute_fluxes_inner_method=flux)
+    U = U.copy()
+    U[0] = np.where(U[3] > 0, U[3], U[0])
+    g, o = make_pair(kw, U, manning_sq=np.full(U[0].shape, 0.025 ** 2))
+    for _ in range(100):
+        g.evolve_one_step()
+        o.evolve_one_step()
+    _, errs = report(f"rk2 sph cor {flux}", g, o)
+    for k in ("STG", "UH", "VH"):
+        assert errs[k + "_exact"] == 1.0, errs
