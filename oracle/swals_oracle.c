@@ -518,6 +518,39 @@ static void nest_flux_tstep(oracle_domain *d, double dt, const REAL *fNS, int ns
     }
 }
 
+/* precompute_friction_work (linear_solver_include.f90:590-618 with
+ * leapfrog_solver_friction_include.f90): g n^2 depth^p at the UH and VH
+ * points, p = -7/3 (Manning) or -2 (Chezy); depth from msl_linear when
+ * truely linear, else from the current stage.  friction_work is (ny, nx, 2)
+ * with the UH component first. */
+static void precompute_friction_work(oracle_domain *d, int truely_linear)
+{
+    const int nx = d->nx, ny = d->ny;
+    const REAL msl = (REAL)d->msl_linear;
+    const size_t plane = (size_t)nx * (size_t)ny;
+    for (int j = 1; j <= ny; j++)
+        for (int i = 1; i <= nx; i++) {
+            const int ip1 = (i + 1 < nx) ? i + 1 : nx, jp1 = (j + 1 < ny) ? j + 1 : ny;
+            REAL depth_iph, depth_jph;
+            if (truely_linear) {
+                depth_iph = HALF * (((msl - UU(OR_ELV, i, j)) + msl) - UU(OR_ELV, ip1, j));
+                depth_jph = HALF * (((msl - UU(OR_ELV, i, j)) + msl) - UU(OR_ELV, i, jp1));
+            } else {
+                depth_iph = HALF * (((UU(OR_STG, i, j) - UU(OR_ELV, i, j)) + UU(OR_STG, ip1, j)) - UU(OR_ELV, ip1, j));
+                depth_jph = HALF * (((UU(OR_STG, i, j) - UU(OR_ELV, i, j)) + UU(OR_STG, i, jp1)) - UU(OR_ELV, i, jp1));
+            }
+            depth_iph = rmax(depth_iph, MINIMUM_ALLOWED_DEPTH);
+            depth_jph = rmax(depth_jph, MINIMUM_ALLOWED_DEPTH);
+            const REAL nsq_iph = HALF * (d->manning_squared[IDX(i, j)] + d->manning_squared[IDX(ip1, j)]);
+            const REAL nsq_jph = HALF * (d->manning_squared[IDX(i, j)] + d->manning_squared[IDX(i, jp1)]);
+            d->friction_work[IDX(i, j)] =
+                GRAVITY * nsq_iph * (REAL)or_pow_friction((double)depth_iph, d->friction_chezy);
+            d->friction_work[plane + IDX(i, j)] =
+                GRAVITY * nsq_jph * (REAL)or_pow_friction((double)depth_jph, d->friction_chezy);
+        }
+    if (truely_linear) d->friction_work_is_setup = 1;
+}
+
 static void linear_leapfrog_step(oracle_domain *d, REAL dt)
 {
     const int nx = d->nx, ny = d->ny;
@@ -568,15 +601,18 @@ static void linear_leapfrog_step(oracle_domain *d, REAL dt)
      * averages use pre-update values exactly as the reference's carried row
      * buffers and thread-boundary snapshots do. */
     size_t plane = (size_t)nx * (size_t)ny;
+    /* leapfrog_linear_plus_nonlinear_friction (LINEAR_PLUS_NONLINEAR_FRICTION) */
+    const int nlfric = (d->method == OR_METHOD_LEAPFROG_LINEAR_PLUS_NONLINEAR_FRICTION);
+    if (nlfric && !d->friction_work_is_setup) precompute_friction_work(d, truely_linear);
     REAL *uh_old = NULL, *vh_old = NULL;
-    if (d->coriolis) {
+    if (d->coriolis || nlfric) {
         uh_old = (REAL *)malloc(plane * sizeof(REAL));
         vh_old = (REAL *)malloc(plane * sizeof(REAL));
         memcpy(uh_old, &UU(OR_UH, 1, 1), plane * sizeof(REAL));
         memcpy(vh_old, &UU(OR_VH, 1, 1), plane * sizeof(REAL));
     }
     REAL lin_fric_mult = ZERO;
-    int lin_fric = ((REAL)d->linear_friction_coeff != ZERO);
+    int lin_fric = ((REAL)d->linear_friction_coeff != ZERO) && !nlfric;
     if (lin_fric) lin_fric_mult = ONE / (ONE + dt * (REAL)d->linear_friction_coeff);
 
     #pragma omp parallel
@@ -633,15 +669,30 @@ static void linear_leapfrog_step(oracle_domain *d, REAL dt)
                           inv_cell_area_dt_g * h_iph[i - 1] * (UU(OR_STG, i + 1, j) - UU(OR_STG, i, j)) * d->dyl[i];
                 REAL vh = UU(OR_VH, i, j) * h_jph_wet[i - 1] -
                           inv_cell_area_dt_vh_g * h_jph[i - 1] * dw_j[i - 1] * d->dxb[j];
-                if (d->coriolis) {
+                if (d->coriolis || nlfric) {
                     int jm = (j > 1) ? j - 1 : 1;
                     REAL vh_iph_jmh = HALF * (vh_old[IDX(i, jm)] + vh_old[IDX(i + 1, jm)]);
                     REAL vh_iph_jph = HALF * (vh_old[IDX(i, j)] + vh_old[IDX(i + 1, j)]);
                     int im = (i > xL) ? i - 1 : ((xL - 1 > 1) ? xL - 1 : 1);
                     REAL uh_i_j = HALF * (uh_old[IDX(i, j)] + uh_old[IDX(im, j)]);
                     REAL uh_i_jp1 = HALF * (uh_old[IDX(i, j + 1)] + uh_old[IDX(im, j + 1)]);
-                    uh = uh + dthc[i - 1] * (vh_iph_jmh + vh_iph_jph);
-                    vh = vh - dthc_jph[i - 1] * (uh_i_j + uh_i_jp1);
+                    if (d->coriolis) {
+                        uh = uh + dthc[i - 1] * (vh_iph_jmh + vh_iph_jph);
+                        vh = vh - dthc_jph[i - 1] * (uh_i_j + uh_i_jp1);
+                    }
+                    if (nlfric) {
+                        /* semi-implicit friction multipliers (:458-505), from the old momenta */
+                        const REAL tv = HALF * (vh_iph_jmh + vh_iph_jph);
+                        const REAL tu = HALF * (uh_i_j + uh_i_jp1);
+                        const REAL u0 = uh_old[IDX(i, j)], v0 = vh_old[IDX(i, j)];
+                        const REAL lf = dt * (REAL)d->linear_friction_coeff;
+                        const REAL fm_uh = ONE / ((ONE + lf) + dt * d->friction_work[IDX(i, j)] *
+                                                                  (REAL)sqrt(u0 * u0 + tv * tv));
+                        const REAL fm_vh = ONE / ((ONE + lf) + dt * d->friction_work[plane + IDX(i, j)] *
+                                                                  (REAL)sqrt(v0 * v0 + tu * tu));
+                        uh = fm_uh * uh;
+                        vh = fm_vh * vh;
+                    }
                 }
                 UU(OR_UH, i, j) = uh;
                 UU(OR_VH, i, j) = vh;
@@ -1200,6 +1251,7 @@ int ORACLE_FN(evolve_one_step)(oracle_domain *d, double dt, int has_dt)
     case OR_METHOD_RK2N: one_rk2n_step(d, dt, has_dt); break;
     case OR_METHOD_MIDPOINT: one_midpoint_step(d, dt, has_dt); break;
     case OR_METHOD_LINEAR:
+    case OR_METHOD_LEAPFROG_LINEAR_PLUS_NONLINEAR_FRICTION:
         if (!has_dt) return 2;
         linear_leapfrog_step(d, (REAL)dt);
         break;

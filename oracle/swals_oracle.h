@@ -125,10 +125,13 @@ typedef struct oracle_domain {
      * an edge variable by variable (STG..ELV), each of length iU-iL+1 (N, S)
      * or jU-jL+1 (E, W). */
     int32_t nest_nbox;
-    int32_t pad1;
+    int32_t friction_work_is_setup;
     const int32_t *nest_boxes;
     const int64_t *nest_offset;
     double *nest_integral;
+    /* leapfrog_linear_plus_nonlinear_friction: g n^2 depth^p at the UH and
+     * VH points (nx*ny*2, domain%friction_work) */
+    REAL *friction_work;
 } oracle_domain;
 
 /* One side of a two_way_nesting_comms_type (nested_grid_comms_mod.f90:

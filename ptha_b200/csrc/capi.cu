@@ -239,8 +239,10 @@ int evolve_t(swals_domain *d, double timestep, int has_dt)
         if (e != cudaSuccess) return cuda_fail(e, "update_max_quantities");
     }
     cudaError_t e = cudaSuccess;
-    if (d->method == M_LINEAR) {
-        if (!has_dt) return fail(SWALS_ERR_TIMESTEP_REQUIRED, "ERROR: timestep must be provided for linear evolve_one_step");
+    if (d->method == M_LINEAR || d->method == M_LF_LIN_NLFRIC) {
+        if (!has_dt)
+            return fail(SWALS_ERR_TIMESTEP_REQUIRED, "ERROR: timestep must be provided for %s evolve_one_step",
+                        d->desc.timestepping_method);
         const int in = d->cur, out = (d->cur + 1) % 3;
         StepPlanes<R> p;
         p.nx = d->nx; p.ny = d->ny; p.pitch = d->pitch;
@@ -254,6 +256,7 @@ int evolve_t(swals_domain *d, double timestep, int has_dt)
         }
         e = launch_linear_step<R>(p, m, c, R(timestep), d->sc, d->stream, hook, d->timers_on ? nullptr : &d->aux);
         if (e != cudaSuccess) return cuda_fail(e, "linear leapfrog step");
+        if (d->cfg.fw) d->cfg.fw_ready = 1;
         d->cur = out;
     } else if (d->method == M_RK2 || d->method == M_EULER || d->method == M_MIDPOINT || d->method == M_RK2N) {
         R *pl[3][3];
@@ -338,7 +341,8 @@ int swals_gpu_domain_create(const swals_domain_desc *desc, swals_domain **out)
     double def_cfl, def_theta;
     if (!parse_method(desc->timestepping_method, &method, &def_cfl, &def_theta))
         return fail(SWALS_ERR_UNKNOWN_METHOD, "timestepping_method: %s not recognized", desc->timestepping_method);
-    if (!(method == M_LINEAR || method == M_RK2 || method == M_EULER || method == M_MIDPOINT || method == M_RK2N))
+    if (!(method == M_LINEAR || method == M_RK2 || method == M_EULER || method == M_MIDPOINT || method == M_RK2N ||
+          method == M_LF_LIN_NLFRIC))
         return fail(SWALS_ERR_UNSUPPORTED, "timestepping_method '%s' is not implemented on the GPU path",
                     desc->timestepping_method);
     const int nx = desc->nx[0], ny = desc->nx[1];
@@ -356,9 +360,9 @@ int swals_gpu_domain_create(const swals_domain_desc *desc, swals_domain **out)
         return fail(SWALS_ERR_INVALID_ARGUMENT, "unknown boundary_kind %d", desc->boundary_kind);
     if (desc->boundary_function_kind < 0 || desc->boundary_function_kind > 1)
         return fail(SWALS_ERR_UNSUPPORTED_CALLBACK, "unknown boundary_function_kind %d", desc->boundary_function_kind);
-    if (method == M_LINEAR && desc->boundary_kind == SWALS_BC_FLATHER && desc->exterior_cells_width == 1)
+    if (is_staggered(method) && desc->boundary_kind == SWALS_BC_FLATHER && desc->exterior_cells_width == 1)
         return fail(SWALS_ERR_UNSUPPORTED, "flather_boundary with the linear solver needs exterior_cells_width >= 2");
-    if (method == M_LINEAR && desc->boundary_kind == SWALS_BC_TRANSMISSIVE)
+    if (is_staggered(method) && desc->boundary_kind == SWALS_BC_TRANSMISSIVE)
         return fail(SWALS_ERR_UNSUPPORTED, "transmissive_boundary with the staggered linear solver is not implemented");
     if (desc->boundary_kind == SWALS_BC_STAGE_TRANSMISSIVE_NORMAL_MOMENTUM && desc->boundary_function_kind != 1)
         return fail(SWALS_ERR_UNSUPPORTED_CALLBACK, "boundary_function must be a device kind (SWALS_BF_*)");
@@ -433,6 +437,8 @@ int swals_gpu_domain_create(const swals_domain_desc *desc, swals_domain **out)
                                d->method == M_RK2N)
                                   ? al((size_t)swals::rk2_edge_bytes(d->pitch, ny, (int)es)) : 0;
     total += edge_bytes;
+    const size_t fw_bytes = (d->method == M_LF_LIN_NLFRIC) ? 2 * al(plane) : 0;   // friction_work
+    total += fw_bytes;
     e = cudaMalloc(&d->pool, total);
     if (e != cudaSuccess) {
         cudaStreamDestroy(d->stream);
@@ -454,6 +460,8 @@ int swals_gpu_domain_create(const swals_domain_desc *desc, swals_domain **out)
     d->d_out = (double *)p; p += al(64);
     d->edges = edge_bytes ? (void *)p : nullptr; p += edge_bytes;
     d->cfg.ring = d->side;   // the staggered solver's Flather ring buffer (the side buffer is for FV stages)
+    d->cfg.fw = fw_bytes ? (void *)p : nullptr; p += fw_bytes;
+    d->cfg.fw_ready = 0;
 
     int rc = SWALS_OK;
     if ((e = cudaMemsetAsync(d->pool, 0, total, d->stream)) != cudaSuccess) rc = cuda_fail(e, "memset");
@@ -759,8 +767,8 @@ int swals_gpu_domain_statistics(swals_domain *d, swals_domain_stats *out)
     if (!d || !out) return fail(SWALS_ERR_INVALID_ARGUMENT, "bad argument");
     if (!d->stats_buf) CK(cudaMalloc(&d->stats_buf, sizeof(double) * (6 * (size_t)d->ny + 8)));
     const int ecw = d->desc.exterior_cells_width;
-    const int staggered = (d->method == M_LINEAR) ? 1 : 0;
-    const int tl = staggered && d->desc.linear_solver_is_truely_linear;
+    const int staggered = is_staggered(d->method) ? 1 : 0;
+    const int tl = (d->method == M_LINEAR || d->method == M_LF_LIN_NLFRIC) && d->desc.linear_solver_is_truely_linear;
     double *o7 = d->stats_buf + 6 * (size_t)d->ny;
     cudaError_t e;
     if (d->fp64)

@@ -44,6 +44,11 @@ struct LinArgs {
     R msl;
     int lin_fric;
     R lin_fric_mult;
+    R lin_fric_dt;          // dt * linear_friction_coeff
+    // leapfrog_linear_plus_nonlinear_friction: friction_work at the UH points,
+    // then (fw_plane elements on) the VH points; null for the other solvers.
+    const R *fw;
+    int64_t fw_plane;
     int nbatch;             // instances sharing ELV and the metrics (1 for a plain domain)
     int64_t inst_stride;    // elements between consecutive instances' planes
     int64_t max_stride;     // elements between consecutive instances' max_stage planes
@@ -57,6 +62,25 @@ struct LinArgs {
 __device__ __forceinline__ bool on_bc_ring(int i, int r, int nx, int ny, const int bext[4])
 {
     return (i == 0 && bext[3]) || (i == nx - 1 && bext[1]) || (r == 0 && bext[2]) || (r == ny - 1 && bext[0]);
+}
+
+// leapfrog_linear_plus_nonlinear_friction (linear_solver_include.f90:
+// 458-505): the semi-implicit friction multipliers of cell o from its old
+// momenta uh0, vh0 and the old two-point averages; linear friction is folded
+// in.  Applied after the pressure-gradient (and Coriolis) update, by
+// linear_nlfric_kernel after the step kernel (which then skips the linear
+// friction), so the plain solvers' step kernels carry none of it.
+template <typename R>
+__device__ __forceinline__ void nl_friction(const LinArgs<R> &a, int64_t o, R uh0, R vh0, R vh_iph_jmh, R vh_iph_jph,
+                                            R uh_i_j, R uh_i_jp1, R &uh_new, R &vh_new)
+{
+    const R half = K<R>::half(), one = K<R>::one();
+    const R tv = half * (vh_iph_jmh + vh_iph_jph);
+    const R tu = half * (uh_i_j + uh_i_jp1);
+    const R fm_uh = one / ((one + a.lin_fric_dt) + a.dt * a.fw[o] * R(sqrt(uh0 * uh0 + tv * tv)));
+    const R fm_vh = one / ((one + a.lin_fric_dt) + a.dt * a.fw[a.fw_plane + o] * R(sqrt(vh0 * vh0 + tu * tu)));
+    uh_new = fm_uh * uh_new;
+    vh_new = fm_vh * vh_new;
 }
 
 // One CTA: a 32 x BY tile (TYT thread rows, BY/TYT cells per thread) for IB
@@ -805,6 +829,79 @@ __global__ void __launch_bounds__(256) linear_flather_fix_kernel(const LinArgs<R
     a.p.vh_o[o] = vh;
 }
 
+// precompute_friction_work (linear_solver_include.f90:590-618,
+// leapfrog_solver_friction_include.f90): g n^2 depth^p at the UH and VH
+// points with p = -7/3 (Manning) or -2 (Chezy), correctly rounded.  The
+// depth is from msl_linear when truely linear (done once), else from the
+// stage after the stage sweep and the boundary (every step; the ring stage
+// of a stage boundary is already in stg_o).
+template <typename R, bool CHEZY>
+__global__ void __launch_bounds__(256) friction_work_kernel(const LinArgs<R> a, const R *nsq, R *fw, int truely_linear)
+{
+    const int nx = a.p.nx, ny = a.p.ny;
+    const int i = blockIdx.x * 32 + threadIdx.x, r = blockIdx.y * 8 + threadIdx.y;
+    if (i >= nx || r >= ny) return;
+    const int64_t P = a.p.pitch;
+    const int ip1 = min(i + 1, nx - 1), jp1 = min(r + 1, ny - 1);
+    const int64_t o = (int64_t)r * P + i, oe = (int64_t)r * P + ip1, on = (int64_t)jp1 * P + i;
+    const R half = K<R>::half(), mad = K<R>::min_depth(), g = K<R>::gravity();
+    const R e0 = a.p.elv[o], e_e = a.p.elv[oe], e_n = a.p.elv[on];
+    R depth_iph, depth_jph;
+    if (truely_linear) {
+        depth_iph = half * (((a.msl - e0) + a.msl) - e_e);
+        depth_jph = half * (((a.msl - e0) + a.msl) - e_n);
+    } else {
+        auto stage = [&](int ii, int rr) -> R {
+            if (a.bc_stage && on_bc_ring(ii, rr, nx, ny, a.bext) &&
+                !((ii >= a.xl + 1) && (ii <= a.xu - 1) && (rr >= a.yl + 1) && (rr <= a.yu - 1)))
+                return a.p.stg_o[(int64_t)rr * P + ii];
+            return swept_stage(a, ii, rr);
+        };
+        const R s0 = stage(i, r);
+        depth_iph = half * (((s0 - e0) + stage(ip1, r)) - e_e);
+        depth_jph = half * (((s0 - e0) + stage(i, jp1)) - e_n);
+    }
+    depth_iph = (depth_iph > mad) ? depth_iph : mad;
+    depth_jph = (depth_jph > mad) ? depth_jph : mad;
+    const R nsq_iph = half * (nsq[o] + nsq[oe]);
+    const R nsq_jph = half * (nsq[o] + nsq[on]);
+    fw[o] = g * nsq_iph * R(pow_friction_cr<CHEZY>((double)depth_iph));
+    fw[(int64_t)ny * P + o] = g * nsq_jph * R(pow_friction_cr<CHEZY>((double)depth_jph));
+}
+
+// The friction multipliers of leapfrog_linear_plus_nonlinear_friction on the
+// momenta the step kernel (and a Flather fix-up) wrote.  The old momenta are
+// those after the boundary routine: the ring buffer on a Flather ring.
+template <typename R>
+__global__ void __launch_bounds__(256) linear_nlfric_kernel(const LinArgs<R> a, const R *ring)
+{
+    const int nx = a.p.nx, ny = a.p.ny;
+    const int i = blockIdx.x * 32 + threadIdx.x, r = blockIdx.y * 8 + threadIdx.y;
+    if (i >= nx || r >= ny) return;
+    if (!(i >= a.xl && i <= a.xu - 1 && r >= a.yl && r <= a.yu - 1)) return;
+    const int64_t P = a.p.pitch;
+    const R half = K<R>::half();
+    auto uhb = [&](int ii, int rr) -> R {
+        return (ring && on_bc_ring(ii, rr, nx, ny, a.bext)) ? ring[2 * ring_index(ii, rr, nx, ny)]
+                                                            : a.p.uh[(int64_t)rr * P + ii];
+    };
+    auto vhb = [&](int ii, int rr) -> R {
+        return (ring && on_bc_ring(ii, rr, nx, ny, a.bext)) ? ring[2 * ring_index(ii, rr, nx, ny) + 1]
+                                                            : a.p.vh[(int64_t)rr * P + ii];
+    };
+    const int64_t o = (int64_t)r * P + i;
+    const int rm = (r > 0) ? r - 1 : 0, im = (i > 0) ? i - 1 : 0;
+    const R uh0 = uhb(i, r), vh0 = vhb(i, r);
+    const R vh_iph_jmh = half * (vhb(i, rm) + vhb(i + 1, rm));
+    const R vh_iph_jph = half * (vh0 + vhb(i + 1, r));
+    const R uh_i_j = half * (uh0 + uhb(im, r));
+    const R uh_i_jp1 = half * (uhb(i, r + 1) + uhb(im, r + 1));
+    R u = a.p.uh_o[o], v = a.p.vh_o[o];
+    nl_friction<R>(a, o, uh0, vh0, vh_iph_jmh, vh_iph_jph, uh_i_j, uh_i_jp1, u, v);
+    a.p.uh_o[o] = u;
+    a.p.vh_o[o] = v;
+}
+
 template <typename R>
 __global__ void max_stage_kernel(int nx, int ny, int64_t P, const R *stg, R *mx, int xl, int xu, int yl, int yu)
 {
@@ -1005,6 +1102,9 @@ LinArgs<R> make_args(const StepPlanes<R> &p, const Metrics<R> &m, const StepConf
     R lfc = R(c.linear_friction_coeff);
     a.lin_fric = (lfc != R(0)) ? 1 : 0;
     a.lin_fric_mult = a.lin_fric ? (R(1) / (R(1) + dt * lfc)) : R(0);
+    a.lin_fric_dt = dt * lfc;
+    a.fw = nullptr;
+    a.fw_plane = 0;
     a.nbatch = 1;
     a.inst_stride = 0;
     a.max_stride = 0;
@@ -1012,6 +1112,32 @@ LinArgs<R> make_args(const StepPlanes<R> &p, const Metrics<R> &m, const StepConf
     a.n_sites = 0;
     a.rec = nullptr;
     return a;
+}
+
+// leapfrog_linear_plus_nonlinear_friction: the friction work, before the
+// step kernel (and after any ring-stage kernel).
+template <typename R>
+void launch_friction_work(LinArgs<R> &a, const StepPlanes<R> &p, const StepConfig &c, cudaStream_t s,
+                          const LaunchHook &hook)
+{
+    a.fw = (const R *)c.fw;
+    a.fw_plane = p.pitch * (int64_t)p.ny;
+    a.lin_fric = 0;   // folded into the friction multipliers
+    if (c.truely_linear && c.fw_ready) return;
+    hook(CAT_LINEAR_EDGE, 0);
+    dim3 block(32, 8), grid((p.nx + 31) / 32, (p.ny + 7) / 8);
+    if (c.chezy) friction_work_kernel<R, true><<<grid, block, 0, s>>>(a, p.manning_sq, (R *)c.fw, c.truely_linear);
+    else friction_work_kernel<R, false><<<grid, block, 0, s>>>(a, p.manning_sq, (R *)c.fw, c.truely_linear);
+    hook(CAT_LINEAR_EDGE, 1);
+}
+
+template <typename R>
+void launch_nlfric(const LinArgs<R> &a, const StepPlanes<R> &p, const R *ring, cudaStream_t s, const LaunchHook &hook)
+{
+    hook(CAT_LINEAR_EDGE, 0);
+    dim3 block(32, 8), grid((p.nx + 31) / 32, (p.ny + 7) / 8);
+    linear_nlfric_kernel<R><<<grid, block, 0, s>>>(a, ring);
+    hook(CAT_LINEAR_EDGE, 1);
 }
 
 template <typename R>
@@ -1031,9 +1157,11 @@ cudaError_t launch_linear_step(const StepPlanes<R> &p, const Metrics<R> &m, cons
         linear_edge_kernel<R><<<1, 512, 0, aux->stream>>>(a, sc, c.exterior_cells_width, c.bf);
         hook(CAT_LINEAR_EDGE, 1);
         cudaEventRecord(aux->join, aux->stream);
+        if (c.fw) launch_friction_work<R>(a, p, c, s, hook);
         hook(CAT_LINEAR_MAIN, 0);
         launch_main<R>(a, c, plain_config(p.nx, p.ny), s);
         hook(CAT_LINEAR_MAIN, 1);
+        if (c.fw) launch_nlfric<R>(a, p, nullptr, s, hook);
         cudaStreamWaitEvent(s, aux->join, 0);
         return cudaGetLastError();
     }
@@ -1049,6 +1177,7 @@ cudaError_t launch_linear_step(const StepPlanes<R> &p, const Metrics<R> &m, cons
     hook(CAT_LINEAR_EDGE, 0);
     linear_edge_kernel<R><<<1, 512, 0, s>>>(a, sc, c.exterior_cells_width, c.bf);
     hook(CAT_LINEAR_EDGE, 1);
+    if (c.fw) launch_friction_work<R>(a, p, c, s, hook);
     hook(CAT_LINEAR_MAIN, 0);
     launch_main<R>(a, c, plain_config(p.nx, p.ny), s);
     hook(CAT_LINEAR_MAIN, 1);
@@ -1063,6 +1192,7 @@ cudaError_t launch_linear_step(const StepPlanes<R> &p, const Metrics<R> &m, cons
         else linear_flather_fix_kernel<R, false, false><<<blocks, 256, 0, s>>>(a, ring);
         hook(CAT_LINEAR_EDGE, 1);
     }
+    if (c.fw) launch_nlfric<R>(a, p, flather ? ring : nullptr, s, hook);
     return cudaGetLastError();
 }
 

@@ -689,7 +689,7 @@ DomTab make_tab(const swals_multidomain *md)
         p.elv = d->elv;
         p.nx = d->nx; p.ny = d->ny; p.P = d->pitch;
         p.fp64 = d->fp64 ? 1 : 0;
-        p.staggered = (d->method == M_LINEAR) ? 1 : 0;
+        p.staggered = is_linear_leapfrog(d->method) ? 1 : 0;
         p.truely_linear = d->desc.linear_solver_is_truely_linear ? 1 : 0;
         p.msl_linear = d->desc.msl_linear;
     }
@@ -716,7 +716,7 @@ int build_corrections(const swals_multidomain *md, int dj, const int32_t *pind, 
     const int nx = d->nx, ny = d->ny;
     auto P = [&](int i, int j) { return pind[(size_t)(j - 1) * nx + (i - 1)]; };
     auto dxof = [&](int idx, int c) -> R { return R(md->dx[2 * (idx - 1) + c]); };  // all_dx_md(c, idx)
-    auto mass_only = [&](int idx) { return md->doms[idx - 1]->method == M_LINEAR; };
+    auto mass_only = [&](int idx) { return is_linear_leapfrog(md->doms[idx - 1]->method); };
     const std::vector<double> &area = d->h_metric[2];
     const int myi = dj + 1;
     for (int pass = 0; pass < 4; pass++) {
@@ -825,7 +825,7 @@ static int integral_step(swals_multidomain *md, int k, int phase, int A, double 
     if (pd.nitems == 0) return SWALS_OK;
     DomPtr p = make_tab(md).d[k];
     const Metrics<R> m = metrics_of<R>(d);
-    if (d->method == M_LINEAR) {
+    if (is_linear_leapfrog(d->method)) {
         if (phase != 0) return SWALS_OK;
         integral_leapfrog_kernel<R><<<grid_for(pd.nitems), 256, 0, md->stream>>>(
             p, m.dxb, m.dyl, pd.d_box, pd.nbox, pd.nitems, md->d_int, R(dt_local));
@@ -862,7 +862,7 @@ int swals_gpu_md_create(swals_domain *const *domains, int32_t ndomains, const do
         const swals_domain *d = domains[k];
         if (!d) return fail(SWALS_ERR_INVALID_ARGUMENT, "domain %d is NULL", k);
         if (d->device != domains[0]->device) return fail(SWALS_ERR_UNSUPPORTED, "all domains must be on one device");
-        if (d->method != M_LINEAR && d->method != M_RK2 && d->method != M_EULER)
+        if (!is_linear_leapfrog(d->method) && d->method != M_RK2 && d->method != M_EULER)
             return fail(SWALS_ERR_UNSUPPORTED, "domain %d: method '%s' is not supported in a multidomain", k,
                         d->desc.timestepping_method);
         if (refinement && refinement[k] < 1) return fail(SWALS_ERR_INVALID_ARGUMENT, "refinement factor < 1");
@@ -906,8 +906,8 @@ int swals_gpu_md_create(swals_domain *const *domains, int32_t ndomains, const do
             sdx[c] = md->dx[2 * h.sender + c];
             rdx[c] = md->dx[2 * h.receiver + c];
         }
-        e.s_stag = (S->method == M_LINEAR) ? 1 : 0;
-        e.r_stag = (Rd->method == M_LINEAR) ? 1 : 0;
+        e.s_stag = is_linear_leapfrog(S->method) ? 1 : 0;
+        e.r_stag = is_linear_leapfrog(Rd->method) ? 1 : 0;
         e.wetdry = use_wetdry_limiting ? 1 : 0;
         for (int c = 0; c < 2; c++) { e.s_cr[c] = sdx[c] / rdx[c]; e.r_cr[c] = rdx[c] / sdx[c]; }
         const bool equal = fabs(e.s_cr[0] - 1.0) < 1e-6 && fabs(e.s_cr[1] - 1.0) < 1e-6;

@@ -52,8 +52,10 @@ struct StepConfig {
     int spherical, coriolis, nofriction, chezy, truely_linear;
     double msl_linear, linear_friction_coeff, theta, cfl, maximum_timestep;
     int exterior_cells_width;
-    int flux_variant;       // compute_fluxes_inner_method as fv::FLUX_* bits
+    int flux_variant;       // compute_fluxes_inner_method as FLUX_* bits
     void *ring;             // linear + Flather: 2 (nx + ny - 2) x 2 reals of ring momenta
+    void *fw;               // leapfrog_linear_plus_nonlinear_friction: friction_work (2 planes), else null
+    int fw_ready;           // truely linear: friction_work already computed (friction_work_is_setup)
 };
 
 // compute_domain_statistics_new: rows6 is 6*ny doubles of scratch; out7 (device)
