@@ -891,7 +891,8 @@ int swals_gpu_md_create(swals_domain *const *domains, int32_t ndomains, const do
     int64_t off_buf = 0, off_int = 0, off_err = 0;
     for (int x = 0; x < nex; x++) {
         const swals_nest_exchange &h = exchanges[x];
-        if (h.sender < 0 || h.sender >= ndomains || h.receiver < 0 || h.receiver >= ndomains || h.sender == h.receiver)
+        // sender == receiver is a periodic self-exchange (check_periodic boxes).
+        if (h.sender < 0 || h.sender >= ndomains || h.receiver < 0 || h.receiver >= ndomains)
             return cleanup(fail(SWALS_ERR_INVALID_ARGUMENT, "exchange %d: bad domain index", x));
         const swals_domain *S = domains[h.sender], *Rd = domains[h.receiver];
         Ex e;

@@ -220,3 +220,76 @@ def test_mixed_precision_nest_close_to_fp64():
         err = np.abs(U[0] - od.U[0])[wet].max()
         assert err <= 2e-5 * max(1.0, np.abs(od.U[0][wet]).max()), (k, err)
     md.close()
+
+
+def test_periodic_exchange_gpu():
+    """The reference's periodic multidomain test on the GPU: the halos of a
+    domain periodic in x and y come from its own interior (self-exchanges),
+    equal to the oracle's and within the reference's tolerance."""
+    from test_nesting_oracle import periodic_case, periodic_check
+    s, ex, pxs, pys, X, Y, U = periodic_case()
+    fresh = nest.NestDomain((-10.0, -80.0), (360.0, 170.0), (200, 200), "euler", 1)   # setup widens its specs
+    md = Multidomain([fresh], use_wetdry_limiting=False, flux_correction=False, periodic_xs=pxs, periodic_ys=pys)
+    assert [(e.send_box, e.recv_box) for e in md.exchanges] == [(e.send_box, e.recv_box) for e in ex]
+    md.domains[0].set_U(U)
+    md.send_halos()
+    md.recv_halos()
+    od = OracleDomain(s.nx[0], s.nx[1], s.lw, s.lower_left, timestepping_method="euler",
+                      boundary_exterior=tuple(not b for b in s.is_nesting_boundary))
+    omd = OracleMultidomain([od], ["euler"], [s.dx], ex, use_wetdry_limiting=False, flux_correction=False)
+    od.U[:] = U
+    omd.send_halos(0)
+    omd.recv_halos()
+    G = md.domains[0].get_U()
+    np.testing.assert_array_equal(G, od.U)
+    assert periodic_check(G, X, Y, pxs, pys) > 0
+    md.close()
+
+
+@pytest.mark.parametrize("method", ["linear", "rk2"])
+def test_periodic_channel_steps(method):
+    """A wave crossing the periodic seam of an x-periodic channel (walls north
+    and south): md steps equal the oracle's bit for bit, and the mass in the
+    priority cells is conserved."""
+    pxs = (0.0, 100000.0)
+    s = nest.NestDomain((0.0, 0.0), (100000.0, 40000.0), (100, 40), method, 1)
+    ex = nest.setup_multidomain([s], periodic_xs=pxs)
+    md = Multidomain([nest.NestDomain((0.0, 0.0), (100000.0, 40000.0), (100, 40), method, 1)],
+                     use_wetdry_limiting=True, flux_correction=True, periodic_xs=pxs)
+    assert md.specs[0].nx == s.nx and [e.send_box for e in md.exchanges] == [e.send_box for e in ex]
+    X, Y = np.meshgrid(s.x(), s.y())
+    U = np.zeros((4, s.nx[1], s.nx[0]))
+    U[3] = -100.0
+    U[3][:2, :] = 50.0
+    U[3][-2:, :] = 50.0
+    U[0] = np.maximum(U[3], 0.5 * np.exp(-((X - 90000.0) ** 2 + (Y - 20000.0) ** 2) / (2 * 5000.0 ** 2)))
+    od = OracleDomain(s.nx[0], s.nx[1], s.lw, s.lower_left, timestepping_method=method,
+                      boundary_exterior=tuple(not b for b in s.is_nesting_boundary))
+    omd = OracleMultidomain([od], [method], [s.dx], ex, refinement=[1], priority_index=[s.priority_domain_index],
+                            use_wetdry_limiting=True, flux_correction=True)
+    md.domains[0].set_U(U)
+    od.U[:] = U
+    if method == "rk2":
+        md.domains[0].set_manning_squared(0.025 ** 2)
+        od.manning_squared[:] = 0.025 ** 2
+    dt = 0.5 * (od.linear_timestep_max() if method == "linear" else od.nonlinear_stationary_timestep_max())
+    # one exchange first, so that the halos are the periodic images (as the
+    # reference's periodic test does); mass over the priority cells that
+    # are not periodic copies (is_priority_domain_not_periodic)
+    md.send_halos()
+    md.recv_halos()
+    omd.send_halos(0)
+    omd.recv_halos()
+    np.testing.assert_array_equal(md.domains[0].get_U(), od.U)
+    pr = (s.priority_domain_index.T == 1) & (X > pxs[0]) & (X < pxs[1])
+    v0 = float(np.sum((od.U[0] - od.U[3])[pr]))
+    for step in range(60):
+        md.evolve_one_step(dt)
+        omd.evolve_one_step(dt)
+    G = md.domains[0].get_U()
+    np.testing.assert_array_equal(G, od.U)
+    v1 = float(np.sum((G[0] - G[3])[pr]))
+    assert abs(v1 - v0) <= 1e-11 * abs(v0)
+    # the wave went through the seam: the west end has moved
+    assert np.max(np.abs(G[0][5:-5, 3:15])) > 1e-3
+    md.close()

@@ -119,3 +119,41 @@ def test_flux_correction_conserves_mass(parent, child, nt, wetdry):
         drift[fc] = abs(_priority_volume(specs, doms) - v0) / v0
     assert drift[True] < 1e-13
     assert drift[False] > 1e-8
+
+
+def periodic_case():
+    """test_multidomain_mod_periodic (multidomain_mod.f90:4185-4298): one
+    200 x 200 'euler' domain over lon -10..350, lat -80..90, periodic in both
+    directions, U(i,j,k) = x + y^2 + k."""
+    pxs, pys = (-10.0, 350.0), (-80.0, 90.0)
+    s = nest.NestDomain((-10.0, -80.0), (360.0, 170.0), (200, 200), "euler", 1)
+    ex = nest.setup_multidomain([s], periodic_xs=pxs, periodic_ys=pys)
+    X, Y = np.meshgrid(s.x(), s.y())
+    U = np.stack([X + Y * Y + k for k in (1.0, 2.0, 3.0, 4.0)])
+    return s, ex, pxs, pys, X, Y, U
+
+
+def periodic_check(U, X, Y, pxs, pys):
+    """The reference test's acceptance: every cell holds the field at its
+    periodic image, within its heuristic tolerance."""
+    px, _ = nest._periodic_shift(X.ravel(), *pxs, True)
+    py, _ = nest._periodic_shift(Y.ravel(), *pys, True)
+    px, py = px.reshape(X.shape), py.reshape(Y.shape)
+    tv = px + py * py
+    err = np.max(np.abs(U - (tv[None] + np.arange(1.0, 5.0)[:, None, None])), axis=0)
+    xc, yc = np.abs(px - X), np.abs(py - Y)
+    tol = 1e-10 + 40.0 * (np.spacing(np.abs(px) + np.abs(py * py)) + (np.spacing(xc) + 2.0 * yc * np.spacing(yc)))
+    assert np.all(err <= tol), float(err.max())
+    return int(np.count_nonzero((xc > 0) | (yc > 0)))
+
+
+def test_periodic_exchange():
+    s, ex, pxs, pys, X, Y, U = periodic_case()
+    assert all(e.sender == 0 and e.receiver == 0 for e in ex)
+    d = OracleDomain(s.nx[0], s.nx[1], s.lw, s.lower_left, timestepping_method="euler",
+                     boundary_exterior=tuple(not b for b in s.is_nesting_boundary))
+    md = OracleMultidomain([d], ["euler"], [s.dx], ex, use_wetdry_limiting=False, flux_correction=False)
+    d.U[:] = U
+    md.send_halos(0)
+    md.recv_halos()
+    assert periodic_check(d.U, X, Y, pxs, pys) > 0
