@@ -551,7 +551,8 @@ def _coast_elevation(lon, lat, coasts):
 
 def _run_multidomain(args, local, peak, peak_kind):
     """Nested multidomain in the shape of the 5-domain configuration: a
-    coarse 'linear' FP32 band (4 arcmin, 5400x1800, 60S-60N), one ratio-3
+    coarse 'linear' FP32 band (4 arcmin, 5400x1800, 60S-60N, periodic in
+    longitude over 0-360 through periodic self-exchanges), one ratio-3
     'rk2' FP64 domain (900x900) and two ratio-9 'rk2' FP64 wet/dry domains
     (1197x801 and 702x1098, the nearest sizes that are whole parent cells)
     on synthetic coastal ramps; one dipole source; fixed md step from the
@@ -579,16 +580,15 @@ def _run_multidomain(args, local, peak, peak_kind):
 
     def build(nts):
         sp = [NestDomain(s.lower_left, s.lw, s.nx, s.timestepping_method, nt) for s, nt in zip(specs, nts)]
-        md = Multidomain(sp, domain_kwargs=kw, use_wetdry_limiting=True, flux_correction=True, device=local)
+        md = Multidomain(sp, domain_kwargs=kw, use_wetdry_limiting=True, flux_correction=True, device=local,
+                         periodic_xs=(0.0, 360.0))
         for k, (s, d) in enumerate(zip(sp, md.domains)):
             lon, lat = s.x(), s.y()
             LON, LAT = np.meshgrid(lon, lat)
             elv = _coast_elevation(LON, LAT, coasts)
-            if k == 0:
+            if k == 0:   # walls north and south; periodic east-west
                 elv[:2, :] = 100.0
                 elv[-2:, :] = 100.0
-                elv[:, :2] = 100.0
-                elv[:, -2:] = 100.0
             eta = _dipoles(lon, lat, 1, seed=11, band=((144.0, -37.0), (150.0, -30.0)))[0]
             U = np.zeros((4, s.nx[1], s.nx[0]))
             U[3] = elv
@@ -626,7 +626,7 @@ def _run_multidomain(args, local, peak, peak_kind):
                       "domains": [{"nx": list(s.nx), "method": s.timestepping_method, "nt": nt,
                                    "nest_layer_width": s.nest_layer_width} for s, nt in zip(sp, nts)],
                       "md_dt": dt, "exchanges": len(md.exchanges), "flux_correction": True,
-                      "graph_steps": K, "sources": 1, "periodic": False},
+                      "graph_steps": K, "sources": 1, "periodic_xs": [0.0, 360.0]},
            "cell_updates_per_md_step": cells,
            "ms_per_md_step_without_graph": ms_plain,
            "graph_replay_speedup": ms_plain / ms_step,
