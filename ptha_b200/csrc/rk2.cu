@@ -298,15 +298,15 @@ __device__ __forceinline__ R bc_get(const BcArgs<R> &a, int i, int r, int v)
 }
 
 // West/east pass value of ring cell (i, r), i in {0, nx-1}.
-template <typename R>
+template <typename R, int KIND>
 __device__ __forceinline__ RingVal<R> we_value(const BcArgs<R> &a, int i, int r, double t)
 {
     const int in = (i == 0) ? 1 : a.nx - 2;
     RingVal<R> v;
-    if (a.kind == 1) {  // transmissive: all four variables from the inner neighbour
+    if (KIND == 1) {  // transmissive: all four variables from the inner neighbour
         v.e = a.elv[(int64_t)r * a.P + in];
         v.s = bc_get(a, in, r, 0); v.uh = bc_get(a, in, r, 1); v.vh = bc_get(a, in, r, 2);
-    } else if (a.kind == 3) {  // flather: normal momentum UH
+    } else if (KIND == 3) {  // flather: normal momentum UH
         v.e = a.elv[(int64_t)r * a.P + i];
         flather_cell<R>(a.bf, a.x, t, i, r, a.msl, i == 0, bc_get(a, in, r, 0), bc_get(a, in, r, 1),
                         bc_get(a, in, r, 2), a.elv[(int64_t)r * a.P + in], v.e, v.s, v.uh, v.vh);
@@ -318,7 +318,9 @@ __device__ __forceinline__ RingVal<R> we_value(const BcArgs<R> &a, int i, int r,
     return v;
 }
 
-template <typename R>
+// KIND (= a.kind) is a template parameter so that each boundary routine's
+// kernel carries only its own code.
+template <typename R, int KIND>
 __global__ void __launch_bounds__(256) rk2_boundary_kernel(const BcArgs<R> a)
 {
     const int nx = a.nx, ny = a.ny;
@@ -352,14 +354,14 @@ __global__ void __launch_bounds__(256) rk2_boundary_kernel(const BcArgs<R> a)
         RingVal<R> nb;
         const bool nb_we = (i == 0 && a.bext[3]) || (i == nx - 1 && a.bext[1]);
         if (nb_we) {
-            nb = we_value<R>(a, i, rn, t);
+            nb = we_value<R, KIND>(a, i, rn, t);
         } else {
             nb.e = a.elv[(int64_t)rn * a.P + i];
             nb.s = bc_get(a, i, rn, 0); nb.uh = bc_get(a, i, rn, 1); nb.vh = bc_get(a, i, rn, 2);
         }
-        if (a.kind == 1) {
+        if (KIND == 1) {
             v = nb;
-        } else if (a.kind == 3) {  // flather: normal momentum VH
+        } else if (KIND == 3) {  // flather: normal momentum VH
             v.e = a.elv[(int64_t)r * a.P + i];
             flather_cell<R>(a.bf, a.x, t, i, r, a.msl, r == 0, nb.s, nb.vh, nb.uh, nb.e, v.e, v.s, v.vh, v.uh);
         } else {
@@ -368,7 +370,7 @@ __global__ void __launch_bounds__(256) rk2_boundary_kernel(const BcArgs<R> a)
             v.vh = nb.vh;
         }
     } else {
-        v = we_value<R>(a, i, r, t);
+        v = we_value<R, KIND>(a, i, r, t);
     }
 
     const int64_t o = (int64_t)r * a.P + i;
@@ -392,7 +394,10 @@ template <typename R>
 cudaError_t launch_boundary(const BcArgs<R> &b, cudaStream_t s)
 {
     const int n = 2 * b.nx + 2 * (b.ny - 2);
-    rk2_boundary_kernel<R><<<(n + 255) / 256, 256, 0, s>>>(b);
+    const int blocks = (n + 255) / 256;
+    if (b.kind == 1) rk2_boundary_kernel<R, 1><<<blocks, 256, 0, s>>>(b);
+    else if (b.kind == 3) rk2_boundary_kernel<R, 3><<<blocks, 256, 0, s>>>(b);
+    else rk2_boundary_kernel<R, 2><<<blocks, 256, 0, s>>>(b);
     return cudaGetLastError();
 }
 
