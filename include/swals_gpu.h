@@ -336,6 +336,29 @@ int swals_gpu_set_priority_mask(swals_domain *d, const uint8_t *mask);
  * kinetic energy per unit density (row sums reduced by warps, rows added in
  * order). */
 int swals_gpu_domain_statistics(swals_domain *d, swals_domain_stats *out);
+/* ---- forcing patches (forcing_mod.f90:23-339) ----------------------------
+ * forcing_patch%setup + forcing_work, applied with apply_forcing_patch_array
+ * (:241-262) as the domain's forcing_subroutine: forcing_work (doubles,
+ * column-major over i0:i1, j0:j1, k0:k1, 1-based, k in STG=1..ELV=4) is
+ * added to U(i0:i1, j0:j1, k0:k1) at a constant rate between start_time and
+ * end_time (add_forcing_work_to_U_over_time, :80-156, with the default
+ * forcing_time_function; host time functions are not supported).  Patches
+ * are applied in the order added, after every update_U and boundary update
+ * of the finite-volume steppers and after the stage sweep and boundary
+ * update of the leapfrog solvers (domain_mod.f90:1564-1582,
+ * linear_solver_include.f90:123).  Elevation forcing follows
+ * support_elevation_forcing: 'euler' and the leapfrog solvers only.
+ * Leapfrog patches keep exterior_cells_width + 1 cells from the edges.
+ * Adding or clearing patches drops a captured evolve_steps graph; capture
+ * multidomain graphs after the patches are in place. */
+int swals_gpu_forcing_patch_add(swals_domain *d, int32_t i0, int32_t i1, int32_t j0, int32_t j1, int32_t k0,
+                                int32_t k1, double start_time, double end_time, const double *forcing_work,
+                                int32_t *index_out);
+int swals_gpu_forcing_clear(swals_domain *d);
+/* domain%apply_forcing(dt) (domain_mod.f90:1600-1646) on the current state
+ * at domain%time, outside a step. */
+int swals_gpu_apply_forcing(swals_domain *d, double dt);
+
 /* volume_in_priority_domain (domain_mod.f90:1851-1889): volume_interior over
  * the cells the priority mask keeps (all cells without a mask). */
 int swals_gpu_volume_in_priority_domain(swals_domain *d, double *out);

@@ -71,11 +71,29 @@ class _OracleDomainC(ctypes.Structure):
         ("explicit_source_VH_j_minus_1", ctypes.c_void_p), ("backup_U", ctypes.c_void_p),
         ("nest_nbox", ctypes.c_int32), ("friction_work_is_setup", ctypes.c_int32), ("nest_boxes", ctypes.c_void_p),
         ("nest_offset", ctypes.c_void_p), ("nest_integral", ctypes.c_void_p), ("friction_work", ctypes.c_void_p),
+        ("n_forcing", ctypes.c_int32), ("pad2", ctypes.c_int32), ("forcing", ctypes.c_void_p),
     ]
+
+
+class _ForcingPatchC(ctypes.Structure):
+    _fields_ = [("i0", ctypes.c_int32), ("i1", ctypes.c_int32), ("j0", ctypes.c_int32), ("j1", ctypes.c_int32),
+                ("k0", ctypes.c_int32), ("k1", ctypes.c_int32), ("start_time", ctypes.c_double),
+                ("end_time", ctypes.c_double), ("work", ctypes.c_void_p)]
 
 
 def _ptr(a):
     return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def add_forcing_work_to_U_over_time(U, work, time, dt, start_time, end_time, real32=False):
+    """forcing_mod.f90:80-156 on numpy arrays (U updated in place)."""
+    lib = _load(real32)
+    f = getattr(lib, ("oracle32_" if real32 else "oracle64_") + "add_forcing_work_to_U_over_time")
+    R = ctypes.c_float if real32 else ctypes.c_double
+    f.restype = None
+    f.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, R, R, R, R]
+    assert U.flags.c_contiguous and work.shape == U.shape
+    f(_ptr(U), _ptr(np.ascontiguousarray(work)), U.size, time, dt, start_time, end_time)
 
 
 class OracleDomain:
@@ -181,6 +199,21 @@ class OracleDomain:
         f.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
         return f(ctypes.addressof(self.c), None if m is None else _ptr(m))
+
+    def add_forcing_patch(self, i0, i1, j0, j1, k0, k1, start_time, end_time, work):
+        """forcing_patch%setup + forcing_work (forcing_mod.f90:264-319),
+        applied with apply_forcing_patch_array: 1-based inclusive indices,
+        work shaped (k1-k0+1, j1-j0+1, i1-i0+1)."""
+        w = np.ascontiguousarray(np.asarray(work, dtype=self.dtype).reshape(k1 - k0 + 1, j1 - j0 + 1, i1 - i0 + 1))
+        if not hasattr(self, "_patches"):
+            self._patches = []
+        self._patches.append((i0, i1, j0, j1, k0, k1, float(start_time), float(end_time), w))
+        arr = (_ForcingPatchC * len(self._patches))()
+        for q, (a, b, c_, d_, e, f, st, en, ww) in enumerate(self._patches):
+            arr[q] = _ForcingPatchC(a, b, c_, d_, e, f, st, en, ww.ctypes.data)
+        self._patch_arr = arr
+        self.c.n_forcing = len(self._patches)
+        self.c.forcing = ctypes.addressof(arr)
 
     def domain_statistics(self, mask=None):
         """compute_domain_statistics_new: (maxstage, maxspeed, minstage,

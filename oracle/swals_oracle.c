@@ -273,6 +273,48 @@ void ORACLE_FN(boundary_function)(const oracle_domain *d, double t, int32_t i, i
     }
 }
 
+/* ------------------------------------------------------------------------ */
+/* Forcing (forcing_mod.f90) */
+
+/* The fraction of the forcing that falls in the step (time - dt, time)
+ * (forcing_mod.f90:97-124, constant rate); 0 outside the forcing interval. */
+static REAL forcing_update_fraction(REAL time, REAL dt, REAL start_time, REAL end_time, int *active)
+{
+    *active = ((time - dt) <= end_time) && (time >= start_time);
+    if (!*active) return ZERO;
+    if (start_time == end_time) return ONE;
+    return (rmin(time, end_time) - rmax(time - dt, start_time)) / (end_time - start_time);
+}
+
+void ORACLE_FN(add_forcing_work_to_U_over_time)(REAL *U, const REAL *work, int64_t n, REAL time, REAL dt,
+                                                REAL start_time, REAL end_time)
+{
+    int active;
+    const REAL uf = forcing_update_fraction(time, dt, start_time, end_time, &active);
+    if (!active) return;
+    for (int64_t q = 0; q < n; q++) U[q] = U[q] + uf * work[q];
+}
+
+/* apply_forcing (domain_mod.f90:1600-1646) with the patches of
+ * apply_forcing_patch_array (forcing_mod.f90:241-262), at domain%time. */
+static void apply_forcing(oracle_domain *d, REAL dt)
+{
+    const int nx = d->nx, ny = d->ny;
+    for (int p = 0; p < d->n_forcing; p++) {
+        const oracle_forcing_patch *fp = &d->forcing[p];
+        int active;
+        const REAL uf = forcing_update_fraction((REAL)d->time, dt, (REAL)fp->start_time, (REAL)fp->end_time, &active);
+        if (!active) continue;
+        const int ni = fp->i1 - fp->i0 + 1, nj = fp->j1 - fp->j0 + 1;
+        for (int k = fp->k0; k <= fp->k1; k++)
+            for (int j = fp->j0; j <= fp->j1; j++)
+                for (int i = fp->i0; i <= fp->i1; i++) {
+                    const REAL w = fp->work[(size_t)(k - fp->k0) * ni * nj + (size_t)(j - fp->j0) * ni + (i - fp->i0)];
+                    UU(k, i, j) = UU(k, i, j) + uf * w;
+                }
+    }
+}
+
 static int is_staggered(const oracle_domain *d)
 {
     return d->method == OR_METHOD_LINEAR || d->method == OR_METHOD_LEAPFROG_LINEAR_PLUS_NONLINEAR_FRICTION ||
@@ -579,6 +621,7 @@ static void linear_leapfrog_step(oracle_domain *d, REAL dt)
     d->time = d->time + (double)(dt * HALF);
 
     update_boundary(d);
+    apply_forcing(d, dt);
 
     /* Boundary flux integration (:130-150); single-domain case */
     {
@@ -1136,6 +1179,7 @@ static void update_U(oracle_domain *d, REAL dt)
     }
     d->time = d->time + (double)dt;
     update_boundary(d);
+    apply_forcing(d, dt);
 }
 
 /* timestepping_alternatives_include.f90:8-62 */

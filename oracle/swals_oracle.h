@@ -132,7 +132,28 @@ typedef struct oracle_domain {
     /* leapfrog_linear_plus_nonlinear_friction: g n^2 depth^p at the UH and
      * VH points (nx*ny*2, domain%friction_work) */
     REAL *friction_work;
+    /* forcing_patch_array_type (forcing_mod.f90:55-60), applied in order */
+    int32_t n_forcing;
+    int32_t pad2;
+    const struct oracle_forcing_patch *forcing;
 } oracle_domain;
+
+/* forcing_patch_type (forcing_mod.f90:23-53) with the default (identity)
+ * forcing_time_function: work (i fastest, then j, then k, over
+ * i0..i1 x j0..j1 x k0..k1, 1-based, k in STG..ELV) is added to
+ * U(i0:i1, j0:j1, k0:k1) at a constant rate between start_time and
+ * end_time. */
+typedef struct oracle_forcing_patch {
+    int32_t i0, i1, j0, j1, k0, k1;
+    double start_time, end_time;
+    const REAL *work;
+} oracle_forcing_patch;
+
+/* add_forcing_work_to_U_over_time (forcing_mod.f90:80-156) on an array U of
+ * n values with the matching forcing_work, for the time step
+ * (time - dt, time). */
+void ORACLE_FN(add_forcing_work_to_U_over_time)(REAL *U, const REAL *work, int64_t n, REAL time, REAL dt,
+                                                REAL start_time, REAL end_time);
 
 /* One side of a two_way_nesting_comms_type (nested_grid_comms_mod.f90:
  * 120-255), as set up by initialise_two_way_nesting_comms (:257-658). */

@@ -390,6 +390,8 @@ int check_adjoint_domain(swals_domain *d)
         return swals::api_fail(SWALS_ERR_UNSUPPORTED, "the adjoint is implemented for timestepping_method='linear'");
     if (!d->cfg.truely_linear)
         return swals::api_fail(SWALS_ERR_UNSUPPORTED, "the adjoint needs linear_solver_is_truely_linear=.true.");
+    if (d->cfg.n_forcing)
+        return swals::api_fail(SWALS_ERR_UNSUPPORTED, "forcing patches are not supported here");
     if (d->cfg.bc_kind != SWALS_BC_NONE)
         return swals::api_fail(SWALS_ERR_UNSUPPORTED, "the adjoint supports walls via elevation only");
     return SWALS_OK;

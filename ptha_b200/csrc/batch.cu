@@ -177,6 +177,8 @@ int swals_gpu_batch_create(swals_domain *grid, int32_t nbatch, int32_t record_ma
     *out = nullptr;
     if (strncmp(grid->desc.timestepping_method, "linear", 6) != 0 || grid->desc.timestepping_method[6] > ' ')
         return api_fail(SWALS_ERR_UNSUPPORTED, "batches are implemented for timestepping_method='linear' only");
+    if (grid->cfg.n_forcing)
+        return swals::api_fail(SWALS_ERR_UNSUPPORTED, "forcing patches are not supported here");
     if (grid->cfg.bc_kind != SWALS_BC_NONE)
         return api_fail(SWALS_ERR_UNSUPPORTED, "batches support walls via elevation only (no boundary routine)");
     swals_batch *b = new swals_batch();

@@ -495,10 +495,22 @@ static void drop_step_graph(swals_domain *d)
     d->step_graph = nullptr;
 }
 
+static void free_forcing(swals_domain *d)
+{
+    for (auto &f : d->forcing) {
+        if (f.work) cudaFree(f.work);
+        if (f.saved_max) cudaFree(f.saved_max);
+    }
+    d->forcing.clear();
+    d->cfg.n_forcing = 0;
+    d->cfg.forcing = nullptr;
+}
+
 int swals_gpu_domain_destroy(swals_domain *d)
 {
     if (!d) return SWALS_OK;
     cudaStreamSynchronize(d->stream);
+    free_forcing(d);
     for (auto &p : d->pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
     for (auto e : d->ev_pool) cudaEventDestroy(e);
     if (d->d_sites) cudaFree(d->d_sites);
@@ -806,6 +818,96 @@ static int volume_impl(swals_domain *d, double *out, const uint8_t *mask)
     if (e != cudaSuccess) return cuda_fail(e, "volume_interior");
     CK(cudaMemcpyAsync(out, d->d_out, sizeof(double), cudaMemcpyDeviceToHost, d->stream));
     CK(cudaStreamSynchronize(d->stream));
+    return SWALS_OK;
+}
+
+int swals_gpu_forcing_patch_add(swals_domain *d, int32_t i0, int32_t i1, int32_t j0, int32_t j1, int32_t k0,
+                                int32_t k1, double start_time, double end_time, const double *forcing_work,
+                                int32_t *index_out)
+{
+    if (!d || !forcing_work) return fail(SWALS_ERR_INVALID_ARGUMENT, "NULL argument");
+    // apply_forcing_patch_base's checks (forcing_mod.f90:175-201)
+    if (i0 > i1 || j0 > j1 || i0 < 1 || j0 < 1 || i1 > d->nx || j1 > d->ny)
+        return fail(SWALS_ERR_INVALID_ARGUMENT, "Error in apply_forcing_patch: the forcing_patch does not have indices "
+                                                "set correctly (%d:%d, %d:%d in a %d x %d domain)",
+                    i0, i1, j0, j1, d->nx, d->ny);
+    if (start_time > end_time)
+        return fail(SWALS_ERR_INVALID_ARGUMENT,
+                    "Error in apply_forcing_patch: the forcing_patch start/end times are not set correctly");
+    if (!(k0 >= 1 && k0 <= 4 && k1 >= 1 && k1 <= 4 && k0 <= k1))
+        return fail(SWALS_ERR_INVALID_ARGUMENT, "forcing_work has a 3rd dimension incompatible with domain%%U (%d:%d)",
+                    k0, k1);
+    const bool elevation_always = (d->method == M_EULER || is_staggered(d->method));
+    if (k1 == 4 && !elevation_always)
+        return fail(SWALS_ERR_UNSUPPORTED, "forcing the elevation with '%s' needs support_elevation_forcing "
+                                           "(elevation in the backed-up state), which this GPU path does not implement",
+                    d->desc.timestepping_method);
+    if (is_staggered(d->method)) {
+        const int m = d->desc.exterior_cells_width + 2;
+        if (i0 < m || j0 < m || i1 > d->nx - m + 1 || j1 > d->ny - m + 1)
+            return fail(SWALS_ERR_UNSUPPORTED, "leapfrog forcing patches must keep exterior_cells_width + 1 cells "
+                                               "from the domain edges (i, j in %d..%d, %d..%d)",
+                        m, d->nx - m + 1, m, d->ny - m + 1);
+        if (d->method == M_LF_LIN_NLFRIC && !d->desc.linear_solver_is_truely_linear)
+            return fail(SWALS_ERR_UNSUPPORTED, "forcing patches with the not truely linear "
+                                               "leapfrog_linear_plus_nonlinear_friction are not implemented");
+    }
+    const int ni = i1 - i0 + 1, nj = j1 - j0 + 1, nk = k1 - k0 + 1;
+    const size_t n = (size_t)ni * nj * nk, es = esize(d);
+    CK(cudaStreamSynchronize(d->stream));   // no step in flight while the patch list changes
+    swals::ForcingPatch f{};
+    f.i0 = i0 - 1; f.i1 = i1 - 1; f.j0 = j0 - 1; f.j1 = j1 - 1; f.k0 = k0 - 1; f.k1 = k1 - 1;
+    f.start_time = start_time;
+    f.end_time = end_time;
+    CK(cudaMalloc(&f.work, n * es));
+    cudaError_t e;
+    if (d->fp64) {
+        e = cudaMemcpy(f.work, forcing_work, n * es, cudaMemcpyHostToDevice);
+    } else {
+        std::vector<float> tmp(forcing_work, forcing_work + n);
+        e = cudaMemcpy(f.work, tmp.data(), n * es, cudaMemcpyHostToDevice);
+    }
+    if (e == cudaSuccess && k0 == 1 && is_staggered(d->method) && d->desc.record_max_stage)
+        e = cudaMalloc(&f.saved_max, (size_t)ni * nj * es);
+    if (e != cudaSuccess) {
+        cudaFree(f.work);
+        if (f.saved_max) cudaFree(f.saved_max);
+        return cuda_fail(e, "forcing patch upload");
+    }
+    d->forcing.push_back(f);
+    d->cfg.n_forcing = (int)d->forcing.size();
+    d->cfg.forcing = d->forcing.data();
+    drop_step_graph(d);
+    if (index_out) *index_out = d->cfg.n_forcing - 1;
+    return SWALS_OK;
+}
+
+int swals_gpu_forcing_clear(swals_domain *d)
+{
+    if (!d) return fail(SWALS_ERR_INVALID_ARGUMENT, "NULL domain");
+    CK(cudaStreamSynchronize(d->stream));
+    free_forcing(d);
+    drop_step_graph(d);
+    return SWALS_OK;
+}
+
+int swals_gpu_apply_forcing(swals_domain *d, double dt)
+{
+    if (!d) return fail(SWALS_ERR_INVALID_ARGUMENT, "NULL domain");
+    swals::ForcingClock clk{};
+    clk.mode = swals::FORCE_EXPLICIT;
+    clk.dt = dt;
+    const swals::LaunchHook hook = swals::hook_of(d);
+    cudaError_t e;
+    if (d->fp64)
+        e = swals::launch_forcing<double>(d->cfg, clk, d->pitch, (double *)d->planes[d->cur][0],
+                                          (double *)d->planes[d->cur][1], (double *)d->planes[d->cur][2],
+                                          (double *)d->elv, d->sc, d->stream, hook, swals::CAT_FINALIZE);
+    else
+        e = swals::launch_forcing<float>(d->cfg, clk, d->pitch, (float *)d->planes[d->cur][0],
+                                         (float *)d->planes[d->cur][1], (float *)d->planes[d->cur][2],
+                                         (float *)d->elv, d->sc, d->stream, hook, swals::CAT_FINALIZE);
+    if (e != cudaSuccess) return cuda_fail(e, "apply_forcing");
     return SWALS_OK;
 }
 

@@ -55,6 +55,9 @@ struct swals_domain {
     double *stats_buf = nullptr;
     // Side stream for the leapfrog's bookkeeping kernel.
     swals::AuxStream aux;
+    // Forcing patches (forcing_mod.f90), device buffers owned here;
+    // cfg.forcing points at this vector's data.
+    std::vector<swals::ForcingPatch> forcing;
     // Replayed graph of a few steps for evolve_steps.
     cudaGraphExec_t step_graph = nullptr;
     double graph_dt = 0.0;

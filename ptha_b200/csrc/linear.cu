@@ -750,40 +750,31 @@ __global__ void __launch_bounds__(256) linear_flather_ring_kernel(const LinArgs<
     ring[2 * q + 1] = v.vh;
 }
 
+// The momentum update (:225-567) of one cell (i, r), redone after the step
+// kernel from the stage in stg_o, the elevation and the old momenta as the
+// boundary routine (ring buffer) and any forcing left them.  Cells outside
+// the update range get their old momenta when write_outside.
 template <typename R, bool CORIOLIS, bool TRUELY_LINEAR>
-__global__ void __launch_bounds__(256) linear_flather_fix_kernel(const LinArgs<R> a, const R *ring)
+__device__ __forceinline__ void momentum_recompute(const LinArgs<R> &a, const R *ring, int i, int r, bool write_outside)
 {
     const int nx = a.p.nx, ny = a.p.ny;
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    // Rows 0, 1, ny-2, ny-1 in full, then columns 0, 1, nx-2, nx-1 of rows 2 .. ny-3.
-    int i, r;
-    if (q < 4 * nx) {
-        const int k = q / nx;
-        i = q - k * nx;
-        r = (k < 2) ? k : ny - 4 + k;
-    } else if (q < 4 * nx + 4 * (ny - 4)) {
-        const int p = q - 4 * nx;
-        const int k = p / (ny - 4);
-        r = 2 + (p - k * (ny - 4));
-        i = (k < 2) ? k : nx - 4 + k;
-    } else {
-        return;
-    }
     const int64_t P = a.p.pitch;
     const R g = K<R>::gravity(), half = K<R>::half(), one = K<R>::one(), zero = K<R>::zero();
     const R mad = K<R>::min_depth();
-    // Momenta as the boundary routine left them.
+    // Momenta as the boundary routine (and any forcing) left them.
     auto uhb = [&](int ii, int rr) -> R {
-        return on_bc_ring(ii, rr, nx, ny, a.bext) ? ring[2 * ring_index(ii, rr, nx, ny)]
-                                                  : a.p.uh[(int64_t)rr * P + ii];
+        return (ring && on_bc_ring(ii, rr, nx, ny, a.bext)) ? ring[2 * ring_index(ii, rr, nx, ny)]
+                                                            : a.p.uh[(int64_t)rr * P + ii];
     };
     auto vhb = [&](int ii, int rr) -> R {
-        return on_bc_ring(ii, rr, nx, ny, a.bext) ? ring[2 * ring_index(ii, rr, nx, ny) + 1]
-                                                  : a.p.vh[(int64_t)rr * P + ii];
+        return (ring && on_bc_ring(ii, rr, nx, ny, a.bext)) ? ring[2 * ring_index(ii, rr, nx, ny) + 1]
+                                                            : a.p.vh[(int64_t)rr * P + ii];
     };
     const int64_t o = (int64_t)r * P + i;
     R uh = uhb(i, r), vh = vhb(i, r);
-    if (i >= a.xl && i <= a.xu - 1 && r >= a.yl && r <= a.yu - 1) {
+    const bool updated = (i >= a.xl && i <= a.xu - 1 && r >= a.yl && r <= a.yu - 1);
+    if (!updated && !write_outside) return;
+    if (updated) {
         const R inv_cell_area_dt_g = g * a.dt / a.m.area[r];
         const R inv_cell_area_dt_vh_g = g * a.dt / (half * (a.m.area[r] + a.m.area[r + 1]));
         const R e0 = a.p.elv[o], e_e = a.p.elv[o + 1], e_n = a.p.elv[o + P];
@@ -827,6 +818,40 @@ __global__ void __launch_bounds__(256) linear_flather_fix_kernel(const LinArgs<R
     }
     a.p.uh_o[o] = uh;
     a.p.vh_o[o] = vh;
+}
+
+template <typename R, bool CORIOLIS, bool TRUELY_LINEAR>
+__global__ void __launch_bounds__(256) linear_flather_fix_kernel(const LinArgs<R> a, const R *ring)
+{
+    const int nx = a.p.nx, ny = a.p.ny;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    // Rows 0, 1, ny-2, ny-1 in full, then columns 0, 1, nx-2, nx-1 of rows 2 .. ny-3.
+    int i, r;
+    if (q < 4 * nx) {
+        const int k = q / nx;
+        i = q - k * nx;
+        r = (k < 2) ? k : ny - 4 + k;
+    } else if (q < 4 * nx + 4 * (ny - 4)) {
+        const int p = q - 4 * nx;
+        const int k = p / (ny - 4);
+        r = 2 + (p - k * (ny - 4));
+        i = (k < 2) ? k : nx - 4 + k;
+    } else {
+        return;
+    }
+    momentum_recompute<R, CORIOLIS, TRUELY_LINEAR>(a, ring, i, r, true);
+}
+
+// The momentum of the cells within one cell of a forcing patch box
+// (0-based inclusive [i0, i1] x [r0, r1], already widened), after the forcing.
+template <typename R, bool CORIOLIS, bool TRUELY_LINEAR>
+__global__ void __launch_bounds__(256) linear_box_fix_kernel(const LinArgs<R> a, int i0, int i1, int r0, int r1)
+{
+    const int w = i1 - i0 + 1;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= w * (r1 - r0 + 1)) return;
+    const int r = r0 + q / w, i = i0 + q % w;
+    momentum_recompute<R, CORIOLIS, TRUELY_LINEAR>(a, nullptr, i, r, false);
 }
 
 // precompute_friction_work (linear_solver_include.f90:590-618,
@@ -1131,6 +1156,38 @@ void launch_friction_work(LinArgs<R> &a, const StepPlanes<R> &p, const StepConfi
     hook(CAT_LINEAR_EDGE, 1);
 }
 
+// apply_forcing between the stage sweep and the momentum sweep
+// (linear_solver_include.f90:123), after the step kernel: the patches are
+// added to the new stage and to the old momenta and elevation (in place:
+// the step kernel has read them), max_stage is redone over the patches, and
+// the momentum of every cell within one cell of a patch is recomputed.
+// Patches keep n_ext + 1 cells from the edges (checked when added), clear of
+// the boundary ring and of the boundary-flux lines.
+template <typename R>
+void launch_leapfrog_forcing(const LinArgs<R> &a, const StepPlanes<R> &p, const StepConfig &c, const DevScalars *sc,
+                             cudaStream_t s, const LaunchHook &hook)
+{
+    ForcingClock clk{};
+    clk.mode = FORCE_LEAPFROG;
+    clk.dt = (double)a.dt;
+    launch_forcing<R>(c, clk, p.pitch, p.stg_o, const_cast<R *>(p.uh), const_cast<R *>(p.vh), p.elv, sc, s, hook,
+                      CAT_LINEAR_EDGE);
+    if (p.max_stage) launch_forcing_restore_max<R>(c, p.pitch, p.stg_o, p.max_stage, s, hook, CAT_LINEAR_EDGE);
+    const bool cor = c.coriolis != 0, tl = c.truely_linear != 0;
+    for (int k = 0; k < c.n_forcing; k++) {
+        const ForcingPatch &f = c.forcing[k];
+        const int i0 = max(f.i0 - 1, 0), i1 = min(f.i1 + 1, p.nx - 1);
+        const int r0 = max(f.j0 - 1, 0), r1 = min(f.j1 + 1, p.ny - 1);
+        const int n = (i1 - i0 + 1) * (r1 - r0 + 1), blocks = (n + 255) / 256;
+        hook(CAT_LINEAR_EDGE, 0);
+        if (cor && tl) linear_box_fix_kernel<R, true, true><<<blocks, 256, 0, s>>>(a, i0, i1, r0, r1);
+        else if (cor && !tl) linear_box_fix_kernel<R, true, false><<<blocks, 256, 0, s>>>(a, i0, i1, r0, r1);
+        else if (!cor && tl) linear_box_fix_kernel<R, false, true><<<blocks, 256, 0, s>>>(a, i0, i1, r0, r1);
+        else linear_box_fix_kernel<R, false, false><<<blocks, 256, 0, s>>>(a, i0, i1, r0, r1);
+        hook(CAT_LINEAR_EDGE, 1);
+    }
+}
+
 template <typename R>
 void launch_nlfric(const LinArgs<R> &a, const StepPlanes<R> &p, const R *ring, cudaStream_t s, const LaunchHook &hook)
 {
@@ -1145,7 +1202,9 @@ cudaError_t launch_linear_step(const StepPlanes<R> &p, const Metrics<R> &m, cons
                                DevScalars *sc, cudaStream_t s, const LaunchHook &hook, const AuxStream *aux)
 {
     LinArgs<R> a = make_args<R>(p, m, c, dt);
-    const bool side = aux && aux->stream && !a.bc_stage;
+    // Forcing patches read domain%time from the edge kernel and change the
+    // old momenta in place, so the edge kernel then runs in line.
+    const bool side = aux && aux->stream && !a.bc_stage && !c.n_forcing;
     if (side) {
         // Bookkeeping beside the main kernel: it reads the input planes and
         // writes only the scalars; the main stream waits for it at the end.
@@ -1178,6 +1237,7 @@ cudaError_t launch_linear_step(const StepPlanes<R> &p, const Metrics<R> &m, cons
     linear_edge_kernel<R><<<1, 512, 0, s>>>(a, sc, c.exterior_cells_width, c.bf);
     hook(CAT_LINEAR_EDGE, 1);
     if (c.fw) launch_friction_work<R>(a, p, c, s, hook);
+    if (c.n_forcing && p.max_stage) launch_forcing_save_max<R>(c, p.pitch, p.max_stage, s, hook, CAT_LINEAR_EDGE);
     hook(CAT_LINEAR_MAIN, 0);
     launch_main<R>(a, c, plain_config(p.nx, p.ny), s);
     hook(CAT_LINEAR_MAIN, 1);
@@ -1192,6 +1252,7 @@ cudaError_t launch_linear_step(const StepPlanes<R> &p, const Metrics<R> &m, cons
         else linear_flather_fix_kernel<R, false, false><<<blocks, 256, 0, s>>>(a, ring);
         hook(CAT_LINEAR_EDGE, 1);
     }
+    if (c.n_forcing) launch_leapfrog_forcing<R>(a, p, c, sc, s, hook);
     if (c.fw) launch_nlfric<R>(a, p, flather ? ring : nullptr, s, hook);
     return cudaGetLastError();
 }

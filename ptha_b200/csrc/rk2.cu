@@ -788,6 +788,49 @@ cudaError_t later_stage(Rk2Args<R> a, R *const planes[3][3], int in, int out, bo
 
 bool has_bc(const StepConfig &c) { return c.bc_kind == 1 || c.bc_kind == 2 || c.bc_kind == 3; }
 
+// The end of update_U into planes[P_] (domain_mod.f90:1564-1582):
+// update_boundary, then apply_forcing, at the update's time time0 + n_dt dt
+// (+ dt * extra, which is then the update's dt).
+template <typename R>
+cudaError_t end_of_update(BcArgs<R> &b, const StepConfig &c, R *const planes[3][3], int P_, int n_dt, R extra,
+                          cudaStream_t s, const LaunchHook &hook, int cat)
+{
+    b.stg = planes[P_][0]; b.uh = planes[P_][1]; b.vh = planes[P_][2];
+    b.stage_mode = 1; b.n_dt = n_dt; b.dt_extra = extra;
+    cudaError_t e = cudaSuccess;
+    if (has_bc(c)) {
+        hook(cat, 0);
+        e = launch_boundary<R>(b, s);
+        hook(cat, 1);
+        if (e != cudaSuccess) return e;
+    }
+    if (c.n_forcing) {
+        ForcingClock clk{};
+        clk.mode = FORCE_FV_STAGE;
+        clk.n_dt = n_dt;
+        clk.dt_extra = (double)extra;
+        clk.dt_from_cfl = b.dt_from_cfl;
+        clk.dt_fixed = b.dt_fixed;
+        clk.max_dt_inv_init = b.max_dt_inv_init;
+        e = launch_forcing<R>(c, clk, b.P, b.stg, b.uh, b.vh, b.elv, b.sc, s, hook, cat);
+    }
+    return e;
+}
+
+// rk2's average U = (U + U0) / 2 (timestepping_alternatives_include.f90:
+// 124-135), for the unfused stage 2 (forcing patches present).
+template <typename R>
+__global__ void rk2_average_kernel(int nx, int ny, int64_t P, R *u0, R *u1, R *u2, const R *b0, const R *b1,
+                                   const R *b2)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, r = blockIdx.y;
+    if (i >= nx) return;
+    const int64_t o = (int64_t)r * P + i;
+    u0[o] = R(0.5) * (u0[o] + b0[o]);
+    u1[o] = R(0.5) * (u1[o] + b1[o]);
+    u2[o] = R(0.5) * (u2[o] + b2[o]);
+}
+
 }  // namespace
 
 template <typename R>
@@ -809,14 +852,7 @@ cudaError_t launch_rk2_step(R *const planes[3][3], int &cur, R *elv, R *max_stag
     if (e != cudaSuccess) return e;
 
     BcArgs<R> b = bc_args<R>(a, c, dt);
-    if (bc) {
-        b.stg = planes[B][0]; b.uh = planes[B][1]; b.vh = planes[B][2];
-        b.stage_mode = 1; b.n_dt = 1;
-        hook(CAT_BC1, 0);
-        e = launch_boundary<R>(b, s);
-        hook(CAT_BC1, 1);
-        if (e != cudaSuccess) return e;
-    }
+    if ((e = end_of_update<R>(b, c, planes, B, 1, R(0), s, hook, CAT_BC1)) != cudaSuccess) return e;
     if (euler_only) {
         if (max_stage) {
             hook(CAT_MAXSTAGE, 0);
@@ -830,6 +866,30 @@ cudaError_t launch_rk2_step(R *const planes[3][3], int &cur, R *elv, R *max_stag
         hook(CAT_FINALIZE, 1);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         cur = B;
+        return cudaSuccess;
+    }
+    if (c.n_forcing) {
+        // Stage 2 as an Euler step, its boundary and forcing, then the average.
+        e = later_stage<R>(a, planes, B, C, has_dt, lines2, c, s, hook, CAT_STAGE2);
+        if (e != cudaSuccess) return e;
+        if ((e = end_of_update<R>(b, c, planes, C, 2, R(0), s, hook, CAT_BC2)) != cudaSuccess) return e;
+        hook(CAT_STAGE2, 0);
+        rk2_average_kernel<R><<<dim3((nx + 255) / 256, ny), 256, 0, s>>>(
+            nx, ny, pitch, planes[C][0], planes[C][1], planes[C][2], planes[A][0], planes[A][1], planes[A][2]);
+        hook(CAT_STAGE2, 1);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if (max_stage) {
+            hook(CAT_MAXSTAGE, 0);
+            e = launch_update_max_stage<R>(nx, ny, pitch, planes[C][0], max_stage, c, s);
+            hook(CAT_MAXSTAGE, 1);
+            if (e != cudaSuccess) return e;
+        }
+        hook(CAT_FINALIZE, 0);
+        rk2_finalize_kernel<R, FIN_RK2><<<1, 1024, 0, s>>>(nx, ny, c.exterior_cells_width, lines1, a.dt_from_cfl,
+                                                           dt, max_dt_inv_init, sc);
+        hook(CAT_FINALIZE, 1);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        cur = C;
         return cudaSuccess;
     }
     // Stage 2: B -> C, averaged with U0 (A)
@@ -919,29 +979,15 @@ cudaError_t launch_midpoint_step(R *const planes[3][3], int &cur, R *elv, R *max
     e = first_stage<R>(a, planes, A, B, has_dt, buf, lines1, c, s, hook);
     if (e != cudaSuccess) return e;
     BcArgs<R> b = bc_args<R>(a, c, dt);
-    if (bc) {
-        // update_U(dt/2) ends with update_boundary at time + dt/2
-        b.stg = planes[B][0]; b.uh = planes[B][1]; b.vh = planes[B][2];
-        b.n_dt = 0; b.dt_extra = K<R>::half();
-        hook(CAT_BC1, 0);
-        e = launch_boundary<R>(b, s);
-        hook(CAT_BC1, 1);
-        if (e != cudaSuccess) return e;
-    }
+    // update_U(dt/2) ends with update_boundary and apply_forcing at time + dt/2
+    if ((e = end_of_update<R>(b, c, planes, B, 0, K<R>::half(), s, hook, CAT_BC1)) != cudaSuccess) return e;
     Rk2Args<R> a2 = a;
     a2.dt_scale = R(1);
     a2.base0 = 1;
     a2.stg0 = planes[A][0]; a2.uh0 = planes[A][1]; a2.vh0 = planes[A][2];
     e = later_stage<R>(a2, planes, B, C, has_dt, lines2, c, s, hook, CAT_STAGE2);
     if (e != cudaSuccess) return e;
-    if (bc) {
-        b.stg = planes[C][0]; b.uh = planes[C][1]; b.vh = planes[C][2];
-        b.n_dt = 1; b.dt_extra = R(0);
-        hook(CAT_BC2, 0);
-        e = launch_boundary<R>(b, s);
-        hook(CAT_BC2, 1);
-        if (e != cudaSuccess) return e;
-    }
+    if ((e = end_of_update<R>(b, c, planes, C, 1, R(0), s, hook, CAT_BC2)) != cudaSuccess) return e;
     if (max_stage) {
         hook(CAT_MAXSTAGE, 0);
         e = launch_update_max_stage<R>(nx, ny, pitch, planes[C][0], max_stage, c, s);
@@ -980,13 +1026,7 @@ cudaError_t launch_rk2n_step(R *const planes[3][3], int &cur, R *elv, R *max_sta
     if (e != cudaSuccess) return e;
     BcArgs<R> b = bc_args<R>(a, c, dt_sub);
     auto boundary = [&](int P_, int n_dt, R extra) -> cudaError_t {
-        if (!bc) return cudaSuccess;
-        b.stg = planes[P_][0]; b.uh = planes[P_][1]; b.vh = planes[P_][2];
-        b.n_dt = n_dt; b.dt_extra = extra;
-        hook(CAT_BC1, 0);
-        cudaError_t r = launch_boundary<R>(b, s);
-        hook(CAT_BC1, 1);
-        return r;
+        return end_of_update<R>(b, c, planes, P_, n_dt, extra, s, hook, CAT_BC1);
     };
     if ((e = boundary(B, 1, R(0))) != cudaSuccess) return e;
     // sub-steps 2 .. n-1

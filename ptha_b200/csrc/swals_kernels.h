@@ -44,6 +44,30 @@ enum {
     FLUX_UPWIND_TRANSVERSE = 2   // upwind_transverse_momentum = .true.
 };
 
+// forcing_patch_type (forcing_mod.f90:23-53) on the device: a 0-based
+// inclusive box, variables k0..k1 (0 STG, 1 UH, 2 VH, 3 ELV), forcing_work as
+// R planes (k, j, i) with i fastest; saved_max holds the leapfrog step's copy
+// of max_stage over the box (patches that force STG).
+struct ForcingPatch {
+    int i0, i1, j0, j1, k0, k1;
+    double start_time, end_time;
+    void *work;
+    void *saved_max;
+};
+
+// The time and timestep a forcing is applied with (domain%time after the
+// update, and the update's dt).
+enum { FORCE_FV_STAGE = 0, FORCE_LEAPFROG = 1, FORCE_EXPLICIT = 2 };
+struct ForcingClock {
+    int mode;
+    int n_dt;               // FV: time = time0 + dt + ... (n_dt additions)
+    double dt_extra;        // FV: then + dt * dt_extra when nonzero, which is also the update's dt
+    int dt_from_cfl;        // FV: dt from the CFL maximum, else dt_fixed
+    double dt_fixed;
+    double max_dt_inv_init;
+    double dt;              // FORCE_EXPLICIT: dt (time = domain%time); FORCE_LEAPFROG: dt (time = time0 + dt/2)
+};
+
 struct StepConfig {
     int xl, xu, yl, yu;     // 0-based inclusive active region (domain%xL-1 ...)
     int bext[4];            // boundary_exterior N,E,S,W
@@ -56,7 +80,23 @@ struct StepConfig {
     void *ring;             // linear + Flather: 2 (nx + ny - 2) x 2 reals of ring momenta
     void *fw;               // leapfrog_linear_plus_nonlinear_friction: friction_work (2 planes), else null
     int fw_ready;           // truely linear: friction_work already computed (friction_work_is_setup)
+    int n_forcing;          // forcing patches, applied in order (apply_forcing_patch_array)
+    const ForcingPatch *forcing;
 };
+
+// Forcing patches (forcing.cu): add each active patch's share of its
+// forcing_work to the planes of k = STG, UH, VH, ELV.
+template <typename R>
+cudaError_t launch_forcing(const StepConfig &c, const ForcingClock &clk, int64_t pitch, R *stg, R *uh, R *vh,
+                           R *elv, const DevScalars *sc, cudaStream_t s, const LaunchHook &hook, int cat);
+// Leapfrog steps: copy max_stage over the STG patches' boxes before the step
+// kernel; afterwards max_stage = max(copy, forced stage) there.
+template <typename R>
+cudaError_t launch_forcing_save_max(const StepConfig &c, int64_t pitch, const R *max_stage, cudaStream_t s,
+                                    const LaunchHook &hook, int cat);
+template <typename R>
+cudaError_t launch_forcing_restore_max(const StepConfig &c, int64_t pitch, const R *stg, R *max_stage,
+                                       cudaStream_t s, const LaunchHook &hook, int cat);
 
 // compute_domain_statistics_new: rows6 is 6*ny doubles of scratch; out7 (device)
 // receives {maxstage, maxspeed, minstage, minspeed, E_pot, E_kin, E_total}.

@@ -213,6 +213,26 @@ class Domain:
         m = np.ascontiguousarray(np.asarray(mask).astype(np.uint8).reshape(self.nx[1], self.nx[0]))
         check(self._L.swals_gpu_set_priority_mask(self._h, _p(m)))
 
+    def add_forcing_patch(self, i0, i1, j0, j1, k0, k1, start_time, end_time, forcing_work):
+        """forcing_patch%setup(start_time, end_time, i0, i1, j0, j1, k0, k1)
+        with its forcing_work (1-based inclusive indices; forcing_work shaped
+        (k1-k0+1, j1-j0+1, i1-i0+1), i.e. [k][j][i] like get_U), applied as
+        the domain's forcing (apply_forcing_patch_array).  Returns the
+        patch's index."""
+        w = np.ascontiguousarray(np.asarray(forcing_work, dtype=np.float64)
+                                 .reshape(k1 - k0 + 1, j1 - j0 + 1, i1 - i0 + 1))
+        idx = ctypes.c_int32()
+        check(self._L.swals_gpu_forcing_patch_add(self._h, i0, i1, j0, j1, k0, k1, float(start_time),
+                                                  float(end_time), _p(w), ctypes.byref(idx)))
+        return idx.value
+
+    def forcing_clear(self):
+        check(self._L.swals_gpu_forcing_clear(self._h))
+
+    def apply_forcing(self, dt):
+        """domain%apply_forcing(dt) on the current state at domain%time."""
+        check(self._L.swals_gpu_apply_forcing(self._h, float(dt)))
+
     def volume_in_priority_domain(self):
         """volume_interior over the cells set_priority_mask kept."""
         return self._scalar(self._L.swals_gpu_volume_in_priority_domain)

@@ -93,3 +93,39 @@ def test_point_gauge_site_index_known_answers():
     # corner case: coordinate exactly on the upper edge maps to nx
     site = orc.gauge_site_index(np.array([[ll[0] + 104.0, ll[1] + 208.0]]), ll, dx, nxy)
     assert tuple(site[0]) == (104, 104)
+
+
+def _forcing_case(n, lw, ll):
+    """setup_domain_for_test (forcing_mod.f90:341-378): U = (x+y, x, y,
+    x+y-10); forcing_work 10, 5, 1, -1 on STG, UH, VH, ELV."""
+    nx, ny = n
+    x = ll[0] + (np.arange(1, nx + 1) - 0.5) * lw[0] / nx
+    y = ll[1] + (np.arange(1, ny + 1) - 0.5) * lw[1] / ny
+    X, Y = np.meshgrid(x, y)
+    U = np.stack([X + Y, X, Y, X + Y - 10.0])
+    W = np.stack([np.full_like(X, v) for v in (10.0, 5.0, 1.0, -1.0)])
+    return U, W
+
+
+@pytest.mark.parametrize("dom", [((50, 30), (50.0, 30.0), (0.0, 0.0)), ((23, 90), (10.0, 10.0), (1.0, 1.0))])
+def test_forcing_known_answers(dom):
+    """test_forcing_mod (forcing_mod.f90:387-562): the fraction of
+    forcing_work added for a step (time - dt, time) against the forcing
+    interval, to spacing(10)*10."""
+    from oracle.oracle import add_forcing_work_to_U_over_time as add
+    U0, W = _forcing_case(*dom)
+    tol = np.spacing(10.0) * 10
+    cases = [((0.0, 10.0), 1.0), ((4.0, 10.0), 1.0), ((-4.0, 10.0), 10.0 / 14.0), ((-15.0, 15.0), 10.0 / 30.0),
+             ((-15.0, 5.0), 5.0 / 20.0), ((-15.0, -5.0), 0.0)]
+    for (st, en), frac in cases:
+        U = U0.copy()
+        add(U, W, 10.0, 10.0, st, en)
+        err = np.max(np.abs(U - (U0 + W * frac)))
+        assert err < tol if frac else err == 0.0, (st, en, err)
+    # Test 7: stepping through the whole interval adds the whole forcing.
+    U = U0.copy()
+    t, dt = -10.01242, 1.4444
+    for _ in range(30):
+        add(U, W, t, dt, -1.332, 5.15430)
+        t = t + dt
+    assert np.max(np.abs(U - (U0 + W))) < tol
