@@ -359,6 +359,21 @@ int swals_gpu_forcing_clear(swals_domain *d);
  * at domain%time, outside a step. */
 int swals_gpu_apply_forcing(swals_domain *d, double dt);
 
+/* ---- REAL4 output staging ------------------------------------------------
+ * What SWALS's netCDF writers store, converted to REAL4 (round to nearest)
+ * on the device and copied to host_out in one transfer; the call returns
+ * when host_out is filled.
+ * Grids (write_grids, util/netcdf_util_mod.f90:437-510; static max_stage,
+ * :store_static_variable): the variables of var_mask (1 STG, 2 UH, 4 VH,
+ * 8 ELV, 16 max_stage), each U(start:nx:stride, start:ny:stride) with
+ * start = stride/2 + 1, x fastest, one after another; count_xy receives the
+ * strided extents. */
+int swals_gpu_stage_grids_real4(swals_domain *d, int32_t var_mask, int32_t spatial_stride, float *host_out,
+                                int64_t capacity_floats, int32_t *count_xy);
+/* Gauges (point_gauge_mod.f90:411-638): the recorded STG, UH and VH series
+ * as three (station, time) blocks, station fastest. */
+int swals_gpu_gauges_read_real4(swals_domain *d, float *out, int32_t max_records, int32_t *n_records);
+
 /* volume_in_priority_domain (domain_mod.f90:1851-1889): volume_interior over
  * the cells the priority mask keeps (all cells without a mask). */
 int swals_gpu_volume_in_priority_domain(swals_domain *d, double *out);

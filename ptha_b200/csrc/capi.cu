@@ -511,6 +511,7 @@ int swals_gpu_domain_destroy(swals_domain *d)
     if (!d) return SWALS_OK;
     cudaStreamSynchronize(d->stream);
     free_forcing(d);
+    if (d->stage_buf) cudaFree(d->stage_buf);
     for (auto &p : d->pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
     for (auto e : d->ev_pool) cudaEventDestroy(e);
     if (d->d_sites) cudaFree(d->d_sites);

@@ -58,6 +58,9 @@ struct swals_domain {
     // Forcing patches (forcing_mod.f90), device buffers owned here;
     // cfg.forcing points at this vector's data.
     std::vector<swals::ForcingPatch> forcing;
+    // REAL4 output staging buffer (floats), allocated on first use.
+    float *stage_buf = nullptr;
+    size_t stage_cap = 0;
     // Replayed graph of a few steps for evolve_steps.
     cudaGraphExec_t step_graph = nullptr;
     double graph_dt = 0.0;

@@ -233,6 +233,35 @@ class Domain:
         """domain%apply_forcing(dt) on the current state at domain%time."""
         check(self._L.swals_gpu_apply_forcing(self._h, float(dt)))
 
+    GRID_VARS = {"stage": 1, "uh": 2, "vh": 4, "elevation": 8, "max_stage": 16}
+
+    def stage_grids_real4(self, variables=("stage", "uh", "vh", "elevation"), spatial_stride=1):
+        """The netCDF grid payload in REAL4: {name: (cy, cx) float32}, each
+        U(start:nx:stride, start:ny:stride) with start = stride/2 + 1."""
+        mask = 0
+        for v in variables:
+            mask |= self.GRID_VARS[v]
+        st = spatial_stride // 2
+        cx = (self.nx[0] - 1 - st) // spatial_stride + 1
+        cy = (self.nx[1] - 1 - st) // spatial_stride + 1
+        order = [v for v in self.GRID_VARS if v in variables]
+        out = np.empty((len(order), cy, cx), dtype=np.float32)
+        cnt = (ctypes.c_int32 * 2)()
+        check(self._L.swals_gpu_stage_grids_real4(self._h, mask, int(spatial_stride), _p(out), out.size, cnt))
+        assert (cnt[0], cnt[1]) == (cx, cy)
+        return {v: out[k] for k, v in enumerate(order)}
+
+    def gauges_read_real4(self):
+        """Recorded gauge series in REAL4: (3, n_records, n_gauges) for STG,
+        UH, VH (station fastest, as the netCDF variables)."""
+        n = self._n_gauges
+        cap = self._gauge_capacity
+        out = np.empty((3, cap, n), dtype=np.float32)
+        nrec = ctypes.c_int32()
+        check(self._L.swals_gpu_gauges_read_real4(self._h, _p(out), cap, ctypes.byref(nrec)))
+        flat = out.reshape(-1)[:3 * nrec.value * n]
+        return flat.reshape(3, nrec.value, n).copy()
+
     def volume_in_priority_domain(self):
         """volume_interior over the cells set_priority_mask kept."""
         return self._scalar(self._L.swals_gpu_volume_in_priority_domain)
