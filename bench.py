@@ -373,7 +373,7 @@ def _dipoles(lon, lat, count, seed, band=((150.0, -40.0), (190.0, -10.0)), width
     return out
 
 
-def run_form(args, local):
+def run_form(args, local, world=1, rank=0):
     import numpy as np
     import torch
     torch.cuda.set_device(local)
@@ -417,8 +417,15 @@ def run_form(args, local):
         # Coriolis on, fixed CFL-0.7 step: one batched launch per step
         # against the same instances stepped one domain at a time.
         from ptha_b200.batch import Batch
+        from ptha_b200.sharding import gather_instance_series, instance_range
+        dist = None
+        if world > 1:
+            import datetime
+            import torch.distributed as dist
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         nxg, nyg = (3600, 2400) if args.n == N else (args.n * 3 // 2, args.n)
         B = args.batch
+        first_inst, count = instance_range(B, world, rank)
         dl = 1.0 / 60.0 * (3600 / nxg)
         gkw, U0 = workloads.spherical_patch(nx=nxg, ny=nyg, dlon=dl, ll=(140.0, -45.0), seed=3)
         grid = Domain(**gkw, timestepping_method="linear", real_bytes=4, device=local)
@@ -427,15 +434,16 @@ def run_form(args, local):
         lon = gkw["lower_left"][0] + (np.arange(nxg) + 0.5) * dl
         lat = gkw["lower_left"][1] + (np.arange(nyg) + 0.5) * dl
         wet = U0[3] < 0
-        b = Batch(grid, B)
+        b = Batch(grid, count)
         chunk = 8
         first_eta = None
+        # instance q's initial condition depends on q only, not on the ranks
         rng_seeds = np.random.default_rng(4).integers(0, 2 ** 31, size=B)
-        for q0 in range(0, B, chunk):
-            cnt = min(chunk, B - q0)
+        for q0 in range(0, count, chunk):
+            cnt = min(chunk, count - q0)
             U3 = np.zeros((cnt, 3, nyg, nxg), np.float32)
             for t in range(cnt):
-                eta = _dipoles(lon, lat, 1, seed=int(rng_seeds[q0 + t]))[0]
+                eta = _dipoles(lon, lat, 1, seed=int(rng_seeds[first_inst + q0 + t]))[0]
                 U3[t, 0] = np.where(wet, eta, 0.0)
                 if first_eta is None:
                     first_eta = U3[t, 0].copy()
@@ -444,10 +452,30 @@ def run_form(args, local):
         cfg, _ = b.tune()
         stream = torch.cuda.ExternalStream(grid.stream(), device=f"cuda:{local}")
         inner = args.inner if args.inner != INNER else 50
+        # 200 gauges at random wet cells (seed 5), sampled every step
+        gr = np.random.default_rng(5)
+        wj, wi = np.nonzero(wet)
+        pick = gr.choice(wj.size, size=200, replace=False)
+        gxy = np.stack([lon[wi[pick]], lat[wj[pick]]], axis=1)
+        b.gauges_setup(gxy, capacity=inner * (args.steps + 1))
         b.evolve(inner, dt)
         torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
         ms_b = _event_ms(stream, lambda: [b.evolve(inner, dt) for _ in range(args.steps)])
+        if dist is not None:
+            t = torch.tensor([ms_b], dtype=torch.float64, device=f"cuda:{local}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms_b = float(t.item())
         v_batched = nxg * nyg * B * inner * args.steps / (ms_b / 1e3)
+        series = gather_instance_series(b.gauges_read(), B, world, rank) if dist is not None else b.gauges_read()
+        if dist is not None and rank != 0:
+            b.close()
+            grid.close()
+            dist.barrier()
+            dist.destroy_process_group()
+            return
         # Per-instance loop: each instance as its own domain step loop.
         single = Domain(**gkw, timestepping_method="linear", real_bytes=4, device=local)
         U = U0.astype(np.float32).copy()
@@ -460,9 +488,12 @@ def run_form(args, local):
         v_loop = nxg * nyg * inner * args.steps / (ms_s / 1e3)
         bytes_cell = 32.0 + 4.0 / B
         line.update({"workload": f"batched_linear_spherical_{nxg}x{nyg}_B{B}_fp32", "value": v_batched,
-                     "steps": args.steps, "ms_per_step": ms_b / args.steps, "dtype": "f32",
+                     "steps": args.steps, "ms_per_step": ms_b / args.steps, "dtype": "f32", "n_gpus": world,
+                     "scaling": "strong",
                      "config": {"workload": f"batched_linear_spherical_{nxg}x{nyg}_B{B}_fp32", "batch": B,
-                                "timesteps_per_step": inner, "dt": dt, "coriolis": True, "tile_config": cfg},
+                                "timesteps_per_step": inner, "dt": dt, "coriolis": True, "tile_config": cfg,
+                                "gauges": 200, "parallelism": f"instances sharded x{world}"},
+                     "gauge_series_gathered": list(series.shape),
                      "per_instance_loop": {"value": v_loop, "ms_per_step_one_instance": ms_s / args.steps},
                      "speedup_vs_loop": v_batched / v_loop,
                      "roofline": {"bound": "hbm", "kernel": "linear_step_kernel (batched)",
@@ -472,6 +503,9 @@ def run_form(args, local):
         b.close()
         single.close()
         grid.close()
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
     elif args.workload == "adjoint":
         # Spherical 1200x800 (2 arcmin) FP64, 30 gauges, a hidden dipole's
         # waveforms as the target, 2 h simulated, checkpoint every 50 steps.
@@ -656,6 +690,9 @@ def main():
     world, rank, local = dist_setup(args.gpus)
     if args.impl == "reference":
         run_reference(args, world, rank)
+        return
+    if args.workload == "batched" and world > 1:
+        run_form(args, local, world, rank)   # instances sharded over the ranks
         return
     if args.workload != "rk2":
         if rank == 0:
