@@ -348,7 +348,8 @@ int swals_gpu_domain_statistics(swals_domain *d, swals_domain_stats *out);
  * update of the leapfrog solvers (domain_mod.f90:1564-1582,
  * linear_solver_include.f90:123).  Elevation forcing follows
  * support_elevation_forcing: 'euler' and the leapfrog solvers only.
- * Leapfrog patches keep exterior_cells_width + 1 cells from the edges.
+ * Leapfrog patches stay off the boundary ring (and, when they force UH or
+ * VH, keep exterior_cells_width + 1 cells from the edges).
  * Adding or clearing patches drops a captured evolve_steps graph; capture
  * multidomain graphs after the patches are in place. */
 int swals_gpu_forcing_patch_add(swals_domain *d, int32_t i0, int32_t i1, int32_t j0, int32_t j1, int32_t k0,

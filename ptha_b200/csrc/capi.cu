@@ -844,14 +844,19 @@ int swals_gpu_forcing_patch_add(swals_domain *d, int32_t i0, int32_t i1, int32_t
                                            "(elevation in the backed-up state), which this GPU path does not implement",
                     d->desc.timestepping_method);
     if (is_staggered(d->method)) {
-        const int m = d->desc.exterior_cells_width + 2;
+        // The leapfrog applies patches after its step kernel, so a patch
+        // must stay clear of what that kernel used before the forcing: the
+        // boundary ring, the boundary-flux lines when it forces momenta, and
+        // a Flather ring's neighbours.
+        const bool momenta = (k0 <= 3 && k1 >= 2);
+        int m = 2;
+        if (momenta) m = d->desc.exterior_cells_width + 2;
+        if (d->cfg.bc_kind == SWALS_BC_FLATHER && m < 3) m = 3;
         if (i0 < m || j0 < m || i1 > d->nx - m + 1 || j1 > d->ny - m + 1)
-            return fail(SWALS_ERR_UNSUPPORTED, "leapfrog forcing patches must keep exterior_cells_width + 1 cells "
-                                               "from the domain edges (i, j in %d..%d, %d..%d)",
-                        m, d->nx - m + 1, m, d->ny - m + 1);
-        if (d->method == M_LF_LIN_NLFRIC && !d->desc.linear_solver_is_truely_linear)
-            return fail(SWALS_ERR_UNSUPPORTED, "forcing patches with the not truely linear "
-                                               "leapfrog_linear_plus_nonlinear_friction are not implemented");
+            return fail(SWALS_ERR_UNSUPPORTED, "this leapfrog forcing patch must lie in i, j = %d..%d, %d..%d (clear "
+                                               "of the boundary ring%s)",
+                        m, d->nx - m + 1, m, d->ny - m + 1,
+                        momenta ? " and the boundary-flux lines" : "");
     }
     const int ni = i1 - i0 + 1, nj = j1 - j0 + 1, nk = k1 - k0 + 1;
     const size_t n = (size_t)ni * nj * nk, es = esize(d);

@@ -860,12 +860,15 @@ __global__ void __launch_bounds__(256) linear_box_fix_kernel(const LinArgs<R> a,
 // depth is from msl_linear when truely linear (done once), else from the
 // stage after the stage sweep and the boundary (every step; the ring stage
 // of a stage boundary is already in stg_o).
+// With from_out the stage is read from stg_o (final, after a forcing) over
+// the sub-box [i_lo, i_hi] x [r_lo, r_hi] only.
 template <typename R, bool CHEZY>
-__global__ void __launch_bounds__(256) friction_work_kernel(const LinArgs<R> a, const R *nsq, R *fw, int truely_linear)
+__global__ void __launch_bounds__(256) friction_work_kernel(const LinArgs<R> a, const R *nsq, R *fw, int truely_linear,
+                                                            int from_out, int i_lo, int i_hi, int r_lo, int r_hi)
 {
     const int nx = a.p.nx, ny = a.p.ny;
-    const int i = blockIdx.x * 32 + threadIdx.x, r = blockIdx.y * 8 + threadIdx.y;
-    if (i >= nx || r >= ny) return;
+    const int i = i_lo + blockIdx.x * 32 + threadIdx.x, r = r_lo + blockIdx.y * 8 + threadIdx.y;
+    if (i > i_hi || r > r_hi) return;
     const int64_t P = a.p.pitch;
     const int ip1 = min(i + 1, nx - 1), jp1 = min(r + 1, ny - 1);
     const int64_t o = (int64_t)r * P + i, oe = (int64_t)r * P + ip1, on = (int64_t)jp1 * P + i;
@@ -877,6 +880,7 @@ __global__ void __launch_bounds__(256) friction_work_kernel(const LinArgs<R> a, 
         depth_jph = half * (((a.msl - e0) + a.msl) - e_n);
     } else {
         auto stage = [&](int ii, int rr) -> R {
+            if (from_out) return a.p.stg_o[(int64_t)rr * P + ii];
             if (a.bc_stage && on_bc_ring(ii, rr, nx, ny, a.bext) &&
                 !((ii >= a.xl + 1) && (ii <= a.xu - 1) && (rr >= a.yl + 1) && (rr <= a.yu - 1)))
                 return a.p.stg_o[(int64_t)rr * P + ii];
@@ -1151,8 +1155,12 @@ void launch_friction_work(LinArgs<R> &a, const StepPlanes<R> &p, const StepConfi
     if (c.truely_linear && c.fw_ready) return;
     hook(CAT_LINEAR_EDGE, 0);
     dim3 block(32, 8), grid((p.nx + 31) / 32, (p.ny + 7) / 8);
-    if (c.chezy) friction_work_kernel<R, true><<<grid, block, 0, s>>>(a, p.manning_sq, (R *)c.fw, c.truely_linear);
-    else friction_work_kernel<R, false><<<grid, block, 0, s>>>(a, p.manning_sq, (R *)c.fw, c.truely_linear);
+    if (c.chezy)
+        friction_work_kernel<R, true><<<grid, block, 0, s>>>(a, p.manning_sq, (R *)c.fw, c.truely_linear, 0, 0,
+                                                             p.nx - 1, 0, p.ny - 1);
+    else
+        friction_work_kernel<R, false><<<grid, block, 0, s>>>(a, p.manning_sq, (R *)c.fw, c.truely_linear, 0, 0,
+                                                              p.nx - 1, 0, p.ny - 1);
     hook(CAT_LINEAR_EDGE, 1);
 }
 
@@ -1161,8 +1169,9 @@ void launch_friction_work(LinArgs<R> &a, const StepPlanes<R> &p, const StepConfi
 // added to the new stage and to the old momenta and elevation (in place:
 // the step kernel has read them), max_stage is redone over the patches, and
 // the momentum of every cell within one cell of a patch is recomputed.
-// Patches keep n_ext + 1 cells from the edges (checked when added), clear of
-// the boundary ring and of the boundary-flux lines.
+// Patches stay off the boundary ring, and patches that force momenta keep
+// n_ext + 1 cells from the edges, clear of the boundary-flux lines (checked
+// when added).
 template <typename R>
 void launch_leapfrog_forcing(const LinArgs<R> &a, const StepPlanes<R> &p, const StepConfig &c, const DevScalars *sc,
                              cudaStream_t s, const LaunchHook &hook)
@@ -1185,6 +1194,21 @@ void launch_leapfrog_forcing(const LinArgs<R> &a, const StepPlanes<R> &p, const 
         else if (!cor && tl) linear_box_fix_kernel<R, false, true><<<blocks, 256, 0, s>>>(a, i0, i1, r0, r1);
         else linear_box_fix_kernel<R, false, false><<<blocks, 256, 0, s>>>(a, i0, i1, r0, r1);
         hook(CAT_LINEAR_EDGE, 1);
+        if (c.fw && !c.truely_linear) {
+            // precompute_friction_work runs after apply_forcing: redo it where
+            // the forced stage enters (the patch widened by one cell west and
+            // south)
+            const int fi0 = max(f.i0 - 1, 0), fr0 = max(f.j0 - 1, 0);
+            dim3 block(32, 8), grid((f.i1 - fi0 + 32) / 32, (f.j1 - fr0 + 8) / 8);
+            hook(CAT_LINEAR_EDGE, 0);
+            if (c.chezy)
+                friction_work_kernel<R, true><<<grid, block, 0, s>>>(a, p.manning_sq, (R *)c.fw, 0, 1, fi0, f.i1, fr0,
+                                                                     f.j1);
+            else
+                friction_work_kernel<R, false><<<grid, block, 0, s>>>(a, p.manning_sq, (R *)c.fw, 0, 1, fi0, f.i1, fr0,
+                                                                      f.j1);
+            hook(CAT_LINEAR_EDGE, 1);
+        }
     }
 }
 

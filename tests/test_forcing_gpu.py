@@ -99,7 +99,8 @@ def test_fv_rise_time_source(method, adaptive):
 
 @pytest.mark.parametrize("method,truely_linear,coriolis", [
     ("linear", True, False), ("linear", False, False), ("linear", True, True),
-    ("leapfrog_linear_plus_nonlinear_friction", True, True)])
+    ("leapfrog_linear_plus_nonlinear_friction", True, True),
+    ("leapfrog_linear_plus_nonlinear_friction", False, False)])
 @pytest.mark.parametrize("kernel", ["tile", "async"])
 def test_leapfrog_rise_time_source(method, truely_linear, coriolis, kernel, monkeypatch):
     monkeypatch.setenv("SWALS_LINEAR_KERNEL", kernel)
@@ -162,6 +163,6 @@ def test_forcing_patch_checks():
     d.close()
     lin = Domain((40, 40), (40.0, 40.0), (0.0, 0.0), "linear")
     with pytest.raises(_lib.SwalsError) as e:
-        lin.add_forcing_patch(2, 6, 10, 14, 1, 1, 0.0, 1.0, w[:1])  # too close to the edge for the leapfrog
+        lin.add_forcing_patch(1, 5, 10, 14, 1, 1, 0.0, 1.0, w[:1])  # on the boundary ring
     assert e.value.code == 3
     lin.close()
