@@ -72,6 +72,7 @@ class _OracleDomainC(ctypes.Structure):
         ("nest_nbox", ctypes.c_int32), ("friction_work_is_setup", ctypes.c_int32), ("nest_boxes", ctypes.c_void_p),
         ("nest_offset", ctypes.c_void_p), ("nest_integral", ctypes.c_void_p), ("friction_work", ctypes.c_void_p),
         ("n_forcing", ctypes.c_int32), ("pad2", ctypes.c_int32), ("forcing", ctypes.c_void_p),
+        ("advection_work", ctypes.c_void_p),
     ]
 
 
@@ -153,6 +154,7 @@ class OracleDomain:
         self.es_jm1 = np.zeros((ny + 1, nx), np.float64)
         self.backup_U = np.zeros((3, ny, nx), dt)
         self.friction_work = np.zeros((2, ny, nx), dt)
+        self.advection_work = np.zeros((5, ny, nx), dt)
         for name, arr in [("U", self.U), ("max_stage", self.max_stage), ("manning_squared", self.manning_squared),
                           ("x", self.x), ("y", self.y), ("dxb", self.dxb), ("dyl", self.dyl), ("area", self.area),
                           ("coriolis_c", self.coriolis_c), ("coriolis_be", self.coriolis_be),
@@ -160,7 +162,7 @@ class OracleDomain:
                           ("flux_NS", self.flux_NS), ("flux_EW", self.flux_EW),
                           ("explicit_source", self.explicit_source),
                           ("explicit_source_VH_j_minus_1", self.es_jm1), ("backup_U", self.backup_U),
-                          ("friction_work", self.friction_work)]:
+                          ("friction_work", self.friction_work), ("advection_work", self.advection_work)]:
             setattr(c, name, _ptr(arr))
         self._fn("apply_method_defaults")(ctypes.byref(c))
         self._fn("setup_geometry")(ctypes.byref(c))

@@ -754,6 +754,243 @@ static void linear_leapfrog_step(oracle_domain *d, REAL dt)
 }
 
 /* ------------------------------------------------------------------------ */
+/* one_leapfrog_nonlinear_step (domain_mod_leapfrog_nonlinear_include.f90,
+ * timestepping_alternatives_include.f90:439-447) in serial order: the stage
+ * sweep, boundary and forcing as for the linear leapfrog, then upwind
+ * advection fluxes of UH and VH from a lagged depth, the momentum update
+ * with nonlinear pressure gradient, Coriolis, spherical metric terms and
+ * semi-implicit friction, and the dry-cell outflow limiter.  The whole
+ * domain is updated (the reference fixes xL = 1, xU = nx, yL = 1, yU = ny). */
+static void leapfrog_nonlinear_step(oracle_domain *d, REAL dt)
+{
+    const int nx = d->nx, ny = d->ny;
+    const size_t plane = (size_t)nx * (size_t)ny;
+    const REAL mad = MINIMUM_ALLOWED_DEPTH;
+#define AW(k, i, j) d->advection_work[(size_t)((k) - 1) * plane + IDX(i, j)]
+#define FNSX(i, j, k) d->flux_NS[(size_t)((k) - 1) * (size_t)nx * (size_t)(ny + 1) + (size_t)((i) - 1) + (size_t)((j) - 1) * (size_t)nx]
+#define FEWX(i, j, k) d->flux_EW[(size_t)((k) - 1) * (size_t)(nx + 1) * (size_t)ny + (size_t)((i) - 1) + (size_t)((j) - 1) * (size_t)(nx + 1)]
+    enum { DEPTH_LAG = 1, UUH = 2, UVH = 3, VUH = 4, VVH = 5 };
+    d->dt_last_update = dt;
+    for (int j = 1; j <= ny; j++)
+        for (int i = 1; i <= nx; i++) {
+            AW(DEPTH_LAG, i, j) = rmax(UU(OR_STG, i, j) - UU(OR_ELV, i, j), ZERO);
+            for (int k = UUH; k <= VVH; k++) AW(k, i, j) = ZERO;
+        }
+    for (size_t q = 0; q < (size_t)nx * (ny + 1) * 3; q++) d->flux_NS[q] = ZERO;
+    for (size_t q = 0; q < (size_t)(nx + 1) * ny * 3; q++) d->flux_EW[q] = ZERO;
+    if (d->nest_nbox > 0)
+        nest_flux_tstep(d, (double)dt, d->U + 2 * plane, ny, plane, 2, d->U + plane, nx, plane, 2, 1, 1, 0);
+
+    /* stage */
+    for (int j = 2; j <= ny - 1; j++) {
+        REAL inv_cell_area_dt = dt / d->area[j - 1];
+        for (int i = 2; i <= nx - 1; i++) {
+            REAL a = (UU(OR_UH, i, j) - UU(OR_UH, i - 1, j)) * d->dyl[i - 1];
+            REAL b = UU(OR_VH, i, j) * d->dxb[j] - UU(OR_VH, i, j - 1) * d->dxb[j - 1];
+            UU(OR_STG, i, j) = UU(OR_STG, i, j) - inv_cell_area_dt * (a + b);
+        }
+    }
+    d->time = d->time + (double)(dt * HALF);
+    update_boundary(d);
+    apply_forcing(d, dt);
+    {
+        int n_ext = d->exterior_cells_width;
+        REAL s;
+        s = ZERO; for (int i = n_ext + 1; i <= nx - n_ext; i++) s += UU(OR_VH, i, ny - n_ext);
+        d->boundary_flux_store[0] = (double)(s * d->dxb[ny - n_ext]);
+        s = ZERO; for (int j = 1 + n_ext; j <= ny - n_ext; j++) s += UU(OR_UH, nx - n_ext, j);
+        d->boundary_flux_store[1] = (double)(s * d->dyl[nx - n_ext]);
+        s = ZERO; for (int i = n_ext + 1; i <= nx - n_ext; i++) s += UU(OR_VH, i, n_ext);
+        d->boundary_flux_store[2] = (double)(-(s * d->dxb[n_ext]));
+        s = ZERO; for (int j = 1 + n_ext; j <= ny - n_ext; j++) s += UU(OR_UH, n_ext, j);
+        d->boundary_flux_store[3] = (double)(-(s * d->dyl[n_ext]));
+        double tot = 0.0;
+        for (int k = 0; k < 4; k++) tot += d->boundary_flux_store[k];
+        d->boundary_flux_evolve_integral = tot * (double)dt;
+    }
+    precompute_friction_work(d, 0);
+
+    /* lagged depth, advection terms (:227-333) */
+    for (int j = 1; j <= ny - 1; j++)
+        for (int i = 1; i <= nx; i++)
+            AW(DEPTH_LAG, i, j) = HALF * (AW(DEPTH_LAG, i, j) + rmax(UU(OR_STG, i, j) - UU(OR_ELV, i, j), ZERO));
+    for (int j = 1; j <= ny - 1; j++) {
+        int jm1 = (j - 1 > 1) ? j - 1 : 1;
+        for (int i = 1; i <= nx - 1; i++) {
+            REAL depth_local = HALF * (AW(DEPTH_LAG, i, j) + AW(DEPTH_LAG, i + 1, j));
+            REAL inv_depth_local = (depth_local > mad) ? ONE / depth_local : ZERO;
+            AW(UUH, i, j) = (UU(OR_UH, i, j) * UU(OR_UH, i, j)) * inv_depth_local;
+            if (i < nx - 1)
+                AW(UVH, i, j) = UU(OR_UH, i, j) * inv_depth_local * (REAL)0.25 *
+                                (UU(OR_VH, i, jm1) + UU(OR_VH, i + 1, jm1) + UU(OR_VH, i, j) + UU(OR_VH, i + 1, j));
+        }
+        AW(UUH, nx, j) = AW(UUH, nx - 1, j);
+        AW(UVH, nx, j) = AW(UVH, nx - 2, j);
+        AW(UVH, nx - 1, j) = AW(UVH, nx - 2, j);
+    }
+    for (int i = 1; i <= nx; i++) {
+        AW(UUH, i, ny) = AW(UUH, i, ny - 1);
+        AW(UVH, i, ny) = AW(UVH, i, ny - 1);
+    }
+    for (int j = 1; j <= ny - 1; j++) {
+        for (int i = 1; i <= nx; i++) {
+            REAL depth_local = HALF * (AW(DEPTH_LAG, i, j) + AW(DEPTH_LAG, i, j + 1));
+            REAL inv_depth_local = (depth_local > mad) ? ONE / depth_local : ZERO;
+            AW(VVH, i, j) = UU(OR_VH, i, j) * UU(OR_VH, i, j) * inv_depth_local;
+            if (i > 1 && j < ny - 1)
+                AW(VUH, i, j) = UU(OR_VH, i, j) * inv_depth_local * (REAL)0.25 *
+                                (UU(OR_UH, i - 1, j) + UU(OR_UH, i, j) + UU(OR_UH, i - 1, j + 1) + UU(OR_UH, i, j + 1));
+        }
+        AW(VUH, 1, j) = AW(VUH, 2, j);
+    }
+    for (int i = 1; i <= nx; i++) {
+        AW(VVH, i, ny) = AW(VVH, i, ny - 1);
+        AW(VUH, i, ny) = AW(VUH, i, ny - 2);
+        AW(VUH, i, ny - 1) = AW(VUH, i, ny - 2);
+    }
+#define WETC(i, j) (UU(OR_STG, i, j) > UU(OR_ELV, i, j) + mad)
+    /* upwind fluxes (:340-498) */
+    for (int j = 1; j <= ny - 1; j++) {
+        for (int i = 2; i <= nx - 1; i++) {
+            REAL s = UU(OR_UH, i, j) + UU(OR_UH, i - 1, j);
+            FEWX(i, j, 2) = d->dyl[i - 1] * ((s > ZERO) ? AW(UUH, i - 1, j) : AW(UUH, i, j));
+        }
+        FEWX(1, j, 2) = AW(UUH, 1, j) * d->dyl[0];
+        FEWX(nx, j, 2) = AW(UUH, nx, j) * d->dyl[nx - 1];
+        for (int i = 2; i <= nx - 1; i++)
+            if ((UU(OR_UH, i, j) + UU(OR_UH, i - 1, j)) == ZERO)
+                FEWX(i, j, 2) = d->dyl[i - 1] * HALF * (AW(UUH, i - 1, j) + AW(UUH, i, j));
+        for (int i = 1; i <= nx; i++)
+            if (!WETC(i, j)) FEWX(i, j, 2) = ZERO;
+    }
+    for (int e = 1; e <= ny; e++) {   /* NS flux of UH on edge e: rows jl = max(e-1,1), ju = e */
+        const int jl = (e - 1 > 1) ? e - 1 : 1, ju = e;
+        for (int i = 1; i <= nx - 1; i++) {
+            REAL s = UU(OR_VH, i, jl) + UU(OR_VH, i + 1, jl);
+            REAL f = d->dxb[e - 1] * ((s > ZERO) ? AW(UVH, i, jl) : AW(UVH, i, ju));
+            if (s == ZERO) f = d->dxb[e - 1] * HALF * (AW(UVH, i, jl) + AW(UVH, i, ju));
+            if (!(WETC(i, ju) && WETC(i + 1, ju) && WETC(i, jl) && WETC(i + 1, jl))) f = ZERO;
+            FNSX(i, e, 2) = f;
+        }
+    }
+    for (int j = 1; j <= ny; j++) {   /* NS flux of VH at the bottom edge of row j */
+        const int jm1 = (j - 1 > 1) ? j - 1 : 1;
+        const REAL w = HALF * (d->dxb[j - 1] + d->dxb[j]);
+        for (int i = 1; i <= nx - 1; i++) {
+            REAL s = UU(OR_VH, i, j) + UU(OR_VH, i, jm1);
+            REAL f = w * ((s > ZERO) ? AW(VVH, i, jm1) : AW(VVH, i, j));
+            if (s == ZERO) f = w * HALF * (AW(VVH, i, jm1) + AW(VVH, i, j));
+            if (!WETC(i, j)) f = ZERO;
+            FNSX(i, j, 3) = f;
+        }
+    }
+    for (int j = 1; j <= ny - 1; j++) {   /* EW flux of VH */
+        for (int i = 2; i <= nx; i++) {
+            REAL s = UU(OR_UH, i - 1, j) + UU(OR_UH, i - 1, j + 1);
+            FEWX(i, j, 3) = d->dyl[i - 2] * ((s > ZERO) ? AW(VUH, i - 1, j) : AW(VUH, i, j));
+        }
+        FEWX(1, j, 3) = FEWX(2, j, 3);
+        for (int i = 2; i <= nx; i++) {
+            if ((UU(OR_UH, i - 1, j) + UU(OR_UH, i - 1, j + 1)) == ZERO)
+                FEWX(i, j, 3) = d->dyl[i - 2] * HALF * (AW(VUH, i - 1, j) + AW(VUH, i, j));
+            if (!(WETC(i - 1, j) && WETC(i, j) && WETC(i - 1, j + 1) && WETC(i, j + 1))) FEWX(i, j, 3) = ZERO;
+        }
+    }
+
+    /* momentum (:576-853), from the old momenta */
+    REAL *uh_old = (REAL *)malloc(plane * sizeof(REAL));
+    REAL *vh_old = (REAL *)malloc(plane * sizeof(REAL));
+    memcpy(uh_old, &UU(OR_UH, 1, 1), plane * sizeof(REAL));
+    memcpy(vh_old, &UU(OR_VH, 1, 1), plane * sizeof(REAL));
+    const REAL lf = dt * (REAL)d->linear_friction_coeff;
+    for (int j = 1; j <= ny - 1; j++) {
+        const REAL inv_cell_area_dt = dt / d->area[j - 1];
+        const REAL inv_cell_area_dt_g = GRAVITY * inv_cell_area_dt;
+        const REAL inv_cell_area_dt_vh = dt / (HALF * (d->area[j - 1] + d->area[j]));
+        const REAL inv_cell_area_dt_vh_g = GRAVITY * inv_cell_area_dt_vh;
+        const int jm = (j > 1) ? j - 1 : 1;
+        for (int i = 1; i <= nx - 1; i++) {
+            REAL h_jph = HALF * ((UU(OR_STG, i, j + 1) + UU(OR_STG, i, j)) - (UU(OR_ELV, i, j + 1) + UU(OR_ELV, i, j)));
+            if (h_jph < mad) h_jph = ZERO;
+            REAL h_iph = HALF * ((UU(OR_STG, i + 1, j) + UU(OR_STG, i, j)) - (UU(OR_ELV, i + 1, j) + UU(OR_ELV, i, j)));
+            if (h_iph < mad) h_iph = ZERO;
+            const int jw1 = WETC(i, j + 1), jw0 = WETC(i, j);
+            const REAL h_jph_wet_strict = (jw1 && jw0) ? ONE : ZERO;
+            const REAL h_jph_wet = ((h_jph_wet_strict > ZERO) ||
+                                    (jw1 && UU(OR_STG, i, j + 1) > UU(OR_ELV, i, j) + mad) ||
+                                    (jw0 && UU(OR_STG, i, j) > UU(OR_ELV, i, j + 1) + mad)) ? ONE : ZERO;
+            const int iw1 = WETC(i + 1, j), iw0 = WETC(i, j);
+            const REAL h_iph_wet_strict = (iw1 && iw0) ? ONE : ZERO;
+            const REAL h_iph_wet = ((h_iph_wet_strict > ZERO) ||
+                                    (iw1 && UU(OR_STG, i + 1, j) > UU(OR_ELV, i, j) + mad) ||
+                                    (iw0 && UU(OR_STG, i, j) > UU(OR_ELV, i + 1, j) + mad)) ? ONE : ZERO;
+            const REAL vh_iph_jmh = HALF * (vh_old[IDX(i, jm)] + vh_old[IDX(i + 1, jm)]);
+            const REAL vh_iph_jph = HALF * (vh_old[IDX(i, j)] + vh_old[IDX(i + 1, j)]);
+            const int im = (i > 1) ? i - 1 : 1;
+            const REAL uh_i_j = HALF * (uh_old[IDX(i, j)] + uh_old[IDX(im, j)]);
+            const REAL uh_i_jp1 = HALF * (uh_old[IDX(i, j + 1)] + uh_old[IDX(im, j + 1)]);
+            REAL dthc = ZERO, dthc_jph = ZERO, tan_uvh = ZERO, tan_uuh = ZERO;
+            if (d->coriolis) {
+                dthc = dt * d->coriolis_c[j - 1] * HALF * ((h_iph_wet_strict > ZERO) ? ONE : ZERO);
+                dthc_jph = dt * d->coriolis_be[j] * HALF * ((h_jph_wet_strict > ZERO) ? ONE : ZERO);
+            }
+            if (d->spherical) {
+                REAL inv_depth_local = ZERO;
+                if (h_iph_wet_strict > ZERO) inv_depth_local = ONE / h_iph;
+                tan_uvh = dt * d->tanlat_on_R[j - 1] * uh_old[IDX(i, j)] * HALF * (vh_iph_jmh + vh_iph_jph) *
+                          inv_depth_local;
+                inv_depth_local = ZERO;
+                if (h_jph_wet_strict > ZERO) inv_depth_local = ONE / h_jph;
+                tan_uuh = dt * HALF * (d->tanlat_on_R[j - 1] + d->tanlat_on_R[j]) * HALF * (uh_i_jp1 + uh_i_j) * HALF *
+                          (uh_i_jp1 + uh_i_j) * inv_depth_local;
+            }
+            const REAL tv = HALF * (vh_iph_jmh + vh_iph_jph);
+            const REAL tu = HALF * (uh_i_j + uh_i_jp1);
+            const REAL u0 = uh_old[IDX(i, j)], v0 = vh_old[IDX(i, j)];
+            const REAL fm_uh = ONE / ((ONE + lf) + dt * d->friction_work[IDX(i, j)] * (REAL)sqrt(u0 * u0 + tv * tv));
+            const REAL fm_vh = ONE / ((ONE + lf) + dt * d->friction_work[plane + IDX(i, j)] *
+                                                      (REAL)sqrt(v0 * v0 + tu * tu));
+            REAL uh = u0 * h_iph_wet - inv_cell_area_dt_g * h_iph * h_iph_wet *
+                      (UU(OR_STG, i + 1, j) - UU(OR_STG, i, j)) * d->dyl[i];
+            REAL vh = v0 * h_jph_wet - inv_cell_area_dt_vh_g * h_jph * h_jph_wet *
+                      (UU(OR_STG, i, j + 1) - UU(OR_STG, i, j)) * d->dxb[j];
+            uh = uh - inv_cell_area_dt * ADVECTION_BETA * h_iph_wet *
+                          ((FEWX(i + 1, j, 2) - FEWX(i, j, 2)) + (FNSX(i, j + 1, 2) - FNSX(i, j, 2)));
+            vh = vh - inv_cell_area_dt_vh * ADVECTION_BETA * h_jph_wet *
+                          ((FEWX(i + 1, j, 3) - FEWX(i, j, 3)) + (FNSX(i, j + 1, 3) - FNSX(i, j, 3)));
+            if (d->coriolis) {
+                uh = uh + dthc * (vh_iph_jmh + vh_iph_jph);
+                vh = vh - dthc_jph * (uh_i_j + uh_i_jp1);
+            }
+            if (d->spherical) {
+                uh = uh + tan_uvh;
+                vh = vh - tan_uuh;
+            }
+            UU(OR_UH, i, j) = fm_uh * uh;
+            UU(OR_VH, i, j) = fm_vh * vh;
+        }
+    }
+    free(uh_old);
+    free(vh_old);
+    /* dry-cell outflow (:855-880) */
+    for (int j = 1; j <= ny - 1; j++)
+        for (int i = 1; i <= nx; i++) {
+            if (UU(OR_STG, i, j) < UU(OR_ELV, i, j) + mad) {
+                if (UU(OR_UH, i, j) > ZERO) UU(OR_UH, i, j) = ZERO;
+                if (i > 1 && UU(OR_UH, i - 1, j) < ZERO) UU(OR_UH, i - 1, j) = ZERO;
+                if (UU(OR_VH, i, j) > ZERO) UU(OR_VH, i, j) = ZERO;
+            }
+            if (UU(OR_STG, i, j + 1) < UU(OR_ELV, i, j + 1) + mad)
+                if (UU(OR_VH, i, j) < ZERO) UU(OR_VH, i, j) = ZERO;
+        }
+    d->time = d->time + (double)(HALF * dt);
+#undef WETC
+#undef AW
+#undef FNSX
+#undef FEWX
+}
+
+/* ------------------------------------------------------------------------ */
 /* Nonlinear finite-volume pieces */
 
 /* domain_mod.f90:1360-1419 */
@@ -1298,6 +1535,10 @@ int ORACLE_FN(evolve_one_step)(oracle_domain *d, double dt, int has_dt)
     case OR_METHOD_LEAPFROG_LINEAR_PLUS_NONLINEAR_FRICTION:
         if (!has_dt) return 2;
         linear_leapfrog_step(d, (REAL)dt);
+        break;
+    case OR_METHOD_LEAPFROG_NONLINEAR:
+        if (!has_dt) return 2;
+        leapfrog_nonlinear_step(d, (REAL)dt);
         break;
     default: return 3;
     }

@@ -136,6 +136,8 @@ typedef struct oracle_domain {
     int32_t n_forcing;
     int32_t pad2;
     const struct oracle_forcing_patch *forcing;
+    /* leapfrog_nonlinear: advection_work (nx*ny*5: DEPTH_LAG, UUH, UVH, VUH, VVH) */
+    REAL *advection_work;
 } oracle_domain;
 
 /* forcing_patch_type (forcing_mod.f90:23-53) with the default (identity)

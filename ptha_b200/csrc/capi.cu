@@ -258,6 +258,19 @@ int evolve_t(swals_domain *d, double timestep, int has_dt)
         if (e != cudaSuccess) return cuda_fail(e, "linear leapfrog step");
         if (d->cfg.fw) d->cfg.fw_ready = 1;
         d->cur = out;
+    } else if (d->method == M_LF_NONLINEAR) {
+        if (!has_dt)
+            return fail(SWALS_ERR_TIMESTEP_REQUIRED, "ERROR: timestep must be provided for leapfrog_nonlinear "
+                                                     "evolve_one_step");
+        const int in = d->cur, out = (d->cur + 1) % 3;
+        StepPlanes<R> p;
+        p.nx = d->nx; p.ny = d->ny; p.pitch = d->pitch;
+        p.stg = (const R *)d->planes[in][0]; p.uh = (const R *)d->planes[in][1]; p.vh = (const R *)d->planes[in][2];
+        p.stg_o = (R *)d->planes[out][0]; p.uh_o = (R *)d->planes[out][1]; p.vh_o = (R *)d->planes[out][2];
+        p.elv = (R *)d->elv; p.max_stage = max_stage; p.manning_sq = (R *)d->manning_sq;
+        e = launch_leapfrog_nonlinear_step<R>(p, m, c, R(timestep), d->sc, d->stream, hook);
+        if (e != cudaSuccess) return cuda_fail(e, "nonlinear leapfrog step");
+        d->cur = out;
     } else if (d->method == M_RK2 || d->method == M_EULER || d->method == M_MIDPOINT || d->method == M_RK2N) {
         R *pl[3][3];
         for (int b = 0; b < 3; b++)
@@ -342,7 +355,7 @@ int swals_gpu_domain_create(const swals_domain_desc *desc, swals_domain **out)
     if (!parse_method(desc->timestepping_method, &method, &def_cfl, &def_theta))
         return fail(SWALS_ERR_UNKNOWN_METHOD, "timestepping_method: %s not recognized", desc->timestepping_method);
     if (!(method == M_LINEAR || method == M_RK2 || method == M_EULER || method == M_MIDPOINT || method == M_RK2N ||
-          method == M_LF_LIN_NLFRIC))
+          method == M_LF_LIN_NLFRIC || method == M_LF_NONLINEAR))
         return fail(SWALS_ERR_UNSUPPORTED, "timestepping_method '%s' is not implemented on the GPU path",
                     desc->timestepping_method);
     const int nx = desc->nx[0], ny = desc->nx[1];
@@ -360,6 +373,8 @@ int swals_gpu_domain_create(const swals_domain_desc *desc, swals_domain **out)
         return fail(SWALS_ERR_INVALID_ARGUMENT, "unknown boundary_kind %d", desc->boundary_kind);
     if (desc->boundary_function_kind < 0 || desc->boundary_function_kind > 1)
         return fail(SWALS_ERR_UNSUPPORTED_CALLBACK, "unknown boundary_function_kind %d", desc->boundary_function_kind);
+    if (method == M_LF_NONLINEAR && desc->boundary_kind == SWALS_BC_FLATHER)
+        return fail(SWALS_ERR_UNSUPPORTED, "flather_boundary with leapfrog_nonlinear is not implemented");
     if (is_staggered(method) && desc->boundary_kind == SWALS_BC_FLATHER && desc->exterior_cells_width == 1)
         return fail(SWALS_ERR_UNSUPPORTED, "flather_boundary with the linear solver needs exterior_cells_width >= 2");
     if (is_staggered(method) && desc->boundary_kind == SWALS_BC_TRANSMISSIVE)
@@ -437,8 +452,10 @@ int swals_gpu_domain_create(const swals_domain_desc *desc, swals_domain **out)
                                d->method == M_RK2N)
                                   ? al((size_t)swals::rk2_edge_bytes(d->pitch, ny, (int)es)) : 0;
     total += edge_bytes;
-    const size_t fw_bytes = (d->method == M_LF_LIN_NLFRIC) ? 2 * al(plane) : 0;   // friction_work
-    total += fw_bytes;
+    const size_t fw_bytes = (d->method == M_LF_LIN_NLFRIC || d->method == M_LF_NONLINEAR) ? 2 * al(plane) : 0;
+    total += fw_bytes;   // friction_work
+    const size_t nl_bytes = (d->method == M_LF_NONLINEAR) ? 9 * al((size_t)d->pitch * (ny + 1) * es) : 0;
+    total += nl_bytes;   // leapfrog_nonlinear work planes
     e = cudaMalloc(&d->pool, total);
     if (e != cudaSuccess) {
         cudaStreamDestroy(d->stream);
@@ -461,6 +478,7 @@ int swals_gpu_domain_create(const swals_domain_desc *desc, swals_domain **out)
     d->edges = edge_bytes ? (void *)p : nullptr; p += edge_bytes;
     d->cfg.ring = d->side;   // the staggered solver's Flather ring buffer (the side buffer is for FV stages)
     d->cfg.fw = fw_bytes ? (void *)p : nullptr; p += fw_bytes;
+    d->cfg.nl_work = nl_bytes ? (void *)p : nullptr; p += nl_bytes;
     d->cfg.fw_ready = 0;
 
     int rc = SWALS_OK;

@@ -11,10 +11,11 @@ enum Method {
     M_RK2 = 1, M_RK2N, M_MIDPOINT, M_EULER, M_LINEAR, M_LF_LIN_NLFRIC, M_CLIFFS, M_LF_NONLINEAR
 };
 
-// The staggered leapfrog solvers whose step is the linear leapfrog
-// ('linear', 'leapfrog_linear_plus_nonlinear_friction'): nesting treats them
-// alike (staggered grid, mass-only flux correction, U(:,:,UH/VH) fluxes).
-inline bool is_linear_leapfrog(int m) { return m == M_LINEAR || m == M_LF_LIN_NLFRIC; }
+// The staggered leapfrog solvers ('linear',
+// 'leapfrog_linear_plus_nonlinear_friction', 'leapfrog_nonlinear'): nesting
+// treats them alike (staggered grid, mass-only flux correction,
+// U(:,:,UH/VH) fluxes with lower index 2).
+inline bool is_linear_leapfrog(int m) { return m == M_LINEAR || m == M_LF_LIN_NLFRIC || m == M_LF_NONLINEAR; }
 
 // Mirrors the parts of SWALS's domain_type (domain_mod.f90:137-507) the time
 // step touches: geometry, solver options, device planes and scalar state.

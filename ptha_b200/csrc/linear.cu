@@ -1281,6 +1281,327 @@ cudaError_t launch_linear_step(const StepPlanes<R> &p, const Metrics<R> &m, cons
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// leapfrog_nonlinear (domain_mod_leapfrog_nonlinear_include.f90): the linear
+// leapfrog's stage sweep, boundary and forcing, then upwind advection of the
+// momenta from a lagged depth, the momentum update with nonlinear pressure
+// gradient, Coriolis, spherical metric terms and semi-implicit friction, and
+// the dry-cell outflow limiter.  A secondary solver: one kernel per stage of
+// the reference's algorithm, reading the old momenta throughout (the
+// reference's row carries and thread-boundary copies only serve that).
+// Work planes (pitch P): lag0, advection UUH, UVH, VUH, VVH, fluxes
+// EW-UH, NS-UH, NS-VH, EW-VH (ny + 1 rows each).
+namespace nl {
+
+template <typename R> struct NLArgs {
+    LinArgs<R> a;
+    const R *nsq;
+    R *lag0;
+    R *adv[4];      // UUH, UVH, VUH, VVH
+    R *flx[4];      // EW-UH, NS-UH, NS-VH, EW-VH
+    const R *fw;    // friction_work, UH then VH plane
+    int64_t plane;  // elements per work plane
+};
+
+template <typename R>
+__device__ __forceinline__ bool wet(const NLArgs<R> &n, int i, int r)
+{
+    const int64_t o = (int64_t)r * n.a.p.pitch + i;
+    return n.a.p.stg_o[o] > n.a.p.elv[o] + K<R>::min_depth();
+}
+
+// depth at the time of the previous momentum update (:227-230): rows
+// 0..ny-2 average the old and the new depth, the last row keeps the old.
+template <typename R>
+__device__ __forceinline__ R lag(const NLArgs<R> &n, int i, int r)
+{
+    const int64_t o = (int64_t)r * n.a.p.pitch + i;
+    const R d0 = n.lag0[o];
+    if (r > n.a.p.ny - 2) return d0;
+    const R dn = n.a.p.stg_o[o] - n.a.p.elv[o];
+    return K<R>::half() * (d0 + ((R(0) > dn) ? R(0) : dn));
+}
+
+template <typename R>
+__global__ void lag0_kernel(NLArgs<R> n)
+{
+    const int i = blockIdx.x * 32 + threadIdx.x, r = blockIdx.y * 8 + threadIdx.y;
+    if (i >= n.a.p.nx || r >= n.a.p.ny) return;
+    const int64_t o = (int64_t)r * n.a.p.pitch + i;
+    const R dp = n.a.p.stg[o] - n.a.p.elv[o];
+    n.lag0[o] = (R(0) > dp) ? R(0) : dp;   // max(depth, 0)
+}
+
+template <typename R>
+__global__ void stage_kernel(NLArgs<R> n)
+{
+    const LinArgs<R> &a = n.a;
+    const int i = blockIdx.x * 32 + threadIdx.x, r = blockIdx.y * 8 + threadIdx.y;
+    if (i >= a.p.nx || r >= a.p.ny) return;
+    const int64_t o = (int64_t)r * a.p.pitch + i;
+    const bool interior = (i >= 1) && (i <= a.p.nx - 2) && (r >= 1) && (r <= a.p.ny - 2);
+    if (interior) a.p.stg_o[o] = swept_stage(a, i, r);
+    else if (!(a.bc_stage && on_bc_ring(i, r, a.p.nx, a.p.ny, a.bext))) a.p.stg_o[o] = a.p.stg[o];
+}
+
+// The advection terms with the reference's edge extrapolations folded in
+// as index remaps (:236-333).
+template <typename R>
+__global__ void advection_kernel(NLArgs<R> n)
+{
+    const int nx = n.a.p.nx, ny = n.a.p.ny;
+    const int i = blockIdx.x * 32 + threadIdx.x, r = blockIdx.y * 8 + threadIdx.y;
+    if (i >= nx || r >= ny) return;
+    const int64_t P = n.a.p.pitch, o = (int64_t)r * P + i;
+    const R half = K<R>::half(), mad = K<R>::min_depth(), quarter = R(0.25);
+    const R *uh = n.a.p.uh, *vh = n.a.p.vh;
+    auto inv_d = [&](R dl) -> R { return (dl > mad) ? R(1) / dl : R(0); };
+    // UUH, UVH at (i+1/2, j), rows 0..ny-2; the last row copies row ny-2
+    {
+        const int rr = (r <= ny - 2) ? r : ny - 2;
+        const int jm1 = (rr - 1 > 0) ? rr - 1 : 0;
+        const int iu = (i <= nx - 2) ? i : nx - 2;
+        const int64_t ou = (int64_t)rr * P + iu;
+        const R dl = half * (lag(n, iu, rr) + lag(n, iu + 1, rr));
+        n.adv[0][o] = (uh[ou] * uh[ou]) * inv_d(dl);
+        const int iv = (i <= nx - 3) ? i : nx - 3;
+        const int64_t ov = (int64_t)rr * P + iv;
+        const R dv = half * (lag(n, iv, rr) + lag(n, iv + 1, rr));
+        n.adv[1][o] = uh[ov] * inv_d(dv) * quarter *
+                      (vh[(int64_t)jm1 * P + iv] + vh[(int64_t)jm1 * P + iv + 1] + vh[ov] + vh[ov + 1]);
+    }
+    // VVH at (i, j+1/2), rows 0..ny-2; VUH rows 0..ny-3 and columns 1..,
+    // the rest copied from column 1 and row ny-3
+    {
+        const int rr = (r <= ny - 2) ? r : ny - 2;
+        const int64_t ov = (int64_t)rr * P + i;
+        const R dl = half * (lag(n, i, rr) + lag(n, i, rr + 1));
+        n.adv[3][o] = vh[ov] * vh[ov] * inv_d(dl);
+        const int ru = (r <= ny - 3) ? r : ny - 3;
+        const int iu = (i >= 1) ? i : 1;
+        const int64_t ou = (int64_t)ru * P + iu;
+        const R du = half * (lag(n, iu, ru) + lag(n, iu, ru + 1));
+        n.adv[2][o] = vh[ou] * inv_d(du) * quarter * (uh[ou - 1] + uh[ou] + uh[ou - 1 + P] + uh[ou + P]);
+    }
+}
+
+// Upwind fluxes of UH and VH (:340-498).  Flux planes have ny + 1 rows.
+template <typename R>
+__global__ void flux_kernel(NLArgs<R> n)
+{
+    const int nx = n.a.p.nx, ny = n.a.p.ny;
+    const int i = blockIdx.x * 32 + threadIdx.x, r = blockIdx.y * 8 + threadIdx.y;
+    if (i > nx || r > ny) return;
+    const int64_t P = n.a.p.pitch, o = (int64_t)r * P + i;
+    const R half = K<R>::half(), zero = R(0);
+    const R *uh = n.a.p.uh, *vh = n.a.p.vh;
+    const Metrics<R> &m = n.a.m;
+    const R *UUH = n.adv[0], *UVH = n.adv[1], *VUH = n.adv[2], *VVH = n.adv[3];
+    // EW flux of UH at cell centres, rows 0..ny-2
+    if (i < nx) {
+        R f = zero;
+        if (r <= ny - 2) {
+            if (i == 0) f = UUH[o] * m.dyl[0];
+            else if (i == nx - 1) f = UUH[o] * m.dyl[nx - 1];
+            else {
+                const R sm = uh[o] + uh[o - 1];
+                f = m.dyl[i] * ((sm > zero) ? UUH[o - 1] : UUH[o]);
+                if (sm == zero) f = m.dyl[i] * half * (UUH[o - 1] + UUH[o]);
+            }
+            if (!wet(n, i, r)) f = zero;
+        }
+        n.flx[0][o] = f;
+    }
+    // NS flux of UH on the bottom edge of row r (rows jl = max(r-1,0), ju = r)
+    if (i < nx) {
+        R f = zero;
+        if (i <= nx - 2 && r <= ny - 1) {
+            const int jl = (r - 1 > 0) ? r - 1 : 0, ju = r;
+            const int64_t ol = (int64_t)jl * P + i, ou = (int64_t)ju * P + i;
+            const R sm = vh[ol] + vh[ol + 1];
+            f = m.dxb[r] * ((sm > zero) ? UVH[ol] : UVH[ou]);
+            if (sm == zero) f = m.dxb[r] * half * (UVH[ol] + UVH[ou]);
+            if (!(wet(n, i, ju) && wet(n, i + 1, ju) && wet(n, i, jl) && wet(n, i + 1, jl))) f = zero;
+        }
+        n.flx[1][o] = f;
+    }
+    // NS flux of VH on the bottom edge of row r
+    if (i < nx) {
+        R f = zero;
+        if (i <= nx - 2 && r <= ny - 1) {
+            const int jm1 = (r - 1 > 0) ? r - 1 : 0;
+            const int64_t om = (int64_t)jm1 * P + i;
+            const R w = half * (m.dxb[r] + m.dxb[r + 1]);
+            const R sm = vh[o] + vh[om];
+            f = w * ((sm > zero) ? VVH[om] : VVH[o]);
+            if (sm == zero) f = w * half * (VVH[om] + VVH[o]);
+            if (!wet(n, i, r)) f = zero;
+        }
+        n.flx[2][o] = f;
+    }
+    // EW flux of VH at the west face of column i, rows 0..ny-2; column 0
+    // takes column 1's upwind value before its tie and wet/dry treatment
+    if (i < nx) {
+        R f = zero;
+        if (r <= ny - 2) {
+            const int ic = (i >= 1) ? i : 1;
+            const int64_t oc = (int64_t)r * P + ic;
+            const R sm = uh[oc - 1] + uh[oc - 1 + P];
+            f = m.dyl[ic - 1] * ((sm > zero) ? VUH[oc - 1] : VUH[oc]);
+            if (i >= 1) {
+                if (sm == zero) f = m.dyl[i - 1] * half * (VUH[oc - 1] + VUH[oc]);
+                if (!(wet(n, i - 1, r) && wet(n, i, r) && wet(n, i - 1, r + 1) && wet(n, i, r + 1))) f = zero;
+            }
+        }
+        n.flx[3][o] = f;
+    }
+}
+
+template <typename R, bool SPH, bool COR>
+__global__ void momentum_kernel(NLArgs<R> n)
+{
+    const LinArgs<R> &a = n.a;
+    const int nx = a.p.nx, ny = a.p.ny;
+    const int i = blockIdx.x * 32 + threadIdx.x, r = blockIdx.y * 8 + threadIdx.y;
+    if (i >= nx || r >= ny) return;
+    const int64_t P = a.p.pitch, o = (int64_t)r * P + i;
+    const R *uh = a.p.uh, *vh = a.p.vh, *st = a.p.stg_o, *el = a.p.elv;
+    if (i > nx - 2 || r > ny - 2) {
+        a.p.uh_o[o] = uh[o];
+        a.p.vh_o[o] = vh[o];
+        return;
+    }
+    const R g = K<R>::gravity(), half = K<R>::half(), one = K<R>::one(), zero = K<R>::zero();
+    const R mad = K<R>::min_depth();
+    const R dt = a.dt;
+    const R inv_cell_area_dt = dt / a.m.area[r];
+    const R inv_cell_area_dt_g = g * inv_cell_area_dt;
+    const R inv_cell_area_dt_vh = dt / (half * (a.m.area[r] + a.m.area[r + 1]));
+    const R inv_cell_area_dt_vh_g = g * inv_cell_area_dt_vh;
+    const int64_t oe = o + 1, on = o + P;
+    R h_jph = half * ((st[on] + st[o]) - (el[on] + el[o]));
+    if (h_jph < mad) h_jph = zero;
+    R h_iph = half * ((st[oe] + st[o]) - (el[oe] + el[o]));
+    if (h_iph < mad) h_iph = zero;
+    const bool jw1 = st[on] > el[on] + mad, jw0 = st[o] > el[o] + mad;
+    const R h_jph_wet_strict = (jw1 && jw0) ? one : zero;
+    const R h_jph_wet = ((h_jph_wet_strict > zero) || (jw1 && st[on] > el[o] + mad) || (jw0 && st[o] > el[on] + mad))
+                            ? one : zero;
+    const bool iw1 = st[oe] > el[oe] + mad, iw0 = jw0;
+    const R h_iph_wet_strict = (iw1 && iw0) ? one : zero;
+    const R h_iph_wet = ((h_iph_wet_strict > zero) || (iw1 && st[oe] > el[o] + mad) || (iw0 && st[o] > el[oe] + mad))
+                            ? one : zero;
+    const int rm = (r > 0) ? r - 1 : 0, im = (i > 0) ? i - 1 : 0;
+    const R vh_iph_jmh = half * (vh[(int64_t)rm * P + i] + vh[(int64_t)rm * P + i + 1]);
+    const R vh_iph_jph = half * (vh[o] + vh[oe]);
+    const R uh_i_j = half * (uh[o] + uh[(int64_t)r * P + im]);
+    const R uh_i_jp1 = half * (uh[on] + uh[(int64_t)(r + 1) * P + im]);
+    const R u0 = uh[o], v0 = vh[o];
+    const R tv = half * (vh_iph_jmh + vh_iph_jph);
+    const R tu = half * (uh_i_j + uh_i_jp1);
+    const R fm_uh = one / ((one + a.lin_fric_dt) + dt * n.fw[o] * R(sqrt(u0 * u0 + tv * tv)));
+    const R fm_vh = one / ((one + a.lin_fric_dt) + dt * n.fw[n.plane + o] * R(sqrt(v0 * v0 + tu * tu)));
+    R u = u0 * h_iph_wet - inv_cell_area_dt_g * h_iph * h_iph_wet * (st[oe] - st[o]) * a.m.dyl[i + 1];
+    R v = v0 * h_jph_wet - inv_cell_area_dt_vh_g * h_jph * h_jph_wet * (st[on] - st[o]) * a.m.dxb[r + 1];
+    const R *F0 = n.flx[0], *F1 = n.flx[1], *F2 = n.flx[2], *F3 = n.flx[3];
+    u = u - inv_cell_area_dt * R(1) * h_iph_wet * ((F0[oe] - F0[o]) + (F1[on] - F1[o]));
+    v = v - inv_cell_area_dt_vh * R(1) * h_jph_wet * ((F3[oe] - F3[o]) + (F2[on] - F2[o]));
+    if (COR) {
+        const R dthc = dt * a.m.cor[r] * half * ((h_iph_wet_strict > zero) ? one : zero);
+        const R dthc_jph = dt * a.m.cor_be[r + 1] * half * ((h_jph_wet_strict > zero) ? one : zero);
+        u = u + dthc * (vh_iph_jmh + vh_iph_jph);
+        v = v - dthc_jph * (uh_i_j + uh_i_jp1);
+    }
+    if (SPH) {
+        R inv_depth_local = zero;
+        if (h_iph_wet_strict > zero) inv_depth_local = one / h_iph;
+        const R tan_uvh = dt * a.m.tanlat[r] * u0 * half * (vh_iph_jmh + vh_iph_jph) * inv_depth_local;
+        inv_depth_local = zero;
+        if (h_jph_wet_strict > zero) inv_depth_local = one / h_jph;
+        const R tan_uuh = dt * half * (a.m.tanlat[r] + a.m.tanlat[r + 1]) * half * (uh_i_jp1 + uh_i_j) * half *
+                          (uh_i_jp1 + uh_i_j) * inv_depth_local;
+        u = u + tan_uvh;
+        v = v - tan_uuh;
+    }
+    a.p.uh_o[o] = fm_uh * u;
+    a.p.vh_o[o] = fm_vh * v;
+}
+
+// No outflow from dry cells (:855-880), per face.
+template <typename R>
+__global__ void dry_outflow_kernel(NLArgs<R> n)
+{
+    const int nx = n.a.p.nx, ny = n.a.p.ny;
+    const int i = blockIdx.x * 32 + threadIdx.x, r = blockIdx.y * 8 + threadIdx.y;
+    if (i >= nx || r > ny - 2) return;
+    const int64_t P = n.a.p.pitch, o = (int64_t)r * P + i;
+    const R mad = K<R>::min_depth();
+    auto dry = [&](int64_t q) { return n.a.p.stg_o[q] < n.a.p.elv[q] + mad; };
+    R u = n.a.p.uh_o[o], v = n.a.p.vh_o[o];
+    if ((dry(o) && u > R(0)) || (i + 1 <= nx - 1 && dry(o + 1) && u < R(0))) n.a.p.uh_o[o] = R(0);
+    if ((dry(o) && v > R(0)) || (dry(o + P) && v < R(0))) n.a.p.vh_o[o] = R(0);
+}
+
+}  // namespace nl
+
+// one_leapfrog_nonlinear_step (timestepping_alternatives_include.f90:
+// 439-447) on the whole domain.  c.nl_work holds the 9 work planes of
+// pitch x (ny + 1) elements; c.fw the friction work.
+template <typename R>
+cudaError_t launch_leapfrog_nonlinear_step(const StepPlanes<R> &p, const Metrics<R> &m, const StepConfig &c, R dt,
+                                           DevScalars *sc, cudaStream_t s, const LaunchHook &hook)
+{
+    LinArgs<R> a = make_args<R>(p, m, c, dt);
+    a.xl = 0; a.xu = p.nx - 1; a.yl = 0; a.yu = p.ny - 1;   // the reference fixes the whole domain
+    nl::NLArgs<R> n;
+    n.a = a;
+    n.nsq = p.manning_sq;
+    const int64_t wplane = p.pitch * (int64_t)(p.ny + 1);
+    R *w = (R *)c.nl_work;
+    n.lag0 = w;
+    for (int k = 0; k < 4; k++) n.adv[k] = w + (1 + k) * wplane;
+    for (int k = 0; k < 4; k++) n.flx[k] = w + (5 + k) * wplane;
+    n.fw = (const R *)c.fw;
+    n.plane = p.pitch * (int64_t)p.ny;
+    const dim3 block(32, 8), g1((p.nx + 31) / 32, (p.ny + 7) / 8), g2((p.nx + 32) / 32, (p.ny + 8) / 8);
+    auto run = [&](int cat, auto &&launch) {
+        hook(cat, 0);
+        launch();
+        hook(cat, 1);
+    };
+    run(CAT_LINEAR_EDGE, [&] { nl::lag0_kernel<R><<<g1, block, 0, s>>>(n); });
+    run(CAT_LINEAR_EDGE, [&] { linear_edge_kernel<R><<<1, 512, 0, s>>>(a, sc, c.exterior_cells_width, c.bf); });
+    run(CAT_LINEAR_MAIN, [&] { nl::stage_kernel<R><<<g1, block, 0, s>>>(n); });
+    if (c.n_forcing) {
+        ForcingClock clk{};
+        clk.mode = FORCE_LEAPFROG;
+        clk.dt = (double)dt;
+        launch_forcing<R>(c, clk, p.pitch, p.stg_o, const_cast<R *>(p.uh), const_cast<R *>(p.vh), p.elv, sc, s,
+                          hook, CAT_LINEAR_EDGE);
+    }
+    run(CAT_LINEAR_EDGE, [&] {
+        if (c.chezy)
+            friction_work_kernel<R, true><<<g1, block, 0, s>>>(a, p.manning_sq, (R *)c.fw, 0, 1, 0, p.nx - 1, 0,
+                                                               p.ny - 1);
+        else
+            friction_work_kernel<R, false><<<g1, block, 0, s>>>(a, p.manning_sq, (R *)c.fw, 0, 1, 0, p.nx - 1, 0,
+                                                                p.ny - 1);
+    });
+    run(CAT_LINEAR_MAIN, [&] { nl::advection_kernel<R><<<g1, block, 0, s>>>(n); });
+    run(CAT_LINEAR_MAIN, [&] { nl::flux_kernel<R><<<g2, block, 0, s>>>(n); });
+    run(CAT_LINEAR_MAIN, [&] {
+        if (c.spherical && c.coriolis) nl::momentum_kernel<R, true, true><<<g1, block, 0, s>>>(n);
+        else if (c.spherical) nl::momentum_kernel<R, true, false><<<g1, block, 0, s>>>(n);
+        else nl::momentum_kernel<R, false, false><<<g1, block, 0, s>>>(n);
+    });
+    run(CAT_LINEAR_MAIN, [&] { nl::dry_outflow_kernel<R><<<g1, block, 0, s>>>(n); });
+    if (p.max_stage)
+        run(CAT_MAXSTAGE, [&] {
+            launch_update_max_stage<R>(p.nx, p.ny, p.pitch, p.stg_o, p.max_stage, c, s);
+        });
+    return cudaGetLastError();
+}
+
 template <typename R>
 cudaError_t launch_linear_map(const StepPlanes<R> &p, const Metrics<R> &m, const StepConfig &c, R dt,
                               const int *sites, int n_sites, double *rec, cudaStream_t s, const LaunchHook &hook)
@@ -1338,6 +1659,12 @@ cudaError_t launch_gauges(int64_t pitch, const R *stg, const R *uh, const R *vh,
     return cudaGetLastError();
 }
 
+template cudaError_t launch_leapfrog_nonlinear_step<double>(const StepPlanes<double> &, const Metrics<double> &,
+                                                             const StepConfig &, double, DevScalars *, cudaStream_t,
+                                                             const LaunchHook &);
+template cudaError_t launch_leapfrog_nonlinear_step<float>(const StepPlanes<float> &, const Metrics<float> &,
+                                                            const StepConfig &, float, DevScalars *, cudaStream_t,
+                                                            const LaunchHook &);
 template cudaError_t launch_linear_step<double>(const StepPlanes<double> &, const Metrics<double> &,
                                                 const StepConfig &, double, DevScalars *, cudaStream_t,
                                                 const LaunchHook &, const AuxStream *);

@@ -80,6 +80,7 @@ struct StepConfig {
     void *ring;             // linear + Flather: 2 (nx + ny - 2) x 2 reals of ring momenta
     void *fw;               // leapfrog_linear_plus_nonlinear_friction: friction_work (2 planes), else null
     int fw_ready;           // truely linear: friction_work already computed (friction_work_is_setup)
+    void *nl_work;          // leapfrog_nonlinear: 9 work planes of pitch x (ny + 1)
     int n_forcing;          // forcing patches, applied in order (apply_forcing_patch_array)
     const ForcingPatch *forcing;
 };
@@ -132,6 +133,10 @@ template <typename R>
 cudaError_t launch_linear_step(const StepPlanes<R> &p, const Metrics<R> &m, const StepConfig &c,
                                R dt, DevScalars *sc, cudaStream_t s, const LaunchHook &hook,
                                const AuxStream *aux = nullptr);
+// one_leapfrog_nonlinear_step (domain_mod_leapfrog_nonlinear_include.f90).
+template <typename R>
+cudaError_t launch_leapfrog_nonlinear_step(const StepPlanes<R> &p, const Metrics<R> &m, const StepConfig &c, R dt,
+                                           DevScalars *sc, cudaStream_t s, const LaunchHook &hook);
 
 // The leapfrog's interior update alone (no boundary routine, boundary-flux
 // sums, time or max_stage): the linear map x' = M x that the adjoint

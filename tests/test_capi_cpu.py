@@ -53,7 +53,7 @@ def test_unknown_method_is_rejected():
     assert e.value.code == 2 and "not recognized" in str(e.value)
 
 
-@pytest.mark.parametrize("m", ["cliffs", "leapfrog_nonlinear"])
+@pytest.mark.parametrize("m", ["cliffs"])
 def test_valid_but_unimplemented_methods(m):
     with pytest.raises(SwalsError) as e:
         _create(timestepping_method=m)
