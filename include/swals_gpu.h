@@ -360,6 +360,17 @@ int swals_gpu_forcing_clear(swals_domain *d);
  * at domain%time, outside a step. */
 int swals_gpu_apply_forcing(swals_domain *d, double dt);
 
+/* domain%use_eddy_viscosity and domain%eddy_visc_constants = [constant,
+ * shiono_knight] (domain_mod.f90:233-243, 890-898): the finite-volume
+ * fluxes take the *_eddyvisc form of their compute_fluxes_inner_method
+ * (compute_fluxes_alternatives_include.f90, domain_mod.f90:1448-1484), with
+ * the viscosity of get_eddy_viscosity (compute_fluxes_DE1_inner_include.f90:
+ * 864-1017; constant when shiono_knight is 0, else constant + Shiono-Knight).
+ * 'rk2', 'rk2n', 'midpoint' and 'euler' only (SWALS_ERR_UNSUPPORTED
+ * otherwise, as the reference's error stop).  use_eddy_viscosity = 0 turns it
+ * off.  Drops a captured evolve_steps graph. */
+int swals_gpu_set_eddy_viscosity(swals_domain *d, int32_t use_eddy_viscosity, double constant, double shiono_knight);
+
 /* ---- REAL4 output staging ------------------------------------------------
  * What SWALS's netCDF writers store, converted to REAL4 (round to nearest)
  * on the device and copied to host_out in one transfer; the call returns

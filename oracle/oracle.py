@@ -73,6 +73,8 @@ class _OracleDomainC(ctypes.Structure):
         ("nest_offset", ctypes.c_void_p), ("nest_integral", ctypes.c_void_p), ("friction_work", ctypes.c_void_p),
         ("n_forcing", ctypes.c_int32), ("pad2", ctypes.c_int32), ("forcing", ctypes.c_void_p),
         ("advection_work", ctypes.c_void_p),
+        ("use_eddy_viscosity", ctypes.c_int32), ("pad3", ctypes.c_int32),
+        ("eddy_visc_constants", ctypes.c_double * 2), ("eddy_visc", ctypes.c_void_p),
     ]
 
 
@@ -155,6 +157,7 @@ class OracleDomain:
         self.backup_U = np.zeros((3, ny, nx), dt)
         self.friction_work = np.zeros((2, ny, nx), dt)
         self.advection_work = np.zeros((5, ny, nx), dt)
+        self.eddy_visc = np.zeros((ny, nx), dt)
         for name, arr in [("U", self.U), ("max_stage", self.max_stage), ("manning_squared", self.manning_squared),
                           ("x", self.x), ("y", self.y), ("dxb", self.dxb), ("dyl", self.dyl), ("area", self.area),
                           ("coriolis_c", self.coriolis_c), ("coriolis_be", self.coriolis_be),
@@ -162,7 +165,8 @@ class OracleDomain:
                           ("flux_NS", self.flux_NS), ("flux_EW", self.flux_EW),
                           ("explicit_source", self.explicit_source),
                           ("explicit_source_VH_j_minus_1", self.es_jm1), ("backup_U", self.backup_U),
-                          ("friction_work", self.friction_work), ("advection_work", self.advection_work)]:
+                          ("friction_work", self.friction_work), ("advection_work", self.advection_work),
+                          ("eddy_visc", self.eddy_visc)]:
             setattr(c, name, _ptr(arr))
         self._fn("apply_method_defaults")(ctypes.byref(c))
         self._fn("setup_geometry")(ctypes.byref(c))
@@ -201,6 +205,16 @@ class OracleDomain:
         f.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
         return f(ctypes.addressof(self.c), None if m is None else _ptr(m))
+
+    def set_eddy_viscosity(self, constant, shiono_knight=0.0):
+        """domain%use_eddy_viscosity = .true. with eddy_visc_constants =
+        [constant, shiono_knight] (domain_mod.f90:233-243, 890-898); only
+        the finite-volume methods support it."""
+        if self.c.method not in (METHODS["rk2"], METHODS["rk2n"], METHODS["midpoint"], METHODS["euler"]):
+            raise ValueError("eddy viscosity is not supported for this timestepping_method")
+        self.c.use_eddy_viscosity = 1
+        self.c.eddy_visc_constants[0] = constant
+        self.c.eddy_visc_constants[1] = shiono_knight
 
     def add_forcing_patch(self, i0, i1, j0, j1, k0, k1, start_time, end_time, work):
         """forcing_patch%setup + forcing_work (forcing_mod.f90:264-319),

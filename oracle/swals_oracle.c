@@ -87,6 +87,37 @@ static double or_pow_friction(double x, int chezy)
 
 double ORACLE_FN(pow_friction)(double x, int32_t chezy) { return or_pow_friction(x, chezy); }
 
+/* depth**(1 - 1/6) of the Shiono-Knight eddy viscosity
+ * (compute_fluxes_DE1_inner_include.f90:1000-1002), correctly rounded for
+ * the double exponent p = fl(1 - 1/6), depth >= 0, in double-double
+ * arithmetic: the Newton-corrected cube root, its Newton-corrected square
+ * root (x**(1/6)), a compensated quotient x / x**(1/6) = x**(5/6), and the
+ * factor x**eps = 1 + eps*ln(x) with eps = p - 5/6 (|eps*ln x| < 1e-14).
+ * Checked against 300-bit arithmetic (tests/test_pow_friction.py). */
+static double or_pow_eddy(double x)
+{
+    if (x == 0.0) return 0.0;
+    double c0 = cbrt(x);
+    or_dd s = or_two_prod(c0, c0);
+    or_dd t = or_two_prod(s.hi, c0);
+    t.lo += s.lo * c0;
+    double r = (x - t.hi) - t.lo;
+    or_dd c = or_fast_two_sum(c0, r / (3.0 * c0 * c0));
+    double q0 = sqrt(c.hi);
+    or_dd q2 = or_two_prod(q0, q0);
+    double rq = ((c.hi - q2.hi) - q2.lo) + c.lo;
+    or_dd q = or_fast_two_sum(q0, rq / (2.0 * q0));
+    double y0 = x / q.hi;
+    or_dd pq = or_two_prod(y0, q.hi);
+    pq.lo += y0 * q.lo;
+    or_dd y = or_fast_two_sum(y0, ((x - pq.hi) - pq.lo) / q.hi);
+    const double p = 1.0 - 1.0 / 6.0;
+    const double eps = fma(p, 6.0, -5.0) / 6.0;
+    const double tl = eps * log(x);
+    return or_fast_two_sum(y.hi, y.lo + y.hi * tl).hi;
+}
+double ORACLE_FN(pow_eddy)(double x) { return or_pow_eddy(x); }
+
 /* Correctly rounded cosh for the analytic boundary functions, evaluated in
  * double-double arithmetic exactly as the device library does (same
  * operation sequence: a = k ln2 + r with a double-double ln2, exp(r) by the
@@ -1111,9 +1142,56 @@ static void get_EW_limited_gradient_dx(oracle_domain *d, int j, grad_set *g)
     g->dv[0] = ZERO; g->dv[nx - 1] = ZERO;
 }
 
-/* DE1_inner_include.f90:78-727 with reduced_momentum_diffusion=.true.,
- * upwind_transverse_momentum=.false., use_eddy_viscosity=.false.
- * (compute_fluxes_alternatives_include.f90:25-36). */
+/* get_eddy_viscosity (DE1_inner_include.f90:864-1017) for every row, with
+ * the reference's model selection: constant when eddy_visc_constants(2) is
+ * 0, else constant + Shiono-Knight (c2 * depth**(5/6) * shear velocity);
+ * clipped to 0.25 min(2dx, 2dy)**2 / (2 dt_last_update + 1e-10) on columns
+ * 2..nx-1 and copied from there to columns 1 and nx. */
+static void eddy_viscosity(oracle_domain *d)
+{
+    const int nx = d->nx, ny = d->ny;
+    const REAL *vu = d->velocity, *vv = d->velocity + (size_t)nx * ny;
+    const REAL c1 = (REAL)d->eddy_visc_constants[0], c2 = (REAL)d->eddy_visc_constants[1];
+    const REAL eps_zerodiv = (REAL)1.0e-10;
+    for (int j = 1; j <= ny; j++) {
+        REAL *ev = d->eddy_visc + (size_t)(j - 1) * nx;
+        for (int i = 1; i <= nx; i++) {
+            if (c2 == ZERO) {
+                ev[i - 1] = c1;
+            } else {
+                const REAL u = vu[IDX(i, j)], v = vv[IDX(i, j)];
+                ev[i - 1] = c1 + c2 * (REAL)or_pow_eddy((double)d->depth[IDX(i, j)]) *
+                                     (REAL)sqrt(d->manning_squared[IDX(i, j)] * GRAVITY * (u * u + v * v));
+            }
+        }
+        const REAL two_dx = d->dxb[j - 1] + d->dxb[j];
+        for (int i = 2; i <= nx - 1; i++) {
+            const REAL two_dy = d->dyl[i - 1] + d->dyl[i];
+            const REAL lim = (REAL)0.25 * rmin(two_dx * two_dx, two_dy * two_dy) /
+                             ((REAL)2.0 * (REAL)d->dt_last_update + eps_zerodiv);
+            ev[i - 1] = rmin(ev[i - 1], lim);
+        }
+        if (nx >= 2) {
+            ev[0] = ev[1];
+            ev[nx - 1] = ev[nx - 2];
+        }
+    }
+}
+
+/* A momentum flux of an *_eddyvisc variant (DE1_inner_include.f90:289-358,
+ * 551-620): the advective part plus the HLL and turbulent diffusions, summed
+ * unless both have the same sign (reduced_numerical_diffusion), when the one
+ * of larger magnitude is taken. */
+static REAL eddy_momentum_flux(REAL adv, REAL hll, REAL turb)
+{
+    const REAL dmax = rmax((REAL)fabs(turb), (REAL)fabs(hll));
+    const REAL tot = (turb * hll > ZERO) ? (REAL)copysign(dmax, turb) : turb + hll;
+    return adv + tot;
+}
+
+/* DE1_inner_include.f90:78-727: the four compute_fluxes_inner_method
+ * variants (flux_variant bits) and their *_eddyvisc forms
+ * (compute_fluxes_alternatives_include.f90:11-64, domain_mod.f90:1448-1484). */
 double ORACLE_FN(compute_fluxes_DE1_low_fr_diffusion)(oracle_domain *d)
 {
     const int nx = d->nx, ny = d->ny;
@@ -1136,6 +1214,7 @@ double ORACLE_FN(compute_fluxes_DE1_low_fr_diffusion)(oracle_domain *d)
         REAL init = (REAL)(ONE / max_dt);
         max_dt_inv_global = init;
     }
+    if (d->use_eddy_viscosity) eddy_viscosity(d);
 
     #pragma omp parallel
     {
@@ -1207,13 +1286,33 @@ double ORACLE_FN(compute_fluxes_DE1_low_fr_diffusion)(oracle_domain *d)
 
                 FNS(i, j, OR_STG) = (REAL)((double)((s_max * vd_neg - s_min * vd_pos) +
                                                      sminsmax * (stage_pos_star - stage_neg_star)) * inv_denom);
-                if (d->flux_variant & OR_FLUX_UPWIND_TRANSVERSE)
-                    FNS(i, j, OR_UH) = ADVECTION_BETA * ((FNS(i, j, OR_STG) > ZERO) ? u_neg : u_pos) * FNS(i, j, OR_STG);
-                else
-                    FNS(i, j, OR_UH) = (REAL)((double)((s_max * ud_neg * vel_beta_neg - s_min * ud_pos * vel_beta_pos) +
-                                                        fr2 * sminsmax * (ud_pos - ud_neg)) * inv_denom);
-                FNS(i, j, OR_VH) = (REAL)((double)((s_max * vd_neg * vel_beta_neg - s_min * vd_pos * vel_beta_pos) +
-                                                    fr2 * sminsmax * (vd_pos - vd_neg)) * inv_denom);
+                if (!d->use_eddy_viscosity) {
+                    if (d->flux_variant & OR_FLUX_UPWIND_TRANSVERSE)
+                        FNS(i, j, OR_UH) = ADVECTION_BETA * ((FNS(i, j, OR_STG) > ZERO) ? u_neg : u_pos) * FNS(i, j, OR_STG);
+                    else
+                        FNS(i, j, OR_UH) = (REAL)((double)((s_max * ud_neg * vel_beta_neg - s_min * ud_pos * vel_beta_pos) +
+                                                            fr2 * sminsmax * (ud_pos - ud_neg)) * inv_denom);
+                    FNS(i, j, OR_VH) = (REAL)((double)((s_max * vd_neg * vel_beta_neg - s_min * vd_pos * vel_beta_pos) +
+                                                        fr2 * sminsmax * (vd_pos - vd_neg)) * inv_denom);
+                } else {
+                    /* turbulent diffusion: eddy_visc * depth * dx * du/dy, geometric-mean depth (:314-358) */
+                    const REAL evh = HALF * (d->eddy_visc[IDX(i, j)] + d->eddy_visc[IDX(i, j - 1)]);
+                    const REAL gdep = (REAL)sqrt(depth_neg_star * depth_pos_star);
+                    REAL adv, hll;
+                    if (d->flux_variant & OR_FLUX_UPWIND_TRANSVERSE) {
+                        adv = ADVECTION_BETA * ((FNS(i, j, OR_STG) > ZERO) ? u_neg : u_pos) * FNS(i, j, OR_STG);
+                        hll = ZERO;
+                    } else {
+                        adv = (REAL)((double)(s_max * ud_neg * vel_beta_neg - s_min * ud_pos * vel_beta_pos) * inv_denom);
+                        hll = (REAL)((double)(fr2 * sminsmax * (ud_pos - ud_neg)) * inv_denom);
+                    }
+                    REAL turb = -(evh * gdep * d->dxb[j - 1] * ((vu[IDX(i, j)] - vu[IDX(i, j - 1)]) / d->dyl[i - 1]));
+                    FNS(i, j, OR_UH) = eddy_momentum_flux(adv, hll, turb);
+                    adv = (REAL)((double)(s_max * vd_neg * vel_beta_neg - s_min * vd_pos * vel_beta_pos) * inv_denom);
+                    hll = (REAL)((double)(fr2 * sminsmax * (vd_pos - vd_neg)) * inv_denom);
+                    turb = -(evh * gdep * d->dxb[j - 1] * ((vv[IDX(i, j)] - vv[IDX(i, j - 1)]) / d->dyl[i - 1]));
+                    FNS(i, j, OR_VH) = eddy_momentum_flux(adv, hll, turb);
+                }
 
                 double half_g_hh_edge = inv_denom * half_gravity *
                     ((double)s_max * depth_neg_star * depth_neg_star - (double)s_min * depth_pos_star * depth_pos_star);
@@ -1285,13 +1384,33 @@ double ORACLE_FN(compute_fluxes_DE1_low_fr_diffusion)(oracle_domain *d)
 
                 FEW(i, j, OR_STG) = (REAL)((double)((s_max * ud_neg - s_min * ud_pos) +
                                                      sminsmax * (stage_pos_star - stage_neg_star)) * inv_denom);
-                FEW(i, j, OR_UH) = (REAL)((double)((s_max * ud_neg * vel_beta_neg - s_min * ud_pos * vel_beta_pos) +
-                                                    fr2 * sminsmax * (ud_pos - ud_neg)) * inv_denom);
-                if (d->flux_variant & OR_FLUX_UPWIND_TRANSVERSE)
-                    FEW(i, j, OR_VH) = ADVECTION_BETA * ((FEW(i, j, OR_STG) > ZERO) ? v_neg : v_pos) * FEW(i, j, OR_STG);
-                else
-                    FEW(i, j, OR_VH) = (REAL)((double)((s_max * vd_neg * vel_beta_neg - s_min * vd_pos * vel_beta_pos) +
-                                                        fr2 * sminsmax * (vd_pos - vd_neg)) * inv_denom);
+                if (!d->use_eddy_viscosity) {
+                    FEW(i, j, OR_UH) = (REAL)((double)((s_max * ud_neg * vel_beta_neg - s_min * ud_pos * vel_beta_pos) +
+                                                        fr2 * sminsmax * (ud_pos - ud_neg)) * inv_denom);
+                    if (d->flux_variant & OR_FLUX_UPWIND_TRANSVERSE)
+                        FEW(i, j, OR_VH) = ADVECTION_BETA * ((FEW(i, j, OR_STG) > ZERO) ? v_neg : v_pos) * FEW(i, j, OR_STG);
+                    else
+                        FEW(i, j, OR_VH) = (REAL)((double)((s_max * vd_neg * vel_beta_neg - s_min * vd_pos * vel_beta_pos) +
+                                                            fr2 * sminsmax * (vd_pos - vd_neg)) * inv_denom);
+                } else {
+                    /* turbulent diffusion: eddy_visc * depth * dy * du/dx (:576-620) */
+                    const REAL evh = HALF * (d->eddy_visc[IDX(i, j)] + d->eddy_visc[IDX(i - 1, j)]);
+                    const REAL gdep = (REAL)sqrt(depth_neg_star * depth_pos_star);
+                    const REAL dxc = HALF * (d->dxb[j - 1] + d->dxb[j]);
+                    REAL adv = (REAL)((double)(s_max * ud_neg * vel_beta_neg - s_min * ud_pos * vel_beta_pos) * inv_denom);
+                    REAL hll = (REAL)((double)(fr2 * sminsmax * (ud_pos - ud_neg)) * inv_denom);
+                    REAL turb = -(evh * gdep * d->dyl[i - 1] * ((vu[IDX(i, j)] - vu[IDX(i - 1, j)]) / dxc));
+                    FEW(i, j, OR_UH) = eddy_momentum_flux(adv, hll, turb);
+                    if (d->flux_variant & OR_FLUX_UPWIND_TRANSVERSE) {
+                        adv = ADVECTION_BETA * ((FEW(i, j, OR_STG) > ZERO) ? v_neg : v_pos) * FEW(i, j, OR_STG);
+                        hll = ZERO;
+                    } else {
+                        adv = (REAL)((double)(s_max * vd_neg * vel_beta_neg - s_min * vd_pos * vel_beta_pos) * inv_denom);
+                        hll = (REAL)((double)(fr2 * sminsmax * (vd_pos - vd_neg)) * inv_denom);
+                    }
+                    turb = -(evh * gdep * d->dyl[i - 1] * ((vv[IDX(i, j)] - vv[IDX(i - 1, j)]) / dxc));
+                    FEW(i, j, OR_VH) = eddy_momentum_flux(adv, hll, turb);
+                }
 
                 double half_g_hh_edge = inv_denom * half_gravity *
                     ((double)s_max * depth_neg_star * depth_neg_star - (double)s_min * depth_pos_star * depth_pos_star);

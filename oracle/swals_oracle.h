@@ -138,6 +138,12 @@ typedef struct oracle_domain {
     const struct oracle_forcing_patch *forcing;
     /* leapfrog_nonlinear: advection_work (nx*ny*5: DEPTH_LAG, UUH, UVH, VUH, VVH) */
     REAL *advection_work;
+    /* eddy viscosity (domain_mod.f90:233-243): flag, constants (constant,
+     * Shiono-Knight), and an nx*ny work plane */
+    int32_t use_eddy_viscosity;
+    int32_t pad3;
+    double eddy_visc_constants[2];
+    REAL *eddy_visc;
 } oracle_domain;
 
 /* forcing_patch_type (forcing_mod.f90:23-53) with the default (identity)
@@ -196,6 +202,7 @@ double ORACLE_FN(area_lonlat_rectangle)(double lon1, double lat1, double dlon, d
 void ORACLE_FN(gauge_site_index)(const double *xy, int32_t n, const double *ll,
         const double *dx, const int32_t *nxy, int32_t *site_index);
 double ORACLE_FN(pow_friction)(double x, int32_t chezy);
+double ORACLE_FN(pow_eddy)(double x);
 double ORACLE_FN(cosh_cr)(double a);
 void ORACLE_FN(boundary_function)(const oracle_domain *d, double t, int32_t i, int32_t j, REAL *out4);
 

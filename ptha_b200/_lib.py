@@ -45,6 +45,7 @@ EXPORTED = [
     "swals_gpu_md_launch_count", "swals_gpu_md_capture_graph", "swals_gpu_md_replay",
     "swals_gpu_set_priority_mask", "swals_gpu_domain_statistics", "swals_gpu_volume_in_priority_domain",
     "swals_gpu_forcing_patch_add", "swals_gpu_forcing_clear", "swals_gpu_apply_forcing",
+    "swals_gpu_set_eddy_viscosity",
     "swals_gpu_stage_grids_real4", "swals_gpu_gauges_read_real4",
 ]
 TIMER_NAMES = ["cfl", "fv_stage1", "boundary1", "fv_stage2", "boundary2", "finalize", "leapfrog_edge",
@@ -159,6 +160,7 @@ def lib():
         "swals_gpu_volume_in_priority_domain": [vp, ctypes.POINTER(dbl)],
         "swals_gpu_forcing_patch_add": [vp, i32, i32, i32, i32, i32, i32, dbl, dbl, vp, ctypes.POINTER(i32)],
         "swals_gpu_forcing_clear": [vp], "swals_gpu_apply_forcing": [vp, dbl],
+        "swals_gpu_set_eddy_viscosity": [vp, i32, dbl, dbl],
         "swals_gpu_stage_grids_real4": [vp, i32, i32, vp, i64, vp],
         "swals_gpu_gauges_read_real4": [vp, vp, i32, ctypes.POINTER(i32)],
     }

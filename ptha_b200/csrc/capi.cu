@@ -530,6 +530,7 @@ int swals_gpu_domain_destroy(swals_domain *d)
     cudaStreamSynchronize(d->stream);
     free_forcing(d);
     if (d->stage_buf) cudaFree(d->stage_buf);
+    if (d->eddy_visc) cudaFree(d->eddy_visc);
     for (auto &p : d->pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
     for (auto e : d->ev_pool) cudaEventDestroy(e);
     if (d->d_sites) cudaFree(d->d_sites);
@@ -912,6 +913,31 @@ int swals_gpu_forcing_clear(swals_domain *d)
     CK(cudaStreamSynchronize(d->stream));
     free_forcing(d);
     drop_step_graph(d);
+    return SWALS_OK;
+}
+
+int swals_gpu_set_eddy_viscosity(swals_domain *d, int32_t use_eddy_viscosity, double constant, double shiono_knight)
+{
+    if (!d) return fail(SWALS_ERR_INVALID_ARGUMENT, "NULL domain");
+    CK(cudaStreamSynchronize(d->stream));
+    drop_step_graph(d);
+    if (!use_eddy_viscosity) {
+        d->cfg.flux_variant &= ~swals::FLUX_EDDY;
+        d->cfg.eddy_visc = nullptr;
+        return SWALS_OK;
+    }
+    // timestepping_metadata(:)%eddy_viscosity_is_supported (timestepping_metadata_mod.f90:79-109)
+    if (!(d->method == M_RK2 || d->method == M_RK2N || d->method == M_MIDPOINT || d->method == M_EULER))
+        return fail(SWALS_ERR_UNSUPPORTED, "Eddy viscosity is not supported for the numerical scheme %s",
+                    d->desc.timestepping_method);
+    if (d->nx < 3) return fail(SWALS_ERR_INVALID_ARGUMENT, "eddy viscosity needs nx >= 3");
+    if (!(constant >= 0.0) || !(shiono_knight >= 0.0))
+        return fail(SWALS_ERR_INVALID_ARGUMENT, "eddy_visc_constants must be >= 0");
+    if (!d->eddy_visc) CK(cudaMalloc(&d->eddy_visc, (size_t)d->pitch * d->ny * esize(d)));
+    d->cfg.eddy_visc = d->eddy_visc;
+    d->cfg.eddy_visc_constants[0] = constant;
+    d->cfg.eddy_visc_constants[1] = shiono_knight;
+    d->cfg.flux_variant |= swals::FLUX_EDDY;
     return SWALS_OK;
 }
 

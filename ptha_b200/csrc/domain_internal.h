@@ -61,6 +61,7 @@ struct swals_domain {
     std::vector<swals::ForcingPatch> forcing;
     // REAL4 output staging buffer (floats), allocated on first use.
     float *stage_buf = nullptr;
+    void *eddy_visc = nullptr;   // use_eddy_viscosity: one plane of pitch x ny reals
     size_t stage_cap = 0;
     // Replayed graph of a few steps for evolve_steps.
     cudaGraphExec_t step_graph = nullptr;

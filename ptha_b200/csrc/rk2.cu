@@ -94,7 +94,7 @@ struct Smem {
     long long negfix[NT / 32];
 };
 
-template <typename R, int MODE, bool SPH, bool COR, int FRIC>
+template <typename R, int MODE, bool SPH, bool COR, int FRIC, bool EDDY>
 __global__ void __launch_bounds__(NT, 3) rk2_stage_kernel(const Rk2Args<R> a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -175,8 +175,10 @@ __global__ void __launch_bounds__(NT, 3) rk2_stage_kernel(const Rk2Args<R> a)
         e.f[0] = R(0); e.f[1] = R(0); e.f[2] = R(0); e.es_pos = 0.0; e.es_neg = 0.0;
         if (r >= 1 && r <= ny - 1 && i >= 1 && i <= nx - 1) {
             double cand;
-            edge_flux<R, true>(S.cell.get(rr + 1, cc + 2), S.gns.get(rr, cc), S.cell.get(rr + 2, cc + 2), S.gns.get(rr + 1, cc),
-                               a.m.dxb[r], inv2, e, cand, a.flux_variant);
+            edge_flux<R, true, EDDY>(S.cell.get(rr + 1, cc + 2), S.gns.get(rr, cc), S.cell.get(rr + 2, cc + 2),
+                                     S.gns.get(rr + 1, cc), a.m.dxb[r], inv2, e, cand, a.flux_variant,
+                                     EDDY ? a.ev[(int64_t)(r - 1) * a.P + i] : R(0),
+                                     EDDY ? a.ev[(int64_t)r * a.P + i] : R(0), EDDY ? a.m.dyl[i] : R(1));
             cfl = fmax(cfl, cand);
             if (MODE != MODE_CFL && a.lines) {
                 if (r == ny - a.n_ext && i >= a.n_ext && i <= nx - a.n_ext - 1) a.lines[i] = (double)e.f[0];
@@ -193,8 +195,11 @@ __global__ void __launch_bounds__(NT, 3) rk2_stage_kernel(const Rk2Args<R> a)
         if (r >= 1 && r <= ny - 1 && i >= 1 && i <= nx - 1) {
             const R inv1 = R(1) / (a.m.dxb[r] * a.half_cfl);  // dx_cfl_half_inv(1)
             double cand;
-            edge_flux<R, false>(S.cell.get(rr + 2, cc + 1), S.gew.get(rr, cc), S.cell.get(rr + 2, cc + 2), S.gew.get(rr, cc + 1),
-                                a.m.dyl[i], inv1, e, cand, a.flux_variant);
+            const int64_t oe = (int64_t)r * a.P + i;
+            edge_flux<R, false, EDDY>(S.cell.get(rr + 2, cc + 1), S.gew.get(rr, cc), S.cell.get(rr + 2, cc + 2),
+                                      S.gew.get(rr, cc + 1), a.m.dyl[i], inv1, e, cand, a.flux_variant,
+                                      EDDY ? a.ev[oe - 1] : R(0), EDDY ? a.ev[oe] : R(0),
+                                      EDDY ? R(0.5) * (a.m.dxb[r] + a.m.dxb[r + 1]) : R(1));
             cfl = fmax(cfl, cand);
             if (MODE != MODE_CFL && a.lines) {
                 if (i == nx - a.n_ext && r >= a.n_ext && r <= ny - a.n_ext - 1) a.lines[nx + r] = (double)e.f[0];
@@ -502,24 +507,35 @@ __global__ void __launch_bounds__(1024) rk2_finalize_kernel(int nx, int ny, int 
     sc->max_dt_inv_bits = 0ull;
 }
 
-template <typename R, int MODE, bool SPH, bool COR, int FRIC>
-cudaError_t launch_stage(const Rk2Args<R> &a, cudaStream_t s)
+template <typename R, int MODE, bool SPH, bool COR, int FRIC, bool EDDY>
+cudaError_t launch_stage_tile(const Rk2Args<R> &a, cudaStream_t s)
 {
     static bool configured = false;
     const size_t smem = sizeof(Smem<R>);
     if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(rk2_stage_kernel<R, MODE, SPH, COR, FRIC>,
+        cudaError_t e = cudaFuncSetAttribute(rk2_stage_kernel<R, MODE, SPH, COR, FRIC, EDDY>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         // Prefer shared memory over L1 so three CTAs fit per SM.
-        e = cudaFuncSetAttribute(rk2_stage_kernel<R, MODE, SPH, COR, FRIC>,
+        e = cudaFuncSetAttribute(rk2_stage_kernel<R, MODE, SPH, COR, FRIC, EDDY>,
                                  cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         if (e != cudaSuccess) return e;
         configured = true;
     }
     dim3 grid((a.nx + TX - 1) / TX, (a.ny + TY - 1) / TY);
-    rk2_stage_kernel<R, MODE, SPH, COR, FRIC><<<grid, NT, smem, s>>>(a);
+    rk2_stage_kernel<R, MODE, SPH, COR, FRIC, EDDY><<<grid, NT, smem, s>>>(a);
     return cudaGetLastError();
+}
+
+// The eddy-viscosity fluxes are a separate instantiation (the CFL pass never
+// needs them), so the default kernels carry none of their code.
+template <typename R, int MODE, bool SPH, bool COR, int FRIC>
+cudaError_t launch_stage(const Rk2Args<R> &a, cudaStream_t s)
+{
+    if constexpr (MODE != MODE_CFL) {
+        if (a.flux_variant & FLUX_EDDY) return launch_stage_tile<R, MODE, SPH, COR, FRIC, true>(a, s);
+    }
+    return launch_stage_tile<R, MODE, SPH, COR, FRIC, false>(a, s);
 }
 
 }  // namespace
@@ -644,14 +660,106 @@ cudaError_t launch_update(const Rk2Args<R> &a, cudaStream_t s)
     if (fric == FRIC_CHEZY) return FN<R, false, false, FRIC_CHEZY>(a, s);                              \
     return FN<R, false, false, FRIC_NONE>(a, s);
 
+// get_eddy_viscosity (DE1_inner_include.f90:864-1017) for every cell of the
+// stage input, before the fluxes that use it: constant when
+// eddy_visc_constants(2) is 0, else constant + Shiono-Knight
+// (c2 depth**(5/6) sqrt(n^2 g speed^2)), clipped to
+// 0.25 min(2dx, 2dy)^2 / (2 dt_last_update + 1e-10); columns 1 and nx take
+// the clipped values of columns 2 and nx-1 (nx >= 3).
 template <typename R>
-cudaError_t dispatch_flux(const Rk2Args<R> &a, const StepConfig &c, cudaStream_t s) { SWALS_DISPATCH_FV(launch_flux_pass) }
+__global__ void __launch_bounds__(256) eddy_visc_kernel(const Rk2Args<R> a)
+{
+    const int i = blockIdx.x * 32 + threadIdx.x, r = blockIdx.y * 8 + threadIdx.y;
+    const int nx = a.nx, ny = a.ny;
+    if (i >= nx || r >= ny) return;
+    const int is = (i < 1) ? 1 : ((i > nx - 2) ? nx - 2 : i);
+    const int64_t o = (int64_t)r * a.P + is;
+    R dep = a.stg[o] - a.elv[o], u = R(0), v = R(0);
+    if (dep > K<R>::min_depth()) {
+        const R depth_inv = R(1) / dep;
+        u = a.uh[o] * depth_inv;
+        v = a.vh[o] * depth_inv;
+    } else if (dep < R(0)) {
+        dep = R(0);
+    }
+    R ev;
+    if (a.ev_c2 == R(0))
+        ev = a.ev_c1;
+    else
+        ev = a.ev_c1 + a.ev_c2 * R(pow_eddy_cr((double)dep)) * R(sqrt(a.nsq[o] * K<R>::gravity() * (u * u + v * v)));
+    const R two_dx = a.m.dxb[r] + a.m.dxb[r + 1];
+    const R two_dy = a.m.dyl[is] + a.m.dyl[is + 1];
+    const R lim = R(0.25) * rmin(two_dx * two_dx, two_dy * two_dy) /
+                  (R(2.0) * R(a.sc->dt_last_update) + R(1.0e-10));
+    a.ev[(int64_t)r * a.P + i] = rmin(ev, lim);
+}
+
+// domain%dt_last_update = dt of the update just made (update_U_DE1_inner_include.f90:17).
+template <typename R>
+__global__ void dt_last_update_kernel(const Rk2Args<R> a)
+{
+    a.sc->dt_last_update = (double)stage_dt<R>(a);
+}
 
 template <typename R>
-cudaError_t dispatch_update(const Rk2Args<R> &a, const StepConfig &c, cudaStream_t s) { SWALS_DISPATCH_FV(launch_update) }
+cudaError_t launch_eddy_visc(const Rk2Args<R> &a, cudaStream_t s)
+{
+    dim3 block(32, 8), grid((a.nx + 31) / 32, (a.ny + 7) / 8);
+    eddy_visc_kernel<R><<<grid, block, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_dt_last_update(const Rk2Args<R> &a, cudaStream_t s)
+{
+    dt_last_update_kernel<R><<<1, 1, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t dispatch_flux(const Rk2Args<R> &a, const StepConfig &c, cudaStream_t s)
+{
+    if (a.flux_variant & FLUX_EDDY) {
+        const cudaError_t e = launch_eddy_visc<R>(a, s);
+        if (e != cudaSuccess) return e;
+    }
+    SWALS_DISPATCH_FV(launch_flux_pass)
+}
+
+template <typename R>
+cudaError_t dispatch_update_fv(const Rk2Args<R> &a, const StepConfig &c, cudaStream_t s) { SWALS_DISPATCH_FV(launch_update) }
+
+template <typename R>
+cudaError_t dispatch_update(const Rk2Args<R> &a, const StepConfig &c, cudaStream_t s)
+{
+    const cudaError_t e = dispatch_update_fv<R>(a, c, s);
+    if (e != cudaSuccess || !(a.flux_variant & FLUX_EDDY)) return e;
+    return launch_dt_last_update<R>(a, s);
+}
 
 template <typename R, int MODE>
+cudaError_t dispatch_stage_fv(const Rk2Args<R> &a, const StepConfig &c, cudaStream_t s);
+
+// A stage kernel launch; with eddy viscosity, the viscosity of the stage
+// input first and, after an update, dt_last_update.  The CFL pass does not
+// depend on the viscosity and runs without it.
+template <typename R, int MODE>
 cudaError_t dispatch_stage(const Rk2Args<R> &a, const StepConfig &c, cudaStream_t s)
+{
+    if (!(a.flux_variant & FLUX_EDDY)) return dispatch_stage_fv<R, MODE>(a, c, s);
+    if (MODE == MODE_CFL) {
+        Rk2Args<R> b = a;
+        b.flux_variant &= ~FLUX_EDDY;
+        return dispatch_stage_fv<R, MODE>(b, c, s);
+    }
+    cudaError_t e = launch_eddy_visc<R>(a, s);
+    if (e == cudaSuccess) e = dispatch_stage_fv<R, MODE>(a, c, s);
+    if (e == cudaSuccess) e = launch_dt_last_update<R>(a, s);
+    return e;
+}
+
+template <typename R, int MODE>
+cudaError_t dispatch_stage_fv(const Rk2Args<R> &a, const StepConfig &c, cudaStream_t s)
 {
     const int fric = c.nofriction ? FRIC_NONE : (c.chezy ? FRIC_CHEZY : FRIC_MANNING);
     if (c.spherical) {
@@ -698,6 +806,10 @@ Rk2Args<R> fv_args(int nx, int ny, int64_t pitch, R *elv, R *manning_sq, const M
     a.lines = nullptr;
     a.write_cfl = 0;
     a.dt_from_cfl = 0;
+    a.ev = reinterpret_cast<R *>(c.eddy_visc);
+    a.ev_c1 = R(c.eddy_visc_constants[0]);
+    a.ev_c2 = R(c.eddy_visc_constants[1]);
+    if (!a.ev) a.flux_variant &= ~FLUX_EDDY;
     return a;
 }
 

@@ -50,6 +50,8 @@ struct Rk2Args {
     int flux_variant;              // FLUX_* bits (compute_fluxes_inner_method)
     R dt_scale;                    // the stage's dt times this (midpoint half step, rk2n last step; else 1)
     int base0;                     // stage 1 updates U0 (stg0..) with this state's fluxes (midpoint)
+    R *ev;                         // per-cell eddy viscosity of the stage input (FLUX_EDDY), else null
+    R ev_c1, ev_c2;                // eddy_visc_constants
 };
 
 template <typename R> struct Cell { R stg, dep, u, v, elv; };
@@ -94,14 +96,29 @@ struct EdgeRes {
     double es_neg;   // contribution to the cell on the - side
 };
 
+// A momentum flux of the *_eddyvisc variants (DE1_inner_include.f90:
+// 289-358, 551-620): the advective part plus the HLL and turbulent
+// diffusions, summed unless both have the same sign
+// (reduced_numerical_diffusion), when the larger magnitude is taken.
+template <typename R>
+__device__ __forceinline__ R eddy_momentum_flux(R adv, R hll, R turb)
+{
+    const R dmax = rmax(R(fabs(turb)), R(fabs(hll)));
+    const R tot = (turb * hll > R(0)) ? R(copysign(dmax, turb)) : turb + hll;
+    return adv + tot;
+}
+
 // One Audusse/HLL edge of DE1_inner_include.f90 (:187-430 NS, :456-716 EW).
 // NS=true: normal velocity v, edge between (i,j-1) and (i,j).
 // variant: compute_fluxes_inner_method as FLUX_* bits (swals_kernels.h);
-// 0 is the default 'DE1_low_fr_diffusion'.
-template <typename R, bool NS>
+// 0 is the default 'DE1_low_fr_diffusion'.  EDDY (FLUX_EDDY): ev_n / ev_p are
+// the eddy viscosities of the two cells and vel_div the distance the
+// velocity difference is taken over (distance_left_edge(i) for NS edges,
+// the mean of distance_bottom_edge(j), (j+1) for EW edges).
+template <typename R, bool NS, bool EDDY = false>
 __device__ __forceinline__ void edge_flux(const Cell<R> &cn, const Grad<R> &gn, const Cell<R> &cp, const Grad<R> &gp,
                                           R edge_len, R dx_cfl_half_inv, EdgeRes<R> &out, double &cfl_cand,
-                                          int variant = 0)
+                                          int variant = 0, R ev_n = R(0), R ev_p = R(0), R vel_div = R(1))
 {
     const R half = R(0.5);
     const double half_gravity = (double)(half * K<R>::gravity());
@@ -159,14 +176,34 @@ __device__ __forceinline__ void edge_flux(const Cell<R> &cn, const Grad<R> &gn, 
     const R qt_neg = NS ? ud_neg : vd_neg, qt_pos = NS ? ud_pos : vd_pos;
     const R f_mass = R((double)((s_max * qn_neg - s_min * qn_pos) + sminsmax * (stage_pos_star - stage_neg_star)) *
                        inv_denom);
-    const R f_norm = R((double)((s_max * qn_neg * vel_beta_neg - s_min * qn_pos * vel_beta_pos) +
-                                fr2 * sminsmax * (qn_pos - qn_neg)) * inv_denom);
-    R f_tran;
-    if (variant & FLUX_UPWIND_TRANSVERSE)   // upwind_transverse_momentum: the transverse velocity upwind of the mass flux
-        f_tran = beta * ((f_mass > R(0)) ? (NS ? u_neg : v_neg) : (NS ? u_pos : v_pos)) * f_mass;
-    else
-        f_tran = R((double)((s_max * qt_neg * vel_beta_neg - s_min * qt_pos * vel_beta_pos) +
-                            fr2 * sminsmax * (qt_pos - qt_neg)) * inv_denom);
+    R f_norm, f_tran;
+    if (!EDDY) {
+        f_norm = R((double)((s_max * qn_neg * vel_beta_neg - s_min * qn_pos * vel_beta_pos) +
+                            fr2 * sminsmax * (qn_pos - qn_neg)) * inv_denom);
+        if (variant & FLUX_UPWIND_TRANSVERSE)   // upwind_transverse_momentum: the transverse velocity upwind of the mass flux
+            f_tran = beta * ((f_mass > R(0)) ? (NS ? u_neg : v_neg) : (NS ? u_pos : v_pos)) * f_mass;
+        else
+            f_tran = R((double)((s_max * qt_neg * vel_beta_neg - s_min * qt_pos * vel_beta_pos) +
+                                fr2 * sminsmax * (qt_pos - qt_neg)) * inv_denom);
+    } else {
+        // turbulent diffusion: eddy_visc * depth * edge length * velocity gradient,
+        // with the geometric mean of the edge depths
+        const R evh = half * (ev_p + ev_n);
+        const R gdep = R(sqrt(depth_neg_star * depth_pos_star));
+        R adv = R((double)(s_max * qn_neg * vel_beta_neg - s_min * qn_pos * vel_beta_pos) * inv_denom);
+        R hll = R((double)(fr2 * sminsmax * (qn_pos - qn_neg)) * inv_denom);
+        R turb = -(evh * gdep * edge_len * ((NS ? (cp.v - cn.v) : (cp.u - cn.u)) / vel_div));
+        f_norm = eddy_momentum_flux<R>(adv, hll, turb);
+        if (variant & FLUX_UPWIND_TRANSVERSE) {
+            adv = beta * ((f_mass > R(0)) ? (NS ? u_neg : v_neg) : (NS ? u_pos : v_pos)) * f_mass;
+            hll = R(0);
+        } else {
+            adv = R((double)(s_max * qt_neg * vel_beta_neg - s_min * qt_pos * vel_beta_pos) * inv_denom);
+            hll = R((double)(fr2 * sminsmax * (qt_pos - qt_neg)) * inv_denom);
+        }
+        turb = -(evh * gdep * edge_len * ((NS ? (cp.u - cn.u) : (cp.v - cn.v)) / vel_div));
+        f_tran = eddy_momentum_flux<R>(adv, hll, turb);
+    }
     out.f[0] = f_mass;
     out.f[1] = NS ? f_tran : f_norm;
     out.f[2] = NS ? f_norm : f_tran;

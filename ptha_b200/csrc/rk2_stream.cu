@@ -102,7 +102,7 @@ __device__ __forceinline__ void zero_edge(EdgeRes<R> &e)
     e.f[0] = R(0); e.f[1] = R(0); e.f[2] = R(0); e.es_pos = 0.0; e.es_neg = 0.0;
 }
 
-template <typename R, int MODE, bool SPH, bool COR, int FRIC, int SH>
+template <typename R, int MODE, bool SPH, bool COR, int FRIC, int SH, bool EDDY>
 __global__ void __launch_bounds__(SLANES *SWARPS, 4) rk2_stream_kernel(const Rk2Args<R> a)
 {
     const int lane = threadIdx.x & 31;
@@ -171,7 +171,9 @@ __global__ void __launch_bounds__(SLANES *SWARPS, 4) rk2_stream_kernel(const Rk2
             const int e = r - 1;
             if (e >= 1 && e <= ny - 1 && i >= 1 && i <= nx - 1) {
                 double cand;
-                edge_flux<R, true>(c2, g2, c1, g1, a.m.dxb[e], inv2, e_n, cand, a.flux_variant);
+                edge_flux<R, true, EDDY>(c2, g2, c1, g1, a.m.dxb[e], inv2, e_n, cand, a.flux_variant,
+                                         EDDY ? a.ev[(int64_t)(e - 1) * a.P + i] : R(0),
+                                         EDDY ? a.ev[(int64_t)e * a.P + i] : R(0), EDDY ? a.m.dyl[i] : R(1));
                 cfl = fmax(cfl, cand);
                 if (MODE != MODE_CFL && a.lines && i >= a.n_ext && i <= nx - a.n_ext - 1) {
                     if (e == ny - a.n_ext) a.lines[i] = (double)e_n.f[0];
@@ -200,7 +202,10 @@ __global__ void __launch_bounds__(SLANES *SWARPS, 4) rk2_stream_kernel(const Rk2
         if (ew_lane && i >= 1 && i <= nx - 1 && R_ >= 1 && R_ <= ny - 1) {
             const R inv1 = R(1) / (a.m.dxb[R_] * a.half_cfl);  // dx_cfl_half_inv(1): EW edges
             double cand;
-            edge_flux<R, false>(cl, gw, c2, gew, a.m.dyl[i], inv1, e_w, cand, a.flux_variant);
+            const int64_t oe = (int64_t)R_ * a.P + i;
+            edge_flux<R, false, EDDY>(cl, gw, c2, gew, a.m.dyl[i], inv1, e_w, cand, a.flux_variant,
+                                      EDDY ? a.ev[oe - 1] : R(0), EDDY ? a.ev[oe] : R(0),
+                                      EDDY ? R(0.5) * (a.m.dxb[R_] + a.m.dxb[R_ + 1]) : R(1));
             cfl = fmax(cfl, cand);
             if (MODE != MODE_CFL && a.lines && R_ >= a.n_ext && R_ <= ny - a.n_ext - 1) {
                 if (i == nx - a.n_ext) a.lines[nx + R_] = (double)e_w.f[0];
@@ -245,7 +250,13 @@ cudaError_t launch_stage_stream(const Rk2Args<R> &a, cudaStream_t s)
     const int strips_y = (a.ny + SH - 1) / SH;
     const int warps = strips_x * strips_y;
     const int blocks = (warps + SWARPS - 1) / SWARPS;
-    rk2_stream_kernel<R, MODE, SPH, COR, FRIC, SH><<<blocks, SLANES * SWARPS, 0, s>>>(a);
+    if constexpr (MODE != MODE_CFL) {
+        if (a.flux_variant & FLUX_EDDY) {
+            rk2_stream_kernel<R, MODE, SPH, COR, FRIC, SH, true><<<blocks, SLANES * SWARPS, 0, s>>>(a);
+            return cudaGetLastError();
+        }
+    }
+    rk2_stream_kernel<R, MODE, SPH, COR, FRIC, SH, false><<<blocks, SLANES * SWARPS, 0, s>>>(a);
     return cudaGetLastError();
 }
 

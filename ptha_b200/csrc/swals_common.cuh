@@ -73,6 +73,36 @@ __device__ __forceinline__ double pow_friction_cr(double x)
     return dd_fast_two_sum(v.hi, v.lo + v.hi * tl).hi;
 }
 
+// Correctly rounded depth**p, p = fl(1 - 1/6), of the Shiono-Knight eddy
+// viscosity (compute_fluxes_DE1_inner_include.f90:1000-1002), depth >= 0.
+// Double-double arithmetic: the Newton-corrected cube root, its
+// Newton-corrected square root (x**(1/6)), the compensated quotient
+// x / x**(1/6), and the factor x**eps = 1 + eps*ln(x), eps = p - 5/6.  The
+// oracle evaluates the same definition (checked there against 300-bit
+// arithmetic).
+__device__ __forceinline__ double pow_eddy_cr(double x)
+{
+    if (x == 0.0) return 0.0;
+    const double c0 = cbrt(x);
+    const DD s = dd_two_prod(c0, c0);
+    DD t = dd_two_prod(s.hi, c0);
+    t.lo += s.lo * c0;
+    const double r = (x - t.hi) - t.lo;
+    const DD c = dd_fast_two_sum(c0, r / (3.0 * c0 * c0));
+    const double q0 = sqrt(c.hi);
+    const DD q2 = dd_two_prod(q0, q0);
+    const double rq = ((c.hi - q2.hi) - q2.lo) + c.lo;
+    const DD q = dd_fast_two_sum(q0, rq / (2.0 * q0));
+    const double y0 = x / q.hi;
+    DD pq = dd_two_prod(y0, q.hi);
+    pq.lo += y0 * q.lo;
+    const DD y = dd_fast_two_sum(y0, ((x - pq.hi) - pq.lo) / q.hi);
+    const double p = 1.0 - 1.0 / 6.0;
+    const double eps = fma(p, 6.0, -5.0) / 6.0;
+    const double tl = eps * log(x);
+    return dd_fast_two_sum(y.hi, y.lo + y.hi * tl).hi;
+}
+
 // Correctly rounded cosh for the device boundary functions, in double-double
 // arithmetic: a = k ln2 + r with a double-double ln2 and |r| <= ln2/2,
 // exp(r) by the Horner form of its Taylor series to r^22/22!, exp(-|a|) by a

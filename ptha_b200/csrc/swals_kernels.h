@@ -41,7 +41,8 @@ struct StepPlanes {
 // UPWIND_TRANSVERSE.
 enum {
     FLUX_PLAIN_DIFFUSION = 1,    // reduced_momentum_diffusion = .false. (fr2 = 1)
-    FLUX_UPWIND_TRANSVERSE = 2   // upwind_transverse_momentum = .true.
+    FLUX_UPWIND_TRANSVERSE = 2,  // upwind_transverse_momentum = .true.
+    FLUX_EDDY = 4                // use_eddy_viscosity (the *_eddyvisc variants)
 };
 
 // forcing_patch_type (forcing_mod.f90:23-53) on the device: a 0-based
@@ -83,6 +84,8 @@ struct StepConfig {
     void *nl_work;          // leapfrog_nonlinear: 9 work planes of pitch x (ny + 1)
     int n_forcing;          // forcing patches, applied in order (apply_forcing_patch_array)
     const ForcingPatch *forcing;
+    void *eddy_visc;        // use_eddy_viscosity: one plane of per-cell eddy viscosity, else null
+    double eddy_visc_constants[2];  // domain%eddy_visc_constants (constant, Shiono-Knight)
 };
 
 // Forcing patches (forcing.cu): add each active patch's share of its

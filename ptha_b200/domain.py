@@ -233,6 +233,16 @@ class Domain:
         """domain%apply_forcing(dt) on the current state at domain%time."""
         check(self._L.swals_gpu_apply_forcing(self._h, float(dt)))
 
+    def set_eddy_viscosity(self, constant, shiono_knight=0.0):
+        """domain%use_eddy_viscosity = .true. with eddy_visc_constants =
+        [constant, shiono_knight]: the *_eddyvisc flux variants, with a
+        constant (shiono_knight = 0) or constant + Shiono-Knight viscosity.
+        Finite-volume methods only."""
+        check(self._L.swals_gpu_set_eddy_viscosity(self._h, 1, float(constant), float(shiono_knight)))
+
+    def clear_eddy_viscosity(self):
+        check(self._L.swals_gpu_set_eddy_viscosity(self._h, 0, 0.0, 0.0))
+
     GRID_VARS = {"stage": 1, "uh": 2, "vh": 4, "elevation": 8, "max_stage": 16}
 
     def stage_grids_real4(self, variables=("stage", "uh", "vh", "elevation"), spatial_stride=1):

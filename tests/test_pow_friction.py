@@ -41,3 +41,21 @@ def test_boundary_cosh_is_correctly_rounded():
         want = float(mpmath.cosh(mpmath.mpf(a)))
         assert f(a) == want, (a, f(a), want)
     assert f(0.0) == 1.0
+
+
+def test_pow_eddy_is_correctly_rounded():
+    """depth**(1 - 1/6) of the Shiono-Knight eddy viscosity
+    (compute_fluxes_DE1_inner_include.f90:1000-1002), correctly rounded."""
+    lib = orc._load(False)
+    f = lib.oracle64_pow_eddy
+    f.restype = ctypes.c_double
+    f.argtypes = [ctypes.c_double]
+    mpmath.mp.prec = 300
+    p = mpmath.mpf(1.0 - 1.0 / 6.0)
+    rng = random.Random(4321)
+    for k in range(20000):
+        u = rng.random()
+        x = 1e-8 * 10 ** (12 * u) if k % 2 else 100 * u
+        want = float(mpmath.power(mpmath.mpf(x), p))
+        assert f(x) == want, (x, f(x), want)
+    assert f(0.0) == 0.0
