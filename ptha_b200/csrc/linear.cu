@@ -473,12 +473,11 @@ __global__ void __launch_bounds__(128, LIN_MINB) linear_async_kernel(const LinAr
             }
             cp_async_commit();
         };
-        auto stage_new = [&](int r, R s_old, R uh_r, R uh_w, R vh_r, R vh_s) -> R {
+        auto stage_new = [&](int r, R s_old, R uh_r, R uh_w, R vh_r, R vh_s, R inv_cell_area_dt) -> R {
             R sn = R(0);
             if (r < ny && in_x) {
                 const bool interior = (i >= a.xl + 1) && (i <= a.xu - 1) && (r >= a.yl + 1) && (r <= a.yu - 1);
                 if (interior) {
-                    const R inv_cell_area_dt = a.dt / a.m.area[r];
                     const R t1 = (uh_r - uh_w) * dyl_i;
                     const R t2 = vh_r * a.m.dxb[r + 1] - vh_s * a.m.dxb[r];
                     sn = s_old - inv_cell_area_dt * (t1 + t2);
@@ -505,10 +504,27 @@ __global__ void __launch_bounds__(128, LIN_MINB) linear_async_kernel(const LinAr
         R sn_j;
         {
             const R uh_w = __shfl_up_sync(FULL, uh_j, 1);
-            sn_j = stage_new(ra, st_j, uh_j, uh_w, vh_j, vh_jm1);
+            sn_j = stage_new(ra, st_j, uh_j, uh_w, vh_j, vh_jm1, a.dt / a.m.area[ra]);
         }
+        // The row factors dt/area (the new stage, row j+1) and g dt/area,
+        // g dt/mean area (the momenta, row j) are the same in every lane:
+        // lane L evaluates them for row jb + L of each 32-row chunk and the
+        // rows take them by shuffle, one division per chunk instead of three
+        // per row.
+        R rc_s = R(0), rc_u = R(0), rc_v = R(0);
         for (int j = ra; j < rb; j++) {
             const int k = j - ra + 2;  // row j+1
+            if (((j - ra) & 31) == 0) {
+                const int rr = min(j + lane, ny - 1);
+                const int rs = min(j + 1 + lane, ny - 1);
+                rc_s = a.dt / a.m.area[rs];
+                rc_u = g * a.dt / a.m.area[rr];
+                rc_v = g * a.dt / (half * (a.m.area[rr] + a.m.area[min(rr + 1, ny - 1)]));
+            }
+            const int rl = (j - ra) & 31;
+            const R inv_cell_area_dt_n = __shfl_sync(FULL, rc_s, rl);
+            const R inv_cell_area_dt_g = __shfl_sync(FULL, rc_u, rl);
+            const R inv_cell_area_dt_vh_g = __shfl_sync(FULL, rc_v, rl);
             cp_async_wait<AD - 2>();
             const int slot = k % AD;
             const R uh_n = rg[slot][0][lane], vh_n = rg[slot][1][lane], st_n = rg[slot][2][lane];
@@ -517,7 +533,7 @@ __global__ void __launch_bounds__(128, LIN_MINB) linear_async_kernel(const LinAr
             const bool in_ms = max_stage && out && i >= a.xl && i <= a.xu && j >= a.yl && j <= a.yu;
 
             const R uh_nw = __shfl_up_sync(FULL, uh_n, 1);
-            const R sn_n = stage_new(j + 1, st_n, uh_n, uh_nw, vh_n, vh_j);
+            const R sn_n = stage_new(j + 1, st_n, uh_n, uh_nw, vh_n, vh_j, inv_cell_area_dt_n);
 
             const R s_e = __shfl_down_sync(FULL, sn_j, 1);
             const R e_e = __shfl_down_sync(FULL, e_j, 1);
@@ -541,8 +557,6 @@ __global__ void __launch_bounds__(128, LIN_MINB) linear_async_kernel(const LinAr
                 if (in_ms) max_stage[o] = (sn_j > mx) ? sn_j : mx;
                 R uh = uh_j, vh = vh_j;
                 if (i >= a.xl && i <= a.xu - 1 && j >= a.yl && j <= a.yu - 1) {
-                    const R inv_cell_area_dt_g = g * a.dt / a.m.area[j];
-                    const R inv_cell_area_dt_vh_g = g * a.dt / (half * (a.m.area[j] + a.m.area[j + 1]));
                     const R e0 = e_j;
                     const R sn = sn_j, s_n = sn_n;
                     R h_iph, h_jph, wet_iph, wet_jph;

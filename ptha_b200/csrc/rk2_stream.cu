@@ -25,7 +25,20 @@ using namespace fv;
 
 constexpr int SLANES = 32;
 constexpr int SOUT = 28;    // output columns per warp
-constexpr int SWARPS = 4;   // warps per CTA
+#ifndef SWALS_STREAM_WARPS
+#define SWALS_STREAM_WARPS 4
+#endif
+constexpr int SWARPS = SWALS_STREAM_WARPS;   // warps per CTA
+#ifndef SWALS_STREAM_MIN_CTAS
+#define SWALS_STREAM_MIN_CTAS 4  // CTAs per SM the register cap is sized for
+#endif
+#ifndef SWALS_STREAM_ROWS
+// Rows per warp strip.  Measured on the 2048^2 rk2 step (B200): 12 rows
+// beat 32 by 4 % despite the larger share of the two lead-in rows, as the
+// more numerous, shorter strips balance better over the SMs; more CTAs
+// per SM (a lower register cap) spill and lose 15-25 %.
+#define SWALS_STREAM_ROWS 12
+#endif
 constexpr unsigned FULL = 0xffffffffu;
 
 template <typename R> struct Raw { R s, uh, vh, e; };
@@ -103,7 +116,7 @@ __device__ __forceinline__ void zero_edge(EdgeRes<R> &e)
 }
 
 template <typename R, int MODE, bool SPH, bool COR, int FRIC, int SH, bool EDDY>
-__global__ void __launch_bounds__(SLANES *SWARPS, 4) rk2_stream_kernel(const Rk2Args<R> a)
+__global__ void __launch_bounds__(SLANES *SWARPS, SWALS_STREAM_MIN_CTAS) rk2_stream_kernel(const Rk2Args<R> a)
 {
     const int lane = threadIdx.x & 31;
     const int wid = blockIdx.x * SWARPS + (threadIdx.x >> 5);
@@ -245,7 +258,7 @@ __global__ void __launch_bounds__(SLANES *SWARPS, 4) rk2_stream_kernel(const Rk2
 template <typename R, int MODE, bool SPH, bool COR, int FRIC>
 cudaError_t launch_stage_stream(const Rk2Args<R> &a, cudaStream_t s)
 {
-    constexpr int SH = 32;
+    constexpr int SH = SWALS_STREAM_ROWS;
     const int strips_x = (a.nx + SOUT - 1) / SOUT;
     const int strips_y = (a.ny + SH - 1) / SH;
     const int warps = strips_x * strips_y;
