@@ -373,8 +373,6 @@ int swals_gpu_domain_create(const swals_domain_desc *desc, swals_domain **out)
         return fail(SWALS_ERR_INVALID_ARGUMENT, "unknown boundary_kind %d", desc->boundary_kind);
     if (desc->boundary_function_kind < 0 || desc->boundary_function_kind > 1)
         return fail(SWALS_ERR_UNSUPPORTED_CALLBACK, "unknown boundary_function_kind %d", desc->boundary_function_kind);
-    if (method == M_LF_NONLINEAR && desc->boundary_kind == SWALS_BC_FLATHER)
-        return fail(SWALS_ERR_UNSUPPORTED, "flather_boundary with leapfrog_nonlinear is not implemented");
     if (is_staggered(method) && desc->boundary_kind == SWALS_BC_FLATHER && desc->exterior_cells_width == 1)
         return fail(SWALS_ERR_UNSUPPORTED, "flather_boundary with the linear solver needs exterior_cells_width >= 2");
     if (is_staggered(method) && desc->boundary_kind == SWALS_BC_TRANSMISSIVE)

@@ -1586,6 +1586,11 @@ cudaError_t launch_leapfrog_nonlinear_step(const StepPlanes<R> &p, const Metrics
     run(CAT_LINEAR_EDGE, [&] { nl::lag0_kernel<R><<<g1, block, 0, s>>>(n); });
     run(CAT_LINEAR_EDGE, [&] { linear_edge_kernel<R><<<1, 512, 0, s>>>(a, sc, c.exterior_cells_width, c.bf); });
     run(CAT_LINEAR_MAIN, [&] { nl::stage_kernel<R><<<g1, block, 0, s>>>(n); });
+    if (c.bc_kind == 3)   // flather_boundary
+        run(CAT_LINEAR_EDGE, [&] {
+            launch_leapfrog_boundary<R>(p.nx, p.ny, p.pitch, p.stg_o, const_cast<R *>(p.uh), const_cast<R *>(p.vh),
+                                        p.elv, m, c, dt, sc, s);
+        });
     if (c.n_forcing) {
         ForcingClock clk{};
         clk.mode = FORCE_LEAPFROG;

@@ -280,6 +280,7 @@ struct BcArgs {
     int n_dt;               // boundary time = time0 + n_dt * dt (n_dt additions) ...
     R dt_extra;             // ... + dt * dt_extra when nonzero (midpoint half step, rk2n last step)
     DevScalars *sc;
+    int leapfrog_half;      // a leapfrog step's boundary: time = time0 + dt/2 (dt = dt_fixed)
 };
 
 template <typename R> struct RingVal { R s, uh, vh, e; };
@@ -348,9 +349,14 @@ __global__ void __launch_bounds__(256) rk2_boundary_kernel(const BcArgs<R> a)
     } else {
         dtd = (double)R(a.dt_fixed);
     }
-    double t = a.sc->time;
-    for (int k = 0; k < a.n_dt; k++) t = t + dtd;
-    if (a.dt_extra != R(0)) t = t + (double)(R(dtd) * a.dt_extra);
+    double t;
+    if (a.leapfrog_half) {
+        t = a.sc->time0 + (double)(R(dtd) * K<R>::half());
+    } else {
+        t = a.sc->time;
+        for (int k = 0; k < a.n_dt; k++) t = t + dtd;
+        if (a.dt_extra != R(0)) t = t + (double)(R(dtd) * a.dt_extra);
+    }
 
     RingVal<R> v;
     if (sn) {
@@ -827,6 +833,7 @@ BcArgs<R> bc_args(const Rk2Args<R> &a, const StepConfig &c, double dt)
     b.stg0 = nullptr; b.uh0 = nullptr; b.vh0 = nullptr;
     b.n_dt = 1;
     b.stage_mode = 1;
+    b.leapfrog_half = 0;
     return b;
 }
 
@@ -1194,5 +1201,33 @@ template cudaError_t launch_rk2_step<float>(float *const[3][3], int &, float *, 
                                             int64_t, const Metrics<float> &, const StepConfig &, bool, double,
                                             bool, const Rk2Buffers &, DevScalars *, cudaStream_t,
                                             const LaunchHook &);
+
+// update_boundary after the stage sweep of 'leapfrog_nonlinear'
+// (domain_mod_leapfrog_nonlinear_include.f90:122-140) for flather_boundary:
+// the ring of the new stage and of the (not yet updated) momenta, in place,
+// at time0 + dt/2, by the finite-volume boundary kernel (west/east pass,
+// then south/north with the corners from the first).
+template <typename R>
+cudaError_t launch_leapfrog_boundary(int nx, int ny, int64_t pitch, R *stg, R *uh, R *vh, R *elv, const Metrics<R> &m,
+                                     const StepConfig &c, R dt, DevScalars *sc, cudaStream_t s)
+{
+    BcArgs<R> b;
+    b.nx = nx; b.ny = ny; b.P = pitch; b.kind = c.bc_kind;
+    for (int k = 0; k < 4; k++) b.bext[k] = c.bext[k];
+    b.bf = c.bf; b.msl = R(c.msl_linear); b.x = m.x;
+    b.stg = stg; b.uh = uh; b.vh = vh; b.elv = elv;
+    b.stg0 = nullptr; b.uh0 = nullptr; b.vh0 = nullptr; b.side = nullptr; b.max_stage = nullptr;
+    b.stage_mode = 1;
+    b.dt_from_cfl = 0; b.dt_fixed = (double)dt; b.max_dt_inv_init = 0.0;
+    b.n_dt = 0; b.dt_extra = R(0); b.sc = sc;
+    b.leapfrog_half = 1;
+    return launch_boundary<R>(b, s);
+}
+template cudaError_t launch_leapfrog_boundary<double>(int, int, int64_t, double *, double *, double *, double *,
+                                                      const Metrics<double> &, const StepConfig &, double,
+                                                      DevScalars *, cudaStream_t);
+template cudaError_t launch_leapfrog_boundary<float>(int, int, int64_t, float *, float *, float *, float *,
+                                                     const Metrics<float> &, const StepConfig &, float, DevScalars *,
+                                                     cudaStream_t);
 
 }  // namespace swals

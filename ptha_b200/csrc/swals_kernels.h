@@ -137,6 +137,10 @@ cudaError_t launch_linear_step(const StepPlanes<R> &p, const Metrics<R> &m, cons
                                R dt, DevScalars *sc, cudaStream_t s, const LaunchHook &hook,
                                const AuxStream *aux = nullptr);
 // one_leapfrog_nonlinear_step (domain_mod_leapfrog_nonlinear_include.f90).
+// flather_boundary on the ring after a leapfrog_nonlinear stage sweep (rk2.cu).
+template <typename R>
+cudaError_t launch_leapfrog_boundary(int nx, int ny, int64_t pitch, R *stg, R *uh, R *vh, R *elv, const Metrics<R> &m,
+                                     const StepConfig &c, R dt, DevScalars *sc, cudaStream_t s);
 template <typename R>
 cudaError_t launch_leapfrog_nonlinear_step(const StepPlanes<R> &p, const Metrics<R> &m, const StepConfig &c, R dt,
                                            DevScalars *sc, cudaStream_t s, const LaunchHook &hook);

@@ -93,3 +93,32 @@ def test_nest_with_rk2_child():
     md, omd = _run_pair(specs, wetdry=False, nsteps=6)
     assert md.time == pytest.approx(omd.time)
     md.close()
+
+
+def test_flather_open_basin():
+    """flather_boundary through update_boundary after the stage sweep
+    (domain_mod_leapfrog_nonlinear_include.f90:122-140): an open basin with
+    a beach on the north edge (some ring cells dry), at half the CFL limit."""
+    from test_flather_gpu import open_basin
+    kw, U = open_basin(n=90, dx=1000.0, depth=200.0, method=M)
+    g, o = make_pair(kw, U, manning_sq=np.full(U[0].shape, 0.025 ** 2))
+    dt = 0.5 * o.linear_timestep_max()
+    for _ in range(150):
+        g.evolve_one_step(dt)
+        o.evolve_one_step(dt)
+    _exact(g, o, "nl flather")
+
+
+def test_flather_solitary_west():
+    """Flather on the west edge with the solitary wave as the outside state."""
+    from ptha_b200 import _lib
+    kw, U, _, nsq = workloads.rk2_beach(n=96, dx=10.0 * 2048 / 96, toe=17580.0 * 96 / 2048)
+    kw = dict(kw, timestepping_method=M, boundary_kind=_lib.BC_FLATHER, boundary_exterior=(False, False, False, True))
+    g, o = make_pair(kw, U, manning_sq=nsq)
+    dt = 0.25 * o.linear_timestep_max()
+    for _ in range(400):
+        g.evolve_one_step(dt)
+        o.evolve_one_step(dt)
+    _exact(g, o, "nl flather solitary")
+    wet = o.U[3][1:-1, 1:20] < -5.0
+    assert np.max(o.U[0][1:-1, 1:20][wet]) > 0.02   # the wave came in
