@@ -278,6 +278,52 @@ typedef struct swals_nest_exchange {
     int32_t recv_box[4];
 } swals_nest_exchange;
 
+/* The nesting metadata builder: setup_multidomain + setup_multidomain_domains
+ * for one image (multidomain_mod.f90:2663-3553), natively.  In: each
+ * domain's interior extent, method, refinement factor, minimum nesting layer
+ * thickness, use_eddy_viscosity and interior bounding box (all zero: the
+ * extent's rectangle, create_all_bbox_and_dx :960-1060).  Out, written into
+ * the same structs: the widened extent (lower_left, lw, nx grow by
+ * nest_layer_width on each nesting boundary, :2860-2895), nest_layer_width,
+ * is_nesting_boundary (N, E, S, W) and max_parent_dx_ratio; and a metadata
+ * object with every domain's priority_domain_index / image and recv_metadata
+ * rows, and the exchanges in the reference's receive order. */
+typedef struct swals_nest_domain_desc {
+    double  lower_left[2];
+    double  lw[2];
+    int32_t nx[2];
+    int32_t timestepping_refinement_factor;
+    int32_t minimum_nesting_layer_thickness;
+    int32_t use_eddy_viscosity;
+    int32_t nest_layer_width;          /* out */
+    int32_t is_nesting_boundary[4];    /* out: N, E, S, W */
+    double  max_parent_dx_ratio;       /* out */
+    double  interior_bounding_box[8];  /* ll, lr, ur, ul (x, y); in/out */
+    char    timestepping_method[64];
+} swals_nest_domain_desc;
+
+typedef struct swals_md_exchange {
+    int32_t sender, receiver;
+    int32_t send_box[4];
+    int32_t recv_box[4];
+    int32_t recv_row, send_row;        /* 0-based rows of recv_metadata / send_metadata */
+} swals_md_exchange;
+
+typedef struct swals_md_metadata swals_md_metadata;
+
+/* periodic_xs / periodic_ys: the periodic extent (NULL: none). */
+int swals_md_build_metadata(swals_nest_domain_desc *domains, int32_t n, int32_t extra_halo_buffer,
+                            int32_t extra_cells_in_halo, const double periodic_xs[2], const double periodic_ys[2],
+                            swals_md_metadata **out);
+/* count = number of exchanges; out (capacity entries, or NULL to query). */
+int swals_md_metadata_exchanges(const swals_md_metadata *m, swals_md_exchange *out, int32_t capacity, int32_t *count);
+/* priority_domain_index / image of a domain (nx*ny of its widened extent, column-major). */
+int swals_md_metadata_priority(const swals_md_metadata *m, int32_t domain, int32_t *index_out, int32_t *image_out);
+/* recv_metadata rows (ind, img, iL, iU, jL, jU) of a domain. */
+int swals_md_metadata_recv_boxes(const swals_md_metadata *m, int32_t domain, int64_t *rows_out, int32_t capacity,
+                                 int32_t *count);
+void swals_md_metadata_free(swals_md_metadata *m);
+
 /* Create a multidomain over `ndomains` (<= 16) domains on one device, with
  * all_dx (2 per domain: the cell sizes setup recorded before widening the
  * domains, all_dx_md of multidomain_mod.f90:960-1060; NULL: lw/nx of each

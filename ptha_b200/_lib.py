@@ -46,6 +46,8 @@ EXPORTED = [
     "swals_gpu_set_priority_mask", "swals_gpu_domain_statistics", "swals_gpu_volume_in_priority_domain",
     "swals_gpu_forcing_patch_add", "swals_gpu_forcing_clear", "swals_gpu_apply_forcing",
     "swals_gpu_set_eddy_viscosity",
+    "swals_md_build_metadata", "swals_md_metadata_exchanges", "swals_md_metadata_priority",
+    "swals_md_metadata_recv_boxes", "swals_md_metadata_free",
     "swals_gpu_stage_grids_real4", "swals_gpu_gauges_read_real4",
 ]
 TIMER_NAMES = ["cfl", "fv_stage1", "boundary1", "fv_stage2", "boundary2", "finalize", "leapfrog_edge",
@@ -161,6 +163,10 @@ def lib():
         "swals_gpu_forcing_patch_add": [vp, i32, i32, i32, i32, i32, i32, dbl, dbl, vp, ctypes.POINTER(i32)],
         "swals_gpu_forcing_clear": [vp], "swals_gpu_apply_forcing": [vp, dbl],
         "swals_gpu_set_eddy_viscosity": [vp, i32, dbl, dbl],
+        "swals_md_build_metadata": [vp, i32, i32, i32, vp, vp, ctypes.POINTER(vp)],
+        "swals_md_metadata_exchanges": [vp, vp, i32, ctypes.POINTER(i32)],
+        "swals_md_metadata_priority": [vp, i32, vp, vp],
+        "swals_md_metadata_recv_boxes": [vp, i32, vp, i32, ctypes.POINTER(i32)],
         "swals_gpu_stage_grids_real4": [vp, i32, i32, vp, i64, vp],
         "swals_gpu_gauges_read_real4": [vp, vp, i32, ctypes.POINTER(i32)],
     }
@@ -168,6 +174,8 @@ def lib():
         f = getattr(L, name)
         f.argtypes = args
         f.restype = ctypes.c_int
+    L.swals_md_metadata_free.argtypes = [vp]
+    L.swals_md_metadata_free.restype = None
     L.swals_gpu_version.restype = ctypes.c_char_p
     L.swals_gpu_version.argtypes = []
     _lib = L

@@ -19,7 +19,7 @@ from . import _lib
 from ._lib import check
 from .domain import Domain
 from .nesting import (EXTRA_CELLS_IN_HALO_DEFAULT, EXTRA_HALO_BUFFER_DEFAULT, HUGE, Exchange, NestDomain,
-                      setup_multidomain)
+                      setup_multidomain_native)
 
 
 class Multidomain:
@@ -37,8 +37,10 @@ class Multidomain:
                  extra_cells_in_halo: int = EXTRA_CELLS_IN_HALO_DEFAULT, use_wetdry_limiting: bool = True,
                  flux_correction: bool = True, periodic_xs=(-HUGE, HUGE), periodic_ys=(-HUGE, HUGE), device=-1):
         self.specs = list(specs)
-        self.exchanges: List[Exchange] = setup_multidomain(self.specs, extra_halo_buffer, extra_cells_in_halo,
-                                                           periodic_xs, periodic_ys)
+        # the library's native metadata builder (the numpy restatement in
+        # nesting.setup_multidomain gives the same tables)
+        self.exchanges: List[Exchange] = setup_multidomain_native(self.specs, extra_halo_buffer, extra_cells_in_halo,
+                                                                  periodic_xs, periodic_ys)
         kw = list(domain_kwargs) if domain_kwargs is not None else [{} for _ in self.specs]
         self.domains: List[Domain] = []
         for s, k in zip(self.specs, kw):

@@ -25,6 +25,7 @@ own known answers for its 4-domain nest are in ``tests/golden``).
 """
 from __future__ import annotations
 
+import ctypes
 import math
 from dataclasses import dataclass, field
 from fractions import Fraction
@@ -450,6 +451,79 @@ def setup_multidomain(domains: Sequence[NestDomain], extra_halo_buffer: int = EX
                                       recv_box=(int(b[2]), int(b[3]), int(b[4]), int(b[5])),
                                       recv_row=i, send_row=srow))
     return exchanges
+
+
+class _NestDomainDesc(ctypes.Structure):
+    """swals_nest_domain_desc (include/swals_gpu.h)."""
+    _fields_ = [("lower_left", ctypes.c_double * 2), ("lw", ctypes.c_double * 2), ("nx", ctypes.c_int32 * 2),
+                ("timestepping_refinement_factor", ctypes.c_int32),
+                ("minimum_nesting_layer_thickness", ctypes.c_int32), ("use_eddy_viscosity", ctypes.c_int32),
+                ("nest_layer_width", ctypes.c_int32), ("is_nesting_boundary", ctypes.c_int32 * 4),
+                ("max_parent_dx_ratio", ctypes.c_double), ("interior_bounding_box", ctypes.c_double * 8),
+                ("timestepping_method", ctypes.c_char * 64)]
+
+
+class _MdExchange(ctypes.Structure):
+    _fields_ = [("sender", ctypes.c_int32), ("receiver", ctypes.c_int32), ("send_box", ctypes.c_int32 * 4),
+                ("recv_box", ctypes.c_int32 * 4), ("recv_row", ctypes.c_int32), ("send_row", ctypes.c_int32)]
+
+
+def setup_multidomain_native(domains: Sequence[NestDomain], extra_halo_buffer: int = EXTRA_HALO_BUFFER_DEFAULT,
+                             extra_cells_in_halo: int = EXTRA_CELLS_IN_HALO_DEFAULT,
+                             periodic_xs=(-HUGE, HUGE), periodic_ys=(-HUGE, HUGE)) -> List[Exchange]:
+    """setup_multidomain through the library's native builder
+    (swals_md_build_metadata): the same fields of the domains are set and the
+    same exchanges returned as by setup_multidomain (send_metadata is not
+    kept)."""
+    from . import _lib
+    L = _lib.lib()
+    n = len(domains)
+    descs = (_NestDomainDesc * n)()
+    for c, d in zip(descs, domains):
+        c.lower_left[:] = [float(v) for v in d.lower_left]
+        c.lw[:] = [float(v) for v in d.lw]
+        c.nx[:] = [int(v) for v in d.nx]
+        c.timestepping_refinement_factor = int(d.timestepping_refinement_factor)
+        c.minimum_nesting_layer_thickness = int(d.minimum_nesting_layer_thickness)
+        c.use_eddy_viscosity = int(bool(d.use_eddy_viscosity))
+        if d.interior_bounding_box is not None:
+            c.interior_bounding_box[:] = [float(v) for v in np.asarray(d.interior_bounding_box).reshape(-1)]
+        c.timestepping_method = d.timestepping_method.encode()
+    handle = ctypes.c_void_p()
+    pxs = (ctypes.c_double * 2)(*periodic_xs)
+    pys = (ctypes.c_double * 2)(*periodic_ys)
+    _lib.check(L.swals_md_build_metadata(descs, n, int(extra_halo_buffer), int(extra_cells_in_halo), pxs, pys,
+                                         ctypes.byref(handle)))
+    try:
+        for c, d in zip(descs, domains):
+            d.dx = (d.lw[0] / (1.0 * d.nx[0]), d.lw[1] / (1.0 * d.nx[1]))   # before widening, as setup records it
+            d.interior_bounding_box = np.array(c.interior_bounding_box[:], dtype=np.float64).reshape(4, 2)
+            d.max_parent_dx_ratio = float(c.max_parent_dx_ratio)
+            d.is_nesting_boundary = tuple(bool(v) for v in c.is_nesting_boundary)
+            d.nest_layer_width = int(c.nest_layer_width)
+            d.lower_left, d.lw, d.nx = tuple(c.lower_left[:]), tuple(c.lw[:]), tuple(int(v) for v in c.nx)
+        for k, d in enumerate(domains):
+            nx, ny = d.nx
+            ind = np.empty(nx * ny, dtype=np.int32)
+            img = np.empty(nx * ny, dtype=np.int32)
+            _lib.check(L.swals_md_metadata_priority(handle, k, ind.ctypes.data, img.ctypes.data))
+            d.priority_domain_index = ind.reshape(ny, nx).T.astype(np.int64)
+            d.priority_domain_image = img.reshape(ny, nx).T.astype(np.int64)
+            cnt = ctypes.c_int32()
+            _lib.check(L.swals_md_metadata_recv_boxes(handle, k, None, 0, ctypes.byref(cnt)))
+            rows = np.empty((cnt.value, 6), dtype=np.int64)
+            _lib.check(L.swals_md_metadata_recv_boxes(handle, k, rows.ctypes.data, cnt.value, ctypes.byref(cnt)))
+            d.recv_metadata = rows
+            d.send_metadata = None
+        cnt = ctypes.c_int32()
+        _lib.check(L.swals_md_metadata_exchanges(handle, None, 0, ctypes.byref(cnt)))
+        exs = (_MdExchange * max(cnt.value, 1))()
+        _lib.check(L.swals_md_metadata_exchanges(handle, exs, cnt.value, ctypes.byref(cnt)))
+        return [Exchange(sender=e.sender, receiver=e.receiver, send_box=tuple(e.send_box[:]),
+                         recv_box=tuple(e.recv_box[:]), recv_row=e.recv_row, send_row=e.send_row)
+                for e in exs[:cnt.value]]
+    finally:
+        L.swals_md_metadata_free(handle)
 
 
 def exchange_cell_ratios(domains: Sequence[NestDomain], e: Exchange) -> Tuple[int, int]:
