@@ -417,6 +417,15 @@ int swals_gpu_apply_forcing(swals_domain *d, double dt);
  * off.  Drops a captured evolve_steps graph. */
 int swals_gpu_set_eddy_viscosity(swals_domain *d, int32_t use_eddy_viscosity, double constant, double shiono_knight);
 
+/* domain%static_before_time (domain_mod.f90:185, 1706-1716): a step that
+ * starts before it only advances the clock by the given timestep (and
+ * counts itself).  The host reads the clock once per step until the time
+ * has passed; such steps are not captured in graphs. */
+int swals_gpu_set_static_before_time(swals_domain *d, double static_before_time);
+/* domain%max_U_update_frequency (domain_mod.f90:431, 1794-1798): max_stage
+ * is updated after steps whose count before the step is a multiple of it. */
+int swals_gpu_set_max_U_update_frequency(swals_domain *d, int32_t every);
+
 /* ---- REAL4 output staging ------------------------------------------------
  * What SWALS's netCDF writers store, converted to REAL4 (round to nearest)
  * on the device and copied to host_out in one transfer; the call returns

@@ -75,6 +75,7 @@ class _OracleDomainC(ctypes.Structure):
         ("advection_work", ctypes.c_void_p),
         ("use_eddy_viscosity", ctypes.c_int32), ("pad3", ctypes.c_int32),
         ("eddy_visc_constants", ctypes.c_double * 2), ("eddy_visc", ctypes.c_void_p),
+        ("static_before_time", ctypes.c_double), ("max_U_update_frequency", ctypes.c_int32), ("pad4", ctypes.c_int32),
     ]
 
 
@@ -137,6 +138,8 @@ class OracleDomain:
         c.msl_linear = msl_linear
         c.linear_friction_coeff = linear_friction_coeff
         c.maximum_timestep = maximum_timestep
+        c.static_before_time = NEG_HUGE
+        c.max_U_update_frequency = 1
         self.c = c
         dt = self.dtype
         self.U = np.zeros((4, ny, nx), dtype=dt)

@@ -1645,7 +1645,12 @@ int ORACLE_FN(evolve_one_step)(oracle_domain *d, double dt, int has_dt)
     double time0 = d->time;
     d->boundary_flux_evolve_integral = 0.0;
     if (d->nsteps_advanced == 0) ORACLE_FN(update_max_quantities)(d);
-    switch (d->method) {
+    /* before static_before_time the step only advances the clock
+     * (domain_mod.f90:1706-1716) */
+    const int is_static = time0 < d->static_before_time;
+    if (is_static) {
+        if (has_dt) d->time = d->time + dt;
+    } else switch (d->method) {
     case OR_METHOD_RK2: one_rk2_step(d, dt, has_dt); break;
     case OR_METHOD_EULER: one_euler_step(d, dt, has_dt, 1); break;
     case OR_METHOD_RK2N: one_rk2n_step(d, dt, has_dt); break;
@@ -1661,7 +1666,9 @@ int ORACLE_FN(evolve_one_step)(oracle_domain *d, double dt, int has_dt)
         break;
     default: return 3;
     }
-    ORACLE_FN(update_max_quantities)(d);
+    /* update_max_quantities every max_U_update_frequency steps (:1794-1798) */
+    const int freq = d->max_U_update_frequency > 0 ? d->max_U_update_frequency : 1;
+    if (!is_static && d->nsteps_advanced % freq == 0) ORACLE_FN(update_max_quantities)(d);
     d->evolve_step_dt = d->time - time0;
     d->boundary_flux_time_integral += d->boundary_flux_evolve_integral;
     d->nsteps_advanced += 1;

@@ -144,6 +144,11 @@ typedef struct oracle_domain {
     int32_t pad3;
     double eddy_visc_constants[2];
     REAL *eddy_visc;
+    /* domain%static_before_time (-HUGE: never static) and
+     * domain%max_U_update_frequency (domain_mod.f90:185, 431) */
+    double static_before_time;
+    int32_t max_U_update_frequency;
+    int32_t pad4;
 } oracle_domain;
 
 /* forcing_patch_type (forcing_mod.f90:23-53) with the default (identity)

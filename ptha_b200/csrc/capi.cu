@@ -239,6 +239,28 @@ int evolve_t(swals_domain *d, double timestep, int has_dt)
         if (e != cudaSuccess) return cuda_fail(e, "update_max_quantities");
     }
     cudaError_t e = cudaSuccess;
+    if (d->static_pending) {
+        // static_before_time (domain_mod.f90:1706-1716): the clock decides
+        // on the host, one read per step until it has passed.
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        CK(cudaStreamIsCapturing(d->stream, &cs));
+        if (cs != cudaStreamCaptureStatusNone)
+            return fail(SWALS_ERR_UNSUPPORTED, "a step before static_before_time cannot be captured in a graph");
+        double time0 = 0.0;
+        CK(cudaMemcpyAsync(&time0, &d->sc->time, sizeof(double), cudaMemcpyDeviceToHost, d->stream));
+        CK(cudaStreamSynchronize(d->stream));
+        if (time0 < d->static_before_time) {
+            e = launch_static_step(d->sc, timestep, has_dt, d->stream);
+            if (e != cudaSuccess) return cuda_fail(e, "static step");
+            d->nsteps++;
+            return SWALS_OK;
+        }
+        d->static_pending = false;
+    }
+    // max_U_update_frequency > 1: the step kernels skip max_stage and one
+    // kernel updates it after the steps the reference updates it after.
+    R *const max_every = (max_stage && d->max_U_update_frequency > 1) ? max_stage : nullptr;
+    if (max_every) max_stage = nullptr;
     if (d->method == M_LINEAR || d->method == M_LF_LIN_NLFRIC) {
         if (!has_dt)
             return fail(SWALS_ERR_TIMESTEP_REQUIRED, "ERROR: timestep must be provided for %s evolve_one_step",
@@ -293,6 +315,13 @@ int evolve_t(swals_domain *d, double timestep, int has_dt)
     } else {
         return fail(SWALS_ERR_UNSUPPORTED, "timestepping_method '%s' is not implemented on the GPU path",
                     d->desc.timestepping_method);
+    }
+    if (max_every) {
+        hook(CAT_MAXSTAGE, 0);
+        e = launch_update_max_stage_every<R>(d->nx, d->ny, d->pitch, (const R *)d->planes[d->cur][0], max_every, c,
+                                             d->sc, d->max_U_update_frequency, d->stream);
+        hook(CAT_MAXSTAGE, 1);
+        if (e != cudaSuccess) return cuda_fail(e, "update_max_quantities");
     }
     if (d->n_gauges > 0) {
         hook(CAT_GAUGES, 0);
@@ -660,7 +689,7 @@ int swals_gpu_evolve_steps(swals_domain *d, int32_t nsteps, double timestep, int
         if (rc) return rc;
         done = 1;
     }
-    const bool use_graph = !d->timers_on && (nsteps - done) >= 2 * GRAPH_STEPS;
+    const bool use_graph = !d->timers_on && !d->static_pending && (nsteps - done) >= 2 * GRAPH_STEPS;
     if (use_graph) {
         const bool same = d->step_graph && d->graph_dt == timestep && d->graph_has_dt == (has_timestep != 0) &&
                           d->graph_stream == d->stream && d->graph_gauges == d->n_gauges;
@@ -936,6 +965,26 @@ int swals_gpu_set_eddy_viscosity(swals_domain *d, int32_t use_eddy_viscosity, do
     d->cfg.eddy_visc_constants[0] = constant;
     d->cfg.eddy_visc_constants[1] = shiono_knight;
     d->cfg.flux_variant |= swals::FLUX_EDDY;
+    return SWALS_OK;
+}
+
+int swals_gpu_set_static_before_time(swals_domain *d, double static_before_time)
+{
+    if (!d) return fail(SWALS_ERR_INVALID_ARGUMENT, "NULL domain");
+    CK(cudaStreamSynchronize(d->stream));
+    drop_step_graph(d);
+    d->static_before_time = static_before_time;
+    d->static_pending = static_before_time > -DBL_MAX;
+    return SWALS_OK;
+}
+
+int swals_gpu_set_max_U_update_frequency(swals_domain *d, int32_t every)
+{
+    if (!d) return fail(SWALS_ERR_INVALID_ARGUMENT, "NULL domain");
+    if (every < 1) return fail(SWALS_ERR_INVALID_ARGUMENT, "max_U_update_frequency must be >= 1");
+    CK(cudaStreamSynchronize(d->stream));
+    drop_step_graph(d);
+    d->max_U_update_frequency = every;
     return SWALS_OK;
 }
 

@@ -62,6 +62,9 @@ struct swals_domain {
     // REAL4 output staging buffer (floats), allocated on first use.
     float *stage_buf = nullptr;
     void *eddy_visc = nullptr;   // use_eddy_viscosity: one plane of pitch x ny reals
+    double static_before_time = -1.7976931348623157e308;  // domain%static_before_time
+    bool static_pending = false;   // static_before_time may still lie ahead (the host checks the clock)
+    int max_U_update_frequency = 1;
     size_t stage_cap = 0;
     // Replayed graph of a few steps for evolve_steps.
     cudaGraphExec_t step_graph = nullptr;

@@ -946,8 +946,12 @@ __global__ void __launch_bounds__(256) linear_nlfric_kernel(const LinArgs<R> a, 
 }
 
 template <typename R>
-__global__ void max_stage_kernel(int nx, int ny, int64_t P, const R *stg, R *mx, int xl, int xu, int yl, int yu)
+__global__ void max_stage_kernel(int nx, int ny, int64_t P, const R *stg, R *mx, int xl, int xu, int yl, int yu,
+                                 const DevScalars *sc, int every)
 {
+    // every > 1: max_U_update_frequency (domain_mod.f90:1794-1798), after a
+    // step that has already counted itself in nsteps_advanced
+    if (every > 1 && (sc->nsteps_advanced - 1) % every != 0) return;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int r = blockIdx.y * blockDim.y + threadIdx.y;
     if (i < xl || i > xu || r < yl || r > yu || i >= nx || r >= ny) return;
@@ -1666,9 +1670,43 @@ cudaError_t launch_update_max_stage(int nx, int ny, int64_t pitch, const R *stg,
 {
     dim3 block(32, 8);
     dim3 grid((nx + 31) / 32, (ny + 7) / 8);
-    max_stage_kernel<R><<<grid, block, 0, s>>>(nx, ny, pitch, stg, max_stage, c.xl, c.xu, c.yl, c.yu);
+    max_stage_kernel<R><<<grid, block, 0, s>>>(nx, ny, pitch, stg, max_stage, c.xl, c.xu, c.yl, c.yu, nullptr, 1);
     return cudaGetLastError();
 }
+
+// Static steps (static_before_time, domain_mod.f90:1706-1716): the clock
+// advances by the step's dt (when given) and the step is counted; nothing
+// else changes.
+__global__ void static_step_kernel(DevScalars *sc, double dt, int has_dt)
+{
+    const double time0 = sc->time;
+    sc->time0 = time0;
+    if (has_dt) sc->time = sc->time + dt;
+    sc->boundary_flux_evolve_integral = 0.0;
+    sc->boundary_flux_time_integral = sc->boundary_flux_time_integral + 0.0;
+    sc->evolve_step_dt = sc->time - time0;
+    sc->nsteps_advanced += 1;
+}
+
+cudaError_t launch_static_step(DevScalars *sc, double dt, int has_dt, cudaStream_t s)
+{
+    static_step_kernel<<<1, 1, 0, s>>>(sc, dt, has_dt);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_update_max_stage_every(int nx, int ny, int64_t pitch, const R *stg, R *max_stage,
+                                          const StepConfig &c, const DevScalars *sc, int every, cudaStream_t s)
+{
+    dim3 block(32, 8);
+    dim3 grid((nx + 31) / 32, (ny + 7) / 8);
+    max_stage_kernel<R><<<grid, block, 0, s>>>(nx, ny, pitch, stg, max_stage, c.xl, c.xu, c.yl, c.yu, sc, every);
+    return cudaGetLastError();
+}
+template cudaError_t launch_update_max_stage_every<double>(int, int, int64_t, const double *, double *,
+                                                           const StepConfig &, const DevScalars *, int, cudaStream_t);
+template cudaError_t launch_update_max_stage_every<float>(int, int, int64_t, const float *, float *,
+                                                          const StepConfig &, const DevScalars *, int, cudaStream_t);
 
 template <typename R>
 cudaError_t launch_gauges(int64_t pitch, const R *stg, const R *uh, const R *vh, const int *site_ij, int n,

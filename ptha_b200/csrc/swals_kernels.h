@@ -169,6 +169,12 @@ cudaError_t launch_batch_gauges(int64_t pitch, const R *stg0, int64_t inst_strid
                                 int n, double *records, int rec, int capacity, cudaStream_t s);
 
 // max_stage = max(max_stage, STG) over the active region (domain_mod.f90:2243-2290).
+// update_max_quantities after a step when (nsteps_advanced - 1) % every == 0.
+template <typename R>
+cudaError_t launch_update_max_stage_every(int nx, int ny, int64_t pitch, const R *stg, R *max_stage,
+                                          const StepConfig &c, const DevScalars *sc, int every, cudaStream_t s);
+// A static step (before static_before_time): clock and counters only.
+cudaError_t launch_static_step(DevScalars *sc, double dt, int has_dt, cudaStream_t s);
 template <typename R>
 cudaError_t launch_update_max_stage(int nx, int ny, int64_t pitch, const R *stg, R *max_stage,
                                     const StepConfig &c, cudaStream_t s);

@@ -240,6 +240,14 @@ class Domain:
         Finite-volume methods only."""
         check(self._L.swals_gpu_set_eddy_viscosity(self._h, 1, float(constant), float(shiono_knight)))
 
+    def set_static_before_time(self, t):
+        """domain%static_before_time: steps starting before t only advance the clock."""
+        check(self._L.swals_gpu_set_static_before_time(self._h, float(t)))
+
+    def set_max_U_update_frequency(self, every):
+        """domain%max_U_update_frequency: max_stage updated every `every` steps."""
+        check(self._L.swals_gpu_set_max_U_update_frequency(self._h, int(every)))
+
     def clear_eddy_viscosity(self):
         check(self._L.swals_gpu_set_eddy_viscosity(self._h, 0, 0.0, 0.0))
 

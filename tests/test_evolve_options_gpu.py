@@ -1,0 +1,69 @@
+"""evolve_one_step's own options (domain_mod.f90:1679-1813) on the GPU
+against the oracle: static_before_time (steps that start before it only
+advance the clock) and max_U_update_frequency (max_stage updated after every
+n-th step), for the finite-volume and the leapfrog solvers, stepped one by
+one and through evolve_steps."""
+import numpy as np
+import pytest
+
+from ptha_b200 import workloads
+from pairs import make_pair, report, water_mask
+
+pytestmark = pytest.mark.gpu
+
+
+def _exact(g, o, tag):
+    _, errs = report(tag, g, o)
+    for k in ("STG", "UH", "VH", "ELV"):
+        assert errs[k + "_exact"] == 1.0, errs
+
+
+def _beach(method):
+    kw, U, _, nsq = workloads.rk2_beach(n=80, dx=10.0 * 2048 / 80, toe=17580.0 * 80 / 2048)
+    return dict(kw, timestepping_method=method), U, nsq
+
+
+@pytest.mark.parametrize("method", ["rk2", "linear", "leapfrog_nonlinear"])
+@pytest.mark.parametrize("graph", [False, True])
+def test_static_before_time(method, graph):
+    kw, U, nsq = _beach(method)
+    g, o = make_pair(kw, U, manning_sq=nsq)
+    dt = 0.25 * o.linear_timestep_max() if method != "rk2" else 0.5 * o.nonlinear_stationary_timestep_max()
+    t_static = 10.5 * dt
+    g.set_static_before_time(t_static)
+    o.c.static_before_time = t_static
+    n = 40
+    if graph:
+        g.evolve_steps(n, dt)
+    else:
+        for _ in range(n):
+            g.evolve_one_step(dt)
+    for _ in range(n):
+        o.evolve_one_step(dt)
+    _exact(g, o, f"{method} static graph={graph}")
+    st = g.state()
+    assert st.time == pytest.approx(o.time, rel=1e-14) and st.nsteps_advanced == o.nsteps_advanced == n
+    np.testing.assert_array_equal(g.max_stage()[water_mask(o.U[3])], o.max_stage[water_mask(o.U[3])])
+    # the first 11 steps were static: the state moved only after them
+    assert o.time == pytest.approx(n * dt)
+
+
+@pytest.mark.parametrize("method", ["rk2", "midpoint", "linear", "leapfrog_linear_plus_nonlinear_friction"])
+def test_max_U_update_frequency(method):
+    kw, U, nsq = _beach(method)
+    g, o = make_pair(kw, U, manning_sq=nsq)
+    b, _ = make_pair(kw, U, manning_sq=nsq)
+    dt = 0.25 * o.linear_timestep_max() if method not in ("rk2", "midpoint") \
+        else 0.5 * o.nonlinear_stationary_timestep_max()
+    for d in (g, b):
+        d.set_max_U_update_frequency(3)
+    o.c.max_U_update_frequency = 3
+    for _ in range(37):
+        g.evolve_one_step(dt)
+        o.evolve_one_step(dt)
+    b.evolve_steps(37, dt)
+    _exact(g, o, f"{method} max_U every 3")
+    m = water_mask(o.U[3])
+    np.testing.assert_array_equal(g.max_stage()[m], o.max_stage[m])
+    np.testing.assert_array_equal(b.max_stage()[m], o.max_stage[m])
+    np.testing.assert_array_equal(b.get_U(), g.get_U())
