@@ -425,6 +425,15 @@ int swals_gpu_set_static_before_time(swals_domain *d, double static_before_time)
 /* domain%max_U_update_frequency (domain_mod.f90:431, 1794-1798): max_stage
  * is updated after steps whose count before the step is a multiple of it. */
 int swals_gpu_set_max_U_update_frequency(swals_domain *d, int32_t every);
+/* The optional max_U_variables after max_stage (domain_mod.f90:1038-1117,
+ * 2243-2404), as a mask: 1 time_of_max_stage, 2 max_speed, 4 max_flux,
+ * 8 arrival_time, 16 min_stage; with stage_extrema_include_dry_cells and
+ * arrival_stage_threshold_above_msl_linear (defaults 1 and 0.01).  Needs
+ * record_max_stage; set before the first step (initialises the planes). */
+int swals_gpu_set_max_U_variables(swals_domain *d, int32_t mask, int32_t stage_extrema_include_dry_cells,
+                                  double arrival_stage_threshold_above_msl_linear);
+/* One recorded variable (a single mask bit) as nx*ny doubles, column-major. */
+int swals_gpu_download_max_U(swals_domain *d, int32_t bit, double *host);
 
 /* ---- REAL4 output staging ------------------------------------------------
  * What SWALS's netCDF writers store, converted to REAL4 (round to nearest)

@@ -75,7 +75,9 @@ class _OracleDomainC(ctypes.Structure):
         ("advection_work", ctypes.c_void_p),
         ("use_eddy_viscosity", ctypes.c_int32), ("pad3", ctypes.c_int32),
         ("eddy_visc_constants", ctypes.c_double * 2), ("eddy_visc", ctypes.c_void_p),
-        ("static_before_time", ctypes.c_double), ("max_U_update_frequency", ctypes.c_int32), ("pad4", ctypes.c_int32),
+        ("static_before_time", ctypes.c_double), ("max_U_update_frequency", ctypes.c_int32),
+        ("max_U_extra", ctypes.c_int32), ("stage_extrema_include_dry_cells", ctypes.c_int32), ("pad5", ctypes.c_int32),
+        ("arrival_stage_threshold_above_msl_linear", ctypes.c_double), ("max_U_extra_planes", ctypes.c_void_p),
     ]
 
 
@@ -140,6 +142,8 @@ class OracleDomain:
         c.maximum_timestep = maximum_timestep
         c.static_before_time = NEG_HUGE
         c.max_U_update_frequency = 1
+        c.stage_extrema_include_dry_cells = 1
+        c.arrival_stage_threshold_above_msl_linear = 0.01
         self.c = c
         dt = self.dtype
         self.U = np.zeros((4, ny, nx), dtype=dt)
@@ -161,6 +165,10 @@ class OracleDomain:
         self.friction_work = np.zeros((2, ny, nx), dt)
         self.advection_work = np.zeros((5, ny, nx), dt)
         self.eddy_visc = np.zeros((ny, nx), dt)
+        # time_of_max_stage, max_speed, max_flux, arrival_time, min_stage
+        self.max_U_extra = np.zeros((5, ny, nx), dt)
+        self.max_U_extra[:] = init
+        self.max_U_extra[4] = -init
         for name, arr in [("U", self.U), ("max_stage", self.max_stage), ("manning_squared", self.manning_squared),
                           ("x", self.x), ("y", self.y), ("dxb", self.dxb), ("dyl", self.dyl), ("area", self.area),
                           ("coriolis_c", self.coriolis_c), ("coriolis_be", self.coriolis_be),
@@ -169,7 +177,7 @@ class OracleDomain:
                           ("explicit_source", self.explicit_source),
                           ("explicit_source_VH_j_minus_1", self.es_jm1), ("backup_U", self.backup_U),
                           ("friction_work", self.friction_work), ("advection_work", self.advection_work),
-                          ("eddy_visc", self.eddy_visc)]:
+                          ("eddy_visc", self.eddy_visc), ("max_U_extra_planes", self.max_U_extra)]:
             setattr(c, name, _ptr(arr))
         self._fn("apply_method_defaults")(ctypes.byref(c))
         self._fn("setup_geometry")(ctypes.byref(c))

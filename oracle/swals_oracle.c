@@ -469,14 +469,82 @@ static void update_boundary(oracle_domain *d)
 /* max_U tracking: domain_mod.f90:2243-2290 (max_stage, dry cells included) */
 void ORACLE_FN(update_max_quantities)(oracle_domain *d)
 {
+    /* update_max_quantities (domain_mod.f90:2243-2404): max_stage (with its
+     * time when time_of_max_stage is recorded), then the optional variables. */
     const int nx = d->nx, ny = d->ny;
     if (!d->record_max_stage || !d->max_stage) return;
+    const int ex = d->max_U_extra;
+    const size_t plane = (size_t)nx * ny;
+    REAL *toms = d->max_U_extra_planes, *mspeed = toms + plane, *mflux = toms + 2 * plane;
+    REAL *arrival = toms + 3 * plane, *minst = toms + 4 * plane;
+    const int dry_ok = d->stage_extrema_include_dry_cells;
     for (int j = d->yL; j <= d->yU; j++)
         for (int i = d->xL; i <= d->xU; i++) {
             REAL m = d->max_stage[IDX(i, j)];
             REAL s = UU(OR_STG, i, j);
-            d->max_stage[IDX(i, j)] = (s > m) ? s : m;
+            const int ok = dry_ok || (s > UU(OR_ELV, i, j) + MINIMUM_ALLOWED_DEPTH);
+            if (ex & 1) {
+                if (s > m && ok) {
+                    d->max_stage[IDX(i, j)] = s;
+                    toms[IDX(i, j)] = (REAL)d->time;
+                }
+            } else if (ok) {
+                d->max_stage[IDX(i, j)] = (s > m) ? s : m;
+            }
         }
+    if (ex & 2) {
+        const int tl = d->truely_linear && (d->method == OR_METHOD_LINEAR ||
+                                            d->method == OR_METHOD_LEAPFROG_LINEAR_PLUS_NONLINEAR_FRICTION);
+        for (int j = d->yL; j <= d->yU; j++)
+            for (int i = d->xL; i <= d->xU; i++) {
+                REAL v;
+                if (is_staggered(d)) {
+                    const int ip1 = (i + 1 < nx) ? i + 1 : nx, jp1 = (j + 1 < ny) ? j + 1 : ny;
+                    REAL de, dn;
+                    if (tl) {
+                        const REAL msl = (REAL)d->msl_linear;
+                        de = (REAL)0.5 * ((msl - UU(OR_ELV, i, j)) + (msl - UU(OR_ELV, ip1, j)));
+                        dn = (REAL)0.5 * ((msl - UU(OR_ELV, i, j)) + (msl - UU(OR_ELV, i, jp1)));
+                    } else {
+                        de = (REAL)0.5 * ((UU(OR_STG, i, j) - UU(OR_ELV, i, j)) + (UU(OR_STG, ip1, j) - UU(OR_ELV, ip1, j)));
+                        dn = (REAL)0.5 * ((UU(OR_STG, i, j) - UU(OR_ELV, i, j)) + (UU(OR_STG, i, jp1) - UU(OR_ELV, i, jp1)));
+                    }
+                    const REAL dei = (de > MINIMUM_ALLOWED_DEPTH) ? ONE / de : ZERO;
+                    const REAL dni = (dn > MINIMUM_ALLOWED_DEPTH) ? ONE / dn : ZERO;
+                    const REAL u = UU(OR_UH, i, j), w = UU(OR_VH, i, j);
+                    v = (REAL)sqrt(u * u * (dei * dei) + w * w * (dni * dni));
+                } else {
+                    const REAL ld = UU(OR_STG, i, j) - UU(OR_ELV, i, j);
+                    const REAL ldi = (ld > MINIMUM_ALLOWED_DEPTH) ? ONE / ld : ZERO;
+                    const REAL u = UU(OR_UH, i, j), w = UU(OR_VH, i, j);
+                    v = (REAL)sqrt((u * u + w * w) * (ldi * ldi));
+                }
+                const REAL m = mspeed[IDX(i, j)];
+                mspeed[IDX(i, j)] = (v > m) ? v : m;
+            }
+    }
+    if (ex & 4)
+        for (int j = d->yL; j <= d->yU; j++)
+            for (int i = d->xL; i <= d->xU; i++) {
+                const REAL u = UU(OR_UH, i, j), w = UU(OR_VH, i, j);
+                const REAL v = (REAL)sqrt(u * u + w * w), m = mflux[IDX(i, j)];
+                mflux[IDX(i, j)] = (v > m) ? v : m;
+            }
+    if (ex & 8) {
+        const REAL arrival_stage = (REAL)d->msl_linear + (REAL)d->arrival_stage_threshold_above_msl_linear;
+        for (int j = d->yL; j <= d->yU; j++)
+            for (int i = d->xL; i <= d->xU; i++) {
+                const REAL ld = UU(OR_STG, i, j) - UU(OR_ELV, i, j);
+                if (ld > MINIMUM_ALLOWED_DEPTH && UU(OR_STG, i, j) > arrival_stage && arrival[IDX(i, j)] < ZERO)
+                    arrival[IDX(i, j)] = (REAL)d->time;
+            }
+    }
+    if (ex & 16)
+        for (int j = d->yL; j <= d->yU; j++)
+            for (int i = d->xL; i <= d->xU; i++) {
+                const REAL s = UU(OR_STG, i, j), m = minst[IDX(i, j)];
+                if (dry_ok || (s > UU(OR_ELV, i, j) + MINIMUM_ALLOWED_DEPTH)) minst[IDX(i, j)] = (s < m) ? s : m;
+            }
 }
 
 /* domain_mod.f90:1906-1931 */

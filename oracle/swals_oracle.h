@@ -148,7 +148,14 @@ typedef struct oracle_domain {
      * domain%max_U_update_frequency (domain_mod.f90:185, 431) */
     double static_before_time;
     int32_t max_U_update_frequency;
-    int32_t pad4;
+    /* the optional max_U_variables (domain_mod.f90:2243-2404) as bits:
+     * 1 time_of_max_stage, 2 max_speed, 4 max_flux, 8 arrival_time,
+     * 16 min_stage; one nx*ny plane each in max_U_extra, in bit order */
+    int32_t max_U_extra;
+    int32_t stage_extrema_include_dry_cells;
+    int32_t pad5;
+    double arrival_stage_threshold_above_msl_linear;
+    REAL *max_U_extra_planes;
 } oracle_domain;
 
 /* forcing_patch_type (forcing_mod.f90:23-53) with the default (identity)

@@ -46,6 +46,7 @@ EXPORTED = [
     "swals_gpu_set_priority_mask", "swals_gpu_domain_statistics", "swals_gpu_volume_in_priority_domain",
     "swals_gpu_forcing_patch_add", "swals_gpu_forcing_clear", "swals_gpu_apply_forcing",
     "swals_gpu_set_eddy_viscosity", "swals_gpu_set_static_before_time", "swals_gpu_set_max_U_update_frequency",
+    "swals_gpu_set_max_U_variables", "swals_gpu_download_max_U",
     "swals_md_build_metadata", "swals_md_metadata_exchanges", "swals_md_metadata_priority",
     "swals_md_metadata_recv_boxes", "swals_md_metadata_free",
     "swals_gpu_stage_grids_real4", "swals_gpu_gauges_read_real4",
@@ -164,6 +165,7 @@ def lib():
         "swals_gpu_forcing_clear": [vp], "swals_gpu_apply_forcing": [vp, dbl],
         "swals_gpu_set_eddy_viscosity": [vp, i32, dbl, dbl],
         "swals_gpu_set_static_before_time": [vp, dbl], "swals_gpu_set_max_U_update_frequency": [vp, i32],
+        "swals_gpu_set_max_U_variables": [vp, i32, i32, dbl], "swals_gpu_download_max_U": [vp, i32, vp],
         "swals_md_build_metadata": [vp, i32, i32, i32, vp, vp, ctypes.POINTER(vp)],
         "swals_md_metadata_exchanges": [vp, vp, i32, ctypes.POINTER(i32)],
         "swals_md_metadata_priority": [vp, i32, vp, vp],

@@ -231,10 +231,17 @@ int evolve_t(swals_domain *d, double timestep, int has_dt)
     const LaunchHook hook = swals::hook_of(d);
     Metrics<R> m = swals::metrics_of<R>(d);
     R *max_stage = d->desc.record_max_stage ? (R *)d->max_stage : nullptr;
+    auto max_u_after = [&](int every) {
+        return launch_update_max_u<R>(d->nx, d->ny, d->pitch, (const R *)d->planes[d->cur][0],
+                                      (const R *)d->planes[d->cur][1], (const R *)d->planes[d->cur][2],
+                                      (const R *)d->elv, max_stage, c, d->max_u, d->sc, every, d->stream);
+    };
     if (d->nsteps == 0 && max_stage) {
         hook(CAT_MAXSTAGE, 0);
-        cudaError_t e = launch_update_max_stage<R>(d->nx, d->ny, d->pitch, (const R *)d->planes[d->cur][0],
-                                                   max_stage, c, d->stream);
+        cudaError_t e = d->max_u_generic ? max_u_after(1)
+                                         : launch_update_max_stage<R>(d->nx, d->ny, d->pitch,
+                                                                      (const R *)d->planes[d->cur][0], max_stage, c,
+                                                                      d->stream);
         hook(CAT_MAXSTAGE, 1);
         if (e != cudaSuccess) return cuda_fail(e, "update_max_quantities");
     }
@@ -259,7 +266,7 @@ int evolve_t(swals_domain *d, double timestep, int has_dt)
     }
     // max_U_update_frequency > 1: the step kernels skip max_stage and one
     // kernel updates it after the steps the reference updates it after.
-    R *const max_every = (max_stage && d->max_U_update_frequency > 1) ? max_stage : nullptr;
+    R *const max_every = (max_stage && (d->max_U_update_frequency > 1 || d->max_u_generic)) ? max_stage : nullptr;
     if (max_every) max_stage = nullptr;
     if (d->method == M_LINEAR || d->method == M_LF_LIN_NLFRIC) {
         if (!has_dt)
@@ -318,8 +325,11 @@ int evolve_t(swals_domain *d, double timestep, int has_dt)
     }
     if (max_every) {
         hook(CAT_MAXSTAGE, 0);
-        e = launch_update_max_stage_every<R>(d->nx, d->ny, d->pitch, (const R *)d->planes[d->cur][0], max_every, c,
-                                             d->sc, d->max_U_update_frequency, d->stream);
+        max_stage = max_every;
+        e = d->max_u_generic ? max_u_after(d->max_U_update_frequency)
+                             : launch_update_max_stage_every<R>(d->nx, d->ny, d->pitch, (const R *)d->planes[d->cur][0],
+                                                                max_every, c, d->sc, d->max_U_update_frequency,
+                                                                d->stream);
         hook(CAT_MAXSTAGE, 1);
         if (e != cudaSuccess) return cuda_fail(e, "update_max_quantities");
     }
@@ -558,6 +568,7 @@ int swals_gpu_domain_destroy(swals_domain *d)
     free_forcing(d);
     if (d->stage_buf) cudaFree(d->stage_buf);
     if (d->eddy_visc) cudaFree(d->eddy_visc);
+    if (d->max_u.planes) cudaFree(d->max_u.planes);
     for (auto &p : d->pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
     for (auto e : d->ev_pool) cudaEventDestroy(e);
     if (d->d_sites) cudaFree(d->d_sites);
@@ -985,6 +996,60 @@ int swals_gpu_set_max_U_update_frequency(swals_domain *d, int32_t every)
     CK(cudaStreamSynchronize(d->stream));
     drop_step_graph(d);
     d->max_U_update_frequency = every;
+    return SWALS_OK;
+}
+
+int swals_gpu_set_max_U_variables(swals_domain *d, int32_t mask, int32_t stage_extrema_include_dry_cells,
+                                  double arrival_stage_threshold_above_msl_linear)
+{
+    if (!d) return fail(SWALS_ERR_INVALID_ARGUMENT, "NULL domain");
+    if (mask < 0 || mask > 31) return fail(SWALS_ERR_INVALID_ARGUMENT, "max_U_variables mask %d", mask);
+    if (!d->desc.record_max_stage && (mask || !stage_extrema_include_dry_cells))
+        return fail(SWALS_ERR_INVALID_ARGUMENT, "max_U_variables need record_max_stage (max_stage comes first)");
+    if (d->nsteps > 0) return fail(SWALS_ERR_INVALID_ARGUMENT, "max_U_variables are set before the first step");
+    CK(cudaStreamSynchronize(d->stream));
+    drop_step_graph(d);
+    const size_t es = esize(d);
+    const int64_t plane = (int64_t)d->nx * d->ny;
+    if (mask && !d->max_u.planes) CK(cudaMalloc(&d->max_u.planes, (size_t)plane * 5 * es));
+    if (d->max_u.planes) {
+        // -0.99 huge(real(1.0, output_precision)); min_stage starts at +0.99 huge (domain_mod.f90:1098-1117)
+        const float init = -0.99f * FLT_MAX;
+        const int blocks = (int)((plane + 255) / 256);
+        for (int k = 0; k < 5; k++) {
+            const float v = (k == 4) ? -init : init;
+            char *p = (char *)d->max_u.planes + (size_t)k * plane * es;
+            if (d->fp64) fill_kernel<double><<<blocks, 256, 0, d->stream>>>((double *)p, plane, (double)v);
+            else fill_kernel<float><<<blocks, 256, 0, d->stream>>>((float *)p, plane, v);
+        }
+        CK(cudaGetLastError());
+    }
+    d->max_u.mask = mask;
+    d->max_u.include_dry = stage_extrema_include_dry_cells ? 1 : 0;
+    d->max_u.staggered = is_staggered(d->method) ? 1 : 0;
+    d->max_u.truely_linear = (d->desc.linear_solver_is_truely_linear &&
+                              (d->method == M_LINEAR || d->method == M_LF_LIN_NLFRIC)) ? 1 : 0;
+    d->max_u.arrival = d->fp64 ? d->desc.msl_linear + arrival_stage_threshold_above_msl_linear
+                               : (double)((float)d->desc.msl_linear + (float)arrival_stage_threshold_above_msl_linear);
+    d->max_u.plane = plane;
+    d->max_u_generic = mask != 0 || !stage_extrema_include_dry_cells;
+    return SWALS_OK;
+}
+
+int swals_gpu_download_max_U(swals_domain *d, int32_t bit, double *host)
+{
+    if (!d || !host) return fail(SWALS_ERR_INVALID_ARGUMENT, "NULL argument");
+    int k = -1;
+    for (int q = 0; q < 5; q++)
+        if (bit == (1 << q)) k = q;
+    if (k < 0 || !(d->max_u.mask & bit)) return fail(SWALS_ERR_INVALID_ARGUMENT, "max_U variable %d not recorded", bit);
+    const size_t es = esize(d), n = (size_t)d->max_u.plane;
+    std::vector<char> tmp(n * es);
+    CK(cudaMemcpyAsync(tmp.data(), (char *)d->max_u.planes + (size_t)k * n * es, n * es, cudaMemcpyDeviceToHost,
+                       d->stream));
+    CK(cudaStreamSynchronize(d->stream));
+    for (size_t q = 0; q < n; q++)
+        host[q] = d->fp64 ? ((const double *)tmp.data())[q] : (double)((const float *)tmp.data())[q];
     return SWALS_OK;
 }
 

@@ -65,6 +65,8 @@ struct swals_domain {
     double static_before_time = -1.7976931348623157e308;  // domain%static_before_time
     bool static_pending = false;   // static_before_time may still lie ahead (the host checks the clock)
     int max_U_update_frequency = 1;
+    swals::MaxUConfig max_u{};     // optional max_U_variables (planes nx x ny, allocated when set)
+    bool max_u_generic = false;     // max_stage and the options by max_u_kernel instead of the step kernels
     size_t stage_cap = 0;
     // Replayed graph of a few steps for evolve_steps.
     cudaGraphExec_t step_graph = nullptr;

@@ -1694,6 +1694,92 @@ cudaError_t launch_static_step(DevScalars *sc, double dt, int has_dt, cudaStream
     return cudaGetLastError();
 }
 
+// update_max_quantities with the optional max_U_variables
+// (domain_mod.f90:2243-2404), one thread per cell of xL..xU x yL..yU, after
+// a step (gated like max_stage_kernel) or before the first one (every 1).
+template <typename R>
+__global__ void max_u_kernel(int nx, int ny, int64_t P, const R *stg, const R *uh, const R *vh, const R *elv,
+                             R *max_stage, int xl, int xu, int yl, int yu, MaxUConfig mu, R msl,
+                             const DevScalars *sc, int every)
+{
+    if (every > 1 && (sc->nsteps_advanced - 1) % every != 0) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int r = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i < xl || i > xu || r < yl || r > yu || i >= nx || r >= ny) return;
+    const int64_t o = (int64_t)r * P + i;
+    const R mad = K<R>::min_depth(), zero = R(0), one = R(1), half = K<R>::half();
+    const R s = stg[o], e = elv[o];
+    const bool ok = mu.include_dry || (s > e + mad);
+    R *pl = (R *)mu.planes;
+    const int64_t q = (int64_t)r * nx + i;   // extra planes: nx x ny, i fastest
+    if (mu.mask & 1) {
+        if (s > max_stage[o] && ok) {
+            max_stage[o] = s;
+            pl[q] = R(sc->time);
+        }
+    } else if (ok) {
+        const R m = max_stage[o];
+        max_stage[o] = (s > m) ? s : m;
+    }
+    if (mu.mask & 2) {
+        R v;
+        if (mu.staggered) {
+            const int ip1 = min(i + 1, nx - 1), jp1 = min(r + 1, ny - 1);
+            const int64_t oe = (int64_t)r * P + ip1, on = (int64_t)jp1 * P + i;
+            R de, dn;
+            if (mu.truely_linear) {
+                de = half * ((msl - e) + (msl - elv[oe]));
+                dn = half * ((msl - e) + (msl - elv[on]));
+            } else {
+                de = half * ((s - e) + (stg[oe] - elv[oe]));
+                dn = half * ((s - e) + (stg[on] - elv[on]));
+            }
+            const R dei = (de > mad) ? one / de : zero, dni = (dn > mad) ? one / dn : zero;
+            const R u = uh[o], w = vh[o];
+            v = R(sqrt(u * u * (dei * dei) + w * w * (dni * dni)));
+        } else {
+            const R ld = s - e;
+            const R ldi = (ld > mad) ? one / ld : zero;
+            const R u = uh[o], w = vh[o];
+            v = R(sqrt((u * u + w * w) * (ldi * ldi)));
+        }
+        R *m = pl + mu.plane;
+        m[q] = (v > m[q]) ? v : m[q];
+    }
+    if (mu.mask & 4) {
+        const R u = uh[o], w = vh[o];
+        const R v = R(sqrt(u * u + w * w));
+        R *m = pl + 2 * mu.plane;
+        m[q] = (v > m[q]) ? v : m[q];
+    }
+    if (mu.mask & 8) {
+        R *m = pl + 3 * mu.plane;
+        if ((s - e) > mad && s > R(mu.arrival) && m[q] < zero) m[q] = R(sc->time);
+    }
+    if (mu.mask & 16) {
+        R *m = pl + 4 * mu.plane;
+        if (ok) m[q] = (s < m[q]) ? s : m[q];
+    }
+}
+
+template <typename R>
+cudaError_t launch_update_max_u(int nx, int ny, int64_t pitch, const R *stg, const R *uh, const R *vh, const R *elv,
+                                R *max_stage, const StepConfig &c, const MaxUConfig &mu, const DevScalars *sc,
+                                int every, cudaStream_t s)
+{
+    dim3 block(32, 8);
+    dim3 grid((nx + 31) / 32, (ny + 7) / 8);
+    max_u_kernel<R><<<grid, block, 0, s>>>(nx, ny, pitch, stg, uh, vh, elv, max_stage, c.xl, c.xu, c.yl, c.yu, mu,
+                                           R(c.msl_linear), sc, every);
+    return cudaGetLastError();
+}
+template cudaError_t launch_update_max_u<double>(int, int, int64_t, const double *, const double *, const double *,
+                                                 const double *, double *, const StepConfig &, const MaxUConfig &,
+                                                 const DevScalars *, int, cudaStream_t);
+template cudaError_t launch_update_max_u<float>(int, int, int64_t, const float *, const float *, const float *,
+                                                const float *, float *, const StepConfig &, const MaxUConfig &,
+                                                const DevScalars *, int, cudaStream_t);
+
 template <typename R>
 cudaError_t launch_update_max_stage_every(int nx, int ny, int64_t pitch, const R *stg, R *max_stage,
                                           const StepConfig &c, const DevScalars *sc, int every, cudaStream_t s)

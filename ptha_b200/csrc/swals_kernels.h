@@ -173,6 +173,23 @@ cudaError_t launch_batch_gauges(int64_t pitch, const R *stg0, int64_t inst_strid
 template <typename R>
 cudaError_t launch_update_max_stage_every(int nx, int ny, int64_t pitch, const R *stg, R *max_stage,
                                           const StepConfig &c, const DevScalars *sc, int every, cudaStream_t s);
+// The optional max_U_variables (bits: 1 time_of_max_stage, 2 max_speed,
+// 4 max_flux, 8 arrival_time, 16 min_stage; planes of nx x ny elements in
+// bit order, `plane` elements apart) and the flags update_max_quantities
+// reads.
+struct MaxUConfig {
+    int mask;
+    int include_dry;        // stage_extrema_include_dry_cells
+    int staggered;          // is_staggered_grid
+    int truely_linear;      // the staggered max_speed uses msl_linear depths
+    double arrival;         // msl_linear + arrival_stage_threshold_above_msl_linear
+    void *planes;
+    int64_t plane;
+};
+template <typename R>
+cudaError_t launch_update_max_u(int nx, int ny, int64_t pitch, const R *stg, const R *uh, const R *vh, const R *elv,
+                                R *max_stage, const StepConfig &c, const MaxUConfig &mu, const DevScalars *sc,
+                                int every, cudaStream_t s);
 // A static step (before static_before_time): clock and counters only.
 cudaError_t launch_static_step(DevScalars *sc, double dt, int has_dt, cudaStream_t s);
 template <typename R>

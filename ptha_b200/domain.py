@@ -248,6 +248,24 @@ class Domain:
         """domain%max_U_update_frequency: max_stage updated every `every` steps."""
         check(self._L.swals_gpu_set_max_U_update_frequency(self._h, int(every)))
 
+    MAX_U_VARIABLES = {"time_of_max_stage": 1, "max_speed": 2, "max_flux": 4, "arrival_time": 8, "min_stage": 16}
+
+    def set_max_U_variables(self, names=(), stage_extrema_include_dry_cells=True,
+                            arrival_stage_threshold_above_msl_linear=0.01):
+        """The max_U_variables recorded after max_stage (before the first step)."""
+        mask = 0
+        for n in names:
+            mask |= self.MAX_U_VARIABLES[n]
+        check(self._L.swals_gpu_set_max_U_variables(self._h, mask, int(bool(stage_extrema_include_dry_cells)),
+                                                     float(arrival_stage_threshold_above_msl_linear)))
+
+    def max_U(self, name):
+        """One recorded max_U variable as an (ny, nx) array."""
+        nx, ny = self.nx
+        out = np.empty(nx * ny, dtype=np.float64)
+        check(self._L.swals_gpu_download_max_U(self._h, self.MAX_U_VARIABLES[name], out.ctypes.data))
+        return out.reshape(ny, nx)
+
     def clear_eddy_viscosity(self):
         check(self._L.swals_gpu_set_eddy_viscosity(self._h, 0, 0.0, 0.0))
 

@@ -67,3 +67,40 @@ def test_max_U_update_frequency(method):
     np.testing.assert_array_equal(g.max_stage()[m], o.max_stage[m])
     np.testing.assert_array_equal(b.max_stage()[m], o.max_stage[m])
     np.testing.assert_array_equal(b.get_U(), g.get_U())
+
+
+MAX_U = ("time_of_max_stage", "max_speed", "max_flux", "arrival_time", "min_stage")
+
+
+@pytest.mark.parametrize("method,include_dry,every", [
+    ("rk2", True, 1), ("rk2", False, 2), ("linear", True, 1), ("leapfrog_nonlinear", False, 1),
+    ("leapfrog_linear_plus_nonlinear_friction", True, 3)])
+def test_max_U_variables(method, include_dry, every):
+    """The optional max_U_variables (time_of_max_stage, max_speed, max_flux,
+    arrival_time, min_stage; domain_mod.f90:2243-2404) and
+    stage_extrema_include_dry_cells, stepped and through evolve_steps."""
+    kw, U, nsq = _beach(method)
+    g, o = make_pair(kw, U, manning_sq=nsq)
+    b, _ = make_pair(kw, U, manning_sq=nsq)
+    dt = 0.25 * o.linear_timestep_max() if method not in ("rk2",) else 0.5 * o.nonlinear_stationary_timestep_max()
+    for d in (g, b):
+        d.set_max_U_variables(MAX_U, stage_extrema_include_dry_cells=include_dry,
+                              arrival_stage_threshold_above_msl_linear=0.02)
+        if every > 1:
+            d.set_max_U_update_frequency(every)
+    o.c.max_U_extra = 31
+    o.c.stage_extrema_include_dry_cells = int(include_dry)
+    o.c.arrival_stage_threshold_above_msl_linear = 0.02
+    o.c.max_U_update_frequency = every
+    for _ in range(45):
+        g.evolve_one_step(dt)
+        o.evolve_one_step(dt)
+    b.evolve_steps(45, dt)
+    _exact(g, o, f"{method} max_U")
+    m = water_mask(o.U[3])
+    for d in (g, b):
+        np.testing.assert_array_equal(d.max_stage()[m], o.max_stage[m])
+        for k, name in enumerate(MAX_U):
+            np.testing.assert_array_equal(d.max_U(name), o.max_U_extra[k], err_msg=name)
+    assert np.any(o.max_U_extra[3] > 0)        # the wave arrived somewhere
+    assert np.any(o.max_U_extra[1] > 0)
