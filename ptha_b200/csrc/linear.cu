@@ -908,8 +908,8 @@ __global__ void __launch_bounds__(256) friction_work_kernel(const LinArgs<R> a, 
     depth_jph = (depth_jph > mad) ? depth_jph : mad;
     const R nsq_iph = half * (nsq[o] + nsq[oe]);
     const R nsq_jph = half * (nsq[o] + nsq[on]);
-    fw[o] = g * nsq_iph * R(pow_friction_cr<CHEZY>((double)depth_iph));
-    fw[(int64_t)ny * P + o] = g * nsq_jph * R(pow_friction_cr<CHEZY>((double)depth_jph));
+    fw[o] = g * nsq_iph * R(pow_friction<CHEZY>((double)depth_iph));
+    fw[(int64_t)ny * P + o] = g * nsq_jph * R(pow_friction<CHEZY>((double)depth_jph));
 }
 
 // The friction multipliers of leapfrog_linear_plus_nonlinear_friction on the
@@ -1724,15 +1724,18 @@ __global__ void max_u_kernel(int nx, int ny, int64_t P, const R *stg, const R *u
     if (mu.mask & 2) {
         R v;
         if (mu.staggered) {
-            const int ip1 = min(i + 1, nx - 1), jp1 = min(r + 1, ny - 1);
-            const int64_t oe = (int64_t)r * P + ip1, on = (int64_t)jp1 * P + i;
+            // 0.5 * sum(x(i:ip1)) with ip1 = min(i+1, nx): on the last column
+            // (row) the slice holds the cell alone, so the face depth is half
+            // the cell's own depth.
+            const bool has_e = (i + 1 < nx), has_n = (r + 1 < ny);
+            const int64_t oe = (int64_t)r * P + (has_e ? i + 1 : i), on = (int64_t)(has_n ? r + 1 : r) * P + i;
             R de, dn;
             if (mu.truely_linear) {
-                de = half * ((msl - e) + (msl - elv[oe]));
-                dn = half * ((msl - e) + (msl - elv[on]));
+                de = has_e ? half * ((msl - e) + (msl - elv[oe])) : half * (msl - e);
+                dn = has_n ? half * ((msl - e) + (msl - elv[on])) : half * (msl - e);
             } else {
-                de = half * ((s - e) + (stg[oe] - elv[oe]));
-                dn = half * ((s - e) + (stg[on] - elv[on]));
+                de = has_e ? half * ((s - e) + (stg[oe] - elv[oe])) : half * (s - e);
+                dn = has_n ? half * ((s - e) + (stg[on] - elv[on])) : half * (s - e);
             }
             const R dei = (de > mad) ? one / de : zero, dni = (dn > mad) ? one / dn : zero;
             const R u = uh[o], w = vh[o];

@@ -104,3 +104,33 @@ def test_max_U_variables(method, include_dry, every):
             np.testing.assert_array_equal(d.max_U(name), o.max_U_extra[k], err_msg=name)
     assert np.any(o.max_U_extra[3] > 0)        # the wave arrived somewhere
     assert np.any(o.max_U_extra[1] > 0)
+
+
+@pytest.mark.parametrize("method", ["rk2", "linear"])
+def test_max_U_variables_fp32(method):
+    """FP32 state (real_bytes=4, the reference's -DREALFLOAT) against the FP32
+    oracle: the device clock is rounded to float for time_of_max_stage and
+    arrival_time, and the arrival threshold is float(msl) + float(threshold)."""
+    kw, U, nsq = _beach(method)
+    g, o = make_pair(kw, U, manning_sq=nsq, real32=True, oracle_real32=True)
+    dt = 0.25 * o.linear_timestep_max() if method != "rk2" else 0.5 * o.nonlinear_stationary_timestep_max()
+    g.set_max_U_variables(MAX_U, stage_extrema_include_dry_cells=True, arrival_stage_threshold_above_msl_linear=0.02)
+    o.c.max_U_extra = 31
+    o.c.arrival_stage_threshold_above_msl_linear = 0.02
+    for _ in range(45):
+        g.evolve_one_step(dt)
+        o.evolve_one_step(dt)
+    Ug = g.get_U()
+    m = water_mask(o.U[3])
+    for k in range(3):
+        a, b = Ug[k][m].astype(np.float64), o.U[k][m].astype(np.float64)
+        assert np.max(np.abs(a - b)) <= 1e-5 * max(np.max(np.abs(b)), 1.0), k
+    for k, name in enumerate(MAX_U):
+        got = np.asarray(g.max_U(name), np.float64)[m]
+        ref = np.asarray(o.max_U_extra[k], np.float64)[m]
+        if name in ("time_of_max_stage", "arrival_time"):
+            # float32 times: equal wherever the same step set the value
+            assert np.mean(got == ref) >= 0.99, name
+        else:
+            assert np.max(np.abs(got - ref)) <= 1e-5 * max(np.max(np.abs(ref)), 1.0), name
+    assert np.any(o.max_U_extra[3] > 0)
