@@ -37,6 +37,7 @@ struct swals_batch {
     int graph_steps = 0;
     double graph_dt = 0.0;
     bool graph_gauges = false;
+    int graph_cur = -1;       // state buffer the graph starts from (and returns to)
     int *d_rec = nullptr;     // device record counter used inside graphs
 };
 
@@ -141,6 +142,7 @@ int build_graph(swals_batch *b, int steps, double dt, bool gauges)
     b->graph_steps = steps;
     b->graph_dt = dt;
     b->graph_gauges = gauges;
+    b->graph_cur = cur0;
     return SWALS_OK;
 }
 
@@ -340,7 +342,10 @@ int swals_gpu_batch_evolve(swals_batch *b, int32_t nsteps, double dt)
     int done = 0;
     if (nsteps >= 2) {
         int gsteps = nsteps < 32 ? (nsteps & ~1) : 32;
-        if (!b->graph || b->graph_steps != gsteps || b->graph_dt != dt || b->graph_gauges != gauges) {
+        // an odd number of single steps since the capture flips the buffer
+        // the graph would start from: capture again
+        if (!b->graph || b->graph_steps != gsteps || b->graph_dt != dt || b->graph_gauges != gauges ||
+            b->graph_cur != b->cur) {
             int rc = build_graph(b, gsteps, dt, gauges);
             if (rc) return rc;
         }

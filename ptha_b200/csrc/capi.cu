@@ -702,8 +702,11 @@ int swals_gpu_evolve_steps(swals_domain *d, int32_t nsteps, double timestep, int
     }
     const bool use_graph = !d->timers_on && !d->static_pending && (nsteps - done) >= 2 * GRAPH_STEPS;
     if (use_graph) {
+        // The graph reads and writes the state buffers it was captured
+        // with: it is valid only while the step sequence starts from the
+        // same buffer (steps taken one by one in between rotate it).
         const bool same = d->step_graph && d->graph_dt == timestep && d->graph_has_dt == (has_timestep != 0) &&
-                          d->graph_stream == d->stream && d->graph_gauges == d->n_gauges;
+                          d->graph_stream == d->stream && d->graph_gauges == d->n_gauges && d->graph_cur == d->cur;
         if (!same) {
             drop_step_graph(d);
             const int cur0 = d->cur;
@@ -729,6 +732,7 @@ int swals_gpu_evolve_steps(swals_domain *d, int32_t nsteps, double timestep, int
             d->graph_has_dt = has_timestep != 0;
             d->graph_stream = d->stream;
             d->graph_gauges = d->n_gauges;
+            d->graph_cur = d->cur;
         }
         while (nsteps - done >= GRAPH_STEPS) {
             CK(cudaGraphLaunch(d->step_graph, d->stream));

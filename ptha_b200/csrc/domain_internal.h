@@ -74,6 +74,7 @@ struct swals_domain {
     bool graph_has_dt = false;
     cudaStream_t graph_stream = nullptr;
     int graph_gauges = -1;
+    int graph_cur = -1;            // state buffer the graph starts from (and returns to)
     int64_t graph_launches = 0;
     // misfit_gradient's replayed graphs (segments of K steps), valid for
     // (adj_K, adj_ng, adj_dt, ws).

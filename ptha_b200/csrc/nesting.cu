@@ -654,6 +654,7 @@ struct swals_multidomain {
     cudaGraphExec_t graph_exec = nullptr;
     int graph_steps = 0;
     double graph_dt = 0.0;
+    std::vector<int> graph_cur;   // each domain's state buffer at the capture
 };
 
 namespace {
@@ -1219,6 +1220,7 @@ int swals_gpu_md_capture_graph(swals_multidomain *md, int32_t nsteps, double dt)
     md->graph = g;
     md->graph_steps = nsteps;
     md->graph_dt = dt;
+    md->graph_cur = cur0;
     return SWALS_OK;
 }
 
@@ -1226,6 +1228,11 @@ int swals_gpu_md_replay(swals_multidomain *md, int32_t nreplays)
 {
     if (!md || nreplays < 0) return fail(SWALS_ERR_INVALID_ARGUMENT, "bad argument");
     if (!md->graph_exec) return fail(SWALS_ERR_INVALID_ARGUMENT, "no captured graph");
+    for (size_t k = 0; k < md->doms.size(); k++)
+        if (md->doms[k]->cur != md->graph_cur[k])
+            return fail(SWALS_ERR_INVALID_ARGUMENT,
+                        "domain %d has moved to another state buffer since the graph was captured (md steps taken "
+                        "in between that are not a multiple of 3); capture the graph again", (int)k);
     MDCK(cudaSetDevice(md->device));
     for (int r = 0; r < nreplays; r++) {
         MDCK(cudaGraphLaunch(md->graph_exec, md->stream));
