@@ -35,8 +35,14 @@ def build():
     subprocess.run(["make", "-s", "-C", HERE], check=True)
 
 
-def _load(real32: bool):
-    name = "liboracle32.so" if real32 else "liboracle64.so"
+# Oracle builds (oracle/Makefile): the IEEE-strict checker, the same with
+# libm's pow for the friction power law, and the -Ofast-style baseline build.
+VARIANTS = {"strict": "liboracle64.so", "libm": "liboracle64_libm.so", "fast": "liboracle64_fast.so",
+            "native": "liboracle64_native.so"}
+
+
+def _load(real32: bool, variant: str = "strict"):
+    name = "liboracle32.so" if real32 else VARIANTS[variant]
     path = os.path.join(HERE, name)
     if not os.path.exists(path):
         build()
@@ -111,10 +117,10 @@ class OracleDomain:
                  linear_friction_coeff=0.0, maximum_timestep=1.0e20,
                  boundary_exterior=(True, True, True, True), bc_kind=BC_NONE,
                  bf_kind=0, bf_params=(), record_max_stage=True, real32=False,
-                 xL=0, xU=0, yL=0, yU=0, compute_fluxes_inner_method="DE1_low_fr_diffusion"):
+                 xL=0, xU=0, yL=0, yU=0, compute_fluxes_inner_method="DE1_low_fr_diffusion", variant="strict"):
         self.real32 = real32
         self.dtype = np.float32 if real32 else np.float64
-        self.lib = _load(real32)
+        self.lib = _load(real32, variant)
         self.pref = "oracle32_" if real32 else "oracle64_"
         if coriolis is None:
             coriolis = bool(spherical)

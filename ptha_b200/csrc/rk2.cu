@@ -241,7 +241,7 @@ __global__ void __launch_bounds__(NT, 3) rk2_stage_kernel(const Rk2Args<R> a)
 
     const R dt = stage_dt<R>(a);
     fv_update<R, MODE, SPH, COR, FRIC>(a, i, r, S.cell.get(rr + 2, cc + 2), S.ens.get(rr, cc), S.ens.get(rr + 1, cc),
-                                       S.eew.get(rr, cc), S.eew.get(rr, cc + 1), dt);
+                                       S.eew.get(rr, cc), S.eew.get(rr, cc + 1), dt, dt / a.m.area[r]);
 }
 
 
@@ -628,7 +628,8 @@ __global__ void __launch_bounds__(256, 4) rk2_update_kernel(const Rk2Args<R> a)
             w_hi.es_neg = 0.0;
         }
         w_hi.es_pos = 0.0;
-        fv_update<R, MODE_STAGE1, SPH, COR, FRIC>(a, i, r, c, n_lo, n_hi, w_lo, w_hi, stage_dt<R>(a));
+        const R dt = stage_dt<R>(a);
+        fv_update<R, MODE_STAGE1, SPH, COR, FRIC>(a, i, r, c, n_lo, n_hi, w_lo, w_hi, dt, dt / a.m.area[r]);
     }
     for (int off = 16; off > 0; off >>= 1) negfix += __shfl_down_sync(0xffffffffu, negfix, off);
     if ((threadIdx.x & 31) == 0 && negfix)

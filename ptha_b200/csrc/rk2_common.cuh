@@ -239,10 +239,12 @@ __device__ __forceinline__ R stage_dt(const Rk2Args<R> &a)
 // update_U for cell (i, r) (update_U_DE1_inner_include.f90:38-96) from its
 // fixed-up centre values and its four edges, with the explicit sources
 // accumulated in the reference's order; stage 2 also forms the rk2 average.
+// inv_cell_area_dt is the row's dt / area_cell_y(r) (a row constant the
+// callers may evaluate once per row).
 template <typename R, int MODE, bool SPH, bool COR, int FRIC>
 __device__ __forceinline__ void fv_update(const Rk2Args<R> &a, int i, int r, const Cell<R> &c, const EdgeRes<R> &n_lo,
                                           const EdgeRes<R> &n_hi, const EdgeRes<R> &w_lo, const EdgeRes<R> &w_hi,
-                                          R dt)
+                                          R dt, R inv_cell_area_dt)
 {
     const int nx = a.nx, ny = a.ny;
     const int64_t P = a.P;
@@ -260,7 +262,6 @@ __device__ __forceinline__ void fv_update(const Rk2Args<R> &a, int i, int r, con
         U_stg = a.stg0[o]; U_uh = a.uh0[o]; U_vh = a.vh0[o];
     }
 
-    const R inv_cell_area_dt = dt / a.m.area[r];
     U_stg = U_stg - inv_cell_area_dt * ((n_hi.f[0] - n_lo.f[0]) + (w_hi.f[0] - w_lo.f[0]));
     U_uh = U_uh - inv_cell_area_dt * ((n_hi.f[1] - n_lo.f[1]) + (w_hi.f[1] - w_lo.f[1]));
     U_vh = U_vh - inv_cell_area_dt * ((n_hi.f[2] - n_lo.f[2]) + (w_hi.f[2] - w_lo.f[2]));
@@ -299,7 +300,7 @@ __device__ __forceinline__ void fv_update(const Rk2Args<R> &a, int i, int r, con
         } else {
             const R depth = c.dep;
             const R fs = a.nsq[o] * R(sqrt(c.u * c.u + c.v * c.v)) *
-                         R(pow_friction_cr<FRIC == FRIC_CHEZY>((double)rmax(depth, mad)));
+                         R(pow_friction<FRIC == FRIC_CHEZY>((double)rmax(depth, mad)));
             implicit_factor = R(1) / ((R(1) + dt * K<R>::gravity() * rmax(depth, R(0)) * fs) + dt * a.lin_fric);
         }
         U_uh = R((double)U_uh + (double)inv_cell_area_dt * es_uh);

@@ -34,9 +34,16 @@ constexpr int SWARPS = SWALS_STREAM_WARPS;   // warps per CTA
 #endif
 #ifndef SWALS_STREAM_ROWS
 // Rows per warp strip.  Measured on the 2048^2 rk2 step (B200): 12 rows
-// beat 32 by 4 % despite the larger share of the two lead-in rows, as the
-// more numerous, shorter strips balance better over the SMs; more CTAs
-// per SM (a lower register cap) spill and lose 15-25 %.
+// beat 32 by 4 % (and 24 by 2 %) despite the larger share of the two
+// lead-in rows, as the more numerous, shorter strips balance better over
+// the SMs; more CTAs per SM (a lower register cap) spill and lose 15-25 %.
+// Also measured and dropped: a persistent one-wave launch with equal
+// contiguous runs per warp (fewer recomputed halo rows, 8 % slower), the
+// same grid looping over 12-row strips (15 % slower), the row constants
+// dt/area and 1/(dx cfl/2) evaluated once per 32 rows and shuffled (2 %
+// slower: the extra live registers spill), 3 CTAs per SM without spills
+// (18 % slower), and FMA contraction (2 % faster, but no longer bit-exact
+// with the IEEE-strict oracle, and 2e-9 relative after 600 steps).
 #define SWALS_STREAM_ROWS 12
 #endif
 constexpr unsigned FULL = 0xffffffffu;
@@ -236,7 +243,7 @@ __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_STREAM_MIN_CTAS) rk2_str
             e_e.f[0] = dn1(e_w.f[0]); e_e.f[1] = dn1(e_w.f[1]); e_e.f[2] = dn1(e_w.f[2]);
             e_e.es_neg = dn1(e_w.es_neg);
             e_e.es_pos = 0.0;
-            if (out_lane) fv_update<R, MODE, SPH, COR, FRIC>(a, i, R_, c2, e_s, e_n, e_w, e_e, dt);
+            if (out_lane) fv_update<R, MODE, SPH, COR, FRIC>(a, i, R_, c2, e_s, e_n, e_w, e_e, dt, dt / a.m.area[R_]);
         }
         e_s = e_n;
     }

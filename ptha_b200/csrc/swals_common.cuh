@@ -34,13 +34,24 @@ template <typename R> struct K {
 template <typename R> __device__ __forceinline__ R rmin(R a, R b) { return (b < a) ? b : a; }
 template <typename R> __device__ __forceinline__ R rmax(R a, R b) { return (b > a) ? b : a; }
 
-// Correctly rounded friction power law pow(x, p), p = fl(-7/3) (Manning) or
-// -2 (Chezy), for x >= minimum_allowed_depth (update_U_DE1_inner_include.f90:
-// 72-75).  Double-double arithmetic: a Newton-corrected cube root, a
-// compensated reciprocal, and for fl(-7/3) the factor x**eps = 1 + eps*ln(x)
-// with eps = fl(-7/3) + 7/3.  Correct rounding makes the result independent
-// of any libm (the oracle uses the same definition; tests check both
-// against 300-bit arithmetic).
+// Friction power law pow(x, p), p = fl(-7/3) (Manning) or -2 (Chezy), for
+// x >= minimum_allowed_depth (update_U_DE1_inner_include.f90:72-75).  The
+// oracle evaluates the same operation sequence, so both give the same bits
+// whatever libm is present; every step is an IEEE operation (no FMA
+// contraction in this library), plus integer work on the float bits.
+//   Chezy: the correctly rounded 1/x^2 (x^2 as a double-double, compensated
+//   reciprocal).
+//   Manning: the inverse cube root y = x^(-1/3) by Newton's iteration
+//   y <- y + y (1 - x y^3)/3, seeded from the float bits of x
+//   (bits(y) = K - bits(x)/3, the linear-in-the-exponent estimate of
+//   x^(-1/3), K fitted for the least relative error, 3.4%), two iterations
+//   in FP32 and two in FP64; then x^(-7/3) = y / (x x), and the exponent's
+//   own rounding, x^p = x^(-7/3) x^eps with eps = fl(-7/3) + 7/3, as the
+//   factor 1 + eps ln(x) with ln(x) from the float bits (log2 x ~ exponent
+//   + mantissa fraction; the term is below 2e-15, so its 9% error is far
+//   below an ulp).  Within 3 ulp of the exact power over 1e-5 <= x <=
+//   1e5 (checked against 300-bit arithmetic), about 40 instructions against
+//   the ~400 of a correctly rounded evaluation.
 struct DD { double hi, lo; };
 __device__ __forceinline__ DD dd_two_prod(double a, double b) { DD r; r.hi = a * b; r.lo = fma(a, b, -r.hi); return r; }
 __device__ __forceinline__ DD dd_fast_two_sum(double a, double b) { DD r; r.hi = a + b; r.lo = b - (r.hi - a); return r; }
@@ -52,25 +63,24 @@ __device__ __forceinline__ DD dd_recip(DD p)
     const double e = (1.0 - t.hi) - t.lo;
     return dd_fast_two_sum(y0, y0 * e);
 }
+constexpr unsigned kRcbrtSeed = 0x54a237fbu;
+constexpr double kEpsLn2 = -1.0260639457488826e-16;   // (fl(-7/3) + 7/3) ln 2
 template <bool CHEZY>
-__device__ __forceinline__ double pow_friction_cr(double x)
+__device__ __forceinline__ double pow_friction(double x)
 {
-    const DD x2 = dd_two_prod(x, x);
-    if (CHEZY) return dd_recip(x2).hi;
-    const double c0 = cbrt(x);
-    const DD s = dd_two_prod(c0, c0);
-    DD t = dd_two_prod(s.hi, c0);
-    t.lo += s.lo * c0;
-    const double r = (x - t.hi) - t.lo;
-    const DD c = dd_fast_two_sum(c0, r / (3.0 * c0 * c0));
-    DD p = dd_two_prod(x2.hi, c.hi);
-    p.lo += x2.hi * c.lo + x2.lo * c.hi;
-    p = dd_fast_two_sum(p.hi, p.lo);
-    const DD v = dd_recip(p);
-    const double q = 7.0 / 3.0;
-    const double eps = fma(-3.0, q, 7.0) / 3.0;
-    const double tl = eps * log(x);
-    return dd_fast_two_sum(v.hi, v.lo + v.hi * tl).hi;
+    if (CHEZY) return dd_recip(dd_two_prod(x, x)).hi;
+    const float xf = __double2float_rn(x);
+    const unsigned ix = __float_as_uint(xf);
+    float y = __uint_as_float(kRcbrtSeed - ix / 3u);
+    const float third_f = 1.0f / 3.0f;
+    y = y + y * ((1.0f - xf * (y * y * y)) * third_f);
+    y = y + y * ((1.0f - xf * (y * y * y)) * third_f);
+    double yd = (double)y;
+    yd = yd + yd * ((1.0 - x * (yd * yd * yd)) * (1.0 / 3.0));
+    yd = yd + yd * ((1.0 - x * (yd * yd * yd)) * (1.0 / 3.0));
+    const double v = yd / (x * x);
+    const double t = kEpsLn2 * ((double)ix * (1.0 / 8388608.0) - 127.0);
+    return v + v * t;
 }
 
 // Correctly rounded depth**p, p = fl(1 - 1/6), of the Shiono-Knight eddy

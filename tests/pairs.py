@@ -5,7 +5,7 @@ import numpy as np
 from oracle import oracle as orc
 
 
-def oracle_from_kw(kw, real32=False):
+def oracle_from_kw(kw, real32=False, variant="strict"):
     nx, ny = kw["nx"]
     return orc.OracleDomain(
         nx, ny, kw["lw"], lower_left=kw.get("lower_left", (0.0, 0.0)),
@@ -20,7 +20,7 @@ def oracle_from_kw(kw, real32=False):
         bf_params=kw.get("boundary_function_params", ()),
         xL=kw.get("xL", 0), xU=kw.get("xU", 0), yL=kw.get("yL", 0), yU=kw.get("yU", 0),
         compute_fluxes_inner_method=kw.get("compute_fluxes_inner_method", "DE1_low_fr_diffusion"),
-        real32=real32)
+        real32=real32, variant=variant)
 
 
 def make_pair(kw, U, manning_sq=None, real32=False, oracle_real32=False):
