@@ -14,10 +14,13 @@
 // device share it and it keeps the last call's partial sums; every row that
 // a call reads is written by the same call first, so nothing has to be
 // cleared between calls.  Calls whose kernels overlap on the GPU (different
-// streams without ordering) race on the shared scratch.
+// streams without ordering) race on the shared scratch.  The array's device
+// address is looked up once per device and context (again after a device
+// reset), never per call.
 #include "swals_kernels.h"
 #include "../../include/swals_gpu.h"
 
+#include <cuda.h>   // CUcontext (type only; the function is fetched through the runtime)
 #include <mutex>
 
 namespace {
@@ -26,7 +29,31 @@ static __device__ __align__(256) double g_noalloc_row_sums[SWALS_NOALLOC_MAX_ROW
 
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
-double *g_row_sums_dev[kMaxDevices] = {};  // device address of g_noalloc_row_sums, per device
+// Device address of g_noalloc_row_sums, per device ordinal, and the context
+// it was looked up in: after cudaDeviceReset (or any new primary context on
+// that ordinal) the array lives at a new address, so a changed context
+// means a fresh look-up rather than a stale pointer.
+double *g_row_sums_dev[kMaxDevices] = {};
+CUcontext g_row_sums_ctx[kMaxDevices] = {};
+
+typedef CUresult (*CtxGetCurrentFn)(CUcontext *);
+
+CUcontext current_context()
+{
+    static CtxGetCurrentFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (CtxGetCurrentFn)p;
+    }
+    CUcontext c = nullptr;
+    if (fn) fn(&c);
+    return c;
+}
 
 template <typename R>
 __global__ void noalloc_row_volume_kernel(int nx, int ny, int64_t P, const R *stg, const R *elv, int n_ext,
@@ -68,11 +95,15 @@ int scratch_for_current_device(double **out)
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
         return noalloc_fail(SWALS_ERR_NO_DEVICE, "no current CUDA device");
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_row_sums_dev[dev]) {
+    // A thread that has not used the runtime yet may have no context bound
+    // (null): the look-up below binds the device's primary context.
+    const CUcontext ctx = current_context();
+    if (!g_row_sums_dev[dev] || !ctx || g_row_sums_ctx[dev] != ctx) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_row_sums);
         if (e != cudaSuccess || !p) return noalloc_fail(SWALS_ERR_CUDA, "cudaGetSymbolAddress failed for the scratch array");
         g_row_sums_dev[dev] = (double *)p;
+        g_row_sums_ctx[dev] = current_context();
     }
     *out = g_row_sums_dev[dev];
     return SWALS_OK;
