@@ -1,21 +1,31 @@
 #!/usr/bin/env python
 """Benchmark of the SWALS time-step hot path on B200.
 
-Workload (one GPU): nonlinear finite-volume 'rk2' with wetting and drying on
-a 2048 x 2048 Cartesian grid, dx = 10 m, planar beach from -50 m to +10 m
-(slope 1/40) plus 30 seeded 0.5 m Gaussian bumps, Manning n = 0.025, a
-solitary wave (H/d = 0.1) entering through the west boundary, walls
-elsewhere, FP64, adaptive CFL timestep (cfl 0.99, theta 1.6).  One bench
-step = 2000 model timesteps, so the default 10 timed steps are the
+Headline workload (one GPU): nonlinear finite-volume 'rk2' with wetting and
+drying on a 2048 x 2048 Cartesian grid, dx = 10 m, planar beach from -50 m
+to +10 m (slope 1/40) plus 30 seeded 0.5 m Gaussian bumps, Manning
+n = 0.025, a solitary wave (H/d = 0.1) entering through the west boundary,
+walls elsewhere, FP64, adaptive CFL timestep (cfl 0.99, theta 1.6).  One
+bench step = 2000 model timesteps, so the default 10 timed steps are the
 configuration's 20000 timesteps.  Synthetic seeded data.
 
 metric: cell-updates/s = nx * ny * timesteps / device seconds (all GPUs).
 
+The same JSON line carries, under "forms", the metric's other forms timed
+on the same GPU right after the headline (N = 1 only): the plain FP64
+leapfrog at 4096^2 and 8192^2 against the HBM roofline, the batched FP32
+leapfrog (3600 x 2400 x 256 instances) against the per-instance loop, the
+adjoint misfit gradient (1200 x 800, K = 50) against one forward solve, and
+the nested four-domain configuration (one source, and 16 sources as a
+batch of nests).
+
   python bench.py [--gpus N --steps K --warmup W]   # our CUDA path
   python bench.py --impl reference ...              # CPU restatement of the
                                                     # reference's OpenMP loops
-Under torchrun each rank advances its own replica of the domain (the path
-does not shard: replicas only) and rank 0 prints one JSON line.
+  python bench.py --workload linear|batched|adjoint|multidomain|nested16
+                                                    # one form on its own line
+Under torchrun each rank advances its own replica of the headline domain
+(the path does not shard: replicas only) and rank 0 prints one JSON line.
 """
 from __future__ import annotations
 
@@ -36,7 +46,6 @@ METRIC = "cell-updates/s/GPU (fwd, batched, adjoint) at FP64-oracle tol; HBM % o
 UNIT = "cell-updates/s"
 INNER = 2000          # model timesteps per bench step (default)
 N = 2048              # grid cells per side (default)
-WORKLOAD = "rk2_beach_2048x2048_fp64_adaptive"
 # Algorithmic HBM bytes per cell for the fused FV stage kernel (FP64):
 #   stage 1 reads STG,UH,VH,ELV,n^2 and writes STG,UH,VH            = 8 planes
 #   stage 2 reads the same 5 + backup U0 (3), writes 3, max_stage r+w = 13 planes
@@ -119,9 +128,11 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(workload="rk2_beach", min_seconds=12.0, exact_steps=0):
+def cpu_baseline(workload="rk2_beach", min_seconds=12.0, exact_steps=0, variant="native"):
+    """The oracle on this machine's host cores, in its own process (its OpenMP
+    runtime never shares a process with the GPU runtime)."""
     cmd = [sys.executable, os.path.join(ROOT, "oracle", "cpu_baseline.py"), "--workload", workload,
-           "--min-seconds", str(min_seconds)]
+           "--min-seconds", str(min_seconds), "--variant", variant]
     if exact_steps:
         cmd += ["--exact-steps", str(exact_steps)]
     env = dict(os.environ)
@@ -129,8 +140,18 @@ def cpu_baseline(workload="rk2_beach", min_seconds=12.0, exact_steps=0):
     env.setdefault("OMP_PROC_BIND", "true")
     out = subprocess.run(cmd, capture_output=True, text=True, env=env, check=True)
     r = json.loads(out.stdout.strip().splitlines()[-1])
-    return {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": "port",
-            "sample": r["sample"] + " (C restatement of the reference's OpenMP loops; no Fortran compiler)"}
+    return {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": "port", "variant": r["variant"],
+            "sample": r["sample"] + "; C restatement of the reference's OpenMP loops (no Fortran compiler)"}
+
+
+def headline_config(n, real32=False, world=1):
+    """The workload, identical in both arms' lines."""
+    return {"workload": f"rk2_beach_{n}x{n}_{'fp32' if real32 else 'fp64'}_adaptive", "nx": n, "ny": n,
+            "parallelism": f"replicas x{world}",
+            "timestepping_method": "rk2", "dt": "adaptive (CFL, cfl=0.99)", "theta": 1.6, "manning_n": 0.025,
+            "boundary": "solitary wave H/d=0.1 west, walls elsewhere", "gauges": 9,
+            "l2": "inputs larger than L2 (state 4x32 MB + manning 32 MB + max_stage 32 MB + stage copies; "
+                  "~0.7 GB streamed per timestep)"}
 
 
 def dist_setup(ngpus):
@@ -141,28 +162,57 @@ def dist_setup(ngpus):
 
 
 def run_reference(args, world, rank):
+    """The reference's CPU path for this workload: the oracle built with the
+    flags the reference ships (-O3 -ffast-math, libm pow) plus -march=native
+    on this machine, all host threads; each bench step a bounded sample of
+    the same 2048^2 workload (a few timesteps from the initial state; the
+    per-timestep cost of these loops does not depend on the state)."""
     if rank != 0:
         return
-    # Each step: a bounded sample (a few timesteps) of the same 2048^2 workload.
-    steps_per = 3
-    cpu_baseline("rk2_beach", exact_steps=steps_per * max(1, args.warmup))  # warm-up (page-in, threads)
+    steps_per = 4
+    r = cpu_baseline("rk2_beach", exact_steps=steps_per * max(1, args.warmup))  # warm-up (build, page-in, threads)
+    variant = r["variant"]
     vals = []
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        r = cpu_baseline("rk2_beach", exact_steps=steps_per)
+        r = cpu_baseline("rk2_beach", exact_steps=steps_per, variant=variant)
         vals.append(r["value"])
     wall = time.perf_counter() - t0
     value = statistics.median(vals)
+    strict = cpu_baseline("rk2_beach", exact_steps=steps_per, variant="strict")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": N * N * steps_per / value * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "nx": N, "ny": N, "timesteps_per_step": steps_per},
+            "config": headline_config(N, world=world), "timesteps_per_step": steps_per,
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": r["cores"], "kind": "port",
-                             "sample": f"{steps_per} rk2 timesteps of the 2048x2048 workload per step"},
+                             "sample": f"{steps_per} rk2 timesteps of the 2048x2048 workload per step; " + r["sample"],
+                             "strict_build_value": strict["value"]},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "wall_s": wall}
     print(json.dumps(line), flush=True)
+
+
+# Nominal FP64 peak of the FV kernels' pipe: 64 FP64 FMA lanes per SM
+# (B200: 37 TFLOP/s FP64 at 1965 MHz over 148 SMs), 2 flops per FMA.
+FP64_LANES_PER_SM = 64
+
+
+def profile_value(tag):
+    """A number committed in a profiles/ summary as `tag = value`."""
+    pdir = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(pdir):
+        return None
+    for fn in sorted(os.listdir(pdir)):
+        if not fn.endswith((".md", ".txt")):
+            continue
+        for line in open(os.path.join(pdir, fn)):
+            if line.startswith(tag + " ="):
+                try:
+                    return float(line.split("=")[1].split()[0])
+                except Exception:
+                    return None
+    return None
 
 
 def run_ours(args, world, rank, local):
@@ -185,7 +235,7 @@ def run_ours(args, world, rank, local):
     d = Domain(**kw, device=local)
     d.set_U(U)
     d.set_manning_squared(nsq)
-    d.gauges_setup(gauges, capacity=INNER * (args.warmup + args.steps + 8) + 16)
+    d.gauges_setup(gauges, capacity=INNER * (args.warmup + 2 * args.steps + 8) + 16)
     stream = torch.cuda.ExternalStream(d.stream(), device=f"cuda:{local}")
     cells = N * N
 
@@ -249,15 +299,31 @@ def run_ours(args, world, rank, local):
     achieved = bytes_kernel / (t2_ms / 1e3) / 1e9
     peak, peak_kind = hbm_peak()
     per_step_ms = {k: (v[0] / v[1] if v[1] else 0.0) for k, v in tm.items()}
+    step_ms = sum(per_step_ms.values())
+    stage2_share = per_step_ms["fv_stage2"] / step_ms if step_ms else None
+    # FP64 work of the same launch: flops per cell from the committed ncu
+    # count (dadd + dmul + 2 dfma thread instructions / cells).
+    fpc = profile_value("fp64_flops_per_cell[rk2_stream_kernel_stage2]") if not args.real32 else None
+    pipe = profile_value("fp64_pipe_active_frac[rk2_stream_kernel_stage2]") if not args.real32 else None
+    fp64 = None
+    if fpc:
+        sm_mhz = clocks.get("sm_mhz") or 1965.0
+        fp64_peak = 2.0 * FP64_LANES_PER_SM * props.multi_processor_count * sm_mhz * 1e6 / 1e12
+        fp64_ach = fpc * cells / (per_step_ms["fv_stage2"] / 1e3) / 1e12
+        fp64 = {"bound": "fp64", "achieved": fp64_ach, "peak": fp64_peak, "unit": "TFLOP/s",
+                "frac": fp64_ach / fp64_peak, "flops_per_cell": fpc,
+                "peak_source": f"nominal: {FP64_LANES_PER_SM} FP64 FMA lanes/SM x {props.multi_processor_count} "
+                               f"SMs x {sm_mhz:.0f} MHz (median under load)",
+                "pipe_active_frac_ncu": pipe}
 
     # End to end through the C ABI with host buffers: pinned H2D of the state,
-    # INNER timesteps, D2H of the state, every step.
+    # INNER timesteps, D2H of the state, every step; as many steps as timed above.
     tdt = torch.float32 if args.real32 else torch.float64
     pin_in = torch.empty((4, N, N), dtype=tdt, pin_memory=True)
     pin_in.copy_(torch.from_numpy(d.get_U()))
     pin_out = torch.empty((4, N, N), dtype=tdt, pin_memory=True)
     h_in, h_out = pin_in.numpy(), pin_out.numpy()
-    e2e_steps = 3
+    e2e_steps = args.steps
     barrier()
     torch.cuda.synchronize()
     e2 = torch.cuda.Event(enable_timing=True)
@@ -275,27 +341,38 @@ def run_ours(args, world, rank, local):
     e2e_value = cells * INNER * e2e_steps * world / (float(e2e_ms.item()) / 1e3)
     h2d = int(h_in.nbytes)
     d2h = int(h_out.nbytes)
+    d.close()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and N == 2048:
         try:
-            cpu = cpu_baseline("rk2_beach", min_seconds=12.0)
+            cpu = cpu_baseline("rk2_beach", min_seconds=10.0)
+            cpu["strict_build_value"] = cpu_baseline("rk2_beach", min_seconds=5.0, variant="strict")["value"]
         except Exception as ex:  # the baseline is reported, never required
             cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port", "sample": f"failed: {ex}"}
 
+    forms = None
+    if rank == 0 and world == 1 and not args.no_forms and N == 2048 and not args.real32:
+        forms = {}
+        for name, fn in (("linear_fp64", form_linear_sweep), ("batched", form_batched), ("adjoint", form_adjoint),
+                         ("multidomain", form_multidomain), ("nested16", form_nested16)):
+            t0 = time.perf_counter()
+            try:
+                forms[name] = fn(local)
+            except Exception as ex:   # a form that fails is reported, the headline stands
+                forms[name] = {"error": f"{type(ex).__name__}: {ex}"}
+            forms[name]["wall_s"] = round(time.perf_counter() - t0, 1)
+            torch.cuda.empty_cache()
+
     if rank == 0:
+        cfg = headline_config(N, args.real32, world)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.real32 else "f64", "data": "synthetic",
-            "config": {"workload": (f"rk2_beach_{N}x{N}_{'fp32' if args.real32 else 'fp64'}_adaptive"),
-                       "nx": N, "ny": N, "timesteps_per_step": INNER,
-                       "timestepping_method": "rk2", "dt": "adaptive (CFL, cfl=0.99)", "theta": 1.6,
-                       "manning_n": 0.025, "boundary": "solitary wave H/d=0.1 west, walls elsewhere",
-                       "l2": "inputs larger than L2 (state 4x32 MB + manning 32 MB + max_stage 32 MB + "
-                             "stage copies; ~0.7 GB streamed per timestep)",
-                       "parallelism": f"replicas x{world}", "gauges": 9},
-            "roofline": {"bound": "hbm", "kernel": "rk2_stream_kernel stage 2 (dominant: ~42% of the step)",
+            "config": cfg, "timesteps_per_step": INNER,
+            "roofline": {"bound": "hbm",
+                         "kernel": f"rk2_stream_kernel stage 2 (dominant: {100 * stage2_share:.0f}% of the step)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": peak_kind,
                          "bytes_per_cell": BYTES_STAGE2 * es_scale,
@@ -303,7 +380,7 @@ def run_ours(args, world, rank, local):
                          "traffic": (profile_traffic("rk2_stream_kernel_stage2") if N == 2048 and not args.real32
                                      else None),
                          "traffic_unit": "DRAM bytes of one stage-2 launch (ncu, 2048x2048 FP64)",
-                         "bound_note": "FP64 issue/latency bound (DRAM ~10% busy); see profiles/",
+                         "fp64": fp64,
                          "step_effective_GBps": cells * BYTES_PER_CELL_UPDATE * es_scale /
                                                 (ms_max / args.steps / INNER / 1e3) / 1e9,
                          "per_launch_ms": per_step_ms},
@@ -313,18 +390,18 @@ def run_ours(args, world, rank, local):
             "gpu_launches": launches,
             "clocks": clocks,
             "state_ok": ok, "sim_time_s": st.time, "max_dt": st.max_dt,
+            "forms": forms,
         }
         print(json.dumps(line), flush=True)
-    d.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
 
 
 # ---------------------------------------------------------------------------
-# Secondary forms (`--workload linear|batched|adjoint`): one JSON line each,
-# for the evidence of the plain leapfrog roofline, the batched form against a
-# per-instance loop, and the adjoint's cost against a forward solve.
+# The metric's other forms.  Each returns a dict of device-timed numbers
+# (CUDA events on the stream the kernels run on); `--workload X` prints one
+# of them as a line of its own.
 
 def _event_ms(stream, fn):
     import torch
@@ -337,337 +414,259 @@ def _event_ms(stream, fn):
     return a.elapsed_time(b)
 
 
-def _dipoles(lon, lat, count, seed, band=((150.0, -40.0), (190.0, -10.0)), width_km=400.0):
-    """Compact dipole uplift patches in a band: a random centre within
-    width_km of the band's axis, extent L in U[50, 200] km, amplitude A in
-    U[0.5, 3] m, eta = A [G(s - L/4, n) - G(s + L/4, n)] with Gaussians of
-    sigma L/6 in band-aligned coordinates; evaluated within 3L of the centre
-    (zero beyond)."""
-    import numpy as np
-    rng = np.random.default_rng(seed)
-    (x0, y0), (x1, y1) = band
-    km_deg = 111.19
-    ang = np.arctan2(y1 - y0, x1 - x0)
-    out = []
-    for _ in range(count):
-        t = rng.uniform(0.0, 1.0)
-        off = rng.uniform(-0.5, 0.5) * width_km / km_deg
-        cx = x0 + t * (x1 - x0) - off * np.sin(ang)
-        cy = y0 + t * (y1 - y0) + off * np.cos(ang)
-        L = rng.uniform(50.0, 200.0)
-        A = rng.uniform(0.5, 3.0)
-        eta = np.zeros((len(lat), len(lon)))
-        r_deg = 3.0 * L / km_deg
-        ii = np.flatnonzero(np.abs(lon - cx) <= r_deg / max(np.cos(np.deg2rad(cy)), 0.2))
-        jj = np.flatnonzero(np.abs(lat - cy) <= r_deg)
-        if len(ii) and len(jj):
-            LON, LAT = np.meshgrid(lon[ii], lat[jj])
-            dx = (LON - cx) * km_deg * np.cos(np.deg2rad(cy))
-            dy = (LAT - cy) * km_deg
-            s_ = dx * np.cos(ang) + dy * np.sin(ang)
-            n_ = -dx * np.sin(ang) + dy * np.cos(ang)
-            sg = L / 6.0
-            eta[np.ix_(jj, ii)] = A * (np.exp(-((s_ - L / 4) ** 2 + n_ ** 2) / (2 * sg ** 2)) -
-                                       np.exp(-((s_ + L / 4) ** 2 + n_ ** 2) / (2 * sg ** 2)))
-        out.append(eta)
-    return out
-
-
-def run_form(args, local, world=1, rank=0):
-    import numpy as np
+def form_linear(local, n, inner=200, reps=3, warmup=1):
+    """The 400x400 Gaussian-basin configuration scaled up for the roofline
+    (dx 1 km, flat 4000 m, walls, CFL 0.7, FP64, max_stage on): device
+    throughput, and the step kernel's HBM fraction at 72 B per cell."""
     import torch
-    torch.cuda.set_device(local)
-    torch.zeros(1, device=f"cuda:{local}")
     from ptha_b200 import Domain, workloads
     peak, peak_kind = hbm_peak()
-    line = {"metric": METRIC, "unit": UNIT, "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
-            "vs_baseline": None}
-    if args.workload == "linear":
-        # The 400x400 Gaussian-basin configuration scaled up for the roofline
-        # sweep (dx 1 km, flat 4000 m, walls, CFL 0.7, FP64, max_stage on).
-        n = args.n if args.n != N else 8192
-        kw, U, gauges = workloads.linear_gaussian_basin(n=n)
-        d = Domain(**kw, device=local)
-        d.set_U(U)
-        dt = d.linear_timestep_max()
-        stream = torch.cuda.ExternalStream(d.stream(), device=f"cuda:{local}")
-        inner = max(1, args.inner if args.inner != INNER else 200)
-        for _ in range(args.warmup):
-            d.evolve_steps(inner, dt)
-        d.synchronize()
-        ms = _event_ms(stream, lambda: [d.evolve_steps(inner, dt) for _ in range(args.steps)])
-        value = n * n * inner * args.steps / (ms / 1e3)
-        d.timers_enable(True)
-        d.evolve_steps(50, dt)
-        tm = d.timers_read()
-        d.timers_enable(False)
-        t_ms, cnt = tm["leapfrog_step"]
-        achieved = n * n * 72.0 * cnt / (t_ms / 1e3) / 1e9
-        line.update({"workload": f"linear_gaussian_basin_{n}x{n}_fp64", "value": value, "steps": args.steps,
-                     "ms_per_step": ms / args.steps, "dtype": "f64",
-                     "config": {"workload": f"linear_gaussian_basin_{n}x{n}_fp64", "timesteps_per_step": inner,
-                                "dt": dt, "max_stage": True},
-                     "roofline": {"bound": "hbm", "kernel": "linear_step_kernel", "achieved": achieved,
-                                  "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-                                  "bytes_per_cell": 72,
-                                  "per_launch_ms": {k: (v[0] / v[1] if v[1] else 0.0) for k, v in tm.items()}}})
-        d.close()
-    elif args.workload == "batched":
-        # Spherical 3600x2400 (1 arcmin) FP32, B dipole initial conditions,
-        # Coriolis on, fixed CFL-0.7 step: one batched launch per step
-        # against the same instances stepped one domain at a time.
-        from ptha_b200.batch import Batch
-        from ptha_b200.sharding import gather_instance_series, instance_range
-        dist = None
-        if world > 1:
-            import datetime
-            import torch.distributed as dist
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-        nxg, nyg = (3600, 2400) if args.n == N else (args.n * 3 // 2, args.n)
-        B = args.batch
-        first_inst, count = instance_range(B, world, rank)
-        dl = 1.0 / 60.0 * (3600 / nxg)
-        gkw, U0 = workloads.spherical_patch(nx=nxg, ny=nyg, dlon=dl, ll=(140.0, -45.0), seed=3)
-        grid = Domain(**gkw, timestepping_method="linear", real_bytes=4, device=local)
-        grid.set_U(U0)
-        dt = grid.linear_timestep_max()
-        lon = gkw["lower_left"][0] + (np.arange(nxg) + 0.5) * dl
-        lat = gkw["lower_left"][1] + (np.arange(nyg) + 0.5) * dl
-        wet = U0[3] < 0
-        b = Batch(grid, count)
-        chunk = 8
-        first_eta = None
-        # instance q's initial condition depends on q only, not on the ranks
-        rng_seeds = np.random.default_rng(4).integers(0, 2 ** 31, size=B)
-        for q0 in range(0, count, chunk):
-            cnt = min(chunk, count - q0)
-            U3 = np.zeros((cnt, 3, nyg, nxg), np.float32)
-            for t in range(cnt):
-                eta = _dipoles(lon, lat, 1, seed=int(rng_seeds[first_inst + q0 + t]))[0]
-                U3[t, 0] = np.where(wet, eta, 0.0)
-                if first_eta is None:
-                    first_eta = U3[t, 0].copy()
-            b.set_U(U3, first=q0)
-            del U3
-        cfg, _ = b.tune()
-        stream = torch.cuda.ExternalStream(grid.stream(), device=f"cuda:{local}")
-        inner = args.inner if args.inner != INNER else 50
-        # 200 gauges at random wet cells (seed 5), sampled every step
-        gr = np.random.default_rng(5)
-        wj, wi = np.nonzero(wet)
-        pick = gr.choice(wj.size, size=200, replace=False)
-        gxy = np.stack([lon[wi[pick]], lat[wj[pick]]], axis=1)
-        b.gauges_setup(gxy, capacity=inner * (args.steps + 1))
-        b.evolve(inner, dt)
-        torch.cuda.synchronize()
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
-        ms_b = _event_ms(stream, lambda: [b.evolve(inner, dt) for _ in range(args.steps)])
-        if dist is not None:
-            t = torch.tensor([ms_b], dtype=torch.float64, device=f"cuda:{local}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms_b = float(t.item())
-        v_batched = nxg * nyg * B * inner * args.steps / (ms_b / 1e3)
-        series = gather_instance_series(b.gauges_read(), B, world, rank) if dist is not None else b.gauges_read()
-        if dist is not None and rank != 0:
-            b.close()
-            grid.close()
-            dist.barrier()
-            dist.destroy_process_group()
-            return
-        # Per-instance loop: each instance as its own domain step loop.
-        single = Domain(**gkw, timestepping_method="linear", real_bytes=4, device=local)
+    kw, U, gauges = workloads.linear_gaussian_basin(n=n)
+    d = Domain(**kw, device=local)
+    d.set_U(U)
+    del U
+    dt = d.linear_timestep_max()
+    stream = torch.cuda.ExternalStream(d.stream(), device=f"cuda:{local}")
+    for _ in range(warmup):
+        d.evolve_steps(inner, dt)
+    d.synchronize()
+    ms = _event_ms(stream, lambda: [d.evolve_steps(inner, dt) for _ in range(reps)])
+    value = n * n * inner * reps / (ms / 1e3)
+    d.timers_enable(True)
+    d.evolve_steps(50, dt)
+    tm = d.timers_read()
+    d.timers_enable(False)
+    t_ms, cnt = tm["leapfrog_step"]
+    achieved = n * n * 72.0 * cnt / (t_ms / 1e3) / 1e9
+    d.close()
+    return {"workload": f"linear_gaussian_basin_{n}x{n}_fp64", "value": value, "unit": UNIT,
+            "ms_per_timestep": ms / (reps * inner), "dt": dt,
+            "roofline": {"bound": "hbm", "kernel": "linear leapfrog step kernel", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                         "bytes_per_cell": 72,
+                         "per_launch_ms": {k: (v[0] / v[1] if v[1] else 0.0) for k, v in tm.items()}}}
+
+
+def form_linear_sweep(local):
+    return {f"n{n}": form_linear(local, n) for n in (4096, 8192)}
+
+
+def form_batched(local, B=256, nx=3600, ny=2400, inner=50, reps=2, world=1, rank=0, dist=None):
+    """Spherical 3600x2400 (1 arcmin) FP32, B dipole initial conditions,
+    Coriolis on, fixed CFL-0.7 step, 200 gauges: one batched launch per step
+    against one instance stepped as a plain domain (the per-instance loop)."""
+    import numpy as np
+    import torch
+    from ptha_b200 import Domain, workloads
+    from ptha_b200.batch import Batch
+    from ptha_b200.sharding import gather_instance_series, instance_range
+    peak, peak_kind = hbm_peak()
+    first_inst, count = instance_range(B, world, rank)
+    gkw, U0, lon, lat = workloads.batched_grid(nx, ny)
+    grid = Domain(**gkw, device=local)
+    grid.set_U(U0)
+    dt = grid.linear_timestep_max()
+    wet = U0[3] < 0
+    b = Batch(grid, count)
+    chunk = 8
+    first_eta = None
+    for q0 in range(0, count, chunk):
+        cnt = min(chunk, count - q0)
+        U3 = np.zeros((cnt, 3, ny, nx), np.float32)
+        for t in range(cnt):
+            U3[t, 0] = workloads.batched_instance_stage(lon, lat, wet, first_inst + q0 + t, B)
+            if first_eta is None:
+                first_eta = U3[t, 0].copy()
+        b.set_U(U3, first=q0)
+        del U3
+    cfg, _ = b.tune()
+    stream = torch.cuda.ExternalStream(grid.stream(), device=f"cuda:{local}")
+    b.gauges_setup(workloads.batched_gauges(lon, lat, wet), capacity=inner * (reps + 1))
+    b.evolve(inner, dt)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms_b = _event_ms(stream, lambda: [b.evolve(inner, dt) for _ in range(reps)])
+    if dist is not None:
+        t = torch.tensor([ms_b], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_b = float(t.item())
+    v_batched = nx * ny * B * inner * reps / (ms_b / 1e3)
+    series = gather_instance_series(b.gauges_read(), B, world, rank) if dist is not None else b.gauges_read()
+    b.close()
+    out = {"workload": f"batched_linear_spherical_{nx}x{ny}_B{B}_fp32", "value": v_batched, "unit": UNIT,
+           "ms_per_timestep": ms_b / (reps * inner), "batch": B, "dt": dt, "tile_config": cfg, "gauges": 200,
+           "gauge_series": list(series.shape)}
+    if rank == 0:
+        # The per-instance loop: one instance as its own domain step loop.
+        single = Domain(**gkw, device=local)
         U = U0.astype(np.float32).copy()
         U[0] = first_eta
         single.set_U(U)
         single.evolve_steps(inner, dt)
         single.synchronize()
         s_stream = torch.cuda.ExternalStream(single.stream(), device=f"cuda:{local}")
-        ms_s = _event_ms(s_stream, lambda: [single.evolve_steps(inner, dt) for _ in range(args.steps)])
-        v_loop = nxg * nyg * inner * args.steps / (ms_s / 1e3)
-        bytes_cell = 32.0 + 4.0 / B
-        line.update({"workload": f"batched_linear_spherical_{nxg}x{nyg}_B{B}_fp32", "value": v_batched,
-                     "steps": args.steps, "ms_per_step": ms_b / args.steps, "dtype": "f32", "n_gpus": world,
-                     "scaling": "strong",
-                     "config": {"workload": f"batched_linear_spherical_{nxg}x{nyg}_B{B}_fp32", "batch": B,
-                                "timesteps_per_step": inner, "dt": dt, "coriolis": True, "tile_config": cfg,
-                                "gauges": 200, "parallelism": f"instances sharded x{world}"},
-                     "gauge_series_gathered": list(series.shape),
-                     "per_instance_loop": {"value": v_loop, "ms_per_step_one_instance": ms_s / args.steps},
-                     "speedup_vs_loop": v_batched / v_loop,
-                     "roofline": {"bound": "hbm", "kernel": "linear_step_kernel (batched)",
-                                  "achieved": v_batched * bytes_cell / 1e9, "peak": peak, "unit": "GB/s",
-                                  "frac": v_batched * bytes_cell / 1e9 / peak, "peak_source": peak_kind,
-                                  "bytes_per_cell": bytes_cell}})
-        b.close()
+        ms_s = _event_ms(s_stream, lambda: [single.evolve_steps(inner, dt) for _ in range(reps)])
         single.close()
-        grid.close()
-        if dist is not None:
-            dist.barrier()
-            dist.destroy_process_group()
-    elif args.workload == "adjoint":
-        # Spherical 1200x800 (2 arcmin) FP64, 30 gauges, a hidden dipole's
-        # waveforms as the target, 2 h simulated, checkpoint every 50 steps.
-        nxg, nyg = (1200, 800) if args.n == N else (args.n * 3 // 2, args.n)
-        dl = 2.0 / 60.0 * (1200 / nxg)
-        gkw, U0 = workloads.spherical_patch(nx=nxg, ny=nyg, dlon=dl, ll=(150.0, -40.0), seed=6)
-        d = Domain(**gkw, timestepping_method="linear", device=local)
-        lon = gkw["lower_left"][0] + (np.arange(nxg) + 0.5) * dl
-        lat = gkw["lower_left"][1] + (np.arange(nyg) + 0.5) * dl
-        wet = U0[3] < 0
-        rng = np.random.default_rng(7)
-        wi = np.argwhere(wet)
-        pick = wi[rng.choice(len(wi), 30, replace=False)]
-        gauges = np.stack([lon[pick[:, 1]], lat[pick[:, 0]]], axis=1)
-        d.set_U(U0)
-        dt = d.linear_timestep_max()
-        nsteps = int(round(2 * 3600.0 / dt))
-        eta_t = _dipoles(lon, lat, 1, seed=8, band=((lon[0] + 5, lat[0] + 5), (lon[-1] - 5, lat[-1] - 5)))[0]
-        Ut = U0.copy()
-        Ut[0] = np.where(wet, eta_t, 0.0)
-        d.set_U(Ut)
-        d.gauges_setup(gauges, capacity=nsteps + 8)
-        stream = torch.cuda.ExternalStream(d.stream(), device=f"cuda:{local}")
-        d.evolve_steps(nsteps, dt)
-        target = d.gauges_read()[:nsteps, :, 0].copy()
-        Ui = U0.copy()
-        Ui[0] = 0.0
-        times_f, times_a = [], []
-        for _ in range(max(1, args.steps)):
-            d.set_U(Ui)
-            d.gauges_reset()
-            d.time = 0.0
-            d.synchronize()
-            times_f.append(_event_ms(stream, lambda: d.evolve_steps(nsteps, dt)))
-            d.set_U(Ui)
-            d.time = 0.0
-            d.synchronize()
-            res = {}
-
-            def grad_call():
-                res["lg"] = d.misfit_gradient(nsteps, dt, target, checkpoint_every=50)
-            # Device time on the domain's stream, including the gradient's
-            # copy back to the host (the forward solve above has no copy).
-            times_a.append(_event_ms(stream, grad_call))
-            loss, grad = res["lg"]
-        f_ms, a_ms = min(times_f), min(times_a)
-        line.update({"workload": f"adjoint_linear_spherical_{nxg}x{nyg}_fp64", "value": nxg * nyg * nsteps /
-                     (a_ms / 1e3), "steps": args.steps, "ms_per_step": a_ms, "dtype": "f64",
-                     "config": {"workload": f"adjoint_linear_spherical_{nxg}x{nyg}_fp64", "nsteps": nsteps,
-                                "dt": dt, "gauges": 30, "checkpoint_every": 50},
-                     "forward_ms": f_ms, "gradient_ms": a_ms, "gradient_over_forward": a_ms / f_ms,
-                     "loss": loss, "grad_norm": float(np.linalg.norm(grad[0]))})
-        d.close()
-    elif args.workload == "multidomain":
-        line.update(_run_multidomain(args, local, peak, peak_kind))
-    print(json.dumps(line), flush=True)
+        v_loop = nx * ny * inner * reps / (ms_s / 1e3)
+        bytes_cell = 32.0 + 4.0 / B
+        out.update({"per_instance_loop": {"value": v_loop, "ms_per_timestep": ms_s / (reps * inner)},
+                    "speedup_vs_loop": v_batched / v_loop,
+                    "roofline": {"bound": "hbm", "kernel": "batched linear leapfrog step kernel",
+                                 "achieved": v_batched * bytes_cell / 1e9, "peak": peak, "unit": "GB/s",
+                                 "frac": v_batched * bytes_cell / 1e9 / peak, "peak_source": peak_kind,
+                                 "bytes_per_cell": bytes_cell,
+                                 "loop_frac": v_loop * 36.0 / 1e9 / peak}})
+    grid.close()
+    return out
 
 
-def _coast_elevation(lon, lat, coasts):
-    """Deep ocean (-4000 m) shoaling over a 60 km shelf slope to -50 m, then a
-    1/40 coastal ramp to +10 m, for each straight coastline (lon0, lat0,
-    bearing of the seaward normal, (lon_min, lon_max, lat_min, lat_max) of
-    the region it shapes)."""
-    import numpy as np
-    km = 111.19
-    elv = np.full(np.broadcast(lon, lat).shape, -4000.0)
-    for (x0, y0, ang, box) in coasts:
-        inside = (lon >= box[0]) & (lon <= box[1]) & (lat >= box[2]) & (lat <= box[3])
-        # seaward distance (km) from the coastline
-        d = ((lon - x0) * np.cos(np.deg2rad(y0)) * np.cos(ang) + (lat - y0) * np.sin(ang)) * km
-        ramp = np.clip(-50.0 - (d * 1000.0) / 40.0, -50.0, 10.0)           # within ~2.4 km of the coast
-        shelf = np.clip(-50.0 - (d - 0.0) * (3950.0 / 60.0), -4000.0, -50.0)  # 60 km shelf slope
-        e = np.where(d <= 0.0, ramp, shelf)
-        elv = np.where(inside, np.maximum(elv, e), elv)
-    return elv
-
-
-def _run_multidomain(args, local, peak, peak_kind):
-    """Nested multidomain in the shape of the 5-domain configuration: a
-    coarse 'linear' FP32 band (4 arcmin, 5400x1800, 60S-60N, periodic in
-    longitude over 0-360 through periodic self-exchanges), one ratio-3
-    'rk2' FP64 domain (900x900) and two ratio-9 'rk2' FP64 wet/dry domains
-    (1197x801 and 702x1098, the nearest sizes that are whole parent cells)
-    on synthetic coastal ramps; one dipole source; fixed md step from the
-    coarse domain's CFL, refinement factors from each domain's stationary
-    CFL; graph-captured md steps."""
-    import math
+def form_adjoint(local, nx=1200, ny=800, reps=2):
+    """Spherical 1200x800 (2 arcmin) FP64, 30 gauges, a hidden dipole's
+    waveforms as the target, 2 h simulated, checkpoint every 50 steps: the
+    misfit gradient's device time against one forward solve."""
     import numpy as np
     import torch
-    from ptha_b200 import Multidomain, NestDomain
-    c = 1.0 / 15.0                     # coarse cell (degrees)
-    f3, f9 = c / 3.0, c / 9.0
-    specs = [
-        NestDomain((0.0, -60.0), (5400 * c, 1800 * c), (5400, 1800), "linear", 1),
-        NestDomain((140.0, -40.0), (900 * f3, 900 * f3), (900, 900), "rk2", 1),
-        NestDomain((141.0 + 2 * c, -39.0), (1197 * f9, 801 * f9), (1197, 801), "rk2", 1),
-        NestDomain((152.0, -35.0), (702 * f9, 1098 * f9), (702, 1098), "rk2", 1),
-    ]
-    coasts = [(141.0 + 2 * c + 1197 * f9 * 0.75, -39.0 + 801 * f9 * 0.5, 0.0,
-               (140.5, 151.0, -39.5, -32.5)),
-              (152.0 + 702 * f9 * 0.5, -35.0 + 1098 * f9 * 0.8, math.pi / 2,
-               (151.5, 157.7, -35.5, -26.3))]
-    # Refinement factors from the stationary CFL limits need the domains;
-    # set them up once with nt = 1, read the limits, then build the real nest.
+    from ptha_b200 import Domain, workloads
+    gkw, U0, gauges, eta_t, _ = workloads.adjoint_case(nx, ny)
+    d = Domain(**gkw, device=local)
+    d.set_U(U0)
+    dt = d.linear_timestep_max()
+    nsteps = int(round(2 * 3600.0 / dt))
+    Ut = U0.copy()
+    Ut[0] = eta_t
+    d.set_U(Ut)
+    d.gauges_setup(gauges, capacity=nsteps + 8)
+    stream = torch.cuda.ExternalStream(d.stream(), device=f"cuda:{local}")
+    d.evolve_steps(nsteps, dt)
+    target = d.gauges_read()[:nsteps, :, 0].copy()
+    Ui = U0.copy()
+    Ui[0] = 0.0
+    times_f, times_a = [], []
+    res = {}
+    for _ in range(reps):
+        d.set_U(Ui)
+        d.gauges_reset()
+        d.time = 0.0
+        d.synchronize()
+        times_f.append(_event_ms(stream, lambda: d.evolve_steps(nsteps, dt)))
+        d.set_U(Ui)
+        d.time = 0.0
+        d.synchronize()
+
+        def grad_call():
+            res["lg"] = d.misfit_gradient(nsteps, dt, target, checkpoint_every=50)
+        # Device time on the domain's stream, including the gradient's copy
+        # back to the host (the forward solve has no copy).
+        times_a.append(_event_ms(stream, grad_call))
+    loss, grad = res["lg"]
+    d.close()
+    f_ms, a_ms = min(times_f), min(times_a)
+    return {"workload": f"adjoint_linear_spherical_{nx}x{ny}_fp64", "value": nx * ny * nsteps / (a_ms / 1e3),
+            "unit": UNIT, "nsteps": nsteps, "dt": dt, "gauges": 30, "checkpoint_every": 50,
+            "forward_ms": f_ms, "gradient_ms": a_ms, "gradient_over_forward": a_ms / f_ms,
+            "loss": loss, "grad_norm": float(np.linalg.norm(grad[0]))}
+
+
+def _nested(local, nts, sources=1):
+    from ptha_b200 import Multidomain, workloads
+    specs, coasts = workloads.nested_specs(nts)
     kw = [dict(real_bytes=4, spherical=True), dict(spherical=True), dict(spherical=True), dict(spherical=True)]
+    md = Multidomain(specs, domain_kwargs=kw, use_wetdry_limiting=True, flux_correction=True, device=local,
+                     periodic_xs=(0.0, 360.0))
+    for k, (s_, d) in enumerate(zip(specs, md.domains)):
+        d.set_U(workloads.nested_initial_state(s_, k, coasts))
+        if d.timestepping_method == "rk2":
+            d.set_manning_squared(0.025 ** 2)
+    return specs, md
 
-    def build(nts):
-        sp = [NestDomain(s.lower_left, s.lw, s.nx, s.timestepping_method, nt) for s, nt in zip(specs, nts)]
-        md = Multidomain(sp, domain_kwargs=kw, use_wetdry_limiting=True, flux_correction=True, device=local,
-                         periodic_xs=(0.0, 360.0))
-        for k, (s, d) in enumerate(zip(sp, md.domains)):
-            lon, lat = s.x(), s.y()
-            LON, LAT = np.meshgrid(lon, lat)
-            elv = _coast_elevation(LON, LAT, coasts)
-            if k == 0:   # walls north and south; periodic east-west
-                elv[:2, :] = 100.0
-                elv[-2:, :] = 100.0
-            eta = _dipoles(lon, lat, 1, seed=11, band=((144.0, -37.0), (150.0, -30.0)))[0]
-            U = np.zeros((4, s.nx[1], s.nx[0]))
-            U[3] = elv
-            U[0] = np.where(elv < 0, eta, elv)
-            d.set_U(U)
-            if d.timestepping_method == "rk2":
-                d.set_manning_squared(0.025 ** 2)
-        return sp, md
 
-    sp, md = build([1, 1, 1, 1])
+def _nested_refinement(local):
+    import math
+    specs, md = _nested(local, (1, 1, 1, 1))
     dt = md.domains[0].linear_timestep_max()
     lims = [d.stationary_timestep_max() if d.timestepping_method == "rk2" else dt for d in md.domains]
-    nts = [max(1, int(math.ceil(dt / l))) for l in lims]
     md.close()
-    sp, md = build(nts)
-    cells = sum(s.nx[0] * s.nx[1] * nt for s, nt in zip(sp, nts))
+    return dt, [max(1, int(math.ceil(dt / lim))) for lim in lims]
+
+
+def form_multidomain(local, reps=20, K=3):
+    """The nested configuration with one source: a coarse 'linear' FP32 band
+    (4 arcmin, 5400x1800, 60S-60N, periodic over 0-360), one ratio-3 'rk2'
+    FP64 domain (900x900) and two ratio-9 'rk2' FP64 wet/dry domains
+    (1197x801, 702x1098) on coastal ramps; fixed md step from the coarse
+    CFL, refinement factors from each domain's stationary CFL; graph-captured
+    md steps."""
+    import numpy as np
+    import torch
+    dt, nts = _nested_refinement(local)
+    specs, md = _nested(local, nts)
+    cells = sum(s_.nx[0] * s_.nx[1] * nt for s_, nt in zip(specs, nts))
     stream = torch.cuda.ExternalStream(md.domains[0].stream(), device=f"cuda:{local}")
-    K = 3
-    for _ in range(args.warmup):
-        md.evolve_one_step(dt)
+    md.evolve_one_step(dt)
     md.synchronize()
-    ms_plain = _event_ms(stream, lambda: [md.evolve_one_step(dt) for _ in range(K * 4)]) / (K * 4)
+    ms_plain = _event_ms(stream, lambda: [md.evolve_one_step(dt) for _ in range(K * 2)]) / (K * 2)
     md.capture_graph(K, dt)
     md.replay(1)
     md.synchronize()
-    reps = max(1, args.inner if args.inner != INNER else 100)
-    l0 = md.launch_count()
     ms = _event_ms(stream, lambda: md.replay(reps))
     ms_step = ms / (reps * K)
-    value = cells / (ms_step / 1e3)
     vols = [d.volume_interior() for d in md.domains]
-    out = {"workload": "nested_multidomain_4dom", "value": value, "steps": reps * K, "ms_per_step": ms_step,
-           "dtype": "f32 coarse / f64 fine",
-           "config": {"workload": "nested_multidomain_4dom",
-                      "domains": [{"nx": list(s.nx), "method": s.timestepping_method, "nt": nt,
-                                   "nest_layer_width": s.nest_layer_width} for s, nt in zip(sp, nts)],
-                      "md_dt": dt, "exchanges": len(md.exchanges), "flux_correction": True,
-                      "graph_steps": K, "sources": 1, "periodic_xs": [0.0, 360.0]},
-           "cell_updates_per_md_step": cells,
-           "ms_per_md_step_without_graph": ms_plain,
-           "graph_replay_speedup": ms_plain / ms_step,
-           "gpu_launches_per_md_step_graph": 1.0 / K,
+    out = {"workload": "nested_multidomain_4dom", "value": cells / (ms_step / 1e3), "unit": UNIT,
+           "ms_per_md_step": ms_step, "dtype": "f32 coarse / f64 fine",
+           "domains": [{"nx": list(s_.nx), "method": s_.timestepping_method, "nt": nt,
+                        "nest_layer_width": s_.nest_layer_width} for s_, nt in zip(specs, nts)],
+           "md_dt": dt, "exchanges": len(md.exchanges), "flux_correction": True, "graph_steps": K, "sources": 1,
+           "cell_updates_per_md_step": cells, "ms_per_md_step_without_graph": ms_plain,
            "finite": bool(all(np.isfinite(v) for v in vols))}
     md.close()
     return out
+
+
+def form_nested16(local):
+    """Placeholder until the batch-of-nests form exists."""
+    return {"skipped": "not built"}
+
+
+def run_form(args, local, world=1, rank=0):
+    import torch
+    torch.cuda.set_device(local)
+    torch.zeros(1, device=f"cuda:{local}")
+    line = {"metric": METRIC, "unit": UNIT, "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
+            "vs_baseline": None}
+    if args.workload == "linear":
+        r = form_linear(local, args.n if args.n != N else 8192,
+                        inner=args.inner if args.inner != INNER else 200, reps=args.steps, warmup=args.warmup)
+        line.update(r, dtype="f64", steps=args.steps, config={"workload": r["workload"], "max_stage": True})
+    elif args.workload == "batched":
+        dist = None
+        if world > 1:
+            import datetime
+            import torch.distributed as dist
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        nx, ny = (3600, 2400) if args.n == N else (args.n * 3 // 2, args.n)
+        r = form_batched(local, B=args.batch, nx=nx, ny=ny, inner=args.inner if args.inner != INNER else 50,
+                         reps=args.steps, world=world, rank=rank, dist=dist)
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        if rank != 0:
+            return
+        line.update(r, dtype="f32", steps=args.steps, n_gpus=world, scaling="strong",
+                    config={"workload": r["workload"], "batch": args.batch,
+                            "parallelism": f"instances sharded x{world}"})
+    elif args.workload == "adjoint":
+        nx, ny = (1200, 800) if args.n == N else (args.n * 3 // 2, args.n)
+        r = form_adjoint(local, nx, ny, reps=max(1, args.steps))
+        line.update(r, dtype="f64", steps=args.steps, config={"workload": r["workload"]})
+    elif args.workload == "multidomain":
+        r = form_multidomain(local)
+        line.update(r, steps=r["graph_steps"], config={"workload": r["workload"]})
+    elif args.workload == "nested16":
+        r = form_nested16(local)
+        line.update(r, config={"workload": "nested_multidomain_4dom_x16_sources"})
+    print(json.dumps(line), flush=True)
 
 
 def main():
@@ -677,11 +676,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="headline only (no secondary forms)")
     ap.add_argument("--n", type=int, default=N, help="grid cells per side (default 2048)")
     ap.add_argument("--inner", type=int, default=INNER, help="timesteps per bench step (default 2000)")
     ap.add_argument("--real32", action="store_true", help="FP32 state (-DREALFLOAT analogue)")
     ap.add_argument("--profile", action="store_true", help="short untimed run for ncu")
-    ap.add_argument("--workload", default="rk2", choices=["rk2", "linear", "batched", "adjoint", "multidomain"],
+    ap.add_argument("--workload", default="rk2",
+                    choices=["rk2", "linear", "batched", "adjoint", "multidomain", "nested16"],
                     help="rk2 (default, the headline) or a secondary form")
     ap.add_argument("--batch", type=int, default=256, help="instances for --workload batched")
     args = ap.parse_args()

@@ -237,6 +237,9 @@ int swals_gpu_batch_time(swals_batch *b, double *time, int64_t *nsteps);
  * dt = 0 steps and keeps the fastest. */
 int swals_gpu_batch_tune(swals_batch *b, int32_t *cfg_out, double *ms_per_step_out);
 int swals_gpu_batch_set_tile_config(swals_batch *b, int32_t cfg);
+/* Number of kernel configurations the autotuner chooses from (valid cfg
+ * values of swals_gpu_batch_set_tile_config are 0 .. n-1). */
+int swals_gpu_batch_tile_config_count(int32_t *n);
 
 /* ---- discrete adjoint of the truly linear leapfrog -------------------------
  * The reference has no adjoint.  For a 'linear' domain with

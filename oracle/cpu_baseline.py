@@ -28,18 +28,30 @@ def main():
     ap.add_argument("--min-seconds", type=float, default=10.0)
     ap.add_argument("--max-steps", type=int, default=1000)
     ap.add_argument("--exact-steps", type=int, default=0)
+    ap.add_argument("--variant", default="fast", choices=["fast", "native", "strict"],
+                    help="oracle build: fast = -O3 -ffast-math with libm pow (the reference's -Ofast), "
+                         "native = the same with -march=native (built here on first use), strict = the "
+                         "IEEE-strict parity checker")
     args = ap.parse_args()
     from ptha_b200 import workloads
     from tests.pairs import oracle_from_kw
+    variant = args.variant
+    if variant == "native" and not os.path.exists(os.path.join(HERE, "liboracle64_native.so")):
+        import subprocess
+        r = subprocess.run(["make", "-s", "-C", HERE, "native"], capture_output=True, text=True)
+        if r.returncode != 0:
+            variant = "fast"
+    flags = {"fast": "-O3 -ffast-math, libm pow", "native": "-O3 -ffast-math -march=native, libm pow",
+             "strict": "-O2 IEEE-strict, no FMA contraction"}[variant]
     if args.workload == "rk2_beach":
         kw, U, gauges, nsq = workloads.rk2_beach()
-        o = oracle_from_kw(kw)
+        o = oracle_from_kw(kw, variant=variant)
         o.U[:] = U
         o.manning_squared[:] = nsq
         dt = None
     elif args.workload == "linear_gaussian_basin":
         kw, U, gauges = workloads.linear_gaussian_basin()
-        o = oracle_from_kw(kw)
+        o = oracle_from_kw(kw, variant=variant)
         o.U[:] = U
         dt = o.linear_timestep_max()
     else:
@@ -60,8 +72,8 @@ def main():
     el = time.perf_counter() - t0
     threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
     print(json.dumps({"value": nx * ny * steps / el, "unit": "cell-updates/s", "cores": threads,
-                      "steps": steps, "seconds": el, "cells": nx * ny,
-                      "sample": f"{args.workload} {nx}x{ny}: {steps} timesteps after 1 untimed"}))
+                      "steps": steps, "seconds": el, "cells": nx * ny, "variant": variant, "flags": flags,
+                      "sample": f"{args.workload} {nx}x{ny}: {steps} timesteps after 1 untimed ({flags})"}))
 
 
 if __name__ == "__main__":

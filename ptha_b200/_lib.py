@@ -37,7 +37,7 @@ EXPORTED = [
     "swals_gpu_batch_create", "swals_gpu_batch_destroy", "swals_gpu_batch_upload_U", "swals_gpu_batch_download_U",
     "swals_gpu_batch_download_max_stage", "swals_gpu_batch_device_state", "swals_gpu_batch_gauges_setup",
     "swals_gpu_batch_gauges_read", "swals_gpu_batch_evolve", "swals_gpu_batch_time", "swals_gpu_batch_tune",
-    "swals_gpu_batch_set_tile_config", "swals_gpu_adjoint_linear", "swals_gpu_misfit_gradient_linear",
+    "swals_gpu_batch_set_tile_config", "swals_gpu_batch_tile_config_count", "swals_gpu_adjoint_linear", "swals_gpu_misfit_gradient_linear",
     "swals_gpu_volume_interior_noalloc",
     "swals_gpu_md_create", "swals_gpu_md_destroy", "swals_gpu_md_evolve_one_step", "swals_gpu_md_send_halos",
     "swals_gpu_md_recv_halos", "swals_gpu_md_flux_correction", "swals_gpu_md_buffer_size",
@@ -147,6 +147,7 @@ def lib():
         "swals_gpu_batch_time": [vp, ctypes.POINTER(dbl), ctypes.POINTER(i64)],
         "swals_gpu_batch_tune": [vp, ctypes.POINTER(i32), ctypes.POINTER(dbl)],
         "swals_gpu_batch_set_tile_config": [vp, i32],
+        "swals_gpu_batch_tile_config_count": [ctypes.POINTER(i32)],
         "swals_gpu_adjoint_linear": [vp, i32, dbl, vp, vp, vp],
         "swals_gpu_misfit_gradient_linear": [vp, i32, dbl, vp, i32, ctypes.POINTER(dbl), vp],
         "swals_gpu_volume_interior_noalloc": [vp, vp, vp, i32, i32, i64, i32, i32, vp, vp],

@@ -93,5 +93,11 @@ class Batch:
         check(self._L.swals_gpu_batch_tune(self._h, ctypes.byref(cfg), ctypes.byref(ms)))
         return cfg.value, ms.value
 
+    @staticmethod
+    def tile_config_count():
+        n = ctypes.c_int32()
+        check(_lib.lib().swals_gpu_batch_tile_config_count(ctypes.byref(n)))
+        return n.value
+
     def set_tile_config(self, cfg):
         check(self._L.swals_gpu_batch_set_tile_config(self._h, int(cfg)))

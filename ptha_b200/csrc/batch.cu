@@ -407,6 +407,13 @@ int swals_gpu_batch_tune(swals_batch *b, int32_t *cfg_out, double *ms_per_step_o
     return SWALS_OK;
 }
 
+int swals_gpu_batch_tile_config_count(int32_t *n)
+{
+    if (!n) return api_fail(SWALS_ERR_INVALID_ARGUMENT, "NULL argument");
+    *n = swals::linear_tile_config_count();
+    return SWALS_OK;
+}
+
 int swals_gpu_batch_set_tile_config(swals_batch *b, int32_t cfg)
 {
     if (!b || cfg < 0 || cfg >= swals::linear_tile_config_count())

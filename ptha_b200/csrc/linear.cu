@@ -605,6 +605,348 @@ __global__ void __launch_bounds__(128, LIN_MINB) linear_async_kernel(const LinAr
     }
 }
 
+// The streaming step with aligned, wide row segments: a warp owns W = 32 CPL
+// columns (lane L holds columns base + L CPL .. + CPL - 1, one 4/8/16-byte
+// cp.async per plane and row), so every strip starts on a 128- or 256-byte
+// boundary and each row of each plane is read and written as whole sectors
+// (the 30-column strips of linear_async_kernel start mid-sector, and two
+// warps write the sector their strips share).  The two neighbour columns
+// the stencil needs outside the strip are single-element copies into a
+// per-warp halo ring: UH of column base - 1 (clamped at the west edge, like
+// the reference's UH(max(xL-1, 1))) and STG, UH, VH, ELV of column base + W,
+// whose new stage every lane evaluates (the same expression).  Lanes read
+// only their own ring entries; lanes 0 and 31 hand the halo values on by
+// shuffle.  The arithmetic is linear_stream_kernel's, column by column.
+#ifndef LIN_WIDE_MINB
+#define LIN_WIDE_MINB 4
+#endif
+
+__device__ __forceinline__ void cp_async_vec(void *smem, const void *gmem, int bytes, int src_bytes)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    if (bytes == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(src_bytes));
+    else if (bytes == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(src_bytes));
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(sa), "l"(gmem), "r"(src_bytes));
+}
+
+template <typename R, int CPL> struct VecOf { typedef R T; };
+template <> struct VecOf<double, 2> { typedef double2 T; };
+template <> struct VecOf<float, 2> { typedef float2 T; };
+template <> struct VecOf<float, 4> { typedef float4 T; };
+template <typename R, int CPL>
+__device__ __forceinline__ void store_vec(R *p, const R (&v)[CPL])
+{
+    typename VecOf<R, CPL>::T x;
+    R *xs = reinterpret_cast<R *>(&x);
+#pragma unroll
+    for (int c = 0; c < CPL; c++) xs[c] = v[c];
+    *reinterpret_cast<typename VecOf<R, CPL>::T *>(p) = x;
+}
+
+template <typename R, int CPL> struct WideRing {
+    R v[AD][5][32 * CPL];   // [slot][UH, VH, STG, ELV, max_stage][column]
+    R h[AD][2][4];          // [slot][lane 0: UH west | lane 31: STG, UH, VH, ELV east][]
+};
+
+template <typename R, bool CORIOLIS, bool TRUELY_LINEAR, bool GAUGES, int CPL>
+__global__ void __launch_bounds__(128, LIN_WIDE_MINB) linear_wide_kernel(const LinArgs<R> a, int SH, int nstrips,
+                                                                         int total)
+{
+    constexpr int W = 32 * CPL;
+    constexpr int VB = CPL * (int)sizeof(R);
+    __shared__ __align__(16) WideRing<R, CPL> rings[4];
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int b = blockIdx.x;
+    if (b >= a.nbatch) return;
+    const int nx = a.p.nx, ny = a.p.ny;
+    const int64_t P = a.p.pitch;
+    const int64_t io = (int64_t)b * a.inst_stride;
+    const R *stg = a.p.stg + io, *uhp = a.p.uh + io, *vhp = a.p.vh + io;
+    R *stg_o = a.p.stg_o + io, *uh_o = a.p.uh_o + io, *vh_o = a.p.vh_o + io;
+    R *max_stage = a.p.max_stage ? a.p.max_stage + (int64_t)b * a.max_stride : nullptr;
+    const R *elv = a.p.elv;
+    const R g = K<R>::gravity();
+    const R half = K<R>::half();
+    const R one = K<R>::one();
+    const R zero = K<R>::zero();
+    const R mad = K<R>::min_depth();
+    WideRing<R, CPL> &rg = rings[wib];
+
+    for (int w = blockIdx.y * 4 + wib; w < total; w += gridDim.y * 4) {
+        const int sx = w % nstrips, sy = w / nstrips;
+        const int ra = sy * SH;
+        const int rb = min(ra + SH, ny);
+        const int base = sx * W;
+        const int c0 = base + lane * CPL;                 // this lane's first column
+        const int iw = max(base - 1, 0);                  // west neighbour column (clamped)
+        const int ie = base + W;                          // east neighbour column
+        const int iec = min(ie, nx - 1);
+        const bool e_in = ie < nx;
+        const int src_bytes = clampi(nx - c0, 0, CPL) * (int)sizeof(R);
+        R dyl_i[CPL], dyl_ip1[CPL];
+#pragma unroll
+        for (int c = 0; c < CPL; c++) {
+            const int ic = min(c0 + c, nx - 1);
+            dyl_i[c] = a.m.dyl[ic];
+            dyl_ip1[c] = a.m.dyl[min(ic + 1, nx)];
+        }
+        const R dyl_e = a.m.dyl[iec];
+        const unsigned long long gmask =
+            GAUGES ? gauges_in(a.sites, a.n_sites, base, base + W - 1, ra, rb - 1) : 0ull;
+        const int nrow = rb - ra + 2;   // rows ra-1 .. rb
+        auto issue = [&](int k) {
+            if (k < nrow) {
+                const int q = ra - 1 + k;
+                const int qc = clampi(q, 0, ny - 1);
+                const int slot = k % AD;
+                const int64_t orow = (int64_t)qc * P;
+                const bool qv = (q >= 0 && q < ny);
+                cp_async_vec(&rg.v[slot][0][lane * CPL], uhp + orow + (src_bytes ? c0 : 0), VB, src_bytes);
+                cp_async_vec(&rg.v[slot][1][lane * CPL], vhp + orow + (src_bytes ? c0 : 0), VB, src_bytes);
+                cp_async_vec(&rg.v[slot][2][lane * CPL], stg + orow + (src_bytes ? c0 : 0), VB,
+                             qv ? src_bytes : 0);
+                cp_async_vec(&rg.v[slot][3][lane * CPL], elv + orow + (src_bytes ? c0 : 0), VB, src_bytes);
+                const bool mv = max_stage && q >= ra && q < rb;
+                cp_async_vec(&rg.v[slot][4][lane * CPL], (max_stage ? max_stage : stg) + orow + (src_bytes ? c0 : 0),
+                             VB, mv ? src_bytes : 0);
+                if (lane == 0) {
+                    cp_async_vec(&rg.h[slot][0][0], uhp + orow + iw, (int)sizeof(R), (int)sizeof(R));
+                } else if (lane == 31) {
+                    cp_async_vec(&rg.h[slot][1][0], stg + orow + iec, (int)sizeof(R), (qv && e_in) ? (int)sizeof(R) : 0);
+                    cp_async_vec(&rg.h[slot][1][1], uhp + orow + iec, (int)sizeof(R), (int)sizeof(R));
+                    cp_async_vec(&rg.h[slot][1][2], vhp + orow + iec, (int)sizeof(R), (int)sizeof(R));
+                    cp_async_vec(&rg.h[slot][1][3], elv + orow + iec, (int)sizeof(R), (int)sizeof(R));
+                }
+            }
+            cp_async_commit();
+        };
+        // New stage of cell (col, r) (domain_mod_linear_solver_include.f90:92-115).
+        auto stage_new = [&](int col, bool in_x, R dyl, int r, R s_old, R uh_r, R uh_w, R vh_r, R vh_s,
+                             R inv_cell_area_dt) -> R {
+            R sn = R(0);
+            if (r < ny && in_x) {
+                const bool interior = (col >= a.xl + 1) && (col <= a.xu - 1) && (r >= a.yl + 1) && (r <= a.yu - 1);
+                if (interior) {
+                    const R t1 = (uh_r - uh_w) * dyl;
+                    const R t2 = vh_r * a.m.dxb[r + 1] - vh_s * a.m.dxb[r];
+                    sn = s_old - inv_cell_area_dt * (t1 + t2);
+                } else if (a.bc_stage && on_bc_ring(col, r, nx, ny, a.bext)) {
+                    sn = stg_o[(int64_t)r * P + col];
+                } else {
+                    sn = s_old;
+                }
+            }
+            return sn;
+        };
+        // Neighbour values across lanes: west (the previous column) and east.
+        auto west = [&](const R (&v)[CPL], R halo_w, int c) -> R {
+            const R up = __shfl_up_sync(FULL, v[CPL - 1], 1);
+            return c > 0 ? v[c > 0 ? c - 1 : 0] : (lane > 0 ? up : halo_w);
+        };
+
+        __syncwarp();  // the previous segment's reads of the ring are done
+        for (int k = 0; k < AD - 1; k++) issue(k);
+        // k = 0: row ra-1 (VH only)
+        cp_async_wait<AD - 2>();
+        R vh_jm1[CPL];
+#pragma unroll
+        for (int c = 0; c < CPL; c++) vh_jm1[c] = rg.v[0][1][lane * CPL + c];
+        R vhE_jm1 = __shfl_sync(FULL, lane == 31 ? rg.h[0][1][2] : R(0), 31);
+        issue(AD - 1);
+        // k = 1: row ra
+        cp_async_wait<AD - 2>();
+        R uh_j[CPL], vh_j[CPL], e_j[CPL], sn_j[CPL], mx[CPL];
+        R st_j[CPL];
+#pragma unroll
+        for (int c = 0; c < CPL; c++) {
+            uh_j[c] = rg.v[1][0][lane * CPL + c];
+            vh_j[c] = rg.v[1][1][lane * CPL + c];
+            st_j[c] = rg.v[1][2][lane * CPL + c];
+            e_j[c] = rg.v[1][3][lane * CPL + c];
+            mx[c] = rg.v[1][4][lane * CPL + c];
+        }
+        R uhW_j = __shfl_sync(FULL, lane == 0 ? rg.h[1][0][0] : R(0), 0);
+        const R stE_j = __shfl_sync(FULL, lane == 31 ? rg.h[1][1][0] : R(0), 31);
+        const R uhE_j0 = __shfl_sync(FULL, lane == 31 ? rg.h[1][1][1] : R(0), 31);
+        R vhE_j = __shfl_sync(FULL, lane == 31 ? rg.h[1][1][2] : R(0), 31);
+        R eE_j = __shfl_sync(FULL, lane == 31 ? rg.h[1][1][3] : R(0), 31);
+        issue(AD);
+        R snE_j;
+        {
+            const R dta = a.dt / a.m.area[ra];
+            R uw[CPL];
+#pragma unroll
+            for (int c = 0; c < CPL; c++) uw[c] = west(uh_j, uhW_j, c);
+#pragma unroll
+            for (int c = 0; c < CPL; c++)
+                sn_j[c] = stage_new(c0 + c, c0 + c < nx, dyl_i[c], ra, st_j[c], uh_j[c], uw[c], vh_j[c], vh_jm1[c], dta);
+            const R uh_last = __shfl_sync(FULL, uh_j[CPL - 1], 31);
+            snE_j = stage_new(ie, e_in, dyl_e, ra, stE_j, uhE_j0, uh_last, vhE_j, vhE_jm1, dta);
+        }
+        // Row factors dt/area (the new stage, row j+1) and g dt/area,
+        // g dt/mean area (the momenta, row j): lane L evaluates them for row
+        // jb + L of each 32-row chunk and the rows take them by shuffle.
+        R rc_s = R(0), rc_u = R(0), rc_v = R(0);
+        for (int j = ra; j < rb; j++) {
+            const int k = j - ra + 2;  // row j+1
+            if (((j - ra) & 31) == 0) {
+                const int rr = min(j + lane, ny - 1);
+                const int rs = min(j + 1 + lane, ny - 1);
+                rc_s = a.dt / a.m.area[rs];
+                rc_u = g * a.dt / a.m.area[rr];
+                rc_v = g * a.dt / (half * (a.m.area[rr] + a.m.area[min(rr + 1, ny - 1)]));
+            }
+            const int rl = (j - ra) & 31;
+            const R inv_cell_area_dt_n = __shfl_sync(FULL, rc_s, rl);
+            const R inv_cell_area_dt_g = __shfl_sync(FULL, rc_u, rl);
+            const R inv_cell_area_dt_vh_g = __shfl_sync(FULL, rc_v, rl);
+            cp_async_wait<AD - 2>();
+            const int slot = k % AD;
+            R uh_n[CPL], vh_n[CPL], st_n[CPL], e_n[CPL], mx_n[CPL];
+#pragma unroll
+            for (int c = 0; c < CPL; c++) {
+                uh_n[c] = rg.v[slot][0][lane * CPL + c];
+                vh_n[c] = rg.v[slot][1][lane * CPL + c];
+                st_n[c] = rg.v[slot][2][lane * CPL + c];
+                e_n[c] = rg.v[slot][3][lane * CPL + c];
+                mx_n[c] = rg.v[slot][4][lane * CPL + c];
+            }
+            const R uhW_n = __shfl_sync(FULL, lane == 0 ? rg.h[slot][0][0] : R(0), 0);
+            const R stE_n = __shfl_sync(FULL, lane == 31 ? rg.h[slot][1][0] : R(0), 31);
+            const R uhE_n = __shfl_sync(FULL, lane == 31 ? rg.h[slot][1][1] : R(0), 31);
+            const R vhE_n = __shfl_sync(FULL, lane == 31 ? rg.h[slot][1][2] : R(0), 31);
+            const R eE_n = __shfl_sync(FULL, lane == 31 ? rg.h[slot][1][3] : R(0), 31);
+            issue(k + AD - 1);
+
+            // New stage of row j+1: own columns and the east neighbour column.
+            R uh_nw[CPL], sn_n[CPL];
+#pragma unroll
+            for (int c = 0; c < CPL; c++) uh_nw[c] = west(uh_n, uhW_n, c);
+#pragma unroll
+            for (int c = 0; c < CPL; c++)
+                sn_n[c] = stage_new(c0 + c, c0 + c < nx, dyl_i[c], j + 1, st_n[c], uh_n[c], uh_nw[c], vh_n[c], vh_j[c],
+                                    inv_cell_area_dt_n);
+            const R uh_n_last = __shfl_sync(FULL, uh_n[CPL - 1], 31);
+            const R snE_n = stage_new(ie, e_in, dyl_e, j + 1, stE_n, uhE_n, uh_n_last, vhE_n, vhE_j,
+                                      inv_cell_area_dt_n);
+
+            // Momentum of row j (:225-567), column by column.
+            const R sn_dn = __shfl_down_sync(FULL, sn_j[0], 1);
+            const R e_dn = __shfl_down_sync(FULL, e_j[0], 1);
+            const R vh_dn = __shfl_down_sync(FULL, vh_j[0], 1);
+            const R vhm_dn = __shfl_down_sync(FULL, vh_jm1[0], 1);
+            R uh_w[CPL];
+#pragma unroll
+            for (int c = 0; c < CPL; c++) uh_w[c] = west(uh_j, uhW_j, c);
+            const int jrow = j;
+            R o_uh[CPL], o_vh[CPL], o_mx[CPL];
+            bool ms_all = true;
+#pragma unroll
+            for (int c = 0; c < CPL; c++) {
+                const int i = c0 + c;
+                const bool last = (c == CPL - 1);
+                const R s_e = !last ? sn_j[c + 1 < CPL ? c + 1 : c] : (lane < 31 ? sn_dn : snE_j);
+                const R e_e = !last ? e_j[c + 1 < CPL ? c + 1 : c] : (lane < 31 ? e_dn : eE_j);
+                const R vh_e = !last ? vh_j[c + 1 < CPL ? c + 1 : c] : (lane < 31 ? vh_dn : vhE_j);
+                const R vh_se = !last ? vh_jm1[c + 1 < CPL ? c + 1 : c] : (lane < 31 ? vhm_dn : vhE_jm1);
+                const R snc = sn_j[c];
+                const bool in_ms = max_stage && i >= a.xl && i <= a.xu && jrow >= a.yl && jrow <= a.yu;
+                ms_all = ms_all && in_ms;
+                o_mx[c] = (snc > mx[c]) ? snc : mx[c];
+                R uh = uh_j[c], vh = vh_j[c];
+                if (i >= a.xl && i <= a.xu - 1 && jrow >= a.yl && jrow <= a.yu - 1) {
+                    const R e0 = e_j[c];
+                    const R sn = snc, s_n = sn_n[c];
+                    R h_iph, h_jph, wet_iph, wet_jph;
+                    if (TRUELY_LINEAR) {
+                        const bool wi = (e0 < -mad + a.msl) && (e_e < -mad + a.msl);
+                        h_iph = wi ? (a.msl - half * (e_e + e0)) : zero;
+                        const bool wj = (e_n[c] < -mad + a.msl) && (e0 < -mad + a.msl);
+                        h_jph = wj ? (a.msl - half * (e_n[c] + e0)) : zero;
+                        wet_iph = one;
+                        wet_jph = one;
+                    } else {
+                        const bool wi = (sn - e0 > mad) && (s_e - e_e > mad);
+                        h_iph = wi ? (half * ((s_e + sn) - (e_e + e0))) : zero;
+                        const bool wj = (s_n - e_n[c] > mad) && (sn - e0 > mad);
+                        h_jph = wj ? (half * ((s_n + sn) - (e_n[c] + e0))) : zero;
+                        wet_iph = (h_iph > zero) ? one : zero;
+                        wet_jph = (h_jph > zero) ? one : zero;
+                    }
+                    const R dw_j = s_n - sn;
+                    R uh_new = uh * wet_iph - inv_cell_area_dt_g * h_iph * (s_e - sn) * dyl_ip1[c];
+                    R vh_new = vh * wet_jph - inv_cell_area_dt_vh_g * h_jph * dw_j * a.m.dxb[jrow + 1];
+                    if (CORIOLIS) {
+                        const R vh_iph_jmh = half * (vh_jm1[c] + vh_se);
+                        const R vh_iph_jph = half * (vh_j[c] + vh_e);
+                        const R uh_i_j = half * (uh_j[c] + uh_w[c]);
+                        const R uh_i_jp1 = half * (uh_n[c] + uh_nw[c]);
+                        const R dt_half_coriolis = a.dt * a.m.cor[jrow] * half * ((h_iph > zero) ? one : zero);
+                        const R dt_half_coriolis_jph =
+                            a.dt * a.m.cor_be[jrow + 1] * half * ((h_jph > zero) ? one : zero);
+                        uh_new = uh_new + dt_half_coriolis * (vh_iph_jmh + vh_iph_jph);
+                        vh_new = vh_new - dt_half_coriolis_jph * (uh_i_j + uh_i_jp1);
+                    }
+                    if (a.lin_fric) {
+                        uh_new = a.lin_fric_mult * uh_new;
+                        vh_new = a.lin_fric_mult * vh_new;
+                    }
+                    uh = uh_new;
+                    vh = vh_new;
+                }
+                o_uh[c] = uh;
+                o_vh[c] = vh;
+                if (GAUGES && gmask && i < nx) {
+                    if (a.n_sites > 64) {
+                        for (int q = 0; q < a.n_sites; q++)
+                            if (a.sites[2 * q] == i && a.sites[2 * q + 1] == jrow) a.rec[q] = (double)snc;
+                    } else {
+                        for (unsigned long long m = gmask; m; m &= m - 1) {
+                            const int q = __ffsll((long long)m) - 1;
+                            if (a.sites[2 * q] == i && a.sites[2 * q + 1] == jrow) a.rec[q] = (double)snc;
+                        }
+                    }
+                }
+            }
+            {
+                const int64_t o = (int64_t)jrow * P + c0;
+                if (src_bytes == VB) {   // the lane's whole vector is inside the row
+                    store_vec<R, CPL>(stg_o + o, sn_j);
+                    store_vec<R, CPL>(uh_o + o, o_uh);
+                    store_vec<R, CPL>(vh_o + o, o_vh);
+                    if (ms_all) store_vec<R, CPL>(max_stage + o, o_mx);
+                }
+                if (src_bytes != VB || (max_stage && !ms_all)) {
+#pragma unroll
+                    for (int c = 0; c < CPL; c++) {
+                        const int i = c0 + c;
+                        if (i >= nx) continue;
+                        if (src_bytes != VB) {
+                            stg_o[o + c] = sn_j[c];
+                            uh_o[o + c] = o_uh[c];
+                            vh_o[o + c] = o_vh[c];
+                        }
+                        if (max_stage && i >= a.xl && i <= a.xu && jrow >= a.yl && jrow <= a.yu)
+                            max_stage[o + c] = o_mx[c];
+                    }
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < CPL; c++) {
+                vh_jm1[c] = vh_j[c];
+                uh_j[c] = uh_n[c]; vh_j[c] = vh_n[c]; e_j[c] = e_n[c]; sn_j[c] = sn_n[c]; mx[c] = mx_n[c];
+            }
+            vhE_jm1 = vhE_j;
+            vhE_j = vhE_n; eE_j = eE_n; snE_j = snE_n; uhW_j = uhW_n;
+        }
+        cp_async_wait<0>();
+    }
+}
+
 // One block: boundary stage/elevation at time+dt/2, boundary flux sums,
 // time bookkeeping (:117-205, :571).
 template <typename R>
@@ -1012,24 +1354,34 @@ template cudaError_t launch_batch_gauges<float>(int64_t, const float *, int64_t,
 // Configurations 0-4: shared-memory tiles (rows per CTA, thread rows,
 // instances per CTA); 5-7: streaming warps with 32, 64 or 128 rows per
 // segment; 8: streaming with the segment height chosen from the grid size;
-// 9-10: cp.async-pipelined streaming, 64 rows or chosen.  Plain domains use
-// ASYNC_DEFAULT.
+// 9-10: cp.async-pipelined streaming, 64 rows or chosen; 11-12: aligned
+// wide strips (8- or 16-byte lanes).  Plain domains use PLAIN_DEFAULT.
 struct TileCfg { int by, tyt, ib; };
 constexpr TileCfg kTileCfgs[] = {{16, 8, 1}, {16, 8, 2}, {16, 8, 4}, {32, 8, 2}, {8, 8, 4}};
 constexpr int kStreamSH[] = {32, 64, 128, 0};
 constexpr int kAsyncSH[] = {64, 0};
+// 11-12: aligned wide strips (linear_wide_kernel) with 8- and 16-byte lanes.
+constexpr int kWideLaneBytes[] = {8, 16};
 constexpr int kNumTileCfgs = sizeof(kTileCfgs) / sizeof(kTileCfgs[0]) + sizeof(kStreamSH) / sizeof(kStreamSH[0]) +
-                             sizeof(kAsyncSH) / sizeof(kAsyncSH[0]);
+                             sizeof(kAsyncSH) / sizeof(kAsyncSH[0]) + sizeof(kWideLaneBytes) / sizeof(kWideLaneBytes[0]);
 constexpr int STREAM_DEFAULT = 8;
 constexpr int ASYNC_DEFAULT = 10;
+constexpr int WIDE8_CFG = 11;
+constexpr int WIDE16_CFG = 12;
+// Plain steps use the aligned wide strips with 16-byte lanes: measured on
+// the 4096^2 / 8192^2 Gaussian basin (whole step against the measured copy
+// bandwidth) 0.84 / 0.93 in FP64 and 0.74 / 0.86 in FP32, against 0.72 /
+// 0.76 and 0.63 / 0.66 for the 30-column cp.async strips and 0.67 / 0.71
+// and 0.59 / 0.66 for wide strips with 8-byte lanes.
+constexpr int PLAIN_DEFAULT = WIDE16_CFG;
 
 // Rows per segment: the longest segment (up to 128 rows, which amortises the
 // two rows a segment reloads) that still gives every SM about 24 warps.
-inline int stream_rows(int nx, int ny, int nbatch)
+inline int stream_rows(int nx, int ny, int nbatch, int strip_cols = SOUT)
 {
     // At least four waves of 20 warps per SM (so the last, partial wave is a
     // small part of the launch), but no segment under 16 rows.
-    const int64_t nstrips = (nx + SOUT - 1) / SOUT;
+    const int64_t nstrips = (nx + strip_cols - 1) / strip_cols;
     const int64_t want = 148 * 20 * 4;
     int sh = 128;
     while (sh > 16 && (int64_t)nbatch * nstrips * ((ny + sh - 1) / sh) < want) sh /= 2;
@@ -1074,11 +1426,35 @@ void launch_async(const LinArgs<R> &a, int sh, cudaStream_t s)
         linear_async_kernel<R, COR, TL, false><<<grid, 128, 0, s>>>(a, sh, nstrips, total);
 }
 
+template <typename R, bool COR, bool TL, int CPL>
+void launch_wide(const LinArgs<R> &a, cudaStream_t s)
+{
+    constexpr int W = 32 * CPL;
+    const int sh = stream_rows(a.p.nx, a.p.ny, a.nbatch, W);
+    const int nstrips = (a.p.nx + W - 1) / W;
+    const int nseg = (a.p.ny + sh - 1) / sh;
+    const int total = nstrips * nseg;
+    const int gy = std::min((total + 3) / 4, 65535);
+    dim3 grid(a.nbatch, gy);
+    if (a.rec && a.n_sites > 0)
+        linear_wide_kernel<R, COR, TL, true, CPL><<<grid, 128, 0, s>>>(a, sh, nstrips, total);
+    else
+        linear_wide_kernel<R, COR, TL, false, CPL><<<grid, 128, 0, s>>>(a, sh, nstrips, total);
+}
+
 template <typename R, bool COR, bool TL>
 void launch_tile(const LinArgs<R> &a, int cfg, cudaStream_t s)
 {
     const int ntile = (int)(sizeof(kTileCfgs) / sizeof(kTileCfgs[0]));
     const int nstream = (int)(sizeof(kStreamSH) / sizeof(kStreamSH[0]));
+    const int nasync = (int)(sizeof(kAsyncSH) / sizeof(kAsyncSH[0]));
+    if (cfg >= ntile + nstream + nasync) {
+        if (kWideLaneBytes[cfg - ntile - nstream - nasync] == 8)
+            launch_wide<R, COR, TL, 8 / (int)sizeof(R)>(a, s);
+        else
+            launch_wide<R, COR, TL, 16 / (int)sizeof(R)>(a, s);
+        return;
+    }
     if (cfg >= ntile + nstream) {
         launch_async<R, COR, TL>(a, kAsyncSH[cfg - ntile - nstream], s);
         return;
@@ -1106,14 +1482,21 @@ void launch_main(const LinArgs<R> &a, const StepConfig &c, int cfg, cudaStream_t
     else launch_tile<R, false, false>(a, cfg, s);
 }
 
-// Kernel of a plain (unbatched) step: the cp.async-pipelined streaming form
-// unless SWALS_LINEAR_KERNEL selects "stream" (registers only) or "tile".
+// Kernel of a plain (unbatched) step: the default streaming form unless
+// SWALS_LINEAR_KERNEL selects "tile", "stream" (registers only), "async"
+// (30-column strips through cp.async) or "wide8" / "wide16" (aligned wide
+// strips, 8- or 16-byte lanes).
 int linear_kernel_config()
 {
     static int cfg = -1;
     if (cfg < 0) {
         const char *e = getenv("SWALS_LINEAR_KERNEL");
-        cfg = (e && strcmp(e, "tile") == 0) ? 0 : (e && strcmp(e, "stream") == 0) ? STREAM_DEFAULT : ASYNC_DEFAULT;
+        cfg = PLAIN_DEFAULT;
+        if (e && strcmp(e, "tile") == 0) cfg = 0;
+        else if (e && strcmp(e, "stream") == 0) cfg = STREAM_DEFAULT;
+        else if (e && strcmp(e, "async") == 0) cfg = ASYNC_DEFAULT;
+        else if (e && strcmp(e, "wide8") == 0) cfg = WIDE8_CFG;
+        else if (e && strcmp(e, "wide16") == 0) cfg = WIDE16_CFG;
     }
     return cfg;
 }

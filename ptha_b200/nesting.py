@@ -21,7 +21,8 @@ GPU path can build the exchange tables the device kernels consume:
 
 All coordinates are computed with the reference's expressions in IEEE double
 so that the integer boxes match the reference's bit for bit (the reference's
-own known answers for its 4-domain nest are in ``tests/golden``).
+own known answers for its 4-domain nest are re-encoded in
+``tests/test_nesting_metadata.py``).
 """
 from __future__ import annotations
 

@@ -50,7 +50,7 @@ def test_batch_equals_single_instances(real32):
         d.close()
     from ptha_b200._lib import lib
     import ctypes
-    for cfg in range(5):
+    for cfg in range(Batch.tile_config_count()):
         bt = Batch(grid, B)
         bt.set_U(ics)
         bt.set_tile_config(cfg)

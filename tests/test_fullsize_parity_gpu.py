@@ -148,7 +148,7 @@ def test_batched_3600x2400_fp32_instances():
     ref = single.get_U()[:3]
     ref_max = single.max_stage()
     single.close()
-    for cfg in range(5):
+    for cfg in range(Batch.tile_config_count()):
         bt = Batch(grid, B)
         bt.set_U(ics)
         bt.set_tile_config(cfg)
