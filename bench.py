@@ -128,20 +128,30 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(workload="rk2_beach", min_seconds=12.0, exact_steps=0, variant="native"):
+def cpu_baseline(workload="rk2_beach", min_seconds=12.0, exact_steps=0, variant="native", samples=0,
+                 warmup_steps=1):
     """The oracle on this machine's host cores, in its own process (its OpenMP
     runtime never shares a process with the GPU runtime)."""
     cmd = [sys.executable, os.path.join(ROOT, "oracle", "cpu_baseline.py"), "--workload", workload,
-           "--min-seconds", str(min_seconds), "--variant", variant]
+           "--min-seconds", str(min_seconds), "--variant", variant, "--warmup-steps", str(warmup_steps)]
     if exact_steps:
         cmd += ["--exact-steps", str(exact_steps)]
+    if samples:
+        cmd += ["--samples", str(samples)]
     env = dict(os.environ)
     env.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
     env.setdefault("OMP_PROC_BIND", "true")
     out = subprocess.run(cmd, capture_output=True, text=True, env=env, check=True)
     r = json.loads(out.stdout.strip().splitlines()[-1])
     return {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": "port", "variant": r["variant"],
+            "values": r.get("values"),
             "sample": r["sample"] + "; C restatement of the reference's OpenMP loops (no Fortran compiler)"}
+
+
+# CPU samples: timesteps per sample of the 2048^2 workload (about 1 s on 16
+# cores), after CPU_WARMUP untimed timesteps; the same procedure in both arms.
+CPU_STEPS_PER_SAMPLE = 12
+CPU_WARMUP = 3
 
 
 def headline_config(n, real32=False, world=1):
@@ -164,29 +174,26 @@ def dist_setup(ngpus):
 def run_reference(args, world, rank):
     """The reference's CPU path for this workload: the oracle built with the
     flags the reference ships (-O3 -ffast-math, libm pow) plus -march=native
-    on this machine, all host threads; each bench step a bounded sample of
-    the same 2048^2 workload (a few timesteps from the initial state; the
-    per-timestep cost of these loops does not depend on the state)."""
+    on this machine, all host threads; each bench step is one sample of
+    CPU_STEPS_PER_SAMPLE timesteps of the same 2048^2 workload, the samples
+    taken one after another in one process after W x CPU_WARMUP untimed
+    timesteps.  The IEEE-strict build's rate is reported beside it."""
     if rank != 0:
         return
-    steps_per = 4
-    r = cpu_baseline("rk2_beach", exact_steps=steps_per * max(1, args.warmup))  # warm-up (build, page-in, threads)
-    variant = r["variant"]
-    vals = []
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        r = cpu_baseline("rk2_beach", exact_steps=steps_per, variant=variant)
-        vals.append(r["value"])
+    r = cpu_baseline("rk2_beach", exact_steps=CPU_STEPS_PER_SAMPLE, samples=args.steps,
+                     warmup_steps=CPU_WARMUP * max(1, args.warmup))
     wall = time.perf_counter() - t0
-    value = statistics.median(vals)
-    strict = cpu_baseline("rk2_beach", exact_steps=steps_per, variant="strict")
+    value = r["value"]
+    strict = cpu_baseline("rk2_beach", exact_steps=CPU_STEPS_PER_SAMPLE, samples=1, variant="strict",
+                          warmup_steps=CPU_WARMUP)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": N * N * steps_per / value * 1e3, "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": N * N * CPU_STEPS_PER_SAMPLE / value * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": headline_config(N, world=world), "timesteps_per_step": steps_per,
+            "config": headline_config(N, world=world), "timesteps_per_step": CPU_STEPS_PER_SAMPLE,
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": r["cores"], "kind": "port",
-                             "sample": f"{steps_per} rk2 timesteps of the 2048x2048 workload per step; " + r["sample"],
+                             "sample": r["sample"], "samples": r["values"],
                              "strict_build_value": strict["value"]},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "wall_s": wall}
@@ -346,8 +353,9 @@ def run_ours(args, world, rank, local):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and N == 2048:
         try:
-            cpu = cpu_baseline("rk2_beach", min_seconds=10.0)
-            cpu["strict_build_value"] = cpu_baseline("rk2_beach", min_seconds=5.0, variant="strict")["value"]
+            cpu = cpu_baseline("rk2_beach", exact_steps=CPU_STEPS_PER_SAMPLE, samples=7, warmup_steps=CPU_WARMUP)
+            cpu["strict_build_value"] = cpu_baseline("rk2_beach", exact_steps=CPU_STEPS_PER_SAMPLE, samples=1,
+                                                     variant="strict", warmup_steps=CPU_WARMUP)["value"]
         except Exception as ex:  # the baseline is reported, never required
             cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port", "sample": f"failed: {ex}"}
 
@@ -569,14 +577,15 @@ def form_adjoint(local, nx=1200, ny=800, reps=2):
             "loss": loss, "grad_norm": float(np.linalg.norm(grad[0]))}
 
 
-def _nested(local, nts, sources=1):
+def _nested(local, nts, source_seed=11, elevations=None):
     from ptha_b200 import Multidomain, workloads
     specs, coasts = workloads.nested_specs(nts)
     kw = [dict(real_bytes=4, spherical=True), dict(spherical=True), dict(spherical=True), dict(spherical=True)]
     md = Multidomain(specs, domain_kwargs=kw, use_wetdry_limiting=True, flux_correction=True, device=local,
                      periodic_xs=(0.0, 360.0))
     for k, (s_, d) in enumerate(zip(specs, md.domains)):
-        d.set_U(workloads.nested_initial_state(s_, k, coasts))
+        d.set_U(workloads.nested_initial_state(s_, k, coasts, source_seed=source_seed,
+                                               elevation=None if elevations is None else elevations[k]))
         if d.timestepping_method == "rk2":
             d.set_manning_squared(0.025 ** 2)
     return specs, md
@@ -624,9 +633,48 @@ def form_multidomain(local, reps=20, K=3):
     return out
 
 
-def form_nested16(local):
-    """Placeholder until the batch-of-nests form exists."""
-    return {"skipped": "not built"}
+def form_nested16(local, B=16, K=3, reps=6):
+    """The nested configuration with B = 16 dipole sources (seeds 11..26):
+    16 instances of the four-domain nest advanced together, K md steps of
+    every instance captured into one CUDA graph (one branch per instance, the
+    instances' kernels running concurrently), against the same instances
+    replayed one after another (each instance's own K-step graph)."""
+    import numpy as np
+    import torch
+    from ptha_b200 import MultidomainGroup, workloads
+    dt, nts = _nested_refinement(local)
+    specs0, coasts = workloads.nested_specs(nts)
+    specs0, md0 = _nested(local, nts)
+    elevations = [workloads.nested_elevation(s_, k, coasts) for k, s_ in enumerate(specs0)]
+    mds = [md0] + [_nested(local, nts, source_seed=11 + q, elevations=elevations)[1] for q in range(1, B)]
+    cells = sum(s_.nx[0] * s_.nx[1] * nt for s_, nt in zip(specs0, nts))
+    for md in mds:
+        md.capture_graph(K, dt)
+        md.replay(1)
+    torch.cuda.synchronize()
+    # one after another: each instance's own graph, device time on its stream
+    seq = 0.0
+    for md in mds:
+        st = torch.cuda.ExternalStream(md.domains[0].stream(), device=f"cuda:{local}")
+        seq += _event_ms(st, lambda: md.replay(reps))
+    group = MultidomainGroup(mds, K, dt)
+    group.replay(1)
+    torch.cuda.synchronize()
+    gs = torch.cuda.ExternalStream(group.stream(), device=f"cuda:{local}")
+    ms = _event_ms(gs, lambda: group.replay(reps))
+    torch.cuda.synchronize()
+    vols = [d.volume_interior() for md in mds for d in md.domains]
+    group.close()
+    for md in mds:
+        md.close()
+    ms_step = ms / (reps * K)
+    return {"workload": "nested_multidomain_4dom_x16_sources", "value": B * cells / (ms_step / 1e3), "unit": UNIT,
+            "sources": B, "ms_per_md_step_all_sources": ms_step, "md_dt": dt, "graph_steps": K,
+            "cell_updates_per_md_step": B * cells,
+            "one_after_another": {"value": B * cells / (seq / (reps * K) / 1e3),
+                                  "ms_per_md_step_all_sources": seq / (reps * K)},
+            "speedup_vs_one_after_another": seq / ms,
+            "dtype": "f32 coarse / f64 fine", "finite": bool(all(np.isfinite(v) for v in vols))}
 
 
 def run_form(args, local, world=1, rank=0):

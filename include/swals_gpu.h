@@ -366,6 +366,22 @@ int swals_gpu_md_download_flux(swals_multidomain *md, int32_t exchange, int32_t 
  * graph launch.  The host time and step counts advance on replay. */
 int swals_gpu_md_capture_graph(swals_multidomain *md, int32_t nsteps, double dt);
 int swals_gpu_md_replay(swals_multidomain *md, int32_t nreplays);
+/* Many multidomains advanced together (for example B sources on the same
+ * nest: the batched form of the nested configuration; the reference steps
+ * each multidomain_type on its own, multidomain_mod.f90:1093-1212).  The
+ * group captures nsteps md steps of fixed dt of every member into one CUDA
+ * graph, each member on its own branch, so one replay advances all of them
+ * with their kernels running concurrently.  The members stay usable on
+ * their own (a replay is ordered after work already issued on their
+ * streams, and work issued later after the replay); every member's domains
+ * must be in the state buffers they were captured in (steps in multiples of
+ * 3 keep them there).  Destroy the group before its members. */
+typedef struct swals_md_group swals_md_group;
+int swals_gpu_md_group_create(swals_multidomain *const *mds, int32_t n, int32_t nsteps, double dt,
+                              swals_md_group **out);
+int swals_gpu_md_group_replay(swals_md_group *g, int32_t nreplays);
+int swals_gpu_md_group_stream(swals_md_group *g, void **stream);
+int swals_gpu_md_group_destroy(swals_md_group *g);
 int swals_gpu_md_time(swals_multidomain *md, double *time);
 int swals_gpu_md_synchronize(swals_multidomain *md);
 int swals_gpu_md_launch_count(swals_multidomain *md, int64_t *n);

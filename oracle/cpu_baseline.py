@@ -28,6 +28,8 @@ def main():
     ap.add_argument("--min-seconds", type=float, default=10.0)
     ap.add_argument("--max-steps", type=int, default=1000)
     ap.add_argument("--exact-steps", type=int, default=0)
+    ap.add_argument("--samples", type=int, default=0, help="time this many samples of --exact-steps timesteps")
+    ap.add_argument("--warmup-steps", type=int, default=1)
     ap.add_argument("--variant", default="fast", choices=["fast", "native", "strict"],
                     help="oracle build: fast = -O3 -ffast-math with libm pow (the reference's -Ofast), "
                          "native = the same with -march=native (built here on first use), strict = the "
@@ -57,7 +59,26 @@ def main():
     else:
         raise SystemExit(f"unknown workload {args.workload}")
     nx, ny = kw["nx"]
-    o.evolve_one_step(dt)  # untimed first step (page-in, thread start)
+    for _ in range(max(1, args.warmup_steps)):
+        o.evolve_one_step(dt)  # untimed (page-in, thread start)
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    if args.samples:
+        # `samples` timed samples of exact_steps timesteps each, in a row
+        vals = []
+        for _ in range(args.samples):
+            t0 = time.perf_counter()
+            for _ in range(args.exact_steps):
+                o.evolve_one_step(dt)
+            vals.append(nx * ny * args.exact_steps / (time.perf_counter() - t0))
+        vals_sorted = sorted(vals)
+        med = vals_sorted[len(vals) // 2] if len(vals) % 2 else 0.5 * (vals_sorted[len(vals) // 2 - 1] +
+                                                                        vals_sorted[len(vals) // 2])
+        print(json.dumps({"value": med, "values": vals, "unit": "cell-updates/s", "cores": threads,
+                          "steps": args.exact_steps * args.samples, "cells": nx * ny, "variant": variant,
+                          "flags": flags,
+                          "sample": f"{args.workload} {nx}x{ny}: {args.samples} samples of {args.exact_steps} "
+                                    f"timesteps after {args.warmup_steps} untimed ({flags})"}))
+        return
     steps = 0
     t0 = time.perf_counter()
     while True:
@@ -70,10 +91,10 @@ def main():
         elif el >= args.min_seconds or steps >= args.max_steps:
             break
     el = time.perf_counter() - t0
-    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
     print(json.dumps({"value": nx * ny * steps / el, "unit": "cell-updates/s", "cores": threads,
                       "steps": steps, "seconds": el, "cells": nx * ny, "variant": variant, "flags": flags,
-                      "sample": f"{args.workload} {nx}x{ny}: {steps} timesteps after 1 untimed ({flags})"}))
+                      "sample": f"{args.workload} {nx}x{ny}: {steps} timesteps after {args.warmup_steps} untimed "
+                                f"({flags})"}))
 
 
 if __name__ == "__main__":

@@ -5,7 +5,7 @@ package builds it and mirrors SWALS's ``domain_type`` API on top of it.
 """
 from ._lib import SwalsError  # noqa: F401
 from .domain import Domain, STG, UH, VH, ELV  # noqa: F401
-from .multidomain import Multidomain  # noqa: F401
+from .multidomain import Multidomain, MultidomainGroup  # noqa: F401
 from .nesting import NestDomain  # noqa: F401
 
-__all__ = ["Domain", "Multidomain", "NestDomain", "SwalsError", "STG", "UH", "VH", "ELV"]
+__all__ = ["Domain", "Multidomain", "MultidomainGroup", "NestDomain", "SwalsError", "STG", "UH", "VH", "ELV"]

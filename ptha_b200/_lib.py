@@ -43,6 +43,8 @@ EXPORTED = [
     "swals_gpu_md_recv_halos", "swals_gpu_md_flux_correction", "swals_gpu_md_buffer_size",
     "swals_gpu_md_download_buffer", "swals_gpu_md_download_flux", "swals_gpu_md_time", "swals_gpu_md_synchronize",
     "swals_gpu_md_launch_count", "swals_gpu_md_capture_graph", "swals_gpu_md_replay",
+    "swals_gpu_md_group_create", "swals_gpu_md_group_replay", "swals_gpu_md_group_stream",
+    "swals_gpu_md_group_destroy",
     "swals_gpu_set_priority_mask", "swals_gpu_domain_statistics", "swals_gpu_volume_in_priority_domain",
     "swals_gpu_forcing_patch_add", "swals_gpu_forcing_clear", "swals_gpu_apply_forcing",
     "swals_gpu_set_eddy_viscosity", "swals_gpu_set_static_before_time", "swals_gpu_set_max_U_update_frequency",
@@ -160,6 +162,9 @@ def lib():
         "swals_gpu_md_time": [vp, ctypes.POINTER(dbl)], "swals_gpu_md_synchronize": [vp],
         "swals_gpu_md_launch_count": [vp, ctypes.POINTER(i64)],
         "swals_gpu_md_capture_graph": [vp, i32, dbl], "swals_gpu_md_replay": [vp, i32],
+        "swals_gpu_md_group_create": [vp, i32, i32, dbl, ctypes.POINTER(vp)],
+        "swals_gpu_md_group_replay": [vp, i32], "swals_gpu_md_group_stream": [vp, ctypes.POINTER(vp)],
+        "swals_gpu_md_group_destroy": [vp],
         "swals_gpu_set_priority_mask": [vp, vp], "swals_gpu_domain_statistics": [vp, vp],
         "swals_gpu_volume_in_priority_domain": [vp, ctypes.POINTER(dbl)],
         "swals_gpu_forcing_patch_add": [vp, i32, i32, i32, i32, i32, i32, dbl, dbl, vp, ctypes.POINTER(i32)],

@@ -237,11 +237,13 @@ int evolve_t(swals_domain *d, double timestep, int has_dt)
                                       (const R *)d->elv, max_stage, c, d->max_u, d->sc, every, d->stream);
     };
     if (d->nsteps == 0 && max_stage) {
+        // Gated on the device step count as well, so that a graph captured
+        // from the first step does this only on its first replay.
         hook(CAT_MAXSTAGE, 0);
-        cudaError_t e = d->max_u_generic ? max_u_after(1)
-                                         : launch_update_max_stage<R>(d->nx, d->ny, d->pitch,
-                                                                      (const R *)d->planes[d->cur][0], max_stage, c,
-                                                                      d->stream);
+        cudaError_t e = d->max_u_generic ? max_u_after(0)
+                                         : launch_update_max_stage_every<R>(d->nx, d->ny, d->pitch,
+                                                                            (const R *)d->planes[d->cur][0],
+                                                                            max_stage, c, d->sc, 0, d->stream);
         hook(CAT_MAXSTAGE, 1);
         if (e != cudaSuccess) return cuda_fail(e, "update_max_quantities");
     }

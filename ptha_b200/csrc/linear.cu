@@ -1292,8 +1292,11 @@ __global__ void max_stage_kernel(int nx, int ny, int64_t P, const R *stg, R *mx,
                                  const DevScalars *sc, int every)
 {
     // every > 1: max_U_update_frequency (domain_mod.f90:1794-1798), after a
-    // step that has already counted itself in nsteps_advanced
+    // step that has already counted itself in nsteps_advanced; every == 0:
+    // the update before the first step (:1719), which a replayed graph
+    // repeats as a launch but only the first replay carries out
     if (every > 1 && (sc->nsteps_advanced - 1) % every != 0) return;
+    if (every == 0 && sc->nsteps_advanced != 0) return;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int r = blockIdx.y * blockDim.y + threadIdx.y;
     if (i < xl || i > xu || r < yl || r > yu || i >= nx || r >= ny) return;
@@ -2086,6 +2089,7 @@ __global__ void max_u_kernel(int nx, int ny, int64_t P, const R *stg, const R *u
                              const DevScalars *sc, int every)
 {
     if (every > 1 && (sc->nsteps_advanced - 1) % every != 0) return;
+    if (every == 0 && sc->nsteps_advanced != 0) return;   // before the first step only
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int r = blockIdx.y * blockDim.y + threadIdx.y;
     if (i < xl || i > xu || r < yl || r > yu || i >= nx || r >= ny) return;

@@ -1243,6 +1243,167 @@ int swals_gpu_md_replay(swals_multidomain *md, int32_t nreplays)
     return SWALS_OK;
 }
 
+// A group of multidomains (independent instances: many sources on the same
+// nest, or different nests) advanced together: nsteps md steps of every
+// member captured into one CUDA graph, each member on its own branch (its
+// own stream, forked from and joined back to the group's stream), so one
+// launch advances all of them and the kernels of different members run
+// concurrently: the small exchange kernels and the partial last waves of
+// each domain's step kernels are overlapped with other members' work.
+struct swals_md_group {
+    std::vector<swals_multidomain *> mds;
+    std::vector<std::vector<int>> cur;   // each member's domains' state buffers at the capture
+    cudaStream_t stream = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int device = 0;
+    int steps = 0;
+    double dt = 0.0;
+};
+
+int swals_gpu_md_group_create(swals_multidomain *const *mds, int32_t n, int32_t nsteps, double dt,
+                              swals_md_group **out)
+{
+    if (!mds || n < 1 || nsteps < 1 || !(dt > 0.0) || !out) return fail(SWALS_ERR_INVALID_ARGUMENT, "bad argument");
+    *out = nullptr;
+    for (int q = 0; q < n; q++) {
+        if (!mds[q]) return fail(SWALS_ERR_INVALID_ARGUMENT, "NULL multidomain %d", q);
+        if (mds[q]->device != mds[0]->device) return fail(SWALS_ERR_INVALID_ARGUMENT, "members on different devices");
+        for (int r = 0; r < q; r++)
+            if (mds[r] == mds[q]) return fail(SWALS_ERR_INVALID_ARGUMENT, "multidomain %d appears twice", q);
+    }
+    MDCK(cudaSetDevice(mds[0]->device));
+    swals_md_group *g = new swals_md_group();
+    g->mds.assign(mds, mds + n);
+    g->device = mds[0]->device;
+    g->steps = nsteps;
+    g->dt = dt;
+    cudaError_t ce = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking);
+    if (ce != cudaSuccess) { delete g; return api_cuda_fail(ce, "group stream"); }
+    // Host bookkeeping of every member, restored after the capture.
+    struct Saved { double time; int64_t launches; std::vector<int> cur; std::vector<int64_t> dl, ns; };
+    std::vector<Saved> saved(n);
+    for (int q = 0; q < n; q++) {
+        swals_multidomain *md = g->mds[q];
+        MDCK(cudaStreamSynchronize(md->stream));
+        saved[q].time = md->time;
+        saved[q].launches = md->launches;
+        for (swals_domain *d : md->doms) {
+            saved[q].cur.push_back(d->cur);
+            saved[q].dl.push_back(d->launches);
+            saved[q].ns.push_back(d->nsteps);
+        }
+    }
+    std::vector<cudaEvent_t> evs(n + 1, nullptr);
+    int rc = SWALS_OK;
+    for (auto &e : evs)
+        if (rc == SWALS_OK && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+            rc = fail(SWALS_ERR_CUDA, "event creation");
+    cudaGraph_t graph = nullptr;
+    if (rc == SWALS_OK) {
+        ce = cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal);
+        if (ce != cudaSuccess) rc = api_cuda_fail(ce, "cudaStreamBeginCapture");
+    }
+    if (rc == SWALS_OK) {
+        bool capturing = true;
+        ce = cudaEventRecord(evs[n], g->stream);   // fork
+        for (int q = 0; q < n && ce == cudaSuccess; q++) ce = cudaStreamWaitEvent(g->mds[q]->stream, evs[n], 0);
+        if (ce != cudaSuccess) rc = api_cuda_fail(ce, "fork");
+        for (int q = 0; q < n && rc == SWALS_OK; q++)
+            for (int s = 0; s < nsteps && rc == SWALS_OK; s++) rc = swals_gpu_md_evolve_one_step(g->mds[q], dt);
+        for (int q = 0; q < n && rc == SWALS_OK; q++) {   // join
+            ce = cudaEventRecord(evs[q], g->mds[q]->stream);
+            if (ce == cudaSuccess) ce = cudaStreamWaitEvent(g->stream, evs[q], 0);
+            if (ce != cudaSuccess) rc = api_cuda_fail(ce, "join");
+        }
+        ce = cudaStreamEndCapture(g->stream, &graph);
+        capturing = false;
+        (void)capturing;
+        if (rc == SWALS_OK && ce != cudaSuccess) rc = api_cuda_fail(ce, "cudaStreamEndCapture");
+    }
+    // Capture records work without running it: restore the bookkeeping, and
+    // require every domain back in its state buffer after nsteps.
+    bool same = true;
+    for (int q = 0; q < n; q++) {
+        swals_multidomain *md = g->mds[q];
+        md->time = saved[q].time;
+        md->launches = saved[q].launches;
+        for (size_t k = 0; k < md->doms.size(); k++) {
+            same &= (md->doms[k]->cur == saved[q].cur[k]);
+            md->doms[k]->cur = saved[q].cur[k];
+            md->doms[k]->launches = saved[q].dl[k];
+            md->doms[k]->nsteps = saved[q].ns[k];
+        }
+        g->cur.push_back(saved[q].cur);
+    }
+    for (auto &e : evs)
+        if (e) cudaEventDestroy(e);
+    if (rc == SWALS_OK && !same)
+        rc = fail(SWALS_ERR_INVALID_ARGUMENT,
+                  "%d md steps do not return every domain to its state buffer; capture a multiple of 3 steps", nsteps);
+    if (rc == SWALS_OK) {
+        ce = cudaGraphInstantiate(&g->exec, graph, 0);
+        if (ce != cudaSuccess) rc = api_cuda_fail(ce, "cudaGraphInstantiate");
+    }
+    if (graph) cudaGraphDestroy(graph);
+    if (rc != SWALS_OK) {
+        if (g->exec) cudaGraphExecDestroy(g->exec);
+        cudaStreamDestroy(g->stream);
+        delete g;
+        return rc;
+    }
+    *out = g;
+    return SWALS_OK;
+}
+
+int swals_gpu_md_group_replay(swals_md_group *g, int32_t nreplays)
+{
+    if (!g || nreplays < 0) return fail(SWALS_ERR_INVALID_ARGUMENT, "bad argument");
+    for (size_t q = 0; q < g->mds.size(); q++)
+        for (size_t k = 0; k < g->mds[q]->doms.size(); k++)
+            if (g->mds[q]->doms[k]->cur != g->cur[q][k])
+                return fail(SWALS_ERR_INVALID_ARGUMENT,
+                            "member %d, domain %d has moved to another state buffer since the group was captured",
+                            (int)q, (int)k);
+    MDCK(cudaSetDevice(g->device));
+    // the members' own streams may hold work issued before: the graph
+    // starts after it
+    cudaEvent_t ev = nullptr;
+    MDCK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    for (swals_multidomain *md : g->mds) {
+        MDCK(cudaEventRecord(ev, md->stream));
+        MDCK(cudaStreamWaitEvent(g->stream, ev, 0));
+    }
+    for (int r = 0; r < nreplays; r++) MDCK(cudaGraphLaunch(g->exec, g->stream));
+    // and work issued on a member's stream afterwards follows the replays
+    MDCK(cudaEventRecord(ev, g->stream));
+    for (swals_multidomain *md : g->mds) MDCK(cudaStreamWaitEvent(md->stream, ev, 0));
+    cudaEventDestroy(ev);
+    for (swals_multidomain *md : g->mds) {
+        md->launches += nreplays;
+        md->time += (double)nreplays * g->steps * g->dt;
+        for (swals_domain *d : md->doms) d->nsteps += (int64_t)nreplays * g->steps;
+    }
+    return SWALS_OK;
+}
+
+int swals_gpu_md_group_stream(swals_md_group *g, void **stream)
+{
+    if (!g || !stream) return fail(SWALS_ERR_INVALID_ARGUMENT, "bad argument");
+    *stream = (void *)g->stream;
+    return SWALS_OK;
+}
+
+int swals_gpu_md_group_destroy(swals_md_group *g)
+{
+    if (!g) return SWALS_OK;
+    cudaSetDevice(g->device);
+    cudaStreamSynchronize(g->stream);
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    cudaStreamDestroy(g->stream);
+    delete g;
+    return SWALS_OK;
+}
+
 int swals_gpu_md_buffer_size(swals_multidomain *md, int32_t x, int64_t *n)
 {
     if (!md || !n || x < 0 || x >= (int32_t)md->ex.size()) return fail(SWALS_ERR_INVALID_ARGUMENT, "bad argument");

@@ -165,3 +165,41 @@ class Multidomain:
         n = ctypes.c_int64()
         check(self._L.swals_gpu_md_launch_count(self._md, ctypes.byref(n)))
         return n.value
+
+
+class MultidomainGroup:
+    """Many multidomains advanced together (``swals_gpu_md_group_*``): e.g.
+    B sources on the same nest.  ``nsteps`` md steps of fixed ``dt`` of every
+    member are captured into one CUDA graph (one branch per member); each
+    ``replay()`` advances every member by nsteps md steps in one launch, the
+    members' kernels running concurrently.  Close the group before its
+    members."""
+
+    def __init__(self, members: Sequence[Multidomain], nsteps: int, dt: float):
+        self._L = _lib.lib()
+        self.members = list(members)
+        arr = (ctypes.c_void_p * len(self.members))(*[m._md for m in self.members])
+        h = ctypes.c_void_p()
+        check(self._L.swals_gpu_md_group_create(arr, len(self.members), int(nsteps), float(dt), ctypes.byref(h)))
+        self._h = h
+        self.nsteps = int(nsteps)
+        self.dt = float(dt)
+
+    def replay(self, nreplays: int = 1):
+        check(self._L.swals_gpu_md_group_replay(self._h, int(nreplays)))
+
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        check(self._L.swals_gpu_md_group_stream(self._h, ctypes.byref(s)))
+        return s.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.swals_gpu_md_group_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

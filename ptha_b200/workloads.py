@@ -223,38 +223,51 @@ def nested_specs(nts=(1, 1, 1, 1), scale=1):
     'linear' band 5400 x 1800 at 4 arcmin over 0-360 x 60S-60N, one
     ratio-3 'rk2' 900 x 900 domain and two ratio-9 'rk2' wet/dry domains
     (1197 x 801 and 702 x 1098: the nearest sizes that are whole parent
-    cells).  `scale` > 1 shrinks every domain by that factor (same
-    geometry, coarser cells) for quick checks.  Returns NestDomain objects
-    and the coastlines of coast_elevation."""
+    cells).  `scale` 3, 5 or 15 shrinks every domain by that factor (same
+    geometry, coarser cells, nested edges still on parent cell edges) for
+    quick checks.  Returns NestDomain objects and the coastlines of
+    coast_elevation."""
     import math
     from .nesting import NestDomain
+    if scale not in (1, 3, 5, 15):
+        raise ValueError("scale must be 1, 3, 5 or 15 (nested edges on parent cell edges)")
     c = NEST_COARSE * scale
     f3, f9 = c / 3.0, c / 9.0
-    n = lambda v: v // scale    # noqa: E731
+    n = lambda v: v // scale                    # noqa: E731
+    n9 = lambda v: max(9, v // scale // 9 * 9)  # noqa: E731  (whole parent cells)
     specs = [
         NestDomain((0.0, -60.0), (n(5400) * c, n(1800) * c), (n(5400), n(1800)), "linear", nts[0]),
         NestDomain((140.0, -40.0), (n(900) * f3, n(900) * f3), (n(900), n(900)), "rk2", nts[1]),
-        NestDomain((141.0 + 2 * c, -39.0), (n(1197) * f9, n(801) * f9), (n(1197), n(801)), "rk2", nts[2]),
-        NestDomain((152.0, -35.0), (n(702) * f9, n(1098) * f9), (n(702), n(1098)), "rk2", nts[3]),
+        NestDomain((141.0 + 2 * c, -39.0), (n9(1197) * f9, n9(801) * f9), (n9(1197), n9(801)), "rk2", nts[2]),
+        NestDomain((152.0, -35.0), (n9(702) * f9, n9(1098) * f9), (n9(702), n9(1098)), "rk2", nts[3]),
     ]
-    coasts = [(141.0 + 2 * c + n(1197) * f9 * 0.75, -39.0 + n(801) * f9 * 0.5, 0.0,
+    coasts = [(141.0 + 2 * c + n9(1197) * f9 * 0.75, -39.0 + n9(801) * f9 * 0.5, 0.0,
                (140.5, 151.0, -39.5, -32.5)),
-              (152.0 + n(702) * f9 * 0.5, -35.0 + n(1098) * f9 * 0.8, math.pi / 2,
+              (152.0 + n9(702) * f9 * 0.5, -35.0 + n9(1098) * f9 * 0.8, math.pi / 2,
                (151.5, 157.7, -35.5, -26.3))]
     return specs, coasts
 
 
-def nested_initial_state(spec, k, coasts, source_seed=11):
-    """U (4, ny, nx) of domain k of the nested configuration (after setup
-    widened it): coastal elevation, walls on the coarse band's north and
-    south rings, one dipole source (seed source_seed) on the wet cells,
-    stage = elevation on land."""
+def nested_elevation(spec, k, coasts):
+    """Elevation (ny, nx) of domain k of the nested configuration (after
+    setup widened it): coastal ramps, walls on the coarse band's north and
+    south rings."""
     lon, lat = spec.x(), spec.y()
     LON, LAT = np.meshgrid(lon, lat)
     elv = coast_elevation(LON, LAT, coasts)
     if k == 0:
         elv[:2, :] = 100.0
         elv[-2:, :] = 100.0
+    return elv
+
+
+def nested_initial_state(spec, k, coasts, source_seed=11, elevation=None):
+    """U (4, ny, nx) of domain k of the nested configuration (after setup
+    widened it): nested_elevation (or the one given), one dipole source
+    (seed source_seed) on the wet cells, stage = elevation on land.  Source
+    seeds 11, 12, ... are the instances of the batched (16-source) form."""
+    lon, lat = spec.x(), spec.y()
+    elv = nested_elevation(spec, k, coasts) if elevation is None else elevation
     eta = dipoles(lon, lat, 1, seed=source_seed, band=((144.0, -37.0), (150.0, -30.0)))[0]
     U = np.zeros((4, spec.nx[1], spec.nx[0]))
     U[3] = elv
