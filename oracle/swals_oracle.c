@@ -1729,8 +1729,33 @@ static void one_midpoint_step(oracle_domain *d, double timestep, int has_ts)
 }
 
 /* domain_mod.f90:1679-1813 */
+/* The baseline build (-O3 -ffast-math) runs with denormals flushed to zero,
+ * as an executable built with the reference's -Ofast does (gfortran links
+ * the start-up code that sets FTZ/DAZ); on every thread of the OpenMP pool,
+ * once.  The IEEE-strict checker builds keep gradual underflow. */
+#if defined(__FAST_MATH__) && defined(__x86_64__)
+#include <pmmintrin.h>
+#include <xmmintrin.h>
+static void or_fast_math_fp_env(void)
+{
+    static int done = 0;
+    if (done) return;
+#pragma omp parallel
+    {
+        _MM_SET_FLUSH_ZERO_MODE(_MM_FLUSH_ZERO_ON);
+        _MM_SET_DENORMALS_ZERO_MODE(_MM_DENORMALS_ZERO_ON);
+    }
+    _MM_SET_FLUSH_ZERO_MODE(_MM_FLUSH_ZERO_ON);
+    _MM_SET_DENORMALS_ZERO_MODE(_MM_DENORMALS_ZERO_ON);
+    done = 1;
+}
+#else
+static void or_fast_math_fp_env(void) {}
+#endif
+
 int ORACLE_FN(evolve_one_step)(oracle_domain *d, double dt, int has_dt)
 {
+    or_fast_math_fp_env();
     double time0 = d->time;
     d->boundary_flux_evolve_integral = 0.0;
     if (d->nsteps_advanced == 0) ORACLE_FN(update_max_quantities)(d);

@@ -620,6 +620,13 @@ __global__ void __launch_bounds__(128, LIN_MINB) linear_async_kernel(const LinAr
 #ifndef LIN_WIDE_MINB
 #define LIN_WIDE_MINB 4
 #endif
+#ifndef LIN_WIDE_AD
+// Ring slots per warp (LIN_WIDE_AD - 1 rows in flight).  Measured at
+// 4096^2 / 8192^2: 3 slots 0.86 / 0.95 of HBM in FP64 and 0.78 / 0.90 in
+// FP32 (batched 0.74), against 0.84 / 0.93, 0.73 / 0.87 (0.71) with 4; a
+// register cap for 3 CTAs per SM loses 6-9 %, for 5 or 6 CTAs about half.
+#define LIN_WIDE_AD 3
+#endif
 
 __device__ __forceinline__ void cp_async_vec(void *smem, const void *gmem, int bytes, int src_bytes)
 {
@@ -647,8 +654,8 @@ __device__ __forceinline__ void store_vec(R *p, const R (&v)[CPL])
 }
 
 template <typename R, int CPL> struct WideRing {
-    R v[AD][5][32 * CPL];   // [slot][UH, VH, STG, ELV, max_stage][column]
-    R h[AD][2][4];          // [slot][lane 0: UH west | lane 31: STG, UH, VH, ELV east][]
+    R v[LIN_WIDE_AD][5][32 * CPL];   // [slot][UH, VH, STG, ELV, max_stage][column]
+    R h[LIN_WIDE_AD][2][4];          // [slot][lane 0: UH west | lane 31: STG, UH, VH, ELV east][]
 };
 
 template <typename R, bool CORIOLIS, bool TRUELY_LINEAR, bool GAUGES, int CPL>
@@ -702,7 +709,7 @@ __global__ void __launch_bounds__(128, LIN_WIDE_MINB) linear_wide_kernel(const L
             if (k < nrow) {
                 const int q = ra - 1 + k;
                 const int qc = clampi(q, 0, ny - 1);
-                const int slot = k % AD;
+                const int slot = k % LIN_WIDE_AD;
                 const int64_t orow = (int64_t)qc * P;
                 const bool qv = (q >= 0 && q < ny);
                 cp_async_vec(&rg.v[slot][0][lane * CPL], uhp + orow + (src_bytes ? c0 : 0), VB, src_bytes);
@@ -749,16 +756,16 @@ __global__ void __launch_bounds__(128, LIN_WIDE_MINB) linear_wide_kernel(const L
         };
 
         __syncwarp();  // the previous segment's reads of the ring are done
-        for (int k = 0; k < AD - 1; k++) issue(k);
+        for (int k = 0; k < LIN_WIDE_AD - 1; k++) issue(k);
         // k = 0: row ra-1 (VH only)
-        cp_async_wait<AD - 2>();
+        cp_async_wait<LIN_WIDE_AD - 2>();
         R vh_jm1[CPL];
 #pragma unroll
         for (int c = 0; c < CPL; c++) vh_jm1[c] = rg.v[0][1][lane * CPL + c];
         R vhE_jm1 = __shfl_sync(FULL, lane == 31 ? rg.h[0][1][2] : R(0), 31);
-        issue(AD - 1);
+        issue(LIN_WIDE_AD - 1);
         // k = 1: row ra
-        cp_async_wait<AD - 2>();
+        cp_async_wait<LIN_WIDE_AD - 2>();
         R uh_j[CPL], vh_j[CPL], e_j[CPL], sn_j[CPL], mx[CPL];
         R st_j[CPL];
 #pragma unroll
@@ -774,7 +781,7 @@ __global__ void __launch_bounds__(128, LIN_WIDE_MINB) linear_wide_kernel(const L
         const R uhE_j0 = __shfl_sync(FULL, lane == 31 ? rg.h[1][1][1] : R(0), 31);
         R vhE_j = __shfl_sync(FULL, lane == 31 ? rg.h[1][1][2] : R(0), 31);
         R eE_j = __shfl_sync(FULL, lane == 31 ? rg.h[1][1][3] : R(0), 31);
-        issue(AD);
+        issue(LIN_WIDE_AD);
         R snE_j;
         {
             const R dta = a.dt / a.m.area[ra];
@@ -804,8 +811,8 @@ __global__ void __launch_bounds__(128, LIN_WIDE_MINB) linear_wide_kernel(const L
             const R inv_cell_area_dt_n = __shfl_sync(FULL, rc_s, rl);
             const R inv_cell_area_dt_g = __shfl_sync(FULL, rc_u, rl);
             const R inv_cell_area_dt_vh_g = __shfl_sync(FULL, rc_v, rl);
-            cp_async_wait<AD - 2>();
-            const int slot = k % AD;
+            cp_async_wait<LIN_WIDE_AD - 2>();
+            const int slot = k % LIN_WIDE_AD;
             R uh_n[CPL], vh_n[CPL], st_n[CPL], e_n[CPL], mx_n[CPL];
 #pragma unroll
             for (int c = 0; c < CPL; c++) {
@@ -820,7 +827,7 @@ __global__ void __launch_bounds__(128, LIN_WIDE_MINB) linear_wide_kernel(const L
             const R uhE_n = __shfl_sync(FULL, lane == 31 ? rg.h[slot][1][1] : R(0), 31);
             const R vhE_n = __shfl_sync(FULL, lane == 31 ? rg.h[slot][1][2] : R(0), 31);
             const R eE_n = __shfl_sync(FULL, lane == 31 ? rg.h[slot][1][3] : R(0), 31);
-            issue(k + AD - 1);
+            issue(k + LIN_WIDE_AD - 1);
 
             // New stage of row j+1: own columns and the east neighbour column.
             R uh_nw[CPL], sn_n[CPL];
