@@ -310,8 +310,8 @@ def run_ours(args, world, rank, local):
     stage2_share = per_step_ms["fv_stage2"] / step_ms if step_ms else None
     # FP64 work of the same launch: flops per cell from the committed ncu
     # count (dadd + dmul + 2 dfma thread instructions / cells).
-    fpc = profile_value("fp64_flops_per_cell[rk2_stream_kernel_stage2]") if not args.real32 else None
-    pipe = profile_value("fp64_pipe_active_frac[rk2_stream_kernel_stage2]") if not args.real32 else None
+    fpc = profile_value("fp64_flops_per_cell[rk2_stage2]") if not args.real32 else None
+    pipe = profile_value("fp64_pipe_active_frac[rk2_stage2]") if not args.real32 else None
     fp64 = None
     if fpc:
         sm_mhz = clocks.get("sm_mhz") or 1965.0
@@ -380,12 +380,12 @@ def run_ours(args, world, rank, local):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.real32 else "f64", "data": "synthetic",
             "config": cfg, "timesteps_per_step": INNER,
             "roofline": {"bound": "hbm",
-                         "kernel": f"rk2_stream_kernel stage 2 (dominant: {100 * stage2_share:.0f}% of the step)",
+                         "kernel": f"rk2 stage-2 kernel, rk2_srow_kernel (dominant: {100 * stage2_share:.0f}% of the step)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": peak_kind,
                          "bytes_per_cell": BYTES_STAGE2 * es_scale,
                          "algorithmic_bytes_per_launch": cells * BYTES_STAGE2 * es_scale,
-                         "traffic": (profile_traffic("rk2_stream_kernel_stage2") if N == 2048 and not args.real32
+                         "traffic": (profile_traffic("rk2_stage2") if N == 2048 and not args.real32
                                      else None),
                          "traffic_unit": "DRAM bytes of one stage-2 launch (ncu, 2048x2048 FP64)",
                          "fp64": fp64,

@@ -704,6 +704,13 @@ __global__ void __launch_bounds__(128, LIN_WIDE_MINB) linear_wide_kernel(const L
         const R dyl_e = a.m.dyl[iec];
         const unsigned long long gmask =
             GAUGES ? gauges_in(a.sites, a.n_sites, base, base + W - 1, ra, rb - 1) : 0ull;
+        // the gauges of the segment in this lane's own columns
+        unsigned long long lmask = 0ull;
+        if (GAUGES && gmask && a.n_sites <= 64)
+            for (unsigned long long m = gmask; m; m &= m - 1) {
+                const int q = __ffsll((long long)m) - 1;
+                if (a.sites[2 * q] >= c0 && a.sites[2 * q] < c0 + CPL) lmask |= 1ull << q;
+            }
         const int nrow = rb - ra + 2;   // rows ra-1 .. rb
         auto issue = [&](int k) {
             if (k < nrow) {
@@ -912,7 +919,7 @@ __global__ void __launch_bounds__(128, LIN_WIDE_MINB) linear_wide_kernel(const L
                         for (int q = 0; q < a.n_sites; q++)
                             if (a.sites[2 * q] == i && a.sites[2 * q + 1] == jrow) a.rec[q] = (double)snc;
                     } else {
-                        for (unsigned long long m = gmask; m; m &= m - 1) {
+                        for (unsigned long long m = lmask; m; m &= m - 1) {
                             const int q = __ffsll((long long)m) - 1;
                             if (a.sites[2 * q] == i && a.sites[2 * q + 1] == jrow) a.rec[q] = (double)snc;
                         }
@@ -1387,14 +1394,14 @@ constexpr int PLAIN_DEFAULT = WIDE16_CFG;
 
 // Rows per segment: the longest segment (up to 128 rows, which amortises the
 // two rows a segment reloads) that still gives every SM about 24 warps.
-inline int stream_rows(int nx, int ny, int nbatch, int strip_cols = SOUT)
+inline int stream_rows(int nx, int ny, int nbatch, int strip_cols = SOUT, int min_rows = 16)
 {
     // At least four waves of 20 warps per SM (so the last, partial wave is a
-    // small part of the launch), but no segment under 16 rows.
+    // small part of the launch), but no segment under min_rows rows.
     const int64_t nstrips = (nx + strip_cols - 1) / strip_cols;
     const int64_t want = 148 * 20 * 4;
     int sh = 128;
-    while (sh > 16 && (int64_t)nbatch * nstrips * ((ny + sh - 1) / sh) < want) sh /= 2;
+    while (sh > min_rows && (int64_t)nbatch * nstrips * ((ny + sh - 1) / sh) < want) sh /= 2;
     return sh;
 }
 
@@ -1440,7 +1447,8 @@ template <typename R, bool COR, bool TL, int CPL>
 void launch_wide(const LinArgs<R> &a, cudaStream_t s)
 {
     constexpr int W = 32 * CPL;
-    const int sh = stream_rows(a.p.nx, a.p.ny, a.nbatch, W);
+    // the wide strips are few on small grids: segments down to 8 rows
+    const int sh = stream_rows(a.p.nx, a.p.ny, a.nbatch, W, 8);
     const int nstrips = (a.p.nx + W - 1) / W;
     const int nseg = (a.p.ny + sh - 1) / sh;
     const int total = nstrips * nseg;
@@ -2030,10 +2038,11 @@ cudaError_t launch_linear_map(const StepPlanes<R> &p, const Metrics<R> &m, const
     a.rec = rec;
     hook(CAT_LINEAR_MAIN, 0);
     const bool cor = c.coriolis != 0, tl = c.truely_linear != 0;
-    if (cor && tl) launch_async<R, true, true>(a, 0, s);
-    else if (cor && !tl) launch_async<R, true, false>(a, 0, s);
-    else if (!cor && tl) launch_async<R, false, true>(a, 0, s);
-    else launch_async<R, false, false>(a, 0, s);
+    constexpr int CPL = 16 / (int)sizeof(R);   // the aligned wide strips of the plain step
+    if (cor && tl) launch_wide<R, true, true, CPL>(a, s);
+    else if (cor && !tl) launch_wide<R, true, false, CPL>(a, s);
+    else if (!cor && tl) launch_wide<R, false, true, CPL>(a, s);
+    else launch_wide<R, false, false, CPL>(a, s);
     hook(CAT_LINEAR_MAIN, 1);
     return cudaGetLastError();
 }

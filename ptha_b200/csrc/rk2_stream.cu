@@ -1,4 +1,6 @@
-// rk2_stream.cu -- finite-volume stage kernel, register-streaming form.
+// rk2_stream.cu -- finite-volume stage kernels, streaming forms: the
+// register form (rk2_stream_kernel, the flux pass of adaptive steps) and the
+// shared-memory-rows form (rk2_srow_kernel, the update stages), below.
 //
 // Same computation as the shared-memory tile kernel in rk2.cu (and the same
 // device functions: edge_flux, mc_gradient, theta_wd, fv_update), organised
@@ -18,6 +20,9 @@
 //     latency-bound, and 16 warps beat 12 unspilled ones (measured 12% faster
 //     on the 2048x2048 beach, a few spilled values included).
 #include "rk2_common.cuh"
+
+#include <cstdlib>
+#include <cstring>
 
 namespace swals {
 namespace {
@@ -42,7 +47,7 @@ constexpr int SWARPS = SWALS_STREAM_WARPS;   // warps per CTA
 // same grid looping over 12-row strips (15 % slower), the row constants
 // dt/area and 1/(dx cfl/2) evaluated once per 32 rows and shuffled (2 %
 // slower: the extra live registers spill), 3 CTAs per SM without spills
-// (18 % slower), and FMA contraction (2 % faster, but no longer bit-exact
+// (9 % slower than 4) or 5 CTAs (13 % slower), and FMA contraction (2 % faster, but no longer bit-exact
 // with the IEEE-strict oracle, and 2e-9 relative after 600 steps).
 #define SWALS_STREAM_ROWS 12
 #endif
@@ -260,6 +265,177 @@ __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_STREAM_MIN_CTAS) rk2_str
     }
 }
 
+// The same march with the rows it carries kept in shared memory instead of
+// registers: per warp a ring of the last three fixed-up rows, the
+// north-south gradients of two rows, the south edge of the row being
+// updated, and the east-west gradient and west edge of that row (read by
+// the neighbouring lanes, in place of shuffles).  Fewer registers per
+// thread, so more warps per SM hide the FP64 latency.  Lanes touch other
+// lanes' entries only after a __syncwarp.
+#ifndef SWALS_SROW_MIN_CTAS
+// Measured on the 2048^2 step: with 4 CTAs per SM (96 registers, no
+// spills) stage 2 takes 0.391 ms against the register form's 0.412, the
+// flux pass 0.280 against 0.275; with 5 CTAs (spills) 0.412 and 0.299.
+#define SWALS_SROW_MIN_CTAS 4
+#endif
+template <typename R>
+struct SRows {
+    Cell<R> c[3][32];     // rows r % 3
+    Grad<R> g[2][32];     // north-south gradients, rows r % 2
+    EdgeRes<R> es[32];    // south edge of the row being updated
+    Grad<R> gew[32];      // east-west gradient of the row being updated
+    EdgeRes<R> ew[32];    // its west edges
+};
+
+template <typename R, int MODE, bool SPH, bool COR, int FRIC, int SH, bool EDDY>
+__global__ void __launch_bounds__(SLANES *SWARPS, SWALS_SROW_MIN_CTAS) rk2_srow_kernel(const Rk2Args<R> a)
+{
+    extern __shared__ __align__(16) unsigned char srow_smem[];
+    const int lane = threadIdx.x & 31;
+    SRows<R> &sm = reinterpret_cast<SRows<R> *>(srow_smem)[threadIdx.x >> 5];
+    const int wid = blockIdx.x * SWARPS + (threadIdx.x >> 5);
+    const int nx = a.nx, ny = a.ny;
+    const int strips_x = (nx + SOUT - 1) / SOUT;
+    const int sx = wid % strips_x, sy = wid / strips_x;
+    const int ra = sy * SH;
+    if (ra >= ny) return;  // whole warp
+    const int rb = min(ra + SH, ny);
+    const int i = sx * SOUT - 2 + lane;
+    const bool col_valid = (i >= 0 && i < nx);
+    const bool out_lane = (lane >= 2 && lane <= 29 && i < nx);
+    const bool ew_lane = (lane >= 2 && lane <= 30);
+    const int lw = max(lane - 1, 0), le = min(lane + 1, 31);   // the shuffles' edge behaviour
+
+    R dt = R(0);
+    if (MODE == MODE_STAGE1 || MODE == MODE_STAGE2) dt = stage_dt<R>(a);
+    const R inv2 = R(1) / (a.m.dyl[0] * a.half_cfl);
+    double cfl = 0.0;
+    long long negfix = 0;
+
+    Raw<R> nxt = load_raw<R>(a, i, ra - 2);
+    for (int r = ra - 2, k = 0; r <= rb + 1; r++, k++) {
+        __syncwarp();   // every lane is done with the entries this iteration rewrites
+        const Raw<R> cur = nxt;
+        if (r + 1 <= rb + 1) nxt = load_raw<R>(a, i, r + 1);
+        if ((MODE == MODE_STAGE1 || MODE == MODE_STAGE2) && out_lane && r + 1 >= ra && r + 1 < rb) {
+            const int64_t o = (int64_t)(r + 1) * a.P + i;
+            if (FRIC != FRIC_NONE) prefetch_l2(a.nsq + o);
+            if (MODE == MODE_STAGE2) {
+                prefetch_l2(a.stg0 + o);
+                prefetch_l2(a.uh0 + o);
+                prefetch_l2(a.vh0 + o);
+                if (a.max_stage) prefetch_l2(a.max_stage + o);
+            }
+        }
+        const int s0 = (r + 3) % 3, s1 = (r + 2) % 3, s2 = (r + 1) % 3;   // rows r, r-1, r-2
+        const Cell<R> c0 = fix_up<R>(cur, col_valid && r >= 0 && r < ny, negfix,
+                                     (MODE == MODE_STAGE1 || MODE == MODE_STAGE2) && out_lane && r >= ra && r < rb);
+        sm.c[s0][lane] = c0;
+        if (k < 2) continue;
+
+        // North-south gradient of row r-1.
+        {
+            const int rg = r - 1;
+            Grad<R> g1;
+            if (col_valid && rg > 0 && rg < ny - 1) g1 = limited<R>(sm.c[s2][lane], sm.c[s1][lane], c0, a.theta);
+            else { g1.ds = R(0); g1.dd = R(0); g1.du = R(0); g1.dv = R(0); }
+            sm.g[(r + 1) & 1][lane] = g1;
+        }
+        if (k < 3) continue;
+
+        // North-south edge between rows r-2 and r-1.
+        EdgeRes<R> e_n;
+        zero_edge(e_n);
+        {
+            const int e = r - 1;
+            if (e >= 1 && e <= ny - 1 && i >= 1 && i <= nx - 1) {
+                double cand;
+                edge_flux<R, true, EDDY>(sm.c[s2][lane], sm.g[r & 1][lane], sm.c[s1][lane], sm.g[(r + 1) & 1][lane],
+                                         a.m.dxb[e], inv2, e_n, cand, a.flux_variant,
+                                         EDDY ? a.ev[(int64_t)(e - 1) * a.P + i] : R(0),
+                                         EDDY ? a.ev[(int64_t)e * a.P + i] : R(0), EDDY ? a.m.dyl[i] : R(1));
+                cfl = fmax(cfl, cand);
+                if (MODE != MODE_CFL && a.lines && i >= a.n_ext && i <= nx - a.n_ext - 1) {
+                    if (e == ny - a.n_ext) a.lines[i] = (double)e_n.f[0];
+                    if (e == a.n_ext) a.lines[nx + ny + i] = (double)e_n.f[0];
+                }
+            }
+        }
+        if (MODE == MODE_FLUX && out_lane && r - 1 >= ra && r - 1 < rb) {
+            const int64_t o = (int64_t)(r - 1) * a.P + i;
+            a.ep.sf[0][o] = e_n.f[0]; a.ep.sf[1][o] = e_n.f[1]; a.ep.sf[2][o] = e_n.f[2];
+            a.ep.s_pos[o] = e_n.es_pos; a.ep.s_neg[o] = e_n.es_neg;
+        }
+        if (k < 4) { sm.es[lane] = e_n; continue; }
+
+        // Row R = r-2: east-west gradient and west edge, then the update.
+        const int R_ = r - 2;
+        {
+            Grad<R> gew;
+            if (col_valid && i > 0 && i < nx - 1) gew = limited<R>(sm.c[s2][lw], sm.c[s2][lane], sm.c[s2][le], a.theta);
+            else { gew.ds = R(0); gew.dd = R(0); gew.du = R(0); gew.dv = R(0); }
+            sm.gew[lane] = gew;
+        }
+        __syncwarp();
+        EdgeRes<R> e_w;
+        zero_edge(e_w);
+        if (ew_lane && i >= 1 && i <= nx - 1 && R_ >= 1 && R_ <= ny - 1) {
+            const R inv1 = R(1) / (a.m.dxb[R_] * a.half_cfl);
+            double cand;
+            const int64_t oe = (int64_t)R_ * a.P + i;
+            edge_flux<R, false, EDDY>(sm.c[s2][lw], sm.gew[lw], sm.c[s2][lane], sm.gew[lane], a.m.dyl[i], inv1, e_w,
+                                      cand, a.flux_variant, EDDY ? a.ev[oe - 1] : R(0), EDDY ? a.ev[oe] : R(0),
+                                      EDDY ? R(0.5) * (a.m.dxb[R_] + a.m.dxb[R_ + 1]) : R(1));
+            cfl = fmax(cfl, cand);
+            if (MODE != MODE_CFL && a.lines && R_ >= a.n_ext && R_ <= ny - a.n_ext - 1) {
+                if (i == nx - a.n_ext) a.lines[nx + R_] = (double)e_w.f[0];
+                if (i == a.n_ext) a.lines[2 * nx + ny + R_] = (double)e_w.f[0];
+            }
+        }
+        if (MODE == MODE_FLUX && out_lane) {
+            const int64_t o = (int64_t)R_ * a.P + i;
+            a.ep.wf[0][o] = e_w.f[0]; a.ep.wf[1][o] = e_w.f[1]; a.ep.wf[2][o] = e_w.f[2];
+            a.ep.w_pos[o] = e_w.es_pos; a.ep.w_neg[o] = e_w.es_neg;
+        }
+        if (MODE == MODE_STAGE1 || MODE == MODE_STAGE2) {
+            sm.ew[lane] = e_w;
+            __syncwarp();
+            EdgeRes<R> e_e;
+            const EdgeRes<R> &en = sm.ew[le];
+            e_e.f[0] = en.f[0]; e_e.f[1] = en.f[1]; e_e.f[2] = en.f[2];
+            e_e.es_neg = en.es_neg;
+            e_e.es_pos = 0.0;
+            if (out_lane)
+                fv_update<R, MODE, SPH, COR, FRIC>(a, i, R_, sm.c[s2][lane], sm.es[lane], e_n, e_w, e_e, dt,
+                                                   dt / a.m.area[R_]);
+        }
+        sm.es[lane] = e_n;
+    }
+
+    if (a.write_cfl || MODE == MODE_CFL || MODE == MODE_FLUX) {
+        for (int o = 16; o > 0; o >>= 1) cfl = fmax(cfl, __shfl_down_sync(FULL, cfl, o));
+        if (lane == 0 && cfl > 0.0) atomicMax(&a.sc->max_dt_inv_bits, (unsigned long long)__double_as_longlong(cfl));
+    }
+    if (MODE == MODE_STAGE1 || MODE == MODE_STAGE2) {
+        for (int o = 16; o > 0; o >>= 1) negfix += __shfl_down_sync(FULL, negfix, o);
+        if (lane == 0 && negfix) atomicAdd((unsigned long long *)&a.sc->negative_depth_fix_counter,
+                                           (unsigned long long)negfix);
+    }
+}
+
+// The shared-memory-rows form for the update stages and the register form
+// for the flux pass (the faster of the two for each), unless
+// SWALS_FV_STREAM=stream or =srow picks one form for all.
+bool use_srow_kernel(int mode)
+{
+    static int v = -1;
+    if (v < 0) {
+        const char *e = getenv("SWALS_FV_STREAM");
+        v = (e && strcmp(e, "stream") == 0) ? 0 : (e && strcmp(e, "srow") == 0) ? 1 : 2;
+    }
+    return v == 1 || (v == 2 && (mode == MODE_STAGE1 || mode == MODE_STAGE2));
+}
+
 }  // namespace
 
 template <typename R, int MODE, bool SPH, bool COR, int FRIC>
@@ -270,6 +446,17 @@ cudaError_t launch_stage_stream(const Rk2Args<R> &a, cudaStream_t s)
     const int strips_y = (a.ny + SH - 1) / SH;
     const int warps = strips_x * strips_y;
     const int blocks = (warps + SWARPS - 1) / SWARPS;
+    if (use_srow_kernel(MODE)) {
+        const size_t smem = sizeof(SRows<R>) * SWARPS;   // 37.9 KB (FP64): under the 48 KB default
+        auto go = [&](auto kernel) -> cudaError_t {
+            kernel<<<blocks, SLANES * SWARPS, smem, s>>>(a);
+            return cudaGetLastError();
+        };
+        if constexpr (MODE != MODE_CFL) {
+            if (a.flux_variant & FLUX_EDDY) return go(rk2_srow_kernel<R, MODE, SPH, COR, FRIC, SH, true>);
+        }
+        return go(rk2_srow_kernel<R, MODE, SPH, COR, FRIC, SH, false>);
+    }
     if constexpr (MODE != MODE_CFL) {
         if (a.flux_variant & FLUX_EDDY) {
             rk2_stream_kernel<R, MODE, SPH, COR, FRIC, SH, true><<<blocks, SLANES * SWARPS, 0, s>>>(a);
