@@ -467,7 +467,7 @@ int adjoint_sweep(swals_domain *d, int nsteps, double dt, const double *gadj_hos
 // new stage at the gauges into rec.
 template <typename R>
 cudaError_t map_step(swals_domain *d, R *const in[3], R *const out[3], double dt, const int *sites, int ng,
-                     double *rec)
+                     double *rec, cudaStream_t stream = nullptr)
 {
     swals::StepPlanes<R> p;
     p.nx = d->nx; p.ny = d->ny; p.pitch = d->pitch;
@@ -476,8 +476,8 @@ cudaError_t map_step(swals_domain *d, R *const in[3], R *const out[3], double dt
     p.elv = (R *)d->elv;
     p.max_stage = nullptr;
     p.manning_sq = nullptr;
-    return swals::launch_linear_map<R>(p, swals::metrics_of<R>(d), d->cfg, R(dt), sites, ng, rec, d->stream,
-                                       swals::hook_of(d));
+    return swals::launch_linear_map<R>(p, swals::metrics_of<R>(d), d->cfg, R(dt), sites, ng, rec,
+                                       stream ? stream : d->stream, swals::hook_of(d));
 }
 
 // Residuals of `count` recorded steps against the target, and each step's
@@ -511,7 +511,11 @@ __global__ void loss_sum_kernel(const double *step_half, int n, double *loss)
 // recomputed from its checkpoint, recording the gauge stage, the segment's
 // residuals are formed, and the adjoint runs back through the segment with
 // the residuals injected as it goes.  Per timestep that is one forward map,
-// one recomputed forward map and one adjoint launch.
+// one recomputed forward map and one adjoint launch.  The recomputation of
+// segment s-1 does not depend on the adjoint through segment s, so it runs
+// on the domain's side stream, into a second buffer set, while the adjoint
+// runs on the main stream: the two grids are smaller than one wave of the
+// GPU each and fill it together.
 template <typename R>
 int misfit_gradient(swals_domain *d, int nsteps, double dt, const double *target_host, int K, double *loss_out,
                     void *grad_host)
@@ -521,57 +525,67 @@ int misfit_gradient(swals_domain *d, int nsteps, double dt, const double *target
     const int64_t plane = d->pitch * (int64_t)d->ny;
     const size_t es = sizeof(R);
     const int nseg = (nsteps + K - 1) / K;
-    size_t need = (size_t)(6 + 6 + 3 * nseg) * plane * es;          // lambda x2, state x2, checkpoints
-    need += sizeof(double) * ((size_t)nsteps * ng + 2 * (size_t)K * ng + (size_t)nsteps + 8);
+    size_t need = (size_t)(6 + 12 + 3 * nseg) * plane * es;          // lambda x2, state x2 x2 sets, checkpoints
+    need += sizeof(double) * ((size_t)nsteps * ng + 4 * (size_t)K * ng + (size_t)nsteps + 8);
     need += sizeof(int) * 2 * (size_t)ng + 1024;
     void *buf = nullptr;
     cudaError_t e = workspace(d, need, &buf);
     if (e != cudaSuccess) return swals::api_cuda_fail(e, "misfit-gradient workspace");
     char *p = (char *)buf;
-    R *lam[2][3], *x[2][3];
+    R *lam[2][3], *xs[2][2][3];   // xs[set][ping-pong][variable]
     for (int b = 0; b < 2; b++)
         for (int v = 0; v < 3; v++) { lam[b][v] = (R *)p; p += plane * es; }
-    for (int b = 0; b < 2; b++)
-        for (int v = 0; v < 3; v++) { x[b][v] = (R *)p; p += plane * es; }
+    for (int q = 0; q < 2; q++)
+        for (int b = 0; b < 2; b++)
+            for (int v = 0; v < 3; v++) { xs[q][b][v] = (R *)p; p += plane * es; }
     R *ckpt = (R *)p; p += (size_t)3 * nseg * plane * es;
     double *d_target = (double *)p; p += sizeof(double) * (size_t)nsteps * ng;
-    double *d_rec = (double *)p; p += sizeof(double) * (size_t)K * ng;
-    double *d_resid = (double *)p; p += sizeof(double) * (size_t)K * ng;
+    double *d_rec[2], *d_resid[2];
+    for (int q = 0; q < 2; q++) { d_rec[q] = (double *)p; p += sizeof(double) * (size_t)K * ng; }
+    for (int q = 0; q < 2; q++) { d_resid[q] = (double *)p; p += sizeof(double) * (size_t)K * ng; }
     double *d_half = (double *)p; p += sizeof(double) * (size_t)nsteps;
     double *d_loss = (double *)p; p += sizeof(double) * 8;
     int *d_sites = (int *)p;
 
     int rc = SWALS_OK;
     auto ck = [&](cudaError_t err, const char *w) { if (err != cudaSuccess && rc == SWALS_OK) rc = swals::api_cuda_fail(err, w); };
+    // The side stream of the domain (created here on first use).
+    const bool overlap = !d->timers_on;
+    if (overlap && !d->aux.stream) {
+        ck(cudaStreamCreateWithFlags(&d->aux.stream, cudaStreamNonBlocking), "side stream");
+        ck(cudaEventCreateWithFlags(&d->aux.fork, cudaEventDisableTiming), "event");
+        ck(cudaEventCreateWithFlags(&d->aux.join, cudaEventDisableTiming), "event");
+    }
     ck(cudaMemsetAsync(lam[0][0], 0, 3 * plane * es, d->stream), "memset");
     ck(cudaMemcpyAsync(d_target, target_host, sizeof(double) * (size_t)nsteps * ng, cudaMemcpyHostToDevice, d->stream),
        "target upload");
     ck(cudaMemcpyAsync(d_sites, d->h_sites.data(), sizeof(int) * 2 * ng, cudaMemcpyHostToDevice, d->stream), "sites");
     for (int v = 0; v < 3; v++)
-        ck(cudaMemcpyAsync(x[0][v], d->planes[d->cur][v], plane * es, cudaMemcpyDeviceToDevice, d->stream), "x0");
+        ck(cudaMemcpyAsync(xs[0][0][v], d->planes[d->cur][v], plane * es, cudaMemcpyDeviceToDevice, d->stream), "x0");
 
-    // The three per-segment step sequences.  For an even K a full segment
-    // leaves the buffer parity unchanged, so each sequence is captured once
-    // as a CUDA graph and replayed for every full segment.
-    auto fwd_seq = [&](int count) {   // x[0] -> x[0] after an even count
+    // The per-segment step sequences.  For an even K a full segment leaves
+    // the buffer parity unchanged, so each sequence is captured once as a
+    // CUDA graph and replayed for every full segment.
+    auto fwd_seq = [&](int count) {   // xs[0][0] -> xs[0][0] after an even count
         int c = 0;
         for (int n = 0; n < count; n++) {
-            ck(map_step<R>(d, x[c], x[1 - c], dt, nullptr, 0, nullptr), "forward");
+            ck(map_step<R>(d, xs[0][c], xs[0][1 - c], dt, nullptr, 0, nullptr), "forward");
             c = 1 - c;
         }
         return c;
     };
-    auto rec_seq = [&](int count) {   // recompute, recording the gauge stage
+    auto rec_seq = [&](int count, int set, cudaStream_t st) {   // recompute, recording the gauge stage
         int c = 0;
         for (int n = 0; n < count; n++) {
-            ck(map_step<R>(d, x[c], x[1 - c], dt, d_sites, ng, d_rec + (size_t)n * ng), "recompute");
+            ck(map_step<R>(d, xs[set][c], xs[set][1 - c], dt, d_sites, ng, d_rec[set] + (size_t)n * ng, st),
+               "recompute");
             c = 1 - c;
         }
         return c;
     };
-    auto adj_seq = [&](int count, int lc) {   // adjoint back through `count` steps
+    auto adj_seq = [&](int count, int lc, int set) {   // adjoint back through `count` steps
         for (int t = count; t > 0; t--) {
-            ck(adjoint_step<R>(d, lam[lc], lam[1 - lc], dt, d_sites, ng, d_resid + (size_t)(t - 1) * ng),
+            ck(adjoint_step<R>(d, lam[lc], lam[1 - lc], dt, d_sites, ng, d_resid[set] + (size_t)(t - 1) * ng),
                "adjoint");
             lc = 1 - lc;
         }
@@ -583,11 +597,11 @@ int misfit_gradient(swals_domain *d, int nsteps, double dt, const double *target
             if (g) { cudaGraphExecDestroy(g); g = nullptr; }
         d->adj_K = 0;
         const int64_t l0 = d->launches;
-        for (int q = 0; q < 4 && rc == SWALS_OK; q++) {
+        for (int q = 0; q < 7 && rc == SWALS_OK; q++) {
             ck(cudaStreamBeginCapture(d->stream, cudaStreamCaptureModeThreadLocal), "capture");
             if (q == 0) fwd_seq(K);
-            else if (q == 1) rec_seq(K);
-            else adj_seq(K, q - 2);
+            else if ((q - 1) % 3 == 0) rec_seq(K, (q - 1) / 3, d->stream);
+            else adj_seq(K, (q - 2) % 3, (q - 2) / 3);
             cudaGraph_t gr = nullptr;
             ck(cudaStreamEndCapture(d->stream, &gr), "end capture");
             if (gr) {
@@ -599,13 +613,13 @@ int misfit_gradient(swals_domain *d, int nsteps, double dt, const double *target
         if (rc == SWALS_OK) { d->adj_K = K; d->adj_ng = ng; d->adj_dt = dt; d->adj_ws = d->ws; }
     }
 
-    // Forward sweep with checkpoints (every segment starts in x[0]).
+    // Forward sweep with checkpoints (every segment starts in xs[0][0]).
     int cur = 0;
     for (int sgm = 0; sgm < nseg && rc == SWALS_OK; sgm++) {
         const int n0 = sgm * K, cnt = (n0 + K < nsteps) ? K : nsteps - n0;
         for (int v = 0; v < 3; v++)
-            ck(cudaMemcpyAsync(ckpt + ((size_t)sgm * 3 + v) * plane, x[cur][v], plane * es, cudaMemcpyDeviceToDevice,
-                               d->stream), "checkpoint");
+            ck(cudaMemcpyAsync(ckpt + ((size_t)sgm * 3 + v) * plane, xs[0][cur][v], plane * es,
+                               cudaMemcpyDeviceToDevice, d->stream), "checkpoint");
         if (graphs && cnt == K && cur == 0) {
             ck(cudaGraphLaunch(d->adj_graph[0], d->stream), "forward graph");
             d->launches += K;
@@ -613,34 +627,55 @@ int misfit_gradient(swals_domain *d, int nsteps, double dt, const double *target
             // A last, shorter segment (no state is needed after it).
             int c = cur;
             for (int n = 0; n < cnt; n++) {
-                ck(map_step<R>(d, x[c], x[1 - c], dt, nullptr, 0, nullptr), "forward");
+                ck(map_step<R>(d, xs[0][c], xs[0][1 - c], dt, nullptr, 0, nullptr), "forward");
                 c = 1 - c;
             }
             cur = c;
         }
     }
-    // Backward, segment by segment from the last.
-    int lc = 0;
-    for (int sgm = nseg - 1; sgm >= 0 && rc == SWALS_OK; sgm--) {
+    // Recompute segment sgm into buffer set `set` on stream st, then its residuals.
+    auto recompute = [&](int sgm, int set, cudaStream_t st) {
         const int n0 = sgm * K, n1 = (n0 + K < nsteps) ? n0 + K : nsteps;
         const int cnt = n1 - n0;
         for (int v = 0; v < 3; v++)
-            ck(cudaMemcpyAsync(x[0][v], ckpt + ((size_t)sgm * 3 + v) * plane, plane * es, cudaMemcpyDeviceToDevice,
-                               d->stream), "restore");
+            ck(cudaMemcpyAsync(xs[set][0][v], ckpt + ((size_t)sgm * 3 + v) * plane, plane * es,
+                               cudaMemcpyDeviceToDevice, st), "restore");
         if (graphs && cnt == K) {
-            ck(cudaGraphLaunch(d->adj_graph[1], d->stream), "recompute graph");
+            ck(cudaGraphLaunch(d->adj_graph[1 + 3 * set], st), "recompute graph");
             d->launches += K;
         } else {
-            rec_seq(cnt);
+            rec_seq(cnt, set, st);
         }
-        segment_residual_kernel<<<1, 128, 0, d->stream>>>(d_rec, d_target + (size_t)n0 * ng, cnt, ng, d_resid,
-                                                          d_half + n0);
+        segment_residual_kernel<<<1, 128, 0, st>>>(d_rec[set], d_target + (size_t)n0 * ng, cnt, ng, d_resid[set],
+                                                   d_half + n0);
+        ck(cudaGetLastError(), "residuals");
+    };
+    // Backward, segment by segment from the last; segment sgm's buffers are
+    // set sgm & 1, and the recomputation of sgm-1 overlaps the adjoint of sgm.
+    recompute(nseg - 1, (nseg - 1) & 1, d->stream);
+    int lc = 0;
+    for (int sgm = nseg - 1; sgm >= 0 && rc == SWALS_OK; sgm--) {
+        const int set = sgm & 1;
+        const int n0 = sgm * K, n1 = (n0 + K < nsteps) ? n0 + K : nsteps;
+        const int cnt = n1 - n0;
+        if (sgm > 0) {
+            // the side stream may reuse set 1-set once the adjoint of sgm+1
+            // (issued before this point on the main stream) is done with it
+            cudaStream_t st = overlap ? d->aux.stream : d->stream;
+            if (overlap) {
+                ck(cudaEventRecord(d->aux.fork, d->stream), "fork");
+                ck(cudaStreamWaitEvent(st, d->aux.fork, 0), "fork wait");
+            }
+            recompute(sgm - 1, 1 - set, st);
+            if (overlap) ck(cudaEventRecord(d->aux.join, st), "join");
+        }
         if (graphs && cnt == K) {
-            ck(cudaGraphLaunch(d->adj_graph[2 + lc], d->stream), "adjoint graph");
+            ck(cudaGraphLaunch(d->adj_graph[2 + 3 * set + lc], d->stream), "adjoint graph");
             d->launches += K;
         } else {
-            lc = adj_seq(cnt, lc);
+            lc = adj_seq(cnt, lc, set);
         }
+        if (sgm > 0 && overlap) ck(cudaStreamWaitEvent(d->stream, d->aux.join, 0), "join wait");
     }
     loss_sum_kernel<<<1, 32, 0, d->stream>>>(d_half, nsteps, d_loss);
     double loss = 0.0;

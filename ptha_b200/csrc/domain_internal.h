@@ -78,7 +78,9 @@ struct swals_domain {
     int64_t graph_launches = 0;
     // misfit_gradient's replayed graphs (segments of K steps), valid for
     // (adj_K, adj_ng, adj_dt, ws).
-    cudaGraphExec_t adj_graph[4] = {};   // forward, recompute, adjoint from lambda 0, from lambda 1
+    // [0] forward; [1 + 3 set] recompute into buffer set `set`;
+    // [2 + 3 set + lc] adjoint from lambda buffer lc with set's residuals
+    cudaGraphExec_t adj_graph[7] = {};
     int adj_K = 0, adj_ng = 0;
     double adj_dt = 0.0;
     void *adj_ws = nullptr;
