@@ -525,10 +525,10 @@ __device__ __forceinline__ fv::Grad<R> fv_grad(const fv::Cell<R> &lo, const fv::
 {
     fv::Grad<R> g;
     const R th = fv::theta_wd<R>(lo.dep, c.dep, up.dep, theta);
-    g.ds = fv::mc_gradient<R>(c.stg, lo.stg, up.stg, th);
-    g.dd = fv::mc_gradient<R>(c.dep, lo.dep, up.dep, th);
-    g.du = fv::mc_gradient<R>(c.u, lo.u, up.u, th);
-    g.dv = fv::mc_gradient<R>(c.v, lo.v, up.v, th);
+    g.ds = fv::mc_half_gradient<R>(c.stg, lo.stg, up.stg, th);
+    g.dd = fv::mc_half_gradient<R>(c.dep, lo.dep, up.dep, th);
+    g.du = fv::mc_half_gradient<R>(c.u, lo.u, up.u, th);
+    g.dv = fv::mc_half_gradient<R>(c.v, lo.v, up.v, th);
     return g;
 }
 

@@ -142,10 +142,10 @@ __global__ void __launch_bounds__(NT, 3) rk2_stage_kernel(const Rk2Args<R> a)
         if (r > 0 && r < ny - 1 && i < nx) {
             const Cell<R> lo = S.cell.get(rr, cc + 2), c = S.cell.get(rr + 1, cc + 2), up = S.cell.get(rr + 2, cc + 2);
             const R th = theta_wd<R>(lo.dep, c.dep, up.dep, a.theta);
-            g.ds = mc_gradient<R>(c.stg, lo.stg, up.stg, th);
-            g.dd = mc_gradient<R>(c.dep, lo.dep, up.dep, th);
-            g.du = mc_gradient<R>(c.u, lo.u, up.u, th);
-            g.dv = mc_gradient<R>(c.v, lo.v, up.v, th);
+            g.ds = mc_half_gradient<R>(c.stg, lo.stg, up.stg, th);
+            g.dd = mc_half_gradient<R>(c.dep, lo.dep, up.dep, th);
+            g.du = mc_half_gradient<R>(c.u, lo.u, up.u, th);
+            g.dv = mc_half_gradient<R>(c.v, lo.v, up.v, th);
         }
         S.gns.set(rr, cc, g);
     }
@@ -156,10 +156,10 @@ __global__ void __launch_bounds__(NT, 3) rk2_stage_kernel(const Rk2Args<R> a)
         if (i > 0 && i < nx - 1 && r < ny) {
             const Cell<R> lo = S.cell.get(rr + 2, cc), c = S.cell.get(rr + 2, cc + 1), up = S.cell.get(rr + 2, cc + 2);
             const R th = theta_wd<R>(lo.dep, c.dep, up.dep, a.theta);
-            g.ds = mc_gradient<R>(c.stg, lo.stg, up.stg, th);
-            g.dd = mc_gradient<R>(c.dep, lo.dep, up.dep, th);
-            g.du = mc_gradient<R>(c.u, lo.u, up.u, th);
-            g.dv = mc_gradient<R>(c.v, lo.v, up.v, th);
+            g.ds = mc_half_gradient<R>(c.stg, lo.stg, up.stg, th);
+            g.dd = mc_half_gradient<R>(c.dep, lo.dep, up.dep, th);
+            g.du = mc_half_gradient<R>(c.u, lo.u, up.u, th);
+            g.dv = mc_half_gradient<R>(c.v, lo.v, up.v, th);
         }
         S.gew.set(rr, cc, g);
     }

@@ -61,9 +61,13 @@ __device__ __forceinline__ void atomic_max_pos_double(unsigned long long *addr, 
     atomicMax(addr, (unsigned long long)__double_as_longlong(v));
 }
 
-// MC limiter, extrapolation_limiting_mod.f90:63-79 (sign(1,a) == copysign).
+// MC limiter, extrapolation_limiting_mod.f90:63-79 (sign(1,a) == copysign),
+// returning HALF the limited gradient: the reconstruction's 1/2 (U -+ 1/2
+// grad at the two edges) is applied here, once per gradient, instead of in
+// each of the two edges that use it (the same product, so the same bits).
+// (A branch form without the sign products measured 3 % slower.)
 template <typename R>
-__device__ __forceinline__ R mc_gradient(R local, R lower, R upper, R th)
+__device__ __forceinline__ R mc_half_gradient(R local, R lower, R upper, R th)
 {
     const R a = upper - local;
     const R b = local - lower;
@@ -73,7 +77,7 @@ __device__ __forceinline__ R mc_gradient(R local, R lower, R upper, R th)
     const R d = rmin(R(fabs(a)), R(fabs(b))) * half_sasb * th;
     const R e = R(0.5) * (a + b);
     const R c = (d == R(0)) ? R(0) : e;
-    return (d > R(0)) ? rmin(c, d) : rmax(c, d);
+    return R(0.5) * ((d > R(0)) ? rmin(c, d) : rmax(c, d));
 }
 
 // theta_wd of DE1_inner_include.f90:751-757 / :813-819.
@@ -87,6 +91,7 @@ __device__ __forceinline__ R theta_wd(R d0, R d1, R d2, R theta)
     return rmax(theta * rmin(R(1), theta_local), R(0));
 }
 
+// Half the limited gradients of stage, depth, u, v (mc_half_gradient).
 template <typename R> struct Grad { R ds, dd, du, dv; };
 
 template <typename R>
@@ -123,17 +128,20 @@ __device__ __forceinline__ void edge_flux(const Cell<R> &cn, const Grad<R> &gn, 
     const R half = R(0.5);
     const double half_gravity = (double)(half * K<R>::gravity());
     const R EPS = R(1.0e-12);
-    const R EPS_gs = R(sqrt(K<R>::gravity() * K<R>::min_depth()));
+    // sqrt(gravity * minimum_allowed_depth) in the state precision (the
+    // correctly rounded root of the rounded product, as written out here)
+    const R EPS_gs = sizeof(R) == 8 ? R(0x1.4462fb7ff5035p-7) : R(0x1.4462fcp-7f);
     const R beta = R(1.0);
 
-    R stage_neg = cn.stg + half * gn.ds;
-    R stage_pos = cp.stg - half * gp.ds;
-    double depth_neg = (double)(cn.dep + half * gn.dd);
-    double depth_pos = (double)(cp.dep - half * gp.dd);
-    R u_neg = cn.u + half * gn.du;
-    R u_pos = cp.u - half * gp.du;
-    R v_neg = cn.v + half * gn.dv;
-    R v_pos = cp.v - half * gp.dv;
+    // (gn, gp hold half gradients: DE1_inner_include.f90's U +- 1/2 grad)
+    R stage_neg = cn.stg + gn.ds;
+    R stage_pos = cp.stg - gp.ds;
+    double depth_neg = (double)(cn.dep + gn.dd);
+    double depth_pos = (double)(cp.dep - gp.dd);
+    R u_neg = cn.u + gn.du;
+    R u_pos = cp.u - gp.du;
+    R v_neg = cn.v + gn.dv;
+    R v_pos = cp.v - gp.dv;
     double depth_neg_c = (double)cn.dep;
     double depth_pos_c = (double)cp.dep;
 

@@ -3,7 +3,7 @@
 // shared-memory-rows form (rk2_srow_kernel, the update stages), below.
 //
 // Same computation as the shared-memory tile kernel in rk2.cu (and the same
-// device functions: edge_flux, mc_gradient, theta_wd, fv_update), organised
+// device functions: edge_flux, mc_half_gradient, theta_wd, fv_update), organised
 // for sm_100a's FP64 pipes instead of for shared memory:
 //   - each warp owns a strip of 28 columns (lanes 2..29; lanes 0,1,30,31
 //     carry the 2-cell x-halo) and marches down SH rows plus a 2-row halo at
@@ -114,10 +114,10 @@ __device__ __forceinline__ Grad<R> limited(const Cell<R> &lo, const Cell<R> &c, 
 {
     Grad<R> g;
     const R th = theta_wd<R>(lo.dep, c.dep, up.dep, theta);
-    g.ds = mc_gradient<R>(c.stg, lo.stg, up.stg, th);
-    g.dd = mc_gradient<R>(c.dep, lo.dep, up.dep, th);
-    g.du = mc_gradient<R>(c.u, lo.u, up.u, th);
-    g.dv = mc_gradient<R>(c.v, lo.v, up.v, th);
+    g.ds = mc_half_gradient<R>(c.stg, lo.stg, up.stg, th);
+    g.dd = mc_half_gradient<R>(c.dep, lo.dep, up.dep, th);
+    g.du = mc_half_gradient<R>(c.u, lo.u, up.u, th);
+    g.dv = mc_half_gradient<R>(c.v, lo.v, up.v, th);
     return g;
 }
 

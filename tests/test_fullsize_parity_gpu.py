@@ -175,10 +175,16 @@ def test_batched_3600x2400_fp32_instances():
 
 
 def _nest(nts, kws):
+    """The nest with its initial states set (the timestep limits depend on
+    the elevation)."""
     from ptha_b200 import Multidomain
     specs, coasts = workloads.nested_specs(nts)
     md = Multidomain(specs, domain_kwargs=kws, use_wetdry_limiting=True, flux_correction=True,
                      periodic_xs=(0.0, 360.0))
+    for k, (s, d) in enumerate(zip(specs, md.domains)):
+        d.set_U(workloads.nested_initial_state(s, k, coasts))
+        if s.timestepping_method == "rk2":
+            d.set_manning_squared(0.025 ** 2)
     return specs, coasts, md
 
 
@@ -199,13 +205,11 @@ def test_nested_four_domain_fp64_two_md_steps():
                             refinement=nts, priority_index=[s.priority_domain_index for s in specs],
                             use_wetdry_limiting=True, flux_correction=True)
     for k, (s, d, od) in enumerate(zip(specs, md.domains, odoms)):
-        U = workloads.nested_initial_state(s, k, coasts)
-        d.set_U(U)
-        od.U[:] = U
+        od.U[:] = d.get_U()
         if s.timestepping_method == "rk2":
-            d.set_manning_squared(0.025 ** 2)
             od.manning_squared[:] = 0.025 ** 2
     print("nest nts", nts, "dt", dt, "exchanges", len(md.exchanges))
+    assert 5.0 < dt < 60.0 and nts[1:] == [3, 9, 8], (dt, nts)
     for step in range(2):
         md.evolve_one_step(dt)
         omd.evolve_one_step(dt)
@@ -213,6 +217,9 @@ def test_nested_four_domain_fp64_two_md_steps():
             np.testing.assert_array_equal(d.get_U(), od.U, err_msg=f"domain {k} md step {step}")
         for q in range(len(md.exchanges)):
             np.testing.assert_array_equal(md.flux(q, "error"), omd.recv[q].recv_error, err_msg=f"exchange {q}")
+    for d in md.domains:
+        U = d.get_U()
+        assert np.all(np.isfinite(U)) and np.max(np.abs(U[0][U[3] < 0])) < 10.0
     md.close()
 
 
