@@ -221,17 +221,32 @@ __global__ void __launch_bounds__(128) linear_adjoint_stream_kernel(const AdjArg
             }
             return v;
         };
+        // Row constants g dt/area(r), g dt/mean area(r, r+1) and dt/area(r),
+        // the same in every lane: lane L evaluates them for row base + L of
+        // a 32-row chunk, and the rows take them by shuffle (the same
+        // divisions, once per row instead of once per cell).
+        int base = ra - 1;
+        R f_gu = zero, f_gv = zero, f_c = zero;
+        auto chunk = [&](int b) {
+            base = b;
+            const int rr = min(max(b + lane, 0), ny - 1);
+            const int rn = min(rr + 1, ny - 1);
+            f_gu = g * a.dt / a.m.area[rr];
+            f_gv = g * a.dt / (half * (a.m.area[rr] + a.m.area[rn]));
+            f_c = a.dt / a.m.area[rr];
+        };
+        chunk(ra - 1);
         // Face coefficients of row r from its ELV and the ELV of row r+1 (zero outside IM).
         auto coef = [&](int r, R e0, R e_e, R e_n) -> ACoef<R> {
             ACoef<R> c;
             c.aU = c.aV = c.cU = c.cV = zero;
+            const R gU = __shfl_sync(FULL, f_gu, r - base);
+            const R gV = __shfl_sync(FULL, f_gv, r - base);
             if (in_x && r >= 0 && r < ny && in_im(i, r, a.xl, a.xu, a.yl, a.yu)) {
                 const bool wi = (e0 < -mad + a.msl) && (e_e < -mad + a.msl);
                 const R hU = wi ? (a.msl - half * (e_e + e0)) : zero;
                 const bool wj = (e_n < -mad + a.msl) && (e0 < -mad + a.msl);
                 const R hV = wj ? (a.msl - half * (e_n + e0)) : zero;
-                const R gU = g * a.dt / a.m.area[r];
-                const R gV = g * a.dt / (half * (a.m.area[r] + a.m.area[r + 1]));
                 c.aU = a.mult * (gU * hU * a.m.dyl[i + 1]);
                 c.aV = a.mult * (gV * hV * a.m.dxb[r + 1]);
                 if (COR) {
@@ -255,6 +270,7 @@ __global__ void __launch_bounds__(128) linear_adjoint_stream_kernel(const AdjArg
         R lst0 = lst_of(v0, c0, cm.aV, vm.lv);
 
         for (int r = ra; r < rb; r++) {
+            if (r + 1 - base > 31) chunk(r);   // warp-uniform
             const ARow<R> v3 = load(r + 3);
             const ACoef<R> c1 = coef(r + 1, v1.e, v1.ee, v2.e);
             const R lst1 = lst_of(v1, c1, c0.aV, v0.lv);
@@ -264,6 +280,8 @@ __global__ void __launch_bounds__(128) linear_adjoint_stream_kernel(const AdjArg
             const R cvlv_em = __shfl_down_sync(FULL, cm.cV * vm.lv, 1);   // at (i+1, r-1)
             const R culu_w0 = __shfl_up_sync(FULL, c0.cU * v0.lu, 1);     // at (i-1, r)
             const R culu_w1 = __shfl_up_sync(FULL, c1.cU * v1.lu, 1);     // at (i-1, r+1)
+            const R c_r = __shfl_sync(FULL, f_c, r - base);              // dt / area(r)
+            const R c_r1 = __shfl_sync(FULL, f_c, r + 1 - base);         // dt / area(r+1)
             if (out) {
                 const R idm = in_im(i, r, a.xl, a.xu, a.yl, a.yu) ? a.mult : one;
                 R lU = idm * v0.lu;
@@ -282,13 +300,12 @@ __global__ void __launch_bounds__(128) linear_adjoint_stream_kernel(const AdjArg
                     lV = lV + culu_w1;
                     lV = lV + c1.cU * R(1) * v1.lu;
                 }
-                const R c_r = a.dt / a.m.area[r];
                 if (in_is(i, r, a.xl, a.xu, a.yl, a.yu)) {
                     lU = lU - c_r * a.m.dyl[i] * lst0;
                     lV = lV - c_r * a.m.dxb[r + 1] * lst0;
                 }
                 if (in_is(i + 1, r, a.xl, a.xu, a.yl, a.yu)) lU = lU + c_r * a.m.dyl[i + 1] * lst_e;
-                if (in_is(i, r + 1, a.xl, a.xu, a.yl, a.yu)) lV = lV + (a.dt / a.m.area[r + 1]) * a.m.dxb[r + 1] * lst1;
+                if (in_is(i, r + 1, a.xl, a.xu, a.yl, a.yu)) lV = lV + c_r1 * a.m.dxb[r + 1] * lst1;
                 const int64_t o = (int64_t)r * P + i;
                 a.ls_o[o] = lst0;
                 a.lu_o[o] = lU;
