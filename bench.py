@@ -12,7 +12,8 @@ configuration's 20000 timesteps.  Synthetic seeded data.
 metric: cell-updates/s = nx * ny * timesteps / device seconds (all GPUs).
 
 The same JSON line carries, under "forms", the metric's other forms timed
-on the same GPU right after the headline (N = 1 only): the plain FP64
+on the same GPU right after the headline (N = 1 only): the headline with
+FP32 state, the plain linear configuration at its own 400^2, the plain FP64
 leapfrog at 4096^2 and 8192^2 against the HBM roofline, the batched FP32
 leapfrog (3600 x 2400 x 256 instances) against the per-instance loop, the
 adjoint misfit gradient (1200 x 800, K = 50) against one forward solve, and
@@ -362,7 +363,8 @@ def run_ours(args, world, rank, local):
     forms = None
     if rank == 0 and world == 1 and not args.no_forms and N == 2048 and not args.real32:
         forms = {}
-        for name, fn in (("linear_fp64", form_linear_sweep), ("batched", form_batched), ("adjoint", form_adjoint),
+        for name, fn in (("rk2_fp32", form_rk2_fp32), ("linear_400", form_linear_400),
+                         ("linear_fp64", form_linear_sweep), ("batched", form_batched), ("adjoint", form_adjoint),
                          ("multidomain", form_multidomain), ("nested16", form_nested16)):
             t0 = time.perf_counter()
             try:
@@ -457,6 +459,46 @@ def form_linear(local, n, inner=200, reps=3, warmup=1):
 
 def form_linear_sweep(local):
     return {f"n{n}": form_linear(local, n) for n in (4096, 8192)}
+
+
+def form_linear_400(local, nsteps=2000, reps=3):
+    """The plain linear configuration at its own size: 400x400, dx 1 km,
+    flat 4000 m, walls, Gaussian hump, FP64, CFL 0.7, 2000 steps, 9 gauges
+    sampled every step (L2-resident: latency and launch bound)."""
+    import torch
+    from ptha_b200 import Domain, workloads
+    kw, U, gauges = workloads.linear_gaussian_basin(n=400)
+    d = Domain(**kw, device=local)
+    d.set_U(U)
+    dt = d.linear_timestep_max()
+    d.gauges_setup(gauges, capacity=nsteps * (reps + 1) + 8)
+    stream = torch.cuda.ExternalStream(d.stream(), device=f"cuda:{local}")
+    d.evolve_steps(nsteps, dt)
+    d.synchronize()
+    ms = _event_ms(stream, lambda: [d.evolve_steps(nsteps, dt) for _ in range(reps)])
+    d.close()
+    return {"workload": "linear_gaussian_basin_400x400_fp64_9_gauges", "value": 400 * 400 * nsteps * reps / (ms / 1e3),
+            "unit": UNIT, "ms_per_timestep": ms / (reps * nsteps), "timesteps": nsteps, "dt": dt}
+
+
+def form_rk2_fp32(local, nsteps=2000, reps=2):
+    """The headline workload with FP32 state (the reference's -DREALFLOAT
+    build; pressure/source terms stay FP64)."""
+    import torch
+    from ptha_b200 import Domain, workloads
+    kw, U, gauges, nsq = workloads.rk2_beach()
+    d = Domain(**kw, real_bytes=4, device=local)
+    d.set_U(U)
+    d.set_manning_squared(nsq)
+    d.gauges_setup(gauges, capacity=nsteps * (reps + 1) + 8)
+    stream = torch.cuda.ExternalStream(d.stream(), device=f"cuda:{local}")
+    d.evolve_steps(nsteps)
+    d.synchronize()
+    ms = _event_ms(stream, lambda: [d.evolve_steps(nsteps) for _ in range(reps)])
+    d.close()
+    cells = kw["nx"][0] * kw["nx"][1]
+    return {"workload": "rk2_beach_2048x2048_fp32_adaptive", "value": cells * nsteps * reps / (ms / 1e3), "unit": UNIT,
+            "ms_per_timestep": ms / (reps * nsteps), "timesteps": nsteps * reps}
 
 
 def form_batched(local, B=256, nx=3600, ny=2400, inner=50, reps=2, world=1, rank=0, dist=None):

@@ -423,17 +423,18 @@ __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_SROW_MIN_CTAS) rk2_srow_
     }
 }
 
-// The shared-memory-rows form for the update stages and the register form
-// for the flux pass (the faster of the two for each), unless
+// The shared-memory-rows form for the FP64 update stages and the register
+// form for the flux pass and for FP32 state (the faster of the two for each:
+// FP32 stage 2 0.311 ms in registers, 0.330 in shared-memory rows), unless
 // SWALS_FV_STREAM=stream or =srow picks one form for all.
-bool use_srow_kernel(int mode)
+bool use_srow_kernel(int mode, int real_bytes)
 {
     static int v = -1;
     if (v < 0) {
         const char *e = getenv("SWALS_FV_STREAM");
         v = (e && strcmp(e, "stream") == 0) ? 0 : (e && strcmp(e, "srow") == 0) ? 1 : 2;
     }
-    return v == 1 || (v == 2 && (mode == MODE_STAGE1 || mode == MODE_STAGE2));
+    return v == 1 || (v == 2 && real_bytes == 8 && (mode == MODE_STAGE1 || mode == MODE_STAGE2));
 }
 
 }  // namespace
@@ -446,7 +447,7 @@ cudaError_t launch_stage_stream(const Rk2Args<R> &a, cudaStream_t s)
     const int strips_y = (a.ny + SH - 1) / SH;
     const int warps = strips_x * strips_y;
     const int blocks = (warps + SWARPS - 1) / SWARPS;
-    if (use_srow_kernel(MODE)) {
+    if (use_srow_kernel(MODE, (int)sizeof(R))) {
         const size_t smem = sizeof(SRows<R>) * SWARPS;   // 37.9 KB (FP64): under the 48 KB default
         auto go = [&](auto kernel) -> cudaError_t {
             kernel<<<blocks, SLANES * SWARPS, smem, s>>>(a);
