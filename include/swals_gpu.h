@@ -144,6 +144,9 @@ int swals_gpu_evolve_steps(swals_domain *d, int32_t nsteps, double timestep, int
 
 int swals_gpu_get_state(swals_domain *d, swals_domain_state *st);
 int swals_gpu_set_time(swals_domain *d, double time);      /* domain%time = time */
+/* Waits for the domain's stream.  Also SWALS_ERR_CUDA when bounded waits of
+ * the bulk-copy linear kernel (SWALS_LINEAR_KERNEL=bulk) ran out since the
+ * last check, i.e. rows of a step were not updated (the count is cleared). */
 int swals_gpu_synchronize(swals_domain *d);
 
 /* domain%max_U(:,:,1) ('max_stage'), column-major (nx,ny). */

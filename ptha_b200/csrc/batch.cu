@@ -166,7 +166,7 @@ int copy_instances(swals_batch *b, int first, int count, void *host, int nvar, b
         }
     }
     BCK(cudaStreamSynchronize(g->stream));
-    return SWALS_OK;
+    return to_dev ? SWALS_OK : swals::api_check_bulk_waits(g->stream);
 }
 
 }  // namespace

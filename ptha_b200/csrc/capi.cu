@@ -89,6 +89,17 @@ bool is_staggered(int m) { return m == M_LINEAR || m == M_LF_LIN_NLFRIC || m == 
 void swals::set_last_error(const char *msg) { g_last_error = msg; }
 int swals::api_fail(int code, const char *msg) { g_last_error = msg; return code; }
 int swals::api_cuda_fail(cudaError_t e, const char *what) { return cuda_fail(e, what); }
+int swals::api_check_bulk_waits(cudaStream_t s)
+{
+    if (!swals::linear_bulk_launched()) return SWALS_OK;
+    unsigned n = 0;
+    cudaError_t e = swals::linear_wait_expired(&n, true, s);
+    if (e != cudaSuccess) return cuda_fail(e, "reading the expired-wait count");
+    if (n)
+        return fail(SWALS_ERR_CUDA,
+                    "%u bounded waits for bulk-copied rows ran out: rows of a linear step were not updated", n);
+    return SWALS_OK;
+}
 
 
 namespace {
@@ -776,7 +787,7 @@ int swals_gpu_synchronize(swals_domain *d)
 {
     if (!d) return fail(SWALS_ERR_INVALID_ARGUMENT, "NULL domain");
     CK(cudaStreamSynchronize(d->stream));
-    return SWALS_OK;
+    return swals::api_check_bulk_waits(d->stream);
 }
 
 static int timestep_max_impl(swals_domain *d, int linear, double *out)

@@ -99,6 +99,10 @@ struct swals_domain {
 namespace swals {
 int api_fail(int code, const char *msg);
 int api_cuda_fail(cudaError_t e, const char *what);
+// After work on stream s: SWALS_ERR_CUDA (and the count cleared) when
+// bounded waits of bulk-copied linear rows ran out since the last check;
+// SWALS_OK at once when no bulk-copy step was ever launched.
+int api_check_bulk_waits(cudaStream_t s);
 LaunchHook hook_of(swals_domain *d);
 
 template <typename R>

@@ -20,8 +20,10 @@
 // staggered branch), forms the boundary flux sums (:126-205) and advances
 // domain%time.
 #include <algorithm>
+#include <atomic>
 #include <cstdlib>
 #include <cstring>
+#include <type_traits>
 
 #include "swals_kernels.h"
 
@@ -57,6 +59,12 @@ struct LinArgs {
     const int *sites;
     int n_sites;
     double *rec;
+    // Bulk-copy rows (linear_wide_kernel<..., BULK>): SM clock cycles a ring
+    // slot may take to arrive before the warp gives up, and bytes added to
+    // every slot's expected count (0; a positive value makes no slot ever
+    // complete, which exercises the give-up path).
+    long long wait_cycles;
+    unsigned bulk_extra_tx;
 };
 
 __device__ __forceinline__ bool on_bc_ring(int i, int r, int nx, int ny, const int bext[4])
@@ -658,17 +666,88 @@ template <typename R, int CPL> struct WideRing {
     R h[LIN_WIDE_AD][2][4];          // [slot][lane 0: UH west | lane 31: STG, UH, VH, ELV east][]
 };
 
-template <typename R, bool CORIOLIS, bool TRUELY_LINEAR, bool GAUGES, int CPL>
+// Ring of the bulk-copy form: per slot, UH, VH, STG and ELV of the strip's
+// row with one 16-byte granule either side (which hold the halo columns),
+// and max_stage of the strip.
+template <typename R> struct BulkRing {
+    R v[LIN_WIDE_AD][4][32 * (16 / (int)sizeof(R)) + 2 * (16 / (int)sizeof(R))];
+    R m[LIN_WIDE_AD][32 * (16 / (int)sizeof(R))];
+};
+#ifndef LIN_BULK_FENCE
+#define LIN_BULK_FENCE 1
+#endif
+
+// Bounded waits of the bulk-copy rows that gave up, on this device.
+__device__ unsigned int g_linear_wait_expired;
+// Set on the host when a bulk-copy step is first launched.
+std::atomic<bool> g_bulk_launched{false};
+
+// mbarrier and bulk-copy primitives (PTX ISA: mbarrier.*, cp.async.bulk).
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long *bar, unsigned bytes)
+{
+    unsigned long long state;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 %0, [%1], %2;\n"
+                 : "=l"(state)
+                 : "r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+    (void)state;
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity)
+{
+    unsigned done;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n}\n"
+                 : "=r"(done)
+                 : "r"(smem_u32(bar)), "r"(parity)
+                 : "memory");
+    return done != 0;
+}
+// Wait until the phase of the given parity has completed, for at most
+// `limit` SM clock cycles; false when the bound ran out first.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, unsigned parity, long long limit)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    const long long t0 = clock64();
+    while (clock64() - t0 < limit)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+// `bytes` (a multiple of 16, both addresses 16-byte aligned) from global to
+// this CTA's shared memory, completing on mbarrier `bar`.  No multicast.
+__device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, unsigned bytes, unsigned long long *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+template <typename R, bool CORIOLIS, bool TRUELY_LINEAR, bool GAUGES, int CPL, bool BULK>
 __global__ void __launch_bounds__(128, LIN_WIDE_MINB) linear_wide_kernel(const LinArgs<R> a, int SH, int nstrips,
                                                                          int total)
 {
     constexpr int W = 32 * CPL;
     constexpr int VB = CPL * (int)sizeof(R);
-    __shared__ __align__(16) WideRing<R, CPL> rings[4];
+    static_assert(!BULK || VB == 16, "bulk-copy rows use 16-byte lanes");
+    typedef typename std::conditional<BULK, BulkRing<R>, WideRing<R, CPL>>::type Ring;
+    __shared__ __align__(128) Ring rings[4];
+    __shared__ __align__(8) unsigned long long bars[4][LIN_WIDE_AD];   // bulk form: one mbarrier per slot
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int b = blockIdx.x;
     if (b >= a.nbatch) return;
+    if constexpr (BULK) {
+        if (threadIdx.x < 4 * LIN_WIDE_AD) {
+            mbar_init(&bars[0][0] + threadIdx.x, 1);
+            asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        }
+        __syncthreads();
+    }
     const int nx = a.p.nx, ny = a.p.ny;
     const int64_t P = a.p.pitch;
     const int64_t io = (int64_t)b * a.inst_stride;
@@ -681,7 +760,27 @@ __global__ void __launch_bounds__(128, LIN_WIDE_MINB) linear_wide_kernel(const L
     const R one = K<R>::one();
     const R zero = K<R>::zero();
     const R mad = K<R>::min_depth();
-    WideRing<R, CPL> &rg = rings[wib];
+    Ring &rg = rings[wib];
+    unsigned long long *bar = bars[wib];
+    unsigned phase = 0u;   // bulk form, per slot: parity of the slot's next completion
+    unsigned pend = 0u;    // bulk form, per slot: copies issued and not yet waited for
+    // Bulk form: wait for ring slot s, in every lane, for at most
+    // a.wait_cycles; false in every lane when one lane's bound ran out.
+    auto wait_slot = [&](int s) -> bool {
+        const bool ok = __all_sync(FULL, mbar_wait_bounded(&bar[s], (phase >> s) & 1u, a.wait_cycles));
+        if (ok) {
+            phase ^= 1u << s;
+            pend &= ~(1u << s);
+        }
+        return ok;
+    };
+    // Bulk form, after a wait that ran out: count it, give the warp's other
+    // copies in flight (with the same bound) time to land, and leave.
+    auto give_up = [&]() {
+        if (lane == 0) atomicAdd(&g_linear_wait_expired, 1u);
+        for (int s = 0; s < LIN_WIDE_AD; s++)
+            if (pend & (1u << s)) (void)mbar_wait_bounded(&bar[s], (phase >> s) & 1u, a.wait_cycles);
+    };
 
     for (int w = blockIdx.y * 4 + wib; w < total; w += gridDim.y * 4) {
         const int sx = w % nstrips, sy = w / nstrips;
@@ -712,31 +811,69 @@ __global__ void __launch_bounds__(128, LIN_WIDE_MINB) linear_wide_kernel(const L
                 if (a.sites[2 * q] >= c0 && a.sites[2 * q] < c0 + CPL) lmask |= 1ull << q;
             }
         const int nrow = rb - ra + 2;   // rows ra-1 .. rb
-        auto issue = [&](int k) {
-            if (k < nrow) {
+        // Bulk form: the columns [lo, hi) copied per plane row -- the strip
+        // and one granule either side, cut to the row (nx rounded up to a
+        // granule, inside the pitch) -- which hold the clamped west and east
+        // halo columns; max_stage takes the strip's nb bytes alone.
+        const int nxg = (nx + CPL - 1) / CPL * CPL;
+        const unsigned nb = (unsigned)(min(W, nxg - base) * (int)sizeof(R));
+        const int lo = max(base - CPL, 0), hi = min(base + W + CPL, nxg);
+        const unsigned hb = (unsigned)((hi - lo) * (int)sizeof(R));
+        const int iwo = CPL + iw - base, ieo = CPL + iec - base;   // halo columns in a plane row
+        auto issue_bulk = [&](int k) {
+            if constexpr (BULK) {
+                if (k >= nrow) return;
                 const int q = ra - 1 + k;
                 const int qc = clampi(q, 0, ny - 1);
                 const int slot = k % LIN_WIDE_AD;
                 const int64_t orow = (int64_t)qc * P;
-                const bool qv = (q >= 0 && q < ny);
-                cp_async_vec(&rg.v[slot][0][lane * CPL], uhp + orow + (src_bytes ? c0 : 0), VB, src_bytes);
-                cp_async_vec(&rg.v[slot][1][lane * CPL], vhp + orow + (src_bytes ? c0 : 0), VB, src_bytes);
-                cp_async_vec(&rg.v[slot][2][lane * CPL], stg + orow + (src_bytes ? c0 : 0), VB,
-                             qv ? src_bytes : 0);
-                cp_async_vec(&rg.v[slot][3][lane * CPL], elv + orow + (src_bytes ? c0 : 0), VB, src_bytes);
                 const bool mv = max_stage && q >= ra && q < rb;
-                cp_async_vec(&rg.v[slot][4][lane * CPL], (max_stage ? max_stage : stg) + orow + (src_bytes ? c0 : 0),
-                             VB, mv ? src_bytes : 0);
-                if (lane == 0) {
-                    cp_async_vec(&rg.h[slot][0][0], uhp + orow + iw, (int)sizeof(R), (int)sizeof(R));
-                } else if (lane == 31) {
-                    cp_async_vec(&rg.h[slot][1][0], stg + orow + iec, (int)sizeof(R), (qv && e_in) ? (int)sizeof(R) : 0);
-                    cp_async_vec(&rg.h[slot][1][1], uhp + orow + iec, (int)sizeof(R), (int)sizeof(R));
-                    cp_async_vec(&rg.h[slot][1][2], vhp + orow + iec, (int)sizeof(R), (int)sizeof(R));
-                    cp_async_vec(&rg.h[slot][1][3], elv + orow + iec, (int)sizeof(R), (int)sizeof(R));
+                if (lane == 0) mbar_arrive_expect_tx(&bar[slot], 4u * hb + (mv ? nb : 0u) + a.bulk_extra_tx);
+                // the slot's last reads (all lanes) and the expected count come
+                // before the copies that overwrite it
+                __syncwarp();
+                if (lane < 5) {
+                    const int64_t o = orow + (lane < 4 ? lo : base);
+                    const R *src = lane == 0 ? uhp + o : lane == 1 ? vhp + o : lane == 2 ? stg + o
+                                 : lane == 3 ? elv + o : (mv ? max_stage + o : nullptr);
+                    R *dst = lane < 4 ? &rg.v[slot][lane][lo - (base - CPL)] : rg.m[slot];
+                    if (src) {
+                        if (LIN_BULK_FENCE) asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+                        bulk_copy_g2s(dst, src, lane < 4 ? hb : nb, &bar[slot]);
+                    }
                 }
+                pend |= 1u << (unsigned)slot;
             }
-            cp_async_commit();
+        };
+        auto issue = [&](int k) {
+            if constexpr (BULK) {
+                issue_bulk(k);
+            } else {
+                if (k < nrow) {
+                    const int q = ra - 1 + k;
+                    const int qc = clampi(q, 0, ny - 1);
+                    const int slot = k % LIN_WIDE_AD;
+                    const int64_t orow = (int64_t)qc * P;
+                    const bool qv = (q >= 0 && q < ny);
+                    cp_async_vec(&rg.v[slot][0][lane * CPL], uhp + orow + (src_bytes ? c0 : 0), VB, src_bytes);
+                    cp_async_vec(&rg.v[slot][1][lane * CPL], vhp + orow + (src_bytes ? c0 : 0), VB, src_bytes);
+                    cp_async_vec(&rg.v[slot][2][lane * CPL], stg + orow + (src_bytes ? c0 : 0), VB,
+                                 qv ? src_bytes : 0);
+                    cp_async_vec(&rg.v[slot][3][lane * CPL], elv + orow + (src_bytes ? c0 : 0), VB, src_bytes);
+                    const bool mv = max_stage && q >= ra && q < rb;
+                    cp_async_vec(&rg.v[slot][4][lane * CPL], (max_stage ? max_stage : stg) + orow + (src_bytes ? c0 : 0),
+                                 VB, mv ? src_bytes : 0);
+                    if (lane == 0) {
+                        cp_async_vec(&rg.h[slot][0][0], uhp + orow + iw, (int)sizeof(R), (int)sizeof(R));
+                    } else if (lane == 31) {
+                        cp_async_vec(&rg.h[slot][1][0], stg + orow + iec, (int)sizeof(R), (qv && e_in) ? (int)sizeof(R) : 0);
+                        cp_async_vec(&rg.h[slot][1][1], uhp + orow + iec, (int)sizeof(R), (int)sizeof(R));
+                        cp_async_vec(&rg.h[slot][1][2], vhp + orow + iec, (int)sizeof(R), (int)sizeof(R));
+                        cp_async_vec(&rg.h[slot][1][3], elv + orow + iec, (int)sizeof(R), (int)sizeof(R));
+                    }
+                }
+                cp_async_commit();
+            }
         };
         // New stage of cell (col, r) (domain_mod_linear_solver_include.f90:92-115).
         auto stage_new = [&](int col, bool in_x, R dyl, int r, R s_old, R uh_r, R uh_w, R vh_r, R vh_s,
@@ -762,32 +899,64 @@ __global__ void __launch_bounds__(128, LIN_WIDE_MINB) linear_wide_kernel(const L
             return c > 0 ? v[c > 0 ? c - 1 : 0] : (lane > 0 ? up : halo_w);
         };
 
+        // Halo values of a ring slot: 0 UH west; 1-4 STG, UH, VH, ELV east.
+        auto halo = [&](int slot, int which) -> R {
+            if constexpr (BULK)
+                return which == 0 ? rg.v[slot][0][iwo] : rg.v[slot][which == 1 ? 2 : which == 4 ? 3 : which - 2][ieo];
+            else
+                return which == 0 ? __shfl_sync(FULL, lane == 0 ? rg.h[slot][0][0] : R(0), 0)
+                                  : __shfl_sync(FULL, lane == 31 ? rg.h[slot][1][which - 1] : R(0), 31);
+        };
+        // Value of plane p (UH, VH, STG, ELV, max_stage) at strip column idx
+        // of a ring slot.
+        auto cell = [&](int slot, int p, int idx) -> R {
+            if constexpr (BULK)
+                return p < 4 ? rg.v[slot][p][CPL + idx] : rg.m[slot][idx];
+            else
+                return rg.v[slot][p][idx];
+        };
+        // Row k of the segment is in its ring slot (false: a bounded wait ran out).
+        auto wait_row = [&](int k) -> bool {
+            if constexpr (BULK) {
+                return wait_slot(k % LIN_WIDE_AD);
+            } else {
+                cp_async_wait<LIN_WIDE_AD - 2>();
+                return true;
+            }
+        };
+
         __syncwarp();  // the previous segment's reads of the ring are done
         for (int k = 0; k < LIN_WIDE_AD - 1; k++) issue(k);
         // k = 0: row ra-1 (VH only)
-        cp_async_wait<LIN_WIDE_AD - 2>();
+        if (!wait_row(0)) {
+            give_up();
+            return;
+        }
         R vh_jm1[CPL];
 #pragma unroll
-        for (int c = 0; c < CPL; c++) vh_jm1[c] = rg.v[0][1][lane * CPL + c];
-        R vhE_jm1 = __shfl_sync(FULL, lane == 31 ? rg.h[0][1][2] : R(0), 31);
+        for (int c = 0; c < CPL; c++) vh_jm1[c] = cell(0, 1, lane * CPL + c);
+        R vhE_jm1 = halo(0, 3);
         issue(LIN_WIDE_AD - 1);
         // k = 1: row ra
-        cp_async_wait<LIN_WIDE_AD - 2>();
+        if (!wait_row(1)) {
+            give_up();
+            return;
+        }
         R uh_j[CPL], vh_j[CPL], e_j[CPL], sn_j[CPL], mx[CPL];
         R st_j[CPL];
 #pragma unroll
         for (int c = 0; c < CPL; c++) {
-            uh_j[c] = rg.v[1][0][lane * CPL + c];
-            vh_j[c] = rg.v[1][1][lane * CPL + c];
-            st_j[c] = rg.v[1][2][lane * CPL + c];
-            e_j[c] = rg.v[1][3][lane * CPL + c];
-            mx[c] = rg.v[1][4][lane * CPL + c];
+            uh_j[c] = cell(1, 0, lane * CPL + c);
+            vh_j[c] = cell(1, 1, lane * CPL + c);
+            st_j[c] = cell(1, 2, lane * CPL + c);
+            e_j[c] = cell(1, 3, lane * CPL + c);
+            mx[c] = cell(1, 4, lane * CPL + c);
         }
-        R uhW_j = __shfl_sync(FULL, lane == 0 ? rg.h[1][0][0] : R(0), 0);
-        const R stE_j = __shfl_sync(FULL, lane == 31 ? rg.h[1][1][0] : R(0), 31);
-        const R uhE_j0 = __shfl_sync(FULL, lane == 31 ? rg.h[1][1][1] : R(0), 31);
-        R vhE_j = __shfl_sync(FULL, lane == 31 ? rg.h[1][1][2] : R(0), 31);
-        R eE_j = __shfl_sync(FULL, lane == 31 ? rg.h[1][1][3] : R(0), 31);
+        R uhW_j = halo(1, 0);
+        const R stE_j = halo(1, 1);
+        const R uhE_j0 = halo(1, 2);
+        R vhE_j = halo(1, 3);
+        R eE_j = halo(1, 4);
         issue(LIN_WIDE_AD);
         R snE_j;
         {
@@ -818,22 +987,25 @@ __global__ void __launch_bounds__(128, LIN_WIDE_MINB) linear_wide_kernel(const L
             const R inv_cell_area_dt_n = __shfl_sync(FULL, rc_s, rl);
             const R inv_cell_area_dt_g = __shfl_sync(FULL, rc_u, rl);
             const R inv_cell_area_dt_vh_g = __shfl_sync(FULL, rc_v, rl);
-            cp_async_wait<LIN_WIDE_AD - 2>();
+            if (!wait_row(k)) {
+                give_up();
+                return;
+            }
             const int slot = k % LIN_WIDE_AD;
             R uh_n[CPL], vh_n[CPL], st_n[CPL], e_n[CPL], mx_n[CPL];
 #pragma unroll
             for (int c = 0; c < CPL; c++) {
-                uh_n[c] = rg.v[slot][0][lane * CPL + c];
-                vh_n[c] = rg.v[slot][1][lane * CPL + c];
-                st_n[c] = rg.v[slot][2][lane * CPL + c];
-                e_n[c] = rg.v[slot][3][lane * CPL + c];
-                mx_n[c] = rg.v[slot][4][lane * CPL + c];
+                uh_n[c] = cell(slot, 0, lane * CPL + c);
+                vh_n[c] = cell(slot, 1, lane * CPL + c);
+                st_n[c] = cell(slot, 2, lane * CPL + c);
+                e_n[c] = cell(slot, 3, lane * CPL + c);
+                mx_n[c] = cell(slot, 4, lane * CPL + c);
             }
-            const R uhW_n = __shfl_sync(FULL, lane == 0 ? rg.h[slot][0][0] : R(0), 0);
-            const R stE_n = __shfl_sync(FULL, lane == 31 ? rg.h[slot][1][0] : R(0), 31);
-            const R uhE_n = __shfl_sync(FULL, lane == 31 ? rg.h[slot][1][1] : R(0), 31);
-            const R vhE_n = __shfl_sync(FULL, lane == 31 ? rg.h[slot][1][2] : R(0), 31);
-            const R eE_n = __shfl_sync(FULL, lane == 31 ? rg.h[slot][1][3] : R(0), 31);
+            const R uhW_n = halo(slot, 0);
+            const R stE_n = halo(slot, 1);
+            const R uhE_n = halo(slot, 2);
+            const R vhE_n = halo(slot, 3);
+            const R eE_n = halo(slot, 4);
             issue(k + LIN_WIDE_AD - 1);
 
             // New stage of row j+1: own columns and the east neighbour column.
@@ -957,7 +1129,7 @@ __global__ void __launch_bounds__(128, LIN_WIDE_MINB) linear_wide_kernel(const L
             vhE_jm1 = vhE_j;
             vhE_j = vhE_n; eE_j = eE_n; snE_j = snE_n; uhW_j = uhW_n;
         }
-        cp_async_wait<0>();
+        if constexpr (!BULK) cp_async_wait<0>();
     }
 }
 
@@ -1372,19 +1544,24 @@ template cudaError_t launch_batch_gauges<float>(int64_t, const float *, int64_t,
 // instances per CTA); 5-7: streaming warps with 32, 64 or 128 rows per
 // segment; 8: streaming with the segment height chosen from the grid size;
 // 9-10: cp.async-pipelined streaming, 64 rows or chosen; 11-12: aligned
-// wide strips (8- or 16-byte lanes).  Plain domains use PLAIN_DEFAULT.
+// wide strips (8- or 16-byte lanes); 13: aligned wide strips whose rows
+// arrive by bulk copies.  Plain domains use PLAIN_DEFAULT.
 struct TileCfg { int by, tyt, ib; };
 constexpr TileCfg kTileCfgs[] = {{16, 8, 1}, {16, 8, 2}, {16, 8, 4}, {32, 8, 2}, {8, 8, 4}};
 constexpr int kStreamSH[] = {32, 64, 128, 0};
 constexpr int kAsyncSH[] = {64, 0};
-// 11-12: aligned wide strips (linear_wide_kernel) with 8- and 16-byte lanes.
-constexpr int kWideLaneBytes[] = {8, 16};
+// 11-13: aligned wide strips (linear_wide_kernel) with 8- and 16-byte lanes,
+// rows through per-lane cp.async, and with 16-byte lanes, rows through bulk
+// copies completing on an mbarrier.
+struct WideCfg { int lane_bytes; bool bulk; };
+constexpr WideCfg kWideCfgs[] = {{8, false}, {16, false}, {16, true}};
 constexpr int kNumTileCfgs = sizeof(kTileCfgs) / sizeof(kTileCfgs[0]) + sizeof(kStreamSH) / sizeof(kStreamSH[0]) +
-                             sizeof(kAsyncSH) / sizeof(kAsyncSH[0]) + sizeof(kWideLaneBytes) / sizeof(kWideLaneBytes[0]);
+                             sizeof(kAsyncSH) / sizeof(kAsyncSH[0]) + sizeof(kWideCfgs) / sizeof(kWideCfgs[0]);
 constexpr int STREAM_DEFAULT = 8;
 constexpr int ASYNC_DEFAULT = 10;
 constexpr int WIDE8_CFG = 11;
 constexpr int WIDE16_CFG = 12;
+constexpr int BULK_CFG = 13;
 // Plain steps use the aligned wide strips with 16-byte lanes: measured on
 // the 4096^2 / 8192^2 Gaussian basin (whole step against the measured copy
 // bandwidth) 0.84 / 0.93 in FP64 and 0.74 / 0.86 in FP32, against 0.72 /
@@ -1443,10 +1620,23 @@ void launch_async(const LinArgs<R> &a, int sh, cudaStream_t s)
         linear_async_kernel<R, COR, TL, false><<<grid, 128, 0, s>>>(a, sh, nstrips, total);
 }
 
-template <typename R, bool COR, bool TL, int CPL>
+template <typename R, bool COR, bool TL, int CPL, bool BULK = false>
 void launch_wide(const LinArgs<R> &a, cudaStream_t s)
 {
     constexpr int W = 32 * CPL;
+    // Every lane vector (and bulk-copied row) starts on a VB-byte boundary
+    // when the planes and strides are VB-aligned, as the library allocates
+    // them (256-byte planes, pitch a multiple of 32 elements); anything else
+    // takes the register-streaming kernel, which has no alignment needs.
+    constexpr uintptr_t VB = CPL * sizeof(R);
+    const uintptr_t mis = (uintptr_t)a.p.stg | (uintptr_t)a.p.uh | (uintptr_t)a.p.vh | (uintptr_t)a.p.stg_o |
+                          (uintptr_t)a.p.uh_o | (uintptr_t)a.p.vh_o | (uintptr_t)a.p.elv |
+                          (uintptr_t)a.p.max_stage | (uintptr_t)(a.p.pitch * sizeof(R)) |
+                          (uintptr_t)(a.inst_stride * sizeof(R)) | (uintptr_t)(a.max_stride * sizeof(R));
+    if (mis % VB) {
+        launch_stream<R, COR, TL>(a, 0, s);
+        return;
+    }
     // the wide strips are few on small grids: segments down to 8 rows
     const int sh = stream_rows(a.p.nx, a.p.ny, a.nbatch, W, 8);
     const int nstrips = (a.p.nx + W - 1) / W;
@@ -1454,10 +1644,11 @@ void launch_wide(const LinArgs<R> &a, cudaStream_t s)
     const int total = nstrips * nseg;
     const int gy = std::min((total + 3) / 4, 65535);
     dim3 grid(a.nbatch, gy);
+    if (BULK) g_bulk_launched.store(true, std::memory_order_relaxed);
     if (a.rec && a.n_sites > 0)
-        linear_wide_kernel<R, COR, TL, true, CPL><<<grid, 128, 0, s>>>(a, sh, nstrips, total);
+        linear_wide_kernel<R, COR, TL, true, CPL, BULK><<<grid, 128, 0, s>>>(a, sh, nstrips, total);
     else
-        linear_wide_kernel<R, COR, TL, false, CPL><<<grid, 128, 0, s>>>(a, sh, nstrips, total);
+        linear_wide_kernel<R, COR, TL, false, CPL, BULK><<<grid, 128, 0, s>>>(a, sh, nstrips, total);
 }
 
 template <typename R, bool COR, bool TL>
@@ -1467,10 +1658,13 @@ void launch_tile(const LinArgs<R> &a, int cfg, cudaStream_t s)
     const int nstream = (int)(sizeof(kStreamSH) / sizeof(kStreamSH[0]));
     const int nasync = (int)(sizeof(kAsyncSH) / sizeof(kAsyncSH[0]));
     if (cfg >= ntile + nstream + nasync) {
-        if (kWideLaneBytes[cfg - ntile - nstream - nasync] == 8)
+        const WideCfg &wc = kWideCfgs[cfg - ntile - nstream - nasync];
+        if (wc.lane_bytes == 8)
             launch_wide<R, COR, TL, 8 / (int)sizeof(R)>(a, s);
-        else
+        else if (!wc.bulk)
             launch_wide<R, COR, TL, 16 / (int)sizeof(R)>(a, s);
+        else
+            launch_wide<R, COR, TL, 16 / (int)sizeof(R), true>(a, s);
         return;
     }
     if (cfg >= ntile + nstream) {
@@ -1502,21 +1696,21 @@ void launch_main(const LinArgs<R> &a, const StepConfig &c, int cfg, cudaStream_t
 
 // Kernel of a plain (unbatched) step: the default streaming form unless
 // SWALS_LINEAR_KERNEL selects "tile", "stream" (registers only), "async"
-// (30-column strips through cp.async) or "wide8" / "wide16" (aligned wide
-// strips, 8- or 16-byte lanes).
+// (30-column strips through cp.async), "wide8" / "wide16" (aligned wide
+// strips, 8- or 16-byte lanes) or "bulk" (wide strips, rows by bulk copy).
+// Read at every launch (not cached), so a process can switch kernels between
+// steps.
 int linear_kernel_config()
 {
-    static int cfg = -1;
-    if (cfg < 0) {
-        const char *e = getenv("SWALS_LINEAR_KERNEL");
-        cfg = PLAIN_DEFAULT;
-        if (e && strcmp(e, "tile") == 0) cfg = 0;
-        else if (e && strcmp(e, "stream") == 0) cfg = STREAM_DEFAULT;
-        else if (e && strcmp(e, "async") == 0) cfg = ASYNC_DEFAULT;
-        else if (e && strcmp(e, "wide8") == 0) cfg = WIDE8_CFG;
-        else if (e && strcmp(e, "wide16") == 0) cfg = WIDE16_CFG;
-    }
-    return cfg;
+    const char *e = getenv("SWALS_LINEAR_KERNEL");
+    if (!e) return PLAIN_DEFAULT;
+    if (strcmp(e, "tile") == 0) return 0;
+    if (strcmp(e, "stream") == 0) return STREAM_DEFAULT;
+    if (strcmp(e, "async") == 0) return ASYNC_DEFAULT;
+    if (strcmp(e, "wide8") == 0) return WIDE8_CFG;
+    if (strcmp(e, "wide16") == 0) return WIDE16_CFG;
+    if (strcmp(e, "bulk") == 0) return BULK_CFG;
+    return PLAIN_DEFAULT;
 }
 
 // Plain-step kernel for a grid: small grids (up to 0.7 M cells; L2-resident,
@@ -1530,6 +1724,34 @@ int plain_config(int nx, int ny)
     if (e && *e) return linear_kernel_config();
     if ((int64_t)nx * ny <= 700000) return 0;
     return linear_kernel_config();
+}
+
+// Bound on a bulk-copy ring slot's wait: 2^31 SM clock cycles (about 1.1 s
+// at 1965 MHz) unless SWALS_BULK_WAIT_CYCLES gives another (positive) bound.
+long long bulk_wait_cycles()
+{
+    static long long v = -1;
+    if (v < 0) {
+        const char *e = getenv("SWALS_BULK_WAIT_CYCLES");
+        const long long x = e ? atoll(e) : 0;
+        v = x > 0 ? x : (1ll << 31);
+    }
+    return v;
+}
+
+// Bytes added to every bulk-copy slot's expected count: 0 unless
+// SWALS_TEST_BULK_EXTRA_TX sets it, in which case no slot ever completes and
+// every warp takes the bounded give-up path (the copies themselves land
+// normally).  Only the give-up test sets it.
+unsigned bulk_extra_tx()
+{
+    static int v = -1;
+    if (v < 0) {
+        const char *e = getenv("SWALS_TEST_BULK_EXTRA_TX");
+        const int x = e ? atoi(e) : 0;
+        v = (x > 0 && x < (1 << 16)) ? x : 0;
+    }
+    return (unsigned)v;
 }
 
 template <typename R>
@@ -1559,6 +1781,8 @@ LinArgs<R> make_args(const StepPlanes<R> &p, const Metrics<R> &m, const StepConf
     a.sites = nullptr;
     a.n_sites = 0;
     a.rec = nullptr;
+    a.wait_cycles = bulk_wait_cycles();
+    a.bulk_extra_tx = bulk_extra_tx();
     return a;
 }
 
@@ -2065,6 +2289,24 @@ cudaError_t launch_linear_batch(const StepPlanes<R> &p0, int64_t inst_stride, in
 }
 
 int linear_tile_config_count() { return kNumTileCfgs; }
+
+bool linear_bulk_launched() { return g_bulk_launched.load(std::memory_order_relaxed); }
+
+cudaError_t linear_wait_expired(unsigned *count, bool clear, cudaStream_t s)
+{
+    void *addr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&addr, g_linear_wait_expired);
+    if (e != cudaSuccess) return e;
+    unsigned h = 0;
+    e = cudaMemcpyAsync(&h, addr, sizeof(h), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess && clear && h) {
+        e = cudaMemsetAsync(addr, 0, sizeof(h), s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    }
+    if (count) *count = h;
+    return e;
+}
 
 template <typename R>
 cudaError_t launch_update_max_stage(int nx, int ny, int64_t pitch, const R *stg, R *max_stage, const StepConfig &c,

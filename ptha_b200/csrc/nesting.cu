@@ -1449,7 +1449,7 @@ int swals_gpu_md_synchronize(swals_multidomain *md)
     if (!md) return fail(SWALS_ERR_INVALID_ARGUMENT, "NULL multidomain");
     MDCK(cudaSetDevice(md->device));
     MDCK(cudaStreamSynchronize(md->stream));
-    return SWALS_OK;
+    return swals::api_check_bulk_waits(md->stream);
 }
 
 int swals_gpu_md_launch_count(swals_multidomain *md, int64_t *n)

@@ -163,6 +163,15 @@ cudaError_t launch_linear_batch(const StepPlanes<R> &p0, int64_t inst_stride, in
                                 const LaunchHook &hook);
 int linear_tile_config_count();
 
+// Bounded waits of the bulk-copy linear rows that gave up on the current
+// device since the count was last cleared (read on `s`, which is then
+// synchronised); `clear` resets it.  A nonzero count means some rows of a
+// step were not updated.
+cudaError_t linear_wait_expired(unsigned *count, bool clear, cudaStream_t s);
+// Whether a bulk-copy linear step has been launched in this process (the
+// count above can only be nonzero then).
+bool linear_bulk_launched();
+
 // Batched gauges: records[rec][b][g] = STG of instance b at gauge g.
 template <typename R>
 cudaError_t launch_batch_gauges(int64_t pitch, const R *stg0, int64_t inst_stride, int nbatch, const int *site_ij,
