@@ -412,6 +412,17 @@ int swals_gpu_domain_create(const swals_domain_desc *desc, swals_domain **out)
                     desc->timestepping_method);
     const int nx = desc->nx[0], ny = desc->nx[1];
     if (nx < 4 || ny < 4) return fail(SWALS_ERR_INVALID_ARGUMENT, "nx, ny must be >= 4 (got %d, %d)", nx, ny);
+    {
+        // The update region xL..xU, yL..yU (1-based, 0 = the full range) lies
+        // inside the grid, as the reference's loop bounds assume; the kernels
+        // index neighbours of its cells.
+        const int xl = desc->xL > 0 ? desc->xL : 1, xu = desc->xU > 0 ? desc->xU : nx;
+        const int yl = desc->yL > 0 ? desc->yL : 1, yu = desc->yU > 0 ? desc->yU : ny;
+        if (xu > nx || yu > ny || xl > xu || yl > yu)
+            return fail(SWALS_ERR_INVALID_ARGUMENT,
+                        "update region xL..xU = %d..%d, yL..yU = %d..%d is not inside 1..%d, 1..%d", xl, xu, yl, yu,
+                        nx, ny);
+    }
     if (!(desc->real_bytes == 8 || desc->real_bytes == 4))
         return fail(SWALS_ERR_INVALID_ARGUMENT, "real_bytes must be 4 or 8");
     if (desc->coriolis && !desc->spherical)

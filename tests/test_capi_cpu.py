@@ -116,3 +116,12 @@ def test_flux_method_checks():
     with pytest.raises(SwalsError) as e:
         _create(timestepping_method="rk2", compute_fluxes_inner_method="EEC")
     assert e.value.code == 3
+
+
+@pytest.mark.parametrize("region", [dict(xU=17), dict(yU=20), dict(xL=9, xU=8), dict(yL=12, yU=3)])
+def test_update_region_outside_the_grid_is_rejected(region):
+    """xL..xU, yL..yU must lie inside 1..nx, 1..ny (the reference's loop
+    bounds); checked before any device work."""
+    with pytest.raises(SwalsError) as e:
+        _create(**region)
+    assert e.value.code == 1 and "update region" in str(e.value)
