@@ -39,7 +39,7 @@ struct swals_domain {
     double *scratch = nullptr;  // row sums / block minima
     int64_t scratch_len = 0;
     double *d_out = nullptr;    // small result slot
-    void *edges = nullptr;      // stored stage-1 edge results (finite-volume methods)
+    void *edges = nullptr;      // stored stage-1 flux-pass results (finite-volume methods)
     int cur = 0;
     int64_t nsteps = 0;
     swals::StepConfig cfg{};

@@ -570,10 +570,10 @@ cudaError_t launch_stage_any(const Rk2Args<R> &a, cudaStream_t s)
     return launch_stage<R, MODE, SPH, COR, FRIC>(a, s);
 }
 
-// Stage-1 update of an adaptive step from the edge results the flux pass
-// stored: the same per-cell fix-ups and fv_update as the stage kernels, one
-// thread per cell.  A memory-latency-bound kernel: 4 CTAs of 256 threads per
-// SM (64 registers, a few spills to L1) measured 6 % faster than 3 CTAs.
+// Stage-1 update of an adaptive step from the per-cell flux and source sums
+// the flux pass stored (cell_flux): the same fix-ups and fv_apply as the
+// stage kernels, one thread per cell.  A memory-latency-bound kernel: 4 CTAs
+// of 256 threads per SM measured 6 % faster than 3 CTAs.
 template <typename R, bool SPH, bool COR, int FRIC>
 __global__ void __launch_bounds__(256, 4) rk2_update_kernel(const Rk2Args<R> a)
 {
@@ -605,31 +605,13 @@ __global__ void __launch_bounds__(256, 4) rk2_update_kernel(const Rk2Args<R> a)
             negfix = 1;
         }
         c.stg = sv; c.dep = dep; c.elv = ev;
-        const EdgePlanes<R> &ep = a.ep;
-        EdgeRes<R> n_lo, n_hi, w_lo, w_hi;
-        n_lo.f[0] = ep.sf[0][o]; n_lo.f[1] = ep.sf[1][o]; n_lo.f[2] = ep.sf[2][o];
-        n_lo.es_pos = ep.s_pos[o]; n_lo.es_neg = 0.0;
-        w_lo.f[0] = ep.wf[0][o]; w_lo.f[1] = ep.wf[1][o]; w_lo.f[2] = ep.wf[2][o];
-        w_lo.es_pos = ep.w_pos[o]; w_lo.es_neg = 0.0;
-        if (r + 1 < ny) {
-            const int64_t on = o + a.P;
-            n_hi.f[0] = ep.sf[0][on]; n_hi.f[1] = ep.sf[1][on]; n_hi.f[2] = ep.sf[2][on];
-            n_hi.es_neg = ep.s_neg[on];
-        } else {
-            n_hi.f[0] = n_hi.f[1] = n_hi.f[2] = R(0);
-            n_hi.es_neg = 0.0;
-        }
-        n_hi.es_pos = 0.0;
-        if (i + 1 < nx) {
-            w_hi.f[0] = ep.wf[0][o + 1]; w_hi.f[1] = ep.wf[1][o + 1]; w_hi.f[2] = ep.wf[2][o + 1];
-            w_hi.es_neg = ep.w_neg[o + 1];
-        } else {
-            w_hi.f[0] = w_hi.f[1] = w_hi.f[2] = R(0);
-            w_hi.es_neg = 0.0;
-        }
-        w_hi.es_pos = 0.0;
+        CellFlux<R> f;
+        f.d[0] = a.cs.d[0][o]; f.d[1] = a.cs.d[1][o]; f.d[2] = a.cs.d[2][o];
+        f.eu = a.cs.eu[o]; f.ev = a.cs.ev[o];
+        R Um_uh, Um_vh;
+        fixed_momenta<R>(a, o, c, Um_uh, Um_vh);
         const R dt = stage_dt<R>(a);
-        fv_update<R, MODE_STAGE1, SPH, COR, FRIC>(a, i, r, c, n_lo, n_hi, w_lo, w_hi, dt, dt / a.m.area[r]);
+        fv_apply<R, MODE_STAGE1, FRIC>(a, i, r, c, Um_uh, Um_vh, f, dt, dt / a.m.area[r]);
     }
     for (int off = 16; off > 0; off >>= 1) negfix += __shfl_down_sync(0xffffffffu, negfix, off);
     if ((threadIdx.x & 31) == 0 && negfix)
@@ -806,7 +788,7 @@ Rk2Args<R> fv_args(int nx, int ny, int64_t pitch, R *elv, R *manning_sq, const M
     a.side = reinterpret_cast<R *>(buf.side);
     a.sc = sc;
     a.stg0 = nullptr; a.uh0 = nullptr; a.vh0 = nullptr;
-    a.ep = EdgePlanes<R>{};
+    a.cs = CellSums<R>{};
     a.flux_variant = c.flux_variant;
     a.dt_scale = R(1);
     a.base0 = 0;
@@ -856,9 +838,8 @@ cudaError_t first_stage(Rk2Args<R> &a, R *const planes[3][3], int A, int B, bool
         auto take_r = [&]() { R *p = reinterpret_cast<R *>(q); q += plane * sizeof(R); return p; };
         auto take_d = [&]() { double *p = reinterpret_cast<double *>(q); q += plane * sizeof(double); return p; };
         // doubles first (8-byte alignment whatever R is)
-        a.ep.s_pos = take_d(); a.ep.s_neg = take_d(); a.ep.w_pos = take_d(); a.ep.w_neg = take_d();
-        for (int k = 0; k < 3; k++) a.ep.sf[k] = take_r();
-        for (int k = 0; k < 3; k++) a.ep.wf[k] = take_r();
+        a.cs.eu = take_d(); a.cs.ev = take_d();
+        for (int k = 0; k < 3; k++) a.cs.d[k] = take_r();
         Rk2Args<R> p = a;
         p.stg = planes[A][0]; p.uh = planes[A][1]; p.vh = planes[A][2];
         p.stg_o = nullptr; p.uh_o = nullptr; p.vh_o = nullptr;

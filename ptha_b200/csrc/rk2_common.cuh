@@ -7,19 +7,17 @@ namespace swals {
 namespace fv {
 
 // MODE_FLUX: the CFL pass of an adaptive step that also stores every
-// cell's south and west edge results (EdgePlanes) for the stage-1 update.
+// cell's dt-independent update terms (CellSums) for the stage-1 update.
 enum { MODE_CFL = 0, MODE_STAGE1 = 1, MODE_STAGE2 = 2, MODE_FLUX = 3 };
 
-// Stored edge results of a stage: for cell (i, j), its south edge (between
-// rows j-1 and j) and its west edge (between columns i-1 and i): the three
-// fluxes (already multiplied by the edge length) and the explicit-source
-// contributions to the + and - side cells.
+// Stored per-cell results of a flux pass, everything of update_U that does
+// not depend on dt: the flux sums (N - S) + (E - W) of STG, UH, VH (fluxes
+// already multiplied by the edge lengths) and the explicit-source sums of
+// UH and VH.
 template <typename R>
-struct EdgePlanes {
-    R *sf[3];
-    double *s_pos, *s_neg;
-    R *wf[3];
-    double *w_pos, *w_neg;
+struct CellSums {
+    R *d[3];
+    double *eu, *ev;
 };
 enum { FRIC_MANNING = 0, FRIC_CHEZY = 1, FRIC_NONE = 2 };
 
@@ -46,7 +44,7 @@ struct Rk2Args {
     R *side;                       // stage-2 pre-average values of the outer two rings
     double *lines;                 // flux_STG on the 4 boundary-flux lines: N[nx], E[ny], S[nx], W[ny]
     DevScalars *sc;
-    EdgePlanes<R> ep;              // MODE_FLUX output / stage-1 update input
+    CellSums<R> cs;                // MODE_FLUX output / stage-1 update input
     int flux_variant;              // FLUX_* bits (compute_fluxes_inner_method)
     R dt_scale;                    // the stage's dt times this (midpoint half step, rk2n last step; else 1)
     int base0;                     // stage 1 updates U0 (stg0..) with this state's fluxes (midpoint)
@@ -244,37 +242,26 @@ __device__ __forceinline__ R stage_dt(const Rk2Args<R> &a)
     return R(a.dt_fixed) * a.dt_scale;
 }
 
-// update_U for cell (i, r) (update_U_DE1_inner_include.f90:38-96) from its
-// fixed-up centre values and its four edges, with the explicit sources
-// accumulated in the reference's order; stage 2 also forms the rk2 average.
-// inv_cell_area_dt is the row's dt / area_cell_y(r) (a row constant the
-// callers may evaluate once per row).
-template <typename R, int MODE, bool SPH, bool COR, int FRIC>
-__device__ __forceinline__ void fv_update(const Rk2Args<R> &a, int i, int r, const Cell<R> &c, const EdgeRes<R> &n_lo,
-                                          const EdgeRes<R> &n_hi, const EdgeRes<R> &w_lo, const EdgeRes<R> &w_hi,
-                                          R dt, R inv_cell_area_dt)
+// The dt-independent part of update_U for cell (i, r)
+// (update_U_DE1_inner_include.f90:38-96) from its four edges: the flux sums
+// (n_hi - n_lo) + (w_hi - w_lo) and the explicit sources of UH and VH,
+// accumulated in the reference's order.  Um_uh / Um_vh are U(i,j,UH/VH)
+// after compute_depth_and_velocity (zero where depth <= minimum_allowed_depth);
+// only the spherical terms read them.
+template <typename R> struct CellFlux {
+    R d[3];
+    double eu, ev;
+};
+template <typename R, bool SPH, bool COR>
+__device__ __forceinline__ CellFlux<R> cell_flux(const Rk2Args<R> &a, int i, int r, const Cell<R> &c, R Um_uh,
+                                                 R Um_vh, const EdgeRes<R> &n_lo, const EdgeRes<R> &n_hi,
+                                                 const EdgeRes<R> &w_lo, const EdgeRes<R> &w_hi)
 {
     const int nx = a.nx, ny = a.ny;
-    const int64_t P = a.P;
-    const R mad = K<R>::min_depth();
-    const int64_t o = (int64_t)r * P + i;
-    // Mutated U (compute_depth_and_velocity zeroes UH/VH where depth <= minimum_allowed_depth)
-    R U_stg = c.stg;
-    R Um_uh, Um_vh;  // U(i,j,UH/VH) after the fix-ups, before the update
-    if (c.dep > mad) { Um_uh = a.uh[o]; Um_vh = a.vh[o]; }
-    else { Um_uh = R(0); Um_vh = R(0); }
-    R U_uh = Um_uh, U_vh = Um_vh;
-    if (MODE == MODE_STAGE1 && a.base0) {
-        // one_midpoint_step's full step: U was reset to the backup, and
-        // update_U applies the midpoint's fluxes to it.
-        U_stg = a.stg0[o]; U_uh = a.uh0[o]; U_vh = a.vh0[o];
-    }
-
-    U_stg = U_stg - inv_cell_area_dt * ((n_hi.f[0] - n_lo.f[0]) + (w_hi.f[0] - w_lo.f[0]));
-    U_uh = U_uh - inv_cell_area_dt * ((n_hi.f[1] - n_lo.f[1]) + (w_hi.f[1] - w_lo.f[1]));
-    U_vh = U_vh - inv_cell_area_dt * ((n_hi.f[2] - n_lo.f[2]) + (w_hi.f[2] - w_lo.f[2]));
-
-    // Explicit sources of cell (i, r), accumulated in the reference's order.
+    CellFlux<R> f;
+    f.d[0] = (n_hi.f[0] - n_lo.f[0]) + (w_hi.f[0] - w_lo.f[0]);
+    f.d[1] = (n_hi.f[1] - n_lo.f[1]) + (w_hi.f[1] - w_lo.f[1]);
+    f.d[2] = (n_hi.f[2] - n_lo.f[2]) + (w_hi.f[2] - w_lo.f[2]);
     double es_uh = 0.0, es_vh = 0.0, es_jm1 = 0.0;
     if (r >= 1) {
         if (i >= 1) {
@@ -297,6 +284,44 @@ __device__ __forceinline__ void fv_update(const Rk2Args<R> &a, int i, int r, con
         es_uh = es_uh + ((i + 1 <= nx - 1) ? w_hi.es_neg : 0.0);  // explicit_source_im1_work (:721)
     }
     if (r + 1 <= ny - 1 && i >= 1) es_jm1 = n_hi.es_neg;          // explicit_source_VH_j_minus_1(i, j+1)
+    f.eu = es_uh;
+    f.ev = es_vh + es_jm1;
+    return f;
+}
+
+// U(i,j,UH/VH) after compute_depth_and_velocity: the stage input where the
+// fixed-up depth exceeds minimum_allowed_depth, else zero.
+template <typename R>
+__device__ __forceinline__ void fixed_momenta(const Rk2Args<R> &a, int64_t o, const Cell<R> &c, R &Um_uh, R &Um_vh)
+{
+    if (c.dep > K<R>::min_depth()) { Um_uh = a.uh[o]; Um_vh = a.vh[o]; }
+    else { Um_uh = R(0); Um_vh = R(0); }
+}
+
+// The rest of update_U for cell (i, r) with the stage's dt: the flux
+// update, the wet/dry test, the semi-implicit friction and the explicit
+// sources; stage 2 also forms the rk2 average and max_stage.
+// inv_cell_area_dt is the row's dt / area_cell_y(r) (a row constant the
+// callers may evaluate once per row).
+template <typename R, int MODE, int FRIC>
+__device__ __forceinline__ void fv_apply(const Rk2Args<R> &a, int i, int r, const Cell<R> &c, R Um_uh, R Um_vh,
+                                         const CellFlux<R> &f, R dt, R inv_cell_area_dt)
+{
+    const int nx = a.nx, ny = a.ny;
+    const int64_t P = a.P;
+    const R mad = K<R>::min_depth();
+    const int64_t o = (int64_t)r * P + i;
+    R U_stg = c.stg;
+    R U_uh = Um_uh, U_vh = Um_vh;
+    if (MODE == MODE_STAGE1 && a.base0) {
+        // one_midpoint_step's full step: U was reset to the backup, and
+        // update_U applies the midpoint's fluxes to it.
+        U_stg = a.stg0[o]; U_uh = a.uh0[o]; U_vh = a.vh0[o];
+    }
+
+    U_stg = U_stg - inv_cell_area_dt * f.d[0];
+    U_uh = U_uh - inv_cell_area_dt * f.d[1];
+    U_vh = U_vh - inv_cell_area_dt * f.d[2];
 
     if (U_stg <= c.elv + mad) {
         U_uh = R(0);
@@ -311,9 +336,9 @@ __device__ __forceinline__ void fv_update(const Rk2Args<R> &a, int i, int r, con
                          R(pow_friction<FRIC == FRIC_CHEZY>((double)rmax(depth, mad)));
             implicit_factor = R(1) / ((R(1) + dt * K<R>::gravity() * rmax(depth, R(0)) * fs) + dt * a.lin_fric);
         }
-        U_uh = R((double)U_uh + (double)inv_cell_area_dt * es_uh);
+        U_uh = R((double)U_uh + (double)inv_cell_area_dt * f.eu);
         U_uh = U_uh * implicit_factor;
-        U_vh = R((double)U_vh + (double)inv_cell_area_dt * (es_vh + es_jm1));
+        U_vh = R((double)U_vh + (double)inv_cell_area_dt * f.ev);
         U_vh = U_vh * implicit_factor;
     }
 
@@ -349,6 +374,19 @@ __device__ __forceinline__ void fv_update(const Rk2Args<R> &a, int i, int r, con
     a.stg_o[o] = U_stg;
     a.uh_o[o] = U_uh;
     a.vh_o[o] = U_vh;
+}
+
+// update_U for cell (i, r) (update_U_DE1_inner_include.f90:38-96) from its
+// fixed-up centre values and its four edges.
+template <typename R, int MODE, bool SPH, bool COR, int FRIC>
+__device__ __forceinline__ void fv_update(const Rk2Args<R> &a, int i, int r, const Cell<R> &c, const EdgeRes<R> &n_lo,
+                                          const EdgeRes<R> &n_hi, const EdgeRes<R> &w_lo, const EdgeRes<R> &w_hi,
+                                          R dt, R inv_cell_area_dt)
+{
+    R Um_uh, Um_vh;
+    fixed_momenta<R>(a, (int64_t)r * a.P + i, c, Um_uh, Um_vh);
+    const CellFlux<R> f = cell_flux<R, SPH, COR>(a, i, r, c, Um_uh, Um_vh, n_lo, n_hi, w_lo, w_hi);
+    fv_apply<R, MODE, FRIC>(a, i, r, c, Um_uh, Um_vh, f, dt, inv_cell_area_dt);
 }
 }  // namespace fv
 }  // namespace swals

@@ -127,6 +127,21 @@ __device__ __forceinline__ void zero_edge(EdgeRes<R> &e)
     e.f[0] = R(0); e.f[1] = R(0); e.f[2] = R(0); e.es_pos = 0.0; e.es_neg = 0.0;
 }
 
+// The flux pass's output for cell (i, r): its dt-independent update terms
+// (cell_flux) from its four edges, for the stage-1 update once dt is known.
+template <typename R, bool SPH, bool COR>
+__device__ __forceinline__ void store_cell_flux(const Rk2Args<R> &a, int i, int r, const Cell<R> &c,
+                                                const EdgeRes<R> &n_lo, const EdgeRes<R> &n_hi,
+                                                const EdgeRes<R> &w_lo, const EdgeRes<R> &w_hi)
+{
+    const int64_t o = (int64_t)r * a.P + i;
+    R Um_uh = R(0), Um_vh = R(0);
+    if (SPH) fixed_momenta<R>(a, o, c, Um_uh, Um_vh);   // only the spherical terms read them
+    const CellFlux<R> f = cell_flux<R, SPH, COR>(a, i, r, c, Um_uh, Um_vh, n_lo, n_hi, w_lo, w_hi);
+    a.cs.d[0][o] = f.d[0]; a.cs.d[1][o] = f.d[1]; a.cs.d[2][o] = f.d[2];
+    a.cs.eu[o] = f.eu; a.cs.ev[o] = f.ev;
+}
+
 template <typename R, int MODE, bool SPH, bool COR, int FRIC, int SH, bool EDDY>
 __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_STREAM_MIN_CTAS) rk2_stream_kernel(const Rk2Args<R> a)
 {
@@ -206,12 +221,6 @@ __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_STREAM_MIN_CTAS) rk2_str
                 }
             }
         }
-        if (MODE == MODE_FLUX && out_lane && r - 1 >= ra && r - 1 < rb) {
-            // The south edge of row r-1 for the stage-1 update.
-            const int64_t o = (int64_t)(r - 1) * a.P + i;
-            a.ep.sf[0][o] = e_n.f[0]; a.ep.sf[1][o] = e_n.f[1]; a.ep.sf[2][o] = e_n.f[2];
-            a.ep.s_pos[o] = e_n.es_pos; a.ep.s_neg[o] = e_n.es_neg;
-        }
         if (k < 4) { e_s = e_n; continue; }
 
         // Row R = r-2: east-west gradient and west edge, then the update.
@@ -237,18 +246,16 @@ __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_STREAM_MIN_CTAS) rk2_str
                 if (i == a.n_ext) a.lines[2 * nx + ny + R_] = (double)e_w.f[0];
             }
         }
-        if (MODE == MODE_FLUX && out_lane) {
-            // The west edge of row R_.
-            const int64_t o = (int64_t)R_ * a.P + i;
-            a.ep.wf[0][o] = e_w.f[0]; a.ep.wf[1][o] = e_w.f[1]; a.ep.wf[2][o] = e_w.f[2];
-            a.ep.w_pos[o] = e_w.es_pos; a.ep.w_neg[o] = e_w.es_neg;
-        }
-        if (MODE == MODE_STAGE1 || MODE == MODE_STAGE2) {
+        if (MODE == MODE_STAGE1 || MODE == MODE_STAGE2 || MODE == MODE_FLUX) {
             EdgeRes<R> e_e;
             e_e.f[0] = dn1(e_w.f[0]); e_e.f[1] = dn1(e_w.f[1]); e_e.f[2] = dn1(e_w.f[2]);
             e_e.es_neg = dn1(e_w.es_neg);
             e_e.es_pos = 0.0;
-            if (out_lane) fv_update<R, MODE, SPH, COR, FRIC>(a, i, R_, c2, e_s, e_n, e_w, e_e, dt, dt / a.m.area[R_]);
+            if (MODE == MODE_FLUX) {
+                if (out_lane) store_cell_flux<R, SPH, COR>(a, i, R_, c2, e_s, e_n, e_w, e_e);
+            } else if (out_lane) {
+                fv_update<R, MODE, SPH, COR, FRIC>(a, i, R_, c2, e_s, e_n, e_w, e_e, dt, dt / a.m.area[R_]);
+            }
         }
         e_s = e_n;
     }
@@ -361,11 +368,6 @@ __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_SROW_MIN_CTAS) rk2_srow_
                 }
             }
         }
-        if (MODE == MODE_FLUX && out_lane && r - 1 >= ra && r - 1 < rb) {
-            const int64_t o = (int64_t)(r - 1) * a.P + i;
-            a.ep.sf[0][o] = e_n.f[0]; a.ep.sf[1][o] = e_n.f[1]; a.ep.sf[2][o] = e_n.f[2];
-            a.ep.s_pos[o] = e_n.es_pos; a.ep.s_neg[o] = e_n.es_neg;
-        }
         if (k < 4) { sm.es[lane] = e_n; continue; }
 
         // Row R = r-2: east-west gradient and west edge, then the update.
@@ -392,12 +394,7 @@ __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_SROW_MIN_CTAS) rk2_srow_
                 if (i == a.n_ext) a.lines[2 * nx + ny + R_] = (double)e_w.f[0];
             }
         }
-        if (MODE == MODE_FLUX && out_lane) {
-            const int64_t o = (int64_t)R_ * a.P + i;
-            a.ep.wf[0][o] = e_w.f[0]; a.ep.wf[1][o] = e_w.f[1]; a.ep.wf[2][o] = e_w.f[2];
-            a.ep.w_pos[o] = e_w.es_pos; a.ep.w_neg[o] = e_w.es_neg;
-        }
-        if (MODE == MODE_STAGE1 || MODE == MODE_STAGE2) {
+        if (MODE == MODE_STAGE1 || MODE == MODE_STAGE2 || MODE == MODE_FLUX) {
             sm.ew[lane] = e_w;
             __syncwarp();
             EdgeRes<R> e_e;
@@ -405,9 +402,12 @@ __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_SROW_MIN_CTAS) rk2_srow_
             e_e.f[0] = en.f[0]; e_e.f[1] = en.f[1]; e_e.f[2] = en.f[2];
             e_e.es_neg = en.es_neg;
             e_e.es_pos = 0.0;
-            if (out_lane)
+            if (MODE == MODE_FLUX) {
+                if (out_lane) store_cell_flux<R, SPH, COR>(a, i, R_, sm.c[s2][lane], sm.es[lane], e_n, e_w, e_e);
+            } else if (out_lane) {
                 fv_update<R, MODE, SPH, COR, FRIC>(a, i, R_, sm.c[s2][lane], sm.es[lane], e_n, e_w, e_e, dt,
                                                    dt / a.m.area[R_]);
+            }
         }
         sm.es[lane] = e_n;
     }

@@ -215,14 +215,14 @@ struct Rk2Buffers {
     void *side;            // ring buffer used when a boundary routine is active
     void *partials;        // per-block partial sums (deterministic reductions)
     int64_t partials_len;
-    void *edges = nullptr; // stored stage-1 edge results (adaptive steps), or null
+    void *edges = nullptr; // stored stage-1 flux-pass results (adaptive steps), or null
 };
 
-// Bytes of the stored stage-1 edge results of a pitch x ny grid: per cell
-// the south and west edges' three fluxes (real) and two sources (double).
+// Bytes of the stored stage-1 flux-pass results of a pitch x ny grid: per
+// cell the three flux sums (real) and two explicit-source sums (double).
 inline int64_t rk2_edge_bytes(int64_t pitch, int ny, int real_bytes)
 {
-    return 2 * (3 * (int64_t)real_bytes + 2 * 8) * pitch * (int64_t)ny + 512;
+    return (3 * (int64_t)real_bytes + 2 * 8) * pitch * (int64_t)ny + 512;
 }
 
 template <typename R>
