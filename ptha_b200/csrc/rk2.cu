@@ -552,15 +552,12 @@ cudaError_t launch_stage_stream(const fv::Rk2Args<R> &a, cudaStream_t s);
 namespace {
 
 // Stage kernel variant: register streaming (default) or shared-memory tiles,
-// chosen once per process from SWALS_FV_KERNEL=stream|tile.
+// chosen by SWALS_FV_KERNEL=stream|tile.
 bool use_stream_kernel()
 {
-    static int v = -1;
-    if (v < 0) {
-        const char *e = getenv("SWALS_FV_KERNEL");
-        v = (e && strcmp(e, "tile") == 0) ? 0 : 1;
-    }
-    return v == 1;
+    // read at every launch, so that a process can switch forms between steps
+    const char *e = getenv("SWALS_FV_KERNEL");
+    return !(e && strcmp(e, "tile") == 0);
 }
 
 template <typename R, int MODE, bool SPH, bool COR, int FRIC>

@@ -429,11 +429,9 @@ __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_SROW_MIN_CTAS) rk2_srow_
 // SWALS_FV_STREAM=stream or =srow picks one form for all.
 bool use_srow_kernel(int mode, int real_bytes)
 {
-    static int v = -1;
-    if (v < 0) {
-        const char *e = getenv("SWALS_FV_STREAM");
-        v = (e && strcmp(e, "stream") == 0) ? 0 : (e && strcmp(e, "srow") == 0) ? 1 : 2;
-    }
+    // read at every launch, so that a process can switch forms between steps
+    const char *e = getenv("SWALS_FV_STREAM");
+    const int v = (e && strcmp(e, "stream") == 0) ? 0 : (e && strcmp(e, "srow") == 0) ? 1 : 2;
     return v == 1 || (v == 2 && real_bytes == 8 && (mode == MODE_STAGE1 || mode == MODE_STAGE2));
 }
 
