@@ -1,6 +1,7 @@
 // rk2_stream.cu -- finite-volume stage kernels, streaming forms: the
-// register form (rk2_stream_kernel, the flux pass of adaptive steps) and the
-// shared-memory-rows form (rk2_srow_kernel, the update stages), below.
+// register form (rk2_stream_kernel) and the shared-memory-rows form
+// (rk2_srow_kernel, below), whose strips are one warp wide or, by default
+// for every stage, as wide as the CTA (four warps, 124 output columns).
 //
 // Same computation as the shared-memory tile kernel in rk2.cu (and the same
 // device functions: edge_flux, mc_half_gradient, theta_wd, fv_update), organised
@@ -288,33 +289,46 @@ __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_STREAM_MIN_CTAS) rk2_str
 // flux pass 0.280 against 0.275; with 5 CTAs (spills) 0.412 and 0.299.
 #define SWALS_SROW_MIN_CTAS 4
 #endif
-template <typename R>
+//
+// SW is the width of a strip in threads: 32 (one warp per strip, 28 output
+// columns, __syncwarp) or 128 (the CTA's four warps side by side on one
+// strip of 124 output columns, __syncthreads): the wider strip spends its
+// two-column halos on 4 of 128 threads instead of 4 of 32.
+template <typename R, int SW>
 struct SRows {
-    Cell<R> c[3][32];     // rows r % 3
-    Grad<R> g[2][32];     // north-south gradients, rows r % 2
-    EdgeRes<R> es[32];    // south edge of the row being updated
-    Grad<R> gew[32];      // east-west gradient of the row being updated
-    EdgeRes<R> ew[32];    // its west edges
+    Cell<R> c[3][SW];     // rows r % 3
+    Grad<R> g[2][SW];     // north-south gradients, rows r % 2
+    EdgeRes<R> es[SW];    // south edge of the row being updated
+    Grad<R> gew[SW];      // east-west gradient of the row being updated
+    EdgeRes<R> ew[SW];    // its west edges
 };
 
-template <typename R, int MODE, bool SPH, bool COR, int FRIC, int SH, bool EDDY>
+template <int SW> __device__ __forceinline__ void strip_sync()
+{
+    if (SW == 32) __syncwarp();
+    else __syncthreads();
+}
+
+template <typename R, int MODE, bool SPH, bool COR, int FRIC, int SH, bool EDDY, int SW>
 __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_SROW_MIN_CTAS) rk2_srow_kernel(const Rk2Args<R> a)
 {
+    static_assert(SW == 32 || SW == SLANES * SWARPS, "a strip is one warp or the whole CTA");
+    constexpr int SO = SW - 4;   // output columns of a strip
     extern __shared__ __align__(16) unsigned char srow_smem[];
-    const int lane = threadIdx.x & 31;
-    SRows<R> &sm = reinterpret_cast<SRows<R> *>(srow_smem)[threadIdx.x >> 5];
-    const int wid = blockIdx.x * SWARPS + (threadIdx.x >> 5);
+    const int lane = threadIdx.x % SW;   // the thread's place in its strip
+    SRows<R, SW> &sm = reinterpret_cast<SRows<R, SW> *>(srow_smem)[threadIdx.x / SW];
+    const int wid = blockIdx.x * (SLANES * SWARPS / SW) + threadIdx.x / SW;
     const int nx = a.nx, ny = a.ny;
-    const int strips_x = (nx + SOUT - 1) / SOUT;
+    const int strips_x = (nx + SO - 1) / SO;
     const int sx = wid % strips_x, sy = wid / strips_x;
     const int ra = sy * SH;
-    if (ra >= ny) return;  // whole warp
+    if (ra >= ny) return;  // the whole strip
     const int rb = min(ra + SH, ny);
-    const int i = sx * SOUT - 2 + lane;
+    const int i = sx * SO - 2 + lane;
     const bool col_valid = (i >= 0 && i < nx);
-    const bool out_lane = (lane >= 2 && lane <= 29 && i < nx);
-    const bool ew_lane = (lane >= 2 && lane <= 30);
-    const int lw = max(lane - 1, 0), le = min(lane + 1, 31);   // the shuffles' edge behaviour
+    const bool out_lane = (lane >= 2 && lane <= SW - 3 && i < nx);
+    const bool ew_lane = (lane >= 2 && lane <= SW - 2);
+    const int lw = max(lane - 1, 0), le = min(lane + 1, SW - 1);   // the shuffles' edge behaviour
 
     R dt = R(0);
     if (MODE == MODE_STAGE1 || MODE == MODE_STAGE2) dt = stage_dt<R>(a);
@@ -324,7 +338,7 @@ __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_SROW_MIN_CTAS) rk2_srow_
 
     Raw<R> nxt = load_raw<R>(a, i, ra - 2);
     for (int r = ra - 2, k = 0; r <= rb + 1; r++, k++) {
-        __syncwarp();   // every lane is done with the entries this iteration rewrites
+        strip_sync<SW>();   // every lane is done with the entries this iteration rewrites
         const Raw<R> cur = nxt;
         if (r + 1 <= rb + 1) nxt = load_raw<R>(a, i, r + 1);
         if ((MODE == MODE_STAGE1 || MODE == MODE_STAGE2) && out_lane && r + 1 >= ra && r + 1 < rb) {
@@ -381,7 +395,7 @@ __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_SROW_MIN_CTAS) rk2_srow_
             else { gew.ds = R(0); gew.dd = R(0); gew.du = R(0); gew.dv = R(0); }
             sm.gew[lane] = gew;
         }
-        __syncwarp();
+        strip_sync<SW>();
         EdgeRes<R> e_w;
         zero_edge(e_w);
         if (ew_lane && i >= 1 && i <= nx - 1 && R_ >= 1 && R_ <= ny - 1) {
@@ -399,7 +413,7 @@ __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_SROW_MIN_CTAS) rk2_srow_
         }
         if (MODE == MODE_STAGE1 || MODE == MODE_STAGE2 || MODE == MODE_FLUX) {
             sm.ew[lane] = e_w;
-            __syncwarp();
+            strip_sync<SW>();
             EdgeRes<R> e_e;
             const EdgeRes<R> &en = sm.ew[le];
             e_e.f[0] = en.f[0]; e_e.f[1] = en.f[1]; e_e.f[2] = en.f[2];
@@ -417,11 +431,12 @@ __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_SROW_MIN_CTAS) rk2_srow_
 
     if (a.write_cfl || MODE == MODE_CFL || MODE == MODE_FLUX) {
         for (int o = 16; o > 0; o >>= 1) cfl = fmax(cfl, __shfl_down_sync(FULL, cfl, o));
-        if (lane == 0 && cfl > 0.0) atomicMax(&a.sc->max_dt_inv_bits, (unsigned long long)__double_as_longlong(cfl));
+        if ((threadIdx.x & 31) == 0 && cfl > 0.0)
+            atomicMax(&a.sc->max_dt_inv_bits, (unsigned long long)__double_as_longlong(cfl));
     }
     if (MODE == MODE_STAGE1 || MODE == MODE_STAGE2) {
         for (int o = 16; o > 0; o >>= 1) negfix += __shfl_down_sync(FULL, negfix, o);
-        if (lane == 0 && negfix) atomicAdd((unsigned long long *)&a.sc->negative_depth_fix_counter,
+        if ((threadIdx.x & 31) == 0 && negfix) atomicAdd((unsigned long long *)&a.sc->negative_depth_fix_counter,
                                            (unsigned long long)negfix);
     }
 }
@@ -430,12 +445,20 @@ __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_SROW_MIN_CTAS) rk2_srow_
 // form for the flux pass and for FP32 state (the faster of the two for each:
 // FP32 stage 2 0.311 ms in registers, 0.330 in shared-memory rows), unless
 // SWALS_FV_STREAM=stream or =srow picks one form for all.
-bool use_srow_kernel(int mode, int real_bytes)
+// 0: register form; 1: shared-memory rows, one warp per strip; 2: shared-
+// memory rows, the CTA's four warps on one strip (the default: on the
+// 2048^2 rk2 step, FP64 flux pass 0.268 ms against 0.283 for the register
+// form, stage 2 0.362 against 0.390 for one-warp strips, the step 0.741
+// against 0.785 ms; FP32 0.624 against 0.640 ms).
+int fv_stream_form(int mode, int real_bytes)
 {
+    (void)mode;
+    (void)real_bytes;
     // read at every launch, so that a process can switch forms between steps
     const char *e = getenv("SWALS_FV_STREAM");
-    const int v = (e && strcmp(e, "stream") == 0) ? 0 : (e && strcmp(e, "srow") == 0) ? 1 : 2;
-    return v == 1 || (v == 2 && real_bytes == 8 && (mode == MODE_STAGE1 || mode == MODE_STAGE2));
+    if (e && strcmp(e, "stream") == 0) return 0;
+    if (e && strcmp(e, "srow") == 0) return 1;
+    return 2;
 }
 
 }  // namespace
@@ -448,16 +471,30 @@ cudaError_t launch_stage_stream(const Rk2Args<R> &a, cudaStream_t s)
     const int strips_y = (a.ny + SH - 1) / SH;
     const int warps = strips_x * strips_y;
     const int blocks = (warps + SWARPS - 1) / SWARPS;
-    if (use_srow_kernel(MODE, (int)sizeof(R))) {
-        const size_t smem = sizeof(SRows<R>) * SWARPS;   // 37.9 KB (FP64): under the 48 KB default
+    const int form = fv_stream_form(MODE, (int)sizeof(R));
+    if (form == 1) {
+        const size_t smem = sizeof(SRows<R, 32>) * SWARPS;   // 37.9 KB (FP64): under the 48 KB default
         auto go = [&](auto kernel) -> cudaError_t {
             kernel<<<blocks, SLANES * SWARPS, smem, s>>>(a);
             return cudaGetLastError();
         };
         if constexpr (MODE != MODE_CFL) {
-            if (a.flux_variant & FLUX_EDDY) return go(rk2_srow_kernel<R, MODE, SPH, COR, FRIC, SH, true>);
+            if (a.flux_variant & FLUX_EDDY) return go(rk2_srow_kernel<R, MODE, SPH, COR, FRIC, SH, true, 32>);
         }
-        return go(rk2_srow_kernel<R, MODE, SPH, COR, FRIC, SH, false>);
+        return go(rk2_srow_kernel<R, MODE, SPH, COR, FRIC, SH, false, 32>);
+    }
+    if (form == 2) {
+        constexpr int SW = SLANES * SWARPS;
+        const int cstrips = ((a.nx + SW - 5) / (SW - 4)) * strips_y;   // one CTA per strip segment
+        const size_t smem = sizeof(SRows<R, SW>);
+        auto go = [&](auto kernel) -> cudaError_t {
+            kernel<<<cstrips, SLANES * SWARPS, smem, s>>>(a);
+            return cudaGetLastError();
+        };
+        if constexpr (MODE != MODE_CFL) {
+            if (a.flux_variant & FLUX_EDDY) return go(rk2_srow_kernel<R, MODE, SPH, COR, FRIC, SH, true, SW>);
+        }
+        return go(rk2_srow_kernel<R, MODE, SPH, COR, FRIC, SH, false, SW>);
     }
     if constexpr (MODE != MODE_CFL) {
         if (a.flux_variant & FLUX_EDDY) {

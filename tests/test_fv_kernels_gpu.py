@@ -6,12 +6,12 @@ domain_mod_compute_fluxes_DE1_inner_include.f90,
 domain_mod_update_U_DE1_inner_include.f90) run in one of three kernel forms:
 shared-memory tiles (SWALS_FV_KERNEL=tile), register-streaming warp strips
 (SWALS_FV_STREAM=stream) and streaming strips with their carried rows in
-shared memory (SWALS_FV_STREAM=srow); by default FP64 update stages use the
-shared-memory rows and everything else the registers.  Adaptive steps add a
-flux pass that stores each cell's dt-independent update terms and a per-cell
-update once dt is known.  Each form runs here on widths that cut the
-28-column strips every way (one partial strip, exactly two strips, ragged
-last strips) and heights that leave short last segments, on a beach where
+shared memory, one warp (SWALS_FV_STREAM=srow) or the CTA's four warps
+(the default, SWALS_FV_STREAM=crow) per strip.  Adaptive steps add a flux
+pass that stores each cell's dt-independent update terms and a per-cell
+update once dt is known.  Each form runs here on widths that cut the 28-
+and 124-column strips every way (one partial strip, exactly one or two
+strips, ragged last strips) and heights that leave short last segments, on a beach where
 a wave runs up and the wet/dry front moves, with rk2 (adaptive and fixed
 dt), euler, midpoint and rk2n, and on a spherical patch with Coriolis; FP64
 against the IEEE-strict oracle, FP32 against the default form bit for bit.
@@ -28,6 +28,7 @@ FORMS = {
     "tile": {"SWALS_FV_KERNEL": "tile"},
     "stream": {"SWALS_FV_STREAM": "stream"},
     "srow": {"SWALS_FV_STREAM": "srow"},
+    "crow": {"SWALS_FV_STREAM": "crow"},
 }
 
 
@@ -71,7 +72,7 @@ def _assert_exact(g, o, tag):
 
 
 @pytest.mark.parametrize("form", list(FORMS))
-@pytest.mark.parametrize("shape", [(30, 25), (56, 40), (97, 61), (130, 150)])
+@pytest.mark.parametrize("shape", [(30, 25), (56, 40), (97, 61), (124, 37), (130, 150)])
 @pytest.mark.parametrize("adaptive", [True, False])
 def test_rk2_form_matches_oracle(form, shape, adaptive, monkeypatch):
     _set_form(monkeypatch, form)
