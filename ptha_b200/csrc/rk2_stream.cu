@@ -44,8 +44,10 @@ constexpr int SWARPS = SWALS_STREAM_WARPS;   // warps per CTA
 // lead-in rows, as the more numerous, shorter strips balance better over
 // the SMs; with the shared-memory-rows update stages, 8 / 10 / 12 / 16 / 20
 // rows give 0.789 / 0.783 / 0.786 / 0.796 / 0.811 ms a step (16 rows fill
-// exactly four waves of 592 CTAs and still lose); more CTAs per SM (a lower
-// register cap) spill and lose 15-25 %.
+// exactly four waves of 592 CTAs and still lose), and with the CTA-wide
+// strips 8 / 10 / 12 / 14 / 16 / 20 rows 0.757 / 0.747 / 0.743 / 0.760 /
+// 0.748 / 0.744 ms; more CTAs per SM (a lower register cap) spill and lose
+// 15-25 %.
 // Also measured and dropped: a persistent one-wave launch with equal
 // contiguous runs per warp (fewer recomputed halo rows, 8 % slower), the
 // same grid looping over 12-row strips (15 % slower), the row constants
