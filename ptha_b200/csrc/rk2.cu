@@ -567,48 +567,76 @@ cudaError_t launch_stage_any(const Rk2Args<R> &a, cudaStream_t s)
     return launch_stage<R, MODE, SPH, COR, FRIC>(a, s);
 }
 
+// The update of one cell from its loaded inputs.
+template <typename R, int FRIC>
+__device__ __forceinline__ void update_cell(const Rk2Args<R> &a, int i, int r, R sv, R ev, R uh_in, R vh_in,
+                                            const CellFlux<R> &f, R dt, R area, long long &negfix)
+{
+    // compute_depth_and_velocity (domain_mod.f90:1387-1412)
+    Cell<R> c;
+    R dep = sv - ev;
+    c.u = R(0); c.v = R(0);
+    if (dep > K<R>::min_depth()) {
+        const R depth_inv = R(1) / dep;
+        c.u = uh_in * depth_inv;
+        c.v = vh_in * depth_inv;
+    } else if (dep < R(0)) {
+        dep = R(0);
+        sv = ev;
+        negfix += 1;
+    }
+    c.stg = sv; c.dep = dep; c.elv = ev;
+    // U(i,j,UH/VH) after the fix-ups (fixed_momenta)
+    const bool wet = c.dep > K<R>::min_depth();
+    const R Um_uh = wet ? uh_in : R(0), Um_vh = wet ? vh_in : R(0);
+    fv_apply<R, MODE_STAGE1, FRIC>(a, i, r, c, Um_uh, Um_vh, f, dt, dt / area);
+}
+
+// Cells per thread and CTAs per SM of the stage-1 update.  Measured on the
+// 2048^2 FP64 step: one cell, 4 CTAs 0.081 ms (0.097 with the stored terms
+// loaded after the depth test); two cells, 3 CTAs 0.077 ms (0.88 of the
+// measured HBM bandwidth for its 104 B a cell); two cells, 2 CTAs 0.093.
+#ifndef SWALS_UPDATE_CELLS
+#define SWALS_UPDATE_CELLS 2
+#endif
+#ifndef SWALS_UPDATE_MINB
+#define SWALS_UPDATE_MINB 3
+#endif
+
 // Stage-1 update of an adaptive step from the per-cell flux and source sums
 // the flux pass stored (cell_flux): the same fix-ups and fv_apply as the
-// stage kernels, one thread per cell.  A memory-latency-bound kernel: 4 CTAs
-// of 256 threads per SM measured 6 % faster than 3 CTAs.
+// stage kernels, SWALS_UPDATE_CELLS adjacent cells per thread.  Every load
+// of a cell is issued before its first branch, so that the cell costs one
+// memory round trip: the state, the stored update terms, the stage dt (one
+// line for all threads), the row's area and (into L1, for the friction
+// branch) n^2.  A memory-latency-bound kernel.
 template <typename R, bool SPH, bool COR, int FRIC>
-__global__ void __launch_bounds__(256, 4) rk2_update_kernel(const Rk2Args<R> a)
+__global__ void __launch_bounds__(256, SWALS_UPDATE_MINB) rk2_update_kernel(const Rk2Args<R> a)
 {
-    const int i = blockIdx.x * 32 + threadIdx.x;
+    constexpr int NC = SWALS_UPDATE_CELLS;
+    const int i0 = (blockIdx.x * 32 + threadIdx.x) * NC;
     const int r = blockIdx.y * 8 + threadIdx.y;
     const int nx = a.nx, ny = a.ny;
     long long negfix = 0;
-    if (i < nx && r < ny) {
-        const int64_t o = (int64_t)r * a.P + i;
-        // The loads that wait on a branch (momenta behind the depth test,
-        // n^2 behind the friction test) are started now, into L1, so the
-        // cell costs one memory round trip.
-        asm volatile("prefetch.global.L1 [%0];" ::"l"(a.uh + o));
-        asm volatile("prefetch.global.L1 [%0];" ::"l"(a.vh + o));
-        if (FRIC != FRIC_NONE) asm volatile("prefetch.global.L1 [%0];" ::"l"(a.nsq + o));
-        // compute_depth_and_velocity (domain_mod.f90:1387-1412)
-        Cell<R> c;
-        R sv = a.stg[o];
-        const R ev = a.elv[o];
-        R dep = sv - ev;
-        c.u = R(0); c.v = R(0);
-        if (dep > K<R>::min_depth()) {
-            const R depth_inv = R(1) / dep;
-            c.u = a.uh[o] * depth_inv;
-            c.v = a.vh[o] * depth_inv;
-        } else if (dep < R(0)) {
-            dep = R(0);
-            sv = ev;
-            negfix = 1;
+    if (i0 < nx && r < ny) {
+        const int64_t o0 = (int64_t)r * a.P + i0;
+        R sv[NC], ev[NC], uh_in[NC], vh_in[NC];
+        CellFlux<R> f[NC];
+#pragma unroll
+        for (int q = 0; q < NC; q++) {
+            if (i0 + q < nx) {
+                const int64_t o = o0 + q;
+                if (FRIC != FRIC_NONE) asm volatile("prefetch.global.L1 [%0];" ::"l"(a.nsq + o));
+                sv[q] = a.stg[o]; ev[q] = a.elv[o]; uh_in[q] = a.uh[o]; vh_in[q] = a.vh[o];
+                f[q].d[0] = a.cs.d[0][o]; f[q].d[1] = a.cs.d[1][o]; f[q].d[2] = a.cs.d[2][o];
+                f[q].eu = a.cs.eu[o]; f[q].ev = a.cs.ev[o];
+            }
         }
-        c.stg = sv; c.dep = dep; c.elv = ev;
-        CellFlux<R> f;
-        f.d[0] = a.cs.d[0][o]; f.d[1] = a.cs.d[1][o]; f.d[2] = a.cs.d[2][o];
-        f.eu = a.cs.eu[o]; f.ev = a.cs.ev[o];
-        R Um_uh, Um_vh;
-        fixed_momenta<R>(a, o, c, Um_uh, Um_vh);
         const R dt = stage_dt<R>(a);
-        fv_apply<R, MODE_STAGE1, FRIC>(a, i, r, c, Um_uh, Um_vh, f, dt, dt / a.m.area[r]);
+        const R area = a.m.area[r];
+#pragma unroll
+        for (int q = 0; q < NC; q++)
+            if (i0 + q < nx) update_cell<R, FRIC>(a, i0 + q, r, sv[q], ev[q], uh_in[q], vh_in[q], f[q], dt, area, negfix);
     }
     for (int off = 16; off > 0; off >>= 1) negfix += __shfl_down_sync(0xffffffffu, negfix, off);
     if ((threadIdx.x & 31) == 0 && negfix)
@@ -624,7 +652,8 @@ cudaError_t launch_flux_pass(const Rk2Args<R> &a, cudaStream_t s)
 template <typename R, bool SPH, bool COR, int FRIC>
 cudaError_t launch_update(const Rk2Args<R> &a, cudaStream_t s)
 {
-    dim3 block(32, 8), grid((a.nx + 31) / 32, (a.ny + 7) / 8);
+    constexpr int NC = SWALS_UPDATE_CELLS;
+    dim3 block(32, 8), grid((a.nx + 32 * NC - 1) / (32 * NC), (a.ny + 7) / 8);
     rk2_update_kernel<R, SPH, COR, FRIC><<<grid, block, 0, s>>>(a);
     return cudaGetLastError();
 }
