@@ -448,19 +448,24 @@ __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_SROW_MIN_CTAS) rk2_srow_
 // FP32 stage 2 0.311 ms in registers, 0.330 in shared-memory rows), unless
 // SWALS_FV_STREAM=stream or =srow picks one form for all.
 // 0: register form; 1: shared-memory rows, one warp per strip; 2: shared-
-// memory rows, the CTA's four warps on one strip (the default: on the
-// 2048^2 rk2 step, FP64 flux pass 0.268 ms against 0.283 for the register
-// form, stage 2 0.362 against 0.390 for one-warp strips, the step 0.741
-// against 0.785 ms; FP32 0.624 against 0.640 ms).
-int fv_stream_form(int mode, int real_bytes)
+// memory rows, the CTA's four warps on one strip.  Grids of 1.5 M cells and
+// more take the CTA-wide strips (2048^2 rk2 step: FP64 flux pass 0.268 ms
+// against 0.283 for the register form, stage 2 0.362 against 0.390 for
+// one-warp strips, the step 0.732 against 0.777 ms; 1536^2 0.460 against
+// 0.465; FP32 2048^2 0.624 against 0.640).  Smaller grids, L2-resident
+// and short of CTAs, keep one-warp strips (1024^2: 0.261 against 0.266 ms
+// at a fixed dt; the nested configuration's 0.9-1.1 M-cell rk2 domains
+// 5.23 against 5.56 ms per md step): shared-memory rows for the FP64
+// update stages, registers for the rest.
+int fv_stream_form(int mode, int real_bytes, int64_t cells)
 {
-    (void)mode;
-    (void)real_bytes;
     // read at every launch, so that a process can switch forms between steps
     const char *e = getenv("SWALS_FV_STREAM");
     if (e && strcmp(e, "stream") == 0) return 0;
     if (e && strcmp(e, "srow") == 0) return 1;
-    return 2;
+    if (e && strcmp(e, "crow") == 0) return 2;
+    if (cells >= 1500000) return 2;
+    return (real_bytes == 8 && (mode == MODE_STAGE1 || mode == MODE_STAGE2)) ? 1 : 0;
 }
 
 }  // namespace
@@ -473,7 +478,7 @@ cudaError_t launch_stage_stream(const Rk2Args<R> &a, cudaStream_t s)
     const int strips_y = (a.ny + SH - 1) / SH;
     const int warps = strips_x * strips_y;
     const int blocks = (warps + SWARPS - 1) / SWARPS;
-    const int form = fv_stream_form(MODE, (int)sizeof(R));
+    const int form = fv_stream_form(MODE, (int)sizeof(R), (int64_t)a.nx * a.ny);
     if (form == 1) {
         const size_t smem = sizeof(SRows<R, 32>) * SWARPS;   // 37.9 KB (FP64): under the 48 KB default
         auto go = [&](auto kernel) -> cudaError_t {

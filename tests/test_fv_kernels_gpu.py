@@ -7,7 +7,9 @@ domain_mod_update_U_DE1_inner_include.f90) run in one of three kernel forms:
 shared-memory tiles (SWALS_FV_KERNEL=tile), register-streaming warp strips
 (SWALS_FV_STREAM=stream) and streaming strips with their carried rows in
 shared memory, one warp (SWALS_FV_STREAM=srow) or the CTA's four warps
-(the default, SWALS_FV_STREAM=crow) per strip.  Adaptive steps add a flux
+(SWALS_FV_STREAM=crow) per strip; by default grids of 1.5 M cells and more
+take the CTA-wide strips, smaller ones the one-warp shared-memory rows for
+FP64 update stages and registers for the rest.  Adaptive steps add a flux
 pass that stores each cell's dt-independent update terms and a per-cell
 update once dt is known.  Each form runs here on widths that cut the 28-
 and 124-column strips every way (one partial strip, exactly one or two
