@@ -22,6 +22,7 @@
 //     on the 2048x2048 beach, a few spilled values included).
 #include "rk2_common.cuh"
 
+#include <cmath>
 #include <cstdlib>
 #include <cstring>
 
@@ -38,25 +39,22 @@ constexpr int SWARPS = SWALS_STREAM_WARPS;   // warps per CTA
 #ifndef SWALS_STREAM_MIN_CTAS
 #define SWALS_STREAM_MIN_CTAS 4  // CTAs per SM the register cap is sized for
 #endif
-#ifndef SWALS_STREAM_ROWS
-// Rows per warp strip.  Measured on the 2048^2 rk2 step (B200): 12 rows
-// beat 32 by 4 % (and 24 by 2 %) despite the larger share of the two
-// lead-in rows, as the more numerous, shorter strips balance better over
-// the SMs; with the shared-memory-rows update stages, 8 / 10 / 12 / 16 / 20
-// rows give 0.789 / 0.783 / 0.786 / 0.796 / 0.811 ms a step (16 rows fill
-// exactly four waves of 592 CTAs and still lose), and with the CTA-wide
-// strips 8 / 10 / 12 / 14 / 16 / 20 rows 0.757 / 0.747 / 0.743 / 0.760 /
-// 0.748 / 0.744 ms; more CTAs per SM (a lower register cap) spill and lose
-// 15-25 %.
+// Rows per strip segment (fv_rows, below): on the 2048^2 rk2 step (B200)
+// 12 rows beat 32 by 4 % (and 24 by 2 %) despite the larger share of the
+// two lead-in rows, as the more numerous, shorter strips balance better
+// over the SMs; with the shared-memory-rows update stages, 8 / 10 / 12 / 16
+// / 20 rows give 0.789 / 0.783 / 0.786 / 0.796 / 0.811 ms a step, and with
+// the CTA-wide strips 8 / 10 / 12 / 14 / 16 / 20 rows 0.757 / 0.747 / 0.743
+// / 0.760 / 0.748 / 0.744 ms; more CTAs per SM (a lower register cap) spill
+// and lose 15-25 %.
 // Also measured and dropped: a persistent one-wave launch with equal
 // contiguous runs per warp (fewer recomputed halo rows, 8 % slower), the
 // same grid looping over 12-row strips (15 % slower), the row constants
 // dt/area and 1/(dx cfl/2) evaluated once per 32 rows and shuffled (2 %
 // slower: the extra live registers spill), 3 CTAs per SM without spills
-// (9 % slower than 4) or 5 CTAs (13 % slower), and FMA contraction (2 % faster, but no longer bit-exact
-// with the IEEE-strict oracle, and 2e-9 relative after 600 steps).
-#define SWALS_STREAM_ROWS 12
-#endif
+// (9 % slower than 4) or 5 CTAs (13 % slower), and FMA contraction (2 %
+// faster, but no longer bit-exact with the IEEE-strict oracle, and 2e-9
+// relative after 600 steps).
 constexpr unsigned FULL = 0xffffffffu;
 
 template <typename R> struct Raw { R s, uh, vh, e; };
@@ -148,8 +146,8 @@ __device__ __forceinline__ void store_cell_flux(const Rk2Args<R> &a, int i, int 
     a.cs.eu[o] = f.eu; a.cs.ev[o] = f.ev;
 }
 
-template <typename R, int MODE, bool SPH, bool COR, int FRIC, int SH, bool EDDY>
-__global__ void __launch_bounds__(SLANES *SWARPS, SWALS_STREAM_MIN_CTAS) rk2_stream_kernel(const Rk2Args<R> a)
+template <typename R, int MODE, bool SPH, bool COR, int FRIC, bool EDDY>
+__global__ void __launch_bounds__(SLANES *SWARPS, SWALS_STREAM_MIN_CTAS) rk2_stream_kernel(const Rk2Args<R> a, int SH)
 {
     const int lane = threadIdx.x & 31;
     const int wid = blockIdx.x * SWARPS + (threadIdx.x >> 5);
@@ -311,8 +309,8 @@ template <int SW> __device__ __forceinline__ void strip_sync()
     else __syncthreads();
 }
 
-template <typename R, int MODE, bool SPH, bool COR, int FRIC, int SH, bool EDDY, int SW>
-__global__ void __launch_bounds__(SLANES *SWARPS, SWALS_SROW_MIN_CTAS) rk2_srow_kernel(const Rk2Args<R> a)
+template <typename R, int MODE, bool SPH, bool COR, int FRIC, bool EDDY, int SW>
+__global__ void __launch_bounds__(SLANES *SWARPS, SWALS_SROW_MIN_CTAS) rk2_srow_kernel(const Rk2Args<R> a, int SH)
 {
     static_assert(SW == 32 || SW == SLANES * SWARPS, "a strip is one warp or the whole CTA");
     constexpr int SO = SW - 4;   // output columns of a strip
@@ -468,48 +466,81 @@ int fv_stream_form(int mode, int real_bytes, int64_t cells)
     return (real_bytes == 8 && (mode == MODE_STAGE1 || mode == MODE_STAGE2)) ? 1 : 0;
 }
 
+// CTAs of a launch of the given form with sh rows per strip segment.
+int64_t fv_ctas(int form, int nx, int ny, int sh)
+{
+    const int64_t segs = (ny + sh - 1) / sh;
+    if (form == 2) return (int64_t)((nx + SLANES * SWARPS - 5) / (SLANES * SWARPS - 4)) * segs;
+    const int64_t warps = (int64_t)((nx + SOUT - 1) / SOUT) * segs;
+    return (warps + SWARPS - 1) / SWARPS;
+}
+
+// Rows per strip segment for a grid: 12 (the best on large grids, where
+// every choice fills its waves about as well) unless another of 8, 16 and
+// 24 rows is at least 2 % cheaper by the estimate
+//   (rows + 4) / rows x ceil(waves) / waves,   waves = CTAs / resident CTAs,
+// the rows marched per output row times the share of the last wave left
+// idle.  Measured (rk2 beach, ms a step, rows 8 / 12 / 16 / 24): 768^2
+// 0.180 / 0.160 / 0.190 / 0.240 (estimate picks 12); 1024^2 0.234 / 0.274 /
+// 0.229 / 0.282 (picks 16); 1536^2 0.467 / 0.458 / 0.498 / 0.524 and
+// 2048^2 0.744 / 0.731 / 0.736 / 0.772 (picks 12).  SWALS_FV_ROWS sets it.
+int fv_rows(int form, int nx, int ny)
+{
+    const char *e = getenv("SWALS_FV_ROWS");
+    if (e && atoi(e) > 0) return atoi(e);
+    static int slots = 0;   // resident CTAs: every form runs 4 CTAs per SM
+    if (slots == 0) {
+        int dev = 0, sms = 148;
+        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        slots = 4 * sms;
+    }
+    const int cand[] = {12, 16, 8, 24};
+    int best = 0;
+    double best_cost = 0.0;
+    for (int sh : cand) {
+        const double w = (double)fv_ctas(form, nx, ny, sh) / slots;
+        const double cost = (sh + 4.0) / sh * std::ceil(w) / w;
+        if (best == 0 || cost < 0.98 * best_cost) {
+            best = sh;
+            best_cost = cost;
+        }
+    }
+    return best;
+}
+
 }  // namespace
 
 template <typename R, int MODE, bool SPH, bool COR, int FRIC>
 cudaError_t launch_stage_stream(const Rk2Args<R> &a, cudaStream_t s)
 {
-    constexpr int SH = SWALS_STREAM_ROWS;
-    const int strips_x = (a.nx + SOUT - 1) / SOUT;
-    const int strips_y = (a.ny + SH - 1) / SH;
-    const int warps = strips_x * strips_y;
-    const int blocks = (warps + SWARPS - 1) / SWARPS;
     const int form = fv_stream_form(MODE, (int)sizeof(R), (int64_t)a.nx * a.ny);
-    if (form == 1) {
-        const size_t smem = sizeof(SRows<R, 32>) * SWARPS;   // 37.9 KB (FP64): under the 48 KB default
-        auto go = [&](auto kernel) -> cudaError_t {
-            kernel<<<blocks, SLANES * SWARPS, smem, s>>>(a);
-            return cudaGetLastError();
-        };
-        if constexpr (MODE != MODE_CFL) {
-            if (a.flux_variant & FLUX_EDDY) return go(rk2_srow_kernel<R, MODE, SPH, COR, FRIC, SH, true, 32>);
-        }
-        return go(rk2_srow_kernel<R, MODE, SPH, COR, FRIC, SH, false, 32>);
-    }
-    if (form == 2) {
+    const int SH = fv_rows(form, a.nx, a.ny);
+    const int blocks = (int)fv_ctas(form, a.nx, a.ny, SH);
+    if (form == 1 || form == 2) {
         constexpr int SW = SLANES * SWARPS;
-        const int cstrips = ((a.nx + SW - 5) / (SW - 4)) * strips_y;   // one CTA per strip segment
-        const size_t smem = sizeof(SRows<R, SW>);
+        const size_t smem = form == 1 ? sizeof(SRows<R, 32>) * SWARPS : sizeof(SRows<R, SW>);   // 37.9 KB (FP64)
         auto go = [&](auto kernel) -> cudaError_t {
-            kernel<<<cstrips, SLANES * SWARPS, smem, s>>>(a);
+            kernel<<<blocks, SLANES * SWARPS, smem, s>>>(a, SH);
             return cudaGetLastError();
         };
-        if constexpr (MODE != MODE_CFL) {
-            if (a.flux_variant & FLUX_EDDY) return go(rk2_srow_kernel<R, MODE, SPH, COR, FRIC, SH, true, SW>);
+        if (form == 1) {
+            if constexpr (MODE != MODE_CFL) {
+                if (a.flux_variant & FLUX_EDDY) return go(rk2_srow_kernel<R, MODE, SPH, COR, FRIC, true, 32>);
+            }
+            return go(rk2_srow_kernel<R, MODE, SPH, COR, FRIC, false, 32>);
         }
-        return go(rk2_srow_kernel<R, MODE, SPH, COR, FRIC, SH, false, SW>);
+        if constexpr (MODE != MODE_CFL) {
+            if (a.flux_variant & FLUX_EDDY) return go(rk2_srow_kernel<R, MODE, SPH, COR, FRIC, true, SW>);
+        }
+        return go(rk2_srow_kernel<R, MODE, SPH, COR, FRIC, false, SW>);
     }
     if constexpr (MODE != MODE_CFL) {
         if (a.flux_variant & FLUX_EDDY) {
-            rk2_stream_kernel<R, MODE, SPH, COR, FRIC, SH, true><<<blocks, SLANES * SWARPS, 0, s>>>(a);
+            rk2_stream_kernel<R, MODE, SPH, COR, FRIC, true><<<blocks, SLANES * SWARPS, 0, s>>>(a, SH);
             return cudaGetLastError();
         }
     }
-    rk2_stream_kernel<R, MODE, SPH, COR, FRIC, SH, false><<<blocks, SLANES * SWARPS, 0, s>>>(a);
+    rk2_stream_kernel<R, MODE, SPH, COR, FRIC, false><<<blocks, SLANES * SWARPS, 0, s>>>(a, SH);
     return cudaGetLastError();
 }
 

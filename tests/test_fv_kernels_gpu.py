@@ -139,3 +139,19 @@ def test_fp32_forms_agree_bit_for_bit(adaptive, monkeypatch):
             np.testing.assert_array_equal(out[form][0][k], out["default"][0][k], err_msg=f"{form} {k}")
         np.testing.assert_array_equal(out[form][1], out["default"][1], err_msg=f"{form} max_stage")
         assert out[form][2] == out["default"][2], form
+
+
+@pytest.mark.parametrize("form", ["crow", "srow", "stream"])
+@pytest.mark.parametrize("rows", [1, 5, 16, 24])
+def test_segment_rows_match_oracle(form, rows, monkeypatch):
+    """Any number of rows per strip segment (SWALS_FV_ROWS; chosen from the
+    grid otherwise) gives the oracle's bits."""
+    _set_form(monkeypatch, form)
+    monkeypatch.setenv("SWALS_FV_ROWS", str(rows))
+    kw, U, nsq = _beach(97, 61)
+    g, o = make_pair(kw, U, manning_sq=nsq)
+    for _ in range(40):
+        g.evolve_one_step()
+        o.evolve_one_step()
+    _assert_exact(g, o, f"rk2 {form} rows={rows}")
+    g.close()
