@@ -52,9 +52,13 @@ constexpr int SWARPS = SWALS_STREAM_WARPS;   // warps per CTA
 // same grid looping over 12-row strips (15 % slower), the row constants
 // dt/area and 1/(dx cfl/2) evaluated once per 32 rows and shuffled (2 %
 // slower: the extra live registers spill), 3 CTAs per SM without spills
-// (9 % slower than 4) or 5 CTAs (13 % slower), and FMA contraction (2 %
+// (9 % slower than 4) or 5 CTAs (13 % slower), FMA contraction (2 %
 // faster, but no longer bit-exact with the IEEE-strict oracle, and 2e-9
-// relative after 600 steps).
+// relative after 600 steps), and a two-phase software pipeline of the
+// shared-memory-rows march (the update of row r-3 and the north-south work
+// of row r between the same two barriers, one barrier fewer a row, 52 KB of
+// shared memory per CTA: flux pass 0.268 -> 0.278 ms, stage 2 0.362 ->
+// 0.366).
 constexpr unsigned FULL = 0xffffffffu;
 
 template <typename R> struct Raw { R s, uh, vh, e; };
