@@ -1637,8 +1637,14 @@ void launch_wide(const LinArgs<R> &a, cudaStream_t s)
         launch_stream<R, COR, TL>(a, 0, s);
         return;
     }
-    // the wide strips are few on small grids: segments down to 8 rows
-    const int sh = stream_rows(a.p.nx, a.p.ny, a.nbatch, W, 8);
+    // The wide strips are few on small grids: FP64 segments down to 8 rows;
+    // FP32 ones, twice as wide, down to 16 (4096^2 FP32: 8 / 16 / 32 rows
+    // 0.742 / 0.770 / 0.776 of HBM; FP64 4096^2 takes 16 rows, 0.86, and
+    // 8192^2 64 rows, 0.95, within 1 % of the best).  SWALS_LINEAR_ROWS sets
+    // the segment height.
+    const char *env_rows = getenv("SWALS_LINEAR_ROWS");
+    const int sh = (env_rows && atoi(env_rows) > 0) ? atoi(env_rows)
+                                                    : stream_rows(a.p.nx, a.p.ny, a.nbatch, W, sizeof(R) == 4 ? 16 : 8);
     const int nstrips = (a.p.nx + W - 1) / W;
     const int nseg = (a.p.ny + sh - 1) / sh;
     const int total = nstrips * nseg;
