@@ -303,8 +303,8 @@ struct SRows {
     Cell<R> c[3][SW];     // rows r % 3
     Grad<R> g[2][SW];     // north-south gradients, rows r % 2
     EdgeRes<R> es[SW];    // south edge of the row being updated
-    Grad<R> gew[SW];      // east-west gradient of the row being updated
-    EdgeRes<R> ew[SW];    // its west edges
+    Grad<R> gew[2][SW];   // east-west gradients, rows r % 2
+    EdgeRes<R> ew[SW];    // west edges of the row being updated
 };
 
 template <int SW> __device__ __forceinline__ void strip_sync()
@@ -371,6 +371,16 @@ __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_SROW_MIN_CTAS) rk2_srow_
         }
         if (k < 3) continue;
 
+        // East-west gradient of row r-1 (its neighbours' fixed-up values were
+        // written before this row's barrier), for the west edges of row r-1
+        // in the next row's pass.
+        if (r <= rb) {
+            Grad<R> gew;
+            if (col_valid && i > 0 && i < nx - 1) gew = limited<R>(sm.c[s1][lw], sm.c[s1][lane], sm.c[s1][le], a.theta);
+            else { gew.ds = R(0); gew.dd = R(0); gew.du = R(0); gew.dv = R(0); }
+            sm.gew[(r + 1) & 1][lane] = gew;
+        }
+
         // North-south edge between rows r-2 and r-1.
         EdgeRes<R> e_n;
         zero_edge(e_n);
@@ -391,22 +401,18 @@ __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_SROW_MIN_CTAS) rk2_srow_
         }
         if (k < 4) { sm.es[lane] = e_n; continue; }
 
-        // Row R = r-2: east-west gradient and west edge, then the update.
+        // Row R = r-2: its west edges (between the same barriers as the
+        // north-south work of row r-1, which they do not depend on), then,
+        // after the barrier, the update.
         const int R_ = r - 2;
-        {
-            Grad<R> gew;
-            if (col_valid && i > 0 && i < nx - 1) gew = limited<R>(sm.c[s2][lw], sm.c[s2][lane], sm.c[s2][le], a.theta);
-            else { gew.ds = R(0); gew.dd = R(0); gew.du = R(0); gew.dv = R(0); }
-            sm.gew[lane] = gew;
-        }
-        strip_sync<SW>();
         EdgeRes<R> e_w;
         zero_edge(e_w);
         if (ew_lane && i >= 1 && i <= nx - 1 && R_ >= 1 && R_ <= ny - 1) {
             const R inv1 = R(1) / (a.m.dxb[R_] * a.half_cfl);
             double cand;
             const int64_t oe = (int64_t)R_ * a.P + i;
-            edge_flux<R, false, EDDY>(sm.c[s2][lw], sm.gew[lw], sm.c[s2][lane], sm.gew[lane], a.m.dyl[i], inv1, e_w,
+            const Grad<R> *gw = sm.gew[r & 1];
+            edge_flux<R, false, EDDY>(sm.c[s2][lw], gw[lw], sm.c[s2][lane], gw[lane], a.m.dyl[i], inv1, e_w,
                                       cand, a.flux_variant, EDDY ? a.ev[oe - 1] : R(0), EDDY ? a.ev[oe] : R(0),
                                       EDDY ? R(0.5) * (a.m.dxb[R_] + a.m.dxb[R_ + 1]) : R(1));
             cfl = fmax(cfl, cand);
