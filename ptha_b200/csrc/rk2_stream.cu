@@ -528,7 +528,7 @@ cudaError_t launch_stage_stream(const Rk2Args<R> &a, cudaStream_t s)
     const int blocks = (int)fv_ctas(form, a.nx, a.ny, SH);
     if (form == 1 || form == 2) {
         constexpr int SW = SLANES * SWARPS;
-        const size_t smem = form == 1 ? sizeof(SRows<R, 32>) * SWARPS : sizeof(SRows<R, SW>);   // 37.9 KB (FP64)
+        const size_t smem = form == 1 ? sizeof(SRows<R, 32>) * SWARPS : sizeof(SRows<R, SW>);   // 41 KB (FP64)
         auto go = [&](auto kernel) -> cudaError_t {
             kernel<<<blocks, SLANES * SWARPS, smem, s>>>(a, SH);
             return cudaGetLastError();
