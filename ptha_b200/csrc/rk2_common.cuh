@@ -343,7 +343,8 @@ __device__ __forceinline__ void fv_apply(const Rk2Args<R> &a, int i, int r, cons
     }
 
     if (MODE == MODE_STAGE2) {
-        if (a.bc_ring) {
+        const bool outer2 = (i <= 1 || i >= nx - 2 || r <= 1 || r >= ny - 2);   // the outer two rings
+        if (a.bc_ring && outer2) {
             // Keep the pre-average outer two rings for the boundary kernel.
             R *side = a.side;
             const int cols[4] = {0, 1, nx - 2, nx - 1};
@@ -363,8 +364,8 @@ __device__ __forceinline__ void fv_apply(const Rk2Args<R> &a, int i, int r, cons
         U_uh = R(0.5) * (U_uh + a.uh0[o]);
         U_vh = R(0.5) * (U_vh + a.vh0[o]);
         if (a.max_stage) {
-            const bool ring = a.bc_ring && ((i == 0 && a.bext[3]) || (i == nx - 1 && a.bext[1]) ||
-                                            (r == 0 && a.bext[2]) || (r == ny - 1 && a.bext[0]));
+            const bool ring = a.bc_ring && outer2 && ((i == 0 && a.bext[3]) || (i == nx - 1 && a.bext[1]) ||
+                                                      (r == 0 && a.bext[2]) || (r == ny - 1 && a.bext[0]));
             if (!ring) {
                 R mx = a.max_stage[o];
                 a.max_stage[o] = (U_stg > mx) ? U_stg : mx;

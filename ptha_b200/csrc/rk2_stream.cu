@@ -341,7 +341,10 @@ __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_SROW_MIN_CTAS) rk2_srow_
     long long negfix = 0;
 
     Raw<R> nxt = load_raw<R>(a, i, ra - 2);
-    for (int r = ra - 2, k = 0; r <= rb + 1; r++, k++) {
+    // ring slots of rows r, r-1, r-2, rotated each row (the first row's
+    // slot is (ra - 2 + 3) % 3 == (ra + 1) % 3)
+    int s0 = (ra + 1) % 3, s1 = (s0 + 2) % 3, s2 = (s0 + 1) % 3;
+    for (int r = ra - 2, k = 0; r <= rb + 1; r++, k++, s2 = s1, s1 = s0, s0 = (s0 == 2) ? 0 : s0 + 1) {
         strip_sync<SW>();   // every lane is done with the entries this iteration rewrites
         const Raw<R> cur = nxt;
         if (r + 1 <= rb + 1) nxt = load_raw<R>(a, i, r + 1);
@@ -355,7 +358,6 @@ __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_SROW_MIN_CTAS) rk2_srow_
                 if (a.max_stage) prefetch_l2(a.max_stage + o);
             }
         }
-        const int s0 = (r + 3) % 3, s1 = (r + 2) % 3, s2 = (r + 1) % 3;   // rows r, r-1, r-2
         const Cell<R> c0 = fix_up<R>(cur, col_valid && r >= 0 && r < ny, negfix,
                                      (MODE == MODE_STAGE1 || MODE == MODE_STAGE2) && out_lane && r >= ra && r < rb);
         sm.c[s0][lane] = c0;
