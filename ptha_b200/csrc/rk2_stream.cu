@@ -395,7 +395,10 @@ __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_SROW_MIN_CTAS) rk2_srow_
                                          EDDY ? a.ev[(int64_t)(e - 1) * a.P + i] : R(0),
                                          EDDY ? a.ev[(int64_t)e * a.P + i] : R(0), EDDY ? a.m.dyl[i] : R(1));
                 cfl = fmax(cfl, cand);
-                if (MODE != MODE_CFL && a.lines && i >= a.n_ext && i <= nx - a.n_ext - 1) {
+                // the boundary-flux lines (rows n_ext and ny - n_ext): tested
+                // on the row first, the same for the whole strip
+                if (MODE != MODE_CFL && (e == ny - a.n_ext || e == a.n_ext) && a.lines && i >= a.n_ext &&
+                    i <= nx - a.n_ext - 1) {
                     if (e == ny - a.n_ext) a.lines[i] = (double)e_n.f[0];
                     if (e == a.n_ext) a.lines[nx + ny + i] = (double)e_n.f[0];
                 }
@@ -418,7 +421,8 @@ __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_SROW_MIN_CTAS) rk2_srow_
                                       cand, a.flux_variant, EDDY ? a.ev[oe - 1] : R(0), EDDY ? a.ev[oe] : R(0),
                                       EDDY ? R(0.5) * (a.m.dxb[R_] + a.m.dxb[R_ + 1]) : R(1));
             cfl = fmax(cfl, cand);
-            if (MODE != MODE_CFL && a.lines && R_ >= a.n_ext && R_ <= ny - a.n_ext - 1) {
+            if (MODE != MODE_CFL && (i == nx - a.n_ext || i == a.n_ext) && a.lines && R_ >= a.n_ext &&
+                R_ <= ny - a.n_ext - 1) {
                 if (i == nx - a.n_ext) a.lines[nx + R_] = (double)e_w.f[0];
                 if (i == a.n_ext) a.lines[2 * nx + ny + R_] = (double)e_w.f[0];
             }
