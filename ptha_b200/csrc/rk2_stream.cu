@@ -298,6 +298,7 @@ __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_STREAM_MIN_CTAS) rk2_str
 // columns, __syncwarp) or 128 (the CTA's four warps side by side on one
 // strip of 124 output columns, __syncthreads): the wider strip spends its
 // two-column halos on 4 of 128 threads instead of 4 of 32.
+constexpr int SROW_RC = 64;   // segments of up to this many rows keep their row constants in shared memory
 template <typename R, int SW>
 struct SRows {
     Cell<R> c[3][SW];     // rows r % 3
@@ -305,6 +306,7 @@ struct SRows {
     EdgeRes<R> es[SW];    // south edge of the row being updated
     Grad<R> gew[2][SW];   // east-west gradients, rows r % 2
     EdgeRes<R> ew[SW];    // west edges of the row being updated
+    R rc[2][SROW_RC];     // the segment's row constants: 1 / (dx cfl/2) of its east-west edges, dt / area
 };
 
 template <int SW> __device__ __forceinline__ void strip_sync()
@@ -339,6 +341,16 @@ __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_SROW_MIN_CTAS) rk2_srow_
     const R inv2 = R(1) / (a.m.dyl[0] * a.half_cfl);
     double cfl = 0.0;
     long long negfix = 0;
+    // The row constants of the segment's rows, one division each by the
+    // strip's threads instead of one per cell (the same expressions; read
+    // after the loop's first barrier).
+    const bool rc_sm = (rb - ra) <= SROW_RC;
+    if (rc_sm)
+        for (int t = lane; t < rb - ra; t += SW) {
+            const int rr = ra + t;
+            sm.rc[0][t] = R(1) / (a.m.dxb[rr] * a.half_cfl);
+            if (MODE == MODE_STAGE1 || MODE == MODE_STAGE2) sm.rc[1][t] = dt / a.m.area[rr];
+        }
 
     Raw<R> nxt = load_raw<R>(a, i, ra - 2);
     // ring slots of rows r, r-1, r-2, rotated each row (the first row's
@@ -413,7 +425,7 @@ __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_SROW_MIN_CTAS) rk2_srow_
         EdgeRes<R> e_w;
         zero_edge(e_w);
         if (ew_lane && i >= 1 && i <= nx - 1 && R_ >= 1 && R_ <= ny - 1) {
-            const R inv1 = R(1) / (a.m.dxb[R_] * a.half_cfl);
+            const R inv1 = rc_sm ? sm.rc[0][R_ - ra] : R(1) / (a.m.dxb[R_] * a.half_cfl);
             double cand;
             const int64_t oe = (int64_t)R_ * a.P + i;
             const Grad<R> *gw = sm.gew[r & 1];
@@ -439,7 +451,7 @@ __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_SROW_MIN_CTAS) rk2_srow_
                 if (out_lane) store_cell_flux<R, SPH, COR>(a, i, R_, sm.c[s2][lane], sm.es[lane], e_n, e_w, e_e);
             } else if (out_lane) {
                 fv_update<R, MODE, SPH, COR, FRIC>(a, i, R_, sm.c[s2][lane], sm.es[lane], e_n, e_w, e_e, dt,
-                                                   dt / a.m.area[R_]);
+                                                   rc_sm ? sm.rc[1][R_ - ra] : dt / a.m.area[R_]);
             }
         }
         sm.es[lane] = e_n;
