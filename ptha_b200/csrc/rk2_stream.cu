@@ -222,7 +222,7 @@ __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_STREAM_MIN_CTAS) rk2_str
                 edge_flux<R, true, EDDY>(c2, g2, c1, g1, a.m.dxb[e], inv2, e_n, cand, a.flux_variant,
                                          EDDY ? a.ev[(int64_t)(e - 1) * a.P + i] : R(0),
                                          EDDY ? a.ev[(int64_t)e * a.P + i] : R(0), EDDY ? a.m.dyl[i] : R(1));
-                cfl = fmax(cfl, cand);
+                if (MODE != MODE_STAGE2) cfl = fmax(cfl, cand);   // stage 2 writes no CFL
                 if (MODE != MODE_CFL && a.lines && i >= a.n_ext && i <= nx - a.n_ext - 1) {
                     if (e == ny - a.n_ext) a.lines[i] = (double)e_n.f[0];
                     if (e == a.n_ext) a.lines[nx + ny + i] = (double)e_n.f[0];
@@ -248,7 +248,7 @@ __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_STREAM_MIN_CTAS) rk2_str
             edge_flux<R, false, EDDY>(cl, gw, c2, gew, a.m.dyl[i], inv1, e_w, cand, a.flux_variant,
                                       EDDY ? a.ev[oe - 1] : R(0), EDDY ? a.ev[oe] : R(0),
                                       EDDY ? R(0.5) * (a.m.dxb[R_] + a.m.dxb[R_ + 1]) : R(1));
-            cfl = fmax(cfl, cand);
+            if (MODE != MODE_STAGE2) cfl = fmax(cfl, cand);
             if (MODE != MODE_CFL && a.lines && R_ >= a.n_ext && R_ <= ny - a.n_ext - 1) {
                 if (i == nx - a.n_ext) a.lines[nx + R_] = (double)e_w.f[0];
                 if (i == a.n_ext) a.lines[2 * nx + ny + R_] = (double)e_w.f[0];
@@ -269,7 +269,7 @@ __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_STREAM_MIN_CTAS) rk2_str
     }
 
     // Warp reductions: CFL max and the negative-depth count.
-    if (a.write_cfl || MODE == MODE_CFL || MODE == MODE_FLUX) {
+    if (MODE != MODE_STAGE2 && (a.write_cfl || MODE == MODE_CFL || MODE == MODE_FLUX)) {
         for (int o = 16; o > 0; o >>= 1) cfl = fmax(cfl, __shfl_down_sync(FULL, cfl, o));
         if (lane == 0 && cfl > 0.0) atomicMax(&a.sc->max_dt_inv_bits, (unsigned long long)__double_as_longlong(cfl));
     }
@@ -406,7 +406,7 @@ __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_SROW_MIN_CTAS) rk2_srow_
                                          a.m.dxb[e], inv2, e_n, cand, a.flux_variant,
                                          EDDY ? a.ev[(int64_t)(e - 1) * a.P + i] : R(0),
                                          EDDY ? a.ev[(int64_t)e * a.P + i] : R(0), EDDY ? a.m.dyl[i] : R(1));
-                cfl = fmax(cfl, cand);
+                if (MODE != MODE_STAGE2) cfl = fmax(cfl, cand);   // stage 2 writes no CFL
                 // the boundary-flux lines (rows n_ext and ny - n_ext): tested
                 // on the row first, the same for the whole strip
                 if (MODE != MODE_CFL && (e == ny - a.n_ext || e == a.n_ext) && a.lines && i >= a.n_ext &&
@@ -432,7 +432,7 @@ __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_SROW_MIN_CTAS) rk2_srow_
             edge_flux<R, false, EDDY>(sm.c[s2][lw], gw[lw], sm.c[s2][lane], gw[lane], a.m.dyl[i], inv1, e_w,
                                       cand, a.flux_variant, EDDY ? a.ev[oe - 1] : R(0), EDDY ? a.ev[oe] : R(0),
                                       EDDY ? R(0.5) * (a.m.dxb[R_] + a.m.dxb[R_ + 1]) : R(1));
-            cfl = fmax(cfl, cand);
+            if (MODE != MODE_STAGE2) cfl = fmax(cfl, cand);
             if (MODE != MODE_CFL && (i == nx - a.n_ext || i == a.n_ext) && a.lines && R_ >= a.n_ext &&
                 R_ <= ny - a.n_ext - 1) {
                 if (i == nx - a.n_ext) a.lines[nx + R_] = (double)e_w.f[0];
@@ -457,7 +457,7 @@ __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_SROW_MIN_CTAS) rk2_srow_
         sm.es[lane] = e_n;
     }
 
-    if (a.write_cfl || MODE == MODE_CFL || MODE == MODE_FLUX) {
+    if (MODE != MODE_STAGE2 && (a.write_cfl || MODE == MODE_CFL || MODE == MODE_FLUX)) {
         for (int o = 16; o > 0; o >>= 1) cfl = fmax(cfl, __shfl_down_sync(FULL, cfl, o));
         if ((threadIdx.x & 31) == 0 && cfl > 0.0)
             atomicMax(&a.sc->max_dt_inv_bits, (unsigned long long)__double_as_longlong(cfl));
@@ -541,6 +541,9 @@ int fv_rows(int form, int nx, int ny)
 template <typename R, int MODE, bool SPH, bool COR, int FRIC>
 cudaError_t launch_stage_stream(const Rk2Args<R> &a, cudaStream_t s)
 {
+    // Stage 2 takes the first stage's dt and accumulates no CFL maximum: its
+    // kernels leave the edges' wave-speed candidates out.
+    if (MODE == MODE_STAGE2 && a.write_cfl) return cudaErrorInvalidValue;
     const int form = fv_stream_form(MODE, (int)sizeof(R), (int64_t)a.nx * a.ny);
     const int SH = fv_rows(form, a.nx, a.ny);
     const int blocks = (int)fv_ctas(form, a.nx, a.ny, SH);
