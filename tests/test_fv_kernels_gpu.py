@@ -142,10 +142,11 @@ def test_fp32_forms_agree_bit_for_bit(adaptive, monkeypatch):
 
 
 @pytest.mark.parametrize("form", ["crow", "srow", "stream"])
-@pytest.mark.parametrize("rows", [1, 5, 16, 24])
+@pytest.mark.parametrize("rows", [1, 5, 16, 24, 80])
 def test_segment_rows_match_oracle(form, rows, monkeypatch):
     """Any number of rows per strip segment (SWALS_FV_ROWS; chosen from the
-    grid otherwise) gives the oracle's bits."""
+    grid otherwise) gives the oracle's bits, segments of more than 64 rows
+    (whose row constants are not kept in shared memory) included."""
     _set_form(monkeypatch, form)
     monkeypatch.setenv("SWALS_FV_ROWS", str(rows))
     kw, U, nsq = _beach(97, 61)
