@@ -149,7 +149,7 @@ def test_segment_rows_match_oracle(form, rows, monkeypatch):
     (whose row constants are not kept in shared memory) included."""
     _set_form(monkeypatch, form)
     monkeypatch.setenv("SWALS_FV_ROWS", str(rows))
-    kw, U, nsq = _beach(97, 61)
+    kw, U, nsq = _beach(97, 61 if rows <= 24 else 150)   # 150 rows: segments of 80 and 70
     g, o = make_pair(kw, U, manning_sq=nsq)
     for _ in range(40):
         g.evolve_one_step()
