@@ -288,9 +288,9 @@ __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_STREAM_MIN_CTAS) rk2_str
 // thread, so more warps per SM hide the FP64 latency.  Lanes touch other
 // lanes' entries only after a __syncwarp.
 #ifndef SWALS_SROW_MIN_CTAS
-// Measured on the 2048^2 step: with 4 CTAs per SM (96 registers, no
-// spills) stage 2 takes 0.391 ms against the register form's 0.412, the
-// flux pass 0.280 against 0.275; with 5 CTAs (spills) 0.412 and 0.299.
+// Measured on the 2048^2 step with warp-wide strips: with 4 CTAs per SM
+// stage 2 takes 0.391 ms against the register form's 0.412, the flux pass
+// 0.280 against 0.275; with 5 CTAs (spills) 0.412 and 0.299.
 #define SWALS_SROW_MIN_CTAS 4
 #endif
 //
@@ -299,6 +299,18 @@ __global__ void __launch_bounds__(SLANES *SWARPS, SWALS_STREAM_MIN_CTAS) rk2_str
 // strip of 124 output columns, __syncthreads): the wider strip spends its
 // two-column halos on 4 of 128 threads instead of 4 of 32.
 constexpr int SROW_RC = 64;   // segments of up to this many rows keep their row constants in shared memory
+// CTAs per SM the register cap of the shared-memory-rows kernel is sized
+// for: 5 (96 registers, 20 warps) for stage 2 of CTA-wide strips, whose
+// shared memory (43 KB FP64) leaves room for five; 4 for the other passes
+// (the flux pass and the fused stage 1 spill at 96 registers), the
+// eddy-viscosity forms (spills of 100-200 bytes) and warp-wide strips
+// (46 KB a CTA).  Measured on the 2048^2 step: stage 2 0.334 -> 0.313 ms
+// with 5, FP32 0.277 -> 0.252; the flux pass at 5 loses 1 %, the fused
+// stage 1 at 1280^2 7 %; 3 CTAs lose 20 %.
+constexpr int srow_min_ctas(int mode, int sw, bool eddy)
+{
+    return (sw == 128 && mode == MODE_STAGE2 && !eddy) ? 5 : SWALS_SROW_MIN_CTAS;
+}
 template <typename R, int SW>
 struct SRows {
     Cell<R> c[3][SW];     // rows r % 3
@@ -316,7 +328,7 @@ template <int SW> __device__ __forceinline__ void strip_sync()
 }
 
 template <typename R, int MODE, bool SPH, bool COR, int FRIC, bool EDDY, int SW>
-__global__ void __launch_bounds__(SLANES *SWARPS, SWALS_SROW_MIN_CTAS) rk2_srow_kernel(const Rk2Args<R> a, int SH)
+__global__ void __launch_bounds__(SLANES *SWARPS, srow_min_ctas(MODE, SW, EDDY)) rk2_srow_kernel(const Rk2Args<R> a, int SH)
 {
     static_assert(SW == 32 || SW == SLANES * SWARPS, "a strip is one warp or the whole CTA");
     constexpr int SO = SW - 4;   // output columns of a strip
@@ -512,16 +524,17 @@ int64_t fv_ctas(int form, int nx, int ny, int sh)
 // 0.180 / 0.160 / 0.190 / 0.240 (estimate picks 12); 1024^2 0.234 / 0.274 /
 // 0.229 / 0.282 (picks 16); 1536^2 0.467 / 0.458 / 0.498 / 0.524 and
 // 2048^2 0.744 / 0.731 / 0.736 / 0.772 (picks 12).  SWALS_FV_ROWS sets it.
-int fv_rows(int form, int nx, int ny)
+int fv_rows(int form, int ctas_per_sm, int nx, int ny)
 {
     const char *e = getenv("SWALS_FV_ROWS");
     if (e && atoi(e) > 0) return atoi(e);
-    static int slots = 0;   // resident CTAs: every form runs 4 CTAs per SM
-    if (slots == 0) {
-        int dev = 0, sms = 148;
-        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        slots = 4 * sms;
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0, n = 148;
+        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        sms = n;
     }
+    const int slots = ctas_per_sm * sms;   // resident CTAs
     const int cand[] = {12, 16, 8, 24};
     int best = 0;
     double best_cost = 0.0;
@@ -545,7 +558,9 @@ cudaError_t launch_stage_stream(const Rk2Args<R> &a, cudaStream_t s)
     // kernels leave the edges' wave-speed candidates out.
     if (MODE == MODE_STAGE2 && a.write_cfl) return cudaErrorInvalidValue;
     const int form = fv_stream_form(MODE, (int)sizeof(R), (int64_t)a.nx * a.ny);
-    const int SH = fv_rows(form, a.nx, a.ny);
+    // (the wave estimate counts 4 resident CTAs per SM for every form: with
+    // stage 2's 5 it would pick 24 rows at 2048^2, 2 % slower than 12)
+    const int SH = fv_rows(form, 4, a.nx, a.ny);
     const int blocks = (int)fv_ctas(form, a.nx, a.ny, SH);
     if (form == 1 || form == 2) {
         constexpr int SW = SLANES * SWARPS;
