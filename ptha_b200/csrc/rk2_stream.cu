@@ -306,10 +306,13 @@ constexpr int SROW_RC = 64;   // segments of up to this many rows keep their row
 // eddy-viscosity forms (spills of 100-200 bytes) and warp-wide strips
 // (46 KB a CTA).  Measured on the 2048^2 step: stage 2 0.334 -> 0.313 ms
 // with 5, FP32 0.277 -> 0.252; the flux pass at 5 loses 1 %, the fused
-// stage 1 at 1280^2 7 %; 3 CTAs lose 20 %.
-constexpr int srow_min_ctas(int mode, int sw, bool eddy)
+// stage 1 at 1280^2 7 %; 3 CTAs lose 20 %.  FP32 state fits every pass of
+// the CTA-wide strips in 96 registers: 5 CTAs for all of them (flux pass
+// 0.208 -> 0.195 ms).
+constexpr int srow_min_ctas(int mode, int sw, bool eddy, int real_bytes)
 {
-    return (sw == 128 && mode == MODE_STAGE2 && !eddy) ? 5 : SWALS_SROW_MIN_CTAS;
+    if (sw == 128 && !eddy && (mode == MODE_STAGE2 || real_bytes == 4)) return 5;
+    return SWALS_SROW_MIN_CTAS;
 }
 template <typename R, int SW>
 struct SRows {
@@ -328,7 +331,7 @@ template <int SW> __device__ __forceinline__ void strip_sync()
 }
 
 template <typename R, int MODE, bool SPH, bool COR, int FRIC, bool EDDY, int SW>
-__global__ void __launch_bounds__(SLANES *SWARPS, srow_min_ctas(MODE, SW, EDDY)) rk2_srow_kernel(const Rk2Args<R> a, int SH)
+__global__ void __launch_bounds__(SLANES *SWARPS, srow_min_ctas(MODE, SW, EDDY, (int)sizeof(R))) rk2_srow_kernel(const Rk2Args<R> a, int SH)
 {
     static_assert(SW == 32 || SW == SLANES * SWARPS, "a strip is one warp or the whole CTA");
     constexpr int SO = SW - 4;   // output columns of a strip
