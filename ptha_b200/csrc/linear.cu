@@ -801,6 +801,18 @@ __global__ void __launch_bounds__(128, LIN_WIDE_MINB) linear_wide_kernel(const L
             dyl_ip1[c] = a.m.dyl[min(ic + 1, nx)];
         }
         const R dyl_e = a.m.dyl[iec];
+        // The lane's columns against the active region (xL..xU), once per
+        // segment: bit c for column c0 + c.
+        unsigned in_xm = 0u, int_xm = 0u, mom_xm = 0u, ms_xm = 0u;
+#pragma unroll
+        for (int c = 0; c < CPL; c++) {
+            const int col = c0 + c;
+            in_xm |= (unsigned)(col < nx) << c;
+            int_xm |= (unsigned)(col >= a.xl + 1 && col <= a.xu - 1) << c;
+            mom_xm |= (unsigned)(col >= a.xl && col <= a.xu - 1) << c;
+            ms_xm |= (unsigned)(col >= a.xl && col <= a.xu) << c;
+        }
+        const bool e_int = (ie >= a.xl + 1) && (ie <= a.xu - 1);
         const unsigned long long gmask =
             GAUGES ? gauges_in(a.sites, a.n_sites, base, base + W - 1, ra, rb - 1) : 0ull;
         // the gauges of the segment in this lane's own columns
@@ -876,14 +888,15 @@ __global__ void __launch_bounds__(128, LIN_WIDE_MINB) linear_wide_kernel(const L
             }
         };
         // New stage of cell (col, r) (domain_mod_linear_solver_include.f90:92-115).
-        auto stage_new = [&](int col, bool in_x, R dyl, int r, R s_old, R uh_r, R uh_w, R vh_r, R vh_s,
-                             R inv_cell_area_dt) -> R {
+        // (interior: the cell is inside xL+1..xU-1, yL+1..yU-1; dxb_r1, dxb_r:
+        // distance_bottom_edge of rows r+1 and r)
+        auto stage_new = [&](int col, bool in_x, bool interior, R dyl, int r, R dxb_r1, R dxb_r, R s_old, R uh_r,
+                             R uh_w, R vh_r, R vh_s, R inv_cell_area_dt) -> R {
             R sn = R(0);
             if (r < ny && in_x) {
-                const bool interior = (col >= a.xl + 1) && (col <= a.xu - 1) && (r >= a.yl + 1) && (r <= a.yu - 1);
                 if (interior) {
                     const R t1 = (uh_r - uh_w) * dyl;
-                    const R t2 = vh_r * a.m.dxb[r + 1] - vh_s * a.m.dxb[r];
+                    const R t2 = vh_r * dxb_r1 - vh_s * dxb_r;
                     sn = s_old - inv_cell_area_dt * (t1 + t2);
                 } else if (a.bc_stage && on_bc_ring(col, r, nx, ny, a.bext)) {
                     sn = stg_o[(int64_t)r * P + col];
@@ -961,14 +974,18 @@ __global__ void __launch_bounds__(128, LIN_WIDE_MINB) linear_wide_kernel(const L
         R snE_j;
         {
             const R dta = a.dt / a.m.area[ra];
+            const bool int_y = (ra >= a.yl + 1) && (ra <= a.yu - 1);
+            const R dxb1 = a.m.dxb[ra + 1], dxb0 = a.m.dxb[ra];
             R uw[CPL];
 #pragma unroll
             for (int c = 0; c < CPL; c++) uw[c] = west(uh_j, uhW_j, c);
 #pragma unroll
             for (int c = 0; c < CPL; c++)
-                sn_j[c] = stage_new(c0 + c, c0 + c < nx, dyl_i[c], ra, st_j[c], uh_j[c], uw[c], vh_j[c], vh_jm1[c], dta);
+                sn_j[c] = stage_new(c0 + c, (in_xm >> c) & 1u, int_y && ((int_xm >> c) & 1u), dyl_i[c], ra, dxb1, dxb0,
+                                    st_j[c], uh_j[c], uw[c], vh_j[c], vh_jm1[c], dta);
             const R uh_last = __shfl_sync(FULL, uh_j[CPL - 1], 31);
-            snE_j = stage_new(ie, e_in, dyl_e, ra, stE_j, uhE_j0, uh_last, vhE_j, vhE_jm1, dta);
+            snE_j = stage_new(ie, e_in, int_y && e_int, dyl_e, ra, dxb1, dxb0, stE_j, uhE_j0, uh_last, vhE_j,
+                              vhE_jm1, dta);
         }
         // Row factors dt/area (the new stage, row j+1) and g dt/area,
         // g dt/mean area (the momenta, row j): lane L evaluates them for row
@@ -1008,17 +1025,31 @@ __global__ void __launch_bounds__(128, LIN_WIDE_MINB) linear_wide_kernel(const L
             const R eE_n = halo(slot, 4);
             issue(k + LIN_WIDE_AD - 1);
 
+            // Row constants: distance_bottom_edge of rows j+1 and j+2 (dxb has
+            // ny + 1 entries; row ny is never updated), the region tests.
+            const R dxb_j1 = a.m.dxb[j + 1], dxb_j2 = a.m.dxb[min(j + 2, ny)];
+            const bool int_y = (j + 1 >= a.yl + 1) && (j + 1 <= a.yu - 1);
+            const bool mom_y = (j >= a.yl) && (j <= a.yu - 1);
+            const bool ms_y = (j >= a.yl) && (j <= a.yu);
+            // dt cor / 2 of row j and of its north face: (dt * cor) * half, the
+            // reference's product order, before the wet factor
+            R dtc_j = zero, dtc_jph = zero;
+            if (CORIOLIS) {
+                dtc_j = a.dt * a.m.cor[j] * half;
+                dtc_jph = a.dt * a.m.cor_be[j + 1] * half;
+            }
+
             // New stage of row j+1: own columns and the east neighbour column.
             R uh_nw[CPL], sn_n[CPL];
 #pragma unroll
             for (int c = 0; c < CPL; c++) uh_nw[c] = west(uh_n, uhW_n, c);
 #pragma unroll
             for (int c = 0; c < CPL; c++)
-                sn_n[c] = stage_new(c0 + c, c0 + c < nx, dyl_i[c], j + 1, st_n[c], uh_n[c], uh_nw[c], vh_n[c], vh_j[c],
-                                    inv_cell_area_dt_n);
+                sn_n[c] = stage_new(c0 + c, (in_xm >> c) & 1u, int_y && ((int_xm >> c) & 1u), dyl_i[c], j + 1, dxb_j2,
+                                    dxb_j1, st_n[c], uh_n[c], uh_nw[c], vh_n[c], vh_j[c], inv_cell_area_dt_n);
             const R uh_n_last = __shfl_sync(FULL, uh_n[CPL - 1], 31);
-            const R snE_n = stage_new(ie, e_in, dyl_e, j + 1, stE_n, uhE_n, uh_n_last, vhE_n, vhE_j,
-                                      inv_cell_area_dt_n);
+            const R snE_n = stage_new(ie, e_in, int_y && e_int, dyl_e, j + 1, dxb_j2, dxb_j1, stE_n, uhE_n, uh_n_last,
+                                      vhE_n, vhE_j, inv_cell_area_dt_n);
 
             // Momentum of row j (:225-567), column by column.
             const R sn_dn = __shfl_down_sync(FULL, sn_j[0], 1);
@@ -1040,11 +1071,11 @@ __global__ void __launch_bounds__(128, LIN_WIDE_MINB) linear_wide_kernel(const L
                 const R vh_e = !last ? vh_j[c + 1 < CPL ? c + 1 : c] : (lane < 31 ? vh_dn : vhE_j);
                 const R vh_se = !last ? vh_jm1[c + 1 < CPL ? c + 1 : c] : (lane < 31 ? vhm_dn : vhE_jm1);
                 const R snc = sn_j[c];
-                const bool in_ms = max_stage && i >= a.xl && i <= a.xu && jrow >= a.yl && jrow <= a.yu;
+                const bool in_ms = max_stage && ms_y && ((ms_xm >> c) & 1u);
                 ms_all = ms_all && in_ms;
                 o_mx[c] = (snc > mx[c]) ? snc : mx[c];
                 R uh = uh_j[c], vh = vh_j[c];
-                if (i >= a.xl && i <= a.xu - 1 && jrow >= a.yl && jrow <= a.yu - 1) {
+                if (mom_y && ((mom_xm >> c) & 1u)) {
                     const R e0 = e_j[c];
                     const R sn = snc, s_n = sn_n[c];
                     R h_iph, h_jph, wet_iph, wet_jph;
@@ -1065,15 +1096,14 @@ __global__ void __launch_bounds__(128, LIN_WIDE_MINB) linear_wide_kernel(const L
                     }
                     const R dw_j = s_n - sn;
                     R uh_new = uh * wet_iph - inv_cell_area_dt_g * h_iph * (s_e - sn) * dyl_ip1[c];
-                    R vh_new = vh * wet_jph - inv_cell_area_dt_vh_g * h_jph * dw_j * a.m.dxb[jrow + 1];
+                    R vh_new = vh * wet_jph - inv_cell_area_dt_vh_g * h_jph * dw_j * dxb_j1;
                     if (CORIOLIS) {
                         const R vh_iph_jmh = half * (vh_jm1[c] + vh_se);
                         const R vh_iph_jph = half * (vh_j[c] + vh_e);
                         const R uh_i_j = half * (uh_j[c] + uh_w[c]);
                         const R uh_i_jp1 = half * (uh_n[c] + uh_nw[c]);
-                        const R dt_half_coriolis = a.dt * a.m.cor[jrow] * half * ((h_iph > zero) ? one : zero);
-                        const R dt_half_coriolis_jph =
-                            a.dt * a.m.cor_be[jrow + 1] * half * ((h_jph > zero) ? one : zero);
+                        const R dt_half_coriolis = dtc_j * ((h_iph > zero) ? one : zero);
+                        const R dt_half_coriolis_jph = dtc_jph * ((h_jph > zero) ? one : zero);
                         uh_new = uh_new + dt_half_coriolis * (vh_iph_jmh + vh_iph_jph);
                         vh_new = vh_new - dt_half_coriolis_jph * (uh_i_j + uh_i_jp1);
                     }
