@@ -2330,8 +2330,19 @@ bool linear_bulk_launched() { return g_bulk_launched.load(std::memory_order_rela
 
 cudaError_t linear_wait_expired(unsigned *count, bool clear, cudaStream_t s)
 {
+    // the count of the stream's device (the caller's current device may differ)
+    int cur = 0, dev = 0;
+    cudaError_t e = cudaGetDevice(&cur);
+    if (e == cudaSuccess && s) e = cudaStreamGetDevice(s, &dev);
+    else dev = cur;
+    if (e != cudaSuccess) return e;
+    if (dev != cur && (e = cudaSetDevice(dev)) != cudaSuccess) return e;
+    struct Restore {
+        int d, c;
+        ~Restore() { if (d != c) cudaSetDevice(c); }
+    } restore{dev, cur};
     void *addr = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&addr, g_linear_wait_expired);
+    e = cudaGetSymbolAddress(&addr, g_linear_wait_expired);
     if (e != cudaSuccess) return e;
     unsigned h = 0;
     e = cudaMemcpyAsync(&h, addr, sizeof(h), cudaMemcpyDeviceToHost, s);
