@@ -259,6 +259,7 @@ int evolve_t(swals_domain *d, double timestep, int has_dt)
         if (e != cudaSuccess) return cuda_fail(e, "update_max_quantities");
     }
     cudaError_t e = cudaSuccess;
+    bool gauges_fused = false;   // the linear step kernel recorded the gauges
     if (d->static_pending) {
         // static_before_time (domain_mod.f90:1706-1716): the clock decides
         // on the host, one read per step until it has passed.
@@ -296,7 +297,14 @@ int evolve_t(swals_domain *d, double timestep, int has_dt)
             cudaEventCreateWithFlags(&d->aux.fork, cudaEventDisableTiming);
             cudaEventCreateWithFlags(&d->aux.join, cudaEventDisableTiming);
         }
-        e = launch_linear_step<R>(p, m, c, R(timestep), d->sc, d->stream, hook, d->timers_on ? nullptr : &d->aux);
+        // the step kernel records the gauges when it is the step's last one
+        StepConfig cg = c;
+        cg.g_sites = d->d_sites;
+        cg.g_n = d->n_gauges;
+        cg.g_records = d->d_records;
+        cg.g_capacity = d->gauge_capacity;
+        gauges_fused = swals::linear_step_fuses_gauges(cg, d->nx, d->ny);
+        e = launch_linear_step<R>(p, m, cg, R(timestep), d->sc, d->stream, hook, d->timers_on ? nullptr : &d->aux);
         if (e != cudaSuccess) return cuda_fail(e, "linear leapfrog step");
         if (d->cfg.fw) d->cfg.fw_ready = 1;
         d->cur = out;
@@ -346,7 +354,7 @@ int evolve_t(swals_domain *d, double timestep, int has_dt)
         hook(CAT_MAXSTAGE, 1);
         if (e != cudaSuccess) return cuda_fail(e, "update_max_quantities");
     }
-    if (d->n_gauges > 0) {
+    if (d->n_gauges > 0 && !gauges_fused) {
         hook(CAT_GAUGES, 0);
         e = launch_gauges<R>(d->pitch, (const R *)d->planes[d->cur][0], (const R *)d->planes[d->cur][1],
                              (const R *)d->planes[d->cur][2], d->d_sites, d->n_gauges, d->d_records,

@@ -65,6 +65,13 @@ struct LinArgs {
     // complete, which exercises the give-up path).
     long long wait_cycles;
     unsigned bulk_extra_tx;
+    // The step's point gauges recorded by the tile kernel (plain steps whose
+    // last kernel it is): g_n sites, records[rec][g][STG, UH, VH].
+    const int *g_sites;
+    int g_n;
+    double *g_records;
+    int g_capacity;
+    DevScalars *g_sc;
 };
 
 __device__ __forceinline__ bool on_bc_ring(int i, int r, int nx, int ny, const int bext[4])
@@ -238,6 +245,34 @@ __global__ void __launch_bounds__(LBX *TYT) linear_step_kernel(const LinArgs<R> 
             }
             uh_o[o] = uh;
             vh_o[o] = vh;
+        }
+    }
+
+    if (a.g_n > 0) {
+        // The step's gauges inside this tile (a plain step: one instance).
+        // This CTA wrote the tile's new values; they are visible to all its
+        // threads after the barrier.  Every CTA reads the record index before
+        // it counts itself done; the last one advances it.
+        const int rec = a.g_sc->gauge_records;
+        __syncthreads();
+        if (rec < a.g_capacity)
+            for (int q = tid; q < a.g_n; q += NT) {
+                const int gi = a.g_sites[2 * q], gr = a.g_sites[2 * q + 1];
+                if (gi >= i0 && gi < i0 + LBX && gr >= r0 && gr < r0 + BY) {
+                    const int64_t o = (int64_t)gr * P + gi;
+                    double *dst = a.g_records + ((int64_t)rec * a.g_n + q) * 3;
+                    dst[0] = (double)a.p.stg_o[o];
+                    dst[1] = (double)a.p.uh_o[o];
+                    dst[2] = (double)a.p.vh_o[o];
+                }
+            }
+        if (tid == 0) {
+            __threadfence();
+            const unsigned nblk = gridDim.x * gridDim.y * gridDim.z;
+            if (atomicAdd(reinterpret_cast<unsigned *>(&a.g_sc->blocks_done), 1u) == nblk - 1) {
+                a.g_sc->gauge_records = rec + 1;
+                a.g_sc->blocks_done = 0;
+            }
         }
     }
 }
@@ -1762,6 +1797,13 @@ int plain_config(int nx, int ny)
     return linear_kernel_config();
 }
 
+// A plain linear step whose last kernel is the tile kernel records its
+// gauges there (one launch fewer a step on the small, launch-bound grids).
+bool fuses_gauges(const StepConfig &c, int nx, int ny)
+{
+    return c.g_n > 0 && c.bc_kind != 3 && c.n_forcing == 0 && !c.fw && plain_config(nx, ny) == 0;
+}
+
 // Bound on a bulk-copy ring slot's wait: 2^31 SM clock cycles (about 1.1 s
 // at 1965 MHz) unless SWALS_BULK_WAIT_CYCLES gives another (positive) bound.
 long long bulk_wait_cycles()
@@ -1819,6 +1861,11 @@ LinArgs<R> make_args(const StepPlanes<R> &p, const Metrics<R> &m, const StepConf
     a.rec = nullptr;
     a.wait_cycles = bulk_wait_cycles();
     a.bulk_extra_tx = bulk_extra_tx();
+    a.g_sites = nullptr;
+    a.g_n = 0;
+    a.g_records = nullptr;
+    a.g_capacity = 0;
+    a.g_sc = nullptr;
     return a;
 }
 
@@ -1905,6 +1952,13 @@ cudaError_t launch_linear_step(const StepPlanes<R> &p, const Metrics<R> &m, cons
                                DevScalars *sc, cudaStream_t s, const LaunchHook &hook, const AuxStream *aux)
 {
     LinArgs<R> a = make_args<R>(p, m, c, dt);
+    if (fuses_gauges(c, p.nx, p.ny)) {
+        a.g_sites = c.g_sites;
+        a.g_n = c.g_n;
+        a.g_records = c.g_records;
+        a.g_capacity = c.g_capacity;
+        a.g_sc = sc;
+    }
     // Forcing patches read domain%time from the edge kernel and change the
     // old momenta in place, so the edge kernel then runs in line.
     const bool side = aux && aux->stream && !a.bc_stage && !c.n_forcing;
@@ -2325,6 +2379,8 @@ cudaError_t launch_linear_batch(const StepPlanes<R> &p0, int64_t inst_stride, in
 }
 
 int linear_tile_config_count() { return kNumTileCfgs; }
+
+bool linear_step_fuses_gauges(const StepConfig &c, int nx, int ny) { return fuses_gauges(c, nx, ny); }
 
 bool linear_bulk_launched() { return g_bulk_launched.load(std::memory_order_relaxed); }
 

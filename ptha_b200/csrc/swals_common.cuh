@@ -196,7 +196,7 @@ struct DevScalars {
     double dt_last_update;
     double evolve_step_dt;
     int    gauge_records;      // number of gauge records written
-    int    pad;
+    int    blocks_done;        // CTAs of the running step kernel past their gauge records (reset by the last)
 };
 
 // Boundary-function parameters (SWALS_BF_*), evaluated on the device.

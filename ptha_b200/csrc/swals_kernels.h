@@ -86,6 +86,12 @@ struct StepConfig {
     const ForcingPatch *forcing;
     void *eddy_visc;        // use_eddy_viscosity: one plane of per-cell eddy viscosity, else null
     double eddy_visc_constants[2];  // domain%eddy_visc_constants (constant, Shiono-Knight)
+    // Point gauges a linear step may record itself (linear_step_fuses_gauges):
+    // 0-based (i, j) sites, records[rec][g][STG, UH, VH], capacity records.
+    const int *g_sites;
+    int g_n;
+    double *g_records;
+    int g_capacity;
 };
 
 // Forcing patches (forcing.cu): add each active patch's share of its
@@ -162,6 +168,11 @@ cudaError_t launch_linear_batch(const StepPlanes<R> &p0, int64_t inst_stride, in
                                 const Metrics<R> &m, const StepConfig &c, R dt, int tile_cfg, cudaStream_t s,
                                 const LaunchHook &hook);
 int linear_tile_config_count();
+// Whether launch_linear_step records the step's gauges itself (c.g_n > 0
+// and the step's last kernel is the shared-memory tile kernel: no Flather
+// fix-up, forcing or friction kernel after it); the caller then launches
+// no gauge kernel.
+bool linear_step_fuses_gauges(const StepConfig &c, int nx, int ny);
 
 // Bounded waits of the bulk-copy linear rows that gave up on the current
 // device since the count was last cleared (read on `s`, which is then
