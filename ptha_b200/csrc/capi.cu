@@ -259,7 +259,7 @@ int evolve_t(swals_domain *d, double timestep, int has_dt)
         if (e != cudaSuccess) return cuda_fail(e, "update_max_quantities");
     }
     cudaError_t e = cudaSuccess;
-    bool gauges_fused = false;   // the linear step kernel recorded the gauges
+    bool gauges_fused = false;   // the step's own kernels recorded the gauges
     if (d->static_pending) {
         // static_before_time (domain_mod.f90:1706-1716): the clock decides
         // on the host, one read per step until it has passed.
@@ -330,15 +330,22 @@ int evolve_t(swals_domain *d, double timestep, int has_dt)
         buf.partials = d->lines;
         buf.partials_len = 5 * (2 * d->nx + 2 * d->ny);
         buf.edges = d->edges;
+        // the step's finalize kernel records the gauges from its final planes
+        StepConfig cg = c;
+        cg.g_sites = d->d_sites;
+        cg.g_n = d->n_gauges;
+        cg.g_records = d->d_records;
+        cg.g_capacity = d->gauge_capacity;
+        gauges_fused = d->n_gauges > 0;
         if (d->method == M_MIDPOINT)
             e = launch_midpoint_step<R>(pl, d->cur, (R *)d->elv, max_stage, (R *)d->manning_sq, d->nx, d->ny,
-                                        d->pitch, m, c, has_dt != 0, timestep, buf, d->sc, d->stream, hook);
+                                        d->pitch, m, cg, has_dt != 0, timestep, buf, d->sc, d->stream, hook);
         else if (d->method == M_RK2N)
             e = launch_rk2n_step<R>(pl, d->cur, (R *)d->elv, max_stage, (R *)d->manning_sq, d->nx, d->ny, d->pitch,
-                                    m, c, has_dt != 0, timestep, buf, d->sc, d->stream, hook);
+                                    m, cg, has_dt != 0, timestep, buf, d->sc, d->stream, hook);
         else
             e = launch_rk2_step<R>(pl, d->cur, (R *)d->elv, max_stage, (R *)d->manning_sq, d->nx, d->ny, d->pitch,
-                                   m, c, has_dt != 0, timestep, d->method == M_EULER, buf, d->sc, d->stream, hook);
+                                   m, cg, has_dt != 0, timestep, d->method == M_EULER, buf, d->sc, d->stream, hook);
         if (e != cudaSuccess) return cuda_fail(e, "finite-volume step");
     } else {
         return fail(SWALS_ERR_UNSUPPORTED, "timestepping_method '%s' is not implemented on the GPU path",

@@ -421,13 +421,52 @@ cudaError_t launch_boundary(const BcArgs<R> &b, cudaStream_t s)
 enum { FIN_RK2 = 0, FIN_EULER = 1, FIN_MIDPOINT = 2, FIN_RK2N = 3 };
 constexpr int RK2N_N = 5;   // rk2n_n_value (domain_mod.f90:90)
 
+// The step's point gauges, recorded by the finalize kernel from the step's
+// final planes (n = 0: none): records[rec][g][STG, UH, VH], as the
+// separate gauge kernel stores them.
+template <typename R>
+struct FinGauges {
+    const R *stg, *uh, *vh;
+    int64_t P;
+    const int *sites;
+    int n;
+    double *records;
+    int capacity;
+};
+
+template <typename R>
+FinGauges<R> fin_gauges(const StepConfig &c, R *const pl[3], int64_t pitch)
+{
+    FinGauges<R> g{};
+    if (c.g_n > 0) {
+        g.stg = pl[0]; g.uh = pl[1]; g.vh = pl[2];
+        g.P = pitch;
+        g.sites = c.g_sites;
+        g.n = c.g_n;
+        g.records = c.g_records;
+        g.capacity = c.g_capacity;
+    }
+    return g;
+}
+
 template <typename R, int KIND>
 __global__ void __launch_bounds__(1024) rk2_finalize_kernel(int nx, int ny, int n_ext, const double *lines,
                                                             int dt_from_cfl, double dt_fixed, double max_dt_inv_init,
-                                                            DevScalars *sc)
+                                                            DevScalars *sc, FinGauges<R> g)
 {
     constexpr int NSETS = (KIND == FIN_EULER) ? 1 : (KIND == FIN_RK2N) ? RK2N_N : 2;
     __shared__ double red[4 * NSETS][32];
+    // gauges first: every read of the record count precedes thread 0's update
+    // below (the __syncthreads of the reduction lies between)
+    const int rec = g.n ? sc->gauge_records : 0;
+    if (rec < g.capacity)
+        for (int q = threadIdx.x; q < g.n; q += blockDim.x) {
+            const int64_t o = (int64_t)g.sites[2 * q + 1] * g.P + g.sites[2 * q];
+            double *dst = g.records + ((int64_t)rec * g.n + q) * 3;
+            dst[0] = (double)g.stg[o];
+            dst[1] = (double)g.uh[o];
+            dst[2] = (double)g.vh[o];
+        }
     double acc[4 * NSETS];
 #pragma unroll
     for (int k = 0; k < 4 * NSETS; k++) acc[k] = 0.0;
@@ -511,6 +550,7 @@ __global__ void __launch_bounds__(1024) rk2_finalize_kernel(int nx, int ny, int 
     sc->evolve_step_dt = sc->time - time0;
     sc->nsteps_advanced += 1;
     sc->max_dt_inv_bits = 0ull;
+    if (g.n) sc->gauge_records = rec + 1;
 }
 
 template <typename R, int MODE, bool SPH, bool COR, int FRIC, bool EDDY>
@@ -989,7 +1029,8 @@ cudaError_t launch_rk2_step(R *const planes[3][3], int &cur, R *elv, R *max_stag
         }
         hook(CAT_FINALIZE, 0);
         rk2_finalize_kernel<R, FIN_EULER><<<1, 1024, 0, s>>>(nx, ny, c.exterior_cells_width, lines1,
-                                                             a.dt_from_cfl, dt, max_dt_inv_init, sc);
+                                                             a.dt_from_cfl, dt, max_dt_inv_init, sc,
+                                                             fin_gauges<R>(c, planes[B], pitch));
         hook(CAT_FINALIZE, 1);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         cur = B;
@@ -1013,7 +1054,8 @@ cudaError_t launch_rk2_step(R *const planes[3][3], int &cur, R *elv, R *max_stag
         }
         hook(CAT_FINALIZE, 0);
         rk2_finalize_kernel<R, FIN_RK2><<<1, 1024, 0, s>>>(nx, ny, c.exterior_cells_width, lines1, a.dt_from_cfl,
-                                                           dt, max_dt_inv_init, sc);
+                                                           dt, max_dt_inv_init, sc,
+                                                           fin_gauges<R>(c, planes[C], pitch));
         hook(CAT_FINALIZE, 1);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         cur = C;
@@ -1044,7 +1086,7 @@ cudaError_t launch_rk2_step(R *const planes[3][3], int &cur, R *elv, R *max_stag
     }
     hook(CAT_FINALIZE, 0);
     rk2_finalize_kernel<R, FIN_RK2><<<1, 1024, 0, s>>>(nx, ny, c.exterior_cells_width, lines1, a.dt_from_cfl,
-                                              dt, max_dt_inv_init, sc);
+                                              dt, max_dt_inv_init, sc, fin_gauges<R>(c, planes[C], pitch));
     hook(CAT_FINALIZE, 1);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     cur = C;
@@ -1123,7 +1165,8 @@ cudaError_t launch_midpoint_step(R *const planes[3][3], int &cur, R *elv, R *max
     }
     hook(CAT_FINALIZE, 0);
     rk2_finalize_kernel<R, FIN_MIDPOINT><<<1, 1024, 0, s>>>(nx, ny, c.exterior_cells_width, lines1,
-                                                            has_dt ? 0 : 1, dt, a.max_dt_inv_init, sc);
+                                                            has_dt ? 0 : 1, dt, a.max_dt_inv_init, sc,
+                                                            fin_gauges<R>(c, planes[C], pitch));
     hook(CAT_FINALIZE, 1);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     cur = C;
@@ -1184,7 +1227,7 @@ cudaError_t launch_rk2n_step(R *const planes[3][3], int &cur, R *elv, R *max_sta
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     hook(CAT_FINALIZE, 0);
     rk2_finalize_kernel<R, FIN_RK2N><<<1, 1024, 0, s>>>(nx, ny, c.exterior_cells_width, lines, has_dt ? 0 : 1,
-                                              dt_sub, a.max_dt_inv_init, sc);
+                                              dt_sub, a.max_dt_inv_init, sc, fin_gauges<R>(c, planes[U5], pitch));
     hook(CAT_FINALIZE, 1);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     cur = U5;

@@ -86,7 +86,8 @@ struct StepConfig {
     const ForcingPatch *forcing;
     void *eddy_visc;        // use_eddy_viscosity: one plane of per-cell eddy viscosity, else null
     double eddy_visc_constants[2];  // domain%eddy_visc_constants (constant, Shiono-Knight)
-    // Point gauges a linear step may record itself (linear_step_fuses_gauges):
+    // Point gauges the step records itself (finite-volume steps always, in
+    // their finalize kernel; linear steps when linear_step_fuses_gauges):
     // 0-based (i, j) sites, records[rec][g][STG, UH, VH], capacity records.
     const int *g_sites;
     int g_n;
