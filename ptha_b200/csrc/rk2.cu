@@ -303,9 +303,12 @@ __device__ __forceinline__ R bc_get(const BcArgs<R> &a, int i, int r, int v)
     return pl[(int64_t)r * a.P + i];
 }
 
-// West/east pass value of ring cell (i, r), i in {0, nx-1}.
+// West/east pass value of ring cell (i, r), i in {0, nx-1}.  fs, fe: the
+// boundary function's stage and elevation at column i (KIND 2; the device
+// boundary functions do not depend on the row, so a corner thread evaluates
+// the function once for its own cell and its column neighbour).
 template <typename R, int KIND>
-__device__ __forceinline__ RingVal<R> we_value(const BcArgs<R> &a, int i, int r, double t)
+__device__ __forceinline__ RingVal<R> we_value(const BcArgs<R> &a, int i, int r, double t, R fs, R fe)
 {
     const int in = (i == 0) ? 1 : a.nx - 2;
     RingVal<R> v;
@@ -317,7 +320,8 @@ __device__ __forceinline__ RingVal<R> we_value(const BcArgs<R> &a, int i, int r,
         flather_cell<R>(a.bf, a.x, t, i, r, a.msl, i == 0, bc_get(a, in, r, 0), bc_get(a, in, r, 1),
                         bc_get(a, in, r, 2), a.elv[(int64_t)r * a.P + in], v.e, v.s, v.uh, v.vh);
     } else {
-        boundary_function<R>(a.bf, a.x, t, i, r, v.s, v.e);
+        v.s = fs;
+        v.e = fe;
         v.uh = bc_get(a, in, r, 1);
         v.vh = R(0);
     }
@@ -358,6 +362,8 @@ __global__ void __launch_bounds__(256) rk2_boundary_kernel(const BcArgs<R> a)
         if (a.dt_extra != R(0)) t = t + (double)(R(dtd) * a.dt_extra);
     }
 
+    R fs = R(0), fe = R(0);
+    if (KIND != 1 && KIND != 3) boundary_function<R>(a.bf, a.x, t, i, r, fs, fe);
     RingVal<R> v;
     if (sn) {
         const int rn = (r == 0) ? 1 : ny - 2;
@@ -365,7 +371,7 @@ __global__ void __launch_bounds__(256) rk2_boundary_kernel(const BcArgs<R> a)
         RingVal<R> nb;
         const bool nb_we = (i == 0 && a.bext[3]) || (i == nx - 1 && a.bext[1]);
         if (nb_we) {
-            nb = we_value<R, KIND>(a, i, rn, t);
+            nb = we_value<R, KIND>(a, i, rn, t, fs, fe);
         } else {
             nb.e = a.elv[(int64_t)rn * a.P + i];
             nb.s = bc_get(a, i, rn, 0); nb.uh = bc_get(a, i, rn, 1); nb.vh = bc_get(a, i, rn, 2);
@@ -376,12 +382,13 @@ __global__ void __launch_bounds__(256) rk2_boundary_kernel(const BcArgs<R> a)
             v.e = a.elv[(int64_t)r * a.P + i];
             flather_cell<R>(a.bf, a.x, t, i, r, a.msl, r == 0, nb.s, nb.vh, nb.uh, nb.e, v.e, v.s, v.vh, v.uh);
         } else {
-            boundary_function<R>(a.bf, a.x, t, i, r, v.s, v.e);
+            v.s = fs;
+            v.e = fe;
             v.uh = R(0);
             v.vh = nb.vh;
         }
     } else {
-        v = we_value<R, KIND>(a, i, r, t);
+        v = we_value<R, KIND>(a, i, r, t, fs, fe);
     }
 
     const int64_t o = (int64_t)r * a.P + i;
@@ -471,6 +478,7 @@ __global__ void __launch_bounds__(1024) rk2_finalize_kernel(int nx, int ny, int 
 #pragma unroll
     for (int k = 0; k < 4 * NSETS; k++) acc[k] = 0.0;
     const int L = 2 * nx + 2 * ny;
+#pragma unroll 4
     for (int q = threadIdx.x; q < L; q += blockDim.x) {
         int line, idx;
         if (q < nx) { line = 0; idx = q; }
@@ -495,14 +503,17 @@ __global__ void __launch_bounds__(1024) rk2_finalize_kernel(int nx, int ny, int 
         if (lane == 0) red[k][warp] = v;
     }
     __syncthreads();
-    if (threadIdx.x != 0) return;
+    // the warps' partial sums, combined by warp 0 (lane w holds warp w's)
+    if (warp != 0) return;
     const int nw = blockDim.x >> 5;
     double s[4 * NSETS];
+#pragma unroll
     for (int k = 0; k < 4 * NSETS; k++) {
-        double v = 0.0;
-        for (int w = 0; w < nw; w++) v += red[k][w];
+        double v = (lane < nw) ? red[k][lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
         s[k] = v;
     }
+    if (lane != 0) return;
     double bits_max = __longlong_as_double((long long)sc->max_dt_inv_bits);
     R max_dt_inv = R(fmax(max_dt_inv_init, bits_max));
     const double max_dt = (double)(R(1) / max_dt_inv);
