@@ -273,6 +273,7 @@ struct BcArgs {
     R *elv;
     const R *side;          // mode 2: saved pre-average outer two rings
     R *max_stage;
+    int pre_bf;             // column 0's boundary-function values from sc->bf_col0[n_dt - 1]
     int stage_mode;
     int dt_from_cfl;
     double dt_fixed;
@@ -363,7 +364,14 @@ __global__ void __launch_bounds__(256) rk2_boundary_kernel(const BcArgs<R> a)
     }
 
     R fs = R(0), fe = R(0);
-    if (KIND != 1 && KIND != 3) boundary_function<R>(a.bf, a.x, t, i, r, fs, fe);
+    if (KIND != 1 && KIND != 3) {
+        if (a.pre_bf && i == 0) {
+            fs = R(a.sc->bf_col0[a.n_dt - 1][0]);
+            fe = R(a.sc->bf_col0[a.n_dt - 1][1]);
+        } else {
+            boundary_function<R>(a.bf, a.x, t, i, r, fs, fe);
+        }
+    }
     RingVal<R> v;
     if (sn) {
         const int rn = (r == 0) ? 1 : ny - 2;
@@ -668,6 +676,20 @@ __global__ void __launch_bounds__(256, SWALS_UPDATE_MINB) rk2_update_kernel(cons
     const int i0 = (blockIdx.x * 32 + threadIdx.x) * NC;
     const int r = blockIdx.y * 8 + threadIdx.y;
     const int nx = a.nx, ny = a.ny;
+    if (a.pre_bf && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0 && threadIdx.y < 2) {
+        // Column 0's boundary-function values at the step's two stage
+        // boundaries (time + dt, time + dt + dt, as the boundary kernel forms
+        // them), one per warp, off the boundary kernels' critical path.
+        const double bits_max = __longlong_as_double((long long)a.sc->max_dt_inv_bits);
+        const R inv = R(fmax(a.max_dt_inv_init, bits_max));
+        const double dtd = (double)(R(1) / inv);
+        double t = a.sc->time + dtd;
+        if (threadIdx.y == 1) t = t + dtd;
+        R fs, fe;
+        boundary_function<R>(a.bf, a.bf_x, t, 0, 0, fs, fe);
+        a.sc->bf_col0[threadIdx.y][0] = (double)fs;
+        a.sc->bf_col0[threadIdx.y][1] = (double)fe;
+    }
     long long negfix = 0;
     if (i0 < nx && r < ny) {
         const int64_t o0 = (int64_t)r * a.P + i0;
@@ -876,6 +898,9 @@ Rk2Args<R> fv_args(int nx, int ny, int64_t pitch, R *elv, R *manning_sq, const M
     a.ev_c1 = R(c.eddy_visc_constants[0]);
     a.ev_c2 = R(c.eddy_visc_constants[1]);
     if (!a.ev) a.flux_variant &= ~FLUX_EDDY;
+    a.pre_bf = 0;
+    a.bf = c.bf;
+    a.bf_x = m.x;
     return a;
 }
 
@@ -894,6 +919,7 @@ BcArgs<R> bc_args(const Rk2Args<R> &a, const StepConfig &c, double dt)
     b.n_dt = 1;
     b.stage_mode = 1;
     b.leapfrog_half = 0;
+    b.pre_bf = a.pre_bf;
     return b;
 }
 
@@ -941,6 +967,7 @@ cudaError_t first_stage(Rk2Args<R> &a, R *const planes[3][3], int A, int B, bool
     a.dt_from_cfl = has_dt ? 0 : 1;
     a.write_cfl = has_dt ? 1 : 0;
     a.lines = lines;
+    if (!stored) a.pre_bf = 0;   // only the update kernel stores the boundary-function values
     hook(CAT_STAGE1, 0);
     e = stored ? dispatch_update<R>(a, c, s) : dispatch_stage<R, MODE_STAGE1>(a, c, s);
     hook(CAT_STAGE1, 1);
@@ -1024,8 +1051,11 @@ cudaError_t launch_rk2_step(R *const planes[3][3], int &cur, R *elv, R *max_stag
     const double max_dt_inv_init = (double)(R(1) / R(c.maximum_timestep));
     cudaError_t e;
 
-    // Stage 1: U0 -> B
+    // Stage 1: U0 -> B.  With the stage-from-function boundary (bc_kind 2)
+    // the stage-1 update kernel (adaptive steps) evaluates column 0's
+    // boundary function for the two stage boundaries (n_dt 1 and 2 below).
     Rk2Args<R> a = fv_args<R>(nx, ny, pitch, elv, manning_sq, m, c, dt, buf, sc);
+    a.pre_bf = (c.bc_kind == 2) ? 1 : 0;
     e = first_stage<R>(a, planes, A, B, has_dt, buf, lines1, c, s, hook);
     if (e != cudaSuccess) return e;
 
@@ -1283,6 +1313,7 @@ cudaError_t launch_leapfrog_boundary(int nx, int ny, int64_t pitch, R *stg, R *u
     b.dt_from_cfl = 0; b.dt_fixed = (double)dt; b.max_dt_inv_init = 0.0;
     b.n_dt = 0; b.dt_extra = R(0); b.sc = sc;
     b.leapfrog_half = 1;
+    b.pre_bf = 0;
     return launch_boundary<R>(b, s);
 }
 template cudaError_t launch_leapfrog_boundary<double>(int, int, int64_t, double *, double *, double *, double *,

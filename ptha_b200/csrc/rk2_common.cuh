@@ -50,6 +50,9 @@ struct Rk2Args {
     int base0;                     // stage 1 updates U0 (stg0..) with this state's fluxes (midpoint)
     R *ev;                         // per-cell eddy viscosity of the stage input (FLUX_EDDY), else null
     R ev_c1, ev_c2;                // eddy_visc_constants
+    int pre_bf;                    // stage-1 update: store sc->bf_col0 for the step's two stage boundaries
+    BoundaryFn bf;                 // ... of this boundary function, cell-centre x coordinates bf_x
+    const R *bf_x;
 };
 
 template <typename R> struct Cell { R stg, dep, u, v, elv; };

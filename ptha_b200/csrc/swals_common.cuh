@@ -197,6 +197,9 @@ struct DevScalars {
     double evolve_step_dt;
     int    gauge_records;      // number of gauge records written
     int    blocks_done;        // CTAs of the running step kernel past their gauge records (reset by the last)
+    double bf_col0[2][2];      // the boundary function's (stage, elevation) at column 0 for times
+                               // time + dt and time + 2 dt of an adaptive rk2 step (its stage-1
+                               // update kernel writes them; the stage-boundary kernels read them)
 };
 
 // Boundary-function parameters (SWALS_BF_*), evaluated on the device.
