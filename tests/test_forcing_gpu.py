@@ -97,6 +97,32 @@ def test_fv_rise_time_source(method, adaptive):
     assert g.state().time > 30.0
 
 
+@pytest.mark.parametrize("method", ["euler", "rk2"])
+def test_fv_forcing_with_stage_boundary(method):
+    """A rise-time source on the beach whose solitary wave enters through the
+    stage-from-function west boundary, adaptive dt: the step's boundary
+    updates (time + dt after stage 1, time + 2 dt after rk2's second Euler
+    stage, each followed by the forcing) take column 0's boundary stage from
+    the values the stage-1 update evaluated; bit for bit with the oracle."""
+    n = 96
+    kw, U, _, nsq = workloads.rk2_beach(n=n, dx=10.0 * 2048 / n, toe=17580.0 * n / 2048)
+    kw = dict(kw)
+    kw["timestepping_method"] = method
+    g, o = make_pair(kw, U, manning_sq=nsq)
+    i0, i1, j0, j1 = 4, 11, 30, 60      # offshore of the beach toe's shoreline
+    S = _source(n, i0, i1, j0, j1, amp=0.3)
+    work = np.stack([S, 0.01 * S, -0.02 * S])
+    for dom in (g, o):
+        dom.add_forcing_patch(i0, i1, j0, j1, 1, 3, 0.0, 200.0, work)
+    for _ in range(120):
+        g.evolve_one_step()
+        o.evolve_one_step()
+    _exact(g, o, f"{method} forcing + stage boundary")
+    assert g.state().time == o.time
+    assert np.max(o.max_stage[1:-1, 1]) > 1.0, "the boundary wave never entered"
+    g.close()
+
+
 @pytest.mark.parametrize("method,truely_linear,coriolis", [
     ("linear", True, False), ("linear", False, False), ("linear", True, True),
     ("leapfrog_linear_plus_nonlinear_friction", True, True),
