@@ -122,5 +122,5 @@ def test_torch_autograd_function():
     loss.backward()
     d.set_U(U)
     L2, g = d.misfit_gradient(nsteps, dt, target.cpu().numpy(), checkpoint_every=10)
-    assert float(loss) == pytest.approx(L2, rel=1e-12)
+    assert float(loss.detach()) == pytest.approx(L2, rel=1e-12)
     assert np.allclose(eta.grad.cpu().numpy(), g[0][window], rtol=1e-10, atol=1e-20)
